@@ -1,0 +1,214 @@
+/*
+ * lfx.h -- C ABI of the B200-native Krylov-solve path for LFRic-style
+ * extruded-mesh finite-element operators (single GPU, sm_100a).
+ *
+ * Drop-in surface: the three abstract types a Krylov solver of the reference
+ * talks to, plus an optional whole-solve object.
+ *   abstract_vector_type          infrastructure/source/field/vector_mod.F90:17-189
+ *   abstract_linear_operator_type components/science/source/solver/sci_linear_operator_mod.f90:18-36
+ *   abstract_preconditioner_type  components/science/source/solver/sci_preconditioner_mod.f90:19-38
+ *   abstract_iterative_solver_type components/science/source/solver/sci_iterative_solver_mod.f90:38-57
+ * A Fortran shim (lfric_core_b200/fortran/lfx_device_mod.f90) extends each
+ * abstract type with one bind(C) call per type-bound procedure.
+ *
+ * Conventions
+ *  - Every function returns an lfx_status; 0 is success. No function aborts;
+ *    lfx_last_error() gives the message of the last failure on a context.
+ *  - Array arguments are the reference's native arrays: dof ids and cell ids
+ *    are 1-based, multi-dimensional arrays are in Fortran (column-major)
+ *    order. Scalars are double at the ABI (the reference's r_def).
+ *  - Data passed at create time is copied to the device; the caller may free
+ *    its arrays afterwards.
+ *  - Objects belong to one context; a context owns one CUDA stream and is
+ *    used from one host thread at a time. Operations are stream-ordered;
+ *    functions that return a scalar (dot, norm) synchronise the stream.
+ */
+#ifndef LFX_H
+#define LFX_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LFX_OK = 0,
+  LFX_NOT_CONVERGED = 1,
+  LFX_NAN_DETECTED = 2,
+  LFX_OUT_OF_MEMORY = 3,
+  LFX_INVALID_ARGUMENT = 4,
+  LFX_TYPE_MISMATCH = 5,
+  LFX_TIMEOUT = 6,
+  LFX_CUDA_ERROR = 7,
+  LFX_NOT_SUPPORTED = 8
+} lfx_status;
+
+/* storage precision of a vector or operator: r_def (FP64) or r_solver (FP32) */
+enum { LFX_R64 = 64, LFX_R32 = 32 };
+
+typedef struct lfx_ctx lfx_ctx;
+typedef struct lfx_vec lfx_vec;
+typedef struct lfx_op lfx_op;
+typedef struct lfx_prec lfx_prec;
+typedef struct lfx_cma lfx_cma;
+typedef struct lfx_solver lfx_solver;
+
+/* ------------------------------------------------------------------ context */
+int lfx_ctx_create(int device, lfx_ctx** out);
+int lfx_ctx_destroy(lfx_ctx* ctx);
+const char* lfx_last_error(const lfx_ctx* ctx);
+int lfx_ctx_synchronize(lfx_ctx* ctx);
+/* the context's cudaStream_t, for callers that time or order work around it */
+void* lfx_ctx_stream(lfx_ctx* ctx);
+/* device bytes currently held by objects of this context */
+int64_t lfx_ctx_device_bytes(const lfx_ctx* ctx);
+
+/* ------------------------------------------------------------------ vectors
+ * field_vector_type (sci_field_vector_mod.x90:24-468) and, for precision 32,
+ * r_solver_field_vector_type (sci_r_solver_field_vector_mod.x90:26-479):
+ * nfields fields of undf[i] values each. Inner products always accumulate
+ * in FP64 (sci_psykal_light_mod.f90:72-214). */
+int lfx_vec_create(lfx_ctx* ctx, int32_t nfields, const int64_t* undf, int32_t precision,
+                   lfx_vec** out);
+/* duplicate: same shape and precision, contents undefined (vector_mod duplicate) */
+int lfx_vec_duplicate(const lfx_vec* src, lfx_vec** out);
+int lfx_vec_destroy(lfx_vec* v);
+int lfx_vec_set_scalar(lfx_vec* v, double scalar);                      /* setval_c      */
+int lfx_vec_axpy(lfx_vec* y, double alpha, const lfx_vec* x);           /* y = y + a x   */
+int lfx_vec_aypx(lfx_vec* y, double alpha, const lfx_vec* x);           /* y = a y + x   */
+int lfx_vec_axpby(lfx_vec* z, double a, const lfx_vec* x, double b, const lfx_vec* y);
+int lfx_vec_norm(const lfx_vec* v, double* out);                        /* sqrt(sum v^2) */
+int lfx_vec_field_norm(const lfx_vec* v, int32_t position, double* out);/* 1-based field */
+int lfx_vec_dot(const lfx_vec* v, const lfx_vec* x, double* out);
+int lfx_vec_scale(lfx_vec* v, double scalar);
+int lfx_vec_copy(lfx_vec* dst, const lfx_vec* src);                     /* dst = src     */
+int lfx_vec_size(const lfx_vec* v, int32_t* nfields);
+/* import_field / export_field (sci_field_vector_mod.x90:294-334): host FP64
+ * data of field `position` (1-based); converts to/from FP32 storage. */
+int lfx_vec_import_field(lfx_vec* v, int32_t position, const double* host, int64_t n);
+int lfx_vec_export_field(const lfx_vec* v, int32_t position, double* host, int64_t n);
+/* raw device pointer of a field (for zero-copy callers); precision tells the type */
+int lfx_vec_field_device_ptr(const lfx_vec* v, int32_t position, void** out);
+
+/* ------------------------------------------------------------------ operators
+ * LMA operator (operator_type, operator_mod.t90:31-122) applied as the
+ * reference's matrix_vector_kernel over a cell colouring
+ * (sci_mass_matrix_operator_alg_mod.x90:98, matrix_vector_kernel_mod.F90:107-140):
+ * y is overwritten with A x. Colour order fixes the summation order, which the
+ * device reproduces bit for bit in FP64.
+ *   map_to / map_from   Fortran (ndf, ncell_2d): dof id of layer 0 of each local dof
+ *   local_stencil       Fortran (ncell_2d*nlayers, ndf_to, ndf_from)
+ *   cells_in_colour     Fortran (ncolours, max_cells_per_colour), 1-based cell ids
+ *   precision           device storage: LFX_R64, or LFX_R32 (rounded copy) */
+int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_to,
+                   int32_t ndf_from, const int32_t* map_to, const int32_t* map_from,
+                   int64_t undf_to, int64_t undf_from, const double* local_stencil,
+                   int32_t ncolours, const int32_t* ncells_per_colour,
+                   const int32_t* cells_in_colour, int32_t max_cells_per_colour,
+                   int32_t precision, lfx_op** out);
+/* A second operator sharing the dofmaps and colouring of `src` but holding
+ * its own local matrices (e.g. the FP32 copy of an FP64 operator). */
+int lfx_lma_create_like(const lfx_op* src, const double* local_stencil, int32_t precision,
+                        lfx_op** out);
+int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y);
+int lfx_op_destroy(lfx_op* op);
+/* diag(A) by mm_diagonal_kernel (sci_mm_diagonal_kernel_mod.F90:99-125) */
+int lfx_lma_diagonal(lfx_op* op, lfx_vec* diag);
+/* transpose apply y = A^T x for a matrix stored as (ncell_3d, ndf_to, ndf_from)
+ * (transpose_matrix_vector_kernel_mod.F90); y is overwritten */
+int lfx_op_apply_transpose(lfx_op* op, const lfx_vec* x, lfx_vec* y);
+
+/* ------------------------------------------------------------------ CMA
+ * columnwise_operator_type (columnwise_operator_mod.f90:42-469): one banded
+ * matrix columnwise_matrix(bandwidth, nrow, ncell_2d) per column.
+ *   first_dof[c]   dof id (1-based) of the column's first dof (map(1) of the
+ *                  CMA space, which may point into a larger vector)
+ *   indirection    (nrow) indirection_dofmap, 1-based offsets within a column */
+int lfx_cma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nrow, int32_t ncol,
+                   int32_t bandwidth, int32_t alpha, int32_t beta, int32_t gamma_m,
+                   int32_t gamma_p, const int32_t* first_dof, const int32_t* indirection,
+                   const double* columnwise_matrix, lfx_cma** out);
+/* columnwise_op_asm (sci_columnwise_op_asm_kernel_mod.F90:72-128) on the
+ * device: assembles the band from the sub-block of an FP64 LMA operator
+ * formed by its local dofs `dfs` (1-based, nsub of them), which must map to
+ * the column's rows through column_banded_dofmap (Fortran (nsub, nlayers)). */
+int lfx_cma_assemble_from_lma(const lfx_op* lma, int32_t nsub, const int32_t* dfs,
+                              const int32_t* column_banded_dofmap, int32_t alpha,
+                              int32_t beta, int32_t gamma_m, int32_t gamma_p,
+                              int32_t bandwidth, int32_t nrow, const int32_t* first_dof,
+                              const int32_t* indirection, lfx_cma** out);
+/* copy of the band back to the host, Fortran (bandwidth, nrow, ncell_2d) */
+int lfx_cma_get_band(const lfx_cma* cma, double* band);
+/* y += A x (columnwise_op_app_kernel_mod.F90:73-124) */
+int lfx_cma_apply(lfx_cma* cma, const lfx_vec* x, lfx_vec* y);
+int lfx_cma_destroy(lfx_cma* cma);
+
+/* ------------------------------------------------------------------ preconditioners
+ * apply writes y = P^{-1} x (sci_preconditioner_mod.f90:19-38). */
+int lfx_null_prec_create(lfx_ctx* ctx, lfx_prec** out);                 /* y = x        */
+int lfx_diag_prec_create(lfx_ctx* ctx, const lfx_vec* diag, lfx_prec** out); /* y = x/diag */
+/* Column-tridiagonal (Thomas, columnwise_op_appinv_kernel_mod.F90:77-145) on
+ * the rows the CMA covers, y = x / diag on every other row (diag may be NULL
+ * if the CMA covers all rows). The factorisation is done once, in FP64.
+ * precision selects the vectors it will be applied to. */
+int lfx_cma_prec_create(lfx_ctx* ctx, const lfx_cma* cma, const lfx_vec* diag,
+                        int32_t precision, lfx_prec** out);
+int lfx_prec_apply(lfx_prec* p, const lfx_vec* x, lfx_vec* y);
+int lfx_prec_destroy(lfx_prec* p);
+
+/* ------------------------------------------------------------------ solvers
+ * Device-resident Krylov solves (sci_iterative_solver_mod.f90): every
+ * scalar recurrence stays on the device; the host only launches work and
+ * polls a convergence flag. */
+enum {
+  LFX_SOLVER_CG = 1,        /* cg_solve       :495-592  */
+  LFX_SOLVER_BICGSTAB = 2,  /* bicgstab_solve :645-779  */
+  LFX_SOLVER_GMRES = 3      /* gmres_solve    :830-1003 */
+};
+
+typedef struct {
+  double r_tol;                  /* relative tolerance                       */
+  double a_tol;                  /* absolute tolerance                       */
+  int32_t max_iter;              /* iterations (CG/BiCGStab) or cycles (GMRES) */
+  int32_t gcrk;                  /* GMRES restart length                     */
+  int32_t monitor_convergence;   /* 0: run exactly max_iter, as the reference */
+  int32_t fail_on_non_converged; /* 1: return LFX_NOT_CONVERGED              */
+} lfx_solver_cfg;
+
+typedef struct {
+  int32_t iterations;   /* iterations (CG/BiCGStab) or restart cycles (GMRES) */
+  int32_t converged;
+  double initial_norm;  /* ||b - A x0||                                       */
+  double final_norm;    /* last monitored residual norm                       */
+  double final_rel;     /* last monitored relative residual                   */
+  int32_t applies;      /* operator applications                              */
+  int32_t status;       /* lfx_status of the solve                            */
+  int32_t outer_iterations; /* refinement steps (refined solver only)         */
+  int32_t inner_iterations; /* total inner iterations (refined solver only)   */
+} lfx_solve_info;
+
+int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
+                      const lfx_solver_cfg* cfg, lfx_solver** out);
+/* x: initial guess on entry, solution on exit; b unchanged */
+int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info* info);
+int lfx_solver_destroy(lfx_solver* s);
+
+/* Mixed-precision solve with FP64 iterative refinement: the residual
+ * b - A x and the solution update stay FP64 (op64, FP64 vectors); each
+ * correction comes from `inner` (typically an FP32 GMRES on an FP32 copy of
+ * the operator) solved to inner_rtol. Converged when ||b - A x||/||b - A x0||
+ * <= cfg->r_tol, with at most cfg->max_iter refinement steps. */
+int lfx_refined_solver_create(lfx_ctx* ctx, lfx_op* op64, lfx_solver* inner,
+                              double inner_rtol, const lfx_solver_cfg* cfg,
+                              lfx_solver** out);
+
+/* Per-kernel device timing of the operator apply inside solves: when
+ * enabled, CUDA events bracket every LMA apply launched by solvers of this
+ * context; lfx_ctx_apply_timing returns the count and total milliseconds
+ * accumulated since the last reset. */
+int lfx_ctx_enable_apply_timing(lfx_ctx* ctx, int32_t enable);
+int lfx_ctx_apply_timing(lfx_ctx* ctx, int64_t* launches, double* total_ms, int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

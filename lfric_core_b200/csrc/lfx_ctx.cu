@@ -1,0 +1,182 @@
+// Context: stream, error reporting, device memory accounting, reduction
+// scratch and the optional per-apply timing of solves.
+#include <cstdio>
+#include <cstring>
+
+#include "lfx_internal.cuh"
+
+namespace lfx {
+
+int fail(lfx_ctx* ctx, int status, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return status;
+}
+
+int cuda_fail(lfx_ctx* ctx, cudaError_t e, const char* what) {
+  if (ctx) ctx->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? LFX_OUT_OF_MEMORY : LFX_CUDA_ERROR;
+}
+
+int dmalloc(lfx_ctx* ctx, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return LFX_OK;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(ctx, LFX_OUT_OF_MEMORY,
+                "device allocation of " + std::to_string(bytes) + " bytes failed: " +
+                    cudaGetErrorString(e));
+  }
+  ctx->device_bytes += (int64_t)bytes;
+  return LFX_OK;
+}
+
+void dfree(lfx_ctx* ctx, void* p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  ctx->device_bytes -= (int64_t)bytes;
+}
+
+int ensure_partials(lfx_ctx* ctx, int64_t n, int nsums) {
+  int64_t need = nchunks(n) * nsums;
+  if (need < 1) need = 1;
+  if (need <= ctx->partials_cap) return LFX_OK;
+  // never reallocate while a graph capture is recording
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(ctx->stream, &cs);
+  if (cs != cudaStreamCaptureStatusNone)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "reduction scratch too small inside a capture");
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, ctx->d_partials, sizeof(double) * ctx->partials_cap);
+  ctx->d_partials = nullptr;
+  ctx->partials_cap = 0;
+  int64_t cap = need * 2;
+  int rc = dmalloc(ctx, (void**)&ctx->d_partials, sizeof(double) * cap);
+  if (rc) return rc;
+  ctx->partials_cap = cap;
+  return LFX_OK;
+}
+
+void timing_begin(lfx_ctx* ctx) {
+  if (!ctx->time_applies) return;
+  if (ctx->ev_used + 2 > (int)ctx->ev_pool.size()) {
+    for (int i = 0; i < 64; ++i) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ctx->ev_pool.push_back(e);
+    }
+  }
+  cudaEventRecord(ctx->ev_pool[ctx->ev_used++], ctx->stream);
+}
+
+void timing_end(lfx_ctx* ctx) {
+  if (!ctx->time_applies) return;
+  cudaEventRecord(ctx->ev_pool[ctx->ev_used++], ctx->stream);
+}
+
+}  // namespace lfx
+
+using namespace lfx;
+
+extern "C" {
+
+int lfx_ctx_create(int device, lfx_ctx** out) {
+  if (!out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LFX_CUDA_ERROR;
+  }
+  if (device < 0 || device >= ndev) return LFX_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return LFX_CUDA_ERROR;
+  lfx_ctx* ctx = new lfx_ctx();
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return LFX_CUDA_ERROR;
+  }
+  int rc = dmalloc(ctx, (void**)&ctx->d_ticket, sizeof(unsigned) * 4);
+  if (!rc) rc = dmalloc(ctx, (void**)&ctx->d_scalars, sizeof(double) * 64);
+  if (!rc && cudaMemset(ctx->d_ticket, 0, sizeof(unsigned) * 4) != cudaSuccess) rc = LFX_CUDA_ERROR;
+  if (!rc && cudaMallocHost((void**)&ctx->h_scalars, sizeof(double) * 64) != cudaSuccess)
+    rc = LFX_OUT_OF_MEMORY;
+  if (!rc) rc = ensure_partials(ctx, (int64_t)RCHUNK * 4096, 1);
+  if (rc) {
+    lfx_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return LFX_OK;
+}
+
+int lfx_ctx_destroy(lfx_ctx* ctx) {
+  if (!ctx) return LFX_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+  dfree(ctx, ctx->d_partials, sizeof(double) * ctx->partials_cap);
+  dfree(ctx, ctx->d_ticket, sizeof(unsigned) * 4);
+  dfree(ctx, ctx->d_scalars, sizeof(double) * 64);
+  if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return LFX_OK;
+}
+
+const char* lfx_last_error(const lfx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int lfx_ctx_synchronize(lfx_ctx* ctx) {
+  if (!ctx) return LFX_INVALID_ARGUMENT;
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return LFX_OK;
+}
+
+void* lfx_ctx_stream(lfx_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int64_t lfx_ctx_device_bytes(const lfx_ctx* ctx) { return ctx ? ctx->device_bytes : 0; }
+
+int lfx_ctx_enable_apply_timing(lfx_ctx* ctx, int32_t enable) {
+  if (!ctx) return LFX_INVALID_ARGUMENT;
+  ctx->time_applies = enable != 0;
+  return LFX_OK;
+}
+
+// Folds the recorded event pairs into the running totals (the stream must be
+// idle, which lfx_solver_apply guarantees on return).
+static int collect_timing(lfx_ctx* ctx) {
+  for (int i = 0; i + 1 < ctx->ev_used; i += 2) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&ms, ctx->ev_pool[i], ctx->ev_pool[i + 1]);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaEventElapsedTime");
+    ctx->timed_ms += ms;
+    ctx->timed_launches += 1;
+  }
+  ctx->ev_used = 0;
+  return LFX_OK;
+}
+
+int lfx_ctx_apply_timing(lfx_ctx* ctx, int64_t* launches, double* total_ms, int32_t reset) {
+  if (!ctx) return LFX_INVALID_ARGUMENT;
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  int rc = collect_timing(ctx);
+  if (rc) return rc;
+  if (launches) *launches = ctx->timed_launches;
+  if (total_ms) *total_ms = ctx->timed_ms;
+  if (reset) {
+    ctx->timed_launches = 0;
+    ctx->timed_ms = 0.0;
+  }
+  return LFX_OK;
+}
+
+}  // extern "C"
+
+namespace lfx {
+// exported for the solver translation unit: drain events between solves so the
+// pool does not grow without bound
+int drain_timing(lfx_ctx* ctx) { return collect_timing(ctx); }
+}  // namespace lfx

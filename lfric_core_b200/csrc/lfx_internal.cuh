@@ -1,0 +1,251 @@
+// Internal definitions shared by the liblfx translation units.
+//
+// Reduction order (shared with the CPU oracle so FP64 results match bit for
+// bit): a vector of n values is cut into chunks of RCHUNK = 2048; in chunk j,
+// lane t (0..255) accumulates elements 2048 j + 256 m + t for m = 0..7 with
+// acc = fma(a, b, acc); each warp combines its 32 lanes with a xor butterfly
+// (16, 8, 4, 2, 1); the 8 warp sums are added left to right. The per-chunk
+// partials are reduced by the last block to finish (atomic ticket) in the same
+// way, lane t adding partials t, t + 256, ... in order. The result does not
+// depend on the grid size.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "lfx.h"
+
+struct lfx_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // reduction scratch: partials of up to 4 simultaneous sums, one ticket
+  double* d_partials = nullptr;
+  int64_t partials_cap = 0;  // doubles
+  unsigned* d_ticket = nullptr;
+  // small device scratch for scalar results of the C-ABI reductions
+  double* d_scalars = nullptr;
+  double* h_scalars = nullptr;  // pinned
+  int64_t device_bytes = 0;
+  // operator-apply timing inside solves
+  bool time_applies = false;
+  std::vector<cudaEvent_t> ev_pool;
+  int ev_used = 0;
+  int64_t timed_launches = 0;
+  double timed_ms = 0.0;
+};
+
+namespace lfx {
+
+constexpr int RT = 256;
+constexpr int RCHUNK = 2048;
+constexpr int RPER = RCHUNK / RT;  // 8 elements per lane per chunk
+
+// ---------------------------------------------------------------- errors
+int fail(lfx_ctx* ctx, int status, const std::string& msg);
+int cuda_fail(lfx_ctx* ctx, cudaError_t e, const char* what);
+
+#define LFX_CK(ctx, call)                                   \
+  do {                                                      \
+    cudaError_t _e = (call);                                \
+    if (_e != cudaSuccess) return lfx::cuda_fail((ctx), _e, #call); \
+  } while (0)
+
+// ---------------------------------------------------------------- memory
+int dmalloc(lfx_ctx* ctx, void** p, size_t bytes);
+void dfree(lfx_ctx* ctx, void* p, size_t bytes);
+int ensure_partials(lfx_ctx* ctx, int64_t n, int nsums);
+
+inline int64_t nchunks(int64_t n) { return (n + RCHUNK - 1) / RCHUNK; }
+inline int grid_for(const lfx_ctx* ctx, int64_t n) {
+  int64_t nc = nchunks(n);
+  int64_t cap = (int64_t)ctx->num_sms * 8;
+  int64_t g = nc < cap ? nc : cap;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// ---------------------------------------------------------------- device math
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+
+__device__ __forceinline__ double warp_butterfly(double v) {
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// block sum in the fixed order; result valid in thread 0
+__device__ __forceinline__ double block_sum(double acc, double* sm) {
+  acc = warp_butterfly(acc);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sm[w] = acc;
+  __syncthreads();
+  double tot = 0.0;
+  if (threadIdx.x == 0) {
+    tot = sm[0];
+#pragma unroll
+    for (int i = 1; i < RT / 32; ++i) tot = tot + sm[i];
+  }
+  __syncthreads();
+  return tot;
+}
+
+// Chunked elementwise kernel with NR fixed-order reductions.
+//   body(i, acc)  : work on element i, add into acc[0..NR)
+//   fin(tot)      : run by one thread after every chunk is done, tot[NR]
+// skip: optional device flag; when non-zero the kernel does nothing (used by
+// device-resident solvers to idle after convergence).
+template <int NR, class Body, class Fin>
+__global__ void __launch_bounds__(RT) chunk_kernel(int64_t n, Body body, Fin fin,
+                                                   double* partials, unsigned* ticket,
+                                                   const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  __shared__ double sm[RT / 32];
+  __shared__ int am_last;
+  const int64_t nch = (n + RCHUNK - 1) / RCHUNK;
+  for (int64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
+    const int64_t base = ch * RCHUNK + threadIdx.x;
+#pragma unroll
+    for (int m = 0; m < RPER; ++m) {
+      const int64_t i = base + (int64_t)m * RT;
+      if (i < n) body(i, acc);
+    }
+    if constexpr (NR > 0) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        double t = block_sum(acc[r], sm);
+        if (threadIdx.x == 0) partials[(int64_t)r * nch + ch] = t;
+      }
+    }
+  }
+  if constexpr (NR > 0) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (am_last) {
+      __threadfence();
+      double tot[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        double a = 0.0;
+        for (int64_t i = threadIdx.x; i < nch; i += RT) a = a + __ldcg(&partials[(int64_t)r * nch + i]);
+        tot[r] = block_sum(a, sm);
+      }
+      if (threadIdx.x == 0) {
+        fin(tot);
+        *ticket = 0u;
+      }
+    }
+  }
+}
+
+struct NoFin {
+  __device__ void operator()(const double*) const {}
+};
+
+template <int NR, class Body, class Fin>
+int launch_chunks(lfx_ctx* ctx, int64_t n, Body body, Fin fin, const int* skip = nullptr) {
+  if (NR > 0) {
+    int rc = ensure_partials(ctx, n, NR);
+    if (rc) return rc;
+  }
+  chunk_kernel<NR><<<grid_for(ctx, n), RT, 0, ctx->stream>>>(n, body, fin, ctx->d_partials,
+                                                              ctx->d_ticket, skip);
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
+}  // namespace lfx
+
+// ---------------------------------------------------------------- objects
+
+struct lfx_vec {
+  lfx_ctx* ctx = nullptr;
+  int32_t precision = LFX_R64;
+  std::vector<int64_t> undf;
+  std::vector<void*> data;
+  size_t elem() const { return precision == LFX_R64 ? 8 : 4; }
+};
+
+// Gather form of the coloured LMA apply: for every to-space "entity column"
+// (a run of consecutive dof ids touched by the same (cell, local dof) pairs)
+// the device keeps the contributing cells in colour order and, per cell, the
+// local dofs (df, vertical offset off) that land on the column. The dof
+// base+l then receives M(c; l-off, df, df2) * x(map_from(c, df2) + l - off) in
+// the reference's order: colour, cell, df2, df.
+struct lfx_lma_layout {
+  int32_t ncell_2d = 0, nlayers = 0, ndf_to = 0, ndf_from = 0;
+  int64_t undf_to = 0, undf_from = 0;
+  int32_t nent = 0, ngrp = 0, max_h = 0, max_off = 0;
+  bool full_cover = true;
+  // device arrays
+  int32_t* ent_base = nullptr;   // [nent] 0-based first dof
+  int32_t* ent_h = nullptr;      // [nent] height
+  int32_t* ent_grp = nullptr;    // [nent+1] group range
+  int32_t* grp_cell = nullptr;   // [ngrp] 0-based cell
+  uint32_t* grp_rec = nullptr;   // [ngrp] packed records
+  int32_t* map_from = nullptr;   // [ncell_2d*ndf_from] 0-based
+  int32_t* map_to = nullptr;     // [ncell_2d*ndf_to] 0-based
+  int refcount = 1;
+  std::vector<int32_t> rank;         // colour-loop position of every cell
+  lfx_lma_layout* tlay = nullptr;    // from-space layout for the transpose apply
+};
+
+struct lfx_op {
+  lfx_ctx* ctx = nullptr;
+  lfx_lma_layout* lay = nullptr;  // shared with ops made by lfx_lma_create_like
+  int32_t precision = LFX_R64;
+  void* mat = nullptr;  // [cell][df][df2][k]
+  size_t mat_bytes = 0;
+  double* mat64_raw = nullptr;  // FP64 operator keeps nothing else
+};
+
+struct lfx_cma {
+  lfx_ctx* ctx = nullptr;
+  int32_t ncell_2d = 0, nrow = 0, ncol = 0, bw = 0, alpha = 0, beta = 0, gamma_m = 0, gamma_p = 0;
+  int32_t* first_dof = nullptr;    // [ncell_2d] 0-based
+  int32_t* indirection = nullptr;  // [nrow] 0-based offsets
+  int32_t* ind_from = nullptr;     // [ncol] 0-based offsets
+  double* band = nullptr;          // Fortran (bw, nrow, ncell_2d)
+  std::vector<int32_t> h_first, h_ind;
+  int64_t max_row = 0;             // largest 0-based dof the columns touch
+};
+
+enum { PREC_NULL = 0, PREC_DIAG = 1, PREC_CMA = 2 };
+struct lfx_prec {
+  lfx_ctx* ctx = nullptr;
+  int kind = PREC_NULL;
+  int32_t precision = LFX_R64;  // for PREC_CMA: the vectors it applies to
+  const lfx_vec* diag = nullptr;  // not owned (PREC_DIAG)
+  // PREC_CMA: factors [row][column]
+  int32_t ncell_2d = 0, nrow = 0;
+  int32_t* first_dof = nullptr;
+  int32_t* indirection = nullptr;
+  void* fa = nullptr;     // sub-diagonal a_i
+  void* finv = nullptr;   // 1 / (b_i - a_i c'_{i-1})
+  void* fc = nullptr;     // c'_i
+  void* rdiag = nullptr;  // diagonal on uncovered rows, by run
+  int32_t nruns = 0;
+  int32_t* run_start = nullptr;
+  int32_t* run_len = nullptr;
+  int32_t* run_off = nullptr;  // offset of each run in rdiag
+  int64_t rdiag_n = 0;
+  size_t bytes = 0;
+  int64_t max_row = -1;  // PREC_CMA: largest 0-based dof the columns touch
+};
+
+namespace lfx {
+int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* skip);
+int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int64_t n,
+                    const int* skip);
+void timing_begin(lfx_ctx* ctx);
+void timing_end(lfx_ctx* ctx);
+}  // namespace lfx

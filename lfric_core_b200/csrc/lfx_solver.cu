@@ -1,0 +1,755 @@
+// Device-resident Krylov solvers: cg_solve, bicgstab_solve and gmres_solve of
+// components/science/source/solver/sci_iterative_solver_mod.f90 (:495-592,
+// :645-779, :830-1003), plus FP64 iterative refinement around a reduced-
+// precision inner solve.
+//
+// Every scalar of the recurrences lives in device memory and is updated by the
+// last block of the fused reduction kernel that produces it (see
+// chunk_kernel), so an iteration issues no host round trip. Kernels take a
+// "done" flag and return at once when it is set; the host launches work in
+// batches and reads the flag once per batch. Vector updates that the
+// reference performs as separate builtins are fused when the fusion does not
+// change a single rounding (e.g. t = r; t += a v  ==>  t = fma(a, v, r)).
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+
+#include "lfx_internal.cuh"
+
+namespace lfx {
+int drain_timing(lfx_ctx* ctx);
+}
+using namespace lfx;
+
+namespace {
+
+constexpr int MAX_GCRK = 64;
+constexpr double EPS_RDEF = DBL_EPSILON;  // constants_mod.F90:167
+
+struct DevState {
+  int done, converged, iter, status;
+  int applies, monitor, max_iter, pad;
+  double r_tol, a_tol;
+  double r_nrm_0, r_nrm, rz, alpha, neg_alpha, beta;
+  // bicgstab
+  double rho, rho_old, omega, coef, tt, ts, sc_err, err;
+  // gmres
+  double gbeta, inv_beta, res_norm, inv_hn;
+};
+
+struct VecPtrs {
+  const void* p[MAX_GCRK];
+};
+
+template <class T>
+struct Tsel {};
+
+}  // namespace
+
+struct lfx_solver {
+  lfx_ctx* ctx = nullptr;
+  int kind = 0;
+  lfx_op* op = nullptr;
+  lfx_prec* prec = nullptr;
+  lfx_solver_cfg cfg{};
+  int32_t precision = LFX_R64;
+  int64_t n = 0;
+  std::vector<void*> work;  // owned device vectors of n elements
+  DevState* d_state = nullptr;
+  DevState* h_state = nullptr;  // pinned
+  double* d_gm = nullptr;       // gmres: H, negH, g, u
+  // refined solver
+  lfx_solver* inner = nullptr;
+  double inner_rtol = 0.0;
+  lfx_vec *r32 = nullptr, *d32 = nullptr;
+  double* d_r64 = nullptr;
+};
+
+namespace {
+
+size_t esz(int32_t p) { return p == LFX_R64 ? 8 : 4; }
+
+int read_state(lfx_solver* s) {
+  lfx_ctx* ctx = s->ctx;
+  LFX_CK(ctx, cudaMemcpyAsync(s->h_state, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return LFX_OK;
+}
+
+int init_state(lfx_solver* s) {
+  DevState h{};
+  h.r_tol = s->cfg.r_tol;
+  h.a_tol = s->cfg.a_tol;
+  h.max_iter = s->cfg.max_iter;
+  h.monitor = s->cfg.monitor_convergence ? 1 : 0;
+  *s->h_state = h;
+  LFX_CK(s->ctx, cudaMemcpyAsync(s->d_state, s->h_state, sizeof(DevState), cudaMemcpyHostToDevice,
+                                 s->ctx->stream));
+  return LFX_OK;
+}
+
+// ------------------------------------------------------------------ CG
+template <class T>
+int cg_run(lfx_solver* s, T* x, const T* b) {
+  lfx_ctx* ctx = s->ctx;
+  DevState* S = s->d_state;
+  const int64_t n = s->n;
+  T* r = (T*)s->work[0];
+  T* p = (T*)s->work[1];
+  T* z = (T*)s->work[2];
+  const int* done = &S->done;
+  int rc;
+  // r = b - A x   (apply, scale(-1), axpy(1, b): one rounding, b - Ax)
+  if ((rc = op_apply_impl(s->op, x, r, b, nullptr))) return rc;
+  rc = launch_chunks<1>(
+      ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)r[i], a[0]); },
+      [=] __device__(const double* t) {
+        S->applies = 1;
+        S->r_nrm_0 = sqrt(t[0]);
+        if (S->r_nrm_0 < EPS_RDEF) {  // :531
+          S->done = 1;
+          S->converged = 1;
+          S->r_nrm = S->r_nrm_0;
+        }
+      });
+  if (rc) return rc;
+  if ((rc = prec_apply_impl(s->prec, s->precision, r, z, n, done))) return rc;
+  rc = launch_chunks<1>(
+      ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)z[i], a[0]); },
+      [=] __device__(const double* t) { S->rz = t[0]; }, done);
+  if (rc) return rc;
+  rc = launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { p[i] = z[i]; }, NoFin{}, done);
+  if (rc) return rc;
+  const bool diag_prec = s->prec->kind == PREC_DIAG;
+  const T* dg = (const T*)s->prec->rdiag;
+  for (;;) {
+    for (int it = 0; it < 8; ++it) {
+      if ((rc = op_apply_impl(s->op, p, z, nullptr, done))) return rc;  // z = A p
+      rc = launch_chunks<1>(
+          ctx, n,
+          [=] __device__(int64_t i, double* a) { a[0] = fma((double)p[i], (double)z[i], a[0]); },
+          [=] __device__(const double* t) {
+            S->applies += 1;
+            S->alpha = S->rz / t[0];
+            S->neg_alpha = -S->alpha;
+          },
+          done);
+      if (rc) return rc;
+      // x += alpha p ; r -= alpha z ; ||r||
+      rc = launch_chunks<1>(
+          ctx, n,
+          [=] __device__(int64_t i, double* a) {
+            const T al = (T)S->alpha, nal = (T)S->neg_alpha;
+            x[i] = fmaT(al, p[i], x[i]);
+            const T ri = fmaT(nal, z[i], r[i]);
+            r[i] = ri;
+            a[0] = fma((double)ri, (double)ri, a[0]);
+          },
+          [=] __device__(const double* t) {
+            S->iter += 1;
+            S->r_nrm = sqrt(t[0]);
+            if (S->monitor) {
+              if (S->r_nrm / S->r_nrm_0 <= S->r_tol || S->r_nrm <= S->a_tol) {  // :563
+                S->done = 1;
+                S->converged = 1;
+              } else if (isnan(S->r_nrm)) {
+                S->done = 1;
+                S->status = LFX_NAN_DETECTED;
+              }
+            }
+            if (S->iter >= S->max_iter) S->done = 1;
+          },
+          done);
+      if (rc) return rc;
+      // z = P r ; rz_new = <r, z> ; beta
+      auto fin_beta = [=] __device__(const double* t) {
+        S->beta = t[0] / S->rz;
+        S->rz = t[0];
+      };
+      if (diag_prec) {
+        rc = launch_chunks<1>(
+            ctx, n,
+            [=] __device__(int64_t i, double* a) {
+              const T zi = r[i] / dg[i];
+              z[i] = zi;
+              a[0] = fma((double)r[i], (double)zi, a[0]);
+            },
+            fin_beta, done);
+      } else {
+        if ((rc = prec_apply_impl(s->prec, s->precision, r, z, n, done))) return rc;
+        rc = launch_chunks<1>(
+            ctx, n,
+            [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)z[i], a[0]); },
+            fin_beta, done);
+      }
+      if (rc) return rc;
+      rc = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i, double*) { p[i] = fmaT((T)S->beta, p[i], z[i]); },
+          NoFin{}, done);
+      if (rc) return rc;
+    }
+    if ((rc = read_state(s))) return rc;
+    if (s->h_state->done) break;
+  }
+  return LFX_OK;
+}
+
+// ------------------------------------------------------------------ BiCGStab
+template <class T>
+int bicgstab_run(lfx_solver* s, T* x, const T* b) {
+  lfx_ctx* ctx = s->ctx;
+  DevState* S = s->d_state;
+  const int64_t n = s->n;
+  T *r = (T*)s->work[0], *r0 = (T*)s->work[1], *p = (T*)s->work[2], *v = (T*)s->work[3];
+  T *t = (T*)s->work[4], *sv = (T*)s->work[5], *y = (T*)s->work[6], *z = (T*)s->work[7];
+  const int* done = &S->done;
+  int rc;
+  // v = A x ; r = b - v ; r0 = r ; sc_err = ||r||
+  if ((rc = op_apply_impl(s->op, x, r, b, nullptr))) return rc;
+  rc = launch_chunks<1>(
+      ctx, n,
+      [=] __device__(int64_t i, double* a) {
+        r0[i] = r[i];
+        v[i] = T(0);
+        p[i] = T(0);
+        a[0] = fma((double)r[i], (double)r[i], a[0]);
+      },
+      [=] __device__(const double* tt) {
+        S->applies = 1;
+        S->r_nrm_0 = sqrt(tt[0]);
+        S->sc_err = S->r_nrm_0;
+        if (S->sc_err < EPS_RDEF) {  // :692
+          S->done = 1;
+          S->converged = 1;
+          S->r_nrm = S->sc_err;
+        } else {
+          S->sc_err = fmax(S->sc_err, S->a_tol);
+        }
+        S->alpha = 1.0;
+        S->omega = 1.0;
+        S->rho_old = 1.0;
+      });
+  if (rc) return rc;
+  for (;;) {
+    for (int it = 0; it < 8; ++it) {
+      // rho = <r, r0> ; beta = (rho/rho_old)(alpha/omega)
+      rc = launch_chunks<1>(
+          ctx, n,
+          [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)r0[i], a[0]); },
+          [=] __device__(const double* tt) {
+            S->rho = tt[0];
+            S->beta = (S->rho / S->rho_old) * (S->alpha / S->omega);
+            S->coef = -(S->beta * S->omega);
+          },
+          done);
+      if (rc) return rc;
+      // t = r - beta*omega v
+      rc = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i, double*) { t[i] = fmaT((T)S->coef, v[i], r[i]); },
+          NoFin{}, done);
+      if (rc) return rc;
+      if ((rc = prec_apply_impl(s->prec, s->precision, t, y, n, done))) return rc;
+      rc = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i, double*) { p[i] = fmaT((T)S->beta, p[i], y[i]); },
+          NoFin{}, done);
+      if (rc) return rc;
+      if ((rc = op_apply_impl(s->op, p, v, nullptr, done))) return rc;
+      rc = launch_chunks<1>(
+          ctx, n,
+          [=] __device__(int64_t i, double* a) { a[0] = fma((double)r0[i], (double)v[i], a[0]); },
+          [=] __device__(const double* tt) {
+            S->alpha = S->rho / tt[0];
+            S->neg_alpha = -S->alpha;
+          },
+          done);
+      if (rc) return rc;
+      rc = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i, double*) { sv[i] = fmaT((T)S->neg_alpha, v[i], r[i]); },
+          NoFin{}, done);
+      if (rc) return rc;
+      if ((rc = prec_apply_impl(s->prec, s->precision, sv, z, n, done))) return rc;
+      if ((rc = op_apply_impl(s->op, z, t, nullptr, done))) return rc;
+      rc = launch_chunks<2>(
+          ctx, n,
+          [=] __device__(int64_t i, double* a) {
+            a[0] = fma((double)t[i], (double)t[i], a[0]);
+            a[1] = fma((double)t[i], (double)sv[i], a[1]);
+          },
+          [=] __device__(const double* tt) {
+            S->applies += 2;
+            S->tt = tt[0];
+            S->ts = tt[1];
+            S->omega = S->ts / S->tt;
+          },
+          done);
+      if (rc) return rc;
+      // x += omega z ; x += alpha p ; r = s - omega t ; ||r||
+      rc = launch_chunks<1>(
+          ctx, n,
+          [=] __device__(int64_t i, double* a) {
+            const T om = (T)S->omega;
+            T xi = fmaT(om, z[i], x[i]);
+            x[i] = fmaT((T)S->alpha, p[i], xi);
+            const T ri = fmaT(-om, t[i], sv[i]);
+            r[i] = ri;
+            a[0] = fma((double)ri, (double)ri, a[0]);
+          },
+          [=] __device__(const double* tt) {
+            S->rho_old = S->rho;
+            S->iter += 1;
+            S->r_nrm = sqrt(tt[0]);
+            S->err = S->r_nrm / S->sc_err;
+            if (S->monitor) {
+              if (S->err < S->r_tol) {  // :760
+                S->done = 1;
+                S->converged = 1;
+              } else if (isnan(S->err)) {
+                S->done = 1;
+                S->status = LFX_NAN_DETECTED;
+              }
+            }
+            if (S->iter >= S->max_iter) S->done = 1;
+          },
+          done);
+      if (rc) return rc;
+    }
+    if ((rc = read_state(s))) return rc;
+    if (s->h_state->done) break;
+  }
+  return LFX_OK;
+}
+
+// ------------------------------------------------------------------ GMRES
+// Givens rotations and back substitution (:930-953) by one thread.
+__global__ void gmres_finish_cycle(DevState* S, double* gm, int K) {
+  if (S->done) return;
+  double* h = gm;                  // H(i,j) at (i-1) + (K+1)(j-1)
+  double* g = gm + 2 * (K + 1) * K;
+  double* u = g + (K + 1);
+#define H(i, j) h[((i) - 1) + (K + 1) * ((j) - 1)]
+  for (int iv = 1; iv <= K; ++iv) {
+    const double nrm = sqrt(fma(H(iv, iv), H(iv, iv), H(iv + 1, iv) * H(iv + 1, iv)));
+    const double si = H(iv + 1, iv) / nrm;
+    const double ci = H(iv, iv) / nrm;
+    const double p = fma(ci, g[iv - 1], si * g[iv]);
+    const double q = fma(-si, g[iv - 1], ci * g[iv]);
+    g[iv - 1] = p;
+    g[iv] = q;
+    for (int ivj = iv; ivj <= K; ++ivj) {
+      const double h1 = fma(ci, H(iv, ivj), si * H(iv + 1, ivj));
+      const double h2 = fma(-si, H(iv, ivj), ci * H(iv + 1, ivj));
+      H(iv, ivj) = h1;
+      H(iv + 1, ivj) = h2;
+    }
+  }
+  u[K - 1] = g[K - 1] / H(K, K);
+  for (int iv = K - 1; iv >= 1; --iv) {
+    double a = g[iv - 1];
+    for (int ivj = iv + 1; ivj <= K; ++ivj) a = fma(-H(iv, ivj), u[ivj - 1], a);
+    u[iv - 1] = a / H(iv, iv);
+  }
+#undef H
+}
+
+template <class T>
+int gmres_run(lfx_solver* s, T* x, const T* b) {
+  lfx_ctx* ctx = s->ctx;
+  DevState* S = s->d_state;
+  const int64_t n = s->n;
+  const int K = s->cfg.gcrk;
+  T* sv = (T*)s->work[0];
+  T* w = (T*)s->work[1];
+  T* res = (T*)s->work[2];
+  T* V[MAX_GCRK];
+  for (int k = 0; k < K; ++k) V[k] = (T*)s->work[3 + k];
+  double* h = s->d_gm;
+  double* nh = h + (K + 1) * K;
+  double* g = nh + (K + 1) * K;
+  double* u = g + (K + 1);
+  const int* done = &S->done;
+  int rc;
+  // res = b - A x ; sc_err = ||res||
+  if ((rc = op_apply_impl(s->op, x, res, b, nullptr))) return rc;
+  rc = launch_chunks<1>(
+      ctx, n,
+      [=] __device__(int64_t i, double* a) { a[0] = fma((double)res[i], (double)res[i], a[0]); },
+      [=] __device__(const double* t) {
+        S->applies = 1;
+        S->r_nrm_0 = sqrt(t[0]);
+        S->sc_err = S->r_nrm_0;
+        if (S->sc_err < EPS_RDEF) {  // :866
+          S->done = 1;
+          S->converged = 1;
+          S->r_nrm = S->sc_err;
+        } else if (S->monitor) {
+          S->sc_err = fmax(S->sc_err, S->a_tol);
+        }
+      });
+  if (rc) return rc;
+  VecPtrs vp{};
+  for (int k = 0; k < K; ++k) vp.p[k] = V[k];
+  for (;;) {
+    // s = P res ; beta = ||s|| ; v1 = s / beta ; g = (beta, 0, ...)
+    if ((rc = prec_apply_impl(s->prec, s->precision, res, sv, n, done))) return rc;
+    rc = launch_chunks<1>(
+        ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma((double)sv[i], (double)sv[i], a[0]); },
+        [=] __device__(const double* t) {
+          S->gbeta = sqrt(t[0]);
+          S->inv_beta = 1.0 / S->gbeta;
+          for (int k = 0; k <= K; ++k) g[k] = 0.0;
+          g[0] = S->gbeta;
+        },
+        done);
+    if (rc) return rc;
+    {
+      T* v0 = V[0];
+      rc = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i, double*) { v0[i] = (T)S->inv_beta * sv[i]; }, NoFin{},
+          done);
+      if (rc) return rc;
+    }
+    for (int iv = 1; iv <= K; ++iv) {
+      if ((rc = op_apply_impl(s->op, V[iv - 1], sv, nullptr, done))) return rc;  // s = A v
+      if ((rc = prec_apply_impl(s->prec, s->precision, sv, w, n, done))) return rc;   // w = P s
+      // modified Gram-Schmidt: h(j,iv) = <v_j, w> ; w -= h(j,iv) v_j
+      {
+        const T* vj = V[0];
+        double* hj = &h[0 + (K + 1) * (iv - 1)];
+        double* nhj = &nh[0 + (K + 1) * (iv - 1)];
+        rc = launch_chunks<1>(
+            ctx, n,
+            [=] __device__(int64_t i, double* a) { a[0] = fma((double)vj[i], (double)w[i], a[0]); },
+            [=] __device__(const double* t) {
+              *hj = t[0];
+              *nhj = -t[0];
+            },
+            done);
+        if (rc) return rc;
+      }
+      for (int j = 2; j <= iv; ++j) {
+        const T* vprev = V[j - 2];
+        const T* vj = V[j - 1];
+        const double* nhp = &nh[(j - 2) + (K + 1) * (iv - 1)];
+        double* hj = &h[(j - 1) + (K + 1) * (iv - 1)];
+        double* nhj = &nh[(j - 1) + (K + 1) * (iv - 1)];
+        rc = launch_chunks<1>(
+            ctx, n,
+            [=] __device__(int64_t i, double* a) {
+              const T wi = fmaT((T)*nhp, vprev[i], w[i]);
+              w[i] = wi;
+              a[0] = fma((double)vj[i], (double)wi, a[0]);
+            },
+            [=] __device__(const double* t) {
+              *hj = t[0];
+              *nhj = -t[0];
+            },
+            done);
+        if (rc) return rc;
+      }
+      {
+        const T* vl = V[iv - 1];
+        const double* nhp = &nh[(iv - 1) + (K + 1) * (iv - 1)];
+        double* hn = &h[iv + (K + 1) * (iv - 1)];
+        rc = launch_chunks<1>(
+            ctx, n,
+            [=] __device__(int64_t i, double* a) {
+              const T wi = fmaT((T)*nhp, vl[i], w[i]);
+              w[i] = wi;
+              a[0] = fma((double)wi, (double)wi, a[0]);
+            },
+            [=] __device__(const double* t) {
+              *hn = sqrt(t[0]);
+              S->inv_hn = 1.0 / *hn;
+              S->applies += 1;
+            },
+            done);
+        if (rc) return rc;
+      }
+      if (iv < K) {
+        T* vn = V[iv];
+        rc = launch_chunks<0>(
+            ctx, n, [=] __device__(int64_t i, double*) { vn[i] = (T)S->inv_hn * w[i]; }, NoFin{},
+            done);
+        if (rc) return rc;
+      }
+    }
+    gmres_finish_cycle<<<1, 1, 0, ctx->stream>>>(S, h, K);
+    LFX_CK(ctx, cudaGetLastError());
+    // x += sum_iv u(iv) v_iv, one pass, the reference's order per element
+    rc = launch_chunks<0>(
+        ctx, n,
+        [=] __device__(int64_t i, double*) {
+          T xi = x[i];
+          for (int k = 0; k < K; ++k) xi = fmaT((T)u[k], ((const T*)vp.p[k])[i], xi);
+          x[i] = xi;
+        },
+        NoFin{}, done);
+    if (rc) return rc;
+    if ((rc = op_apply_impl(s->op, x, res, b, done))) return rc;  // res = b - A x
+    rc = launch_chunks<1>(
+        ctx, n,
+        [=] __device__(int64_t i, double* a) { a[0] = fma((double)res[i], (double)res[i], a[0]); },
+        [=] __device__(const double* t) {
+          S->applies += 1;
+          S->iter += 1;
+          S->res_norm = sqrt(t[0]);
+          S->r_nrm = S->res_norm;
+          S->err = S->res_norm / S->sc_err;
+          if (S->monitor) {
+            if (S->err < S->r_tol) {  // :970
+              S->done = 1;
+              S->converged = 1;
+            } else if (isnan(S->err)) {
+              S->done = 1;
+              S->status = LFX_NAN_DETECTED;
+            }
+          }
+          if (S->iter >= S->max_iter) S->done = 1;
+        },
+        done);
+    if (rc) return rc;
+    if ((rc = read_state(s))) return rc;
+    if (s->h_state->done) break;
+  }
+  return LFX_OK;
+}
+
+void fill_info(lfx_solver* s, lfx_solve_info* info) {
+  const DevState& h = *s->h_state;
+  info->iterations = h.iter;
+  info->converged = h.converged;
+  info->initial_norm = h.r_nrm_0;
+  info->final_norm = h.r_nrm;
+  info->final_rel = s->kind == LFX_SOLVER_CG ? (h.r_nrm_0 > 0 ? h.r_nrm / h.r_nrm_0 : 0.0) : h.err;
+  if (h.converged && h.iter == 0) info->final_rel = 0.0;
+  info->applies = h.applies;
+  info->status = h.status;
+}
+
+int free_solver(lfx_solver* s) {
+  if (!s) return LFX_OK;
+  lfx_ctx* ctx = s->ctx;
+  for (void* p : s->work) dfree(ctx, p, s->n * esz(s->precision));
+  dfree(ctx, s->d_state, sizeof(DevState));
+  if (s->h_state) cudaFreeHost(s->h_state);
+  if (s->d_gm) dfree(ctx, s->d_gm, sizeof(double) * (4 * (size_t)(s->cfg.gcrk + 1) * s->cfg.gcrk + 8));
+  if (s->r32) lfx_vec_destroy(s->r32);
+  if (s->d32) lfx_vec_destroy(s->d32);
+  if (s->d_r64) dfree(ctx, s->d_r64, s->n * 8);
+  delete s;
+  return LFX_OK;
+}
+
+int alloc_common(lfx_solver* s, int nwork) {
+  lfx_ctx* ctx = s->ctx;
+  int rc = dmalloc(ctx, (void**)&s->d_state, sizeof(DevState));
+  if (rc) return rc;
+  if (cudaMallocHost((void**)&s->h_state, sizeof(DevState)) != cudaSuccess)
+    return fail(ctx, LFX_OUT_OF_MEMORY, "pinned allocation failed");
+  for (int k = 0; k < nwork; ++k) {
+    void* p = nullptr;
+    rc = dmalloc(ctx, &p, s->n * esz(s->precision));
+    if (rc) return rc;
+    s->work.push_back(p);
+  }
+  return ensure_partials(ctx, s->n, 4);
+}
+
+// ------------------------------------------------------------------ refinement
+int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* info) {
+  lfx_ctx* ctx = s->ctx;
+  const int64_t n = s->n;
+  double* x = (double*)xv->data[0];
+  const double* b = (const double*)bv->data[0];
+  double* r = s->d_r64;
+  float* r32 = (float*)s->r32->data[0];
+  float* d32 = (float*)s->d32->data[0];
+  double* sc = ctx->d_scalars;
+  int rc;
+  auto resid_norm = [&](double* out) -> int {
+    int q = op_apply_impl(s->op, x, r, b, nullptr);
+    if (q) return q;
+    q = launch_chunks<1>(
+        ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma(r[i], r[i], a[0]); },
+        [=] __device__(const double* t) { sc[0] = sqrt(t[0]); });
+    if (q) return q;
+    LFX_CK(ctx, cudaMemcpyAsync(ctx->h_scalars, sc, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = ctx->h_scalars[0];
+    return LFX_OK;
+  };
+  double r0 = 0.0, rn = 0.0;
+  if ((rc = resid_norm(&r0))) return rc;
+  memset(info, 0, sizeof *info);
+  info->initial_norm = r0;
+  info->applies = 1;
+  rn = r0;
+  if (r0 < EPS_RDEF) {
+    info->converged = 1;
+    info->final_norm = r0;
+    return LFX_OK;
+  }
+  for (int k = 1; k <= s->cfg.max_iter; ++k) {
+    // r32 = r / ||r|| ; d32 = 0
+    const double inv = 1.0 / rn;
+    rc = launch_chunks<0>(
+        ctx, n,
+        [=] __device__(int64_t i, double*) {
+          r32[i] = (float)(r[i] * inv);
+          d32[i] = 0.0f;
+        },
+        NoFin{});
+    if (rc) return rc;
+    lfx_solve_info ii{};
+    rc = lfx_solver_apply(s->inner, s->d32, s->r32, &ii);
+    if (rc && rc != LFX_NOT_CONVERGED) return rc;
+    info->inner_iterations += ii.iterations;
+    info->applies += ii.applies;
+    // x += ||r|| d
+    const double scale = rn;
+    rc = launch_chunks<0>(
+        ctx, n, [=] __device__(int64_t i, double*) { x[i] = fma(scale, (double)d32[i], x[i]); },
+        NoFin{});
+    if (rc) return rc;
+    if ((rc = resid_norm(&rn))) return rc;
+    info->applies += 1;
+    info->outer_iterations = k;
+    info->iterations = k;
+    info->final_norm = rn;
+    info->final_rel = rn / r0;
+    if (std::isnan(rn)) {
+      info->status = LFX_NAN_DETECTED;
+      return fail(ctx, LFX_NAN_DETECTED, "NaN in refined residual");
+    }
+    if (rn / r0 <= s->cfg.r_tol || rn <= s->cfg.a_tol) {
+      info->converged = 1;
+      break;
+    }
+  }
+  return LFX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
+                      const lfx_solver_cfg* cfg, lfx_solver** out) {
+  if (!ctx || !op || !prec || !cfg || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (kind != LFX_SOLVER_CG && kind != LFX_SOLVER_BICGSTAB && kind != LFX_SOLVER_GMRES)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "unknown solver kind");
+  if (op->lay->undf_to != op->lay->undf_from)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "Krylov solve needs a square operator");
+  if (prec->kind != PREC_NULL && prec->precision != op->precision)
+    return fail(ctx, LFX_TYPE_MISMATCH, "operator and preconditioner precision differ");
+  if ((prec->kind == PREC_DIAG || (prec->kind == PREC_CMA && prec->rdiag)) &&
+      prec->rdiag_n != op->lay->undf_to)
+    return fail(ctx, LFX_TYPE_MISMATCH, "preconditioner diagonal does not match the operator");
+  if (prec->kind == PREC_CMA && prec->max_row >= op->lay->undf_to)
+    return fail(ctx, LFX_TYPE_MISMATCH, "CMA rows fall outside the operator's space");
+  if (cfg->max_iter < 1) return fail(ctx, LFX_INVALID_ARGUMENT, "max_iter must be positive");
+  if (kind == LFX_SOLVER_GMRES && (cfg->gcrk < 1 || cfg->gcrk > MAX_GCRK))
+    return fail(ctx, LFX_INVALID_ARGUMENT, "gcrk must be in 1..64");
+  lfx_solver* s = new lfx_solver();
+  s->ctx = ctx;
+  s->kind = kind;
+  s->op = op;
+  s->prec = prec;
+  s->cfg = *cfg;
+  s->precision = op->precision;
+  s->n = op->lay->undf_to;
+  int nwork = kind == LFX_SOLVER_CG ? 3 : kind == LFX_SOLVER_BICGSTAB ? 8 : 3 + cfg->gcrk;
+  int rc = alloc_common(s, nwork);
+  if (!rc && kind == LFX_SOLVER_GMRES)
+    rc = dmalloc(ctx, (void**)&s->d_gm,
+                 sizeof(double) * (4 * (size_t)(cfg->gcrk + 1) * cfg->gcrk + 8));
+  if (rc) {
+    free_solver(s);
+    return rc;
+  }
+  *out = s;
+  return LFX_OK;
+}
+
+int lfx_refined_solver_create(lfx_ctx* ctx, lfx_op* op64, lfx_solver* inner, double inner_rtol,
+                              const lfx_solver_cfg* cfg, lfx_solver** out) {
+  if (!ctx || !op64 || !inner || !cfg || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (op64->precision != LFX_R64) return fail(ctx, LFX_TYPE_MISMATCH, "outer operator must be FP64");
+  if (inner->precision != LFX_R32 || inner->n != op64->lay->undf_to)
+    return fail(ctx, LFX_TYPE_MISMATCH, "inner solver must be FP32 on the same space");
+  lfx_solver* s = new lfx_solver();
+  s->ctx = ctx;
+  s->kind = 100;
+  s->op = op64;
+  s->cfg = *cfg;
+  s->precision = LFX_R64;
+  s->n = op64->lay->undf_to;
+  s->inner = inner;
+  s->inner_rtol = inner_rtol;
+  int64_t n = s->n;
+  int rc = dmalloc(ctx, (void**)&s->d_r64, n * 8);
+  if (!rc) rc = lfx_vec_create(ctx, 1, &n, LFX_R32, &s->r32);
+  if (!rc) rc = lfx_vec_create(ctx, 1, &n, LFX_R32, &s->d32);
+  if (!rc) rc = dmalloc(ctx, (void**)&s->d_state, sizeof(DevState));
+  if (!rc && cudaMallocHost((void**)&s->h_state, sizeof(DevState)) != cudaSuccess)
+    rc = LFX_OUT_OF_MEMORY;
+  if (!rc) rc = ensure_partials(ctx, n, 4);
+  if (rc) {
+    free_solver(s);
+    return rc;
+  }
+  inner->cfg.r_tol = inner_rtol;
+  *out = s;
+  return LFX_OK;
+}
+
+int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info* info) {
+  if (!s || !x || !b) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = s->ctx;
+  lfx_solve_info local{};
+  if (!info) info = &local;
+  memset(info, 0, sizeof *info);
+  if (x->precision != s->precision || b->precision != s->precision)
+    return fail(ctx, LFX_TYPE_MISMATCH, "solver and vector precision differ");
+  if (x->data.size() != 1 || b->data.size() != 1)
+    return fail(ctx, LFX_NOT_SUPPORTED, "device solves take single-field vectors");
+  if (x->undf[0] != s->n || b->undf[0] != s->n)
+    return fail(ctx, LFX_TYPE_MISMATCH, "vector length does not match the operator");
+  int rc;
+  if (s->kind == 100) {
+    rc = refined_run(s, x, b, info);
+  } else {
+    if ((rc = init_state(s))) return rc;
+    if (s->kind == LFX_SOLVER_CG)
+      rc = s->precision == LFX_R64 ? cg_run<double>(s, (double*)x->data[0], (const double*)b->data[0])
+                                   : cg_run<float>(s, (float*)x->data[0], (const float*)b->data[0]);
+    else if (s->kind == LFX_SOLVER_BICGSTAB)
+      rc = s->precision == LFX_R64
+               ? bicgstab_run<double>(s, (double*)x->data[0], (const double*)b->data[0])
+               : bicgstab_run<float>(s, (float*)x->data[0], (const float*)b->data[0]);
+    else
+      rc = s->precision == LFX_R64
+               ? gmres_run<double>(s, (double*)x->data[0], (const double*)b->data[0])
+               : gmres_run<float>(s, (float*)x->data[0], (const float*)b->data[0]);
+    if (!rc) rc = read_state(s);
+    if (!rc) fill_info(s, info);
+  }
+  if (ctx->time_applies) drain_timing(ctx);
+  if (rc) {
+    info->status = rc;
+    return rc;
+  }
+  if (info->status == LFX_NAN_DETECTED) return fail(ctx, LFX_NAN_DETECTED, "NaN in residual");
+  if (!info->converged && s->cfg.monitor_convergence && s->cfg.fail_on_non_converged) {
+    info->status = LFX_NOT_CONVERGED;
+    return fail(ctx, LFX_NOT_CONVERGED, "solver did not converge");
+  }
+  return LFX_OK;
+}
+
+int lfx_solver_destroy(lfx_solver* s) { return free_solver(s); }
+
+}  // extern "C"

@@ -1,0 +1,464 @@
+"""Python mirror of the reference's solver API over the liblfx C ABI.
+
+The classes follow the reference's abstract types and their concrete
+extensions, with the same procedure names and argument meanings:
+
+  FieldVector            abstract_vector_type (vector_mod.F90:17-189),
+                         field_vector_type / r_solver_field_vector_type
+  LmaOperator            abstract_linear_operator_type + operator_type /
+                         mass_matrix_operator_type (matrix_vector_kernel)
+  NullPreconditioner,
+  DiagonalPreconditioner,
+  ColumnwisePreconditioner abstract_preconditioner_type
+  ColumnwiseOperator     columnwise_operator_type (CMA)
+  ConjugateGradient, BiCGStab, GMRES
+                         conjugate_gradient_type, BiCGstab_type, gmres_type
+                         (sci_iterative_solver_mod.f90), device resident
+  RefinedSolver          FP64 iterative refinement around an FP32 inner solve
+
+Where the reference calls log_event(..., LOG_LEVEL_ERROR) (which aborts), the
+mirror raises LfxError carrying the C status code. Everything runs on the GPU
+through liblfx.so; there is no CPU fallback, and importing this module on a
+machine without the built library or without a GPU fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "lib" / "liblfx.so"
+_lib = None
+
+STATUS = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN_DETECTED", 3: "OUT_OF_MEMORY",
+          4: "INVALID_ARGUMENT", 5: "TYPE_MISMATCH", 6: "TIMEOUT", 7: "CUDA_ERROR",
+          8: "NOT_SUPPORTED"}
+R64, R32 = 64, 32
+CG, BICGSTAB, GMRES_KIND = 1, 2, 3
+
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+vp = C.c_void_p
+
+
+class SolverCfg(C.Structure):
+    _fields_ = [("r_tol", C.c_double), ("a_tol", C.c_double), ("max_iter", C.c_int32),
+                ("gcrk", C.c_int32), ("monitor_convergence", C.c_int32),
+                ("fail_on_non_converged", C.c_int32)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32),
+                ("initial_norm", C.c_double), ("final_norm", C.c_double),
+                ("final_rel", C.c_double), ("applies", C.c_int32), ("status", C.c_int32),
+                ("outer_iterations", C.c_int32), ("inner_iterations", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# (name, argtypes, restype)
+_SIGS = [
+    ("lfx_ctx_create", [C.c_int, C.POINTER(vp)], C.c_int),
+    ("lfx_ctx_destroy", [vp], C.c_int),
+    ("lfx_last_error", [vp], C.c_char_p),
+    ("lfx_ctx_synchronize", [vp], C.c_int),
+    ("lfx_ctx_stream", [vp], vp),
+    ("lfx_ctx_device_bytes", [vp], C.c_int64),
+    ("lfx_ctx_enable_apply_timing", [vp, C.c_int32], C.c_int),
+    ("lfx_ctx_apply_timing", [vp, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int32], C.c_int),
+    ("lfx_vec_create", [vp, C.c_int32, i64p, C.c_int32, C.POINTER(vp)], C.c_int),
+    ("lfx_vec_duplicate", [vp, C.POINTER(vp)], C.c_int),
+    ("lfx_vec_destroy", [vp], C.c_int),
+    ("lfx_vec_set_scalar", [vp, C.c_double], C.c_int),
+    ("lfx_vec_axpy", [vp, C.c_double, vp], C.c_int),
+    ("lfx_vec_aypx", [vp, C.c_double, vp], C.c_int),
+    ("lfx_vec_axpby", [vp, C.c_double, vp, C.c_double, vp], C.c_int),
+    ("lfx_vec_norm", [vp, C.POINTER(C.c_double)], C.c_int),
+    ("lfx_vec_field_norm", [vp, C.c_int32, C.POINTER(C.c_double)], C.c_int),
+    ("lfx_vec_dot", [vp, vp, C.POINTER(C.c_double)], C.c_int),
+    ("lfx_vec_scale", [vp, C.c_double], C.c_int),
+    ("lfx_vec_copy", [vp, vp], C.c_int),
+    ("lfx_vec_size", [vp, C.POINTER(C.c_int32)], C.c_int),
+    ("lfx_vec_import_field", [vp, C.c_int32, f64p, C.c_int64], C.c_int),
+    ("lfx_vec_export_field", [vp, C.c_int32, f64p, C.c_int64], C.c_int),
+    ("lfx_vec_field_device_ptr", [vp, C.c_int32, C.POINTER(vp)], C.c_int),
+    ("lfx_lma_create", [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p, C.c_int64,
+                        C.c_int64, f64p, C.c_int32, i32p, i32p, C.c_int32, C.c_int32,
+                        C.POINTER(vp)], C.c_int),
+    ("lfx_lma_create_like", [vp, f64p, C.c_int32, C.POINTER(vp)], C.c_int),
+    ("lfx_op_apply", [vp, vp, vp], C.c_int),
+    ("lfx_op_apply_transpose", [vp, vp, vp], C.c_int),
+    ("lfx_op_destroy", [vp], C.c_int),
+    ("lfx_lma_diagonal", [vp, vp], C.c_int),
+    ("lfx_cma_create", [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                        C.c_int32, C.c_int32, i32p, i32p, vp, C.POINTER(vp)], C.c_int),
+    ("lfx_cma_assemble_from_lma", [vp, C.c_int32, i32p, i32p, C.c_int32, C.c_int32, C.c_int32,
+                                   C.c_int32, C.c_int32, C.c_int32, i32p, i32p, C.POINTER(vp)],
+     C.c_int),
+    ("lfx_cma_get_band", [vp, f64p], C.c_int),
+    ("lfx_cma_apply", [vp, vp, vp], C.c_int),
+    ("lfx_cma_destroy", [vp], C.c_int),
+    ("lfx_null_prec_create", [vp, C.POINTER(vp)], C.c_int),
+    ("lfx_diag_prec_create", [vp, vp, C.POINTER(vp)], C.c_int),
+    ("lfx_cma_prec_create", [vp, vp, vp, C.c_int32, C.POINTER(vp)], C.c_int),
+    ("lfx_prec_apply", [vp, vp, vp], C.c_int),
+    ("lfx_prec_destroy", [vp], C.c_int),
+    ("lfx_solver_create", [vp, C.c_int32, vp, vp, C.POINTER(SolverCfg), C.POINTER(vp)], C.c_int),
+    ("lfx_refined_solver_create", [vp, vp, vp, C.c_double, C.POINTER(SolverCfg), C.POINTER(vp)],
+     C.c_int),
+    ("lfx_solver_apply", [vp, vp, vp, C.POINTER(SolveInfo)], C.c_int),
+    ("lfx_solver_destroy", [vp], C.c_int),
+]
+EXPORTED = [s[0] for s in _SIGS]
+
+
+def load_library(path: Path | None = None):
+    """Load liblfx.so (no GPU needed to load) and bind every signature."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else _LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is not built; run python -m lfric_core_b200.build")
+    L = C.CDLL(str(p))
+    for name, args, res in _SIGS:
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    if path is None:
+        _lib = L
+    return L
+
+
+class LfxError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Context:
+    """One device, one CUDA stream (lfx_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.L = load_library()
+        h = vp()
+        rc = self.L.lfx_ctx_create(device, C.byref(h))
+        if rc:
+            raise LfxError(rc, f"cannot create a context on device {device}")
+        self.h = h
+
+    def check(self, rc):
+        if rc:
+            raise LfxError(rc, self.L.lfx_last_error(self.h).decode())
+        return rc
+
+    def synchronize(self):
+        self.check(self.L.lfx_ctx_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return self.L.lfx_ctx_stream(self.h) or 0
+
+    def device_bytes(self) -> int:
+        return self.L.lfx_ctx_device_bytes(self.h)
+
+    def enable_apply_timing(self, on: bool = True):
+        self.check(self.L.lfx_ctx_enable_apply_timing(self.h, 1 if on else 0))
+
+    def apply_timing(self, reset: bool = True):
+        n = C.c_int64()
+        ms = C.c_double()
+        self.check(self.L.lfx_ctx_apply_timing(self.h, C.byref(n), C.byref(ms), 1 if reset else 0))
+        return n.value, ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.lfx_ctx_destroy(self.h)
+            self.h = None
+
+
+class _Handle:
+    _destroy = None
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h and self._destroy and _lib is not None:
+            getattr(_lib, self._destroy)(h)
+            self.h = None
+
+
+class FieldVector(_Handle):
+    """field_vector_type: nfields device fields (FP64, or FP32 for the
+    r_solver variant)."""
+
+    _destroy = "lfx_vec_destroy"
+
+    def __init__(self, ctx: Context, undf, precision: int = R64, _h=None):
+        self.ctx = ctx
+        self.undf = [int(u) for u in (undf if np.ndim(undf) else [undf])]
+        self.precision = precision
+        if _h is not None:
+            self.h = _h
+            return
+        h = vp()
+        ctx.check(ctx.L.lfx_vec_create(ctx.h, len(self.undf), np.array(self.undf, dtype=np.int64),
+                                       precision, C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_array(cls, ctx, data, precision=R64):
+        v = cls(ctx, [len(data)], precision)
+        v.import_field(np.asarray(data, dtype=np.float64), 1)
+        return v
+
+    # abstract_vector_type procedures
+    def set_scalar(self, scalar):
+        self.ctx.check(self.ctx.L.lfx_vec_set_scalar(self.h, scalar))
+
+    def axpy(self, alpha, x):
+        self.ctx.check(self.ctx.L.lfx_vec_axpy(self.h, alpha, x.h))
+
+    def aypx(self, alpha, x):
+        self.ctx.check(self.ctx.L.lfx_vec_aypx(self.h, alpha, x.h))
+
+    def axpby(self, a, x, b, y):
+        self.ctx.check(self.ctx.L.lfx_vec_axpby(self.h, a, x.h, b, y.h))
+
+    def norm(self):
+        out = C.c_double()
+        self.ctx.check(self.ctx.L.lfx_vec_norm(self.h, C.byref(out)))
+        return out.value
+
+    def field_norm(self, n):
+        out = C.c_double()
+        self.ctx.check(self.ctx.L.lfx_vec_field_norm(self.h, n, C.byref(out)))
+        return out.value
+
+    def dot(self, x):
+        out = C.c_double()
+        self.ctx.check(self.ctx.L.lfx_vec_dot(self.h, x.h, C.byref(out)))
+        return out.value
+
+    def scale(self, scalar):
+        self.ctx.check(self.ctx.L.lfx_vec_scale(self.h, scalar))
+
+    def duplicate(self):
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_vec_duplicate(self.h, C.byref(h)))
+        return FieldVector(self.ctx, self.undf, self.precision, _h=h)
+
+    def copy(self, source):
+        self.ctx.check(self.ctx.L.lfx_vec_copy(self.h, source.h))
+
+    def vector_size(self):
+        n = C.c_int32()
+        self.ctx.check(self.ctx.L.lfx_vec_size(self.h, C.byref(n)))
+        return n.value
+
+    def import_field(self, data, position=1):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        self.ctx.check(self.ctx.L.lfx_vec_import_field(self.h, position, a, len(a)))
+
+    def export_field(self, position=1):
+        out = np.empty(self.undf[position - 1], dtype=np.float64)
+        self.ctx.check(self.ctx.L.lfx_vec_export_field(self.h, position, out, len(out)))
+        return out
+
+    def device_ptr(self, position=1) -> int:
+        p = vp()
+        self.ctx.check(self.ctx.L.lfx_vec_field_device_ptr(self.h, position, C.byref(p)))
+        return p.value
+
+
+class LmaOperator(_Handle):
+    """operator_type applied by the coloured matrix_vector_kernel: y = A x."""
+
+    _destroy = "lfx_op_destroy"
+
+    def __init__(self, ctx, ncell_2d, nlayers, ndf_to, ndf_from, map_to, map_from, undf_to,
+                 undf_from, local_stencil, ncells_per_colour, cells_in_colour,
+                 precision=R64, _h=None):
+        self.ctx = ctx
+        self.precision = precision
+        self.undf_to, self.undf_from = int(undf_to), int(undf_from)
+        self._shape = (ncell_2d, nlayers, ndf_to, ndf_from)
+        if _h is not None:
+            self.h = _h
+            return
+        cic = np.ascontiguousarray(cells_in_colour, dtype=np.int32)
+        h = vp()
+        ctx.check(ctx.L.lfx_lma_create(
+            ctx.h, ncell_2d, nlayers, ndf_to, ndf_from,
+            np.ascontiguousarray(map_to, dtype=np.int32), np.ascontiguousarray(map_from, dtype=np.int32),
+            undf_to, undf_from, np.ascontiguousarray(local_stencil, dtype=np.float64),
+            len(ncells_per_colour), np.ascontiguousarray(ncells_per_colour, dtype=np.int32), cic,
+            cic.shape[0], precision, C.byref(h)))
+        self.h = h
+
+    def like(self, local_stencil, precision):
+        """Same dofmaps and colouring, new local matrices / precision."""
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_lma_create_like(
+            self.h, np.ascontiguousarray(local_stencil, dtype=np.float64), precision, C.byref(h)))
+        op = LmaOperator(self.ctx, *self._shape, None, None, self.undf_to, self.undf_from, None,
+                         None, None, precision=precision, _h=h)
+        op._parent = self
+        return op
+
+    def apply(self, x, y):
+        self.ctx.check(self.ctx.L.lfx_op_apply(self.h, x.h, y.h))
+
+    def apply_transpose(self, x, y):
+        self.ctx.check(self.ctx.L.lfx_op_apply_transpose(self.h, x.h, y.h))
+
+    def diagonal(self, diag):
+        self.ctx.check(self.ctx.L.lfx_lma_diagonal(self.h, diag.h))
+
+
+class ColumnwiseOperator(_Handle):
+    """columnwise_operator_type: banded matrix per column."""
+
+    _destroy = "lfx_cma_destroy"
+
+    def __init__(self, ctx, h, ncell_2d, nrow, bandwidth):
+        self.ctx, self.h = ctx, h
+        self.ncell_2d, self.nrow, self.bandwidth = ncell_2d, nrow, bandwidth
+
+    @classmethod
+    def from_band(cls, ctx, ncell_2d, nrow, bandwidth, alpha, beta, gamma_m, gamma_p, first_dof,
+                  indirection, band):
+        h = vp()
+        b = np.ascontiguousarray(band, dtype=np.float64)
+        ctx.check(ctx.L.lfx_cma_create(ctx.h, ncell_2d, nrow, nrow, bandwidth, alpha, beta,
+                                       gamma_m, gamma_p,
+                                       np.ascontiguousarray(first_dof, dtype=np.int32),
+                                       np.ascontiguousarray(indirection, dtype=np.int32),
+                                       b.ctypes.data, C.byref(h)))
+        return cls(ctx, h, ncell_2d, nrow, bandwidth)
+
+    @classmethod
+    def assemble(cls, lma: LmaOperator, dfs, column_banded_dofmap, params, first_dof):
+        """columnwise_op_asm from the local dofs `dfs` (1-based) of an FP64 LMA."""
+        ctx = lma.ctx
+        h = vp()
+        cbd = np.ascontiguousarray(column_banded_dofmap, dtype=np.int32)
+        ctx.check(ctx.L.lfx_cma_assemble_from_lma(
+            lma.h, len(dfs), np.ascontiguousarray(dfs, dtype=np.int32), cbd, params["alpha"],
+            params["beta"], params["gamma_m"], params["gamma_p"], params["bandwidth"],
+            params["nrow"], np.ascontiguousarray(first_dof, dtype=np.int32),
+            np.ascontiguousarray(params["indirection"], dtype=np.int32), C.byref(h)))
+        return cls(ctx, h, lma._shape[0], params["nrow"], params["bandwidth"])
+
+    def band(self):
+        out = np.empty(self.ncell_2d * self.nrow * self.bandwidth)
+        self.ctx.check(self.ctx.L.lfx_cma_get_band(self.h, out))
+        return out
+
+    def apply(self, x, y):
+        self.ctx.check(self.ctx.L.lfx_cma_apply(self.h, x.h, y.h))
+
+
+class _Prec(_Handle):
+    _destroy = "lfx_prec_destroy"
+
+    def apply(self, x, y):
+        self.ctx.check(self.ctx.L.lfx_prec_apply(self.h, x.h, y.h))
+
+
+class NullPreconditioner(_Prec):
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = vp()
+        ctx.check(ctx.L.lfx_null_prec_create(ctx.h, C.byref(h)))
+        self.h = h
+
+
+class DiagonalPreconditioner(_Prec):
+    def __init__(self, ctx, diag: FieldVector):
+        self.ctx = ctx
+        h = vp()
+        ctx.check(ctx.L.lfx_diag_prec_create(ctx.h, diag.h, C.byref(h)))
+        self.h = h
+
+
+class ColumnwisePreconditioner(_Prec):
+    """Column tridiagonal inverse on the CMA's rows, Jacobi elsewhere."""
+
+    def __init__(self, ctx, cma: ColumnwiseOperator, diag: FieldVector | None, precision=R64):
+        self.ctx = ctx
+        h = vp()
+        ctx.check(ctx.L.lfx_cma_prec_create(ctx.h, cma.h, diag.h if diag is not None else None,
+                                            precision, C.byref(h)))
+        self.h = h
+        self._keep = (cma, diag)
+
+
+class _Solver(_Handle):
+    _destroy = "lfx_solver_destroy"
+
+    def apply(self, x: FieldVector, b: FieldVector) -> SolveInfo:
+        info = SolveInfo()
+        rc = self.ctx.L.lfx_solver_apply(self.h, x.h, b.h, C.byref(info))
+        self.last_info = info
+        if rc:
+            self.ctx.check(rc)
+        return info
+
+
+def _cfg(r_tol, a_tol, max_iter, gcrk, monitor, fail):
+    return SolverCfg(r_tol, a_tol, max_iter, gcrk, 1 if monitor else 0, 1 if fail else 0)
+
+
+class _KrylovSolver(_Solver):
+    KIND = 0
+
+    def __init__(self, lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence=True,
+                 fail_on_non_converged=False, gcrk=1):
+        self.ctx = lin_op.ctx
+        self.precision = lin_op.precision
+        cfg = _cfg(r_tol, a_tol, max_iter, gcrk, monitor_convergence, fail_on_non_converged)
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_solver_create(self.ctx.h, self.KIND, lin_op.h, prec.h,
+                                                     C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._keep = (lin_op, prec)
+
+
+class ConjugateGradient(_KrylovSolver):
+    """conjugate_gradient_type(lin_op, prec, r_tol, a_tol, max_iter, ...)"""
+    KIND = CG
+
+
+class BiCGStab(_KrylovSolver):
+    """BiCGstab_type(lin_op, prec, r_tol, a_tol, max_iter, ...)"""
+    KIND = BICGSTAB
+
+
+class GMRES(_KrylovSolver):
+    """gmres_type(lin_op, prec, gcrk, r_tol, a_tol, max_iter, ...)"""
+    KIND = GMRES_KIND
+
+    def __init__(self, lin_op, prec, gcrk, r_tol, a_tol, max_iter, monitor_convergence=True,
+                 fail_on_non_converged=False):
+        super().__init__(lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence,
+                         fail_on_non_converged, gcrk=gcrk)
+
+
+class RefinedSolver(_Solver):
+    """FP64 iterative refinement: r = b - A64 x in FP64, correction from an FP32
+    inner solver run to inner_rtol, x += ||r|| d. Converged when
+    ||b - A x|| / ||b - A x0|| <= r_tol."""
+
+    def __init__(self, op64: LmaOperator, inner: _Solver, inner_rtol, r_tol, a_tol=0.0,
+                 max_outer=20, fail_on_non_converged=False):
+        self.ctx = op64.ctx
+        self.precision = R64
+        cfg = _cfg(r_tol, a_tol, max_outer, 0, True, fail_on_non_converged)
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_refined_solver_create(self.ctx.h, op64.h, inner.h,
+                                                             inner_rtol, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._keep = (op64, inner)

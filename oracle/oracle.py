@@ -1,0 +1,179 @@
+"""ctypes wrapper of the oracle library (CPU FP64 restatement of the path).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU legs of bench.py, never by the lfric_core_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_lib = None
+
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+class Info(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32),
+                ("initial_norm", C.c_double), ("final_norm", C.c_double),
+                ("final_rel", C.c_double), ("applies", C.c_int32)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = HERE / "build" / "liboracle.so"
+        if not path.exists():
+            raise RuntimeError(f"{path} missing; run python oracle/build.py")
+        L = C.CDLL(str(path))
+        L.or_set_reduction_order.argtypes = [C.c_int]
+        L.or_set_threads.argtypes = [C.c_int]
+        L.or_dot.argtypes = [f64p, f64p, C.c_int64]
+        L.or_dot.restype = C.c_double
+        L.or_sumsq.argtypes = [f64p, C.c_int64]
+        L.or_sumsq.restype = C.c_double
+        L.or_setval_c.argtypes = [f64p, C.c_double, C.c_int64]
+        L.or_setval_x.argtypes = [f64p, f64p, C.c_int64]
+        L.or_inc_x_plus_by.argtypes = [f64p, C.c_double, f64p, C.c_int64]
+        L.or_inc_ax_plus_y.argtypes = [C.c_double, f64p, f64p, C.c_int64]
+        L.or_ax_plus_by.argtypes = [f64p, C.c_double, f64p, C.c_double, f64p, C.c_int64]
+        L.or_inc_a_times_x.argtypes = [C.c_double, f64p, C.c_int64]
+        L.or_x_divideby_y.argtypes = [f64p, f64p, f64p, C.c_int64]
+        L.or_matrix_vector_code.argtypes = [C.c_int32, C.c_int32, f64p, f64p, C.c_int64, f64p,
+                                            C.c_int32, i32p, C.c_int32, i32p]
+        L.or_transpose_matrix_vector_code.argtypes = L.or_matrix_vector_code.argtypes
+        L.or_dg_matrix_vector_code.argtypes = L.or_matrix_vector_code.argtypes
+        L.or_tri_solve_code.argtypes = [C.c_int32, f64p, f64p, f64p, f64p, f64p, i32p]
+        L.or_columnwise_op_asm_code.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, f64p,
+                                                f64p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                                C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p,
+                                                C.c_int32, i32p]
+        L.or_columnwise_op_app_code.argtypes = [C.c_int32, f64p, f64p, f64p, C.c_int32, C.c_int32,
+                                                C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                                C.c_int32, i32p, i32p, i32p, i32p]
+        L.or_columnwise_op_appinv_code.argtypes = [C.c_int32, f64p, f64p, f64p, C.c_int32,
+                                                   C.c_int32, i32p, i32p]
+        L.or_lma_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p,
+                                    C.c_int64, C.c_int64, f64p, C.c_int32, i32p, i32p,
+                                    C.c_int32, C.c_int32]
+        L.or_lma_create.restype = C.c_void_p
+        L.or_op_apply.argtypes = [C.c_void_p, f64p, f64p]
+        L.or_op_destroy.argtypes = [C.c_void_p]
+        L.or_lma_diagonal.argtypes = [C.c_void_p, f64p]
+        L.or_null_prec_create.argtypes = [C.c_int64]
+        L.or_null_prec_create.restype = C.c_void_p
+        L.or_diag_prec_create.argtypes = [f64p, C.c_int64]
+        L.or_diag_prec_create.restype = C.c_void_p
+        L.or_cma_prec_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, i32p, i32p, f64p,
+                                         C.c_void_p, C.c_int64]
+        L.or_cma_prec_create.restype = C.c_void_p
+        L.or_prec_apply.argtypes = [C.c_void_p, f64p, f64p]
+        L.or_prec_destroy.argtypes = [C.c_void_p]
+        for name in ("or_cg", "or_bicgstab"):
+            getattr(L, name).argtypes = [C.c_void_p, C.c_void_p, f64p, f64p, C.c_int64, C.c_double,
+                                         C.c_double, C.c_int32, C.POINTER(Info)]
+        L.or_gmres.argtypes = [C.c_void_p, C.c_void_p, f64p, f64p, C.c_int64, C.c_int32,
+                               C.c_double, C.c_double, C.c_int32, C.POINTER(Info)]
+        _lib = L
+    return _lib
+
+
+class LmaOperator:
+    """Coloured LMA apply, y = A x (matrix_vector_kernel over colours)."""
+
+    def __init__(self, ncell_2d, nlayers, ndf_to, ndf_from, map_to, map_from, undf_to,
+                 undf_from, stencil, ncells_per_colour, cells_in_colour, transpose=False):
+        self._keep = [np.ascontiguousarray(a) for a in
+                      (map_to, map_from, stencil, ncells_per_colour, cells_in_colour)]
+        mt, mf, st, npc, cic = self._keep
+        self.undf_to, self.undf_from = int(undf_to), int(undf_from)
+        self.transpose = transpose
+        self.h = lib().or_lma_create(ncell_2d, nlayers, ndf_to, ndf_from, mt, mf, undf_to,
+                                     undf_from, st, len(npc), npc, cic, cic.shape[0],
+                                     1 if transpose else 0)
+
+    def apply(self, x):
+        y = np.empty(self.undf_from if self.transpose else self.undf_to)
+        lib().or_op_apply(self.h, np.ascontiguousarray(x, dtype=np.float64), y)
+        return y
+
+    def diagonal(self):
+        d = np.empty(self.undf_to)
+        lib().or_lma_diagonal(self.h, d)
+        return d
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.or_op_destroy(self.h)
+
+
+class Preconditioner:
+    def __init__(self, h, n, keep):
+        self.h, self.n, self._keep = h, n, keep
+
+    @classmethod
+    def null(cls, n):
+        return cls(lib().or_null_prec_create(n), n, [])
+
+    @classmethod
+    def diagonal(cls, diag):
+        d = np.ascontiguousarray(diag, dtype=np.float64)
+        return cls(lib().or_diag_prec_create(d, len(d)), len(d), [d])
+
+    @classmethod
+    def cma(cls, ncell_2d, nrow, bandwidth, first_dof, indirection, band, diag, n):
+        keep = [np.ascontiguousarray(first_dof, dtype=np.int32),
+                np.ascontiguousarray(indirection, dtype=np.int32),
+                np.ascontiguousarray(band, dtype=np.float64)]
+        dptr = None
+        if diag is not None:
+            keep.append(np.ascontiguousarray(diag, dtype=np.float64))
+            dptr = keep[-1].ctypes.data
+        h = lib().or_cma_prec_create(ncell_2d, nrow, bandwidth, keep[0], keep[1], keep[2], dptr, n)
+        return cls(h, n, keep)
+
+    def apply(self, x):
+        y = np.zeros(self.n)
+        lib().or_prec_apply(self.h, np.ascontiguousarray(x, dtype=np.float64), y)
+        return y
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.or_prec_destroy(self.h)
+
+
+def solve(kind, op, prec, b, x0=None, r_tol=1e-8, a_tol=1e-16, max_iter=1000, gcrk=10):
+    """Run the oracle's cg / bicgstab / gmres; returns (x, Info)."""
+    n = len(b)
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    info = Info()
+    L = lib()
+    if kind == "cg":
+        L.or_cg(op.h, prec.h, x, b, n, r_tol, a_tol, max_iter, C.byref(info))
+    elif kind == "bicgstab":
+        L.or_bicgstab(op.h, prec.h, x, b, n, r_tol, a_tol, max_iter, C.byref(info))
+    elif kind == "gmres":
+        L.or_gmres(op.h, prec.h, x, b, n, gcrk, r_tol, a_tol, max_iter, C.byref(info))
+    else:
+        raise ValueError(kind)
+    return x, info
+
+
+def assemble_cma(lma_sub, ncell_2d, nlayers, params):
+    """columnwise_op_asm over every column of a (ncell_3d, ndf, ndf) sub-LMA."""
+    L = lib()
+    bw, nrow, ncol = params["bandwidth"], params["nrow"], params["ncol"]
+    band = np.zeros(ncell_2d * bw * nrow)
+    cbd = np.ascontiguousarray(params["column_banded_dofmap"], dtype=np.int32)
+    ndf = cbd.shape[1]
+    lma = np.ascontiguousarray(lma_sub, dtype=np.float64)
+    for cell in range(1, ncell_2d + 1):
+        L.or_columnwise_op_asm_code(cell, nlayers, ncell_2d, ncell_2d * nlayers, lma, band, nrow,
+                                    ncol, bw, params["alpha"], params["beta"], params["gamma_m"],
+                                    params["gamma_p"], ndf, cbd, ndf, cbd)
+    return band

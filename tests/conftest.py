@@ -1,0 +1,40 @@
+import os
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+def _ensure_built():
+    """Build whatever native library is missing (no rebuild when present, so
+    prebuilt libraries shipped with the tree are used as they are)."""
+    from lfric_core_b200 import build as pkg_build
+    from oracle import build as oracle_build
+    if not (pkg_build.LIB / "liblfx_meshgen.so").exists():
+        pkg_build.build_meshgen()
+    if not oracle_build.OUT.exists():
+        oracle_build.build()
+    if not (pkg_build.LIB / "liblfx.so").exists():
+        pkg_build.build_lfx()
+
+
+_ensure_built()
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    import torch  # noqa: F401  (only to report a clear skip reason below)
+    from lfric_core_b200 import lfx
+    try:
+        c = lfx.Context(int(os.environ.get("LFX_DEVICE", "0")))
+    except Exception as e:  # pragma: no cover - GPU tests need a GPU
+        pytest.fail(f"GPU context unavailable: {e}")
+    yield c
+    c.close()

@@ -1,0 +1,306 @@
+"""GPU parity of the CUDA path (through the C ABI) against the oracle.
+
+FP64 results are compared bit for bit: the device reproduces the reference's
+coloured summation order in the LMA apply and shares the oracle's fixed
+reduction order, and both compute every a + b*c as one fma. FP32 results are
+compared with stated tolerances."""
+import numpy as np
+import pytest
+
+from lfric_core_b200 import lfx
+from lfric_core_b200 import meshgen as mg
+from lfric_core_b200 import workloads as wl
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def o_lma(p):
+    npc, cic = p.mesh.colour_lookup()
+    return orc.LmaOperator(p.ncell_2d, p.nlayers, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf, p.lma,
+                           npc, cic)
+
+
+def o_w2_prec(p, op):
+    prm = mg.w2v_cma_params(p.nlayers)
+    band = orc.assemble_cma(mg.lma_block(p.lma, p.mesh.ncell_3d, 6, mg.W2V_DFS), p.ncell_2d,
+                            p.nlayers, prm)
+    diag = op.diagonal()
+    return orc.Preconditioner.cma(p.ncell_2d, prm["nrow"], 3, p.map[:, 4], prm["indirection"],
+                                  band, diag, p.undf), band
+
+
+def same(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+# ------------------------------------------------------------------ vectors
+@pytest.mark.parametrize("n", [1, 2047, 2048, 100003])
+def test_vector_ops_bitwise(ctx, n):
+    rng = np.random.default_rng(n)
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    L = orc.lib()
+    X, Y = lfx.FieldVector.from_array(ctx, x), lfx.FieldVector.from_array(ctx, y)
+    assert X.dot(Y) == L.or_dot(x, y, n)
+    assert X.norm() == np.sqrt(L.or_sumsq(x, n))
+    Z = X.duplicate()
+    Z.copy(X)
+    Z.axpy(0.37, Y)
+    z = x.copy()
+    L.or_inc_x_plus_by(z, 0.37, y, n)
+    assert same(Z.export_field(), z)
+    Z.aypx(-1.25, Y)
+    L.or_inc_ax_plus_y(-1.25, z, y, n)
+    assert same(Z.export_field(), z)
+    Z.axpby(2.5, X, -0.5, Y)
+    L.or_ax_plus_by(z, 2.5, x, -0.5, y, n)
+    assert same(Z.export_field(), z)
+    Z.scale(1.0 / 3.0)
+    L.or_inc_a_times_x(1.0 / 3.0, z, n)
+    assert same(Z.export_field(), z)
+    Z.set_scalar(4.0)
+    assert np.all(Z.export_field() == 4.0)
+    assert Z.vector_size() == 1
+
+
+def test_fp32_vector_semantics(ctx):
+    n = 50000
+    rng = np.random.default_rng(2)
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    X, Y = lfx.FieldVector.from_array(ctx, x, lfx.R32), lfx.FieldVector.from_array(ctx, y, lfx.R32)
+    x32, y32 = x.astype(np.float32), y.astype(np.float32)
+    np.testing.assert_allclose(X.dot(Y), float(x32.astype(np.float64) @ y32.astype(np.float64)),
+                               rtol=1e-13)
+    X.axpy(0.5, Y)
+    np.testing.assert_allclose(X.export_field(), (x32 + np.float32(0.5) * y32).astype(np.float64),
+                               rtol=1e-6)
+
+
+def test_multifield_vector(ctx):
+    undf = [1000, 3001]
+    rng = np.random.default_rng(4)
+    v = lfx.FieldVector(ctx, undf)
+    w = v.duplicate()
+    a, b = [rng.standard_normal(u) for u in undf], [rng.standard_normal(u) for u in undf]
+    for i in range(2):
+        v.import_field(a[i], i + 1)
+        w.import_field(b[i], i + 1)
+    L = orc.lib()
+    want = 0.0 + L.or_dot(a[0], b[0], undf[0])
+    want = want + L.or_dot(a[1], b[1], undf[1])
+    assert v.dot(w) == want
+    assert v.vector_size() == 2
+    assert v.field_norm(2) == np.sqrt(L.or_sumsq(a[1], undf[1]))
+    with pytest.raises(lfx.LfxError):
+        v.import_field(a[0], 3)
+
+
+# ------------------------------------------------------------------ operators
+@pytest.mark.parametrize("n,nl", [(4, 3), (12, 7), (24, 20)])
+def test_lma_apply_w0_bitwise(ctx, n, nl):
+    p = mg.w0_problem(n, nl, seed=n)
+    sysd = wl.device_w0(ctx, p)
+    op = o_lma(p)
+    x = mg.uniform(99, p.undf)
+    X, Y = sysd.vector(x), sysd.vector()
+    sysd.op.apply(X, Y)
+    assert same(Y.export_field(), op.apply(x))
+    assert same(sysd.diag.export_field(), op.diagonal())
+
+
+@pytest.mark.parametrize("n,nl", [(3, 2), (12, 10), (24, 30)])
+def test_lma_apply_w2_bitwise(ctx, n, nl):
+    p = mg.w2_problem(n, nl, seed=n + 1)
+    sysd = wl.device_w2(ctx, p)
+    op = o_lma(p)
+    x = mg.normal(7, p.undf)
+    X, Y = sysd.vector(x), sysd.vector()
+    sysd.op.apply(X, Y)
+    assert same(Y.export_field(), op.apply(x))
+    assert same(sysd.diag.export_field(), op.diagonal())
+
+
+def test_divergence_and_transpose_bitwise(ctx):
+    q = mg.w2_problem(6, 4, seed=3, keep_parts=True)
+    npc, cic = q.mesh.colour_lookup()
+    m3, u3 = q.extra["map_w3"], q.extra["undf_w3"]
+    D = lfx.LmaOperator(ctx, q.ncell_2d, 4, 1, 6, m3, q.map, u3, q.undf, q.extra["div"], npc, cic)
+    oD = orc.LmaOperator(q.ncell_2d, 4, 1, 6, m3, q.map, u3, q.undf, q.extra["div"], npc, cic)
+    oDt = orc.LmaOperator(q.ncell_2d, 4, 1, 6, m3, q.map, u3, q.undf, q.extra["div"], npc, cic,
+                          transpose=True)
+    u = mg.normal(5, q.undf)
+    w = mg.normal(6, u3)
+    U = lfx.FieldVector.from_array(ctx, u)
+    W = lfx.FieldVector(ctx, [u3])
+    D.apply(U, W)  # dg_matrix_vector: W2 -> W3
+    assert same(W.export_field(), oD.apply(u))
+    W.import_field(w)
+    U2 = lfx.FieldVector(ctx, [q.undf])
+    D.apply_transpose(W, U2)  # transpose_matrix_vector: W3 -> W2
+    assert same(U2.export_field(), oDt.apply(w))
+
+
+def test_lma_fp32_apply(ctx):
+    p = mg.w2_problem(12, 10, seed=8)
+    s32 = wl.device_w2(ctx, p, lfx.R32)
+    x = mg.normal(3, p.undf)
+    X, Y = s32.vector(x), s32.vector()
+    s32.op.apply(X, Y)
+    ref = o_lma(p).apply(x)
+    err = np.linalg.norm(Y.export_field() - ref) / np.linalg.norm(ref)
+    assert err < 1e-6
+
+
+# ------------------------------------------------------------------ CMA
+def test_cma_assembly_and_preconditioner_bitwise(ctx):
+    p = mg.w2_problem(12, 10, seed=5)
+    sysd = wl.device_w2(ctx, p)
+    op = o_lma(p)
+    oprec, band = o_w2_prec(p, op)
+    assert same(sysd.cma.band(), band)
+    x = mg.normal(11, p.undf)
+    X, Y = sysd.vector(x), sysd.vector()
+    sysd.prec.apply(X, Y)
+    assert same(Y.export_field(), oprec.apply(x))
+    # y += A x on the column space (columnwise_op_app)
+    prm = mg.w2v_cma_params(p.nlayers)
+    y0 = mg.normal(12, p.undf)
+    Y.import_field(y0)
+    sysd.cma.apply(X, Y)
+    want = y0.copy()
+    first = np.ascontiguousarray(p.map[:, 4])
+    for c in range(p.ncell_2d):
+        orc.lib().or_columnwise_op_app_code(c + 1, want, x, band, prm["nrow"], prm["nrow"], 3, 1, 1,
+                                            1, 1, first[c:c + 1], prm["indirection"], first[c:c + 1],
+                                            prm["indirection"])
+    assert same(Y.export_field(), want)
+
+
+def test_cma_zero_pivot_is_reported(ctx):
+    nrow, ncell = 5, 3
+    band = np.zeros(3 * nrow * ncell)
+    ind = np.arange(1, nrow + 1, dtype=np.int32)
+    first = np.array([1, 6, 11], dtype=np.int32)
+    cma = lfx.ColumnwiseOperator.from_band(ctx, ncell, nrow, 3, 1, 1, 1, 1, first, ind, band)
+    with pytest.raises(lfx.LfxError) as e:
+        lfx.ColumnwisePreconditioner(ctx, cma, None)
+    assert e.value.status == 2
+
+
+# ------------------------------------------------------------------ solvers
+def test_cg_config0_parity(ctx):
+    """C24 x 20 W0 mass+diffusion, Jacobi CG to 1e-8: the device solve equals
+    the oracle's: same iteration count, bit-identical residual and solution."""
+    p = mg.w0_problem(24, 20, seed=1)
+    sysd = wl.device_w0(ctx, p)
+    op = o_lma(p)
+    x_o, info_o = orc.solve("cg", op, orc.Preconditioner.diagonal(op.diagonal()), p.rhs,
+                            r_tol=1e-8, a_tol=1e-16, max_iter=2000)
+    cg = lfx.ConjugateGradient(sysd.op, sysd.prec, 1e-8, 1e-16, 2000)
+    X, B = sysd.vector(), sysd.vector(p.rhs)
+    info = cg.apply(X, B)
+    assert info.converged and info_o.converged
+    assert info.iterations == info_o.iterations
+    assert abs(info.final_rel - info_o.final_rel) <= 1e-12 * info_o.final_rel
+    assert same(X.export_field(), x_o)
+
+
+@pytest.mark.parametrize("kind", ["bicgstab", "gmres"])
+def test_w0_solvers_parity(ctx, kind):
+    p = mg.w0_problem(12, 10, seed=2)
+    sysd = wl.device_w0(ctx, p)
+    op = o_lma(p)
+    P = orc.Preconditioner.diagonal(op.diagonal())
+    x_o, info_o = orc.solve(kind, op, P, p.rhs, r_tol=1e-8, a_tol=1e-16, max_iter=2000, gcrk=10)
+    if kind == "bicgstab":
+        s = lfx.BiCGStab(sysd.op, sysd.prec, 1e-8, 1e-16, 2000)
+    else:
+        s = lfx.GMRES(sysd.op, sysd.prec, 10, 1e-8, 1e-16, 2000)
+    X, B = sysd.vector(), sysd.vector(p.rhs)
+    info = s.apply(X, B)
+    assert info.converged and info.iterations == info_o.iterations
+    assert abs(info.final_rel - info_o.final_rel) <= 1e-12 * info_o.final_rel
+    assert same(X.export_field(), x_o)
+
+
+@pytest.mark.parametrize("n,nl", [(24, 30), (96, 30)])
+def test_gmres_w2_cma_parity(ctx, n, nl):
+    """W2-W3 Helmholtz GMRES(10) with the column-tridiagonal preconditioner
+    (the C96 x 30 case is the full-size configuration)."""
+    p = mg.w2_problem(n, nl, seed=2)
+    sysd = wl.device_w2(ctx, p)
+    op = o_lma(p)
+    oprec, _ = o_w2_prec(p, op)
+    x_o, info_o = orc.solve("gmres", op, oprec, p.rhs, r_tol=1e-8, a_tol=1e-16, max_iter=200,
+                            gcrk=10)
+    g = lfx.GMRES(sysd.op, sysd.prec, 10, 1e-8, 1e-16, 200)
+    X, B = sysd.vector(), sysd.vector(p.rhs)
+    info = g.apply(X, B)
+    assert info.converged and info.iterations == info_o.iterations
+    assert abs(info.final_rel - info_o.final_rel) <= 1e-12 * info_o.final_rel
+    assert same(X.export_field(), x_o)
+
+
+def test_mixed_precision_refinement(ctx):
+    """FP32 GMRES inside FP64 refinement reaches the 1e-8 true FP64 residual;
+    the solution agrees with the FP64 oracle within the solve tolerance."""
+    p = mg.w2_problem(24, 30, seed=4)
+    s32 = wl.device_w2(ctx, p, lfx.R32)
+    ir = wl.refined_gmres(s32, gcrk=10, inner_rtol=1e-4)
+    X = lfx.FieldVector(ctx, [p.undf])
+    X.set_scalar(0.0)
+    B = lfx.FieldVector.from_array(ctx, p.rhs)
+    info = ir.apply(X, B)
+    assert info.converged and info.final_rel <= 1e-8
+    op = o_lma(p)
+    x = X.export_field()
+    true_rel = np.linalg.norm(p.rhs - op.apply(x)) / np.linalg.norm(p.rhs)
+    assert true_rel <= 1.01e-8
+    oprec, _ = o_w2_prec(p, op)
+    x_o, _ = orc.solve("gmres", op, oprec, p.rhs, r_tol=1e-10, max_iter=200, gcrk=10)
+    assert np.linalg.norm(x - x_o) / np.linalg.norm(x_o) < 1e-6
+
+
+# ------------------------------------------------------------------ edge cases
+def test_zero_rhs_and_nan_and_nonconvergence(ctx):
+    p = mg.w0_problem(6, 4, seed=3)
+    sysd = wl.device_w0(ctx, p)
+    for cls in (lfx.ConjugateGradient, lfx.BiCGStab):
+        X, B = sysd.vector(), sysd.vector()
+        info = cls(sysd.op, sysd.prec, 1e-8, 1e-16, 50).apply(X, B)
+        assert info.converged and info.iterations == 0
+    info = lfx.GMRES(sysd.op, sysd.prec, 5, 1e-8, 1e-16, 50).apply(sysd.vector(), sysd.vector())
+    assert info.converged and info.iterations == 0
+    bad = p.rhs.copy()
+    bad[17] = np.nan
+    with pytest.raises(lfx.LfxError) as e:
+        lfx.ConjugateGradient(sysd.op, sysd.prec, 1e-8, 1e-16, 50).apply(sysd.vector(), sysd.vector(bad))
+    assert e.value.status == 2
+    # one iteration only: reported, and an error when fail_on_non_converged
+    info = lfx.ConjugateGradient(sysd.op, sysd.prec, 1e-8, 1e-16, 1).apply(sysd.vector(),
+                                                                           sysd.vector(p.rhs))
+    assert not info.converged and info.iterations == 1
+    with pytest.raises(lfx.LfxError) as e:
+        lfx.ConjugateGradient(sysd.op, sysd.prec, 1e-8, 1e-16, 1, True, True).apply(
+            sysd.vector(), sysd.vector(p.rhs))
+    assert e.value.status == 1
+
+
+def test_argument_errors(ctx):
+    p = mg.w0_problem(4, 2, seed=1)
+    sysd = wl.device_w0(ctx, p)
+    X = sysd.vector()
+    Y32 = lfx.FieldVector(ctx, [p.undf], lfx.R32)
+    with pytest.raises(lfx.LfxError) as e:
+        sysd.op.apply(X, Y32)
+    assert e.value.status == 5
+    with pytest.raises(lfx.LfxError) as e:
+        X.axpy(1.0, lfx.FieldVector(ctx, [p.undf + 1]))
+    assert e.value.status == 5
+    npc, cic = p.mesh.colour_lookup()
+    cic_bad = cic.copy()
+    cic_bad[0, 0] = cic_bad[0, 1]  # a cell listed twice
+    with pytest.raises(lfx.LfxError) as e:
+        lfx.LmaOperator(ctx, p.ncell_2d, 2, 8, 8, p.map, p.map, p.undf, p.undf, p.lma, npc, cic_bad)
+    assert e.value.status == 4

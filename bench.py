@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the Krylov-solve path on one node.
+
+Workload (one "step" = one complete solve from x0 = 0 to a 1e-8 relative
+residual): W2-W3 Helmholtz-type operator A = M2 + 0.1 D^T D on an extruded
+C96 cubed sphere with 30 levels (1 658 880 cells, 5 031 936 W2 dofs; seeded
+perturbed geometry, b ~ N(0,1)), GMRES(10) preconditioned by a column
+tridiagonal on the vertical faces and Jacobi on the horizontal faces.
+
+  value     solves/s of the mixed-precision solve (FP32 LMA apply and FP32
+            Krylov vectors inside FP64 iterative refinement; residual,
+            correction update and convergence test in FP64), inputs resident
+  fp64      the same solve in plain FP64 (bit-identical to the CPU oracle)
+  e2e       the mixed-precision solve through the C ABI with the right-hand
+            side copied in from pinned host memory and the solution copied
+            out every step
+  roofline  the FP32 LMA apply (dominant kernel) against the measured HBM peak
+  cpu_baseline  the oracle (CPU restatement of the reference) on this host
+
+--impl reference times the oracle port on the host cores instead (the
+reference itself is Fortran + PSyclone and cannot be built here).
+Multi-GPU runs are replicas: every rank solves its own copy of the system.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "solves/sec and p50/p99 latency at 1e-8 rel. residual vs plain FP64, 1 B200"
+N_EDGE, NLAYERS, GCRK, RTOL, SEED = 96, 30, 10, 1e-8, 2
+WORKLOAD = ("C96x30 W2-W3 Helmholtz A=M2+0.1*D^T*D, GMRES(10) + column-tridiagonal(W2V)"
+            " / Jacobi(W2H) preconditioner, solve to 1e-8 rel. residual")
+INNER_RTOL = 1e-4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=3, help="oracle solves timed on the host")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while a timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self._t.join(timeout=2)
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def measured_hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per FP32 apply launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "lma_apply_fp32_c96x30.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+        except ValueError:
+            return None
+    return None
+
+
+def cpu_baseline(problem, nsolves):
+    """The oracle (CPU FP64 restatement of the reference path) on all host
+    threads: full GMRES solves of the same system."""
+    from oracle import oracle as orc
+    from lfric_core_b200 import meshgen as mg
+    p = problem
+    npc, cic = p.mesh.colour_lookup()
+    op = orc.LmaOperator(p.ncell_2d, p.nlayers, 6, 6, p.map, p.map, p.undf, p.undf, p.lma, npc, cic)
+    prm = mg.w2v_cma_params(p.nlayers)
+    band = orc.assemble_cma(mg.lma_block(p.lma, p.mesh.ncell_3d, 6, mg.W2V_DFS), p.ncell_2d,
+                            p.nlayers, prm)
+    P = orc.Preconditioner.cma(p.ncell_2d, prm["nrow"], 3, p.map[:, 4], prm["indirection"], band,
+                               op.diagonal(), p.undf)
+    times, info = [], None
+    for _ in range(nsolves):
+        t0 = time.perf_counter()
+        _, info = orc.solve("gmres", op, P, p.rhs, r_tol=RTOL, max_iter=200, gcrk=GCRK)
+        times.append(time.perf_counter() - t0)
+    cores = os.cpu_count()
+    return {"value": nsolves / sum(times), "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{nsolves} full FP64 GMRES(10) solves of the same C96x30 system "
+                      f"({info.iterations} cycles each), OpenMP on {cores} threads",
+            "p50_ms": 1e3 * statistics.median(times)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from lfric_core_b200 import meshgen as mg
+    p = mg.w2_problem(N_EDGE, NLAYERS, seed=SEED)
+    steps, warm = max(args.steps, 1), max(args.warmup, 0)
+    # each step is one full oracle solve; bounded so the whole run stays short
+    steps = min(steps, 20)
+    cb = cpu_baseline(p, warm) if warm else None
+    cb = cpu_baseline(p, steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": 1e3 / cb["value"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "implementation": "CPU restatement of the reference "
+                       "(Fortran reference not buildable here: no Fortran compiler / PSyclone)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA GPU")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from lfric_core_b200 import lfx, meshgen as mg, workloads as wl
+
+    p = mg.w2_problem(N_EDGE, NLAYERS, seed=SEED)
+    ctx = lfx.Context(local)
+    s64 = wl.device_w2(ctx, p, lfx.R64)
+    s32 = wl.device_w2(ctx, p, lfx.R32, op64=s64.op64, cma=s64.cma, diag64=s64.diag)
+    fp64 = lfx.GMRES(s64.op, s64.prec, GCRK, RTOL, 1e-16, 200)
+    mixed = wl.refined_gmres(s32, gcrk=GCRK, inner_rtol=INNER_RTOL, r_tol=RTOL)
+    B = lfx.FieldVector.from_array(ctx, p.rhs)
+    X = lfx.FieldVector(ctx, [p.undf])
+    R = lfx.FieldVector(ctx, [p.undf])
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    bnorm = B.norm()
+
+    def true_rel():
+        s64.op.apply(X, R)
+        R.aypx(-1.0, B)
+        return R.norm() / bnorm
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def timed(solver, steps, e2e=False, host=None):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        t_all = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        infos = []
+        barrier()
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        l0 = ctx.launch_count()
+        w0 = time.perf_counter()
+        t_all[0].record(stream)
+        for k in range(steps):
+            ev[k][0].record(stream)
+            if e2e:
+                B.import_field(host["rhs"])          # pinned host -> device
+            X.set_scalar(0.0)
+            infos.append(solver.apply(X, B).as_dict())
+            if e2e:
+                host["x"][:] = X.export_field()       # device -> host
+            ev[k][1].record(stream)
+        t_all[1].record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        barrier()
+        lat = [a.elapsed_time(b) for a, b in ev]
+        return {"ms": t_all[0].elapsed_time(t_all[1]), "wall_ms": 1e3 * wall, "lat": lat,
+                "infos": infos, "launches": ctx.launch_count() - l0}
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (also checks both paths reach the tolerance)
+    for _ in range(max(args.warmup, 3)):
+        X.set_scalar(0.0)
+        i64 = fp64.apply(X, B)
+        X.set_scalar(0.0)
+        imx = mixed.apply(X, B)
+    assert i64.converged and imx.converged, (i64.as_dict(), imx.as_dict())
+
+    K = args.steps
+    # mixed precision: the headline, with the apply kernels timed by events
+    ctx.enable_apply_timing(True)
+    ctx.apply_timing(0, reset=True)
+    with ClockSampler(local) as clk:
+        mx = timed(mixed, K)
+    n32, ms32 = ctx.apply_timing(32, reset=False)
+    n64m, ms64m = ctx.apply_timing(64, reset=True)
+    ctx.enable_apply_timing(False)
+    rel_mixed = true_rel()
+    # plain FP64 solve
+    f = timed(fp64, K)
+    rel_fp64 = true_rel()
+    # end to end through the C ABI with pinned host buffers
+    pin = torch.empty(2 * p.undf, dtype=torch.float64, pin_memory=True).numpy()
+    host = {"rhs": pin[:p.undf], "x": pin[p.undf:]}
+    host["rhs"][:] = p.rhs
+    e = timed(mixed, K, e2e=True, host=host)
+
+    t_mx = max_over_ranks(mx["ms"])
+    t_64 = max_over_ranks(f["ms"])
+    t_e2e = max_over_ranks(e["ms"])
+    value = world * K / (t_mx / 1e3)
+    fp64_value = world * K / (t_64 / 1e3)
+    e2e_value = world * K / (t_e2e / 1e3)
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    # roofline of the FP32 LMA apply (dominant kernel of the mixed solve)
+    nc3 = p.mesh.ncell_3d
+    bytes32 = nc3 * 36 * 4 + 2 * p.undf * 4 + p.ncell_2d * 6 * 4
+    avg32 = ms32 / max(n32, 1)
+    achieved = bytes32 / (avg32 / 1e3) / 1e9
+    peak, peak_kind = measured_hbm_peak()
+    traffic = profiled_traffic()
+    roof = {"kernel": "lma_gather<float,6> (FP32 LMA apply)", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": traffic, "algorithmic_bytes_per_launch": bytes32,
+            "launches_timed": n32, "avg_launch_us": round(1e3 * avg32, 2)}
+    if n64m:
+        bytes64 = nc3 * 36 * 8 + 2 * p.undf * 8 + p.ncell_2d * 6 * 4
+        avg64 = ms64m / n64m
+        roof["fp64_apply"] = {"achieved": round(bytes64 / (avg64 / 1e3) / 1e9, 1),
+                              "avg_launch_us": round(1e3 * avg64, 2), "launches_timed": n64m}
+
+    cb = None
+    if world == 1 and not args.no_cpu:
+        cb = cpu_baseline(p, args.cpu_sample)
+
+    def pct(v, q):
+        return float(np.percentile(np.array(v), q))
+
+    inf_mx = mx["infos"][-1]
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": round(t_mx / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 apply + f64 refinement", "data": "synthetic (seeded perturbed geometry, b~N(0,1))",
+        "config": {"workload": WORKLOAD, "ncell_3d": nc3, "undf_w2": p.undf,
+                   "precision": "FP32 LMA/CMA apply and Krylov vectors, FP64 dots, residual, "
+                                "refinement and column factorisation",
+                   "inner": f"GMRES({GCRK}) FP32 to {INNER_RTOL:g}",
+                   "l2": "inputs larger than L2 (FP32 LMA 239 MB, FP64 LMA 478 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "latency_ms": {"p50": round(pct(mx["lat"], 50), 4), "p99": round(pct(mx["lat"], 99), 4)},
+        "final_rel_residual": rel_mixed,
+        "mixed": {"outer_iterations": inf_mx["outer_iterations"],
+                  "inner_cycles": inf_mx["inner_iterations"], "applies": inf_mx["applies"]},
+        "fp64": {"solves_per_s": round(fp64_value, 3), "p50_ms": round(pct(f["lat"], 50), 4),
+                 "p99_ms": round(pct(f["lat"], 99), 4), "cycles": f["infos"][-1]["iterations"],
+                 "final_rel_residual": rel_fp64},
+        "speedup_vs_fp64": round(value / fp64_value, 3),
+        "roofline": roof,
+        "cpu_baseline": cb,
+        "e2e": {"value": round(e2e_value, 3), "unit": "solves/s",
+                "h2d_bytes_per_step": p.undf * 8, "d2h_bytes_per_step": p.undf * 8,
+                "p50_ms": round(pct(e["lat"], 50), 4)},
+        "gpu_launches": mx["launches"],
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

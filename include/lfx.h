@@ -201,12 +201,15 @@ int lfx_refined_solver_create(lfx_ctx* ctx, lfx_op* op64, lfx_solver* inner,
                               double inner_rtol, const lfx_solver_cfg* cfg,
                               lfx_solver** out);
 
-/* Per-kernel device timing of the operator apply inside solves: when
- * enabled, CUDA events bracket every LMA apply launched by solvers of this
- * context; lfx_ctx_apply_timing returns the count and total milliseconds
- * accumulated since the last reset. */
+/* Per-kernel device timing of the operator apply: when enabled, CUDA events
+ * bracket every LMA apply launched on this context; lfx_ctx_apply_timing
+ * returns the count and total milliseconds of the applies of the given
+ * storage precision (0 = all) accumulated since the last reset. */
 int lfx_ctx_enable_apply_timing(lfx_ctx* ctx, int32_t enable);
-int lfx_ctx_apply_timing(lfx_ctx* ctx, int64_t* launches, double* total_ms, int32_t reset);
+int lfx_ctx_apply_timing(lfx_ctx* ctx, int32_t precision, int64_t* launches, double* total_ms,
+                         int32_t reset);
+/* number of kernels this context has launched so far */
+int64_t lfx_ctx_launch_count(const lfx_ctx* ctx);
 
 #ifdef __cplusplus
 }

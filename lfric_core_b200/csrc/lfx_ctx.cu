@@ -58,15 +58,17 @@ int ensure_partials(lfx_ctx* ctx, int64_t n, int nsums) {
   return LFX_OK;
 }
 
-void timing_begin(lfx_ctx* ctx) {
+void timing_begin(lfx_ctx* ctx, int32_t precision) {
   if (!ctx->time_applies) return;
   if (ctx->ev_used + 2 > (int)ctx->ev_pool.size()) {
     for (int i = 0; i < 64; ++i) {
       cudaEvent_t e;
       cudaEventCreate(&e);
       ctx->ev_pool.push_back(e);
+      ctx->ev_prec.push_back(0);
     }
   }
+  ctx->ev_prec[ctx->ev_used] = precision;
   cudaEventRecord(ctx->ev_pool[ctx->ev_used++], ctx->stream);
 }
 
@@ -152,26 +154,34 @@ static int collect_timing(lfx_ctx* ctx) {
     float ms = 0.f;
     cudaError_t e = cudaEventElapsedTime(&ms, ctx->ev_pool[i], ctx->ev_pool[i + 1]);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaEventElapsedTime");
-    ctx->timed_ms += ms;
-    ctx->timed_launches += 1;
+    const int k = ctx->ev_prec[i] == LFX_R32 ? 1 : 0;
+    ctx->timed_ms[k] += ms;
+    ctx->timed_launches[k] += 1;
   }
   ctx->ev_used = 0;
   return LFX_OK;
 }
 
-int lfx_ctx_apply_timing(lfx_ctx* ctx, int64_t* launches, double* total_ms, int32_t reset) {
+int lfx_ctx_apply_timing(lfx_ctx* ctx, int32_t precision, int64_t* launches, double* total_ms,
+                         int32_t reset) {
   if (!ctx) return LFX_INVALID_ARGUMENT;
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
   int rc = collect_timing(ctx);
   if (rc) return rc;
-  if (launches) *launches = ctx->timed_launches;
-  if (total_ms) *total_ms = ctx->timed_ms;
+  const bool all = precision == 0;
+  const int k = precision == LFX_R32 ? 1 : 0;
+  if (launches) *launches = all ? ctx->timed_launches[0] + ctx->timed_launches[1] : ctx->timed_launches[k];
+  if (total_ms) *total_ms = all ? ctx->timed_ms[0] + ctx->timed_ms[1] : ctx->timed_ms[k];
   if (reset) {
-    ctx->timed_launches = 0;
-    ctx->timed_ms = 0.0;
+    for (int j = 0; j < 2; ++j) {
+      ctx->timed_launches[j] = 0;
+      ctx->timed_ms[j] = 0.0;
+    }
   }
   return LFX_OK;
 }
+
+int64_t lfx_ctx_launch_count(const lfx_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 }  // extern "C"
 

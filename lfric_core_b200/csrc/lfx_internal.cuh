@@ -31,12 +31,15 @@ struct lfx_ctx {
   double* d_scalars = nullptr;
   double* h_scalars = nullptr;  // pinned
   int64_t device_bytes = 0;
-  // operator-apply timing inside solves
+  // operator-apply timing: event pairs, the precision of each timed apply,
+  // and running totals per precision (index 0: FP64, 1: FP32)
   bool time_applies = false;
   std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_prec;
   int ev_used = 0;
-  int64_t timed_launches = 0;
-  double timed_ms = 0.0;
+  int64_t timed_launches[2] = {0, 0};
+  double timed_ms[2] = {0.0, 0.0};
+  int64_t launches = 0;  // kernels launched on this context
 };
 
 namespace lfx {
@@ -159,6 +162,7 @@ int launch_chunks(lfx_ctx* ctx, int64_t n, Body body, Fin fin, const int* skip =
   }
   chunk_kernel<NR><<<grid_for(ctx, n), RT, 0, ctx->stream>>>(n, body, fin, ctx->d_partials,
                                                               ctx->d_ticket, skip);
+  ctx->launches++;
   LFX_CK(ctx, cudaGetLastError());
   return LFX_OK;
 }
@@ -246,6 +250,6 @@ namespace lfx {
 int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* skip);
 int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int64_t n,
                     const int* skip);
-void timing_begin(lfx_ctx* ctx);
+void timing_begin(lfx_ctx* ctx, int32_t precision);
 void timing_end(lfx_ctx* ctx);
 }  // namespace lfx

@@ -336,7 +336,8 @@ int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* 
   }
   const LayoutArgs A = args_of(L);
   const int grid = gather_grid(ctx, L->nent);
-  timing_begin(ctx);
+  timing_begin(ctx, op->precision);
+  ctx->launches++;
 #define LAUNCH(T, N)                                                                   \
   lma_gather<T, N><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, \
                                                   (const T*)b, skip)

@@ -164,6 +164,7 @@ int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int6
       return r64 ? k_divide(ctx, (double*)y, (const double*)x, (const double*)p->rdiag, n, skip)
                  : k_divide(ctx, (float*)y, (const float*)x, (const float*)p->rdiag, n, skip);
     case PREC_CMA: {
+      ctx->launches++;
       const int tb = (p->ncell_2d + 127) / 128;
       int rb = (int)std::min<int64_t>(((int64_t)p->nruns + 3) / 4, (int64_t)ctx->num_sms * 8);
       if (p->nruns == 0) rb = 0;

@@ -475,6 +475,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
       }
     }
     gmres_finish_cycle<<<1, 1, 0, ctx->stream>>>(S, h, K);
+    ctx->launches++;
     LFX_CK(ctx, cudaGetLastError());
     // x += sum_iv u(iv) v_iv, one pass, the reference's order per element
     rc = launch_chunks<0>(

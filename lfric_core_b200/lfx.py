@@ -68,7 +68,9 @@ _SIGS = [
     ("lfx_ctx_stream", [vp], vp),
     ("lfx_ctx_device_bytes", [vp], C.c_int64),
     ("lfx_ctx_enable_apply_timing", [vp, C.c_int32], C.c_int),
-    ("lfx_ctx_apply_timing", [vp, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int32], C.c_int),
+    ("lfx_ctx_apply_timing", [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                              C.c_int32], C.c_int),
+    ("lfx_ctx_launch_count", [vp], C.c_int64),
     ("lfx_vec_create", [vp, C.c_int32, i64p, C.c_int32, C.POINTER(vp)], C.c_int),
     ("lfx_vec_duplicate", [vp, C.POINTER(vp)], C.c_int),
     ("lfx_vec_destroy", [vp], C.c_int),
@@ -168,11 +170,17 @@ class Context:
     def enable_apply_timing(self, on: bool = True):
         self.check(self.L.lfx_ctx_enable_apply_timing(self.h, 1 if on else 0))
 
-    def apply_timing(self, reset: bool = True):
+    def apply_timing(self, precision: int = 0, reset: bool = True):
+        """(launches, total ms) of the timed LMA applies of one storage
+        precision (0 = all) since the last reset."""
         n = C.c_int64()
         ms = C.c_double()
-        self.check(self.L.lfx_ctx_apply_timing(self.h, C.byref(n), C.byref(ms), 1 if reset else 0))
+        self.check(self.L.lfx_ctx_apply_timing(self.h, precision, C.byref(n), C.byref(ms),
+                                               1 if reset else 0))
         return n.value, ms.value
+
+    def launch_count(self) -> int:
+        return self.L.lfx_ctx_launch_count(self.h)
 
     def close(self):
         if getattr(self, "h", None):

@@ -111,6 +111,17 @@ int lfx_lma_create_like(const lfx_op* src, const double* local_stencil, int32_t 
                         lfx_op** out);
 int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y);
 int lfx_op_destroy(lfx_op* op);
+/* Apply autotuner (no counterpart in the reference, whose loop shape is fixed
+ * by PSyclone): times each launch configuration of the apply on this
+ * operator -- register gather, and the bulk-copy pipeline with 2..8 stages and
+ * 1..8 warps per block that fit the shared memory -- over `reps` launches and
+ * keeps the fastest for later applies. Outputs (nullable) name the choice:
+ * kernel 0 pipeline / 1 register gather / 2 generic, and its time per apply. */
+int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
+                    float* us);
+/* time one configuration (as above) without keeping it */
+int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps, int32_t reps,
+                      float* us);
 /* diag(A) by mm_diagonal_kernel (sci_mm_diagonal_kernel_mod.F90:99-125) */
 int lfx_lma_diagonal(lfx_op* op, lfx_vec* diag);
 /* transpose apply y = A^T x for a matrix stored as (ncell_3d, ndf_to, ndf_from)
@@ -210,6 +221,14 @@ int lfx_ctx_apply_timing(lfx_ctx* ctx, int32_t precision, int64_t* launches, dou
                          int32_t reset);
 /* number of kernels this context has launched so far */
 int64_t lfx_ctx_launch_count(const lfx_ctx* ctx);
+/* LMA apply kernel for every operator of the context: -1 = each operator's
+ * autotuned choice, else the register gather (default); 0 = force the
+ * bulk-copy pipeline; 1 = force the register gather. All give bit-identical
+ * results. */
+int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which);
+/* LFX_TIMEOUT if a kernel's bounded device-side wait ran out since the last
+ * check (the kernel then skipped its work); synchronises the stream */
+int lfx_ctx_check_device_error(lfx_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -60,6 +60,16 @@ int ensure_partials(lfx_ctx* ctx, int64_t n, int nsums) {
 
 void timing_begin(lfx_ctx* ctx, int32_t precision) {
   if (!ctx->time_applies) return;
+  if (ctx->capture_ev) {
+    TimedPair p{};
+    cudaEventCreate(&p.a);
+    cudaEventCreate(&p.b);
+    p.prec = precision;
+    ctx->capture_ev->push_back(p);
+    // inside a capture only an "external" record becomes an event node
+    cudaEventRecordWithFlags(p.a, ctx->stream, cudaEventRecordExternal);
+    return;
+  }
   if (ctx->ev_used + 2 > (int)ctx->ev_pool.size()) {
     for (int i = 0; i < 64; ++i) {
       cudaEvent_t e;
@@ -74,6 +84,10 @@ void timing_begin(lfx_ctx* ctx, int32_t precision) {
 
 void timing_end(lfx_ctx* ctx) {
   if (!ctx->time_applies) return;
+  if (ctx->capture_ev) {
+    cudaEventRecordWithFlags(ctx->capture_ev->back().b, ctx->stream, cudaEventRecordExternal);
+    return;
+  }
   cudaEventRecord(ctx->ev_pool[ctx->ev_used++], ctx->stream);
 }
 
@@ -103,7 +117,9 @@ int lfx_ctx_create(int device, lfx_ctx** out) {
   }
   int rc = dmalloc(ctx, (void**)&ctx->d_ticket, sizeof(unsigned) * 4);
   if (!rc) rc = dmalloc(ctx, (void**)&ctx->d_scalars, sizeof(double) * 64);
+  if (!rc) rc = dmalloc(ctx, (void**)&ctx->d_err, sizeof(int) * 4);
   if (!rc && cudaMemset(ctx->d_ticket, 0, sizeof(unsigned) * 4) != cudaSuccess) rc = LFX_CUDA_ERROR;
+  if (!rc && cudaMemset(ctx->d_err, 0, sizeof(int) * 4) != cudaSuccess) rc = LFX_CUDA_ERROR;
   if (!rc && cudaMallocHost((void**)&ctx->h_scalars, sizeof(double) * 64) != cudaSuccess)
     rc = LFX_OUT_OF_MEMORY;
   if (!rc) rc = ensure_partials(ctx, (int64_t)RCHUNK * 4096, 1);
@@ -123,6 +139,7 @@ int lfx_ctx_destroy(lfx_ctx* ctx) {
   dfree(ctx, ctx->d_partials, sizeof(double) * ctx->partials_cap);
   dfree(ctx, ctx->d_ticket, sizeof(unsigned) * 4);
   dfree(ctx, ctx->d_scalars, sizeof(double) * 64);
+  dfree(ctx, ctx->d_err, sizeof(int) * 4);
   if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -182,6 +199,24 @@ int lfx_ctx_apply_timing(lfx_ctx* ctx, int32_t precision, int64_t* launches, dou
 }
 
 int64_t lfx_ctx_launch_count(const lfx_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which) {
+  if (!ctx || which < -1 || which > 1) return LFX_INVALID_ARGUMENT;
+  ctx->lma_kernel = which;
+  return LFX_OK;
+}
+
+int lfx_ctx_check_device_error(lfx_ctx* ctx) {
+  if (!ctx) return LFX_INVALID_ARGUMENT;
+  int h = 0;
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  LFX_CK(ctx, cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    LFX_CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int)));
+    return fail(ctx, LFX_TIMEOUT, "a device-side bounded wait ran out (pipeline stage never filled)");
+  }
+  return LFX_OK;
+}
 
 }  // extern "C"
 

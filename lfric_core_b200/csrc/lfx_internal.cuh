@@ -18,6 +18,12 @@
 
 #include "lfx.h"
 
+// a start/stop event pair around one timed operator apply
+struct TimedPair {
+  cudaEvent_t a, b;
+  int prec;
+};
+
 struct lfx_ctx {
   int device = 0;
   int num_sms = 148;
@@ -40,6 +46,11 @@ struct lfx_ctx {
   int64_t timed_launches[2] = {0, 0};
   double timed_ms[2] = {0.0, 0.0};
   int64_t launches = 0;  // kernels launched on this context
+  int lma_kernel = -1;   // -1: per-operator choice, 0: force pipeline, 1: force gather
+  int* d_err = nullptr;  // set by a kernel whose bounded wait ran out
+  // while a solver captures a CUDA graph, timed applies record into fresh
+  // event pairs owned by that graph
+  std::vector<TimedPair>* capture_ev = nullptr;
 };
 
 namespace lfx {
@@ -66,7 +77,7 @@ int ensure_partials(lfx_ctx* ctx, int64_t n, int nsums);
 inline int64_t nchunks(int64_t n) { return (n + RCHUNK - 1) / RCHUNK; }
 inline int grid_for(const lfx_ctx* ctx, int64_t n) {
   int64_t nc = nchunks(n);
-  int64_t cap = (int64_t)ctx->num_sms * 8;
+  int64_t cap = (int64_t)ctx->num_sms * 32;
   int64_t g = nc < cap ? nc : cap;
   return (int)(g < 1 ? 1 : g);
 }
@@ -97,28 +108,44 @@ __device__ __forceinline__ double block_sum(double acc, double* sm) {
   return tot;
 }
 
+// small tuples returned by the load phase of a chunk kernel
+template <class T> struct V1 { T a; };
+template <class T> struct V2 { T a, b; };
+template <class T> struct V3 { T a, b, c; };
+template <class T> struct V4 { T a, b, c, d; };
+
 // Chunked elementwise kernel with NR fixed-order reductions.
-//   body(i, acc)  : work on element i, add into acc[0..NR)
-//   fin(tot)      : run by one thread after every chunk is done, tot[NR]
+//   ld(i)           : load phase for element i, returns a small tuple
+//   op(i, v, acc)   : compute/store phase for element i, adds into acc[0..NR)
+//   fin(tot)        : run by one thread after every chunk is done, tot[NR]
+// All RPER loads of a lane are issued before any store, so stores (which the
+// compiler must assume may alias) do not serialise the loads.
 // skip: optional device flag; when non-zero the kernel does nothing (used by
 // device-resident solvers to idle after convergence).
-template <int NR, class Body, class Fin>
-__global__ void __launch_bounds__(RT) chunk_kernel(int64_t n, Body body, Fin fin,
+template <int NR, class Ld, class Op, class Fin>
+__global__ void __launch_bounds__(RT) chunk_kernel(int64_t n, Ld ld, Op op, Fin fin,
                                                    double* partials, unsigned* ticket,
                                                    const int* skip) {
   if (skip && *((volatile const int*)skip)) return;
   __shared__ double sm[RT / 32];
   __shared__ int am_last;
+  using V = decltype(ld(int64_t(0)));
   const int64_t nch = (n + RCHUNK - 1) / RCHUNK;
   for (int64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
     const int64_t base = ch * RCHUNK + threadIdx.x;
+    V v[RPER];
 #pragma unroll
     for (int m = 0; m < RPER; ++m) {
       const int64_t i = base + (int64_t)m * RT;
-      if (i < n) body(i, acc);
+      if (i < n) v[m] = ld(i);
+    }
+#pragma unroll
+    for (int m = 0; m < RPER; ++m) {
+      const int64_t i = base + (int64_t)m * RT;
+      if (i < n) op(i, v[m], acc);
     }
     if constexpr (NR > 0) {
 #pragma unroll
@@ -154,13 +181,13 @@ struct NoFin {
   __device__ void operator()(const double*) const {}
 };
 
-template <int NR, class Body, class Fin>
-int launch_chunks(lfx_ctx* ctx, int64_t n, Body body, Fin fin, const int* skip = nullptr) {
+template <int NR, class Ld, class Op, class Fin>
+int launch_chunks(lfx_ctx* ctx, int64_t n, Ld ld, Op op, Fin fin, const int* skip = nullptr) {
   if (NR > 0) {
     int rc = ensure_partials(ctx, n, NR);
     if (rc) return rc;
   }
-  chunk_kernel<NR><<<grid_for(ctx, n), RT, 0, ctx->stream>>>(n, body, fin, ctx->d_partials,
+  chunk_kernel<NR><<<grid_for(ctx, n), RT, 0, ctx->stream>>>(n, ld, op, fin, ctx->d_partials,
                                                               ctx->d_ticket, skip);
   ctx->launches++;
   LFX_CK(ctx, cudaGetLastError());
@@ -188,7 +215,7 @@ struct lfx_vec {
 struct lfx_lma_layout {
   int32_t ncell_2d = 0, nlayers = 0, ndf_to = 0, ndf_from = 0;
   int64_t undf_to = 0, undf_from = 0;
-  int32_t nent = 0, ngrp = 0, max_h = 0, max_off = 0;
+  int32_t nent = 0, ngrp = 0, max_h = 0, max_off = 0, max_nrec = 0;
   bool full_cover = true;
   // device arrays
   int32_t* ent_base = nullptr;   // [nent] 0-based first dof
@@ -198,6 +225,13 @@ struct lfx_lma_layout {
   uint32_t* grp_rec = nullptr;   // [ngrp] packed records
   int32_t* map_from = nullptr;   // [ncell_2d*ndf_from] 0-based
   int32_t* map_to = nullptr;     // [ncell_2d*ndf_to] 0-based
+  // packed copies read by the fast kernels: per entity {base, h, g0, g1};
+  // per group {cell, record, map_from row...} padded to gp_stride ints
+  int4* ent_pack = nullptr;
+  int32_t* grp_pack = nullptr;
+  int32_t gp_stride = 0;
+  int32_t max_groups = 0;  // groups of one entity column, at most
+  int32_t max_blocks = 0;  // (cell, df) matrix blocks one entity column reads, at most
   int refcount = 1;
   std::vector<int32_t> rank;         // colour-loop position of every cell
   lfx_lma_layout* tlay = nullptr;    // from-space layout for the transpose apply
@@ -207,9 +241,17 @@ struct lfx_op {
   lfx_ctx* ctx = nullptr;
   lfx_lma_layout* lay = nullptr;  // shared with ops made by lfx_lma_create_like
   int32_t precision = LFX_R64;
-  void* mat = nullptr;  // [cell][df][df2][k]
+  // local matrices [cell][df][df2][k]; each (cell, df) block of ndf2*nlayers
+  // values starts at a multiple of blk elements (blk*elem a multiple of 16
+  // bytes, so a block is one aligned bulk copy)
+  void* mat = nullptr;
   size_t mat_bytes = 0;
-  double* mat64_raw = nullptr;  // FP64 operator keeps nothing else
+  int32_t blk = 0;
+  // apply launch configuration (set by lfx_op_autotune; kernel -1 = default):
+  // kernel 0 bulk-copy pipelined with `stages` and `warps` per block,
+  // kernel 1 register gather, kernel 2 generic gather
+  int32_t tune_kernel = -1, tune_stages = 0, tune_warps = 0;
+  float tune_us = 0.f;
 };
 
 struct lfx_cma {

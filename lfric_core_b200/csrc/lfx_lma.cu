@@ -10,10 +10,14 @@
 // that same order, so the FP64 result equals the coloured scatter bit for
 // bit, with one launch and no atomics.
 //
-// Device layout of the local matrices: [cell][df][df2][k] (k fastest), so a
-// warp that owns one dof column reads each (cell, df, df2) run of nlayers
-// values as one contiguous segment, and each (cell, df) block of
-// ndf2*nlayers values exactly once.
+// Device layout of the local matrices: [cell][df][df2][k] (k fastest), each
+// (cell, df) block padded to a multiple of 16 bytes. A warp owns one dof
+// column ("entity") at a time; the (cell, df) blocks it needs are each read
+// exactly once. The main kernel (lma_tma) streams those blocks into shared
+// memory with bulk asynchronous copies (cp.async.bulk, completion on an
+// mbarrier) several entities ahead of the computation, so HBM reads are
+// large, aligned and always in flight; the lanes then combine them with x
+// gathered from L2.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -25,18 +29,22 @@ using namespace lfx;
 namespace {
 
 struct LayoutArgs {
-  int32_t nent, nlayers, ndf1, ndf2;
+  int32_t nent, nlayers, ndf1, ndf2, blk;
   const int32_t* ent_base;
   const int32_t* ent_h;
   const int32_t* ent_grp;
   const int32_t* grp_cell;
   const uint32_t* grp_rec;
   const int32_t* map_from;
+  const int4* ent_pack;
+  const int32_t* grp_pack;
+  int32_t gp_stride;
 };
 
-LayoutArgs args_of(const lfx_lma_layout* L) {
-  return LayoutArgs{L->nent,     L->nlayers,  L->ndf_to,   L->ndf_from, L->ent_base,
-                    L->ent_h,    L->ent_grp,  L->grp_cell, L->grp_rec,  L->map_from};
+LayoutArgs args_of(const lfx_lma_layout* L, int blk) {
+  return LayoutArgs{L->nent,     L->nlayers,  L->ndf_to,   L->ndf_from, blk,
+                    L->ent_base, L->ent_h,    L->ent_grp,  L->grp_cell, L->grp_rec,
+                    L->map_from, L->ent_pack, L->grp_pack, L->gp_stride};
 }
 
 // packed group record: bits 0-1 nrec (1..3); record r at bit 2+9r: df (6 bits), off (3 bits)
@@ -44,16 +52,60 @@ __host__ __device__ inline int rec_n(uint32_t p) { return p & 3u; }
 __host__ __device__ inline int rec_df(uint32_t p, int r) { return (p >> (2 + 9 * r)) & 63u; }
 __host__ __device__ inline int rec_off(uint32_t p, int r) { return (p >> (8 + 9 * r)) & 7u; }
 
-template <class T, int NDF2>
+// elements per (cell, df) block: ndf2*nl rounded up to 16 bytes
+int block_elems(int ndf2, int nl, size_t esz) {
+  const size_t b = (size_t)ndf2 * nl * esz;
+  return (int)(((b + 15) / 16 * 16) / esz);
+}
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// ---------------------------------------------------------------- kernels
+
+// Generic gather (any ndf, up to three records per group).
+template <class T>
 __global__ void __launch_bounds__(256) lma_gather(LayoutArgs A, const T* __restrict__ M,
                                                   const T* __restrict__ x, T* __restrict__ y,
                                                   const T* __restrict__ b, const int* skip) {
   if (skip && *((volatile const int*)skip)) return;
-  const int ndf2 = NDF2 > 0 ? NDF2 : A.ndf2;
+  const int ndf2 = A.ndf2;
   const int nl = A.nlayers;
   const int lane = threadIdx.x & 31;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const size_t cell_stride = (size_t)A.ndf1 * ndf2 * nl;
+  const size_t cell_stride = (size_t)A.ndf1 * A.blk;
   for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.nent; e += nwarp) {
     const int base = A.ent_base[e], h = A.ent_h[e];
     const int g0 = A.ent_grp[e], g1 = A.ent_grp[e + 1];
@@ -65,28 +117,12 @@ __global__ void __launch_bounds__(256) lma_gather(LayoutArgs A, const T* __restr
         const int nrec = rec_n(pk);
         const T* Mc = M + (size_t)c * cell_stride;
         const int* mf = A.map_from + (size_t)c * ndf2;
-        const int k0 = l - rec_off(pk, 0), k1 = l - rec_off(pk, 1), k2 = l - rec_off(pk, 2);
-        const bool v0 = k0 >= 0 && k0 < nl;
-        const bool v1 = nrec > 1 && k1 >= 0 && k1 < nl;
-        const bool v2 = nrec > 2 && k2 >= 0 && k2 < nl;
-        const T* M0 = Mc + (size_t)rec_df(pk, 0) * ndf2 * nl + k0;
-        const T* M1 = Mc + (size_t)rec_df(pk, 1) * ndf2 * nl + k1;
-        const T* M2 = Mc + (size_t)rec_df(pk, 2) * ndf2 * nl + k2;
-#pragma unroll
-        for (int j = 0; j < (NDF2 > 0 ? NDF2 : 1); ++j) {
-          // NDF2 == 0 falls through to the runtime loop below
-          if (NDF2 == 0) break;
+        for (int j = 0; j < ndf2; ++j) {
           const int xb = mf[j];
-          if (v0) acc = fmaT(__ldg(M0 + j * nl), __ldg(x + xb + k0), acc);
-          if (v1) acc = fmaT(__ldg(M1 + j * nl), __ldg(x + xb + k1), acc);
-          if (v2) acc = fmaT(__ldg(M2 + j * nl), __ldg(x + xb + k2), acc);
-        }
-        if (NDF2 == 0) {
-          for (int j = 0; j < ndf2; ++j) {
-            const int xb = mf[j];
-            if (v0) acc = fmaT(M0[j * nl], x[xb + k0], acc);
-            if (v1) acc = fmaT(M1[j * nl], x[xb + k1], acc);
-            if (v2) acc = fmaT(M2[j * nl], x[xb + k2], acc);
+          for (int r = 0; r < nrec; ++r) {
+            const int k = l - rec_off(pk, r);
+            if (k >= 0 && k < nl)
+              acc = fmaT(Mc[(size_t)rec_df(pk, r) * A.blk + j * nl + k], x[xb + k], acc);
           }
         }
       }
@@ -94,6 +130,202 @@ __global__ void __launch_bounds__(256) lma_gather(LayoutArgs A, const T* __restr
         y[base + l] = b[base + l] - acc;
       else
         y[base + l] = acc;
+    }
+  }
+}
+
+// Register path (no shared memory) for groups of at most two records: all
+// loads of a cell group are issued before the FMA chain that consumes them.
+template <class T, int NDF2>
+__global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __restrict__ M,
+                                                   const T* __restrict__ x, T* __restrict__ y,
+                                                   const T* __restrict__ b, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  const int nl = A.nlayers;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const size_t cell_stride = (size_t)A.ndf1 * A.blk;
+  for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.nent; e += nwarp) {
+    const int4 ep = __ldg(A.ent_pack + e);
+    const int base = ep.x, h = ep.y, g0 = ep.z, g1 = ep.w;
+    for (int l = lane; l < h; l += 32) {
+      T acc = T(0);
+      for (int g = g0; g < g1; ++g) {
+        const int32_t* gp = A.grp_pack + (size_t)g * A.gp_stride;
+        const int c = __ldg(gp);
+        const uint32_t pk = (uint32_t)__ldg(gp + 1);
+        int mf[NDF2];
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) mf[j] = __ldg(gp + 2 + j);
+        const int k0 = l - rec_off(pk, 0), k1 = l - rec_off(pk, 1);
+        const bool v0 = (unsigned)k0 < (unsigned)nl;
+        const bool v1 = rec_n(pk) > 1 && (unsigned)k1 < (unsigned)nl;
+        const T* Mc = M + (size_t)c * cell_stride;
+        const T* M0 = Mc + (size_t)rec_df(pk, 0) * A.blk + (v0 ? k0 : 0);
+        const T* M1 = Mc + (size_t)rec_df(pk, 1) * A.blk + (v1 ? k1 : 0);
+        T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) {
+          a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+          b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
+          a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+          b1[j] = v1 ? __ldg(x + mf[j] + k1) : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) {
+          if (v0) acc = fmaT(a0[j], b0[j], acc);
+          if (v1) acc = fmaT(a1[j], b1[j], acc);
+        }
+      }
+      if (b)
+        y[base + l] = b[base + l] - acc;
+      else
+        y[base + l] = acc;
+    }
+  }
+}
+
+// Shared-memory layout of one warp in lma_tma: S stages, each holding up to
+// MAXB (cell, df) blocks, the stage's mbarrier and the entity's metadata.
+struct TmaMeta {
+  int base, h, ng, nblk;
+  int grp[8 * 10];  // per group: pk, mf[ndf2] (at most 8 groups, ndf2 <= 8)
+};
+
+constexpr unsigned kWaitLimit = 1u << 26;  // bounded mbarrier spin (~seconds)
+
+// Bulk-copy pipelined gather for groups of at most two records, at most
+// MAXG groups per entity and NDF2 <= 8. err receives 1 if a stage wait ran
+// out (then the kernel stops issuing, drains what it issued and returns).
+template <class T, int NDF2>
+__global__ void __launch_bounds__(256) lma_tma(LayoutArgs A, const T* __restrict__ M,
+                                               const T* __restrict__ x, T* __restrict__ y,
+                                               const T* __restrict__ b, const int* skip,
+                                               int stages, int maxb, int* err) {
+  if (skip && *((volatile const int*)skip)) return;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int nl = A.nlayers;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const size_t stage_bytes = (size_t)maxb * A.blk * sizeof(T);
+  const size_t warp_bytes = stages * (stage_bytes + sizeof(TmaMeta) + 16);
+  unsigned char* wsm = smem_raw + wib * warp_bytes;
+  T* buf = (T*)wsm;                                              // [stages][maxb*blk]
+  TmaMeta* meta = (TmaMeta*)(wsm + stages * stage_bytes);        // [stages]
+  uint64_t* bar = (uint64_t*)(wsm + stages * (stage_bytes + sizeof(TmaMeta)));  // [stages]
+  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const size_t cell_stride = (size_t)A.ndf1 * A.blk;
+  const unsigned blk_bytes = (unsigned)(A.blk * sizeof(T));
+
+  // lane 0: read entity i's metadata into stage s and start its block copies
+  auto issue = [&](int64_t e, int s) {
+    const int4 ep = __ldg(A.ent_pack + e);
+    TmaMeta& mt = meta[s];
+    mt.base = ep.x;
+    mt.h = ep.y;
+    mt.ng = ep.w - ep.z;
+    int nb = 0;
+    for (int g = 0; g < mt.ng; ++g) {
+      const int32_t* gp = A.grp_pack + (size_t)(ep.z + g) * A.gp_stride;
+      const int c = __ldg(gp);
+      const int pk = __ldg(gp + 1);
+      mt.grp[g * 10] = pk;
+#pragma unroll
+      for (int j = 0; j < NDF2; ++j) mt.grp[g * 10 + 1 + j] = __ldg(gp + 2 + j);
+      nb += rec_n((uint32_t)pk);
+    }
+    mt.nblk = nb;
+    fence_proxy_async();
+    mbar_expect_tx(&bar[s], (unsigned)nb * blk_bytes);
+    int q = 0;
+    for (int g = 0; g < mt.ng; ++g) {
+      const uint32_t pk = (uint32_t)mt.grp[g * 10];
+      const int c = __ldg(A.grp_pack + (size_t)(ep.z + g) * A.gp_stride);
+      for (int r = 0; r < rec_n(pk); ++r, ++q)
+        bulk_load(buf + (size_t)s * maxb * A.blk + (size_t)q * A.blk,
+                  M + (size_t)c * cell_stride + (size_t)rec_df(pk, r) * A.blk, blk_bytes, &bar[s]);
+    }
+  };
+
+  if (lane == 0) {
+    for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
+    fence_proxy_async();
+  }
+  __syncwarp();
+  // prologue: fill the pipeline
+  if (lane == 0)
+    for (int s = 0; s < stages; ++s) {
+      const int64_t e = warp0 + (int64_t)s * nwarp;
+      if (e < A.nent) issue(e, s);
+    }
+  __syncwarp();
+  int64_t it = 0;
+  bool failed = false;
+  int64_t e = warp0;
+  for (; e < A.nent; e += nwarp, ++it) {
+    const int s = (int)(it % stages);
+    const unsigned parity = (unsigned)((it / stages) & 1);
+    unsigned spins = 0;
+    while (!mbar_try_wait(&bar[s], parity)) {
+      if (++spins > kWaitLimit) {
+        failed = true;
+        break;
+      }
+    }
+    if (__any_sync(0xffffffffu, failed)) {
+      if (lane == 0) atomicExch(err, 1);
+      break;
+    }
+    const TmaMeta& mt = meta[s];
+    const T* sb = buf + (size_t)s * maxb * A.blk;
+    for (int l = lane; l < mt.h; l += 32) {
+      T acc = T(0);
+      int q = 0;
+      for (int g = 0; g < mt.ng; ++g) {
+        const uint32_t pk = (uint32_t)mt.grp[g * 10];
+        const int* mf = &mt.grp[g * 10 + 1];
+        const int k0 = l - rec_off(pk, 0), k1 = l - rec_off(pk, 1);
+        const bool v0 = (unsigned)k0 < (unsigned)nl;
+        const bool v1 = rec_n(pk) > 1 && (unsigned)k1 < (unsigned)nl;
+        const T* s0 = sb + (size_t)q * A.blk + (v0 ? k0 : 0);
+        const T* s1 = v1 ? sb + (size_t)(q + 1) * A.blk + k1 : sb;
+        T b0[NDF2], b1[NDF2];
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) {
+          b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
+          b1[j] = v1 ? __ldg(x + mf[j] + k1) : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) {
+          if (v0) acc = fmaT(s0[j * nl], b0[j], acc);
+          if (v1) acc = fmaT(s1[j * nl], b1[j], acc);
+        }
+        q += rec_n(pk);
+      }
+      if (b)
+        y[mt.base + l] = b[mt.base + l] - acc;
+      else
+        y[mt.base + l] = acc;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const int64_t en = e + (int64_t)stages * nwarp;
+      if (en < A.nent) issue(en, s);
+    }
+    __syncwarp();
+  }
+  if (failed && lane == 0) {
+    // drain: the stages of iterations it .. it+stages-1 may still have copies
+    // in flight; wait (bounded) for each before the shared memory is released
+    for (int k = 0; k < stages; ++k) {
+      const int64_t ik = it + k;
+      if (warp0 + ik * nwarp >= A.nent) break;
+      const int s = (int)(ik % stages);
+      const unsigned parity = (unsigned)((ik / stages) & 1);
+      unsigned spins = 0;
+      while (!mbar_try_wait(&bar[s], parity) && ++spins < kWaitLimit) {
+      }
     }
   }
 }
@@ -106,7 +338,7 @@ __global__ void lma_diag(LayoutArgs A, int max_off, const T* __restrict__ M, T* 
   const int nl = A.nlayers, ndf = A.ndf1;
   const int lane = threadIdx.x & 31;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const size_t cell_stride = (size_t)ndf * ndf * nl;
+  const size_t cell_stride = (size_t)ndf * A.blk;
   for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.nent; e += nwarp) {
     const int base = A.ent_base[e], h = A.ent_h[e];
     for (int l = lane; l < h; l += 32) {
@@ -118,7 +350,7 @@ __global__ void lma_diag(LayoutArgs A, int max_off, const T* __restrict__ M, T* 
           for (int r = 0; r < rec_n(pk); ++r) {
             if (rec_off(pk, r) != o) continue;
             const int k = l - o, df = rec_df(pk, r);
-            if (k >= 0 && k < nl) acc = acc + Mc[((size_t)df * ndf + df) * nl + k];
+            if (k >= 0 && k < nl) acc = acc + Mc[(size_t)df * A.blk + df * nl + k];
           }
       }
       d[base + l] = acc;
@@ -129,16 +361,16 @@ __global__ void lma_diag(LayoutArgs A, int max_off, const T* __restrict__ M, T* 
 // transpose_matrix_vector (transpose_matrix_vector_kernel_mod.F90:128-144):
 // per layer k and from-space dof df, s = sum_j M(ik, j, df) x(map_to(j)+k) and
 // lhs += s. Gather over the from-space layout; records of one cell in
-// increasing k, then increasing df.
+// increasing k, then increasing df. blk is the stored matrix's block stride.
 template <class T>
-__global__ void lma_gather_t(LayoutArgs A, int max_off, const T* __restrict__ M,
+__global__ void lma_gather_t(LayoutArgs A, int max_off, int blk, const T* __restrict__ M,
                              const T* __restrict__ x, const int32_t* __restrict__ map_to,
                              T* __restrict__ y) {
   // here A.ndf1 is the from-space ndf (output), A.ndf2 the to-space ndf
   const int nl = A.nlayers, ndf_out = A.ndf1, ndf_in = A.ndf2;
   const int lane = threadIdx.x & 31;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const size_t cell_stride = (size_t)ndf_out * ndf_in * nl;
+  const size_t cell_stride = (size_t)ndf_in * blk;  // stored as [c][j(to)][df(from)][k]
   for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.nent; e += nwarp) {
     const int base = A.ent_base[e], h = A.ent_h[e];
     for (int l = lane; l < h; l += 32) {
@@ -146,7 +378,7 @@ __global__ void lma_gather_t(LayoutArgs A, int max_off, const T* __restrict__ M,
       for (int g = A.ent_grp[e]; g < A.ent_grp[e + 1]; ++g) {
         const uint32_t pk = A.grp_rec[g];
         const int c = A.grp_cell[g];
-        const T* Mc = M + (size_t)c * cell_stride;  // [c][j(to)][df(from)][k]
+        const T* Mc = M + (size_t)c * cell_stride;
         const int* mt = map_to + (size_t)c * ndf_in;
         for (int o = max_off; o >= 0; --o)
           for (int r = 0; r < rec_n(pk); ++r) {
@@ -155,7 +387,7 @@ __global__ void lma_gather_t(LayoutArgs A, int max_off, const T* __restrict__ M,
             if (k < 0 || k >= nl) continue;
             T s = T(0);
             for (int j = 0; j < ndf_in; ++j)
-              s = fmaT(Mc[((size_t)j * ndf_out + df) * nl + k], x[mt[j] + k], s);
+              s = fmaT(Mc[(size_t)j * blk + df * nl + k], x[mt[j] + k], s);
             acc = acc + s;
           }
       }
@@ -164,21 +396,23 @@ __global__ void lma_gather_t(LayoutArgs A, int max_off, const T* __restrict__ M,
   }
 }
 
-// Fortran (nc3, ndf1, ndf2) FP64 -> [c][df][df2][k] in T
+// Fortran (nc3, ndf1, ndf2) FP64 -> [c][df] blocks of blk elements, [df2][k] inside
 template <class T>
 __global__ void relayout(const double* __restrict__ src, T* __restrict__ dst, int64_t ncell,
-                         int nl, int ndf1, int ndf2) {
-  const int64_t total = ncell * ndf1 * ndf2 * nl;
+                         int nl, int ndf1, int ndf2, int blk) {
+  const int64_t total = ncell * ndf1 * blk;
   const int64_t nc3 = ncell * nl;
   for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < total;
        d += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = d;
-    const int k = (int)(r % nl);
-    r /= nl;
-    const int df2 = (int)(r % ndf2);
-    r /= ndf2;
-    const int df = (int)(r % ndf1);
-    const int64_t c = r / ndf1;
+    const int in = (int)(d % blk);
+    const int64_t cd = d / blk;
+    const int df = (int)(cd % ndf1);
+    const int64_t c = cd / ndf1;
+    if (in >= ndf2 * nl) {
+      dst[d] = T(0);
+      continue;
+    }
+    const int df2 = in / nl, k = in % nl;
     dst[d] = (T)src[(c * nl + k) + nc3 * (df + (int64_t)ndf1 * df2)];
   }
 }
@@ -188,9 +422,12 @@ struct HostRec {
 };
 
 // Builds the gather layout of the space described by `map` (ndf dofs per
-// cell, [c][df] 1-based) for a colouring given as rank[c].
+// cell, [c][df] 1-based) for a colouring given as rank[c]. When mf0 (the
+// 0-based from-space map, ndf_from per cell) is given, the packed records of
+// the fast kernels are built too.
 int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int32_t ndf,
-                 const int32_t* map, int64_t undf, const std::vector<int32_t>& rank) {
+                 const int32_t* map, int64_t undf, const std::vector<int32_t>& rank,
+                 const int32_t* mf0, int32_t ndf_from) {
   std::vector<HostRec> recs;
   recs.reserve((size_t)ncell * ndf);
   for (int32_t c = 0; c < ncell; ++c)
@@ -206,7 +443,7 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
   std::vector<uint32_t> grp_rec;
   size_t i = 0;
   int64_t covered = 0;
-  int max_off = 0, max_h = 0;
+  int max_off = 0, max_h = 0, max_groups = 0, max_blocks = 0;
   while (i < recs.size()) {
     const int32_t base = recs[i].start;
     int32_t end = base + nl;
@@ -227,6 +464,7 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
     covered += end - base;
     ent_grp.push_back((int32_t)grp_cell.size());
     size_t q = 0;
+    int ng = 0, nb = 0;
     while (q < er.size()) {
       size_t r = q;
       uint32_t pk = 0;
@@ -244,10 +482,15 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
         ++r;
       }
       pk |= (uint32_t)n;
+      L->max_nrec = std::max(L->max_nrec, n);
       grp_cell.push_back(er[q].cell);
       grp_rec.push_back(pk);
+      ++ng;
+      nb += n;
       q = r;
     }
+    max_groups = std::max(max_groups, ng);
+    max_blocks = std::max(max_blocks, nb);
     i = j;
   }
   ent_grp.push_back((int32_t)grp_cell.size());
@@ -255,6 +498,8 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
   L->ngrp = (int32_t)grp_cell.size();
   L->max_h = max_h;
   L->max_off = max_off;
+  L->max_groups = max_groups;
+  L->max_blocks = max_blocks;
   L->full_cover = covered == undf;
   int rc = 0;
   auto up = [&](void** dst, const void* src, size_t bytes) {
@@ -268,6 +513,20 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
   up((void**)&L->ent_grp, ent_grp.data(), ent_grp.size() * 4);
   up((void**)&L->grp_cell, grp_cell.data(), grp_cell.size() * 4);
   up((void**)&L->grp_rec, grp_rec.data(), grp_rec.size() * 4);
+  if (mf0) {
+    std::vector<int4> ep(L->nent);
+    for (int32_t e = 0; e < L->nent; ++e) ep[e] = make_int4(ent_base[e], ent_h[e], ent_grp[e], ent_grp[e + 1]);
+    L->gp_stride = (2 + ndf_from + 3) / 4 * 4;
+    std::vector<int32_t> gp((size_t)L->ngrp * L->gp_stride, 0);
+    for (int32_t g = 0; g < L->ngrp; ++g) {
+      int32_t* row = &gp[(size_t)g * L->gp_stride];
+      row[0] = grp_cell[g];
+      row[1] = (int32_t)grp_rec[g];
+      for (int j = 0; j < ndf_from; ++j) row[2 + j] = mf0[(size_t)grp_cell[g] * ndf_from + j];
+    }
+    up((void**)&L->ent_pack, ep.data(), ep.size() * sizeof(int4));
+    up((void**)&L->grp_pack, gp.data(), gp.size() * 4);
+  }
   return rc;
 }
 
@@ -278,6 +537,8 @@ void free_layout(lfx_ctx* ctx, lfx_lma_layout* L) {
   dfree(ctx, L->ent_grp, (size_t)(L->nent + 1) * 4);
   dfree(ctx, L->grp_cell, (size_t)L->ngrp * 4);
   dfree(ctx, L->grp_rec, (size_t)L->ngrp * 4);
+  dfree(ctx, L->ent_pack, (size_t)L->nent * sizeof(int4));
+  dfree(ctx, L->grp_pack, (size_t)L->ngrp * L->gp_stride * 4);
   dfree(ctx, L->map_from, (size_t)L->ncell_2d * L->ndf_from * 4);
   dfree(ctx, L->map_to, (size_t)L->ncell_2d * L->ndf_to * 4);
   free_layout(ctx, L->tlay);
@@ -286,28 +547,30 @@ void free_layout(lfx_ctx* ctx, lfx_lma_layout* L) {
 
 int upload_matrix(lfx_ctx* ctx, lfx_op* op, const double* stencil) {
   const lfx_lma_layout* L = op->lay;
-  const int64_t total = (int64_t)L->ncell_2d * L->ndf_to * L->ndf_from * L->nlayers;
   const size_t esz = op->precision == LFX_R64 ? 8 : 4;
+  op->blk = block_elems(L->ndf_from, L->nlayers, esz);
+  const int64_t total_in = (int64_t)L->ncell_2d * L->ndf_to * L->ndf_from * L->nlayers;
+  const int64_t total = (int64_t)L->ncell_2d * L->ndf_to * op->blk;
   double* raw = nullptr;
-  int rc = dmalloc(ctx, (void**)&raw, (size_t)total * 8);
+  int rc = dmalloc(ctx, (void**)&raw, (size_t)total_in * 8);
   if (rc) return rc;
   rc = dmalloc(ctx, &op->mat, (size_t)total * esz);
   if (rc) {
-    dfree(ctx, raw, (size_t)total * 8);
+    dfree(ctx, raw, (size_t)total_in * 8);
     return rc;
   }
   op->mat_bytes = (size_t)total * esz;
-  LFX_CK(ctx, cudaMemcpyAsync(raw, stencil, (size_t)total * 8, cudaMemcpyHostToDevice, ctx->stream));
+  LFX_CK(ctx, cudaMemcpyAsync(raw, stencil, (size_t)total_in * 8, cudaMemcpyHostToDevice, ctx->stream));
   const int grid = ctx->num_sms * 16;
   if (op->precision == LFX_R64)
     relayout<double><<<grid, 256, 0, ctx->stream>>>(raw, (double*)op->mat, L->ncell_2d, L->nlayers,
-                                                     L->ndf_to, L->ndf_from);
+                                                     L->ndf_to, L->ndf_from, op->blk);
   else
     relayout<float><<<grid, 256, 0, ctx->stream>>>(raw, (float*)op->mat, L->ncell_2d, L->nlayers,
-                                                    L->ndf_to, L->ndf_from);
+                                                    L->ndf_to, L->ndf_from, op->blk);
   LFX_CK(ctx, cudaGetLastError());
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
-  dfree(ctx, raw, (size_t)total * 8);
+  dfree(ctx, raw, (size_t)total_in * 8);
   return LFX_OK;
 }
 
@@ -316,6 +579,124 @@ int gather_grid(const lfx_ctx* ctx, int32_t nent) {
   int64_t cap = (int64_t)ctx->num_sms * 16;
   if (g > cap) g = cap;
   return (int)(g < 1 ? 1 : g);
+}
+
+// launch shape of lma_tma: warps per block and pipeline stages, with the
+// dynamic shared memory they need (0 warps when the operator does not fit)
+struct TmaShape {
+  int warps = 0, stages = 0;
+  size_t smem = 0;
+};
+constexpr size_t kTmaSmemMax = 96 * 1024;
+
+bool tma_ok(const lfx_op* op) {
+  const lfx_lma_layout* L = op->lay;
+  // the kernel is instantiated for ndf_from 1, 6 and 8 only; its metadata
+  // holds at most 8 groups of at most 2 records
+  if (L->max_nrec > 2 || L->max_groups > 8) return false;
+  return L->ndf_from == 1 || L->ndf_from == 6 || L->ndf_from == 8;
+}
+
+TmaShape tma_shape(const lfx_op* op, int stages, int warps) {
+  TmaShape t;
+  if (!tma_ok(op) || stages < 1 || warps < 1) return t;
+  const size_t esz = op->precision == LFX_R64 ? 8 : 4;
+  const size_t stage = (size_t)op->lay->max_blocks * op->blk * esz;
+  const size_t per_warp = stages * (stage + sizeof(TmaMeta) + 16);
+  if (per_warp * warps > kTmaSmemMax) return t;
+  t.warps = warps;
+  t.stages = stages;
+  t.smem = per_warp * warps;
+  return t;
+}
+
+TmaShape tma_default(const lfx_op* op) {
+  for (int stages = 4; stages >= 2; --stages)
+    for (int warps = 4; warps >= 1; warps >>= 1) {
+      TmaShape t = tma_shape(op, stages, warps);
+      if (t.warps) return t;
+    }
+  return TmaShape{};
+}
+
+template <class T, int N>
+void launch_tma(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const TmaShape& ts,
+                const void* x, void* y, const void* b, const int* skip) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(lma_tma<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kTmaSmemMax);
+    attr = true;
+  }
+  // persistent warps: one resident wave of blocks, each warp walking its
+  // entity columns with `stages` of them in flight
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_tma<T, N>, 32 * ts.warps, ts.smem);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = (int)std::min<int64_t>(((int64_t)A.nent + ts.warps - 1) / ts.warps,
+                                          (int64_t)ctx->num_sms * per_sm);
+  lma_tma<T, N><<<grid, 32 * ts.warps, ts.smem, ctx->stream>>>(
+      A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip, ts.stages,
+      op->lay->max_blocks, ctx->d_err);
+}
+
+// kernel: 0 bulk-copy pipelined (shape ts), 1 register gather, 2 generic
+template <class T>
+void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& ts,
+                    const void* x, void* y, const void* b, const int* skip) {
+  const lfx_lma_layout* L = op->lay;
+  const LayoutArgs A = args_of(L, op->blk);
+  if (kernel == 0) {
+    switch (L->ndf_from) {
+      case 1: launch_tma<T, 1>(ctx, op, A, ts, x, y, b, skip); return;
+      case 6: launch_tma<T, 6>(ctx, op, A, ts, x, y, b, skip); return;
+      default: launch_tma<T, 8>(ctx, op, A, ts, x, y, b, skip); return;
+    }
+  }
+  const int grid = gather_grid(ctx, L->nent);
+  if (kernel == 1) {
+    switch (L->ndf_from) {
+      case 1: lma_gather2<T, 1><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
+      case 6: lma_gather2<T, 6><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
+      default: lma_gather2<T, 8><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
+    }
+  }
+  lma_gather<T><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y,
+                                               (const T*)b, skip);
+}
+
+// the register gather needs at most two records per group and ndf_from 1, 6 or 8
+bool gather2_ok(const lfx_op* op) {
+  const lfx_lma_layout* L = op->lay;
+  return L->max_nrec <= 2 && (L->ndf_from == 1 || L->ndf_from == 6 || L->ndf_from == 8);
+}
+
+void launch_apply(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& ts, const void* x,
+                  void* y, const void* b, const int* skip) {
+  if (op->precision == LFX_R64)
+    launch_apply_t<double>(ctx, op, kernel, ts, x, y, b, skip);
+  else
+    launch_apply_t<float>(ctx, op, kernel, ts, x, y, b, skip);
+}
+
+// the configuration an apply of this operator uses
+void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts) {
+  *ts = TmaShape{};
+  if (ctx->lma_kernel == 0 && tma_ok(op)) {
+    *kernel = 0;
+    *ts = tma_default(op);
+    if (ts->warps) return;
+  }
+  if (ctx->lma_kernel == 1 && gather2_ok(op)) {
+    *kernel = 1;
+    return;
+  }
+  if (ctx->lma_kernel < 0 && op->tune_kernel >= 0) {
+    *kernel = op->tune_kernel;
+    if (*kernel == 0) *ts = tma_shape(op, op->tune_stages, op->tune_warps);
+    if (*kernel != 0 || ts->warps) return;
+  }
+  *kernel = gather2_ok(op) ? 1 : 2;
 }
 
 }  // namespace
@@ -334,29 +715,12 @@ int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* 
     else
       LFX_CK(ctx, cudaMemsetAsync(y, 0, L->undf_to * esz, ctx->stream));
   }
-  const LayoutArgs A = args_of(L);
-  const int grid = gather_grid(ctx, L->nent);
+  int kernel = 2;
+  TmaShape ts;
+  pick_apply(ctx, op, &kernel, &ts);
   timing_begin(ctx, op->precision);
   ctx->launches++;
-#define LAUNCH(T, N)                                                                   \
-  lma_gather<T, N><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, \
-                                                  (const T*)b, skip)
-  if (op->precision == LFX_R64) {
-    switch (L->ndf_from) {
-      case 1: LAUNCH(double, 1); break;
-      case 6: LAUNCH(double, 6); break;
-      case 8: LAUNCH(double, 8); break;
-      default: LAUNCH(double, 0); break;
-    }
-  } else {
-    switch (L->ndf_from) {
-      case 1: LAUNCH(float, 1); break;
-      case 6: LAUNCH(float, 6); break;
-      case 8: LAUNCH(float, 8); break;
-      default: LAUNCH(float, 0); break;
-    }
-  }
-#undef LAUNCH
+  launch_apply(ctx, op, kernel, ts, x, y, b, skip);
   timing_end(ctx);
   LFX_CK(ctx, cudaGetLastError());
   return LFX_OK;
@@ -398,6 +762,14 @@ int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_
   }
   if (pos != ncell_2d)
     return fail(ctx, LFX_INVALID_ARGUMENT, "colouring does not list every cell exactly once");
+  // 0-based maps
+  std::vector<int32_t> mf((size_t)ncell_2d * ndf_from), mt((size_t)ncell_2d * ndf_to);
+  for (size_t i = 0; i < mf.size(); ++i) {
+    mf[i] = map_from[i] - 1;
+    if (mf[i] < 0 || (int64_t)mf[i] + nlayers > undf_from)
+      return fail(ctx, LFX_INVALID_ARGUMENT, "from-space dofmap entry out of range");
+  }
+  for (size_t i = 0; i < mt.size(); ++i) mt[i] = map_to[i] - 1;
   lfx_lma_layout* L = new lfx_lma_layout();
   L->ncell_2d = ncell_2d;
   L->nlayers = nlayers;
@@ -405,15 +777,8 @@ int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_
   L->ndf_from = ndf_from;
   L->undf_to = undf_to;
   L->undf_from = undf_from;
-  int rc = build_layout(ctx, L, ncell_2d, nlayers, ndf_to, map_to, undf_to, rank);
-  // 0-based maps on the device
-  std::vector<int32_t> mf((size_t)ncell_2d * ndf_from), mt((size_t)ncell_2d * ndf_to);
-  for (size_t i = 0; i < mf.size(); ++i) {
-    mf[i] = map_from[i] - 1;
-    if (mf[i] < 0 || (int64_t)mf[i] + nlayers > undf_from)
-      rc = rc ? rc : fail(ctx, LFX_INVALID_ARGUMENT, "from-space dofmap entry out of range");
-  }
-  for (size_t i = 0; i < mt.size(); ++i) mt[i] = map_to[i] - 1;
+  int rc = build_layout(ctx, L, ncell_2d, nlayers, ndf_to, map_to, undf_to, rank, mf.data(),
+                        ndf_from);
   if (!rc) rc = dmalloc(ctx, (void**)&L->map_from, mf.size() * 4);
   if (!rc) rc = dmalloc(ctx, (void**)&L->map_to, mt.size() * 4);
   if (!rc) cudaMemcpy(L->map_from, mf.data(), mf.size() * 4, cudaMemcpyHostToDevice);
@@ -474,6 +839,86 @@ int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y) {
   return op_apply_impl(op, x->data[0], y->data[0], nullptr, nullptr);
 }
 
+// Times `reps` applies of one launch configuration on scratch vectors.
+int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps, int32_t reps,
+                      float* us) {
+  if (!op || !us || reps < 1 || kernel < 0 || kernel > 2) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = op->ctx;
+  const lfx_lma_layout* L = op->lay;
+  TmaShape ts;
+  if (kernel == 0) {
+    ts = tma_shape(op, stages, warps);
+    if (!ts.warps) return fail(ctx, LFX_NOT_SUPPORTED, "configuration does not fit this operator");
+  }
+  if (kernel == 1 && !gather2_ok(op))
+    return fail(ctx, LFX_NOT_SUPPORTED, "register gather does not fit this operator");
+  const size_t esz = op->precision == LFX_R64 ? 8 : 4;
+  void *x = nullptr, *y = nullptr;
+  int rc = dmalloc(ctx, &x, L->undf_from * esz);
+  if (!rc) rc = dmalloc(ctx, &y, L->undf_to * esz);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!rc) {
+    cudaMemsetAsync(x, 0, L->undf_from * esz, ctx->stream);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    launch_apply(ctx, op, kernel, ts, x, y, nullptr, nullptr);  // warm
+    cudaEventRecord(e0, ctx->stream);
+    for (int r = 0; r < reps; ++r) launch_apply(ctx, op, kernel, ts, x, y, nullptr, nullptr);
+    cudaEventRecord(e1, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+      rc = fail(ctx, LFX_CUDA_ERROR, "apply timing failed");
+    float ms = 0.f;
+    if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+    *us = 1e3f * ms / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  dfree(ctx, x, L->undf_from * esz);
+  dfree(ctx, y, L->undf_to * esz);
+  if (!rc) rc = lfx_ctx_check_device_error(ctx);
+  return rc;
+}
+
+// Picks the fastest apply configuration for this operator by timing the
+// candidates (register gather; bulk-copy pipeline with 2..8 stages and 1..8
+// warps per block that fit the shared memory) and keeps it for later applies.
+int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
+                    float* us) {
+  if (!op) return LFX_INVALID_ARGUMENT;
+  int bk = -1, bs = 0, bw = 0;
+  float best = 3.4e38f;
+  auto consider = [&](int k, int s, int w) -> int {
+    float t = 0.f;
+    int rc = lfx_op_time_apply(op, k, s, w, reps, &t);
+    if (rc == LFX_NOT_SUPPORTED) return LFX_OK;
+    if (rc) return rc;
+    if (t < best) {
+      best = t;
+      bk = k;
+      bs = s;
+      bw = w;
+    }
+    return LFX_OK;
+  };
+  int rc = LFX_OK;
+  if (gather2_ok(op)) rc = consider(1, 0, 0);
+  else rc = consider(2, 0, 0);
+  if (!rc && tma_ok(op))
+    for (int s : {2, 3, 4, 6, 8})
+      for (int w : {1, 2, 4, 8})
+        if (!rc && tma_shape(op, s, w).warps) rc = consider(0, s, w);
+  if (rc) return rc;
+  op->tune_kernel = bk;
+  op->tune_stages = bs;
+  op->tune_warps = bw;
+  op->tune_us = best;
+  if (kernel) *kernel = bk;
+  if (stages) *stages = bs;
+  if (warps) *warps = bw;
+  if (us) *us = best;
+  return LFX_OK;
+}
+
 int lfx_lma_diagonal(lfx_op* op, lfx_vec* diag) {
   if (!op || !diag) return LFX_INVALID_ARGUMENT;
   lfx_ctx* ctx = op->ctx;
@@ -484,7 +929,8 @@ int lfx_lma_diagonal(lfx_op* op, lfx_vec* diag) {
     return fail(ctx, LFX_TYPE_MISMATCH, "diagonal vector does not match the operator");
   if (!L->full_cover)
     LFX_CK(ctx, cudaMemsetAsync(diag->data[0], 0, L->undf_to * diag->elem(), ctx->stream));
-  const LayoutArgs A = args_of(L);
+  const LayoutArgs A = args_of(L, op->blk);
+  ctx->launches++;
   if (op->precision == LFX_R64)
     lma_diag<double><<<gather_grid(ctx, L->nent), 256, 0, ctx->stream>>>(
         A, L->max_off, (const double*)op->mat, (double*)diag->data[0]);
@@ -516,7 +962,7 @@ int lfx_op_apply_transpose(lfx_op* op, const lfx_vec* x, lfx_vec* y) {
     T->undf_to = L->undf_from;
     T->undf_from = L->undf_to;
     int rc = build_layout(ctx, T, L->ncell_2d, L->nlayers, L->ndf_from, mf.data(), L->undf_from,
-                          L->rank);
+                          L->rank, nullptr, 0);
     if (rc) {
       free_layout(ctx, T);
       return rc;
@@ -526,16 +972,15 @@ int lfx_op_apply_transpose(lfx_op* op, const lfx_vec* x, lfx_vec* y) {
   lfx_lma_layout* T = L->tlay;
   if (!T->full_cover)
     LFX_CK(ctx, cudaMemsetAsync(y->data[0], 0, T->undf_to * y->elem(), ctx->stream));
-  LayoutArgs A = args_of(T);
-  // the stored matrix is [c][df_to][df_from][k]; lma_gather_t indexes it as
-  // [c][j(in)][df(out)][k] with in = to-space, out = from-space
+  LayoutArgs A = args_of(T, op->blk);
+  ctx->launches++;
   if (op->precision == LFX_R64)
     lma_gather_t<double><<<gather_grid(ctx, T->nent), 256, 0, ctx->stream>>>(
-        A, T->max_off, (const double*)op->mat, (const double*)x->data[0], L->map_to,
+        A, T->max_off, op->blk, (const double*)op->mat, (const double*)x->data[0], L->map_to,
         (double*)y->data[0]);
   else
     lma_gather_t<float><<<gather_grid(ctx, T->nent), 256, 0, ctx->stream>>>(
-        A, T->max_off, (const float*)op->mat, (const float*)x->data[0], L->map_to,
+        A, T->max_off, op->blk, (const float*)op->mat, (const float*)x->data[0], L->map_to,
         (float*)y->data[0]);
   LFX_CK(ctx, cudaGetLastError());
   return LFX_OK;

@@ -33,15 +33,17 @@ __host__ __device__ inline int floor_div_i(int a, int b) {
   return a >= 0 ? a / b : -((-a + b - 1) / b);
 }
 
-// columnwise_op_asm on a sub-block (dfs) of an FP64 LMA stored [c][df][df2][k]
-__global__ void cma_asm(int ncell, int nl, int ndf_full, const double* __restrict__ M, int nsub,
-                        const int* __restrict__ dfs, const int* __restrict__ cbd, int nrow, int bw,
-                        int alpha, int beta, int gamma_p, double* __restrict__ band) {
+// columnwise_op_asm on a sub-block (dfs) of an FP64 LMA stored [c][df] blocks
+// of blk elements, [df2][k] inside
+__global__ void cma_asm(int ncell, int nl, int ndf_full, int blk, const double* __restrict__ M,
+                        int nsub, const int* __restrict__ dfs, const int* __restrict__ cbd,
+                        int nrow, int bw, int alpha, int beta, int gamma_p,
+                        double* __restrict__ band) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   double* col = band + (size_t)c * bw * nrow;
   for (int i = 0; i < bw * nrow; ++i) col[i] = 0.0;
-  const double* Mc = M + (size_t)c * ndf_full * ndf_full * nl;
+  const double* Mc = M + (size_t)c * ndf_full * blk;
   for (int k = 1; k <= nl; ++k)
     for (int a = 0; a < nsub; ++a) {
       const int i = cbd[a + nsub * (k - 1)];
@@ -50,7 +52,7 @@ __global__ void cma_asm(int ncell, int nl, int ndf_full, const double* __restric
         const int j = cbd[b + nsub * (k - 1)];
         if (j - jm < 0 || j - jm >= bw) continue;  // outside the band (host validates)
         double* e = &col[(j - jm) + (size_t)bw * (i - 1)];
-        *e = *e + Mc[((size_t)dfs[a] * ndf_full + dfs[b]) * nl + (k - 1)];
+        *e = *e + Mc[(size_t)dfs[a] * blk + (size_t)dfs[b] * nl + (k - 1)];
       }
     }
 }
@@ -135,8 +137,15 @@ __global__ void __launch_bounds__(128) cma_prec_apply(
 
 template <class T>
 int k_divide(lfx_ctx* ctx, T* y, const T* x, const T* d, int64_t n, const int* skip) {
-  return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { y[i] = x[i] / d[i]; },
-                          NoFin{}, skip);
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V2<T>{x[i], d[i]}; },
+      [=] __device__(int64_t i, const V2<T>& v, double*) { y[i] = v.a / v.b; }, NoFin{}, skip);
+}
+template <class S, class D>
+int k_cast(lfx_ctx* ctx, D* d, const S* s, int64_t n, const int* skip) {
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V1<S>{s[i]}; },
+      [=] __device__(int64_t i, const V1<S>& v, double*) { d[i] = (D)v.a; }, NoFin{}, skip);
 }
 
 }  // namespace
@@ -149,17 +158,8 @@ int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int6
   const bool r64 = precision == LFX_R64;
   switch (p->kind) {
     case PREC_NULL:
-      if (r64) {
-        const double* xs = (const double*)x;
-        double* ys = (double*)y;
-        return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { ys[i] = xs[i]; },
-                                NoFin{}, skip);
-      } else {
-        const float* xs = (const float*)x;
-        float* ys = (float*)y;
-        return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { ys[i] = xs[i]; },
-                                NoFin{}, skip);
-      }
+      return r64 ? k_cast(ctx, (double*)y, (const double*)x, n, skip)
+                 : k_cast(ctx, (float*)y, (const float*)x, n, skip);
     case PREC_DIAG:
       return r64 ? k_divide(ctx, (double*)y, (const double*)x, (const double*)p->rdiag, n, skip)
                  : k_divide(ctx, (float*)y, (const float*)x, (const float*)p->rdiag, n, skip);
@@ -195,13 +195,9 @@ static int copy_diag(lfx_ctx* ctx, const lfx_vec* diag, int32_t precision, void*
   if (diag->precision == precision) {
     LFX_CK(ctx, cudaMemcpyAsync(*out, diag->data[0], n * esz, cudaMemcpyDeviceToDevice, ctx->stream));
   } else if (precision == LFX_R32) {
-    float* d = (float*)*out;
-    const double* s = (const double*)diag->data[0];
-    rc = launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { d[i] = (float)s[i]; }, NoFin{});
+    rc = k_cast(ctx, (float*)*out, (const double*)diag->data[0], n, nullptr);
   } else {
-    double* d = (double*)*out;
-    const float* s = (const float*)diag->data[0];
-    rc = launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { d[i] = (double)s[i]; }, NoFin{});
+    rc = k_cast(ctx, (double*)*out, (const float*)diag->data[0], n, nullptr);
   }
   return rc;
 }
@@ -303,8 +299,8 @@ int lfx_cma_assemble_from_lma(const lfx_op* lma, int32_t nsub, const int32_t* df
     cudaMemcpy(d_dfs, d0.data(), 4 * (size_t)nsub, cudaMemcpyHostToDevice);
     cudaMemcpy(d_cbd, column_banded_dofmap, 4 * (size_t)nsub * L->nlayers, cudaMemcpyHostToDevice);
     cma_asm<<<(L->ncell_2d + 127) / 128, 128, 0, ctx->stream>>>(
-        L->ncell_2d, L->nlayers, L->ndf_to, (const double*)lma->mat, nsub, d_dfs, d_cbd, nrow,
-        bandwidth, alpha, beta, gamma_p, (*out)->band);
+        L->ncell_2d, L->nlayers, L->ndf_to, lma->blk, (const double*)lma->mat, nsub, d_dfs, d_cbd,
+        nrow, bandwidth, alpha, beta, gamma_p, (*out)->band);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
       rc = fail(ctx, LFX_CUDA_ERROR, "CMA assembly kernel failed");
   }

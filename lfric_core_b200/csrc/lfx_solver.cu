@@ -6,13 +6,16 @@
 // Every scalar of the recurrences lives in device memory and is updated by the
 // last block of the fused reduction kernel that produces it (see
 // chunk_kernel), so an iteration issues no host round trip. Kernels take a
-// "done" flag and return at once when it is set; the host launches work in
-// batches and reads the flag once per batch. Vector updates that the
-// reference performs as separate builtins are fused when the fusion does not
-// change a single rounding (e.g. t = r; t += a v  ==>  t = fma(a, v, r)).
+// "done" flag and return at once when it is set. The kernel sequence of one
+// GMRES restart cycle, or of 8 CG / BiCGStab iterations, is captured once into
+// a CUDA graph (per solution / right-hand-side buffer pair) and replayed; the
+// host reads the flag once per replay. Vector updates that the reference
+// performs as separate builtins are fused when the fusion does not change a
+// single rounding (e.g. t = r; t += a v  ==>  t = fma(a, v, r)).
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <functional>
 
 #include "lfx_internal.cuh"
 
@@ -28,21 +31,28 @@ constexpr double EPS_RDEF = DBL_EPSILON;  // constants_mod.F90:167
 
 struct DevState {
   int done, converged, iter, status;
-  int applies, monitor, max_iter, pad;
+  int applies, monitor, max_iter, askip;  // askip: skip the rest of a GMRES cycle
+  int m, inner_mode, pad0, pad1;          // m: Krylov vectors used by the cycle
   double r_tol, a_tol;
   double r_nrm_0, r_nrm, rz, alpha, neg_alpha, beta;
   // bicgstab
   double rho, rho_old, omega, coef, tt, ts, sc_err, err;
   // gmres
-  double gbeta, inv_beta, res_norm, inv_hn;
+  double gbeta, gbeta0, inv_beta, res_norm, inv_hn;
 };
 
 struct VecPtrs {
   const void* p[MAX_GCRK];
 };
 
-template <class T>
-struct Tsel {};
+struct GraphEntry {
+  const void* x = nullptr;
+  const void* b = nullptr;
+  bool timed = false;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<TimedPair> ev;  // apply-timing events recorded by the graph
+  int64_t kernels = 0;
+};
 
 }  // namespace
 
@@ -57,7 +67,9 @@ struct lfx_solver {
   std::vector<void*> work;  // owned device vectors of n elements
   DevState* d_state = nullptr;
   DevState* h_state = nullptr;  // pinned
-  double* d_gm = nullptr;       // gmres: H, negH, g, u
+  double* d_gm = nullptr;       // gmres: H, negH, g, u, cs, sn
+  bool inner_mode = false;      // GMRES used as the inner solve of a refinement
+  std::vector<GraphEntry> graphs;
   // refined solver
   lfx_solver* inner = nullptr;
   double inner_rtol = 0.0;
@@ -68,6 +80,7 @@ struct lfx_solver {
 namespace {
 
 size_t esz(int32_t p) { return p == LFX_R64 ? 8 : 4; }
+size_t gm_doubles(int K) { return 2 * (size_t)(K + 1) * K + (K + 1) + 3 * (size_t)K + 8; }
 
 int read_state(lfx_solver* s) {
   lfx_ctx* ctx = s->ctx;
@@ -83,10 +96,85 @@ int init_state(lfx_solver* s) {
   h.a_tol = s->cfg.a_tol;
   h.max_iter = s->cfg.max_iter;
   h.monitor = s->cfg.monitor_convergence ? 1 : 0;
+  h.inner_mode = s->inner_mode ? 1 : 0;
+  h.m = s->cfg.gcrk;
   *s->h_state = h;
   LFX_CK(s->ctx, cudaMemcpyAsync(s->d_state, s->h_state, sizeof(DevState), cudaMemcpyHostToDevice,
                                  s->ctx->stream));
   return LFX_OK;
+}
+
+// Runs `body` (a fixed sequence of launches on the context stream) through a
+// CUDA graph cached per (x, b) pair, then reads the device state.
+int run_graph(lfx_solver* s, const void* x, const void* b, const std::function<int()>& body) {
+  lfx_ctx* ctx = s->ctx;
+  GraphEntry* ge = nullptr;
+  for (auto& g : s->graphs)
+    if (g.x == x && g.b == b && g.timed == ctx->time_applies) ge = &g;
+  if (!ge) {
+    GraphEntry g;
+    g.x = x;
+    g.b = b;
+    g.timed = ctx->time_applies;
+    cudaGraph_t graph = nullptr;
+    LFX_CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    std::vector<TimedPair> ev;
+    ctx->capture_ev = &ev;
+    const int64_t l0 = ctx->launches;
+    int rc = body();
+    ctx->capture_ev = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (rc || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      for (auto& p : ev) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+      }
+      return rc ? rc : cuda_fail(ctx, e, "cudaStreamEndCapture");
+    }
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+    g.ev = std::move(ev);
+    g.kernels = ctx->launches - l0;  // kernels in one replay (capture launched none)
+    ctx->launches = l0;
+    s->graphs.push_back(std::move(g));
+    ge = &s->graphs.back();
+  }
+  LFX_CK(ctx, cudaGraphLaunch(ge->exec, ctx->stream));
+  ctx->launches += ge->kernels;
+  int rc = read_state(s);
+  if (rc) return rc;
+  if (ctx->time_applies) {
+    for (auto& p : ge->ev) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+        const int k = p.prec == LFX_R32 ? 1 : 0;
+        ctx->timed_ms[k] += ms;
+        ctx->timed_launches[k] += 1;
+      }
+    }
+  }
+  return LFX_OK;
+}
+
+void free_graphs(lfx_solver* s) {
+  for (auto& g : s->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& p : g.ev) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+  }
+  s->graphs.clear();
+}
+
+template <class T>
+int norm_kernel(lfx_ctx* ctx, int64_t n, const T* v, double* out, const int* skip) {
+  return launch_chunks<1>(
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{v[i]}; },
+      [=] __device__(int64_t, const V1<T>& q, double* a) { a[0] = fma((double)q.a, (double)q.a, a[0]); },
+      [=] __device__(const double* t) { *out = sqrt(t[0]); }, skip);
 }
 
 // ------------------------------------------------------------------ CG
@@ -103,7 +191,8 @@ int cg_run(lfx_solver* s, T* x, const T* b) {
   // r = b - A x   (apply, scale(-1), axpy(1, b): one rounding, b - Ax)
   if ((rc = op_apply_impl(s->op, x, r, b, nullptr))) return rc;
   rc = launch_chunks<1>(
-      ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)r[i], a[0]); },
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{r[i]}; },
+      [=] __device__(int64_t, const V1<T>& q, double* a) { a[0] = fma((double)q.a, (double)q.a, a[0]); },
       [=] __device__(const double* t) {
         S->applies = 1;
         S->r_nrm_0 = sqrt(t[0]);
@@ -116,33 +205,37 @@ int cg_run(lfx_solver* s, T* x, const T* b) {
   if (rc) return rc;
   if ((rc = prec_apply_impl(s->prec, s->precision, r, z, n, done))) return rc;
   rc = launch_chunks<1>(
-      ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)z[i], a[0]); },
+      ctx, n, [=] __device__(int64_t i) { return V2<T>{r[i], z[i]}; },
+      [=] __device__(int64_t i, const V2<T>& q, double* a) {
+        p[i] = q.b;
+        a[0] = fma((double)q.a, (double)q.b, a[0]);
+      },
       [=] __device__(const double* t) { S->rz = t[0]; }, done);
-  if (rc) return rc;
-  rc = launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { p[i] = z[i]; }, NoFin{}, done);
   if (rc) return rc;
   const bool diag_prec = s->prec->kind == PREC_DIAG;
   const T* dg = (const T*)s->prec->rdiag;
-  for (;;) {
+  auto batch = [&]() -> int {
+    int q;
     for (int it = 0; it < 8; ++it) {
-      if ((rc = op_apply_impl(s->op, p, z, nullptr, done))) return rc;  // z = A p
-      rc = launch_chunks<1>(
-          ctx, n,
-          [=] __device__(int64_t i, double* a) { a[0] = fma((double)p[i], (double)z[i], a[0]); },
+      if ((q = op_apply_impl(s->op, p, z, nullptr, done))) return q;  // z = A p
+      q = launch_chunks<1>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{p[i], z[i]}; },
+          [=] __device__(int64_t, const V2<T>& v, double* a) {
+            a[0] = fma((double)v.a, (double)v.b, a[0]);
+          },
           [=] __device__(const double* t) {
             S->applies += 1;
             S->alpha = S->rz / t[0];
             S->neg_alpha = -S->alpha;
           },
           done);
-      if (rc) return rc;
+      if (q) return q;
       // x += alpha p ; r -= alpha z ; ||r||
-      rc = launch_chunks<1>(
-          ctx, n,
-          [=] __device__(int64_t i, double* a) {
-            const T al = (T)S->alpha, nal = (T)S->neg_alpha;
-            x[i] = fmaT(al, p[i], x[i]);
-            const T ri = fmaT(nal, z[i], r[i]);
+      q = launch_chunks<1>(
+          ctx, n, [=] __device__(int64_t i) { return V4<T>{x[i], p[i], r[i], z[i]}; },
+          [=] __device__(int64_t i, const V4<T>& v, double* a) {
+            x[i] = fmaT((T)S->alpha, v.b, v.a);
+            const T ri = fmaT((T)S->neg_alpha, v.d, v.c);
             r[i] = ri;
             a[0] = fma((double)ri, (double)ri, a[0]);
           },
@@ -161,37 +254,42 @@ int cg_run(lfx_solver* s, T* x, const T* b) {
             if (S->iter >= S->max_iter) S->done = 1;
           },
           done);
-      if (rc) return rc;
-      // z = P r ; rz_new = <r, z> ; beta
+      if (q) return q;
+      // z = P r ; rz_new = <r, z> ; beta ; p = beta p + z
       auto fin_beta = [=] __device__(const double* t) {
         S->beta = t[0] / S->rz;
         S->rz = t[0];
       };
       if (diag_prec) {
-        rc = launch_chunks<1>(
-            ctx, n,
-            [=] __device__(int64_t i, double* a) {
-              const T zi = r[i] / dg[i];
+        q = launch_chunks<1>(
+            ctx, n, [=] __device__(int64_t i) { return V2<T>{r[i], dg[i]}; },
+            [=] __device__(int64_t i, const V2<T>& v, double* a) {
+              const T zi = v.a / v.b;
               z[i] = zi;
-              a[0] = fma((double)r[i], (double)zi, a[0]);
+              a[0] = fma((double)v.a, (double)zi, a[0]);
             },
             fin_beta, done);
       } else {
-        if ((rc = prec_apply_impl(s->prec, s->precision, r, z, n, done))) return rc;
-        rc = launch_chunks<1>(
-            ctx, n,
-            [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)z[i], a[0]); },
+        if ((q = prec_apply_impl(s->prec, s->precision, r, z, n, done))) return q;
+        q = launch_chunks<1>(
+            ctx, n, [=] __device__(int64_t i) { return V2<T>{r[i], z[i]}; },
+            [=] __device__(int64_t, const V2<T>& v, double* a) {
+              a[0] = fma((double)v.a, (double)v.b, a[0]);
+            },
             fin_beta, done);
       }
-      if (rc) return rc;
-      rc = launch_chunks<0>(
-          ctx, n, [=] __device__(int64_t i, double*) { p[i] = fmaT((T)S->beta, p[i], z[i]); },
+      if (q) return q;
+      q = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{p[i], z[i]}; },
+          [=] __device__(int64_t i, const V2<T>& v, double*) { p[i] = fmaT((T)S->beta, v.a, v.b); },
           NoFin{}, done);
-      if (rc) return rc;
+      if (q) return q;
     }
-    if ((rc = read_state(s))) return rc;
-    if (s->h_state->done) break;
-  }
+    return LFX_OK;
+  };
+  if ((rc = read_state(s))) return rc;
+  while (!s->h_state->done)
+    if ((rc = run_graph(s, x, b, batch))) return rc;
   return LFX_OK;
 }
 
@@ -205,15 +303,15 @@ int bicgstab_run(lfx_solver* s, T* x, const T* b) {
   T *t = (T*)s->work[4], *sv = (T*)s->work[5], *y = (T*)s->work[6], *z = (T*)s->work[7];
   const int* done = &S->done;
   int rc;
-  // v = A x ; r = b - v ; r0 = r ; sc_err = ||r||
+  // v = A x ; r = b - v ; r0 = r ; sc_err = ||r|| ; v = p = 0
   if ((rc = op_apply_impl(s->op, x, r, b, nullptr))) return rc;
   rc = launch_chunks<1>(
-      ctx, n,
-      [=] __device__(int64_t i, double* a) {
-        r0[i] = r[i];
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{r[i]}; },
+      [=] __device__(int64_t i, const V1<T>& q, double* a) {
+        r0[i] = q.a;
         v[i] = T(0);
         p[i] = T(0);
-        a[0] = fma((double)r[i], (double)r[i], a[0]);
+        a[0] = fma((double)q.a, (double)q.a, a[0]);
       },
       [=] __device__(const double* tt) {
         S->applies = 1;
@@ -231,50 +329,60 @@ int bicgstab_run(lfx_solver* s, T* x, const T* b) {
         S->rho_old = 1.0;
       });
   if (rc) return rc;
-  for (;;) {
+  auto batch = [&]() -> int {
+    int q;
     for (int it = 0; it < 8; ++it) {
       // rho = <r, r0> ; beta = (rho/rho_old)(alpha/omega)
-      rc = launch_chunks<1>(
-          ctx, n,
-          [=] __device__(int64_t i, double* a) { a[0] = fma((double)r[i], (double)r0[i], a[0]); },
+      q = launch_chunks<1>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{r[i], r0[i]}; },
+          [=] __device__(int64_t, const V2<T>& w, double* a) {
+            a[0] = fma((double)w.a, (double)w.b, a[0]);
+          },
           [=] __device__(const double* tt) {
             S->rho = tt[0];
             S->beta = (S->rho / S->rho_old) * (S->alpha / S->omega);
             S->coef = -(S->beta * S->omega);
           },
           done);
-      if (rc) return rc;
+      if (q) return q;
       // t = r - beta*omega v
-      rc = launch_chunks<0>(
-          ctx, n, [=] __device__(int64_t i, double*) { t[i] = fmaT((T)S->coef, v[i], r[i]); },
+      q = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{v[i], r[i]}; },
+          [=] __device__(int64_t i, const V2<T>& w, double*) { t[i] = fmaT((T)S->coef, w.a, w.b); },
           NoFin{}, done);
-      if (rc) return rc;
-      if ((rc = prec_apply_impl(s->prec, s->precision, t, y, n, done))) return rc;
-      rc = launch_chunks<0>(
-          ctx, n, [=] __device__(int64_t i, double*) { p[i] = fmaT((T)S->beta, p[i], y[i]); },
+      if (q) return q;
+      if ((q = prec_apply_impl(s->prec, s->precision, t, y, n, done))) return q;
+      q = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{p[i], y[i]}; },
+          [=] __device__(int64_t i, const V2<T>& w, double*) { p[i] = fmaT((T)S->beta, w.a, w.b); },
           NoFin{}, done);
-      if (rc) return rc;
-      if ((rc = op_apply_impl(s->op, p, v, nullptr, done))) return rc;
-      rc = launch_chunks<1>(
-          ctx, n,
-          [=] __device__(int64_t i, double* a) { a[0] = fma((double)r0[i], (double)v[i], a[0]); },
+      if (q) return q;
+      if ((q = op_apply_impl(s->op, p, v, nullptr, done))) return q;
+      q = launch_chunks<1>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{r0[i], v[i]}; },
+          [=] __device__(int64_t, const V2<T>& w, double* a) {
+            a[0] = fma((double)w.a, (double)w.b, a[0]);
+          },
           [=] __device__(const double* tt) {
             S->alpha = S->rho / tt[0];
             S->neg_alpha = -S->alpha;
           },
           done);
-      if (rc) return rc;
-      rc = launch_chunks<0>(
-          ctx, n, [=] __device__(int64_t i, double*) { sv[i] = fmaT((T)S->neg_alpha, v[i], r[i]); },
+      if (q) return q;
+      q = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{v[i], r[i]}; },
+          [=] __device__(int64_t i, const V2<T>& w, double*) {
+            sv[i] = fmaT((T)S->neg_alpha, w.a, w.b);
+          },
           NoFin{}, done);
-      if (rc) return rc;
-      if ((rc = prec_apply_impl(s->prec, s->precision, sv, z, n, done))) return rc;
-      if ((rc = op_apply_impl(s->op, z, t, nullptr, done))) return rc;
-      rc = launch_chunks<2>(
-          ctx, n,
-          [=] __device__(int64_t i, double* a) {
-            a[0] = fma((double)t[i], (double)t[i], a[0]);
-            a[1] = fma((double)t[i], (double)sv[i], a[1]);
+      if (q) return q;
+      if ((q = prec_apply_impl(s->prec, s->precision, sv, z, n, done))) return q;
+      if ((q = op_apply_impl(s->op, z, t, nullptr, done))) return q;
+      q = launch_chunks<2>(
+          ctx, n, [=] __device__(int64_t i) { return V2<T>{t[i], sv[i]}; },
+          [=] __device__(int64_t, const V2<T>& w, double* a) {
+            a[0] = fma((double)w.a, (double)w.a, a[0]);
+            a[1] = fma((double)w.a, (double)w.b, a[1]);
           },
           [=] __device__(const double* tt) {
             S->applies += 2;
@@ -283,14 +391,17 @@ int bicgstab_run(lfx_solver* s, T* x, const T* b) {
             S->omega = S->ts / S->tt;
           },
           done);
-      if (rc) return rc;
+      if (q) return q;
       // x += omega z ; x += alpha p ; r = s - omega t ; ||r||
-      rc = launch_chunks<1>(
+      q = launch_chunks<1>(
           ctx, n,
-          [=] __device__(int64_t i, double* a) {
+          [=] __device__(int64_t i) {
+            return V3<T>{x[i], z[i], p[i]};
+          },
+          [=] __device__(int64_t i, const V3<T>& w, double* a) {
             const T om = (T)S->omega;
-            T xi = fmaT(om, z[i], x[i]);
-            x[i] = fmaT((T)S->alpha, p[i], xi);
+            const T xi = fmaT(om, w.b, w.a);
+            x[i] = fmaT((T)S->alpha, w.c, xi);
             const T ri = fmaT(-om, t[i], sv[i]);
             r[i] = ri;
             a[0] = fma((double)ri, (double)ri, a[0]);
@@ -312,43 +423,51 @@ int bicgstab_run(lfx_solver* s, T* x, const T* b) {
             if (S->iter >= S->max_iter) S->done = 1;
           },
           done);
-      if (rc) return rc;
+      if (q) return q;
     }
-    if ((rc = read_state(s))) return rc;
-    if (s->h_state->done) break;
-  }
+    return LFX_OK;
+  };
+  if ((rc = read_state(s))) return rc;
+  while (!s->h_state->done)
+    if ((rc = run_graph(s, x, b, batch))) return rc;
   return LFX_OK;
 }
 
 // ------------------------------------------------------------------ GMRES
-// Givens rotations and back substitution (:930-953) by one thread.
+// Givens rotations and back substitution (:930-953) by one thread. In inner
+// mode the rotations were already applied column by column as the Arnoldi
+// process ran, and only the back substitution over the m vectors is left.
 __global__ void gmres_finish_cycle(DevState* S, double* gm, int K) {
   if (S->done) return;
   double* h = gm;                  // H(i,j) at (i-1) + (K+1)(j-1)
   double* g = gm + 2 * (K + 1) * K;
   double* u = g + (K + 1);
 #define H(i, j) h[((i) - 1) + (K + 1) * ((j) - 1)]
-  for (int iv = 1; iv <= K; ++iv) {
-    const double nrm = sqrt(fma(H(iv, iv), H(iv, iv), H(iv + 1, iv) * H(iv + 1, iv)));
-    const double si = H(iv + 1, iv) / nrm;
-    const double ci = H(iv, iv) / nrm;
-    const double p = fma(ci, g[iv - 1], si * g[iv]);
-    const double q = fma(-si, g[iv - 1], ci * g[iv]);
-    g[iv - 1] = p;
-    g[iv] = q;
-    for (int ivj = iv; ivj <= K; ++ivj) {
-      const double h1 = fma(ci, H(iv, ivj), si * H(iv + 1, ivj));
-      const double h2 = fma(-si, H(iv, ivj), ci * H(iv + 1, ivj));
-      H(iv, ivj) = h1;
-      H(iv + 1, ivj) = h2;
+  const int m = S->inner_mode ? S->m : K;
+  if (!S->inner_mode) {
+    for (int iv = 1; iv <= K; ++iv) {
+      const double nrm = sqrt(fma(H(iv, iv), H(iv, iv), H(iv + 1, iv) * H(iv + 1, iv)));
+      const double si = H(iv + 1, iv) / nrm;
+      const double ci = H(iv, iv) / nrm;
+      const double p = fma(ci, g[iv - 1], si * g[iv]);
+      const double q = fma(-si, g[iv - 1], ci * g[iv]);
+      g[iv - 1] = p;
+      g[iv] = q;
+      for (int ivj = iv; ivj <= K; ++ivj) {
+        const double h1 = fma(ci, H(iv, ivj), si * H(iv + 1, ivj));
+        const double h2 = fma(-si, H(iv, ivj), ci * H(iv + 1, ivj));
+        H(iv, ivj) = h1;
+        H(iv + 1, ivj) = h2;
+      }
     }
   }
-  u[K - 1] = g[K - 1] / H(K, K);
-  for (int iv = K - 1; iv >= 1; --iv) {
+  u[m - 1] = g[m - 1] / H(m, m);
+  for (int iv = m - 1; iv >= 1; --iv) {
     double a = g[iv - 1];
-    for (int ivj = iv + 1; ivj <= K; ++ivj) a = fma(-H(iv, ivj), u[ivj - 1], a);
+    for (int ivj = iv + 1; ivj <= m; ++ivj) a = fma(-H(iv, ivj), u[ivj - 1], a);
     u[iv - 1] = a / H(iv, iv);
   }
+  S->m = m;
 #undef H
 }
 
@@ -367,19 +486,23 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
   double* nh = h + (K + 1) * K;
   double* g = nh + (K + 1) * K;
   double* u = g + (K + 1);
+  double* cs = u + K;
+  double* sn = cs + K;
   const int* done = &S->done;
+  const int* askip = &S->askip;
   int rc;
   // res = b - A x ; sc_err = ||res||
   if ((rc = op_apply_impl(s->op, x, res, b, nullptr))) return rc;
   rc = launch_chunks<1>(
-      ctx, n,
-      [=] __device__(int64_t i, double* a) { a[0] = fma((double)res[i], (double)res[i], a[0]); },
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{res[i]}; },
+      [=] __device__(int64_t, const V1<T>& q, double* a) { a[0] = fma((double)q.a, (double)q.a, a[0]); },
       [=] __device__(const double* t) {
         S->applies = 1;
         S->r_nrm_0 = sqrt(t[0]);
         S->sc_err = S->r_nrm_0;
         if (S->sc_err < EPS_RDEF) {  // :866
           S->done = 1;
+          S->askip = 1;
           S->converged = 1;
           S->r_nrm = S->sc_err;
         } else if (S->monitor) {
@@ -389,43 +512,50 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
   if (rc) return rc;
   VecPtrs vp{};
   for (int k = 0; k < K; ++k) vp.p[k] = V[k];
-  for (;;) {
+  auto cycle = [&]() -> int {
+    int q;
     // s = P res ; beta = ||s|| ; v1 = s / beta ; g = (beta, 0, ...)
-    if ((rc = prec_apply_impl(s->prec, s->precision, res, sv, n, done))) return rc;
-    rc = launch_chunks<1>(
-        ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma((double)sv[i], (double)sv[i], a[0]); },
+    if ((q = prec_apply_impl(s->prec, s->precision, res, sv, n, done))) return q;
+    q = launch_chunks<1>(
+        ctx, n, [=] __device__(int64_t i) { return V1<T>{sv[i]}; },
+        [=] __device__(int64_t, const V1<T>& v, double* a) { a[0] = fma((double)v.a, (double)v.a, a[0]); },
         [=] __device__(const double* t) {
           S->gbeta = sqrt(t[0]);
+          if (S->iter == 0) S->gbeta0 = S->gbeta;
           S->inv_beta = 1.0 / S->gbeta;
+          S->m = K;
           for (int k = 0; k <= K; ++k) g[k] = 0.0;
           g[0] = S->gbeta;
         },
         done);
-    if (rc) return rc;
+    if (q) return q;
     {
       T* v0 = V[0];
-      rc = launch_chunks<0>(
-          ctx, n, [=] __device__(int64_t i, double*) { v0[i] = (T)S->inv_beta * sv[i]; }, NoFin{},
-          done);
-      if (rc) return rc;
+      q = launch_chunks<0>(
+          ctx, n, [=] __device__(int64_t i) { return V1<T>{sv[i]}; },
+          [=] __device__(int64_t i, const V1<T>& v, double*) { v0[i] = (T)S->inv_beta * v.a; },
+          NoFin{}, done);
+      if (q) return q;
     }
     for (int iv = 1; iv <= K; ++iv) {
-      if ((rc = op_apply_impl(s->op, V[iv - 1], sv, nullptr, done))) return rc;  // s = A v
-      if ((rc = prec_apply_impl(s->prec, s->precision, sv, w, n, done))) return rc;   // w = P s
+      if ((q = op_apply_impl(s->op, V[iv - 1], sv, nullptr, askip))) return q;  // s = A v
+      if ((q = prec_apply_impl(s->prec, s->precision, sv, w, n, askip))) return q;  // w = P s
       // modified Gram-Schmidt: h(j,iv) = <v_j, w> ; w -= h(j,iv) v_j
       {
         const T* vj = V[0];
         double* hj = &h[0 + (K + 1) * (iv - 1)];
         double* nhj = &nh[0 + (K + 1) * (iv - 1)];
-        rc = launch_chunks<1>(
-            ctx, n,
-            [=] __device__(int64_t i, double* a) { a[0] = fma((double)vj[i], (double)w[i], a[0]); },
+        q = launch_chunks<1>(
+            ctx, n, [=] __device__(int64_t i) { return V2<T>{vj[i], w[i]}; },
+            [=] __device__(int64_t, const V2<T>& v, double* a) {
+              a[0] = fma((double)v.a, (double)v.b, a[0]);
+            },
             [=] __device__(const double* t) {
               *hj = t[0];
               *nhj = -t[0];
             },
-            done);
-        if (rc) return rc;
+            askip);
+        if (q) return q;
       }
       for (int j = 2; j <= iv; ++j) {
         const T* vprev = V[j - 2];
@@ -433,64 +563,93 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
         const double* nhp = &nh[(j - 2) + (K + 1) * (iv - 1)];
         double* hj = &h[(j - 1) + (K + 1) * (iv - 1)];
         double* nhj = &nh[(j - 1) + (K + 1) * (iv - 1)];
-        rc = launch_chunks<1>(
-            ctx, n,
-            [=] __device__(int64_t i, double* a) {
-              const T wi = fmaT((T)*nhp, vprev[i], w[i]);
+        q = launch_chunks<1>(
+            ctx, n, [=] __device__(int64_t i) { return V3<T>{vprev[i], w[i], vj[i]}; },
+            [=] __device__(int64_t i, const V3<T>& v, double* a) {
+              const T wi = fmaT((T)*nhp, v.a, v.b);
               w[i] = wi;
-              a[0] = fma((double)vj[i], (double)wi, a[0]);
+              a[0] = fma((double)v.c, (double)wi, a[0]);
             },
             [=] __device__(const double* t) {
               *hj = t[0];
               *nhj = -t[0];
             },
-            done);
-        if (rc) return rc;
+            askip);
+        if (q) return q;
       }
       {
         const T* vl = V[iv - 1];
         const double* nhp = &nh[(iv - 1) + (K + 1) * (iv - 1)];
-        double* hn = &h[iv + (K + 1) * (iv - 1)];
-        rc = launch_chunks<1>(
-            ctx, n,
-            [=] __device__(int64_t i, double* a) {
-              const T wi = fmaT((T)*nhp, vl[i], w[i]);
+        double* col = &h[(K + 1) * (iv - 1)];  // H(:, iv)
+        const int ivc = iv;
+        q = launch_chunks<1>(
+            ctx, n, [=] __device__(int64_t i) { return V2<T>{vl[i], w[i]}; },
+            [=] __device__(int64_t i, const V2<T>& v, double* a) {
+              const T wi = fmaT((T)*nhp, v.a, v.b);
               w[i] = wi;
               a[0] = fma((double)wi, (double)wi, a[0]);
             },
             [=] __device__(const double* t) {
-              *hn = sqrt(t[0]);
-              S->inv_hn = 1.0 / *hn;
+              const double hn = sqrt(t[0]);
+              col[ivc] = hn;  // H(iv+1, iv)
+              S->inv_hn = 1.0 / hn;
               S->applies += 1;
+              if (S->inner_mode) {
+                // apply the previous rotations to column iv, form rotation iv,
+                // and test the residual estimate |g(iv+1)|
+                for (int j = 1; j < ivc; ++j) {
+                  const double h1 = fma(cs[j - 1], col[j - 1], sn[j - 1] * col[j]);
+                  const double h2 = fma(-sn[j - 1], col[j - 1], cs[j - 1] * col[j]);
+                  col[j - 1] = h1;
+                  col[j] = h2;
+                }
+                const double a0 = col[ivc - 1], a1 = col[ivc];
+                const double nrm = sqrt(fma(a0, a0, a1 * a1));
+                const double ci = a0 / nrm, si = a1 / nrm;
+                cs[ivc - 1] = ci;
+                sn[ivc - 1] = si;
+                col[ivc - 1] = fma(ci, a0, si * a1);
+                col[ivc] = 0.0;
+                const double gp = g[ivc - 1], gq = g[ivc];
+                g[ivc - 1] = fma(ci, gp, si * gq);
+                g[ivc] = fma(-si, gp, ci * gq);
+                if (fabs(g[ivc]) <= S->r_tol * S->gbeta0 || ivc == K) {
+                  S->m = ivc;
+                  S->askip = 1;
+                }
+              }
             },
-            done);
-        if (rc) return rc;
+            askip);
+        if (q) return q;
       }
       if (iv < K) {
         T* vn = V[iv];
-        rc = launch_chunks<0>(
-            ctx, n, [=] __device__(int64_t i, double*) { vn[i] = (T)S->inv_hn * w[i]; }, NoFin{},
-            done);
-        if (rc) return rc;
+        q = launch_chunks<0>(
+            ctx, n, [=] __device__(int64_t i) { return V1<T>{w[i]}; },
+            [=] __device__(int64_t i, const V1<T>& v, double*) { vn[i] = (T)S->inv_hn * v.a; },
+            NoFin{}, askip);
+        if (q) return q;
       }
     }
     gmres_finish_cycle<<<1, 1, 0, ctx->stream>>>(S, h, K);
     ctx->launches++;
     LFX_CK(ctx, cudaGetLastError());
-    // x += sum_iv u(iv) v_iv, one pass, the reference's order per element
-    rc = launch_chunks<0>(
-        ctx, n,
-        [=] __device__(int64_t i, double*) {
-          T xi = x[i];
-          for (int k = 0; k < K; ++k) xi = fmaT((T)u[k], ((const T*)vp.p[k])[i], xi);
+    // x += sum_iv u(iv) v_iv over the m vectors of the cycle, one pass, the
+    // reference's order per element
+    q = launch_chunks<0>(
+        ctx, n, [=] __device__(int64_t i) { return V1<T>{x[i]}; },
+        [=] __device__(int64_t i, const V1<T>& v, double*) {
+          T xi = v.a;
+          const int m = S->m;
+          for (int k = 0; k < m; ++k) xi = fmaT((T)u[k], ((const T*)vp.p[k])[i], xi);
           x[i] = xi;
         },
         NoFin{}, done);
-    if (rc) return rc;
-    if ((rc = op_apply_impl(s->op, x, res, b, done))) return rc;  // res = b - A x
-    rc = launch_chunks<1>(
-        ctx, n,
-        [=] __device__(int64_t i, double* a) { a[0] = fma((double)res[i], (double)res[i], a[0]); },
+    if (q) return q;
+    if ((q = op_apply_impl(s->op, x, res, b, done))) return q;  // res = b - A x
+    q = launch_chunks<1>(
+        ctx, n, [=] __device__(int64_t i) { return V1<T>{res[i]}; },
+        [=] __device__(int64_t, const V1<T>& v, double* a) { a[0] = fma((double)v.a, (double)v.a, a[0]); },
         [=] __device__(const double* t) {
           S->applies += 1;
           S->iter += 1;
@@ -507,12 +666,14 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
             }
           }
           if (S->iter >= S->max_iter) S->done = 1;
+          S->askip = S->done;
         },
         done);
-    if (rc) return rc;
-    if ((rc = read_state(s))) return rc;
-    if (s->h_state->done) break;
-  }
+    return q;
+  };
+  if ((rc = read_state(s))) return rc;
+  while (!s->h_state->done)
+    if ((rc = run_graph(s, x, b, cycle))) return rc;
   return LFX_OK;
 }
 
@@ -531,10 +692,11 @@ void fill_info(lfx_solver* s, lfx_solve_info* info) {
 int free_solver(lfx_solver* s) {
   if (!s) return LFX_OK;
   lfx_ctx* ctx = s->ctx;
+  free_graphs(s);
   for (void* p : s->work) dfree(ctx, p, s->n * esz(s->precision));
   dfree(ctx, s->d_state, sizeof(DevState));
   if (s->h_state) cudaFreeHost(s->h_state);
-  if (s->d_gm) dfree(ctx, s->d_gm, sizeof(double) * (4 * (size_t)(s->cfg.gcrk + 1) * s->cfg.gcrk + 8));
+  if (s->d_gm) dfree(ctx, s->d_gm, sizeof(double) * gm_doubles(s->cfg.gcrk));
   if (s->r32) lfx_vec_destroy(s->r32);
   if (s->d32) lfx_vec_destroy(s->d32);
   if (s->d_r64) dfree(ctx, s->d_r64, s->n * 8);
@@ -571,9 +733,7 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
   auto resid_norm = [&](double* out) -> int {
     int q = op_apply_impl(s->op, x, r, b, nullptr);
     if (q) return q;
-    q = launch_chunks<1>(
-        ctx, n, [=] __device__(int64_t i, double* a) { a[0] = fma(r[i], r[i], a[0]); },
-        [=] __device__(const double* t) { sc[0] = sqrt(t[0]); });
+    q = norm_kernel(ctx, n, (const double*)r, sc, nullptr);
     if (q) return q;
     LFX_CK(ctx, cudaMemcpyAsync(ctx->h_scalars, sc, 8, cudaMemcpyDeviceToHost, ctx->stream));
     LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -595,9 +755,9 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
     // r32 = r / ||r|| ; d32 = 0
     const double inv = 1.0 / rn;
     rc = launch_chunks<0>(
-        ctx, n,
-        [=] __device__(int64_t i, double*) {
-          r32[i] = (float)(r[i] * inv);
+        ctx, n, [=] __device__(int64_t i) { return V1<double>{r[i]}; },
+        [=] __device__(int64_t i, const V1<double>& v, double*) {
+          r32[i] = (float)(v.a * inv);
           d32[i] = 0.0f;
         },
         NoFin{});
@@ -610,7 +770,8 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
     // x += ||r|| d
     const double scale = rn;
     rc = launch_chunks<0>(
-        ctx, n, [=] __device__(int64_t i, double*) { x[i] = fma(scale, (double)d32[i], x[i]); },
+        ctx, n, [=] __device__(int64_t i) { return V2<double>{x[i], (double)d32[i]}; },
+        [=] __device__(int64_t i, const V2<double>& v, double*) { x[i] = fma(scale, v.b, v.a); },
         NoFin{});
     if (rc) return rc;
     if ((rc = resid_norm(&rn))) return rc;
@@ -664,8 +825,7 @@ int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
   int nwork = kind == LFX_SOLVER_CG ? 3 : kind == LFX_SOLVER_BICGSTAB ? 8 : 3 + cfg->gcrk;
   int rc = alloc_common(s, nwork);
   if (!rc && kind == LFX_SOLVER_GMRES)
-    rc = dmalloc(ctx, (void**)&s->d_gm,
-                 sizeof(double) * (4 * (size_t)(cfg->gcrk + 1) * cfg->gcrk + 8));
+    rc = dmalloc(ctx, (void**)&s->d_gm, sizeof(double) * gm_doubles(cfg->gcrk));
   if (rc) {
     free_solver(s);
     return rc;
@@ -702,7 +862,12 @@ int lfx_refined_solver_create(lfx_ctx* ctx, lfx_op* op64, lfx_solver* inner, dou
     free_solver(s);
     return rc;
   }
+  // the inner GMRES runs in "inner mode": rotations applied as the Arnoldi
+  // process goes, and the cycle ends as soon as the residual estimate meets
+  // the inner tolerance (the outer FP64 residual decides convergence)
   inner->cfg.r_tol = inner_rtol;
+  inner->inner_mode = inner->kind == LFX_SOLVER_GMRES;
+  free_graphs(inner);
   *out = s;
   return LFX_OK;
 }
@@ -719,6 +884,7 @@ int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info
     return fail(ctx, LFX_NOT_SUPPORTED, "device solves take single-field vectors");
   if (x->undf[0] != s->n || b->undf[0] != s->n)
     return fail(ctx, LFX_TYPE_MISMATCH, "vector length does not match the operator");
+  if (x->data[0] == b->data[0]) return fail(ctx, LFX_INVALID_ARGUMENT, "x and b must differ");
   int rc;
   if (s->kind == 100) {
     rc = refined_run(s, x, b, info);
@@ -739,6 +905,7 @@ int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info
     if (!rc) fill_info(s, info);
   }
   if (ctx->time_applies) drain_timing(ctx);
+  if (!rc) rc = lfx_ctx_check_device_error(ctx);
   if (rc) {
     info->status = rc;
     return rc;

@@ -17,37 +17,55 @@ namespace lfx {
 
 template <class T>
 static int k_set(lfx_ctx* ctx, T* x, T c, int64_t n) {
-  return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { x[i] = c; }, NoFin{});
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t) { return V1<T>{c}; },
+      [=] __device__(int64_t i, const V1<T>& v, double*) { x[i] = v.a; }, NoFin{});
 }
 template <class T>
 static int k_copy(lfx_ctx* ctx, T* y, const T* x, int64_t n) {
-  return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { y[i] = x[i]; }, NoFin{});
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{x[i]}; },
+      [=] __device__(int64_t i, const V1<T>& v, double*) { y[i] = v.a; }, NoFin{});
 }
 template <class T>
 static int k_axpy(lfx_ctx* ctx, T* y, T a, const T* x, int64_t n) {
-  return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { y[i] = fmaT(a, x[i], y[i]); },
-                          NoFin{});
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V2<T>{x[i], y[i]}; },
+      [=] __device__(int64_t i, const V2<T>& v, double*) { y[i] = fmaT(a, v.a, v.b); }, NoFin{});
 }
 template <class T>
 static int k_aypx(lfx_ctx* ctx, T* y, T a, const T* x, int64_t n) {
-  return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { y[i] = fmaT(a, y[i], x[i]); },
-                          NoFin{});
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V2<T>{x[i], y[i]}; },
+      [=] __device__(int64_t i, const V2<T>& v, double*) { y[i] = fmaT(a, v.b, v.a); }, NoFin{});
 }
 template <class T>
 static int k_axpby(lfx_ctx* ctx, T* z, T a, const T* x, T b, const T* y, int64_t n) {
   return launch_chunks<0>(
-      ctx, n, [=] __device__(int64_t i, double*) { z[i] = fmaT(a, x[i], b * y[i]); }, NoFin{});
+      ctx, n, [=] __device__(int64_t i) { return V2<T>{x[i], y[i]}; },
+      [=] __device__(int64_t i, const V2<T>& v, double*) { z[i] = fmaT(a, v.a, b * v.b); },
+      NoFin{});
 }
 template <class T>
 static int k_scale(lfx_ctx* ctx, T* x, T a, int64_t n) {
-  return launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { x[i] = a * x[i]; }, NoFin{});
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{x[i]}; },
+      [=] __device__(int64_t i, const V1<T>& v, double*) { x[i] = a * v.a; }, NoFin{});
 }
 template <class T>
 static int k_dot(lfx_ctx* ctx, const T* x, const T* y, int64_t n, double* out) {
   return launch_chunks<1>(
-      ctx, n,
-      [=] __device__(int64_t i, double* acc) { acc[0] = fma((double)x[i], (double)y[i], acc[0]); },
+      ctx, n, [=] __device__(int64_t i) { return V2<T>{x[i], y[i]}; },
+      [=] __device__(int64_t, const V2<T>& v, double* acc) {
+        acc[0] = fma((double)v.a, (double)v.b, acc[0]);
+      },
       [=] __device__(const double* tot) { *out = tot[0]; });
+}
+template <class S, class D>
+static int k_convert(lfx_ctx* ctx, D* d, const S* s, int64_t n) {
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V1<S>{s[i]}; },
+      [=] __device__(int64_t i, const V1<S>& v, double*) { d[i] = (D)v.a; }, NoFin{});
 }
 
 }  // namespace lfx
@@ -268,8 +286,7 @@ int lfx_vec_import_field(lfx_vec* v, int32_t position, const double* host, int64
   int rc = dmalloc(ctx, (void**)&tmp, n * 8);
   if (rc) return rc;
   LFX_CK(ctx, cudaMemcpyAsync(tmp, host, n * 8, cudaMemcpyHostToDevice, ctx->stream));
-  float* d = (float*)v->data[f];
-  rc = launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { d[i] = (float)tmp[i]; }, NoFin{});
+  rc = k_convert(ctx, (float*)v->data[f], (const double*)tmp, n);
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
   dfree(ctx, tmp, n * 8);
   return rc;
@@ -290,8 +307,7 @@ int lfx_vec_export_field(const lfx_vec* v, int32_t position, double* host, int64
   double* tmp = nullptr;
   int rc = dmalloc(ctx, (void**)&tmp, n * 8);
   if (rc) return rc;
-  const float* d = (const float*)v->data[f];
-  rc = launch_chunks<0>(ctx, n, [=] __device__(int64_t i, double*) { tmp[i] = (double)d[i]; }, NoFin{});
+  rc = k_convert(ctx, tmp, (const float*)v->data[f], n);
   LFX_CK(ctx, cudaMemcpyAsync(host, tmp, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
   dfree(ctx, tmp, n * 8);

@@ -71,6 +71,8 @@ _SIGS = [
     ("lfx_ctx_apply_timing", [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double),
                               C.c_int32], C.c_int),
     ("lfx_ctx_launch_count", [vp], C.c_int64),
+    ("lfx_ctx_set_apply_kernel", [vp, C.c_int32], C.c_int),
+    ("lfx_ctx_check_device_error", [vp], C.c_int),
     ("lfx_vec_create", [vp, C.c_int32, i64p, C.c_int32, C.POINTER(vp)], C.c_int),
     ("lfx_vec_duplicate", [vp, C.POINTER(vp)], C.c_int),
     ("lfx_vec_destroy", [vp], C.c_int),
@@ -92,6 +94,10 @@ _SIGS = [
                         C.POINTER(vp)], C.c_int),
     ("lfx_lma_create_like", [vp, f64p, C.c_int32, C.POINTER(vp)], C.c_int),
     ("lfx_op_apply", [vp, vp, vp], C.c_int),
+    ("lfx_op_autotune", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                         C.POINTER(C.c_int32), C.POINTER(C.c_float)], C.c_int),
+    ("lfx_op_time_apply", [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                           C.POINTER(C.c_float)], C.c_int),
     ("lfx_op_apply_transpose", [vp, vp, vp], C.c_int),
     ("lfx_op_destroy", [vp], C.c_int),
     ("lfx_lma_diagonal", [vp, vp], C.c_int),
@@ -182,6 +188,13 @@ class Context:
     def launch_count(self) -> int:
         return self.L.lfx_ctx_launch_count(self.h)
 
+    def set_apply_kernel(self, which: int):
+        """0: bulk-copy pipelined LMA apply (default), 1: register gather."""
+        self.check(self.L.lfx_ctx_set_apply_kernel(self.h, which))
+
+    def check_device_error(self):
+        self.check(self.L.lfx_ctx_check_device_error(self.h))
+
     def close(self):
         if getattr(self, "h", None):
             self.L.lfx_ctx_destroy(self.h)
@@ -270,8 +283,11 @@ class FieldVector(_Handle):
         a = np.ascontiguousarray(data, dtype=np.float64)
         self.ctx.check(self.ctx.L.lfx_vec_import_field(self.h, position, a, len(a)))
 
-    def export_field(self, position=1):
-        out = np.empty(self.undf[position - 1], dtype=np.float64)
+    def export_field(self, position=1, out=None):
+        """Field `position` as FP64 host data; `out` (e.g. pinned memory) is
+        filled in place when given."""
+        if out is None:
+            out = np.empty(self.undf[position - 1], dtype=np.float64)
         self.ctx.check(self.ctx.L.lfx_vec_export_field(self.h, position, out, len(out)))
         return out
 
@@ -318,6 +334,23 @@ class LmaOperator(_Handle):
 
     def apply(self, x, y):
         self.ctx.check(self.ctx.L.lfx_op_apply(self.h, x.h, y.h))
+
+    def autotune(self, reps: int = 10) -> dict:
+        """Time the apply launch configurations on this operator and keep the
+        fastest; returns the choice."""
+        k, s, w, us = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
+        self.ctx.check(self.ctx.L.lfx_op_autotune(self.h, reps, C.byref(k), C.byref(s),
+                                                   C.byref(w), C.byref(us)))
+        name = {0: "pipeline", 1: "register-gather", 2: "generic"}[k.value]
+        return {"kernel": name, "stages": s.value, "warps": w.value, "us": round(us.value, 2)}
+
+    def time_apply(self, kernel: int, stages: int = 0, warps: int = 0, reps: int = 10):
+        us = C.c_float()
+        rc = self.ctx.L.lfx_op_time_apply(self.h, kernel, stages, warps, reps, C.byref(us))
+        if rc == 8:  # configuration does not fit
+            return None
+        self.ctx.check(rc)
+        return us.value
 
     def apply_transpose(self, x, y):
         self.ctx.check(self.ctx.L.lfx_op_apply_transpose(self.h, x.h, y.h))

@@ -121,6 +121,50 @@ def test_lma_apply_w2_bitwise(ctx, n, nl):
     assert same(sysd.diag.export_field(), op.diagonal())
 
 
+@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("space,n,nl,prec", [("w0", 6, 5, 64), ("w2", 8, 7, 64), ("w2", 8, 7, 32),
+                                             ("w2", 12, 30, 64), ("w0", 5, 21, 32)])
+def test_apply_kernels_agree(ctx, kernel, space, n, nl, prec):
+    """Both LMA apply kernels (bulk-copy pipelined and register gather) give
+    the oracle's FP64 result bit for bit, and the same FP32 result."""
+    p = mg.w0_problem(n, nl, seed=3) if space == "w0" else mg.w2_problem(n, nl, seed=3)
+    npc, cic = p.mesh.colour_lookup()
+    ctx.set_apply_kernel(kernel)
+    try:
+        op = lfx.LmaOperator(ctx, p.ncell_2d, nl, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf,
+                             p.lma, npc, cic, precision=prec)
+        x = mg.normal(17, p.undf)
+        X = lfx.FieldVector.from_array(ctx, x, prec)
+        Y = lfx.FieldVector(ctx, [p.undf], prec)
+        op.apply(X, Y)
+        got = Y.export_field()
+        ctx.check_device_error()
+    finally:
+        ctx.set_apply_kernel(-1)
+    if prec == 64:
+        assert same(got, o_lma(p).apply(x))
+    else:
+        ctx.set_apply_kernel(1 - kernel)
+        try:
+            op.apply(X, Y)
+            other = Y.export_field()
+        finally:
+            ctx.set_apply_kernel(-1)
+        assert same(got, other)
+
+
+def test_autotune_keeps_results(ctx):
+    p = mg.w2_problem(12, 10, seed=6)
+    npc, cic = p.mesh.colour_lookup()
+    op = lfx.LmaOperator(ctx, p.ncell_2d, 10, 6, 6, p.map, p.map, p.undf, p.undf, p.lma, npc, cic)
+    x = mg.normal(2, p.undf)
+    X, Y = lfx.FieldVector.from_array(ctx, x), lfx.FieldVector(ctx, [p.undf])
+    choice = op.autotune(reps=3)
+    assert choice["us"] > 0 and choice["kernel"] in ("pipeline", "register-gather")
+    op.apply(X, Y)
+    assert same(Y.export_field(), o_lma(p).apply(x))
+
+
 def test_divergence_and_transpose_bitwise(ctx):
     q = mg.w2_problem(6, 4, seed=3, keep_parts=True)
     npc, cic = q.mesh.colour_lookup()

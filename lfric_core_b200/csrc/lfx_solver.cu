@@ -12,6 +12,7 @@
 // host reads the flag once per replay. Vector updates that the reference
 // performs as separate builtins are fused when the fusion does not change a
 // single rounding (e.g. t = r; t += a v  ==>  t = fma(a, v, r)).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -168,6 +169,79 @@ void free_graphs(lfx_solver* s) {
   }
   s->graphs.clear();
 }
+
+template <class T, int N>
+struct Pack {
+  T v[N];
+};
+
+// Classical Gram-Schmidt, inner products: h(j) = <v_j, w>, j < NR, one pass.
+template <class T, int NR>
+int cgs_dots(lfx_ctx* ctx, int64_t n, const VecPtrs& vp, const T* w, double* hcol, double* nhcol,
+             const int* skip) {
+  return launch_chunks<NR>(
+      ctx, n,
+      [=] __device__(int64_t i) {
+        Pack<T, NR + 1> q;
+#pragma unroll
+        for (int j = 0; j < NR; ++j) q.v[j] = ((const T*)vp.p[j])[i];
+        q.v[NR] = w[i];
+        return q;
+      },
+      [=] __device__(int64_t, const Pack<T, NR + 1>& q, double* a) {
+#pragma unroll
+        for (int j = 0; j < NR; ++j) a[j] = fma((double)q.v[j], (double)q.v[NR], a[j]);
+      },
+      [=] __device__(const double* t) {
+        for (int j = 0; j < NR; ++j) {
+          hcol[j] = t[j];
+          nhcol[j] = -t[j];
+        }
+      },
+      skip);
+}
+
+// Classical Gram-Schmidt, update: w -= sum_j h(j) v_j (in order) and ||w||;
+// fin receives the norm.
+template <class T, int NR, class Fin>
+int cgs_update(lfx_ctx* ctx, int64_t n, const VecPtrs& vp, T* w, const double* nhcol, Fin fin,
+               const int* skip) {
+  return launch_chunks<1>(
+      ctx, n,
+      [=] __device__(int64_t i) {
+        Pack<T, NR + 1> q;
+#pragma unroll
+        for (int j = 0; j < NR; ++j) q.v[j] = ((const T*)vp.p[j])[i];
+        q.v[NR] = w[i];
+        return q;
+      },
+      [=] __device__(int64_t i, const Pack<T, NR + 1>& q, double* a) {
+        T wi = q.v[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) wi = fmaT((T)nhcol[j], q.v[j], wi);
+        w[i] = wi;
+        a[0] = fma((double)wi, (double)wi, a[0]);
+      },
+      fin, skip);
+}
+
+template <class T, class Fin>
+int cgs_step(lfx_ctx* ctx, int64_t n, int nr, const VecPtrs& vp, T* w, double* hcol,
+             double* nhcol, Fin fin, const int* skip) {
+  int rc = LFX_INVALID_ARGUMENT;
+  switch (nr) {
+#define CGS_CASE(N)                                                          \
+  case N:                                                                    \
+    rc = cgs_dots<T, N>(ctx, n, vp, w, hcol, nhcol, skip);                   \
+    if (!rc) rc = cgs_update<T, N>(ctx, n, vp, w, nhcol, fin, skip);         \
+    break;
+    CGS_CASE(1) CGS_CASE(2) CGS_CASE(3) CGS_CASE(4) CGS_CASE(5) CGS_CASE(6)
+    CGS_CASE(7) CGS_CASE(8) CGS_CASE(9) CGS_CASE(10) CGS_CASE(11) CGS_CASE(12)
+#undef CGS_CASE
+  }
+  return rc;
+}
+constexpr int kMaxCgs = 12;
 
 template <class T>
 int norm_kernel(lfx_ctx* ctx, int64_t n, const T* v, double* out, const int* skip) {
@@ -540,7 +614,46 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
     for (int iv = 1; iv <= K; ++iv) {
       if ((q = op_apply_impl(s->op, V[iv - 1], sv, nullptr, askip))) return q;  // s = A v
       if ((q = prec_apply_impl(s->prec, s->precision, sv, w, n, askip))) return q;  // w = P s
-      // modified Gram-Schmidt: h(j,iv) = <v_j, w> ; w -= h(j,iv) v_j
+      double* col = &h[(K + 1) * (iv - 1)];  // H(:, iv)
+      const int ivc = iv;
+      // last step of the orthogonalisation: H(iv+1, iv) = ||w||, and in inner
+      // mode the column's Givens rotation and the in-cycle convergence test
+      auto fin_norm = [=] __device__(const double* t) {
+        const double hn = sqrt(t[0]);
+        col[ivc] = hn;  // H(iv+1, iv)
+        S->inv_hn = 1.0 / hn;
+        S->applies += 1;
+        if (S->inner_mode) {
+          for (int j = 1; j < ivc; ++j) {
+            const double h1 = fma(cs[j - 1], col[j - 1], sn[j - 1] * col[j]);
+            const double h2 = fma(-sn[j - 1], col[j - 1], cs[j - 1] * col[j]);
+            col[j - 1] = h1;
+            col[j] = h2;
+          }
+          const double a0 = col[ivc - 1], a1 = col[ivc];
+          const double nrm = sqrt(fma(a0, a0, a1 * a1));
+          const double ci = a0 / nrm, si = a1 / nrm;
+          cs[ivc - 1] = ci;
+          sn[ivc - 1] = si;
+          col[ivc - 1] = fma(ci, a0, si * a1);
+          col[ivc] = 0.0;
+          const double gp = g[ivc - 1], gq = g[ivc];
+          g[ivc - 1] = fma(ci, gp, si * gq);
+          g[ivc] = fma(-si, gp, ci * gq);
+          if (fabs(g[ivc]) <= S->r_tol * S->gbeta0 || ivc == K) {
+            S->m = ivc;
+            S->askip = 1;
+          }
+        }
+      };
+      if (s->inner_mode && K <= kMaxCgs) {
+        // inner solve: classical Gram-Schmidt, two passes per step
+        VecPtrs vpi{};
+        for (int k = 0; k < iv; ++k) vpi.p[k] = V[k];
+        q = cgs_step<T>(ctx, n, iv, vpi, w, col, &nh[(K + 1) * (iv - 1)], fin_norm, askip);
+        if (q) return q;
+      } else {
+      // modified Gram-Schmidt (the reference's): h(j,iv) = <v_j, w> ; w -= h(j,iv) v_j
       {
         const T* vj = V[0];
         double* hj = &h[0 + (K + 1) * (iv - 1)];
@@ -580,8 +693,6 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
       {
         const T* vl = V[iv - 1];
         const double* nhp = &nh[(iv - 1) + (K + 1) * (iv - 1)];
-        double* col = &h[(K + 1) * (iv - 1)];  // H(:, iv)
-        const int ivc = iv;
         q = launch_chunks<1>(
             ctx, n, [=] __device__(int64_t i) { return V2<T>{vl[i], w[i]}; },
             [=] __device__(int64_t i, const V2<T>& v, double* a) {
@@ -589,38 +700,9 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
               w[i] = wi;
               a[0] = fma((double)wi, (double)wi, a[0]);
             },
-            [=] __device__(const double* t) {
-              const double hn = sqrt(t[0]);
-              col[ivc] = hn;  // H(iv+1, iv)
-              S->inv_hn = 1.0 / hn;
-              S->applies += 1;
-              if (S->inner_mode) {
-                // apply the previous rotations to column iv, form rotation iv,
-                // and test the residual estimate |g(iv+1)|
-                for (int j = 1; j < ivc; ++j) {
-                  const double h1 = fma(cs[j - 1], col[j - 1], sn[j - 1] * col[j]);
-                  const double h2 = fma(-sn[j - 1], col[j - 1], cs[j - 1] * col[j]);
-                  col[j - 1] = h1;
-                  col[j] = h2;
-                }
-                const double a0 = col[ivc - 1], a1 = col[ivc];
-                const double nrm = sqrt(fma(a0, a0, a1 * a1));
-                const double ci = a0 / nrm, si = a1 / nrm;
-                cs[ivc - 1] = ci;
-                sn[ivc - 1] = si;
-                col[ivc - 1] = fma(ci, a0, si * a1);
-                col[ivc] = 0.0;
-                const double gp = g[ivc - 1], gq = g[ivc];
-                g[ivc - 1] = fma(ci, gp, si * gq);
-                g[ivc] = fma(-si, gp, ci * gq);
-                if (fabs(g[ivc]) <= S->r_tol * S->gbeta0 || ivc == K) {
-                  S->m = ivc;
-                  S->askip = 1;
-                }
-              }
-            },
-            askip);
+            fin_norm, askip);
         if (q) return q;
+      }
       }
       if (iv < K) {
         T* vn = V[iv];
@@ -716,7 +798,8 @@ int alloc_common(lfx_solver* s, int nwork) {
     if (rc) return rc;
     s->work.push_back(p);
   }
-  return ensure_partials(ctx, s->n, 4);
+  // up to gcrk simultaneous sums (classical Gram-Schmidt of the inner solve)
+  return ensure_partials(ctx, s->n, std::max(4, s->cfg.gcrk + 1));
 }
 
 // ------------------------------------------------------------------ refinement

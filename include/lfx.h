@@ -230,6 +230,27 @@ int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which);
  * check (the kernel then skipped its work); synchronises the stream */
 int lfx_ctx_check_device_error(lfx_ctx* ctx);
 
+/* ------------------------------------------------------------------ no allocation
+ * Allocation-free inner product (no counterpart in the reference): for
+ * callers that cannot allocate device memory where they need a dot product --
+ * device memory owned by another runtime's pool, a CUDA graph capture open on
+ * their stream, or a loop that must not take cudaMalloc's implicit
+ * synchronisation. x, y (n FP64 values) and result (one FP64 value) are device
+ * pointers owned by the caller; the work is queued on `stream` (a
+ * cudaStream_t, NULL for the default stream) and *result is valid once it
+ * completes. The reduction scratch is a fixed array built into the library
+ * (about 64 KiB on every GPU that loads it, held until exit), so n is limited
+ * to lfx_dot_noalloc_max_n() (16 Mi) values; larger n is rejected with
+ * LFX_INVALID_ARGUMENT and a message from lfx_noalloc_last_error(). The first
+ * call on each device looks up the array's device address; make that first
+ * call before any stream capture. All calls share the array: calls that
+ * overlap on the GPU (different streams, or concurrent host threads) race and
+ * must be serialised by the caller. The result equals lfx_vec_dot's bit for
+ * bit. */
+int lfx_dot_noalloc(const double* x, const double* y, int64_t n, double* result, void* stream);
+int64_t lfx_dot_noalloc_max_n(void);
+const char* lfx_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

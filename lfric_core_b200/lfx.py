@@ -119,6 +119,9 @@ _SIGS = [
      C.c_int),
     ("lfx_solver_apply", [vp, vp, vp, C.POINTER(SolveInfo)], C.c_int),
     ("lfx_solver_destroy", [vp], C.c_int),
+    ("lfx_dot_noalloc", [vp, vp, C.c_int64, vp, vp], C.c_int),
+    ("lfx_dot_noalloc_max_n", [], C.c_int64),
+    ("lfx_noalloc_last_error", [], C.c_char_p),
 ]
 EXPORTED = [s[0] for s in _SIGS]
 

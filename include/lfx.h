@@ -98,7 +98,8 @@ int lfx_vec_field_device_ptr(const lfx_vec* v, int32_t position, void** out);
  *   map_to / map_from   Fortran (ndf, ncell_2d): dof id of layer 0 of each local dof
  *   local_stencil       Fortran (ncell_2d*nlayers, ndf_to, ndf_from)
  *   cells_in_colour     Fortran (ncolours, max_cells_per_colour), 1-based cell ids
- *   precision           device storage: LFX_R64, or LFX_R32 (rounded copy) */
+ *   precision           device storage: LFX_R64, or LFX_R32 (rounded copy)
+ * local_stencil may be host or device memory. */
 int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_to,
                    int32_t ndf_from, const int32_t* map_to, const int32_t* map_from,
                    int64_t undf_to, int64_t undf_from, const double* local_stencil,
@@ -127,6 +128,28 @@ int lfx_lma_diagonal(lfx_op* op, lfx_vec* diag);
 /* transpose apply y = A^T x for a matrix stored as (ncell_3d, ndf_to, ndf_from)
  * (transpose_matrix_vector_kernel_mod.F90); y is overwritten */
 int lfx_op_apply_transpose(lfx_op* op, const lfx_vec* x, lfx_vec* y);
+
+/* ------------------------------------------------------------------ FEM set-up
+ * Device assembly of the local matrices by 3x3x3 Gauss quadrature on the
+ * trilinear hexahedra of an extruded mesh (the role of the reference's
+ * compute_mass_matrix_kernel_w_scalar / _w2 and compute_div_operator_kernel,
+ * components/science/source/kernel/fem/), followed by lfx_lma_create. Either
+ * output may be NULL; both share one layout.
+ *   verts_on_cell  [ncell_2d][4] 1-based (SW, SE, NE, NW)
+ *   xyz3d          [nvert_2d][nlayers+1][3] vertex positions
+ *   cell_next      [ncell_2d][4] 1-based (W, S, E, N): orients the RT0 faces
+ * W0: A = M + nu K (Q1 mass + diffusion). W2: A = M2 + tau D^T D (RT0 mass
+ * plus the W3 divergence penalty). */
+int lfx_fem_w0_operator(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers,
+                        const int32_t* verts_on_cell, int64_t nvert_2d, const double* xyz3d,
+                        double nu, const int32_t* map, int64_t undf, int32_t ncolours,
+                        const int32_t* ncells_per_colour, const int32_t* cells_in_colour,
+                        int32_t max_cells_per_colour, lfx_op** op64, lfx_op** op32);
+int lfx_fem_w2_operator(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, const int32_t* cell_next,
+                        const int32_t* verts_on_cell, int64_t nvert_2d, const double* xyz3d,
+                        double tau, const int32_t* map, int64_t undf, int32_t ncolours,
+                        const int32_t* ncells_per_colour, const int32_t* cells_in_colour,
+                        int32_t max_cells_per_colour, lfx_op** op64, lfx_op** op32);
 
 /* ------------------------------------------------------------------ CMA
  * columnwise_operator_type (columnwise_operator_mod.f90:42-469): one banded
@@ -229,6 +252,36 @@ int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which);
 /* LFX_TIMEOUT if a kernel's bounded device-side wait ran out since the last
  * check (the kernel then skipped its work); synchronises the stream */
 int lfx_ctx_check_device_error(lfx_ctx* ctx);
+
+/* ------------------------------------------------------------------ batched solves
+ * Continuous batching of many independent SPD solves (no counterpart in the
+ * reference, which solves one system per call). Each slot runs preconditioned
+ * CG in FP32 with the solution accumulated in FP64 and reliable updates: the
+ * true residual b - A x is recomputed with the FP64 operator whenever the
+ * FP32 residual has dropped by 1e-2 since the last one, and a slot converges
+ * only when ||b - A x|| / ||b - A x0|| <= tol. Every kernel covers all
+ * admitted slots, and one CUDA graph replays `iters_per_launch`
+ * super-iterations for the whole batch; a slot's result does not depend on
+ * the other slots. The pools (max_dofs unknowns in total, max_entities dof
+ * columns, max_columns preconditioner columns) are allocated at creation:
+ * admission allocates nothing and fails with LFX_OUT_OF_MEMORY when they are
+ * full. ndf is 8 (W0) or 6 (W2) for every slot of a batch. */
+typedef struct lfx_batch lfx_batch;
+int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t max_dofs,
+                     int64_t max_entities, int64_t max_columns, int32_t iters_per_launch,
+                     lfx_batch** out);
+int lfx_batch_destroy(lfx_batch* b);
+/* op64/op32: FP64 and FP32 copies of one operator (lfx_lma_create_like);
+ * prec32: its FP32 Jacobi or column preconditioner; b, x: FP64 vectors kept
+ * alive until the slot is retired (x: initial guess in, solution out). */
+int lfx_batch_admit(lfx_batch* b, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, const lfx_vec* rhs,
+                    lfx_vec* x, double tol, int32_t max_iter, int64_t tag, int32_t* slot);
+/* one graph replay for every slot; *ndone = slots done and not yet retired */
+int lfx_batch_step(lfx_batch* b, int32_t* ndone);
+/* phase: 0 empty, 1 starting, 2 iterating, 3 done; info as lfx_solve_info */
+int lfx_batch_slot_info(const lfx_batch* b, int32_t slot, int32_t* phase, int64_t* tag,
+                        lfx_solve_info* info);
+int lfx_batch_retire(lfx_batch* b, int32_t slot);
 
 /* ------------------------------------------------------------------ no allocation
  * Allocation-free inner product (no counterpart in the reference): for

@@ -286,6 +286,7 @@ struct lfx_prec {
   int64_t rdiag_n = 0;
   size_t bytes = 0;
   int64_t max_row = -1;  // PREC_CMA: largest 0-based dof the columns touch
+  bool jacobi_zeroed = false;  // PREC_CMA: rdiag zeroed on the column rows (batched use)
 };
 
 namespace lfx {

@@ -134,6 +134,34 @@ __global__ void __launch_bounds__(256) lma_gather(LayoutArgs A, const T* __restr
   }
 }
 
+// One group record {cell, records, map_from row} read as 16-byte vectors
+// (gp_stride is a multiple of 4 ints).
+template <int NDF2>
+__device__ __forceinline__ void gather_record(const LayoutArgs& A, int g, int& c, uint32_t& pk,
+                                              int* mf) {
+  const int4* gp4 = reinterpret_cast<const int4*>(A.grp_pack + (size_t)g * A.gp_stride);
+  const int4 h0 = __ldg(gp4);
+  c = h0.x;
+  pk = (uint32_t)h0.y;
+  int tmp[12];
+  tmp[0] = h0.z;
+  tmp[1] = h0.w;
+  if (NDF2 > 2) {
+    const int4 h1 = __ldg(gp4 + 1);
+    tmp[2] = h1.x;
+    tmp[3] = h1.y;
+    tmp[4] = h1.z;
+    tmp[5] = h1.w;
+  }
+  if (NDF2 > 6) {
+    const int4 h2 = __ldg(gp4 + 2);
+    tmp[6] = h2.x;
+    tmp[7] = h2.y;
+  }
+#pragma unroll
+  for (int j = 0; j < NDF2; ++j) mf[j] = tmp[j];
+}
+
 // Register path (no shared memory) for groups of at most two records: all
 // loads of a cell group are issued before the FMA chain that consumes them.
 template <class T, int NDF2>
@@ -148,18 +176,22 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
   for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.nent; e += nwarp) {
     const int4 ep = __ldg(A.ent_pack + e);
     const int base = ep.x, h = ep.y, g0 = ep.z, g1 = ep.w;
-    for (int l = lane; l < h; l += 32) {
+    // all 32 lanes run every pass (lanes past the column's top just carry no
+    // valid record) so that the shuffles below see a converged warp
+    for (int l0 = 0; l0 < h; l0 += 32) {
+      const int l = l0 + lane;
       T acc = T(0);
       for (int g = g0; g < g1; ++g) {
-        const int32_t* gp = A.grp_pack + (size_t)g * A.gp_stride;
-        const int c = __ldg(gp);
-        const uint32_t pk = (uint32_t)__ldg(gp + 1);
+        int c;
+        uint32_t pk;
         int mf[NDF2];
-#pragma unroll
-        for (int j = 0; j < NDF2; ++j) mf[j] = __ldg(gp + 2 + j);
+        gather_record<NDF2>(A, g, c, pk, mf);
         const int k0 = l - rec_off(pk, 0), k1 = l - rec_off(pk, 1);
         const bool v0 = (unsigned)k0 < (unsigned)nl;
         const bool v1 = rec_n(pk) > 1 && (unsigned)k1 < (unsigned)nl;
+        // second record one level above the first (bottom/top vertex or
+        // face): its x values are the neighbouring lane's first-record values
+        const bool pair = rec_n(pk) == 2 && rec_off(pk, 1) == rec_off(pk, 0) + 1;
         const T* Mc = M + (size_t)c * cell_stride;
         const T* M0 = Mc + (size_t)rec_df(pk, 0) * A.blk + (v0 ? k0 : 0);
         const T* M1 = Mc + (size_t)rec_df(pk, 1) * A.blk + (v1 ? k1 : 0);
@@ -169,7 +201,16 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
           a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
           b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
           a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
-          b1[j] = v1 ? __ldg(x + mf[j] + k1) : T(0);
+        }
+        if (pair) {
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            const T up = __shfl_up_sync(0xffffffffu, b0[j], 1);
+            b1[j] = (lane == 0) ? (v1 ? __ldg(x + mf[j] + k1) : T(0)) : up;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) b1[j] = v1 ? __ldg(x + mf[j] + k1) : T(0);
         }
 #pragma unroll
         for (int j = 0; j < NDF2; ++j) {
@@ -177,10 +218,12 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
           if (v1) acc = fmaT(a1[j], b1[j], acc);
         }
       }
-      if (b)
-        y[base + l] = b[base + l] - acc;
-      else
-        y[base + l] = acc;
+      if (l < h) {
+        if (b)
+          y[base + l] = b[base + l] - acc;
+        else
+          y[base + l] = acc;
+      }
     }
   }
 }
@@ -560,7 +603,8 @@ int upload_matrix(lfx_ctx* ctx, lfx_op* op, const double* stencil) {
     return rc;
   }
   op->mat_bytes = (size_t)total * esz;
-  LFX_CK(ctx, cudaMemcpyAsync(raw, stencil, (size_t)total_in * 8, cudaMemcpyHostToDevice, ctx->stream));
+  // the stencil may be host or device memory (unified addressing)
+  LFX_CK(ctx, cudaMemcpyAsync(raw, stencil, (size_t)total_in * 8, cudaMemcpyDefault, ctx->stream));
   const int grid = ctx->num_sms * 16;
   if (op->precision == LFX_R64)
     relayout<double><<<grid, 256, 0, ctx->stream>>>(raw, (double*)op->mat, L->ncell_2d, L->nlayers,

@@ -119,6 +119,21 @@ _SIGS = [
      C.c_int),
     ("lfx_solver_apply", [vp, vp, vp, C.POINTER(SolveInfo)], C.c_int),
     ("lfx_solver_destroy", [vp], C.c_int),
+    ("lfx_fem_w0_operator", [vp, C.c_int32, C.c_int32, i32p, C.c_int64, f64p, C.c_double, i32p,
+                             C.c_int64, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(vp),
+                             C.POINTER(vp)], C.c_int),
+    ("lfx_fem_w2_operator", [vp, C.c_int32, C.c_int32, i32p, i32p, C.c_int64, f64p, C.c_double,
+                             i32p, C.c_int64, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(vp),
+                             C.POINTER(vp)], C.c_int),
+    ("lfx_batch_create", [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int32,
+                          C.POINTER(vp)], C.c_int),
+    ("lfx_batch_destroy", [vp], C.c_int),
+    ("lfx_batch_admit", [vp, vp, vp, vp, vp, vp, C.c_double, C.c_int32, C.c_int64,
+                         C.POINTER(C.c_int32)], C.c_int),
+    ("lfx_batch_step", [vp, C.POINTER(C.c_int32)], C.c_int),
+    ("lfx_batch_slot_info", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                             C.POINTER(SolveInfo)], C.c_int),
+    ("lfx_batch_retire", [vp, C.c_int32], C.c_int),
     ("lfx_dot_noalloc", [vp, vp, C.c_int64, vp, vp], C.c_int),
     ("lfx_dot_noalloc_max_n", [], C.c_int64),
     ("lfx_noalloc_last_error", [], C.c_char_p),
@@ -360,6 +375,81 @@ class LmaOperator(_Handle):
 
     def diagonal(self, diag):
         self.ctx.check(self.ctx.L.lfx_lma_diagonal(self.h, diag.h))
+
+
+def fem_operators(ctx, mesh, space, coef, precisions=(R64, R32)):
+    """Assemble the W0 (A = M + coef K) or W2 (A = M2 + coef D^T D) local
+    matrices of an extruded mesh on the device; returns {precision: LmaOperator}
+    sharing one layout, plus the dofmap and undf."""
+    from . import meshgen as mg
+    m, undf = mesh.dofmap(space)
+    npc, cic = mesh.colour_lookup()
+    h64, h32 = vp(), vp()
+    p64 = C.byref(h64) if R64 in precisions else None
+    p32 = C.byref(h32) if R32 in precisions else None
+    nv = len(mesh.vert_xyz)
+    args = (ctx.h, mesh.ncell_2d, mesh.nlayers)
+    tail = (m, undf, len(npc), npc, np.ascontiguousarray(cic), cic.shape[0], p64, p32)
+    if space == mg.W0:
+        ctx.check(ctx.L.lfx_fem_w0_operator(*args, mesh.verts_on_cell, nv, mesh.xyz3d, coef, *tail))
+        ndf = 8
+    else:
+        ctx.check(ctx.L.lfx_fem_w2_operator(*args, mesh.cell_next, mesh.verts_on_cell, nv,
+                                            mesh.xyz3d, coef, *tail))
+        ndf = 6
+    ops = {}
+    for prec, h in ((R64, h64), (R32, h32)):
+        if prec in precisions:
+            ops[prec] = LmaOperator(ctx, mesh.ncell_2d, mesh.nlayers, ndf, ndf, None, None, undf,
+                                    undf, None, None, None, precision=prec, _h=h)
+    first = ops.get(R64)
+    for op in ops.values():
+        if op is not first and first is not None:
+            op._parent = first
+    return ops, m, undf
+
+
+class Batch(_Handle):
+    """Continuous batching of independent SPD solves (lfx_batch)."""
+
+    _destroy = "lfx_batch_destroy"
+
+    def __init__(self, ctx, ndf, max_slots, max_dofs, max_entities, max_columns=0, iters=4):
+        self.ctx = ctx
+        h = vp()
+        ctx.check(ctx.L.lfx_batch_create(ctx.h, ndf, max_slots, max_dofs, max_entities,
+                                         max_columns, iters, C.byref(h)))
+        self.h = h
+        self.max_slots = max_slots
+        self._keep = {}
+
+    def admit(self, op64, op32, prec32, b, x, tol, max_iter=10000, tag=0):
+        s = C.c_int32()
+        rc = self.ctx.L.lfx_batch_admit(self.h, op64.h, op32.h, prec32.h, b.h, x.h, tol, max_iter,
+                                        tag, C.byref(s))
+        if rc == 3:  # pools or slots full
+            return None
+        self.ctx.check(rc)
+        self._keep[s.value] = (op64, op32, prec32, b, x)
+        return s.value
+
+    def step(self):
+        nd = C.c_int32()
+        self.ctx.check(self.ctx.L.lfx_batch_step(self.h, C.byref(nd)))
+        return nd.value
+
+    def slot(self, s):
+        ph, tag, info = C.c_int32(), C.c_int64(), SolveInfo()
+        self.ctx.check(self.ctx.L.lfx_batch_slot_info(self.h, s, C.byref(ph), C.byref(tag),
+                                                      C.byref(info)))
+        return ph.value, tag.value, info
+
+    def done_slots(self):
+        return [s for s in range(self.max_slots) if self.slot(s)[0] == 3]
+
+    def retire(self, s):
+        self.ctx.check(self.ctx.L.lfx_batch_retire(self.h, s))
+        self._keep.pop(s, None)
 
 
 class ColumnwiseOperator(_Handle):

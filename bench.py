@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=3, help="oracle solves timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="skip the batched and serving legs")
     return ap.parse_args()
 
 
@@ -138,6 +139,155 @@ def profiled_traffic():
         except ValueError:
             return None
     return None
+
+
+def leg_batched(ctx, lfx, mg, wl, torch, stream):
+    """256 independent W0 solves of uneven size (C12-C48 x 10-70 levels,
+    tolerances 1e-10..1e-6) in one batch (FP32 PCG with FP64 reliable
+    updates, one CUDA graph per 8 super-iterations), against the same solves
+    run one after another with the plain FP64 device-resident CG."""
+    specs = wl.config3_specs()
+    t0 = time.perf_counter()
+    systems = [wl.batch_system(ctx, n, l, sd, mg.W0) for n, l, _, sd in specs]
+    setup_s = time.perf_counter() - t0
+    tot = sum(s.undf for s in systems)
+    ent = sum(s.entities for s in systems)
+    B = lfx.Batch(ctx, 8, len(systems), tot, ent, 0, 8)
+    xs = [lfx.FieldVector(ctx, [s.undf]) for s in systems]
+
+    def batched():
+        slots = []
+        for s, x, (_, _, tol, _) in zip(systems, xs, specs):
+            x.set_scalar(0.0)
+            slots.append(B.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x, tol, 20000))
+        steps = 0
+        while B.step() < len(systems):
+            steps += 1
+        infos = [B.slot(sl)[2].as_dict() for sl in slots]
+        for sl in slots:
+            B.retire(sl)
+        return infos, steps
+
+    batched()  # warm-up (graph already captured; pages the pools in)
+    ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    ctx.synchronize()
+    ev[0].record(stream)
+    w0 = time.perf_counter()
+    infos, steps = batched()
+    ev[1].record(stream)
+    ctx.synchronize()
+    t_batch = ev[0].elapsed_time(ev[1]) / 1e3
+    wall_batch = time.perf_counter() - w0
+    ok = all(i["status"] == 0 and i["final_rel"] <= tol * 1.0001
+             for i, (_, _, tol, _) in zip(infos, specs))
+    # plain FP64 serial solves of the same systems (graphs warmed first)
+    cgs = [s.cg64(tol) for s, (_, _, tol, _) in zip(systems, specs)]
+    for c, s, x in zip(cgs, systems, xs):
+        x.set_scalar(0.0)
+        c.apply(x, s.b)
+    ctx.synchronize()
+    ev[0].record(stream)
+    it64 = []
+    for c, s, x in zip(cgs, systems, xs):
+        x.set_scalar(0.0)
+        it64.append(c.apply(x, s.b).iterations)
+    ev[1].record(stream)
+    ctx.synchronize()
+    t_serial = ev[0].elapsed_time(ev[1]) / 1e3
+    cells = sum(6 * n * n * l for n, l, _, _ in specs)
+    return {
+        "workload": "256 uneven W0 mass+diffusion solves, C12-C48 x 10-70 levels, tol 1e-10..1e-6 "
+                    "(seeded), FP32 PCG + FP64 reliable updates, one batch",
+        "cells_total": cells, "dofs_total": tot,
+        "batched_solves_per_s": round(len(specs) / t_batch, 2),
+        "batched_s": round(t_batch, 4), "batched_wall_s": round(wall_batch, 4),
+        "graph_replays": steps + 1, "iterations_max": max(i["iterations"] for i in infos),
+        "all_converged_on_fp64_residual": ok,
+        "serial_fp64_solves_per_s": round(len(specs) / t_serial, 2), "serial_fp64_s": round(t_serial, 4),
+        "serial_fp64_iterations_max": max(it64),
+        "speedup_vs_serial_fp64": round(t_serial / t_batch, 3), "setup_s": round(setup_s, 1),
+    }
+
+
+def leg_serving(ctx, lfx, mg, wl, nreq=200):
+    """Poisson stream (2000 requests/s, seeded) of W2 Helmholtz solves of
+    mixed size (a pool of 12 operators, C12-C96 x 20-70 levels; right-hand
+    sides staged in HBM), tolerances 1e-10..1e-6: continuous batching against
+    serial plain FP64 solves of the same request list."""
+    shapes, reqs = wl.config4_stream(nreq=nreq)
+    systems = [wl.batch_system(ctx, n, l, 500 + i, mg.W2) for i, (n, l) in enumerate(shapes)]
+    big = max(s.undf for s in systems)
+    B = lfx.Batch(ctx, 6, 32, 6 * big, 6 * max(s.entities for s in systems),
+                  6 * max(s.columns for s in systems), 4)
+    free_x = {i: [lfx.FieldVector(ctx, [s.undf]) for _ in range(4)] for i, s in enumerate(systems)}
+    # serial FP64 service times: one device-resident CG per operator, warmed
+    # (graphs captured) before timing; each request sets its tolerance
+    cgs = {}
+    for i, s in enumerate(systems):
+        cgs[i] = s.cg64(1e-10)
+        x = free_x[i][0]
+        x.set_scalar(0.0)
+        cgs[i].apply(x, s.b)
+    service = []
+    for _, w, tol in reqs:
+        s, x = systems[w], free_x[w][0]
+        cgs[w].set_tolerance(tol)
+        x.set_scalar(0.0)
+        ctx.synchronize()
+        t = time.perf_counter()
+        cgs[w].apply(x, s.b)
+        service.append(time.perf_counter() - t)
+    fin, lat_serial = 0.0, []
+    for (arr, _, _), sv in zip(reqs, service):
+        fin = max(fin, arr) + sv
+        lat_serial.append(fin - arr)
+    serial_makespan = fin - reqs[0][0]
+    # continuous batching
+    pending, inflight, lat, done = list(range(nreq)), {}, [0.0] * nreq, 0
+    occupancy = []
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    while done < nreq:
+        now = time.perf_counter() - t0
+        while pending and reqs[pending[0]][0] <= now and free_x[reqs[pending[0]][1]]:
+            r = pending[0]
+            _, w, tol = reqs[r]
+            s = systems[w]
+            x = free_x[w].pop()
+            x.set_scalar(0.0)
+            slot = B.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x, tol, 20000, r)
+            if slot is None:
+                free_x[w].append(x)
+                break
+            inflight[slot] = (r, w, x)
+            pending.pop(0)
+        if not inflight:
+            if pending:
+                time.sleep(max(0.0, reqs[pending[0]][0] - (time.perf_counter() - t0)))
+            continue
+        occupancy.append(len(inflight))
+        B.step()
+        now = time.perf_counter() - t0
+        for slot in B.done_slots():
+            r, w, x = inflight.pop(slot)
+            ph, tag, info = B.slot(slot)
+            lat[r] = now - reqs[r][0]
+            B.retire(slot)
+            free_x[w].append(x)
+            done += 1
+    makespan = time.perf_counter() - t0 - reqs[0][0]
+    pct = lambda v, q: round(1e3 * float(np.percentile(v, q)), 3)
+    return {
+        "workload": f"{nreq} W2 Helmholtz requests, Poisson 2000/s, 12-operator pool C12-C96 x "
+                    "20-70 levels, tol 1e-10..1e-6, continuous batching (FP32 PCG + FP64 "
+                    "reliable updates, column preconditioner)",
+        "solves_per_s": round(nreq / makespan, 2), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+        "mean_inflight": round(float(np.mean(occupancy)), 2) if occupancy else 0,
+        "serial_fp64_solves_per_s": round(nreq / serial_makespan, 2),
+        "serial_fp64_p50_ms": pct(lat_serial, 50), "serial_fp64_p99_ms": pct(lat_serial, 99),
+        "serial_fp64_mean_service_ms": round(1e3 * float(np.mean(service)), 3),
+        "speedup_vs_serial_fp64": round(serial_makespan / makespan, 3),
+    }
 
 
 def cpu_baseline(problem, nsolves):
@@ -326,6 +476,10 @@ def main():
     cb = None
     if world == 1 and not args.no_cpu:
         cb = cpu_baseline(p, args.cpu_sample)
+    extra = {}
+    if not args.quick:
+        extra["batched_uneven_w0"] = leg_batched(ctx, lfx, mg, wl, torch, stream)
+        extra["serving_w2"] = leg_serving(ctx, lfx, mg, wl)
 
     def pct(v, q):
         return float(np.percentile(np.array(v), q))
@@ -357,6 +511,7 @@ def main():
                 "p50_ms": round(pct(e["lat"], 50), 4)},
         "gpu_launches": mx["launches"],
         "clocks": clk.summary(),
+        "workloads": extra,
     }
     print(json.dumps(line), flush=True)
     if dist:

@@ -225,6 +225,8 @@ int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
 /* x: initial guess on entry, solution on exit; b unchanged */
 int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info* info);
 int lfx_solver_destroy(lfx_solver* s);
+/* change r_tol / a_tol for the next solves (keeps the solver's CUDA graphs) */
+int lfx_solver_set_tolerance(lfx_solver* s, double r_tol, double a_tol);
 
 /* Mixed-precision solve with FP64 iterative refinement: the residual
  * b - A x and the solution update stay FP64 (op64, FP64 vectors); each

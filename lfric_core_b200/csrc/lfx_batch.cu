@@ -60,7 +60,7 @@ struct BState {
   double tol, r0, rlast, rnorm, rz, alpha, beta, true_rel;
 };
 
-constexpr double kDelta = 1e-2;  // reliable update when ||r|| drops by this factor
+constexpr double kDelta = 1e-3;  // reliable update when ||r|| drops by this factor
 
 __device__ __forceinline__ bool ph_run(const BState& s) { return s.phase == PH_RUN; }
 __device__ __forceinline__ bool ph_resid(const BState& s) {
@@ -72,20 +72,27 @@ __device__ __forceinline__ bool ph_active(const BState& s) {
 
 // Batched chunk kernel: items are (slot, chunk); ld/op as in chunk_kernel but
 // with the slot's descriptor; fin(slot desc, state, tot) runs once per slot
-// after all its chunks.
+// after all its chunks. A non-null gate that reads zero skips the launch; a
+// non-null reset is cleared by the first thread.
 template <int NR, class Pred, class Ld, class Op, class Fin>
 __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, const BSlot* slots,
                                             BState* st, double* partials, unsigned* tickets,
-                                            Pred pred, Ld ld, Op op, Fin fin) {
+                                            const int* gate, int* reset, Pred pred, Ld ld, Op op,
+                                            Fin fin) {
   __shared__ double sm[RT / 32];
   __shared__ int am_last;
+  if (gate && !*((volatile const int*)gate)) return;
+  if (reset && blockIdx.x == 0 && threadIdx.x == 0) *reset = 0;
   const int L = *len;
   for (int u = blockIdx.x; u < L; u += gridDim.x) {
     const int2 w = list[u];
     if (w.x < 0) continue;
-    BState& S = st[w.x];
-    if (!pred(S)) continue;
-    const BSlot& D = slots[w.x];
+    BState& Sg = st[w.x];
+    if (!pred(Sg)) continue;
+    // local copies: the element loop's stores cannot alias them, so pointers
+    // and scalars stay in registers
+    const BSlot D = slots[w.x];
+    const BState S = Sg;
     const int64_t base = (int64_t)w.y * RCHUNK + threadIdx.x;
     using V = decltype(ld(D, int64_t(0)));
     V v[RPER];
@@ -122,7 +129,7 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
         tot[r] = block_sum(a, sm);
       }
       if (threadIdx.x == 0) {
-        fin(D, S, tot);
+        fin(D, Sg, tot);
         tickets[w.x] = 0u;
       }
       __syncthreads();
@@ -131,40 +138,63 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
 }
 
 // Batched LMA apply (register gather), items (slot, entity). RESID: y = b - A64 x
-// with x = slot.x, y = slot.r64; else z = A32 p.
+// with x = slot.x, y = slot.r64; else z = A32 p. A non-null gate that reads
+// zero skips the launch.
 template <int NDF2, bool RESID>
 __global__ void __launch_bounds__(256) bapply(const int2* list, const int* len, const BSlot* slots,
-                                              const BState* st) {
+                                              const BState* st, const int* gate) {
   using T = typename std::conditional<RESID, double, float>::type;
+  if (gate && !*((volatile const int*)gate)) return;
   const int lane = threadIdx.x & 31;
   const int L = *len;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < L; u += nwarp) {
     const int2 w = list[u];
     if (w.x < 0) continue;
-    const BState& S = st[w.x];
-    if (RESID ? !ph_resid(S) : !ph_run(S)) continue;
-    const BSlot& D = slots[w.x];
-    const T* M = RESID ? (const T*)D.M64 : (const T*)D.M32;
+    if (RESID ? !ph_resid(st[w.x]) : !ph_run(st[w.x])) continue;
+    // local copy: the stores below cannot alias it, so the pointers stay in
+    // registers across the column loop
+    const BSlot D = slots[w.x];
+    const T* __restrict__ M = RESID ? (const T*)D.M64 : (const T*)D.M32;
     const int blk = RESID ? D.blk64 : D.blk32;
-    const T* x = RESID ? (const T*)D.x : (const T*)D.p;
-    T* y = RESID ? (T*)D.r64 : (T*)D.z;
+    const T* __restrict__ x = RESID ? (const T*)D.x : (const T*)D.p;
+    T* __restrict__ y = RESID ? (T*)D.r64 : (T*)D.z;
     const int nl = D.nl;
     const size_t cell_stride = (size_t)D.ndf1 * blk;
     const int4 ep = __ldg(D.ent_pack + w.y);
-    for (int l = lane; l < ep.y; l += 32) {
+    // all 32 lanes run every pass so the shuffles below see a converged warp
+    for (int l0 = 0; l0 < ep.y; l0 += 32) {
+      const int l = l0 + lane;
       T acc = T(0);
       for (int g = ep.z; g < ep.w; ++g) {
-        const int32_t* gp = D.grp_pack + (size_t)g * D.gp_stride;
-        const int c = __ldg(gp);
-        const uint32_t pk = (uint32_t)__ldg(gp + 1);
-        int mf[NDF2];
-#pragma unroll
-        for (int j = 0; j < NDF2; ++j) mf[j] = __ldg(gp + 2 + j);
+        // group record {cell, records, map_from row} as 16-byte vectors
+        // (gp_stride is a multiple of 4 ints)
+        const int4* gp4 = reinterpret_cast<const int4*>(D.grp_pack + (size_t)g * D.gp_stride);
+        const int4 h0 = __ldg(gp4);
+        const int c = h0.x;
+        const uint32_t pk = (uint32_t)h0.y;
+        int tmp[8];
+        tmp[0] = h0.z;
+        tmp[1] = h0.w;
+        if (NDF2 > 2) {
+          const int4 h1 = __ldg(gp4 + 1);
+          tmp[2] = h1.x;
+          tmp[3] = h1.y;
+          tmp[4] = h1.z;
+          tmp[5] = h1.w;
+        }
+        if (NDF2 > 6) {
+          const int4 h2 = __ldg(gp4 + 2);
+          tmp[6] = h2.x;
+          tmp[7] = h2.y;
+        }
         const int o0 = (pk >> 8) & 7u, o1 = (pk >> 17) & 7u;
         const int k0 = l - o0, k1 = l - o1;
         const bool v0 = (unsigned)k0 < (unsigned)nl;
         const bool v1 = (pk & 3u) > 1 && (unsigned)k1 < (unsigned)nl;
+        // second record one level above the first: its x values are the
+        // neighbouring lane's first-record values
+        const bool pair = (pk & 3u) == 2 && o1 == o0 + 1;
         const T* Mc = M + (size_t)c * cell_stride;
         const T* M0 = Mc + (size_t)((pk >> 2) & 63u) * blk + (v0 ? k0 : 0);
         const T* M1 = Mc + (size_t)((pk >> 11) & 63u) * blk + (v1 ? k1 : 0);
@@ -172,9 +202,18 @@ __global__ void __launch_bounds__(256) bapply(const int2* list, const int* len, 
 #pragma unroll
         for (int j = 0; j < NDF2; ++j) {
           a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
-          b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
+          b0[j] = v0 ? __ldg(x + tmp[j] + k0) : T(0);
           a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
-          b1[j] = v1 ? __ldg(x + mf[j] + k1) : T(0);
+        }
+        if (pair) {
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            const T up = __shfl_up_sync(0xffffffffu, b0[j], 1);
+            b1[j] = (lane == 0) ? (v1 ? __ldg(x + tmp[j] + k1) : T(0)) : up;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) b1[j] = v1 ? __ldg(x + tmp[j] + k1) : T(0);
         }
 #pragma unroll
         for (int j = 0; j < NDF2; ++j) {
@@ -182,11 +221,13 @@ __global__ void __launch_bounds__(256) bapply(const int2* list, const int* len, 
           if (v1) acc = fmaT(a1[j], b1[j], acc);
         }
       }
-      const int row = ep.x + l;
-      if (RESID)
-        y[row] = (T)D.b[row] - acc;
-      else
-        y[row] = acc;
+      if (l < ep.y) {
+        const int row = ep.x + l;
+        if (RESID)
+          y[row] = (T)D.b[row] - acc;
+        else
+          y[row] = acc;
+      }
     }
   }
 }
@@ -198,22 +239,9 @@ __global__ void bthomas(const int2* list, const int* len, const BSlot* slots, co
   for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < L; u += gridDim.x * blockDim.x) {
     const int2 w = list[u];
     if (w.x < 0 || !ph_active(st[w.x])) continue;
-    const BSlot& D = slots[w.x];
-    const int c = w.y, nc = D.ncol;
-    const int f = D.first[c];
-    double d = 0.0;
-    for (int i = 0; i < D.nrow; ++i) {
-      const int mu = f + D.ind[i];
-      const double xv = (double)D.r[mu];
-      const double inv = (double)D.finv[(size_t)i * nc + c];
-      d = (i == 0) ? inv * xv : inv * fma(-(double)D.fa[(size_t)i * nc + c], d, xv);
-      D.z[mu] = (float)d;
-    }
-    for (int i = D.nrow - 2; i >= 0; --i) {
-      const int mu = f + D.ind[i];
-      d = fma(-(double)D.fc[(size_t)i * nc + c], d, (double)D.z[mu]);
-      D.z[mu] = (float)d;
-    }
+    const BSlot D = slots[w.x];  // local copy: the z stores cannot alias it
+    thomas_sweep<8>(__ldg(D.first + w.y), D.ind, D.nrow, D.ncol, w.y, D.fa, D.finv, D.fc,
+                    (const float*)D.r, D.z);
   }
 }
 
@@ -302,47 +330,52 @@ int launch_super(lfx_batch* B) {
   const int* le = B->d_len;
   const int* lc = B->d_len + 1;
   const int* lk = B->d_len + 2;
+  // nonzero while some slot needs a true residual this super-iteration: set
+  // by admission and by step 3, cleared by step 6
+  int* need = B->d_len + 3;
   double* pa = B->d_partials;
   unsigned* tk = B->d_tickets;
   auto run = [] __device__(const BState& s) { return ph_run(s); };
   auto resid = [] __device__(const BState& s) { return ph_resid(s); };
   auto active = [] __device__(const BState& s) { return ph_active(s); };
   // 1. z = A32 p
-  bapply<NDF2, false><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st);
+  bapply<NDF2, false><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, nullptr);
   // 2. alpha = rz / <p, z>
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, run,
+      B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, run,
       [] __device__(const BSlot& D, int64_t i) { return V2<float>{D.p[i], D.z[i]}; },
-      [] __device__(const BSlot&, BState&, int64_t, const V2<float>& v, double* a) {
+      [] __device__(const BSlot&, const BState&, int64_t, const V2<float>& v, double* a) {
         a[0] = fma((double)v.a, (double)v.b, a[0]);
       },
       [] __device__(const BSlot&, BState& S, const double* t) { S.alpha = S.rz / t[0]; });
   // 3. x += alpha p (FP64); r -= alpha z (FP32); ||r||; decide on a true residual
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, run,
+      B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, run,
       [] __device__(const BSlot& D, int64_t i) {
         return V4<double>{D.x[i], (double)D.p[i], (double)D.r[i], (double)D.z[i]};
       },
-      [] __device__(const BSlot& D, BState& S, int64_t i, const V4<double>& v, double* a) {
+      [] __device__(const BSlot& D, const BState& S, int64_t i, const V4<double>& v, double* a) {
         D.x[i] = fma(S.alpha, v.b, v.a);
         const float ri = fmaf((float)(-S.alpha), (float)v.d, (float)v.c);
         D.r[i] = ri;
         a[0] = fma((double)ri, (double)ri, a[0]);
       },
-      [] __device__(const BSlot&, BState& S, const double* t) {
+      [need] __device__(const BSlot&, BState& S, const double* t) {
         S.iter += 1;
         S.rnorm = sqrt(t[0]);
         if (S.rnorm <= kDelta * S.rlast || S.rnorm <= S.tol * S.r0 || S.iter >= S.max_iter ||
-            !(S.rnorm == S.rnorm))
+            !(S.rnorm == S.rnorm)) {
           S.flag = 1;
+          *need = 1;
+        }
       });
   // 4. r64 = b - A64 x (new slots, and slots taking a true residual)
-  bapply<NDF2, true><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st);
+  bapply<NDF2, true><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, need);
   // 5. ||r64||, r = r64 (FP32); convergence on the true residual
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, resid,
+      B->d_ch, lc, sl, st, pa, tk, need, nullptr, resid,
       [] __device__(const BSlot& D, int64_t i) { return V1<double>{D.r64[i]}; },
-      [] __device__(const BSlot& D, BState&, int64_t i, const V1<double>& v, double* a) {
+      [] __device__(const BSlot& D, const BState&, int64_t i, const V1<double>& v, double* a) {
         D.r[i] = (float)v.a;
         a[0] = fma(v.a, v.a, a[0]);
       },
@@ -375,9 +408,9 @@ int launch_super(lfx_batch* B) {
   //    with rz_new = <r, z> and beta
   if (B->cap_col > 0) bthomas<<<ctx->num_sms * 8, 128, 0, ctx->stream>>>(B->d_col, lk, sl, st);
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, active,
+      B->d_ch, lc, sl, st, pa, tk, nullptr, need, active,
       [] __device__(const BSlot& D, int64_t i) { return V3<float>{D.r[i], D.diag[i], D.z[i]}; },
-      [] __device__(const BSlot& D, BState&, int64_t i, const V3<float>& v, double* a) {
+      [] __device__(const BSlot& D, const BState&, int64_t i, const V3<float>& v, double* a) {
         // rows with a positive diagonal entry are Jacobi rows; the column rows
         // (written by the sweeps) carry a zero in the Jacobi diagonal
         float zi = v.c;
@@ -393,9 +426,9 @@ int launch_super(lfx_batch* B) {
       });
   // 7. p = z + beta p (p = z for a new slot); new slots start iterating
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, active,
+      B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, active,
       [] __device__(const BSlot& D, int64_t i) { return V2<float>{D.p[i], D.z[i]}; },
-      [] __device__(const BSlot& D, BState& S, int64_t i, const V2<float>& v, double*) {
+      [] __device__(const BSlot& D, const BState& S, int64_t i, const V2<float>& v, double*) {
         D.p[i] = S.fresh ? v.b : fmaf((float)S.beta, v.a, v.b);
       },
       [] __device__(const BSlot&, BState& S, const double*) {
@@ -615,6 +648,8 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
                                        cudaMemcpyHostToDevice, ctx->stream));
   if (!rc) LFX_CK(ctx, cudaMemcpyAsync(B->d_state + s, &B->h_state[s], sizeof(BState),
                                        cudaMemcpyHostToDevice, ctx->stream));
+  // the new slot takes its first residual in the next super-iteration
+  if (!rc) LFX_CK(ctx, cudaMemsetAsync(B->d_len + 3, 1, sizeof(int), ctx->stream));
   if (!rc) rc = set_lengths(B);
   if (rc) {
     H = SlotHost();

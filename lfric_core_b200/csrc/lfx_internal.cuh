@@ -194,6 +194,64 @@ int launch_chunks(lfx_ctx* ctx, int64_t n, Ld ld, Op op, Fin fin, const int* ski
   return LFX_OK;
 }
 
+// Thomas sweeps of one column with x-independent factors stored [row][column]
+// (nc columns): y = T^{-1} x on rows f + ind[i], i < nrow, in FP64 with the
+// forward result rounded to TX between the sweeps. The loads of R rows are
+// issued ahead of their dependent recurrence steps, so a column costs about
+// 2 nrow / R memory latencies instead of 2 nrow. Every row is read before it
+// is written, so x == y is allowed.
+template <int R, class TF, class TX>
+__device__ __forceinline__ void thomas_sweep(int f, const int* __restrict__ ind, int nrow, int nc,
+                                             int c, const TF* __restrict__ fa,
+                                             const TF* __restrict__ finv,
+                                             const TF* __restrict__ fc, const TX* x, TX* y) {
+  double d = 0.0;
+  for (int i0 = 0; i0 < nrow; i0 += R) {
+    int mu[R];
+    double xv[R], iv[R], av[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int i = i0 + j;
+      if (i < nrow) {
+        mu[j] = f + __ldg(ind + i);
+        xv[j] = (double)x[mu[j]];
+        iv[j] = (double)__ldg(finv + (size_t)i * nc + c);
+        av[j] = (double)__ldg(fa + (size_t)i * nc + c);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int i = i0 + j;
+      if (i < nrow) {
+        d = (i == 0) ? iv[j] * xv[j] : iv[j] * fma(-av[j], d, xv[j]);
+        y[mu[j]] = (TX)d;
+      }
+    }
+  }
+  // back substitution; d holds row nrow-1, already final
+  for (int i0 = nrow - 2; i0 >= 0; i0 -= R) {
+    int mu[R];
+    double yv[R], cv[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int i = i0 - j;
+      if (i >= 0) {
+        mu[j] = f + __ldg(ind + i);
+        yv[j] = (double)y[mu[j]];
+        cv[j] = (double)__ldg(fc + (size_t)i * nc + c);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int i = i0 - j;
+      if (i >= 0) {
+        d = fma(-cv[j], d, yv[j]);
+        y[mu[j]] = (TX)d;
+      }
+    }
+  }
+}
+
 }  // namespace lfx
 
 // ---------------------------------------------------------------- objects

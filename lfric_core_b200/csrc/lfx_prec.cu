@@ -109,21 +109,7 @@ __global__ void __launch_bounds__(128) cma_prec_apply(
   if ((int)blockIdx.x < thomas_blocks) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
-    const int f = first[c];
-    double d = 0.0;
-    for (int i = 0; i < nrow; ++i) {
-      const int mu = f + ind[i];
-      const double xv = (double)x[mu];
-      const double inv = (double)finv[(size_t)i * ncell + c];
-      d = (i == 0) ? inv * xv : inv * fma(-(double)fa[(size_t)i * ncell + c], d, xv);
-      y[mu] = (T)d;
-    }
-    // back substitution; d holds row nrow-1, already final
-    for (int i = nrow - 2; i >= 0; --i) {
-      const int mu = f + ind[i];
-      d = fma(-(double)fc[(size_t)i * ncell + c], d, (double)y[mu]);
-      y[mu] = (T)d;
-    }
+    thomas_sweep<8>(first[c], ind, nrow, ncell, c, fa, finv, fc, x, y);
   } else {
     const int lane = threadIdx.x & 31;
     const int64_t w = ((int64_t)(blockIdx.x - thomas_blocks) * blockDim.x + threadIdx.x) >> 5;

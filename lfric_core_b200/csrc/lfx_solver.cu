@@ -1003,4 +1003,13 @@ int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info
 
 int lfx_solver_destroy(lfx_solver* s) { return free_solver(s); }
 
+// The tolerances are read from the solver's device state at every solve, so
+// changing them keeps the captured graphs valid.
+int lfx_solver_set_tolerance(lfx_solver* s, double r_tol, double a_tol) {
+  if (!s || !(r_tol >= 0.0) || !(a_tol >= 0.0)) return LFX_INVALID_ARGUMENT;
+  s->cfg.r_tol = r_tol;
+  s->cfg.a_tol = a_tol;
+  return LFX_OK;
+}
+
 }  // extern "C"

@@ -119,6 +119,7 @@ _SIGS = [
      C.c_int),
     ("lfx_solver_apply", [vp, vp, vp, C.POINTER(SolveInfo)], C.c_int),
     ("lfx_solver_destroy", [vp], C.c_int),
+    ("lfx_solver_set_tolerance", [vp, C.c_double, C.c_double], C.c_int),
     ("lfx_fem_w0_operator", [vp, C.c_int32, C.c_int32, i32p, C.c_int64, f64p, C.c_double, i32p,
                              C.c_int64, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(vp),
                              C.POINTER(vp)], C.c_int),
@@ -532,6 +533,9 @@ class ColumnwisePreconditioner(_Prec):
 
 class _Solver(_Handle):
     _destroy = "lfx_solver_destroy"
+
+    def set_tolerance(self, r_tol, a_tol=0.0):
+        self.ctx.check(self.ctx.L.lfx_solver_set_tolerance(self.h, r_tol, a_tol))
 
     def apply(self, x: FieldVector, b: FieldVector) -> SolveInfo:
         info = SolveInfo()

@@ -75,6 +75,75 @@ def device_w2(ctx, p: mg.Problem, precision=lfx.R64, op64=None, cma=None, diag64
     return DeviceSystem(ctx, p, op32, prec32, diag64, lfx.R32, cma, op64)
 
 
+@dataclass
+class BatchSystem:
+    """One independent SPD system for lfx.Batch, assembled on the device:
+    FP64 and FP32 copies of the operator, the FP32 preconditioner the batch
+    iterates with and the FP64 one for plain FP64 solves, and a right-hand side."""
+
+    space: int
+    n: int
+    nlayers: int
+    undf: int
+    entities: int
+    columns: int
+    ops: dict
+    prec32: object
+    prec64: object
+    b: lfx.FieldVector
+    keep: tuple = ()
+
+    def cg64(self, r_tol, max_iter=20000):
+        return lfx.ConjugateGradient(self.ops[lfx.R64], self.prec64, r_tol, 0.0, max_iter)
+
+
+def batch_system(ctx, n, nlayers, seed, space, rhs_seed=None) -> BatchSystem:
+    mesh = mg.cubed_sphere(n, nlayers, seed=seed)
+    ncell = 6 * n * n
+    rhs_seed = seed + 1000 if rhs_seed is None else rhs_seed
+    if space == mg.W0:
+        ops, m, undf = lfx.fem_operators(ctx, mesh, mg.W0, 1.0)
+        d32 = lfx.FieldVector(ctx, [undf], lfx.R32)
+        ops[lfx.R32].diagonal(d32)
+        d64 = lfx.FieldVector(ctx, [undf], lfx.R64)
+        ops[lfx.R64].diagonal(d64)
+        p32 = lfx.DiagonalPreconditioner(ctx, d32)
+        p64 = lfx.DiagonalPreconditioner(ctx, d64)
+        b = lfx.FieldVector.from_array(ctx, mg.uniform(rhs_seed, undf))
+        return BatchSystem(space, n, nlayers, undf, ncell + 2, 0, ops, p32, p64, b, (d32, d64))
+    ops, m, undf = lfx.fem_operators(ctx, mesh, mg.W2, 0.1)
+    prm = mg.w2v_cma_params(nlayers)
+    cma = lfx.ColumnwiseOperator.assemble(ops[lfx.R64], [d + 1 for d in mg.W2V_DFS],
+                                          prm["column_banded_dofmap"], prm,
+                                          np.ascontiguousarray(m[:, mg.W2V_DFS[0]]))
+    d64 = lfx.FieldVector(ctx, [undf], lfx.R64)
+    ops[lfx.R64].diagonal(d64)
+    p64 = lfx.ColumnwisePreconditioner(ctx, cma, d64, lfx.R64)
+    p32 = lfx.ColumnwisePreconditioner(ctx, cma, d64, lfx.R32)
+    b = lfx.FieldVector.from_array(ctx, mg.normal(rhs_seed, undf))
+    return BatchSystem(space, n, nlayers, undf, 3 * ncell, ncell, ops, p32, p64, b, (cma, d64))
+
+
+def config3_specs(count=256, seed=3):
+    """Uneven batch: N ~ U{12..48}, nlayers ~ U{10..70}, tol ~ logU[1e-10, 1e-6]."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(12, 49, count)
+    ls = rng.integers(10, 71, count)
+    tols = 10.0 ** rng.uniform(-10, -6, count)
+    return [(int(n), int(l), float(t), 100 + i) for i, (n, l, t) in enumerate(zip(ns, ls, tols))]
+
+
+def config4_stream(nreq=200, rate=2000.0, pool=12, seed=4):
+    """Poisson arrivals (rate per second) of W2 Helmholtz solves drawn from a
+    pool of operators with N ~ U{12..96}, nlayers ~ U{20..70}; tol ~ logU[1e-10, 1e-6]."""
+    rng = np.random.default_rng(seed)
+    shapes = [(int(n), int(l)) for n, l in zip(rng.integers(12, 97, pool), rng.integers(20, 71, pool))]
+    t = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    which = rng.integers(0, pool, nreq)
+    tols = 10.0 ** rng.uniform(-10, -6, nreq)
+    return shapes, [(float(a), int(w), float(tl)) for a, w, tl in zip(t, which, tols)]
+
+
 def refined_gmres(sys32: DeviceSystem, gcrk=10, inner_rtol=1e-4, inner_cycles=50, r_tol=1e-8,
                   max_outer=20):
     """FP32 GMRES(gcrk) inner solve wrapped in FP64 iterative refinement."""

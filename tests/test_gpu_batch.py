@@ -116,6 +116,47 @@ def test_batch_admission_while_running(ctx):
         assert same(finished[i], ref[i])
 
 
+def test_batch_w2_line_preconditioner(ctx):
+    """W2 Helmholtz systems with the column preconditioner: batch results are
+    the same alone and in the mix, and reach the tolerance on FP64."""
+    from lfric_core_b200 import workloads as wl
+    systems = [wl.batch_system(ctx, n, nl, sd, mg.W2) for n, nl, sd in ((4, 6, 1), (6, 5, 2), (5, 9, 3))]
+    tols = [1e-7, 1e-9, 1e-10]
+    tot = sum(s.undf for s in systems)
+    ent = sum(s.entities for s in systems)
+    col = sum(s.columns for s in systems)
+
+    def run(idx):
+        B = lfx.Batch(ctx, 6, len(idx), sum(systems[i].undf for i in idx),
+                      sum(systems[i].entities for i in idx), sum(systems[i].columns for i in idx), 3)
+        xs = []
+        for i in idx:
+            s = systems[i]
+            x = lfx.FieldVector(ctx, [s.undf])
+            x.set_scalar(0.0)
+            xs.append((B.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x, tols[i], 5000), x))
+        for _ in range(3000):
+            if B.step() == len(idx):
+                break
+        out = []
+        for slot, x in xs:
+            ph, _, info = B.slot(slot)
+            assert ph == 3 and info.status == 0
+            out.append(x.export_field())
+        return out
+
+    assert tot and ent and col
+    mixed = run([0, 1, 2])
+    for i in range(3):
+        assert same(run([i])[0], mixed[i])
+        s = systems[i]
+        X = lfx.FieldVector.from_array(ctx, mixed[i])
+        R = lfx.FieldVector(ctx, [s.undf])
+        s.ops[lfx.R64].apply(X, R)
+        R.aypx(-1.0, s.b)
+        assert R.norm() / s.b.norm() <= tols[i] * 1.0001
+
+
 def test_batch_refuses_when_full(ctx):
     s = w0_system(ctx, 4, 3, 5)
     B = lfx.Batch(ctx, 8, 1, s["undf"], s["undf"], 0, 2)

@@ -260,7 +260,7 @@ int lfx_ctx_check_device_error(lfx_ctx* ctx);
  * reference, which solves one system per call). Each slot runs preconditioned
  * CG in FP32 with the solution accumulated in FP64 and reliable updates: the
  * true residual b - A x is recomputed with the FP64 operator whenever the
- * FP32 residual has dropped by 1e-2 since the last one, and a slot converges
+ * FP32 residual has dropped by 1e-3 since the last one, and a slot converges
  * only when ||b - A x|| / ||b - A x0|| <= tol. Every kernel covers all
  * admitted slots, and one CUDA graph replays `iters_per_launch`
  * super-iterations for the whole batch; a slot's result does not depend on
@@ -284,6 +284,47 @@ int lfx_batch_step(lfx_batch* b, int32_t* ndone);
 int lfx_batch_slot_info(const lfx_batch* b, int32_t slot, int32_t* phase, int64_t* tag,
                         lfx_solve_info* info);
 int lfx_batch_retire(lfx_batch* b, int32_t slot);
+
+/* ------------------------------------------------------------------ many right-hand sides
+ * One operator applied to, and solved for, nrhs right-hand sides at once (no
+ * counterpart in the reference, whose solvers take one field_vector_type).
+ * The per-cell product becomes an (nrhs x 8) by (8 x 8) small GEMM on the
+ * tensor cores, in TF32 or BF16 with FP32 accumulation. Operators with the
+ * lowest-order nodal (W0) dofmap only: ndf = 8, map_to == map_from, dofs 4..7
+ * one level above dofs 0..3. */
+typedef struct lfx_mrhs lfx_mrhs;
+enum { LFX_MRHS_TF32 = 1, LFX_MRHS_BF16 = 2 };
+/* From an FP64 (or FP32) LMA operator: its matrices rounded to `kind`, the
+ * cell columns split into patches of about cells_per_patch (0: 16). nrhs is
+ * 16, 32 or 64. */
+int lfx_mrhs_create(const lfx_op* op, int32_t kind, int32_t nrhs, int32_t cells_per_patch,
+                    lfx_mrhs** out);
+int lfx_mrhs_destroy(lfx_mrhs* m);
+/* patches, cell levels computed per apply (halo cells of two patches count
+ * twice), most vertex columns one patch owns, most colours in one patch, and
+ * the bytes of the rounded matrices */
+int lfx_mrhs_info(const lfx_mrhs* m, int32_t* npatch, int64_t* cell_levels, int32_t* max_owned,
+                  int32_t* max_colours, int64_t* matrix_bytes);
+/* y = A x for device arrays x, y of undf x nrhs FP32 values, dof-major
+ * (element (dof, rhs) at dof * nrhs + rhs); x and y must differ */
+int lfx_mrhs_apply(lfx_mrhs* m, const float* x, float* y);
+/* mean time of one apply over reps applies (after one untimed), microseconds */
+int lfx_mrhs_time_apply(lfx_mrhs* m, const float* x, float* y, int32_t reps, float* us);
+typedef struct {
+  double r_tol;      /* per right-hand side: ||b - A x|| <= r_tol ||b - A x0|| */
+  double inner_tol;  /* each inner FP32 solve reduces its residual by this */
+  int32_t max_outer; /* refinement steps, at most */
+  int32_t max_inner; /* iterations of one inner solve, at most */
+} lfx_mrhs_cfg;
+/* FP64 iterative refinement around an FP32 Jacobi-preconditioned CG run on
+ * all right-hand sides together (each with its own step lengths), with the
+ * tensor-core apply. op64: the FP64 operator (residuals); diag: its FP64
+ * diagonal (lfx_lma_diagonal). b, x: device arrays of nrhs FP64 vectors,
+ * right-hand side r at b + r * ld (x: initial guess in, solution out). info:
+ * nrhs entries; iterations = inner iterations of that right-hand side,
+ * outer_iterations = refinement steps it took part in. */
+int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double* b, double* x,
+                   int64_t ld, const lfx_mrhs_cfg* cfg, lfx_solve_info* info);
 
 /* ------------------------------------------------------------------ no allocation
  * Allocation-free inner product (no counterpart in the reference): for

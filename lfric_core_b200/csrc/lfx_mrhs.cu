@@ -1,0 +1,1003 @@
+// Many right-hand sides of one LMA operator at once, with the per-cell
+// products on the tensor cores.
+//
+// Vectors of nrhs (16, 32 or 64) right-hand sides are stored dof-major,
+// [undf][nrhs]. For one cell at one level the local product
+//   Y_loc (nrhs x 8) = X_loc (nrhs x 8) . M^T (8 x 8)
+// is a small GEMM: the right-hand sides are the rows of an mma.sync m16n8k8
+// (TF32, or BF16, with FP32 accumulation), the cell's eight local dofs its
+// columns, the local matrix its B operand. The operator must have the
+// lowest-order nodal (W0) structure: ndf = 8, dofs 0..3 on the bottom and
+// 4..7 on the top vertices, top = bottom + 1, so every dof lies on a vertex
+// column of nlayers + 1 dofs.
+//
+// Summation without atomics (deterministic): the cell columns are split into
+// compact patches (breadth-first over shared vertices), and every vertex
+// column is owned by one patch (the patch holding most of its cells). One
+// thread block per patch computes every cell column touching its owned
+// vertices -- a few cells next to the patch are computed by two blocks -- and
+// keeps the owned rows of a block of kLB levels in shared memory. A warp walks
+// one cell column up the levels of the block: the top-vertex results of level
+// k are carried in registers to the bottom rows of level k + 1, so each
+// (cell column, vertex, level) adds once into shared memory. Cells are taken
+// in colours (no two of a colour share an owned vertex) with a barrier
+// between colours, so every sum has a fixed order.
+//
+// The solve wraps an FP32 preconditioned CG over all right-hand sides (each
+// with its own step lengths; Jacobi preconditioner) in FP64 iterative
+// refinement: the residual b - A x and the solution stay FP64 (RHS-major, the
+// plain FP64 operator applies them), each inner solve reduces its residual by
+// the inner tolerance, and a right-hand side converges on its true FP64
+// residual ||b - A x|| / ||b - A x0||.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <queue>
+#include <unordered_map>
+#include <vector>
+
+#include "lfx_internal.cuh"
+
+using namespace lfx;
+
+namespace {
+
+constexpr int kLB = 4;      // levels per block of the apply
+constexpr int kMaxPC = 12;  // colours inside one patch, at most
+constexpr int kWarps = 4;   // warps per patch block
+constexpr int kDefaultPatch = 16;
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+// D = A B with A 16x8 (rows: right-hand sides), B 8x8, FP32 accumulate from 0
+__device__ __forceinline__ void mma_tf32(float* d, uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%10,%10,%10,%10};\n"
+      : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1), "f"(0.0f));
+}
+__device__ __forceinline__ void mma_bf16(float* d, uint32_t a01, uint32_t a23, uint32_t b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%7,%7,%7,%7};\n"
+      : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+      : "r"(a01), "r"(a23), "r"(b), "f"(0.0f));
+}
+
+// Local matrices in B-fragment order, one 32-lane record per cell level
+// (c2d * nl + k). Lane (g = lane / 4, t = lane % 4) holds M(g, t), M(g, t + 4)
+// as TF32 (float2), or M(g, 2t), M(g, 2t + 1) as packed BF16; M(df, df2) is
+// element (c * ndf + df) * blk + df2 * nl + k of the operator's matrices.
+template <class TM, bool BF>
+__global__ void mrhs_relayout(const TM* __restrict__ M, int64_t nc3, int nl, int blk, void* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc3 * 32) return;
+  const int lane = (int)(i & 31);
+  const int64_t c3 = i >> 5;
+  const int64_t c = c3 / nl;
+  const int k = (int)(c3 % nl);
+  const int g = lane >> 2, t = lane & 3;
+  auto at = [&](int df, int df2) {
+    return (float)M[(c * 8 + df) * (int64_t)blk + (int64_t)df2 * nl + k];
+  };
+  if (BF) {
+    reinterpret_cast<uint32_t*>(out)[i] = pack_bf16(at(g, 2 * t), at(g, 2 * t + 1));
+  } else {
+    float2 v;
+    v.x = __uint_as_float(to_tf32(at(g, t)));
+    v.y = __uint_as_float(to_tf32(at(g, t + 4)));
+    reinterpret_cast<float2*>(out)[i] = v;
+  }
+}
+
+struct MrhsArgs {
+  const int4* pinfo;     // [npatch] {owned offset, owned count, cell offset, colours}
+  const int* pcol;       // [npatch][kMaxPC + 1] first entry of each colour
+  const int* own_base;   // first dof of each owned vertex column
+  const int4* cells;     // per entry {c2d, xb0, xb1, xb2}, {xb3, owned slots, 0, 0}
+  const void* Mf;
+  int nl;
+};
+
+// One cell column over the levels [l0, l0 + nlb) of a block: MMAs per level,
+// vertical carry, adds into the owned rows ys[slot][level - l0][rhs].
+template <int RB, bool BF>
+__device__ __forceinline__ void mrhs_cell(const MrhsArgs& A, const float* __restrict__ X,
+                                          float* ys, int e, int l0, int nlb, int lane) {
+  constexpr int NR = 16 * RB, RS = NR + 4, SLAB = (kLB + 1) * RS;
+  const int g = lane >> 2, t = lane & 3;
+  const int4 ca = A.cells[2 * e], cb = A.cells[2 * e + 1];
+  const int nl = A.nl;
+  const int va = 2 * (t & 1);  // this lane's result columns: vertices va, va + 1
+  const unsigned sp = (unsigned)cb.y;
+  const unsigned sa = (sp >> (8 * va)) & 255u, sb = (sp >> (8 * va + 8)) & 255u;
+  const size_t mrec = ((size_t)ca.x * nl + l0) * 32 + lane;
+
+  // operands of all levels of the block, loaded before the first MMA
+  uint32_t xa[kLB + 1][RB][2];  // TF32: rows of vertex t; BF16: [kk][rb][rhs g / g+8]
+  uint32_t bm[kLB][2];
+  if (!BF) {
+    const int xbt = t == 0 ? ca.y : t == 1 ? ca.z : t == 2 ? ca.w : cb.x;
+    const float* xc = X + (size_t)(xbt + l0) * NR + g;
+#pragma unroll
+    for (int kk = 0; kk <= kLB; ++kk)
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) {
+        xa[kk][rb][0] = kk <= nlb ? to_tf32(__ldg(xc + kk * NR + rb * 16)) : 0u;
+        xa[kk][rb][1] = kk <= nlb ? to_tf32(__ldg(xc + kk * NR + rb * 16 + 8)) : 0u;
+      }
+    const float2* mc = reinterpret_cast<const float2*>(A.Mf) + mrec;
+#pragma unroll
+    for (int kk = 0; kk < kLB; ++kk) {
+      const float2 v = kk < nlb ? __ldg(mc + kk * 32) : make_float2(0.f, 0.f);
+      bm[kk][0] = __float_as_uint(v.x);
+      bm[kk][1] = __float_as_uint(v.y);
+    }
+  } else {
+    // A columns 2t, 2t + 1: vertices va, va + 1 at level offset t / 2
+    const int lo = t >> 1;
+    const int x0 = (t & 1) ? ca.w : ca.y, x1 = (t & 1) ? cb.x : ca.z;
+    const float* p0 = X + (size_t)(x0 + l0 + lo) * NR + g;
+    const float* p1 = X + (size_t)(x1 + l0 + lo) * NR + g;
+#pragma unroll
+    for (int kk = 0; kk < kLB; ++kk)
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) {
+        const int o = kk * NR + rb * 16;
+        xa[kk][rb][0] = kk < nlb ? pack_bf16(__ldg(p0 + o), __ldg(p1 + o)) : 0u;
+        xa[kk][rb][1] = kk < nlb ? pack_bf16(__ldg(p0 + o + 8), __ldg(p1 + o + 8)) : 0u;
+      }
+    const uint32_t* mc = reinterpret_cast<const uint32_t*>(A.Mf) + mrec;
+#pragma unroll
+    for (int kk = 0; kk < kLB; ++kk) bm[kk][0] = kk < nlb ? __ldg(mc + kk * 32) : 0u;
+  }
+
+  float carry[RB][4];
+#pragma unroll
+  for (int kk = 0; kk < kLB; ++kk) {
+    if (kk >= nlb) break;  // warp-uniform
+    float d[RB][4];
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+      if (!BF)
+        mma_tf32(d[rb], xa[kk][rb][0], xa[kk][rb][1], xa[kk + 1][rb][0], xa[kk + 1][rb][1],
+                 bm[kk][0], bm[kk][1]);
+      else
+        mma_bf16(d[rb], xa[kk][rb][0], xa[kk][rb][1], bm[kk][0]);
+    }
+    // lanes t < 2: bottom rows (level l0 + kk) of vertices va, va + 1, plus the
+    // carried top rows of the level below; lanes t >= 2: top rows
+    if (t < 2) {
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (kk > 0) d[rb][q] += carry[rb][q];
+      if (sa != 255u) {
+        float* r = ys + sa * SLAB + kk * RS + g;
+#pragma unroll
+        for (int rb = 0; rb < RB; ++rb) {
+          r[rb * 16] += d[rb][0];
+          r[rb * 16 + 8] += d[rb][2];
+        }
+      }
+      if (sb != 255u) {
+        float* r = ys + sb * SLAB + kk * RS + g;
+#pragma unroll
+        for (int rb = 0; rb < RB; ++rb) {
+          r[rb * 16] += d[rb][1];
+          r[rb * 16 + 8] += d[rb][3];
+        }
+      }
+    }
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) carry[rb][q] = __shfl_down_sync(0xffffffffu, d[rb][q], 2);
+    if (kk == nlb - 1 && t < 2) {
+      // top rows of the block's last level: row nlb, carried to the next block
+      if (sa != 255u) {
+        float* r = ys + sa * SLAB + (kk + 1) * RS + g;
+#pragma unroll
+        for (int rb = 0; rb < RB; ++rb) {
+          r[rb * 16] += carry[rb][0];
+          r[rb * 16 + 8] += carry[rb][2];
+        }
+      }
+      if (sb != 255u) {
+        float* r = ys + sb * SLAB + (kk + 1) * RS + g;
+#pragma unroll
+        for (int rb = 0; rb < RB; ++rb) {
+          r[rb * 16] += carry[rb][1];
+          r[rb * 16 + 8] += carry[rb][3];
+        }
+      }
+    }
+  }
+}
+
+template <int RB, bool BF>
+__global__ void __launch_bounds__(kWarps * 32) mrhs_apply_k(MrhsArgs A, const float* __restrict__ X,
+                                                          float* __restrict__ Y) {
+  constexpr int NR = 16 * RB, RS = NR + 4, SLAB = (kLB + 1) * RS, C4 = NR / 4;
+  extern __shared__ float4 ys4[];
+  float* ys = reinterpret_cast<float*>(ys4);
+  const int p = blockIdx.x;
+  const int4 pi = A.pinfo[p];
+  const int nown = pi.y, nl = A.nl;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int* pc = A.pcol + (size_t)p * (kMaxPC + 1);
+  for (int i = threadIdx.x; i < nown * SLAB; i += blockDim.x) ys[i] = 0.f;
+  for (int l0 = 0; l0 < nl; l0 += kLB) {
+    const int nlb = min(kLB, nl - l0);
+    for (int q = 0; q < pi.w; ++q) {
+      __syncthreads();  // zeroing / the previous colour's adds are done
+      const int e1 = pi.z + pc[q + 1];
+      for (int e = pi.z + pc[q] + warp; e < e1; e += kWarps)
+        mrhs_cell<RB, BF>(A, X, ys, e, l0, nlb, lane);
+    }
+    __syncthreads();
+    const bool last = l0 + nlb >= nl;
+    const int rows = nlb + (last ? 1 : 0);
+    for (int i = threadIdx.x; i < nown * rows * C4; i += blockDim.x) {
+      const int c4 = i % C4, rr = (i / C4) % rows, s = i / (C4 * rows);
+      const float4 v = *reinterpret_cast<const float4*>(ys + s * SLAB + rr * RS + 4 * c4);
+      *reinterpret_cast<float4*>(Y + (size_t)(A.own_base[pi.x + s] + l0 + rr) * NR + 4 * c4) = v;
+    }
+    if (last) break;
+    __syncthreads();
+    // row nlb (top of the block) becomes row 0 of the next block
+    for (int i = threadIdx.x; i < nown * RS; i += blockDim.x) {
+      float* b = ys + (i / RS) * SLAB + (i % RS);
+      b[0] = b[nlb * RS];
+      for (int r = 1; r <= kLB; ++r) b[r * RS] = 0.f;
+    }
+  }
+}
+
+// ------------------------------------------------ dof-major vector kernels
+
+// Sums acc over the rows of the block, then over all blocks in block order
+// (the last block to finish, by ticket), into tot[r * NR + col]. Returns true
+// in that last block, with tot complete.
+template <int NR, int NRED>
+__device__ bool mv_finish(const double (&acc)[NRED], double* partials, unsigned* ticket,
+                          double* tot) {
+  constexpr int RPB = 256 / NR;
+  __shared__ double sm[256];
+  __shared__ int am_last;
+  const int G = gridDim.x;
+#pragma unroll
+  for (int r = 0; r < NRED; ++r) {
+    sm[threadIdx.x] = acc[r];
+    __syncthreads();
+    if (threadIdx.x < NR) {
+      double s = 0.0;
+      for (int q = 0; q < RPB; ++q) s = s + sm[q * NR + threadIdx.x];
+      partials[((size_t)r * NR + threadIdx.x) * G + blockIdx.x] = s;
+    }
+    __syncthreads();
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) am_last = atomicAdd(ticket, 1u) == (unsigned)G - 1;
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int pr = w; pr < NRED * NR; pr += 8) {
+    double s = 0.0;
+    for (int b = lane; b < G; b += 32) s = s + __ldcg(partials + (size_t)pr * G + b);
+    s = warp_butterfly(s);
+    if (lane == 0) tot[pr] = s;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+  __syncthreads();
+  return true;
+}
+
+struct MvState {
+  double rz[64], alpha[64], beta[64], r0[64], rn[64];
+  int active[64], iters[64];
+  int nactive;
+};
+
+__device__ void count_active(MvState* S, int nr) {
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int c = 0; c < nr; ++c) n += S->active[c];
+    S->nactive = n;
+  }
+}
+
+// x = 0, p = z = D^-1 r; rz = <r, z>, r0 = ||r|| per right-hand side
+template <int NR>
+__global__ void __launch_bounds__(256) mv_init(int64_t n, const float* __restrict__ dinv,
+                                               const float* __restrict__ r, float* __restrict__ p,
+                                               float* __restrict__ x, const int* act_out,
+                                               MvState* S, double* partials, unsigned* ticket) {
+  constexpr int RPB = 256 / NR;
+  __shared__ double tot[2 * NR];
+  const int col = threadIdx.x % NR;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
+       row += (int64_t)gridDim.x * RPB) {
+    const size_t i = (size_t)row * NR + col;
+    const float ri = r[i];
+    const float zi = ri * dinv[row];
+    p[i] = zi;
+    x[i] = 0.f;
+    acc[0] = fma((double)ri, (double)ri, acc[0]);
+    acc[1] = fma((double)ri, (double)zi, acc[1]);
+  }
+  if (!mv_finish<NR, 2>(acc, partials, ticket, tot)) return;
+  if (threadIdx.x < NR) {
+    const int c = threadIdx.x;
+    const double r0 = sqrt(tot[c]);
+    S->r0[c] = r0;
+    S->rn[c] = r0;
+    S->rz[c] = tot[NR + c];
+    S->alpha[c] = 0.0;
+    S->beta[c] = 0.0;
+    S->active[c] = act_out[c] && r0 > 0.0 && tot[NR + c] > 0.0;
+  }
+  __syncthreads();
+  count_active(S, NR);
+}
+
+// alpha = rz / <p, q>
+template <int NR>
+__global__ void __launch_bounds__(256) mv_alpha(int64_t n, const float* __restrict__ p,
+                                                const float* __restrict__ q, MvState* S,
+                                                double* partials, unsigned* ticket) {
+  constexpr int RPB = 256 / NR;
+  __shared__ double tot[NR];
+  const int col = threadIdx.x % NR;
+  double acc[1] = {0.0};
+  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
+       row += (int64_t)gridDim.x * RPB) {
+    const size_t i = (size_t)row * NR + col;
+    acc[0] = fma((double)p[i], (double)q[i], acc[0]);
+  }
+  if (!mv_finish<NR, 1>(acc, partials, ticket, tot)) return;
+  if (threadIdx.x < NR) {
+    const int c = threadIdx.x;
+    S->alpha[c] = (S->active[c] && tot[c] != 0.0) ? S->rz[c] / tot[c] : 0.0;
+  }
+}
+
+// x += alpha p, r -= alpha q; ||r||, rz_new = <r, D^-1 r>; beta; inner
+// convergence ||r|| <= tol ||r0||
+template <int NR>
+__global__ void __launch_bounds__(256) mv_update(int64_t n, const float* __restrict__ dinv,
+                                                 const float* __restrict__ p,
+                                                 const float* __restrict__ q, float* __restrict__ x,
+                                                 float* __restrict__ r, double tol, MvState* S,
+                                                 double* partials, unsigned* ticket) {
+  constexpr int RPB = 256 / NR;
+  __shared__ double tot[2 * NR];
+  const int col = threadIdx.x % NR;
+  const float a = (float)S->alpha[col];
+  double acc[2] = {0.0, 0.0};
+  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
+       row += (int64_t)gridDim.x * RPB) {
+    const size_t i = (size_t)row * NR + col;
+    const float pi = p[i], qi = q[i], xi = x[i], ri0 = r[i], di = dinv[row];
+    x[i] = fmaf(a, pi, xi);
+    const float ri = fmaf(-a, qi, ri0);
+    r[i] = ri;
+    acc[0] = fma((double)ri, (double)ri, acc[0]);
+    acc[1] = fma((double)ri, (double)(ri * di), acc[1]);
+  }
+  if (!mv_finish<NR, 2>(acc, partials, ticket, tot)) return;
+  if (threadIdx.x < NR) {
+    const int c = threadIdx.x;
+    if (S->active[c]) {
+      const double rn = sqrt(tot[c]);
+      S->rn[c] = rn;
+      S->beta[c] = tot[NR + c] / S->rz[c];
+      S->rz[c] = tot[NR + c];
+      S->iters[c] += 1;
+      if (!(rn > tol * S->r0[c]) || !(tot[NR + c] > 0.0)) S->active[c] = 0;
+    } else {
+      S->beta[c] = 0.0;
+    }
+  }
+  __syncthreads();
+  count_active(S, NR);
+}
+
+// p = D^-1 r + beta p
+template <int NR>
+__global__ void __launch_bounds__(256) mv_direction(int64_t n, const float* __restrict__ dinv,
+                                                    const float* __restrict__ r,
+                                                    float* __restrict__ p, const MvState* S) {
+  constexpr int RPB = 256 / NR;
+  const int col = threadIdx.x % NR;
+  const float b = (float)S->beta[col];
+  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
+       row += (int64_t)gridDim.x * RPB) {
+    const size_t i = (size_t)row * NR + col;
+    p[i] = fmaf(b, p[i], r[i] * dinv[row]);
+  }
+}
+
+// r[row][col] = (float) R[col * ld + row] (RHS-major FP64 to dof-major FP32)
+template <int NR>
+__global__ void mv_from_rhs_major(int64_t n, const double* __restrict__ R, int64_t ld,
+                                  float* __restrict__ r) {
+  constexpr int TW = NR < 32 ? NR : 32;
+  __shared__ float tile[TW][33];
+  const int64_t row0 = (int64_t)blockIdx.x * 32;
+  const int col0 = blockIdx.y * TW;
+  for (int j = threadIdx.y; j < TW; j += blockDim.y) {
+    const int64_t row = row0 + threadIdx.x;
+    if (row < n) tile[j][threadIdx.x] = (float)R[(size_t)(col0 + j) * ld + row];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int64_t row = row0 + j;
+    if (row < n && threadIdx.x < TW) r[(size_t)row * NR + col0 + threadIdx.x] = tile[threadIdx.x][j];
+  }
+}
+
+// X[col * ld + row] += x[row][col]
+template <int NR>
+__global__ void mv_add_to_rhs_major(int64_t n, const float* __restrict__ x, double* __restrict__ X,
+                                    int64_t ld) {
+  constexpr int TW = NR < 32 ? NR : 32;
+  __shared__ float tile[TW][33];
+  const int64_t row0 = (int64_t)blockIdx.x * 32;
+  const int col0 = blockIdx.y * TW;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int64_t row = row0 + j;
+    if (row < n && threadIdx.x < TW) tile[threadIdx.x][j] = x[(size_t)row * NR + col0 + threadIdx.x];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < TW; j += blockDim.y) {
+    const int64_t row = row0 + threadIdx.x;
+    if (row < n) X[(size_t)(col0 + j) * ld + row] += (double)tile[j][threadIdx.x];
+  }
+}
+
+__global__ void k_dinv(int64_t n, const double* __restrict__ d, float* __restrict__ dinv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dinv[i] = (float)(1.0 / d[i]);
+}
+
+}  // namespace
+
+struct lfx_mrhs {
+  lfx_ctx* ctx = nullptr;
+  int32_t kind = LFX_MRHS_TF32, nrhs = 64, nl = 0, ncell_2d = 0;
+  int64_t undf = 0;
+  int32_t npatch = 0, own_max = 0, max_colours = 0;
+  int64_t nent = 0;
+  int4* pinfo = nullptr;
+  int* pcol = nullptr;
+  int* own_base = nullptr;
+  int4* cells = nullptr;
+  void* Mf = nullptr;
+  size_t Mf_bytes = 0;
+  size_t smem = 0;
+  size_t pinfo_b = 0, pcol_b = 0, own_b = 0, cells_b = 0;
+  // solve work space, allocated by the first solve
+  float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *dinv = nullptr;
+  double* R64 = nullptr;
+  double* nrm = nullptr;      // [nrhs] device
+  double* h_nrm = nullptr;    // [nrhs] pinned
+  int* d_act = nullptr;       // [nrhs]
+  MvState* S = nullptr;
+  MvState* h_S = nullptr;     // pinned
+  double* partials = nullptr;
+  unsigned* ticket = nullptr;
+  int grid = 0;
+  size_t work_bytes = 0;
+};
+
+namespace {
+
+int mrhs_launch(lfx_mrhs* m, const float* x, float* y) {
+  lfx_ctx* ctx = m->ctx;
+  MrhsArgs A{m->pinfo, m->pcol, m->own_base, m->cells, m->Mf, m->nl};
+  const bool bf = m->kind == LFX_MRHS_BF16;
+  const dim3 grid(m->npatch), block(kWarps * 32);
+#define LFX_MRHS_CASE(RB)                                                                  \
+  if (bf)                                                                                  \
+    mrhs_apply_k<RB, true><<<grid, block, m->smem, ctx->stream>>>(A, x, y);                \
+  else                                                                                     \
+    mrhs_apply_k<RB, false><<<grid, block, m->smem, ctx->stream>>>(A, x, y);
+  switch (m->nrhs) {
+    case 16: LFX_MRHS_CASE(1) break;
+    case 32: LFX_MRHS_CASE(2) break;
+    default: LFX_MRHS_CASE(4) break;
+  }
+#undef LFX_MRHS_CASE
+  ctx->launches++;
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
+template <int RB>
+int set_smem_attr(size_t smem) {
+  if (cudaFuncSetAttribute(mrhs_apply_k<RB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 1;
+  if (cudaFuncSetAttribute(mrhs_apply_k<RB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 1;
+  return 0;
+}
+
+void mrhs_free(lfx_mrhs* m) {
+  lfx_ctx* ctx = m->ctx;
+  dfree(ctx, m->pinfo, m->pinfo_b);
+  dfree(ctx, m->pcol, m->pcol_b);
+  dfree(ctx, m->own_base, m->own_b);
+  dfree(ctx, m->cells, m->cells_b);
+  dfree(ctx, m->Mf, m->Mf_bytes);
+  const size_t v32 = (size_t)m->undf * m->nrhs * 4;
+  dfree(ctx, m->x32, v32);
+  dfree(ctx, m->r32, v32);
+  dfree(ctx, m->p32, v32);
+  dfree(ctx, m->q32, v32);
+  dfree(ctx, m->dinv, (size_t)m->undf * 4);
+  dfree(ctx, m->R64, (size_t)m->undf * m->nrhs * 8);
+  dfree(ctx, m->nrm, sizeof(double) * 64);
+  dfree(ctx, m->d_act, sizeof(int) * 64);
+  dfree(ctx, m->S, sizeof(MvState));
+  dfree(ctx, m->partials, sizeof(double) * 2 * 64 * m->grid);
+  dfree(ctx, m->ticket, sizeof(unsigned));
+  if (m->h_nrm) cudaFreeHost(m->h_nrm);
+  if (m->h_S) cudaFreeHost(m->h_S);
+}
+
+}  // namespace
+
+int lfx_mrhs_create(const lfx_op* op, int32_t kind, int32_t nrhs, int32_t cells_per_patch,
+                    lfx_mrhs** out) {
+  if (!op || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  lfx_ctx* ctx = op->ctx;
+  const lfx_lma_layout* L = op->lay;
+  if (kind != LFX_MRHS_TF32 && kind != LFX_MRHS_BF16)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "kind must be LFX_MRHS_TF32 or LFX_MRHS_BF16");
+  if (nrhs != 16 && nrhs != 32 && nrhs != 64)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "nrhs must be 16, 32 or 64");
+  if (cells_per_patch < 0 || cells_per_patch > 256)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "cells_per_patch must be in [0, 256]");
+  const int P = cells_per_patch ? cells_per_patch : kDefaultPatch;
+  if (L->ndf_to != 8 || L->ndf_from != 8 || L->undf_to != L->undf_from)
+    return fail(ctx, LFX_NOT_SUPPORTED, "multi-RHS apply needs a square ndf = 8 (W0) operator");
+  const int nc = L->ncell_2d, nl = L->nlayers;
+  std::vector<int32_t> mt((size_t)nc * 8), mf((size_t)nc * 8);
+  LFX_CK(ctx, cudaMemcpy(mt.data(), L->map_to, mt.size() * 4, cudaMemcpyDeviceToHost));
+  LFX_CK(ctx, cudaMemcpy(mf.data(), L->map_from, mf.size() * 4, cudaMemcpyDeviceToHost));
+  if (mt != mf) return fail(ctx, LFX_NOT_SUPPORTED, "multi-RHS apply needs map_to == map_from");
+  // vertex columns
+  std::unordered_map<int32_t, int32_t> vid;
+  std::vector<int32_t> vbase;
+  std::vector<int32_t> cv((size_t)nc * 4);
+  for (int c = 0; c < nc; ++c)
+    for (int v = 0; v < 4; ++v) {
+      const int32_t b = mt[(size_t)c * 8 + v];
+      if (mt[(size_t)c * 8 + 4 + v] != b + 1)
+        return fail(ctx, LFX_NOT_SUPPORTED,
+                    "multi-RHS apply needs W0 dofs: top vertex dof = bottom dof + 1");
+      if (b < 0 || (int64_t)b + nl >= L->undf_to)
+        return fail(ctx, LFX_INVALID_ARGUMENT, "dofmap entry out of range");
+      auto it = vid.find(b);
+      int id;
+      if (it == vid.end()) {
+        id = (int)vbase.size();
+        vid.emplace(b, id);
+        vbase.push_back(b);
+      } else {
+        id = it->second;
+      }
+      cv[(size_t)c * 4 + v] = id;
+    }
+  const int nv = (int)vbase.size();
+  if ((int64_t)nv * (nl + 1) != L->undf_to)
+    return fail(ctx, LFX_NOT_SUPPORTED, "multi-RHS apply needs every dof on a vertex column");
+  std::vector<int32_t> voff(nv + 1, 0), vcells;
+  for (int c = 0; c < nc; ++c)
+    for (int v = 0; v < 4; ++v) voff[cv[(size_t)c * 4 + v] + 1]++;
+  for (int i = 0; i < nv; ++i) voff[i + 1] += voff[i];
+  vcells.resize(voff[nv]);
+  {
+    std::vector<int32_t> fill(voff.begin(), voff.end() - 1);
+    for (int c = 0; c < nc; ++c)
+      for (int v = 0; v < 4; ++v) vcells[fill[cv[(size_t)c * 4 + v]]++] = c;
+  }
+  // compact patches: breadth-first over cells sharing a vertex
+  std::vector<int32_t> patch(nc, -1);
+  int npatch = 0;
+  {
+    std::vector<int32_t> queue;
+    for (int s = 0; s < nc; ++s) {
+      if (patch[s] >= 0) continue;
+      queue.clear();
+      queue.push_back(s);
+      patch[s] = npatch;
+      int taken = 1;
+      for (size_t h = 0; h < queue.size() && taken < P; ++h) {
+        const int c = queue[h];
+        for (int v = 0; v < 4 && taken < P; ++v) {
+          const int id = cv[(size_t)c * 4 + v];
+          for (int k = voff[id]; k < voff[id + 1] && taken < P; ++k) {
+            const int n2 = vcells[k];
+            if (patch[n2] < 0) {
+              patch[n2] = npatch;
+              queue.push_back(n2);
+              ++taken;
+            }
+          }
+        }
+      }
+      ++npatch;
+    }
+  }
+  // owner of a vertex column: the patch holding most of its cells (ties: the
+  // patch of its lowest cell)
+  std::vector<int32_t> owner(nv);
+  for (int i = 0; i < nv; ++i) {
+    int best = -1, bestn = 0;
+    for (int k = voff[i]; k < voff[i + 1]; ++k) {
+      const int pk = patch[vcells[k]];
+      int n = 0;
+      for (int k2 = voff[i]; k2 < voff[i + 1]; ++k2) n += patch[vcells[k2]] == pk;
+      if (n > bestn || (n == bestn && pk < best)) {
+        best = pk;
+        bestn = n;
+      }
+    }
+    owner[i] = best;
+  }
+  std::vector<std::vector<int32_t>> pown(npatch);
+  for (int i = 0; i < nv; ++i) pown[owner[i]].push_back(i);
+  std::vector<int4> h_pinfo(npatch);
+  std::vector<int> h_pcol((size_t)npatch * (kMaxPC + 1), 0);
+  std::vector<int> h_own;
+  std::vector<int4> h_cells;
+  int own_max = 0, max_col = 0;
+  std::vector<int32_t> slot_of(nv, -1);
+  for (int p = 0; p < npatch; ++p) {
+    const auto& ov = pown[p];
+    if (ov.size() > 254) return fail(ctx, LFX_NOT_SUPPORTED, "patch owns too many vertex columns");
+    for (size_t s = 0; s < ov.size(); ++s) slot_of[ov[s]] = (int)s;
+    std::vector<int32_t> need;
+    for (int id : ov)
+      for (int k = voff[id]; k < voff[id + 1]; ++k) need.push_back(vcells[k]);
+    std::sort(need.begin(), need.end());
+    need.erase(std::unique(need.begin(), need.end()), need.end());
+    // greedy colours: cells sharing an owned vertex differ
+    std::vector<uint32_t> used(ov.size(), 0u);
+    std::vector<int> colour(need.size());
+    int ncol = 0;
+    for (size_t i = 0; i < need.size(); ++i) {
+      uint32_t forbid = 0u;
+      for (int v = 0; v < 4; ++v) {
+        const int s = slot_of[cv[(size_t)need[i] * 4 + v]];
+        if (s >= 0) forbid |= used[s];
+      }
+      int col = 0;
+      while (forbid & (1u << col)) ++col;
+      if (col >= kMaxPC) return fail(ctx, LFX_NOT_SUPPORTED, "patch needs too many colours");
+      colour[i] = col;
+      ncol = std::max(ncol, col + 1);
+      for (int v = 0; v < 4; ++v) {
+        const int s = slot_of[cv[(size_t)need[i] * 4 + v]];
+        if (s >= 0) used[s] |= 1u << col;
+      }
+    }
+    h_pinfo[p] = make_int4((int)h_own.size(), (int)ov.size(), (int)(h_cells.size() / 2), ncol);
+    int* pc = h_pcol.data() + (size_t)p * (kMaxPC + 1);
+    int n = 0;
+    for (int col = 0; col < ncol; ++col) {
+      pc[col] = n;
+      for (size_t i = 0; i < need.size(); ++i) {
+        if (colour[i] != col) continue;
+        const int c = need[i];
+        unsigned sp = 0u;
+        for (int v = 0; v < 4; ++v) {
+          const int s = slot_of[cv[(size_t)c * 4 + v]];
+          sp |= (unsigned)(s >= 0 ? s : 255) << (8 * v);
+        }
+        const int32_t* mc = mt.data() + (size_t)c * 8;
+        h_cells.push_back(make_int4(c, mc[0], mc[1], mc[2]));
+        h_cells.push_back(make_int4(mc[3], (int)sp, 0, 0));
+        ++n;
+      }
+    }
+    pc[ncol] = n;
+    for (int id : ov) h_own.push_back(vbase[id]);
+    for (int id : ov) slot_of[id] = -1;
+    own_max = std::max(own_max, (int)ov.size());
+    max_col = std::max(max_col, ncol);
+  }
+
+  auto* m = new lfx_mrhs();
+  m->ctx = ctx;
+  m->kind = kind;
+  m->nrhs = nrhs;
+  m->nl = nl;
+  m->ncell_2d = nc;
+  m->undf = L->undf_to;
+  m->npatch = npatch;
+  m->own_max = own_max;
+  m->max_colours = max_col;
+  m->nent = (int64_t)h_cells.size() / 2;
+  const int RS = nrhs + 4;
+  m->smem = (size_t)own_max * (kLB + 1) * RS * sizeof(float);
+  int rc = LFX_OK;
+  if (m->smem > 227 * 1024) rc = fail(ctx, LFX_NOT_SUPPORTED, "patch too large for shared memory");
+  if (!rc && m->smem > 48 * 1024) {
+    const int bad = nrhs == 16 ? set_smem_attr<1>(m->smem)
+                    : nrhs == 32 ? set_smem_attr<2>(m->smem)
+                                 : set_smem_attr<4>(m->smem);
+    if (bad) rc = fail(ctx, LFX_CUDA_ERROR, "cannot set the apply's shared memory size");
+  }
+  auto up = [&](void** dst, size_t* held, const void* src, size_t bytes) {
+    if (rc) return;
+    rc = dmalloc(ctx, dst, bytes);
+    if (!rc) *held = bytes;
+    if (!rc && cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = fail(ctx, LFX_CUDA_ERROR, "upload of the patch tables failed");
+  };
+  up((void**)&m->pinfo, &m->pinfo_b, h_pinfo.data(), h_pinfo.size() * sizeof(int4));
+  up((void**)&m->pcol, &m->pcol_b, h_pcol.data(), h_pcol.size() * sizeof(int));
+  up((void**)&m->own_base, &m->own_b, h_own.data(), h_own.size() * sizeof(int));
+  up((void**)&m->cells, &m->cells_b, h_cells.data(), h_cells.size() * sizeof(int4));
+  const int64_t nc3 = (int64_t)nc * nl;
+  m->Mf_bytes = (size_t)nc3 * 32 * (kind == LFX_MRHS_BF16 ? 4 : 8);
+  if (!rc) rc = dmalloc(ctx, &m->Mf, m->Mf_bytes);
+  if (!rc) {
+    const int64_t nthr = nc3 * 32;
+    const int blocks = (int)((nthr + 255) / 256);
+    const bool bf = kind == LFX_MRHS_BF16;
+    if (op->precision == LFX_R64) {
+      if (bf)
+        mrhs_relayout<double, true><<<blocks, 256, 0, ctx->stream>>>((const double*)op->mat, nc3, nl, op->blk, m->Mf);
+      else
+        mrhs_relayout<double, false><<<blocks, 256, 0, ctx->stream>>>((const double*)op->mat, nc3, nl, op->blk, m->Mf);
+    } else {
+      if (bf)
+        mrhs_relayout<float, true><<<blocks, 256, 0, ctx->stream>>>((const float*)op->mat, nc3, nl, op->blk, m->Mf);
+      else
+        mrhs_relayout<float, false><<<blocks, 256, 0, ctx->stream>>>((const float*)op->mat, nc3, nl, op->blk, m->Mf);
+    }
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+      rc = fail(ctx, LFX_CUDA_ERROR, "matrix relayout failed");
+  }
+  if (rc) {
+    mrhs_free(m);
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return LFX_OK;
+}
+
+int lfx_mrhs_destroy(lfx_mrhs* m) {
+  if (!m) return LFX_OK;
+  mrhs_free(m);
+  delete m;
+  return LFX_OK;
+}
+
+int lfx_mrhs_info(const lfx_mrhs* m, int32_t* npatch, int64_t* cell_entries, int32_t* max_owned,
+                  int32_t* max_colours, int64_t* matrix_bytes) {
+  if (!m) return LFX_INVALID_ARGUMENT;
+  if (npatch) *npatch = m->npatch;
+  if (cell_entries) *cell_entries = m->nent * m->nl;
+  if (max_owned) *max_owned = m->own_max;
+  if (max_colours) *max_colours = m->max_colours;
+  if (matrix_bytes) *matrix_bytes = (int64_t)m->Mf_bytes;
+  return LFX_OK;
+}
+
+int lfx_mrhs_apply(lfx_mrhs* m, const float* x, float* y) {
+  if (!m || !x || !y || x == y) return LFX_INVALID_ARGUMENT;
+  return mrhs_launch(m, x, y);
+}
+
+int lfx_mrhs_time_apply(lfx_mrhs* m, const float* x, float* y, int32_t reps, float* us) {
+  if (!m || !x || !y || x == y || reps < 1 || !us) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = m->ctx;
+  int rc = mrhs_launch(m, x, y);  // warm
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  LFX_CK(ctx, cudaEventCreate(&e0));
+  LFX_CK(ctx, cudaEventCreate(&e1));
+  cudaEventRecord(e0, ctx->stream);
+  for (int r = 0; r < reps && !rc; ++r) rc = mrhs_launch(m, x, y);
+  cudaEventRecord(e1, ctx->stream);
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && !rc)
+    rc = fail(ctx, LFX_CUDA_ERROR, "multi-RHS apply timing failed");
+  float ms = 0.f;
+  if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+  *us = 1e3f * ms / reps;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+namespace {
+
+int ensure_work(lfx_mrhs* m) {
+  if (m->x32) return LFX_OK;
+  lfx_ctx* ctx = m->ctx;
+  const size_t v32 = (size_t)m->undf * m->nrhs * 4;
+  m->grid = ctx->num_sms * 4;
+  int rc = dmalloc(ctx, (void**)&m->x32, v32);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->r32, v32);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->p32, v32);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->q32, v32);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->dinv, (size_t)m->undf * 4);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->R64, (size_t)m->undf * m->nrhs * 8);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->nrm, sizeof(double) * 64);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->d_act, sizeof(int) * 64);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->S, sizeof(MvState));
+  if (!rc) rc = dmalloc(ctx, (void**)&m->partials, sizeof(double) * 2 * 64 * m->grid);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->ticket, sizeof(unsigned));
+  if (!rc && cudaMallocHost(&m->h_nrm, sizeof(double) * 64) != cudaSuccess)
+    rc = fail(ctx, LFX_OUT_OF_MEMORY, "pinned allocation failed");
+  if (!rc && cudaMallocHost(&m->h_S, sizeof(MvState)) != cudaSuccess)
+    rc = fail(ctx, LFX_OUT_OF_MEMORY, "pinned allocation failed");
+  if (!rc) LFX_CK(ctx, cudaMemsetAsync(m->ticket, 0, sizeof(unsigned), ctx->stream));
+  if (!rc) LFX_CK(ctx, cudaMemsetAsync(m->S, 0, sizeof(MvState), ctx->stream));
+  return rc;
+}
+
+// R = B - A64 X per right-hand side, and ||R|| into m->h_nrm
+int outer_residual(lfx_mrhs* m, lfx_op* op64, const double* b, double* x, int64_t ld) {
+  lfx_ctx* ctx = m->ctx;
+  const int64_t n = m->undf;
+  for (int r = 0; r < m->nrhs; ++r) {
+    int rc = op_apply_impl(op64, x + (size_t)r * ld, m->R64 + (size_t)r * n, b + (size_t)r * ld,
+                           nullptr);
+    if (rc) return rc;
+    const double* R = m->R64 + (size_t)r * n;
+    double* out = m->nrm + r;
+    rc = launch_chunks<1>(
+        ctx, n, [=] __device__(int64_t i) { return V1<double>{R[i]}; },
+        [=] __device__(int64_t, const V1<double>& v, double* acc) {
+          acc[0] = fma(v.a, v.a, acc[0]);
+        },
+        [=] __device__(const double* tot) { *out = sqrt(tot[0]); });
+    if (rc) return rc;
+  }
+  LFX_CK(ctx, cudaMemcpyAsync(m->h_nrm, m->nrm, sizeof(double) * m->nrhs, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return LFX_OK;
+}
+
+template <int NR>
+int inner_solve(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner_its) {
+  lfx_ctx* ctx = m->ctx;
+  const int64_t n = m->undf;
+  const int G = m->grid;
+  const dim3 tb(32, 8), tg((unsigned)((n + 31) / 32), NR < 32 ? 1 : NR / 32);
+  mv_from_rhs_major<NR><<<tg, tb, 0, ctx->stream>>>(n, m->R64, n, m->r32);
+  LFX_CK(ctx, cudaMemcpyAsync(m->d_act, act, sizeof(int) * NR, cudaMemcpyHostToDevice, ctx->stream));
+  mv_init<NR><<<G, 256, 0, ctx->stream>>>(n, m->dinv, m->r32, m->p32, m->x32, m->d_act, m->S,
+                                          m->partials, m->ticket);
+  ctx->launches += 2;
+  LFX_CK(ctx, cudaGetLastError());
+  int it = 0;
+  constexpr int kCheck = 8;
+  while (it < max_inner) {
+    const int nb = std::min(kCheck, max_inner - it);
+    for (int s = 0; s < nb; ++s) {
+      int rc = mrhs_launch(m, m->p32, m->q32);
+      if (rc) return rc;
+      mv_alpha<NR><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->S, m->partials, m->ticket);
+      mv_update<NR><<<G, 256, 0, ctx->stream>>>(n, m->dinv, m->p32, m->q32, m->x32, m->r32, tol,
+                                                m->S, m->partials, m->ticket);
+      mv_direction<NR><<<G, 256, 0, ctx->stream>>>(n, m->dinv, m->r32, m->p32, m->S);
+      ctx->launches += 3;
+    }
+    LFX_CK(ctx, cudaGetLastError());
+    it += nb;
+    LFX_CK(ctx, cudaMemcpyAsync(&m->h_S->nactive, &m->S->nactive, sizeof(int),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (m->h_S->nactive == 0) break;
+  }
+  *inner_its = it;
+  return LFX_OK;
+}
+
+template <int NR>
+int add_correction(lfx_mrhs* m, double* x, int64_t ld) {
+  lfx_ctx* ctx = m->ctx;
+  const int64_t n = m->undf;
+  const dim3 tb(32, 8), tg((unsigned)((n + 31) / 32), NR < 32 ? 1 : NR / 32);
+  mv_add_to_rhs_major<NR><<<tg, tb, 0, ctx->stream>>>(n, m->x32, x, ld);
+  ctx->launches++;
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
+}  // namespace
+
+int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double* b, double* x,
+                   int64_t ld, const lfx_mrhs_cfg* cfg, lfx_solve_info* info) {
+  if (!m || !op64 || !diag || !b || !x || !cfg || !info) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = m->ctx;
+  if (op64->precision != LFX_R64 || op64->lay->undf_to != m->undf || op64->lay->undf_from != m->undf)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "op64 must be the FP64 operator of the same space");
+  if (diag->precision != LFX_R64 || diag->data.size() != 1 || diag->undf[0] != m->undf)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "diag must be one FP64 field of undf values");
+  if (ld < m->undf) return fail(ctx, LFX_INVALID_ARGUMENT, "ld must be at least undf");
+  if (!(cfg->r_tol > 0.0) || !(cfg->inner_tol > 0.0) || !(cfg->inner_tol < 1.0) ||
+      cfg->max_outer < 1 || cfg->max_inner < 1)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "bad tolerances or iteration limits");
+  int rc = ensure_work(m);
+  if (rc) return rc;
+  const int nr = m->nrhs;
+  const int64_t n = m->undf;
+  k_dinv<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, (const double*)diag->data[0],
+                                                                m->dinv);
+  LFX_CK(ctx, cudaGetLastError());
+  LFX_CK(ctx, cudaMemsetAsync(m->S, 0, sizeof(MvState), ctx->stream));
+  std::vector<double> r0(nr), rn(nr);
+  std::vector<int> act(64, 0), outer_n(nr, 0);
+  rc = outer_residual(m, op64, b, x, ld);
+  if (rc) return rc;
+  for (int r = 0; r < nr; ++r) r0[r] = rn[r] = m->h_nrm[r];
+  int outer = 0, inner_total = 0;
+  for (;;) {
+    int nact = 0;
+    for (int r = 0; r < nr; ++r) {
+      const bool conv = r0[r] == 0.0 || rn[r] <= cfg->r_tol * r0[r];
+      act[r] = !conv && std::isfinite(rn[r]);
+      nact += act[r];
+    }
+    if (nact == 0 || outer >= cfg->max_outer) break;
+    int its = 0;
+    rc = nr == 16 ? inner_solve<16>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its)
+         : nr == 32 ? inner_solve<32>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its)
+                    : inner_solve<64>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its);
+    if (!rc) rc = nr == 16 ? add_correction<16>(m, x, ld)
+                  : nr == 32 ? add_correction<32>(m, x, ld)
+                             : add_correction<64>(m, x, ld);
+    if (rc) return rc;
+    inner_total += its;
+    for (int r = 0; r < nr; ++r) outer_n[r] += act[r];
+    ++outer;
+    rc = outer_residual(m, op64, b, x, ld);
+    if (rc) return rc;
+    for (int r = 0; r < nr; ++r) rn[r] = m->h_nrm[r];
+  }
+  LFX_CK(ctx, cudaMemcpyAsync(m->h_S, m->S, sizeof(MvState), cudaMemcpyDeviceToHost, ctx->stream));
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  rc = lfx_ctx_check_device_error(ctx);
+  for (int r = 0; r < nr; ++r) {
+    lfx_solve_info& I = info[r];
+    memset(&I, 0, sizeof I);
+    I.initial_norm = r0[r];
+    I.final_norm = rn[r];
+    I.final_rel = r0[r] > 0.0 ? rn[r] / r0[r] : 0.0;
+    I.converged = r0[r] == 0.0 || rn[r] <= cfg->r_tol * r0[r];
+    I.outer_iterations = outer_n[r];
+    I.inner_iterations = m->h_S->iters[r];
+    I.iterations = m->h_S->iters[r];
+    I.applies = inner_total;
+    I.status = I.converged ? LFX_OK : (std::isfinite(rn[r]) ? LFX_NOT_CONVERGED : LFX_NAN_DETECTED);
+  }
+  return rc;
+}

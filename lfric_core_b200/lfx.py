@@ -59,6 +59,14 @@ class SolveInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class MrhsCfg(C.Structure):
+    _fields_ = [("r_tol", C.c_double), ("inner_tol", C.c_double), ("max_outer", C.c_int32),
+                ("max_inner", C.c_int32)]
+
+
+MRHS_TF32, MRHS_BF16 = 1, 2
+
+
 # (name, argtypes, restype)
 _SIGS = [
     ("lfx_ctx_create", [C.c_int, C.POINTER(vp)], C.c_int),
@@ -135,6 +143,14 @@ _SIGS = [
     ("lfx_batch_slot_info", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                              C.POINTER(SolveInfo)], C.c_int),
     ("lfx_batch_retire", [vp, C.c_int32], C.c_int),
+    ("lfx_mrhs_create", [vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(vp)], C.c_int),
+    ("lfx_mrhs_destroy", [vp], C.c_int),
+    ("lfx_mrhs_info", [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                       C.POINTER(C.c_int32), C.POINTER(C.c_int64)], C.c_int),
+    ("lfx_mrhs_apply", [vp, vp, vp], C.c_int),
+    ("lfx_mrhs_time_apply", [vp, vp, vp, C.c_int32, C.POINTER(C.c_float)], C.c_int),
+    ("lfx_mrhs_solve", [vp, vp, vp, vp, vp, C.c_int64, C.POINTER(MrhsCfg), C.POINTER(SolveInfo)],
+     C.c_int),
     ("lfx_dot_noalloc", [vp, vp, C.c_int64, vp, vp], C.c_int),
     ("lfx_dot_noalloc_max_n", [], C.c_int64),
     ("lfx_noalloc_last_error", [], C.c_char_p),
@@ -408,6 +424,51 @@ def fem_operators(ctx, mesh, space, coef, precisions=(R64, R32)):
         if op is not first and first is not None:
             op._parent = first
     return ops, m, undf
+
+
+class MultiRhsOperator(_Handle):
+    """One LMA operator applied to nrhs right-hand sides at once, the per-cell
+    products on the tensor cores (lfx_mrhs). Vectors are device arrays of
+    undf x nrhs FP32 values, dof-major, passed as device pointers (ints)."""
+
+    _destroy = "lfx_mrhs_destroy"
+
+    def __init__(self, op: "LmaOperator", kind: int = MRHS_TF32, nrhs: int = 64,
+                 cells_per_patch: int = 0):
+        self.ctx = op.ctx
+        self.op = op
+        self.kind = kind
+        self.nrhs = nrhs
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_mrhs_create(op.h, kind, nrhs, cells_per_patch, C.byref(h)))
+        self.h = h
+
+    def info(self) -> dict:
+        npatch, mo, mc = C.c_int32(), C.c_int32(), C.c_int32()
+        cl, mb = C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.L.lfx_mrhs_info(self.h, C.byref(npatch), C.byref(cl), C.byref(mo),
+                                                C.byref(mc), C.byref(mb)))
+        return {"patches": npatch.value, "cell_levels": cl.value, "max_owned": mo.value,
+                "max_colours": mc.value, "matrix_bytes": mb.value}
+
+    def apply(self, x_ptr: int, y_ptr: int):
+        self.ctx.check(self.ctx.L.lfx_mrhs_apply(self.h, x_ptr, y_ptr))
+
+    def time_apply(self, x_ptr: int, y_ptr: int, reps: int = 20) -> float:
+        us = C.c_float()
+        self.ctx.check(self.ctx.L.lfx_mrhs_time_apply(self.h, x_ptr, y_ptr, reps, C.byref(us)))
+        return us.value
+
+    def solve(self, op64: "LmaOperator", diag: "FieldVector", b_ptr: int, x_ptr: int, ld: int,
+              r_tol=1e-8, inner_tol=1e-2, max_outer=20, max_inner=5000):
+        """FP64 refinement around the FP32 tensor-core CG for all right-hand
+        sides; b, x: device FP64 arrays, right-hand side r at offset r * ld.
+        Returns one SolveInfo per right-hand side."""
+        cfg = MrhsCfg(r_tol, inner_tol, max_outer, max_inner)
+        info = (SolveInfo * self.nrhs)()
+        self.ctx.check(self.ctx.L.lfx_mrhs_solve(self.h, op64.h, diag.h, b_ptr, x_ptr, ld,
+                                                 C.byref(cfg), info))
+        return list(info)
 
 
 class Batch(_Handle):

@@ -310,6 +310,10 @@ int lfx_mrhs_info(const lfx_mrhs* m, int32_t* npatch, int64_t* cell_levels, int3
 int lfx_mrhs_apply(lfx_mrhs* m, const float* x, float* y);
 /* mean time of one apply over reps applies (after one untimed), microseconds */
 int lfx_mrhs_time_apply(lfx_mrhs* m, const float* x, float* y, int32_t reps, float* us);
+/* apply autotuner: times 2, 4 and 8 levels per shared-memory block (those
+ * that fit) over reps applies and keeps the fastest; outputs (nullable) the
+ * choice and its time per apply in microseconds */
+int lfx_mrhs_autotune(lfx_mrhs* m, int32_t reps, int32_t* levels_per_block, float* us);
 typedef struct {
   double r_tol;      /* per right-hand side: ||b - A x|| <= r_tol ||b - A x0|| */
   double inner_tol;  /* each inner FP32 solve reduces its residual by this */

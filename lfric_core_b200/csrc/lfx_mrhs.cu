@@ -16,11 +16,13 @@
 // column is owned by one patch (the patch holding most of its cells). One
 // thread block per patch computes every cell column touching its owned
 // vertices -- a few cells next to the patch are computed by two blocks -- and
-// keeps the owned rows of a block of kLB levels in shared memory. A warp walks
-// one cell column up the levels of the block: the top-vertex results of level
-// k are carried in registers to the bottom rows of level k + 1, so each
-// (cell column, vertex, level) adds once into shared memory. Cells are taken
-// in colours (no two of a colour share an owned vertex) with a barrier
+// keeps the owned rows of a block of LB levels (2, 4 or 8, picked by
+// lfx_mrhs_autotune) in shared memory. A warp walks one cell column up the
+// levels of the block. The MMA's output columns are ordered (bottom, top) per
+// vertex, so one lane holds both rows of a vertex: the top-vertex result of
+// level k stays in its registers and joins the bottom rows of level k + 1, and
+// each (cell column, vertex, level) adds once into shared memory. Cells are
+// taken in colours (no two of a colour share an owned vertex) with a barrier
 // between colours, so every sum has a fixed order.
 //
 // The solve wraps an FP32 preconditioned CG over all right-hand sides (each
@@ -44,7 +46,6 @@ using namespace lfx;
 
 namespace {
 
-constexpr int kLB = 4;      // levels per block of the apply
 constexpr int kMaxPC = 12;  // colours inside one patch, at most
 constexpr int kWarps = 4;   // warps per patch block
 constexpr int kDefaultPatch = 16;
@@ -76,9 +77,11 @@ __device__ __forceinline__ void mma_bf16(float* d, uint32_t a01, uint32_t a23, u
 }
 
 // Local matrices in B-fragment order, one 32-lane record per cell level
-// (c2d * nl + k). Lane (g = lane / 4, t = lane % 4) holds M(g, t), M(g, t + 4)
-// as TF32 (float2), or M(g, 2t), M(g, 2t + 1) as packed BF16; M(df, df2) is
-// element (c * ndf + df) * blk + df2 * nl + k of the operator's matrices.
+// (c2d * nl + k). B(j, n) = M(i(n), j) with the output dofs ordered (bottom,
+// top) per vertex: i(2v) = v, i(2v + 1) = v + 4. Lane (g = lane / 4,
+// t = lane % 4) holds B(t, g), B(t + 4, g) as TF32 (float2), or B(2t, g),
+// B(2t + 1, g) as packed BF16; M(df, df2) is element
+// (c * ndf + df) * blk + df2 * nl + k of the operator's matrices.
 template <class TM, bool BF>
 __global__ void mrhs_relayout(const TM* __restrict__ M, int64_t nc3, int nl, int blk, void* out) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -88,15 +91,16 @@ __global__ void mrhs_relayout(const TM* __restrict__ M, int64_t nc3, int nl, int
   const int64_t c = c3 / nl;
   const int k = (int)(c3 % nl);
   const int g = lane >> 2, t = lane & 3;
+  const int ig = (g >> 1) + 4 * (g & 1);
   auto at = [&](int df, int df2) {
     return (float)M[(c * 8 + df) * (int64_t)blk + (int64_t)df2 * nl + k];
   };
   if (BF) {
-    reinterpret_cast<uint32_t*>(out)[i] = pack_bf16(at(g, 2 * t), at(g, 2 * t + 1));
+    reinterpret_cast<uint32_t*>(out)[i] = pack_bf16(at(ig, 2 * t), at(ig, 2 * t + 1));
   } else {
     float2 v;
-    v.x = __uint_as_float(to_tf32(at(g, t)));
-    v.y = __uint_as_float(to_tf32(at(g, t + 4)));
+    v.x = __uint_as_float(to_tf32(at(ig, t)));
+    v.y = __uint_as_float(to_tf32(at(ig, t + 4)));
     reinterpret_cast<float2*>(out)[i] = v;
   }
 }
@@ -110,127 +114,153 @@ struct MrhsArgs {
   int nl;
 };
 
+// Rounding on the integer pipe (the conversion instructions share a narrow
+// pipe): TF32 round-half-away, BF16 round-half-even of two values packed.
+__device__ __forceinline__ uint32_t tf32_bits(float x) {
+  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
+}
+__device__ __forceinline__ uint32_t bf16_pair(float lo, float hi) {
+  uint32_t a = __float_as_uint(lo), b = __float_as_uint(hi);
+  a += 0x7FFFu + ((a >> 16) & 1u);
+  b += 0x7FFFu + ((b >> 16) & 1u);
+  return __byte_perm(a, b, 0x7632);
+}
+// W consecutive floats (W = 2, 4 or 8; aligned to W)
+template <int W, class P>
+__device__ __forceinline__ void ldw(P p, float (&v)[W]) {
+  if constexpr (W == 2) {
+    const float2 a = __ldg(reinterpret_cast<const float2*>(p));
+    v[0] = a.x; v[1] = a.y;
+  } else {
+#pragma unroll
+    for (int h = 0; h < W / 4; ++h) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(p) + h);
+      v[4 * h] = a.x; v[4 * h + 1] = a.y; v[4 * h + 2] = a.z; v[4 * h + 3] = a.w;
+    }
+  }
+}
+template <int W>
+__device__ __forceinline__ void addw(float* r, const float (&o)[W]) {
+  if constexpr (W == 2) {
+    float2* q = reinterpret_cast<float2*>(r);
+    float2 a = *q;
+    a.x += o[0]; a.y += o[1];
+    *q = a;
+  } else {
+#pragma unroll
+    for (int h = 0; h < W / 4; ++h) {
+      float4* q = reinterpret_cast<float4*>(r) + h;
+      float4 a = *q;
+      a.x += o[4 * h]; a.y += o[4 * h + 1]; a.z += o[4 * h + 2]; a.w += o[4 * h + 3];
+      *q = a;
+    }
+  }
+}
+
 // One cell column over the levels [l0, l0 + nlb) of a block: MMAs per level,
 // vertical carry, adds into the owned rows ys[slot][level - l0][rhs].
-template <int RB, bool BF>
+// Right-hand side map: with W = 2 RB, MMA row g of right-hand-side block rb
+// is right-hand side W g + 2 rb and row g + 8 is W g + 2 rb + 1, so lane
+// group g loads and adds the W consecutive right-hand sides W g .. W g + W - 1.
+// Output columns 2t, 2t + 1 are the bottom and top rows of vertex t.
+template <int RB, bool BF, int LB>
 __device__ __forceinline__ void mrhs_cell(const MrhsArgs& A, const float* __restrict__ X,
                                           float* ys, int e, int l0, int nlb, int lane) {
-  constexpr int NR = 16 * RB, RS = NR + 4, SLAB = (kLB + 1) * RS;
+  constexpr int NR = 16 * RB, RS = NR + 4, SLAB = (LB + 1) * RS, W = 2 * RB;
   const int g = lane >> 2, t = lane & 3;
   const int4 ca = A.cells[2 * e], cb = A.cells[2 * e + 1];
   const int nl = A.nl;
-  const int va = 2 * (t & 1);  // this lane's result columns: vertices va, va + 1
-  const unsigned sp = (unsigned)cb.y;
-  const unsigned sa = (sp >> (8 * va)) & 255u, sb = (sp >> (8 * va + 8)) & 255u;
+  const unsigned st = ((unsigned)cb.y >> (8 * t)) & 255u;  // owned slot of vertex t
   const size_t mrec = ((size_t)ca.x * nl + l0) * 32 + lane;
 
   // operands of all levels of the block, loaded before the first MMA
-  uint32_t xa[kLB + 1][RB][2];  // TF32: rows of vertex t; BF16: [kk][rb][rhs g / g+8]
-  uint32_t bm[kLB][2];
+  uint32_t xa[LB + 1][W];
+  uint32_t bm[LB][2];
   if (!BF) {
+    // A columns t (bottom) and t + 4 (top): vertex t at levels k and k + 1
     const int xbt = t == 0 ? ca.y : t == 1 ? ca.z : t == 2 ? ca.w : cb.x;
-    const float* xc = X + (size_t)(xbt + l0) * NR + g;
+    const float* xc = X + (size_t)(xbt + l0) * NR + W * g;
 #pragma unroll
-    for (int kk = 0; kk <= kLB; ++kk)
+    for (int kk = 0; kk <= LB; ++kk) {
+      float v[W];
+      if (kk <= nlb) {
+        ldw<W>(xc + kk * NR, v);
+      } else {
 #pragma unroll
-      for (int rb = 0; rb < RB; ++rb) {
-        xa[kk][rb][0] = kk <= nlb ? to_tf32(__ldg(xc + kk * NR + rb * 16)) : 0u;
-        xa[kk][rb][1] = kk <= nlb ? to_tf32(__ldg(xc + kk * NR + rb * 16 + 8)) : 0u;
+        for (int w = 0; w < W; ++w) v[w] = 0.f;
       }
+#pragma unroll
+      for (int w = 0; w < W; ++w) xa[kk][w] = tf32_bits(v[w]);
+    }
     const float2* mc = reinterpret_cast<const float2*>(A.Mf) + mrec;
 #pragma unroll
-    for (int kk = 0; kk < kLB; ++kk) {
+    for (int kk = 0; kk < LB; ++kk) {
       const float2 v = kk < nlb ? __ldg(mc + kk * 32) : make_float2(0.f, 0.f);
       bm[kk][0] = __float_as_uint(v.x);
       bm[kk][1] = __float_as_uint(v.y);
     }
   } else {
-    // A columns 2t, 2t + 1: vertices va, va + 1 at level offset t / 2
+    // A columns 2t, 2t + 1: vertices 2 (t % 2), 2 (t % 2) + 1 at level offset t / 2
     const int lo = t >> 1;
     const int x0 = (t & 1) ? ca.w : ca.y, x1 = (t & 1) ? cb.x : ca.z;
-    const float* p0 = X + (size_t)(x0 + l0 + lo) * NR + g;
-    const float* p1 = X + (size_t)(x1 + l0 + lo) * NR + g;
+    const float* p0 = X + (size_t)(x0 + l0 + lo) * NR + W * g;
+    const float* p1 = X + (size_t)(x1 + l0 + lo) * NR + W * g;
 #pragma unroll
-    for (int kk = 0; kk < kLB; ++kk)
+    for (int kk = 0; kk < LB; ++kk) {
+      float v0[W], v1[W];
+      if (kk < nlb) {
+        ldw<W>(p0 + kk * NR, v0);
+        ldw<W>(p1 + kk * NR, v1);
+      } else {
 #pragma unroll
-      for (int rb = 0; rb < RB; ++rb) {
-        const int o = kk * NR + rb * 16;
-        xa[kk][rb][0] = kk < nlb ? pack_bf16(__ldg(p0 + o), __ldg(p1 + o)) : 0u;
-        xa[kk][rb][1] = kk < nlb ? pack_bf16(__ldg(p0 + o + 8), __ldg(p1 + o + 8)) : 0u;
+        for (int w = 0; w < W; ++w) v0[w] = v1[w] = 0.f;
       }
+#pragma unroll
+      for (int w = 0; w < W; ++w) xa[kk][w] = bf16_pair(v0[w], v1[w]);
+    }
     const uint32_t* mc = reinterpret_cast<const uint32_t*>(A.Mf) + mrec;
 #pragma unroll
-    for (int kk = 0; kk < kLB; ++kk) bm[kk][0] = kk < nlb ? __ldg(mc + kk * 32) : 0u;
+    for (int kk = 0; kk < LB; ++kk) bm[kk][0] = kk < nlb ? __ldg(mc + kk * 32) : 0u;
   }
 
-  float carry[RB][4];
+  float carry[W];  // top rows of the level below (row kk)
+  float* yr = ys + st * SLAB + W * g;
 #pragma unroll
-  for (int kk = 0; kk < kLB; ++kk) {
+  for (int kk = 0; kk < LB; ++kk) {
     if (kk >= nlb) break;  // warp-uniform
     float d[RB][4];
 #pragma unroll
     for (int rb = 0; rb < RB; ++rb) {
       if (!BF)
-        mma_tf32(d[rb], xa[kk][rb][0], xa[kk][rb][1], xa[kk + 1][rb][0], xa[kk + 1][rb][1],
-                 bm[kk][0], bm[kk][1]);
+        mma_tf32(d[rb], xa[kk][2 * rb], xa[kk][2 * rb + 1], xa[kk + 1][2 * rb],
+                 xa[kk + 1][2 * rb + 1], bm[kk][0], bm[kk][1]);
       else
-        mma_bf16(d[rb], xa[kk][rb][0], xa[kk][rb][1], bm[kk][0]);
+        mma_bf16(d[rb], xa[kk][2 * rb], xa[kk][2 * rb + 1], bm[kk][0]);
     }
-    // lanes t < 2: bottom rows (level l0 + kk) of vertices va, va + 1, plus the
-    // carried top rows of the level below; lanes t >= 2: top rows
-    if (t < 2) {
+    float o[W];
 #pragma unroll
-      for (int rb = 0; rb < RB; ++rb)
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (kk > 0) d[rb][q] += carry[rb][q];
-      if (sa != 255u) {
-        float* r = ys + sa * SLAB + kk * RS + g;
-#pragma unroll
-        for (int rb = 0; rb < RB; ++rb) {
-          r[rb * 16] += d[rb][0];
-          r[rb * 16 + 8] += d[rb][2];
-        }
+    for (int rb = 0; rb < RB; ++rb) {
+      o[2 * rb] = d[rb][0];
+      o[2 * rb + 1] = d[rb][2];
+      if (kk > 0) {
+        o[2 * rb] += carry[2 * rb];
+        o[2 * rb + 1] += carry[2 * rb + 1];
       }
-      if (sb != 255u) {
-        float* r = ys + sb * SLAB + kk * RS + g;
-#pragma unroll
-        for (int rb = 0; rb < RB; ++rb) {
-          r[rb * 16] += d[rb][1];
-          r[rb * 16 + 8] += d[rb][3];
-        }
-      }
+      carry[2 * rb] = d[rb][1];
+      carry[2 * rb + 1] = d[rb][3];
     }
-#pragma unroll
-    for (int rb = 0; rb < RB; ++rb)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) carry[rb][q] = __shfl_down_sync(0xffffffffu, d[rb][q], 2);
-    if (kk == nlb - 1 && t < 2) {
+    if (st != 255u) {
+      addw<W>(yr + kk * RS, o);
       // top rows of the block's last level: row nlb, carried to the next block
-      if (sa != 255u) {
-        float* r = ys + sa * SLAB + (kk + 1) * RS + g;
-#pragma unroll
-        for (int rb = 0; rb < RB; ++rb) {
-          r[rb * 16] += carry[rb][0];
-          r[rb * 16 + 8] += carry[rb][2];
-        }
-      }
-      if (sb != 255u) {
-        float* r = ys + sb * SLAB + (kk + 1) * RS + g;
-#pragma unroll
-        for (int rb = 0; rb < RB; ++rb) {
-          r[rb * 16] += carry[rb][1];
-          r[rb * 16 + 8] += carry[rb][3];
-        }
-      }
+      if (kk == nlb - 1) addw<W>(yr + (kk + 1) * RS, carry);
     }
   }
 }
 
-template <int RB, bool BF>
+template <int RB, bool BF, int LB>
 __global__ void __launch_bounds__(kWarps * 32) mrhs_apply_k(MrhsArgs A, const float* __restrict__ X,
                                                           float* __restrict__ Y) {
-  constexpr int NR = 16 * RB, RS = NR + 4, SLAB = (kLB + 1) * RS, C4 = NR / 4;
+  constexpr int NR = 16 * RB, RS = NR + 4, SLAB = (LB + 1) * RS, C4 = NR / 4;
   extern __shared__ float4 ys4[];
   float* ys = reinterpret_cast<float*>(ys4);
   const int p = blockIdx.x;
@@ -239,21 +269,26 @@ __global__ void __launch_bounds__(kWarps * 32) mrhs_apply_k(MrhsArgs A, const fl
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int* pc = A.pcol + (size_t)p * (kMaxPC + 1);
   for (int i = threadIdx.x; i < nown * SLAB; i += blockDim.x) ys[i] = 0.f;
-  for (int l0 = 0; l0 < nl; l0 += kLB) {
-    const int nlb = min(kLB, nl - l0);
+  for (int l0 = 0; l0 < nl; l0 += LB) {
+    const int nlb = min(LB, nl - l0);
     for (int q = 0; q < pi.w; ++q) {
       __syncthreads();  // zeroing / the previous colour's adds are done
       const int e1 = pi.z + pc[q + 1];
       for (int e = pi.z + pc[q] + warp; e < e1; e += kWarps)
-        mrhs_cell<RB, BF>(A, X, ys, e, l0, nlb, lane);
+        mrhs_cell<RB, BF, LB>(A, X, ys, e, l0, nlb, lane);
     }
     __syncthreads();
     const bool last = l0 + nlb >= nl;
     const int rows = nlb + (last ? 1 : 0);
-    for (int i = threadIdx.x; i < nown * rows * C4; i += blockDim.x) {
-      const int c4 = i % C4, rr = (i / C4) % rows, s = i / (C4 * rows);
-      const float4 v = *reinterpret_cast<const float4*>(ys + s * SLAB + rr * RS + 4 * c4);
-      *reinterpret_cast<float4*>(Y + (size_t)(A.own_base[pi.x + s] + l0 + rr) * NR + 4 * c4) = v;
+    // flush: one warp per owned vertex column, lanes over (row, float4)
+    for (int sl = warp; sl < nown; sl += kWarps) {
+      const float* src = ys + sl * SLAB;
+      float* dst = Y + (size_t)(A.own_base[pi.x + sl] + l0) * NR;
+      for (int i = lane; i < rows * C4; i += 32) {
+        const int rr = i / C4, c4 = i % C4;
+        *reinterpret_cast<float4*>(dst + (size_t)rr * NR + 4 * c4) =
+            *reinterpret_cast<const float4*>(src + rr * RS + 4 * c4);
+      }
     }
     if (last) break;
     __syncthreads();
@@ -261,30 +296,45 @@ __global__ void __launch_bounds__(kWarps * 32) mrhs_apply_k(MrhsArgs A, const fl
     for (int i = threadIdx.x; i < nown * RS; i += blockDim.x) {
       float* b = ys + (i / RS) * SLAB + (i % RS);
       b[0] = b[nlb * RS];
-      for (int r = 1; r <= kLB; ++r) b[r * RS] = 0.f;
+#pragma unroll
+      for (int r = 1; r <= LB; ++r) b[r * RS] = 0.f;
     }
   }
 }
 
 // ------------------------------------------------ dof-major vector kernels
+// A thread handles four consecutive right-hand sides of a row (16-byte
+// accesses): NR / 4 threads per row, RPB = 1024 / NR rows per block pass.
+
+template <int NR>
+struct MvShape {
+  static constexpr int TPR = NR / 4;      // threads per row
+  static constexpr int RPB = 256 / TPR;   // rows per block pass
+};
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
 // Sums acc over the rows of the block, then over all blocks in block order
 // (the last block to finish, by ticket), into tot[r * NR + col]. Returns true
-// in that last block, with tot complete.
+// in that last block, with tot complete. acc[r][j] belongs to column
+// 4 (threadIdx.x % TPR) + j.
 template <int NR, int NRED>
-__device__ bool mv_finish(const double (&acc)[NRED], double* partials, unsigned* ticket,
+__device__ bool mv_finish(const double (&acc)[NRED][4], double* partials, unsigned* ticket,
                           double* tot) {
-  constexpr int RPB = 256 / NR;
-  __shared__ double sm[256];
+  using S = MvShape<NR>;
+  __shared__ double sm[S::RPB * NR];
   __shared__ int am_last;
   const int G = gridDim.x;
+  const int c4 = threadIdx.x % S::TPR, rr = threadIdx.x / S::TPR;
 #pragma unroll
   for (int r = 0; r < NRED; ++r) {
-    sm[threadIdx.x] = acc[r];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sm[rr * NR + 4 * c4 + j] = acc[r][j];
     __syncthreads();
     if (threadIdx.x < NR) {
       double s = 0.0;
-      for (int q = 0; q < RPB; ++q) s = s + sm[q * NR + threadIdx.x];
+      for (int q = 0; q < S::RPB; ++q) s = s + sm[q * NR + threadIdx.x];
       partials[((size_t)r * NR + threadIdx.x) * G + blockIdx.x] = s;
     }
     __syncthreads();
@@ -321,25 +371,33 @@ __device__ void count_active(MvState* S, int nr) {
   }
 }
 
+#define LFX_MV_ROWS(NR)                                                      \
+  const int c4 = threadIdx.x % MvShape<NR>::TPR;                             \
+  for (int64_t row = (int64_t)blockIdx.x * MvShape<NR>::RPB +                \
+                     threadIdx.x / MvShape<NR>::TPR;                         \
+       row < n; row += (int64_t)gridDim.x * MvShape<NR>::RPB)
+
 // x = 0, p = z = D^-1 r; rz = <r, z>, r0 = ||r|| per right-hand side
 template <int NR>
 __global__ void __launch_bounds__(256) mv_init(int64_t n, const float* __restrict__ dinv,
                                                const float* __restrict__ r, float* __restrict__ p,
                                                float* __restrict__ x, const int* act_out,
                                                MvState* S, double* partials, unsigned* ticket) {
-  constexpr int RPB = 256 / NR;
   __shared__ double tot[2 * NR];
-  const int col = threadIdx.x % NR;
-  double acc[2] = {0.0, 0.0};
-  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
-       row += (int64_t)gridDim.x * RPB) {
-    const size_t i = (size_t)row * NR + col;
-    const float ri = r[i];
-    const float zi = ri * dinv[row];
-    p[i] = zi;
-    x[i] = 0.f;
-    acc[0] = fma((double)ri, (double)ri, acc[0]);
-    acc[1] = fma((double)ri, (double)zi, acc[1]);
+  double acc[2][4] = {};
+  LFX_MV_ROWS(NR) {
+    const size_t i = (size_t)row * NR + 4 * c4;
+    const float4 rv = ld4(r + i);
+    const float d = dinv[row];
+    const float4 zv = make_float4(rv.x * d, rv.y * d, rv.z * d, rv.w * d);
+    st4(p + i, zv);
+    st4(x + i, make_float4(0.f, 0.f, 0.f, 0.f));
+    const float ra[4] = {rv.x, rv.y, rv.z, rv.w}, za[4] = {zv.x, zv.y, zv.z, zv.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      acc[0][j] = fma((double)ra[j], (double)ra[j], acc[0][j]);
+      acc[1][j] = fma((double)ra[j], (double)za[j], acc[1][j]);
+    }
   }
   if (!mv_finish<NR, 2>(acc, partials, ticket, tot)) return;
   if (threadIdx.x < NR) {
@@ -361,14 +419,15 @@ template <int NR>
 __global__ void __launch_bounds__(256) mv_alpha(int64_t n, const float* __restrict__ p,
                                                 const float* __restrict__ q, MvState* S,
                                                 double* partials, unsigned* ticket) {
-  constexpr int RPB = 256 / NR;
   __shared__ double tot[NR];
-  const int col = threadIdx.x % NR;
-  double acc[1] = {0.0};
-  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
-       row += (int64_t)gridDim.x * RPB) {
-    const size_t i = (size_t)row * NR + col;
-    acc[0] = fma((double)p[i], (double)q[i], acc[0]);
+  double acc[1][4] = {};
+  LFX_MV_ROWS(NR) {
+    const size_t i = (size_t)row * NR + 4 * c4;
+    const float4 pv = ld4(p + i), qv = ld4(q + i);
+    acc[0][0] = fma((double)pv.x, (double)qv.x, acc[0][0]);
+    acc[0][1] = fma((double)pv.y, (double)qv.y, acc[0][1]);
+    acc[0][2] = fma((double)pv.z, (double)qv.z, acc[0][2]);
+    acc[0][3] = fma((double)pv.w, (double)qv.w, acc[0][3]);
   }
   if (!mv_finish<NR, 1>(acc, partials, ticket, tot)) return;
   if (threadIdx.x < NR) {
@@ -385,20 +444,28 @@ __global__ void __launch_bounds__(256) mv_update(int64_t n, const float* __restr
                                                  const float* __restrict__ q, float* __restrict__ x,
                                                  float* __restrict__ r, double tol, MvState* S,
                                                  double* partials, unsigned* ticket) {
-  constexpr int RPB = 256 / NR;
   __shared__ double tot[2 * NR];
-  const int col = threadIdx.x % NR;
-  const float a = (float)S->alpha[col];
-  double acc[2] = {0.0, 0.0};
-  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
-       row += (int64_t)gridDim.x * RPB) {
-    const size_t i = (size_t)row * NR + col;
-    const float pi = p[i], qi = q[i], xi = x[i], ri0 = r[i], di = dinv[row];
-    x[i] = fmaf(a, pi, xi);
-    const float ri = fmaf(-a, qi, ri0);
-    r[i] = ri;
-    acc[0] = fma((double)ri, (double)ri, acc[0]);
-    acc[1] = fma((double)ri, (double)(ri * di), acc[1]);
+  float a[4];
+  {
+    const int c0 = 4 * (threadIdx.x % MvShape<NR>::TPR);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) a[j] = (float)S->alpha[c0 + j];
+  }
+  double acc[2][4] = {};
+  LFX_MV_ROWS(NR) {
+    const size_t i = (size_t)row * NR + 4 * c4;
+    const float4 pv = ld4(p + i), qv = ld4(q + i), xv = ld4(x + i), rv = ld4(r + i);
+    const float d = dinv[row];
+    st4(x + i, make_float4(fmaf(a[0], pv.x, xv.x), fmaf(a[1], pv.y, xv.y), fmaf(a[2], pv.z, xv.z),
+                           fmaf(a[3], pv.w, xv.w)));
+    const float rn[4] = {fmaf(-a[0], qv.x, rv.x), fmaf(-a[1], qv.y, rv.y),
+                         fmaf(-a[2], qv.z, rv.z), fmaf(-a[3], qv.w, rv.w)};
+    st4(r + i, make_float4(rn[0], rn[1], rn[2], rn[3]));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      acc[0][j] = fma((double)rn[j], (double)rn[j], acc[0][j]);
+      acc[1][j] = fma((double)rn[j], (double)(rn[j] * d), acc[1][j]);
+    }
   }
   if (!mv_finish<NR, 2>(acc, partials, ticket, tot)) return;
   if (threadIdx.x < NR) {
@@ -423,15 +490,21 @@ template <int NR>
 __global__ void __launch_bounds__(256) mv_direction(int64_t n, const float* __restrict__ dinv,
                                                     const float* __restrict__ r,
                                                     float* __restrict__ p, const MvState* S) {
-  constexpr int RPB = 256 / NR;
-  const int col = threadIdx.x % NR;
-  const float b = (float)S->beta[col];
-  for (int64_t row = (int64_t)blockIdx.x * RPB + threadIdx.x / NR; row < n;
-       row += (int64_t)gridDim.x * RPB) {
-    const size_t i = (size_t)row * NR + col;
-    p[i] = fmaf(b, p[i], r[i] * dinv[row]);
+  float b[4];
+  {
+    const int c0 = 4 * (threadIdx.x % MvShape<NR>::TPR);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = (float)S->beta[c0 + j];
+  }
+  LFX_MV_ROWS(NR) {
+    const size_t i = (size_t)row * NR + 4 * c4;
+    const float4 rv = ld4(r + i), pv = ld4(p + i);
+    const float d = dinv[row];
+    st4(p + i, make_float4(fmaf(b[0], pv.x, rv.x * d), fmaf(b[1], pv.y, rv.y * d),
+                           fmaf(b[2], pv.z, rv.z * d), fmaf(b[3], pv.w, rv.w * d)));
   }
 }
+#undef LFX_MV_ROWS
 
 // r[row][col] = (float) R[col * ld + row] (RHS-major FP64 to dof-major FP32)
 template <int NR>
@@ -490,7 +563,7 @@ struct lfx_mrhs {
   int4* cells = nullptr;
   void* Mf = nullptr;
   size_t Mf_bytes = 0;
-  size_t smem = 0;
+  int32_t lb = 4;  // levels per block of the apply (2, 4 or 8)
   size_t pinfo_b = 0, pcol_b = 0, own_b = 0, cells_b = 0;
   // solve work space, allocated by the first solve
   float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *dinv = nullptr;
@@ -508,37 +581,44 @@ struct lfx_mrhs {
 
 namespace {
 
-int mrhs_launch(lfx_mrhs* m, const float* x, float* y) {
+size_t mrhs_smem(const lfx_mrhs* m, int lb) {
+  return (size_t)m->own_max * (lb + 1) * (m->nrhs + 4) * sizeof(float);
+}
+
+template <int RB, bool BF, int LB>
+int launch_t(lfx_mrhs* m, const float* x, float* y) {
   lfx_ctx* ctx = m->ctx;
   MrhsArgs A{m->pinfo, m->pcol, m->own_base, m->cells, m->Mf, m->nl};
-  const bool bf = m->kind == LFX_MRHS_BF16;
-  const dim3 grid(m->npatch), block(kWarps * 32);
-#define LFX_MRHS_CASE(RB)                                                                  \
-  if (bf)                                                                                  \
-    mrhs_apply_k<RB, true><<<grid, block, m->smem, ctx->stream>>>(A, x, y);                \
-  else                                                                                     \
-    mrhs_apply_k<RB, false><<<grid, block, m->smem, ctx->stream>>>(A, x, y);
-  switch (m->nrhs) {
-    case 16: LFX_MRHS_CASE(1) break;
-    case 32: LFX_MRHS_CASE(2) break;
-    default: LFX_MRHS_CASE(4) break;
-  }
-#undef LFX_MRHS_CASE
+  const size_t smem = mrhs_smem(m, LB);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(mrhs_apply_k<RB, BF, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return fail(ctx, LFX_NOT_SUPPORTED, "apply shared memory exceeds the device limit");
+  mrhs_apply_k<RB, BF, LB><<<m->npatch, kWarps * 32, smem, ctx->stream>>>(A, x, y);
   ctx->launches++;
   LFX_CK(ctx, cudaGetLastError());
   return LFX_OK;
 }
 
-template <int RB>
-int set_smem_attr(size_t smem) {
-  if (cudaFuncSetAttribute(mrhs_apply_k<RB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return 1;
-  if (cudaFuncSetAttribute(mrhs_apply_k<RB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return 1;
-  return 0;
+template <int RB, bool BF>
+int launch_lb(lfx_mrhs* m, int lb, const float* x, float* y) {
+  switch (lb) {
+    case 2: return launch_t<RB, BF, 2>(m, x, y);
+    case 8: return launch_t<RB, BF, 8>(m, x, y);
+    default: return launch_t<RB, BF, 4>(m, x, y);
+  }
 }
+
+int mrhs_launch_lb(lfx_mrhs* m, int lb, const float* x, float* y) {
+  const bool bf = m->kind == LFX_MRHS_BF16;
+  switch (m->nrhs) {
+    case 16: return bf ? launch_lb<1, true>(m, lb, x, y) : launch_lb<1, false>(m, lb, x, y);
+    case 32: return bf ? launch_lb<2, true>(m, lb, x, y) : launch_lb<2, false>(m, lb, x, y);
+    default: return bf ? launch_lb<4, true>(m, lb, x, y) : launch_lb<4, false>(m, lb, x, y);
+  }
+}
+
+int mrhs_launch(lfx_mrhs* m, const float* x, float* y) { return mrhs_launch_lb(m, m->lb, x, y); }
 
 void mrhs_free(lfx_mrhs* m) {
   lfx_ctx* ctx = m->ctx;
@@ -739,16 +819,9 @@ int lfx_mrhs_create(const lfx_op* op, int32_t kind, int32_t nrhs, int32_t cells_
   m->own_max = own_max;
   m->max_colours = max_col;
   m->nent = (int64_t)h_cells.size() / 2;
-  const int RS = nrhs + 4;
-  m->smem = (size_t)own_max * (kLB + 1) * RS * sizeof(float);
   int rc = LFX_OK;
-  if (m->smem > 227 * 1024) rc = fail(ctx, LFX_NOT_SUPPORTED, "patch too large for shared memory");
-  if (!rc && m->smem > 48 * 1024) {
-    const int bad = nrhs == 16 ? set_smem_attr<1>(m->smem)
-                    : nrhs == 32 ? set_smem_attr<2>(m->smem)
-                                 : set_smem_attr<4>(m->smem);
-    if (bad) rc = fail(ctx, LFX_CUDA_ERROR, "cannot set the apply's shared memory size");
-  }
+  if (mrhs_smem(m, 2) > 227 * 1024) rc = fail(ctx, LFX_NOT_SUPPORTED, "patch too large for shared memory");
+  m->lb = mrhs_smem(m, 4) <= 227 * 1024 ? 4 : 2;
   auto up = [&](void** dst, size_t* held, const void* src, size_t bytes) {
     if (rc) return;
     rc = dmalloc(ctx, dst, bytes);
@@ -832,6 +905,51 @@ int lfx_mrhs_time_apply(lfx_mrhs* m, const float* x, float* y, int32_t reps, flo
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
+}
+
+// Times the apply with 2, 4 and 8 levels per block (those whose shared
+// memory fits) over reps applies each and keeps the fastest.
+int lfx_mrhs_autotune(lfx_mrhs* m, int32_t reps, int32_t* lb, float* us) {
+  if (!m || reps < 1) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = m->ctx;
+  const size_t bytes = (size_t)m->undf * m->nrhs * sizeof(float);
+  float *x = nullptr, *y = nullptr;
+  int rc = dmalloc(ctx, (void**)&x, bytes);
+  if (!rc) rc = dmalloc(ctx, (void**)&y, bytes);
+  if (!rc) LFX_CK(ctx, cudaMemsetAsync(x, 0, bytes, ctx->stream));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!rc) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+  }
+  int best = m->lb;
+  float best_us = 0.f;
+  for (int cand : {2, 4, 8}) {
+    if (rc) break;
+    if (mrhs_smem(m, cand) > 227 * 1024) continue;
+    rc = mrhs_launch_lb(m, cand, x, y);  // warm
+    cudaEventRecord(e0, ctx->stream);
+    for (int r = 0; r < reps && !rc; ++r) rc = mrhs_launch_lb(m, cand, x, y);
+    cudaEventRecord(e1, ctx->stream);
+    if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+      rc = fail(ctx, LFX_CUDA_ERROR, "multi-RHS apply timing failed");
+    float ms = 0.f;
+    if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+    const float t = 1e3f * ms / reps;
+    if (!rc && (best_us == 0.f || t < best_us)) {
+      best_us = t;
+      best = cand;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  dfree(ctx, x, bytes);
+  dfree(ctx, y, bytes);
+  if (rc) return rc;
+  m->lb = best;
+  if (lb) *lb = best;
+  if (us) *us = best_us;
+  return LFX_OK;
 }
 
 namespace {

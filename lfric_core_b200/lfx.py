@@ -149,6 +149,7 @@ _SIGS = [
                        C.POINTER(C.c_int32), C.POINTER(C.c_int64)], C.c_int),
     ("lfx_mrhs_apply", [vp, vp, vp], C.c_int),
     ("lfx_mrhs_time_apply", [vp, vp, vp, C.c_int32, C.POINTER(C.c_float)], C.c_int),
+    ("lfx_mrhs_autotune", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_float)], C.c_int),
     ("lfx_mrhs_solve", [vp, vp, vp, vp, vp, C.c_int64, C.POINTER(MrhsCfg), C.POINTER(SolveInfo)],
      C.c_int),
     ("lfx_dot_noalloc", [vp, vp, C.c_int64, vp, vp], C.c_int),
@@ -458,6 +459,11 @@ class MultiRhsOperator(_Handle):
         us = C.c_float()
         self.ctx.check(self.ctx.L.lfx_mrhs_time_apply(self.h, x_ptr, y_ptr, reps, C.byref(us)))
         return us.value
+
+    def autotune(self, reps: int = 10) -> dict:
+        lb, us = C.c_int32(), C.c_float()
+        self.ctx.check(self.ctx.L.lfx_mrhs_autotune(self.h, reps, C.byref(lb), C.byref(us)))
+        return {"levels_per_block": lb.value, "us": us.value}
 
     def solve(self, op64: "LmaOperator", diag: "FieldVector", b_ptr: int, x_ptr: int, ld: int,
               r_tol=1e-8, inner_tol=1e-2, max_outer=20, max_inner=5000):

@@ -70,6 +70,22 @@ def test_mrhs_patch_sizes_agree_within_bound(ctx):
             assert np.all(np.abs(Y[:, r] - Ys[0][:, r]) <= 8 * U[TF32] * ya)
 
 
+@pytest.mark.parametrize("kind", [TF32, BF16])
+def test_mrhs_autotune_keeps_results_within_bound(ctx, kind):
+    p = mg.w0_problem(6, 11, seed=21)
+    s = wl.device_w0(ctx, p)
+    M = lfx.MultiRhsOperator(s.op, kind, 64)
+    X = np.random.default_rng(8).standard_normal((p.undf, 64)).astype(np.float32)
+    before = mrhs_apply(ctx, M, X)
+    t = M.autotune(reps=3)
+    assert t["levels_per_block"] in (2, 4, 8) and t["us"] > 0
+    after = mrhs_apply(ctx, M, X)
+    oa = o_lma(p, np.abs(p.lma))
+    for r in range(0, 64, 7):
+        ya = oa.apply(np.abs(X[:, r]).astype(np.float64))
+        assert np.all(np.abs(after[:, r] - before[:, r]) <= 8 * U[kind] * ya)
+
+
 def test_mrhs_rejects_non_nodal_operator(ctx):
     p = mg.w2_problem(4, 3)
     s = wl.device_w2(ctx, p)

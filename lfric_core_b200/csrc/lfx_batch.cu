@@ -191,6 +191,20 @@ __global__ void __launch_bounds__(256) bapply(const int2* list, const int* len, 
         const int o0 = (pk >> 8) & 7u, o1 = (pk >> 17) & 7u;
         const int k0 = l - o0, k1 = l - o1;
         const bool v0 = (unsigned)k0 < (unsigned)nl;
+        if ((pk & 3u) == 1) {
+          // one record (warp-uniform branch): no second-record instructions
+          const T* M0 = M + (size_t)c * cell_stride + (size_t)((pk >> 2) & 63u) * blk + (v0 ? k0 : 0);
+          T a0[NDF2], b0[NDF2];
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+            b0[j] = v0 ? __ldg(x + tmp[j] + k0) : T(0);
+          }
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j)
+            if (v0) acc = fmaT(a0[j], b0[j], acc);
+          continue;
+        }
         const bool v1 = (pk & 3u) > 1 && (unsigned)k1 < (unsigned)nl;
         // second record one level above the first: its x values are the
         // neighbouring lane's first-record values

@@ -288,6 +288,10 @@ struct lfx_lma_layout {
   int4* ent_pack = nullptr;
   int32_t* grp_pack = nullptr;
   int32_t gp_stride = 0;
+  // per entity column one descriptor of 32 * desc_ipl ints: {base, h, groups,
+  // blocks} then per group {cell, record, map_from row} (0 when not built)
+  int32_t* desc = nullptr;
+  int32_t desc_ipl = 0;
   int32_t max_groups = 0;  // groups of one entity column, at most
   int32_t max_blocks = 0;  // (cell, df) matrix blocks one entity column reads, at most
   int refcount = 1;

@@ -39,12 +39,13 @@ struct LayoutArgs {
   const int4* ent_pack;
   const int32_t* grp_pack;
   int32_t gp_stride;
+  const int32_t* desc;
 };
 
 LayoutArgs args_of(const lfx_lma_layout* L, int blk) {
   return LayoutArgs{L->nent,     L->nlayers,  L->ndf_to,   L->ndf_from, blk,
                     L->ent_base, L->ent_h,    L->ent_grp,  L->grp_cell, L->grp_rec,
-                    L->map_from, L->ent_pack, L->grp_pack, L->gp_stride};
+                    L->map_from, L->ent_pack, L->grp_pack, L->gp_stride, L->desc};
 }
 
 // packed group record: bits 0-1 nrec (1..3); record r at bit 2+9r: df (6 bits), off (3 bits)
@@ -91,6 +92,18 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 }
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// 4- or 8-byte asynchronous copy global -> shared, and an mbarrier arrival
+// that fires once all of this thread's earlier copies have landed (the
+// pending count is raised first, so the phase waits for them)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "n"(BYTES)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.shared.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // ---------------------------------------------------------------- kernels
@@ -162,14 +175,68 @@ __device__ __forceinline__ void gather_record(const LayoutArgs& A, int g, int& c
   for (int j = 0; j < NDF2; ++j) mf[j] = tmp[j];
 }
 
-// Register path (no shared memory) for groups of at most two records: all
-// loads of a cell group are issued before the FMA chain that consumes them.
+// One cell group's contribution to output row l of an entity column (groups of
+// at most two records): all loads of the group are issued before the FMA
+// chain that consumes them. The warp must be converged (pair shuffles).
+template <class T, int NDF2>
+__device__ __forceinline__ T group_acc(const LayoutArgs& A, const T* __restrict__ M,
+                                       const T* __restrict__ x, size_t cell_stride, int l,
+                                       int lane, int c, uint32_t pk, const int* mf, T acc) {
+  const int nl = A.nlayers;
+  const int k0 = l - rec_off(pk, 0), k1 = l - rec_off(pk, 1);
+  const bool v0 = (unsigned)k0 < (unsigned)nl;
+  if (rec_n(pk) == 1) {
+    // one record (warp-uniform branch): no second-record instructions
+    const T* M0 = M + (size_t)c * cell_stride + (size_t)rec_df(pk, 0) * A.blk + (v0 ? k0 : 0);
+    T a0[NDF2], b0[NDF2];
+#pragma unroll
+    for (int j = 0; j < NDF2; ++j) {
+      a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+      b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < NDF2; ++j)
+      if (v0) acc = fmaT(a0[j], b0[j], acc);
+    return acc;
+  }
+  const bool v1 = rec_n(pk) > 1 && (unsigned)k1 < (unsigned)nl;
+  // second record one level above the first (bottom/top vertex or face): its
+  // x values are the neighbouring lane's first-record values
+  const bool pair = rec_n(pk) == 2 && rec_off(pk, 1) == rec_off(pk, 0) + 1;
+  const T* Mc = M + (size_t)c * cell_stride;
+  const T* M0 = Mc + (size_t)rec_df(pk, 0) * A.blk + (v0 ? k0 : 0);
+  const T* M1 = Mc + (size_t)rec_df(pk, 1) * A.blk + (v1 ? k1 : 0);
+  T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
+#pragma unroll
+  for (int j = 0; j < NDF2; ++j) {
+    a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+    b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
+    a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+  }
+  if (pair) {
+#pragma unroll
+    for (int j = 0; j < NDF2; ++j) {
+      const T up = __shfl_up_sync(0xffffffffu, b0[j], 1);
+      b1[j] = (lane == 0) ? (v1 ? __ldg(x + mf[j] + k1) : T(0)) : up;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < NDF2; ++j) b1[j] = v1 ? __ldg(x + mf[j] + k1) : T(0);
+  }
+#pragma unroll
+  for (int j = 0; j < NDF2; ++j) {
+    if (v0) acc = fmaT(a0[j], b0[j], acc);
+    if (v1) acc = fmaT(a1[j], b1[j], acc);
+  }
+  return acc;
+}
+
+// Register path (no shared memory) for groups of at most two records.
 template <class T, int NDF2>
 __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __restrict__ M,
                                                    const T* __restrict__ x, T* __restrict__ y,
                                                    const T* __restrict__ b, const int* skip) {
   if (skip && *((volatile const int*)skip)) return;
-  const int nl = A.nlayers;
   const int lane = threadIdx.x & 31;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const size_t cell_stride = (size_t)A.ndf1 * A.blk;
@@ -177,7 +244,7 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
     const int4 ep = __ldg(A.ent_pack + e);
     const int base = ep.x, h = ep.y, g0 = ep.z, g1 = ep.w;
     // all 32 lanes run every pass (lanes past the column's top just carry no
-    // valid record) so that the shuffles below see a converged warp
+    // valid record) so that the shuffles see a converged warp
     for (int l0 = 0; l0 < h; l0 += 32) {
       const int l = l0 + lane;
       T acc = T(0);
@@ -186,37 +253,7 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
         uint32_t pk;
         int mf[NDF2];
         gather_record<NDF2>(A, g, c, pk, mf);
-        const int k0 = l - rec_off(pk, 0), k1 = l - rec_off(pk, 1);
-        const bool v0 = (unsigned)k0 < (unsigned)nl;
-        const bool v1 = rec_n(pk) > 1 && (unsigned)k1 < (unsigned)nl;
-        // second record one level above the first (bottom/top vertex or
-        // face): its x values are the neighbouring lane's first-record values
-        const bool pair = rec_n(pk) == 2 && rec_off(pk, 1) == rec_off(pk, 0) + 1;
-        const T* Mc = M + (size_t)c * cell_stride;
-        const T* M0 = Mc + (size_t)rec_df(pk, 0) * A.blk + (v0 ? k0 : 0);
-        const T* M1 = Mc + (size_t)rec_df(pk, 1) * A.blk + (v1 ? k1 : 0);
-        T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
-#pragma unroll
-        for (int j = 0; j < NDF2; ++j) {
-          a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
-          b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
-          a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
-        }
-        if (pair) {
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            const T up = __shfl_up_sync(0xffffffffu, b0[j], 1);
-            b1[j] = (lane == 0) ? (v1 ? __ldg(x + mf[j] + k1) : T(0)) : up;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) b1[j] = v1 ? __ldg(x + mf[j] + k1) : T(0);
-        }
-#pragma unroll
-        for (int j = 0; j < NDF2; ++j) {
-          if (v0) acc = fmaT(a0[j], b0[j], acc);
-          if (v1) acc = fmaT(a1[j], b1[j], acc);
-        }
+        acc = group_acc<T, NDF2>(A, M, x, cell_stride, l, lane, c, pk, mf, acc);
       }
       if (l < h) {
         if (b)
@@ -225,6 +262,97 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
           y[base + l] = acc;
       }
     }
+  }
+}
+
+// Group record as int4 vectors (NI of them) and its decoding.
+template <int NDF2>
+struct GroupRec {
+  static constexpr int NI = NDF2 > 6 ? 3 : (NDF2 > 2 ? 2 : 1);
+  int4 v[NI];
+  __device__ __forceinline__ void load(const LayoutArgs& A, int g) {
+    const int4* gp4 = reinterpret_cast<const int4*>(A.grp_pack + (size_t)g * A.gp_stride);
+#pragma unroll
+    for (int i = 0; i < NI; ++i) v[i] = __ldg(gp4 + i);
+  }
+  __device__ __forceinline__ void decode(int& c, uint32_t& pk, int* mf) const {
+    c = v[0].x;
+    pk = (uint32_t)v[0].y;
+    int tmp[12];
+    tmp[0] = v[0].z;
+    tmp[1] = v[0].w;
+    if (NI > 1) {
+      tmp[2] = v[NI > 1 ? 1 : 0].x;
+      tmp[3] = v[NI > 1 ? 1 : 0].y;
+      tmp[4] = v[NI > 1 ? 1 : 0].z;
+      tmp[5] = v[NI > 1 ? 1 : 0].w;
+    }
+    if (NI > 2) {
+      tmp[6] = v[NI > 2 ? 2 : 0].x;
+      tmp[7] = v[NI > 2 ? 2 : 0].y;
+    }
+#pragma unroll
+    for (int j = 0; j < NDF2; ++j) mf[j] = tmp[j];
+  }
+};
+
+// The register gather with metadata lookahead: while a warp computes entity
+// column e it already holds the pack of e + nwarp and loads the records of
+// its first two groups, and the pack of e + 2 nwarp, so only the matrix and x
+// loads of each column wait on memory. Same arithmetic (and bits) as
+// lma_gather2.
+template <class T, int NDF2>
+__global__ void __launch_bounds__(256) lma_gather3(LayoutArgs A, const T* __restrict__ M,
+                                                   const T* __restrict__ x, T* __restrict__ y,
+                                                   const T* __restrict__ b, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const size_t cell_stride = (size_t)A.ndf1 * A.blk;
+  const int4 zero = make_int4(0, 0, 0, 0);
+  int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (e >= A.nent) return;
+  int4 ep = __ldg(A.ent_pack + e);
+  int4 epn = e + nwarp < A.nent ? __ldg(A.ent_pack + e + nwarp) : zero;
+  GroupRec<NDF2> r0, r1;
+  if (ep.z < ep.w) r0.load(A, ep.z);
+  if (ep.z + 1 < ep.w) r1.load(A, ep.z + 1);
+  for (; e < A.nent; e += nwarp) {
+    // lookahead loads for the next two columns
+    GroupRec<NDF2> s0, s1;
+    if (epn.z < epn.w) s0.load(A, epn.z);
+    if (epn.z + 1 < epn.w) s1.load(A, epn.z + 1);
+    const int4 ep2 = e + 2 * nwarp < A.nent ? __ldg(A.ent_pack + e + 2 * nwarp) : zero;
+    const int base = ep.x, h = ep.y, g0 = ep.z, g1 = ep.w;
+    for (int l0 = 0; l0 < h; l0 += 32) {
+      const int l = l0 + lane;
+      T acc = T(0);
+      for (int g = g0; g < g1; ++g) {
+        int c;
+        uint32_t pk;
+        int mf[NDF2];
+        if (g == g0) {
+          r0.decode(c, pk, mf);
+        } else if (g == g0 + 1) {
+          r1.decode(c, pk, mf);
+        } else {
+          GroupRec<NDF2> rr;
+          rr.load(A, g);
+          rr.decode(c, pk, mf);
+        }
+        acc = group_acc<T, NDF2>(A, M, x, cell_stride, l, lane, c, pk, mf, acc);
+      }
+      if (l < h) {
+        if (b)
+          y[base + l] = b[base + l] - acc;
+        else
+          y[base + l] = acc;
+      }
+    }
+    ep = epn;
+    epn = ep2;
+    r0 = s0;
+    r1 = s1;
   }
 }
 
@@ -368,6 +496,184 @@ __global__ void __launch_bounds__(256) lma_tma(LayoutArgs A, const T* __restrict
       const unsigned parity = (unsigned)((ik / stages) & 1);
       unsigned spins = 0;
       while (!mbar_try_wait(&bar[s], parity) && ++spins < kWaitLimit) {
+      }
+    }
+  }
+}
+
+// Pipelined gather for columns of at most 32 NP dofs, groups of at most two
+// records. Each warp walks its entity columns with `stages` in flight; a
+// stage holds the column's descriptor, its (cell, df) matrix blocks (bulk
+// copies) and, per record, lane and level, the x values the FMAs need
+// (4/8-byte cp.async), all tracked by the stage's mbarrier. Descriptors are
+// loaded one coalesced request per column, two columns ahead. The compute
+// reads shared memory only, in lma_gather2's order (same bits). err receives
+// 1 if a stage wait ran out (the kernel then drains and returns).
+template <class T, int NDF2, int IPL, int NP>
+__global__ void __launch_bounds__(256) lma_pipe(LayoutArgs A, const T* __restrict__ M,
+                                                const T* __restrict__ x, T* __restrict__ y,
+                                                const T* __restrict__ b, const int* skip,
+                                                int stages, int maxb, int* err) {
+  if (skip && *((volatile const int*)skip)) return;
+  constexpr int GS = 2 + NDF2;
+  constexpr int DS = 32 * IPL;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int nl = A.nlayers;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const size_t mat_b = (size_t)maxb * A.blk * sizeof(T);
+  const size_t xs_b = (size_t)maxb * NDF2 * 32 * NP * sizeof(T);
+  const size_t stage_b = mat_b + xs_b + DS * 4 + 16;
+  unsigned char* wsm = smem_raw + (size_t)wib * stages * stage_b;
+  auto mat_of = [&](int s) { return (T*)(wsm + s * stage_b); };
+  auto xs_of = [&](int s) { return (T*)(wsm + s * stage_b + mat_b); };
+  auto meta_of = [&](int s) { return (int*)(wsm + s * stage_b + mat_b + xs_b); };
+  auto bar_of = [&](int s) { return (uint64_t*)(wsm + s * stage_b + mat_b + xs_b + DS * 4); };
+  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  if (warp0 >= A.nent) return;  // whole warp: no barrier of this warp is used
+  const size_t cell_stride = (size_t)A.ndf1 * A.blk;
+  const unsigned blk_bytes = (unsigned)(A.blk * sizeof(T));
+
+  // descriptor of column e, lane i holding ints IPL i .. IPL i + IPL - 1
+  auto load_desc = [&](int64_t e, int (&d)[IPL]) {
+    if (e < A.nent) {
+      const int* src = A.desc + (size_t)e * DS + lane * IPL;
+      if (IPL == 2) {
+        const int2 v = __ldg(reinterpret_cast<const int2*>(src));
+        d[0] = v.x;
+        d[IPL - 1] = v.y;
+      } else {
+        d[0] = __ldg(src);
+      }
+    }
+  };
+  // int k of a descriptor held across the warp (k warp-uniform)
+  auto D = [&](const int (&d)[IPL], int k) {
+    const int v = (IPL == 2 && (k & 1)) ? d[IPL - 1] : d[0];
+    return __shfl_sync(0xffffffffu, v, k / IPL);
+  };
+
+  // whole warp: start column e's copies into stage s
+  auto issue = [&](int s, const int (&d)[IPL]) {
+    int* mt = meta_of(s);
+#pragma unroll
+    for (int i = 0; i < IPL; ++i) mt[lane * IPL + i] = d[i];
+    const int h = D(d, 1), ng = D(d, 2), nb = D(d, 3);
+    T* xs = xs_of(s);
+    int q = 0;
+    const T* src = M;  // this lane's matrix block (lane < nb)
+    for (int g = 0; g < ng; ++g) {
+      const int c = D(d, 4 + g * GS);
+      const uint32_t pk = (uint32_t)D(d, 5 + g * GS);
+      int mf[NDF2];
+#pragma unroll
+      for (int j = 0; j < NDF2; ++j) mf[j] = D(d, 6 + g * GS + j);
+      for (int r = 0; r < rec_n(pk); ++r, ++q) {
+        if (lane == q) src = M + (size_t)c * cell_stride + (size_t)rec_df(pk, r) * A.blk;
+        const int off = rec_off(pk, r);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const int l = lane + 32 * p, k = l - off;
+          if (l < h && (unsigned)k < (unsigned)nl) {
+#pragma unroll
+            for (int j = 0; j < NDF2; ++j)
+              cp_async<sizeof(T)>(xs + ((size_t)(q * NDF2 + j) * NP + p) * 32 + lane,
+                                  x + mf[j] + k);
+          }
+        }
+      }
+    }
+    cp_async_mbar_arrive(bar_of(s));
+    __syncwarp();
+    if (lane == 0) mbar_expect_tx(bar_of(s), (unsigned)nb * blk_bytes);
+    __syncwarp();
+    if (lane < nb) {
+      fence_proxy_async();
+      bulk_load(mat_of(s) + (size_t)lane * A.blk, src, blk_bytes, bar_of(s));
+    }
+  };
+
+  if (lane == 0) {
+    for (int s = 0; s < stages; ++s) mbar_init(bar_of(s), 1);
+    fence_proxy_async();
+  }
+  __syncwarp();
+  int d0[IPL] = {}, d1[IPL] = {};
+  for (int s = 0; s < stages; ++s) {
+    const int64_t e = warp0 + (int64_t)s * nwarp;
+    if (e >= A.nent) break;
+    int d[IPL] = {};
+    load_desc(e, d);
+    issue(s, d);
+  }
+  load_desc(warp0 + (int64_t)stages * nwarp, d0);
+  load_desc(warp0 + (int64_t)(stages + 1) * nwarp, d1);
+  int64_t it = 0;
+  bool failed = false;
+  for (int64_t e = warp0; e < A.nent; e += nwarp, ++it) {
+    const int s = (int)(it % stages);
+    const unsigned parity = (unsigned)((it / stages) & 1);
+    unsigned spins = 0;
+    while (!mbar_try_wait(bar_of(s), parity)) {
+      if (++spins > kWaitLimit) {
+        failed = true;
+        break;
+      }
+    }
+    if (__any_sync(0xffffffffu, failed)) {
+      failed = true;
+      if (lane == 0) atomicExch(err, 1);
+      break;
+    }
+    const int* mt = meta_of(s);
+    const T* ms = mat_of(s);
+    const T* xs = xs_of(s);
+    const int base = mt[0], h = mt[1], ng = mt[2];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int l = lane + 32 * p;
+      if (l < h) {
+        T acc = T(0);
+        int q = 0;
+        for (int g = 0; g < ng; ++g) {
+          const uint32_t pk = (uint32_t)mt[5 + g * GS];
+          const int k0 = l - rec_off(pk, 0), k1 = l - rec_off(pk, 1);
+          const bool v0 = (unsigned)k0 < (unsigned)nl;
+          const bool v1 = rec_n(pk) > 1 && (unsigned)k1 < (unsigned)nl;
+          const T* s0 = ms + (size_t)q * A.blk + (v0 ? k0 : 0);
+          const T* s1 = v1 ? ms + (size_t)(q + 1) * A.blk + k1 : ms;
+          const T* x0 = xs + ((size_t)q * NDF2 * NP + p) * 32 + lane;
+          const T* x1 = xs + ((size_t)(q + 1) * NDF2 * NP + p) * 32 + lane;
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            if (v0) acc = fmaT(s0[j * nl], x0[j * NP * 32], acc);
+            if (v1) acc = fmaT(s1[j * nl], x1[j * NP * 32], acc);
+          }
+          q += rec_n(pk);
+        }
+        if (b)
+          y[base + l] = b[base + l] - acc;
+        else
+          y[base + l] = acc;
+      }
+    }
+    __syncwarp();
+    if (e + (int64_t)stages * nwarp < A.nent) issue(s, d0);
+#pragma unroll
+    for (int i = 0; i < IPL; ++i) d0[i] = d1[i];
+    load_desc(e + (int64_t)(stages + 2) * nwarp, d1);
+  }
+  if (failed && lane == 0) {
+    // drain: stages of iterations it .. it+stages-1 may still have copies in
+    // flight; wait (bounded) for each before the shared memory is released
+    for (int k = 0; k < stages; ++k) {
+      const int64_t ik = it + k;
+      if (warp0 + ik * nwarp >= A.nent) break;
+      const int s = (int)(ik % stages);
+      const unsigned parity = (unsigned)((ik / stages) & 1);
+      unsigned spins = 0;
+      while (!mbar_try_wait(bar_of(s), parity) && ++spins < kWaitLimit) {
       }
     }
   }
@@ -569,6 +875,31 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
     }
     up((void**)&L->ent_pack, ep.data(), ep.size() * sizeof(int4));
     up((void**)&L->grp_pack, gp.data(), gp.size() * 4);
+    // one-load descriptors for the pipelined gather (groups of at most two
+    // records, at most 64 ints, columns of at most 96 dofs)
+    const int gs = 2 + ndf_from;
+    const int need = 4 + max_groups * gs;
+    if (L->max_nrec <= 2 && need <= 64 && max_h <= 96) {
+      L->desc_ipl = need <= 32 ? 1 : 2;
+      const int ds = 32 * L->desc_ipl;
+      std::vector<int32_t> d((size_t)L->nent * ds, 0);
+      for (int32_t e = 0; e < L->nent; ++e) {
+        int32_t* row = &d[(size_t)e * ds];
+        row[0] = ent_base[e];
+        row[1] = ent_h[e];
+        row[2] = ent_grp[e + 1] - ent_grp[e];
+        int nb = 0;
+        for (int32_t g = ent_grp[e]; g < ent_grp[e + 1]; ++g) {
+          int32_t* gr = row + 4 + (g - ent_grp[e]) * gs;
+          gr[0] = grp_cell[g];
+          gr[1] = (int32_t)grp_rec[g];
+          for (int j = 0; j < ndf_from; ++j) gr[2 + j] = mf0[(size_t)grp_cell[g] * ndf_from + j];
+          nb += rec_n(grp_rec[g]);
+        }
+        row[3] = nb;
+      }
+      up((void**)&L->desc, d.data(), d.size() * 4);
+    }
   }
   return rc;
 }
@@ -582,6 +913,7 @@ void free_layout(lfx_ctx* ctx, lfx_lma_layout* L) {
   dfree(ctx, L->grp_rec, (size_t)L->ngrp * 4);
   dfree(ctx, L->ent_pack, (size_t)L->nent * sizeof(int4));
   dfree(ctx, L->grp_pack, (size_t)L->ngrp * L->gp_stride * 4);
+  dfree(ctx, L->desc, (size_t)L->nent * 32 * L->desc_ipl * 4);
   dfree(ctx, L->map_from, (size_t)L->ncell_2d * L->ndf_from * 4);
   dfree(ctx, L->map_to, (size_t)L->ncell_2d * L->ndf_to * 4);
   free_layout(ctx, L->tlay);
@@ -663,6 +995,86 @@ TmaShape tma_default(const lfx_op* op) {
   return TmaShape{};
 }
 
+// pipelined gather (kernel 4): needs the one-load descriptors
+bool pipe_ok(const lfx_op* op) {
+  const lfx_lma_layout* L = op->lay;
+  if (!L->desc || L->max_nrec > 2 || L->max_h > 96 || L->max_blocks > 32) return false;
+  return L->ndf_from == 1 || L->ndf_from == 6 || L->ndf_from == 8;
+}
+
+TmaShape pipe_shape(const lfx_op* op, int stages, int warps) {
+  TmaShape t;
+  if (!pipe_ok(op) || stages < 1 || warps < 1) return t;
+  const lfx_lma_layout* L = op->lay;
+  const size_t esz = op->precision == LFX_R64 ? 8 : 4;
+  const int np = (L->max_h + 31) / 32;
+  const size_t stage = (size_t)L->max_blocks * op->blk * esz +
+                       (size_t)L->max_blocks * L->ndf_from * 32 * np * esz +
+                       (size_t)32 * L->desc_ipl * 4 + 16;
+  const size_t per_warp = stages * stage;
+  if (per_warp * warps > kTmaSmemMax) return t;
+  t.warps = warps;
+  t.stages = stages;
+  t.smem = per_warp * warps;
+  return t;
+}
+
+TmaShape pipe_default(const lfx_op* op) {
+  for (int stages = 4; stages >= 2; --stages)
+    for (int warps = 4; warps >= 1; warps >>= 1) {
+      TmaShape t = pipe_shape(op, stages, warps);
+      if (t.warps) return t;
+    }
+  return TmaShape{};
+}
+
+template <class T, int N, int IPL, int NP>
+void launch_pipe_t(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const TmaShape& ts,
+                   const void* x, void* y, const void* b, const int* skip) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(lma_pipe<T, N, IPL, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kTmaSmemMax);
+    attr = true;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_pipe<T, N, IPL, NP>, 32 * ts.warps,
+                                                ts.smem);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = (int)std::min<int64_t>(((int64_t)A.nent + ts.warps - 1) / ts.warps,
+                                          (int64_t)ctx->num_sms * per_sm);
+  lma_pipe<T, N, IPL, NP><<<grid, 32 * ts.warps, ts.smem, ctx->stream>>>(
+      A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip, ts.stages,
+      op->lay->max_blocks, ctx->d_err);
+}
+
+template <class T, int N, int IPL>
+void launch_pipe_np(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const TmaShape& ts,
+                    const void* x, void* y, const void* b, const int* skip) {
+  switch ((op->lay->max_h + 31) / 32) {
+    case 1: launch_pipe_t<T, N, IPL, 1>(ctx, op, A, ts, x, y, b, skip); return;
+    case 2: launch_pipe_t<T, N, IPL, 2>(ctx, op, A, ts, x, y, b, skip); return;
+    default: launch_pipe_t<T, N, IPL, 3>(ctx, op, A, ts, x, y, b, skip); return;
+  }
+}
+
+template <class T>
+void launch_pipe(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const TmaShape& ts,
+                 const void* x, void* y, const void* b, const int* skip) {
+  const bool two = op->lay->desc_ipl == 2;
+  switch (op->lay->ndf_from) {
+    case 1: launch_pipe_np<T, 1, 1>(ctx, op, A, ts, x, y, b, skip); return;
+    case 6:
+      if (two) launch_pipe_np<T, 6, 2>(ctx, op, A, ts, x, y, b, skip);
+      else launch_pipe_np<T, 6, 1>(ctx, op, A, ts, x, y, b, skip);
+      return;
+    default:
+      if (two) launch_pipe_np<T, 8, 2>(ctx, op, A, ts, x, y, b, skip);
+      else launch_pipe_np<T, 8, 1>(ctx, op, A, ts, x, y, b, skip);
+      return;
+  }
+}
+
 template <class T, int N>
 void launch_tma(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const TmaShape& ts,
                 const void* x, void* y, const void* b, const int* skip) {
@@ -684,12 +1096,17 @@ void launch_tma(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const TmaSh
       op->lay->max_blocks, ctx->d_err);
 }
 
-// kernel: 0 bulk-copy pipelined (shape ts), 1 register gather, 2 generic
+// kernel: 0 bulk-copy pipelined (shape ts), 1 register gather, 2 generic,
+// 3 register gather with metadata lookahead, 4 copy-staged pipeline (shape ts)
 template <class T>
 void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& ts,
                     const void* x, void* y, const void* b, const int* skip) {
   const lfx_lma_layout* L = op->lay;
   const LayoutArgs A = args_of(L, op->blk);
+  if (kernel == 4) {
+    launch_pipe<T>(ctx, op, A, ts, x, y, b, skip);
+    return;
+  }
   if (kernel == 0) {
     switch (L->ndf_from) {
       case 1: launch_tma<T, 1>(ctx, op, A, ts, x, y, b, skip); return;
@@ -703,6 +1120,13 @@ void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& 
       case 1: lma_gather2<T, 1><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
       case 6: lma_gather2<T, 6><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
       default: lma_gather2<T, 8><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
+    }
+  }
+  if (kernel == 3) {
+    switch (L->ndf_from) {
+      case 1: lma_gather3<T, 1><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
+      case 6: lma_gather3<T, 6><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
+      default: lma_gather3<T, 8><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
     }
   }
   lma_gather<T><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y,
@@ -731,14 +1155,20 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     *ts = tma_default(op);
     if (ts->warps) return;
   }
-  if (ctx->lma_kernel == 1 && gather2_ok(op)) {
-    *kernel = 1;
+  if ((ctx->lma_kernel == 1 || ctx->lma_kernel == 3) && gather2_ok(op)) {
+    *kernel = ctx->lma_kernel;
     return;
+  }
+  if (ctx->lma_kernel == 4 && pipe_ok(op)) {
+    *kernel = 4;
+    *ts = pipe_default(op);
+    if (ts->warps) return;
   }
   if (ctx->lma_kernel < 0 && op->tune_kernel >= 0) {
     *kernel = op->tune_kernel;
     if (*kernel == 0) *ts = tma_shape(op, op->tune_stages, op->tune_warps);
-    if (*kernel != 0 || ts->warps) return;
+    if (*kernel == 4) *ts = pipe_shape(op, op->tune_stages, op->tune_warps);
+    if ((*kernel != 0 && *kernel != 4) || ts->warps) return;
   }
   *kernel = gather2_ok(op) ? 1 : 2;
 }
@@ -886,15 +1316,15 @@ int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y) {
 // Times `reps` applies of one launch configuration on scratch vectors.
 int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps, int32_t reps,
                       float* us) {
-  if (!op || !us || reps < 1 || kernel < 0 || kernel > 2) return LFX_INVALID_ARGUMENT;
+  if (!op || !us || reps < 1 || kernel < 0 || kernel > 4) return LFX_INVALID_ARGUMENT;
   lfx_ctx* ctx = op->ctx;
   const lfx_lma_layout* L = op->lay;
   TmaShape ts;
-  if (kernel == 0) {
-    ts = tma_shape(op, stages, warps);
+  if (kernel == 0 || kernel == 4) {
+    ts = kernel == 0 ? tma_shape(op, stages, warps) : pipe_shape(op, stages, warps);
     if (!ts.warps) return fail(ctx, LFX_NOT_SUPPORTED, "configuration does not fit this operator");
   }
-  if (kernel == 1 && !gather2_ok(op))
+  if ((kernel == 1 || kernel == 3) && !gather2_ok(op))
     return fail(ctx, LFX_NOT_SUPPORTED, "register gather does not fit this operator");
   const size_t esz = op->precision == LFX_R64 ? 8 : 4;
   void *x = nullptr, *y = nullptr;
@@ -924,8 +1354,9 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
 }
 
 // Picks the fastest apply configuration for this operator by timing the
-// candidates (register gather; bulk-copy pipeline with 2..8 stages and 1..8
-// warps per block that fit the shared memory) and keeps it for later applies.
+// candidates (register gather with and without metadata lookahead; bulk-copy
+// pipeline with 2..8 stages and 1..8 warps per block that fit the shared
+// memory) and keeps it for later applies.
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
                     float* us) {
   if (!op) return LFX_INVALID_ARGUMENT;
@@ -945,12 +1376,20 @@ int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, 
     return LFX_OK;
   };
   int rc = LFX_OK;
-  if (gather2_ok(op)) rc = consider(1, 0, 0);
-  else rc = consider(2, 0, 0);
+  if (gather2_ok(op)) {
+    rc = consider(1, 0, 0);
+    if (!rc) rc = consider(3, 0, 0);
+  } else {
+    rc = consider(2, 0, 0);
+  }
   if (!rc && tma_ok(op))
     for (int s : {2, 3, 4, 6, 8})
       for (int w : {1, 2, 4, 8})
         if (!rc && tma_shape(op, s, w).warps) rc = consider(0, s, w);
+  if (!rc && pipe_ok(op))
+    for (int s : {2, 3, 4, 6})
+      for (int w : {2, 4, 8})
+        if (!rc && pipe_shape(op, s, w).warps) rc = consider(4, s, w);
   if (rc) return rc;
   op->tune_kernel = bk;
   op->tune_stages = bs;

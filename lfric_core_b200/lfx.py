@@ -225,7 +225,9 @@ class Context:
         return self.L.lfx_ctx_launch_count(self.h)
 
     def set_apply_kernel(self, which: int):
-        """0: bulk-copy pipelined LMA apply (default), 1: register gather."""
+        """-1: per-operator choice (autotuned, else register gather), 0: bulk-copy
+        pipelined LMA apply, 1: register gather, 3: register gather with
+        metadata lookahead, 4: copy-staged pipeline."""
         self.check(self.L.lfx_ctx_set_apply_kernel(self.h, which))
 
     def check_device_error(self):
@@ -377,7 +379,8 @@ class LmaOperator(_Handle):
         k, s, w, us = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
         self.ctx.check(self.ctx.L.lfx_op_autotune(self.h, reps, C.byref(k), C.byref(s),
                                                    C.byref(w), C.byref(us)))
-        name = {0: "pipeline", 1: "register-gather", 2: "generic"}[k.value]
+        name = {0: "pipeline", 1: "register-gather", 2: "generic",
+                3: "register-gather-lookahead", 4: "staged-pipeline"}[k.value]
         return {"kernel": name, "stages": s.value, "warps": w.value, "us": round(us.value, 2)}
 
     def time_apply(self, kernel: int, stages: int = 0, warps: int = 0, reps: int = 10):

@@ -121,7 +121,7 @@ def test_lma_apply_w2_bitwise(ctx, n, nl):
     assert same(sysd.diag.export_field(), op.diagonal())
 
 
-@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("kernel", [0, 1, 3, 4])
 @pytest.mark.parametrize("space,n,nl,prec", [("w0", 6, 5, 64), ("w2", 8, 7, 64), ("w2", 8, 7, 32),
                                              ("w2", 12, 30, 64), ("w0", 5, 21, 32)])
 def test_apply_kernels_agree(ctx, kernel, space, n, nl, prec):
@@ -144,7 +144,7 @@ def test_apply_kernels_agree(ctx, kernel, space, n, nl, prec):
     if prec == 64:
         assert same(got, o_lma(p).apply(x))
     else:
-        ctx.set_apply_kernel(1 - kernel)
+        ctx.set_apply_kernel(1 if kernel != 1 else 0)
         try:
             op.apply(X, Y)
             other = Y.export_field()
@@ -160,7 +160,9 @@ def test_autotune_keeps_results(ctx):
     x = mg.normal(2, p.undf)
     X, Y = lfx.FieldVector.from_array(ctx, x), lfx.FieldVector(ctx, [p.undf])
     choice = op.autotune(reps=3)
-    assert choice["us"] > 0 and choice["kernel"] in ("pipeline", "register-gather")
+    assert choice["us"] > 0 and choice["kernel"] in ("pipeline", "register-gather",
+                                                     "register-gather-lookahead",
+                                                     "staged-pipeline")
     op.apply(X, Y)
     assert same(Y.export_field(), o_lma(p).apply(x))
 

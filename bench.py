@@ -16,6 +16,10 @@ tridiagonal on the vertical faces and Jacobi on the horizontal faces.
             out every step
   roofline  the FP32 LMA apply (dominant kernel) against the measured HBM peak
   cpu_baseline  the oracle (CPU restatement of the reference) on this host
+  workloads the other configurations: plain FP64 CG on C24x20 W0 against the
+            oracle; 64 right-hand sides of C48x30 W0 with tensor-core (TF32 /
+            BF16) applies in FP64 refinement; 256 batched uneven W0 solves;
+            a Poisson stream of W2 requests served by continuous batching
 
 --impl reference times the oracle port on the host cores instead (the
 reference itself is Fortran + PSyclone and cannot be built here).
@@ -207,6 +211,46 @@ def leg_batched(ctx, lfx, mg, wl, torch, stream):
         "serial_fp64_iterations_max": max(it64),
         "speedup_vs_serial_fp64": round(t_serial / t_batch, 3), "setup_s": round(setup_s, 1),
     }
+
+
+def leg_plain_cg(ctx, lfx, mg, wl, torch, stream, nsolves=50, ncpu=5):
+    """Plain FP64 Jacobi CG on the C24x20 W0 mass+diffusion system
+    (b ~ U[-1,1], x0 = 0, r_tol 1e-8, a_tol 1e-16): device-resident solves
+    against the oracle's CG on the host cores, and the solution compared bit
+    for bit with the oracle's."""
+    from oracle import oracle as orc
+    p = mg.w0_problem(24, 20, seed=1)
+    s = wl.device_w0(ctx, p)
+    cg = lfx.ConjugateGradient(s.op, s.prec, RTOL, 1e-16, 1000)
+    B = lfx.FieldVector.from_array(ctx, p.rhs)
+    X = lfx.FieldVector(ctx, [p.undf])
+    for _ in range(3):
+        X.set_scalar(0.0)
+        cg.apply(X, B)
+    ctx.synchronize()
+    ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    ev[0].record(stream)
+    for _ in range(nsolves):
+        X.set_scalar(0.0)
+        info = cg.apply(X, B)
+    ev[1].record(stream)
+    ctx.synchronize()
+    t = ev[0].elapsed_time(ev[1]) / 1e3
+    x_gpu = X.export_field()
+    npc, cic = p.mesh.colour_lookup()
+    o = orc.LmaOperator(p.ncell_2d, p.nlayers, 8, 8, p.map, p.map, p.undf, p.undf, p.lma, npc, cic)
+    od = orc.Preconditioner.diagonal(o.diagonal())
+    times = []
+    for _ in range(ncpu):
+        t0 = time.perf_counter()
+        x_cpu, oi = orc.solve("cg", o, od, p.rhs, r_tol=RTOL, a_tol=1e-16, max_iter=1000)
+        times.append(time.perf_counter() - t0)
+    return {"workload": "C24x20 W0 mass+diffusion, Jacobi CG, FP64, b ~ U[-1,1], 1e-8",
+            "undf": p.undf, "iterations": info.iterations, "oracle_iterations": oi.iterations,
+            "gpu_solves_per_s": round(nsolves / t, 2), "gpu_ms_per_solve": round(1e3 * t / nsolves, 4),
+            "cpu_oracle_solves_per_s": round(ncpu / sum(times), 2), "cpu_threads": os.cpu_count(),
+            "solution_bitwise_equal_to_oracle": bool(np.array_equal(x_gpu.view(np.int64),
+                                                                     x_cpu.view(np.int64)))}
 
 
 def leg_multi_rhs(ctx, lfx, mg, wl, torch, stream, n=48, nl=30, nrhs=64):
@@ -553,6 +597,7 @@ def main():
         cb = cpu_baseline(p, args.cpu_sample)
     extra = {}
     if not args.quick:
+        extra["plain_cg_w0"] = leg_plain_cg(ctx, lfx, mg, wl, torch, stream)
         extra["multi_rhs_w0"] = leg_multi_rhs(ctx, lfx, mg, wl, torch, stream)
         extra["batched_uneven_w0"] = leg_batched(ctx, lfx, mg, wl, torch, stream)
         extra["serving_w2"] = leg_serving(ctx, lfx, mg, wl)

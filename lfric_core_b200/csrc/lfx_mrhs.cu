@@ -114,16 +114,16 @@ struct MrhsArgs {
   int nl;
 };
 
-// Rounding on the integer pipe (the conversion instructions share a narrow
-// pipe): TF32 round-half-away, BF16 round-half-even of two values packed.
+// TF32 rounding (half away from zero) on the integer pipe; BF16: one
+// round-to-nearest-even conversion of two values into a packed pair (lo in
+// the low half).
 __device__ __forceinline__ uint32_t tf32_bits(float x) {
   return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
 }
 __device__ __forceinline__ uint32_t bf16_pair(float lo, float hi) {
-  uint32_t a = __float_as_uint(lo), b = __float_as_uint(hi);
-  a += 0x7FFFu + ((a >> 16) & 1u);
-  b += 0x7FFFu + ((b >> 16) & 1u);
-  return __byte_perm(a, b, 0x7632);
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
 }
 // W consecutive floats (W = 2, 4 or 8; aligned to W)
 template <int W, class P>

@@ -151,3 +151,113 @@ def refined_gmres(sys32: DeviceSystem, gcrk=10, inner_rtol=1e-4, inner_cycles=50
     outer = lfx.RefinedSolver(sys32.op64, inner, inner_rtol, r_tol, 0.0, max_outer)
     outer._inner = inner
     return outer
+
+
+# ------------------------------------------------------------------ profiling runs
+def _run_apply(args):
+    p = mg.w2_problem(args.n, args.nl, seed=2) if args.space == "w2" else mg.w0_problem(
+        args.n, args.nl, seed=1)
+    ctx = lfx.Context(0)
+    prec = lfx.R32 if args.precision == 32 else lfx.R64
+    op = _lma(ctx, p, prec)
+    x = lfx.FieldVector.from_array(ctx, mg.normal(3, p.undf), prec)
+    y = lfx.FieldVector(ctx, [p.undf], prec)
+    for k in [int(v) for v in args.kernels.split(",")]:
+        ctx.set_apply_kernel(k)
+        for _ in range(args.reps):
+            op.apply(x, y)
+        ctx.synchronize()
+    ctx.set_apply_kernel(-1)
+    ctx.check_device_error()
+    print("applies done", flush=True)
+
+
+def _run_time_apply(args):
+    p = mg.w2_problem(args.n, args.nl, seed=2) if args.space == "w2" else mg.w0_problem(
+        args.n, args.nl, seed=1)
+    ctx = lfx.Context(0)
+    op64 = _lma(ctx, p, lfx.R64)
+    op32 = op64.like(p.lma, lfx.R32)
+    configs = [tuple(int(v) for v in c.split(":")) for c in args.configs.split(",")]
+    for name, op in (("fp32", op32), ("fp64", op64)):
+        for k, st, w in configs:
+            us = op.time_apply(k, st, w, args.reps)
+            print(f"{name} kernel {k} stages {st} warps {w}: "
+                  + ("does not fit" if us is None else f"{us:.2f} us"), flush=True)
+
+
+def _run_mrhs(args):
+    import torch
+    ctx = lfx.Context(0)
+    p = mg.w0_problem(args.n, args.nl, seed=1, rhs="normal")
+    s = device_w0(ctx, p)
+    kind = lfx.MRHS_BF16 if args.kind == "bf16" else lfx.MRHS_TF32
+    m = lfx.MultiRhsOperator(s.op, kind, args.nrhs)
+    tune = m.autotune(reps=args.autotune_reps)
+    x = torch.randn(p.undf, args.nrhs, device="cuda")
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    for _ in range(args.reps):
+        m.apply(x.data_ptr(), y.data_ptr())
+    ctx.synchronize()
+    print(m.info(), tune, flush=True)
+
+
+def _run_batch_w2(args):
+    ctx = lfx.Context(0)
+    s = batch_system(ctx, args.n, args.nl, args.seed, mg.W2)
+    cg = s.cg64(1e-10)
+    x = lfx.FieldVector(ctx, [s.undf])
+    x.set_scalar(0.0)
+    info = cg.apply(x, s.b)
+    b = lfx.Batch(ctx, 6, 1, s.undf, s.entities, s.columns, 4)
+    x2 = lfx.FieldVector(ctx, [s.undf])
+    x2.set_scalar(0.0)
+    slot = b.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x2, 1e-10, 20000)
+    while b.step() < 1:
+        pass
+    ctx.synchronize()
+    print("fp64 cg iterations", info.iterations, "batch iterations", b.slot(slot)[2].iterations,
+          flush=True)
+
+
+def main(argv=None):
+    """One named workload, run once, for profilers:
+    ``python -m lfric_core_b200.workloads apply|time-apply|mrhs|batch-w2 [options]``."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m lfric_core_b200.workloads")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    a = sub.add_parser("apply", help="LMA applies with each forced kernel in turn")
+    a.add_argument("--space", choices=["w0", "w2"], default="w2")
+    a.add_argument("--n", type=int, default=96)
+    a.add_argument("--nl", type=int, default=30)
+    a.add_argument("--precision", type=int, choices=[32, 64], default=32)
+    a.add_argument("--kernels", default="1,4", help="comma-separated apply kernels (0,1,3,4)")
+    a.add_argument("--reps", type=int, default=2)
+    t = sub.add_parser("time-apply", help="time LMA apply configurations (FP32 and FP64)")
+    t.add_argument("--space", choices=["w0", "w2"], default="w2")
+    t.add_argument("--n", type=int, default=96)
+    t.add_argument("--nl", type=int, default=30)
+    t.add_argument("--configs", default="1:0:0,3:0:0,0:2:4,4:2:8",
+                   help="comma-separated kernel:stages:warps")
+    t.add_argument("--reps", type=int, default=50)
+    m = sub.add_parser("mrhs", help="tensor-core multi-RHS applies of the W0 operator")
+    m.add_argument("--n", type=int, default=48)
+    m.add_argument("--nl", type=int, default=30)
+    m.add_argument("--kind", choices=["tf32", "bf16"], default="tf32")
+    m.add_argument("--nrhs", type=int, default=64)
+    m.add_argument("--autotune-reps", type=int, default=1)
+    m.add_argument("--reps", type=int, default=2)
+    b = sub.add_parser("batch-w2", help="one W2 solve by FP64 CG and by the batch engine")
+    b.add_argument("--n", type=int, default=94)
+    b.add_argument("--nl", type=int, default=64)
+    b.add_argument("--seed", type=int, default=505)
+    args = ap.parse_args(argv)
+    {"apply": _run_apply, "time-apply": _run_time_apply, "mrhs": _run_mrhs,
+     "batch-w2": _run_batch_w2}[args.cmd](args)
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

@@ -200,14 +200,26 @@ int lfx_prec_destroy(lfx_prec* p);
 enum {
   LFX_SOLVER_CG = 1,        /* cg_solve       :495-592  */
   LFX_SOLVER_BICGSTAB = 2,  /* bicgstab_solve :645-779  */
-  LFX_SOLVER_GMRES = 3      /* gmres_solve    :830-1003 */
+  LFX_SOLVER_GMRES = 3,     /* gmres_solve    :830-1003 */
+  /* Flexible GMRES and GCR run their vector operations, applies and
+   * preconditioners on the device in the reference's order, with the short
+   * scalar recurrences on the host (each inner product returns to the host,
+   * as in the reference). As in the reference, FGMRES starts its residual
+   * from b (it assumes a zero initial guess) and adds the correction to x;
+   * GCR starts from dx = P b, measures against ||b||, and reports
+   * non-convergence (with monitoring on) as LFX_NOT_CONVERGED whatever
+   * fail_on_non_converged says, as the reference logs it as an error in both
+   * branches. iterations = restart cycles; GCR's inner_iterations = the inner
+   * step of the last check. */
+  LFX_SOLVER_FGMRES = 4,    /* fgmres_solve   :1055-1237 */
+  LFX_SOLVER_GCR = 5        /* gcr_solve      :1288-1408 */
 };
 
 typedef struct {
   double r_tol;                  /* relative tolerance                       */
   double a_tol;                  /* absolute tolerance                       */
   int32_t max_iter;              /* iterations (CG/BiCGStab) or cycles (GMRES) */
-  int32_t gcrk;                  /* GMRES restart length                     */
+  int32_t gcrk;                  /* GMRES / FGMRES / GCR restart length      */
   int32_t monitor_convergence;   /* 0: run exactly max_iter, as the reference */
   int32_t fail_on_non_converged; /* 1: return LFX_NOT_CONVERGED              */
 } lfx_solver_cfg;

@@ -56,10 +56,12 @@ def build_lfx(force: bool = False) -> Path:
         for src in CU_SOURCES:
             obj = obj_dir / (src.stem + ".o")
             if force or _stale(obj, [src] + CU_HEADERS):
-                # -fmad=false: only the explicit fma() calls in the sources are
-                # fused, so FP64 results match the CPU oracle bit for bit.
+                # -fmad=false (device) and -ffp-contract=off (host): only the
+                # explicit fma() calls in the sources are fused, so FP64 results
+                # match the CPU oracle bit for bit.
                 _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--extended-lambda",
-                      "-Xcompiler", "-fPIC", "-Xptxas", "-v" if os.environ.get("LFX_PTXAS_V") else "-O3",
+                      "-Xcompiler", "-fPIC,-ffp-contract=off",
+                      "-Xptxas", "-v" if os.environ.get("LFX_PTXAS_V") else "-O3",
                       f"-I{INCLUDE}", f"-I{CSRC}", "-c", src, "-o", obj])
             objs.append(obj)
         _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", out,

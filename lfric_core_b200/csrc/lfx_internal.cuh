@@ -353,6 +353,14 @@ struct lfx_prec {
 
 namespace lfx {
 int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* skip);
+// flexible GMRES / GCR over the C ABI's vector calls (lfx_solver_flex.cu);
+// work: FGMRES s, w, dx, Ax, res, v[gcrk], Pv[gcrk]; GCR dx, res, Ax, v, Pv
+int fgmres_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,
+                const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+                lfx_solve_info* info);
+int gcr_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,
+             const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+             lfx_solve_info* info);
 int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int64_t n,
                     const int* skip);
 void timing_begin(lfx_ctx* ctx, int32_t precision);

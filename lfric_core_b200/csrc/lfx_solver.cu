@@ -71,6 +71,7 @@ struct lfx_solver {
   double* d_gm = nullptr;       // gmres: H, negH, g, u, cs, sn
   bool inner_mode = false;      // GMRES used as the inner solve of a refinement
   std::vector<GraphEntry> graphs;
+  std::vector<lfx_vec*> hv;  // FGMRES / GCR work vectors
   // refined solver
   lfx_solver* inner = nullptr;
   double inner_rtol = 0.0;
@@ -782,6 +783,7 @@ int free_solver(lfx_solver* s) {
   if (s->r32) lfx_vec_destroy(s->r32);
   if (s->d32) lfx_vec_destroy(s->d32);
   if (s->d_r64) dfree(ctx, s->d_r64, s->n * 8);
+  for (lfx_vec* v : s->hv) lfx_vec_destroy(v);
   delete s;
   return LFX_OK;
 }
@@ -883,7 +885,7 @@ int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
                       const lfx_solver_cfg* cfg, lfx_solver** out) {
   if (!ctx || !op || !prec || !cfg || !out) return LFX_INVALID_ARGUMENT;
   *out = nullptr;
-  if (kind != LFX_SOLVER_CG && kind != LFX_SOLVER_BICGSTAB && kind != LFX_SOLVER_GMRES)
+  if (kind < LFX_SOLVER_CG || kind > LFX_SOLVER_GCR)
     return fail(ctx, LFX_INVALID_ARGUMENT, "unknown solver kind");
   if (op->lay->undf_to != op->lay->undf_from)
     return fail(ctx, LFX_INVALID_ARGUMENT, "Krylov solve needs a square operator");
@@ -895,8 +897,32 @@ int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
   if (prec->kind == PREC_CMA && prec->max_row >= op->lay->undf_to)
     return fail(ctx, LFX_TYPE_MISMATCH, "CMA rows fall outside the operator's space");
   if (cfg->max_iter < 1) return fail(ctx, LFX_INVALID_ARGUMENT, "max_iter must be positive");
-  if (kind == LFX_SOLVER_GMRES && (cfg->gcrk < 1 || cfg->gcrk > MAX_GCRK))
+  if (kind >= LFX_SOLVER_GMRES && (cfg->gcrk < 1 || cfg->gcrk > MAX_GCRK))
     return fail(ctx, LFX_INVALID_ARGUMENT, "gcrk must be in 1..64");
+  if (kind == LFX_SOLVER_FGMRES || kind == LFX_SOLVER_GCR) {
+    lfx_solver* s = new lfx_solver();
+    s->ctx = ctx;
+    s->kind = kind;
+    s->op = op;
+    s->prec = prec;
+    s->cfg = *cfg;
+    s->precision = op->precision;
+    s->n = op->lay->undf_to;
+    const int nv = (kind == LFX_SOLVER_FGMRES ? 5 : 3) + 2 * cfg->gcrk;
+    int64_t n = s->n;
+    int rc = LFX_OK;
+    for (int i = 0; i < nv && !rc; ++i) {
+      lfx_vec* v = nullptr;
+      rc = lfx_vec_create(ctx, 1, &n, s->precision, &v);
+      if (!rc) s->hv.push_back(v);
+    }
+    if (rc) {
+      free_solver(s);
+      return rc;
+    }
+    *out = s;
+    return LFX_OK;
+  }
   lfx_solver* s = new lfx_solver();
   s->ctx = ctx;
   s->kind = kind;
@@ -969,6 +995,22 @@ int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info
     return fail(ctx, LFX_TYPE_MISMATCH, "vector length does not match the operator");
   if (x->data[0] == b->data[0]) return fail(ctx, LFX_INVALID_ARGUMENT, "x and b must differ");
   int rc;
+  if (s->kind == LFX_SOLVER_FGMRES || s->kind == LFX_SOLVER_GCR) {
+    rc = s->kind == LFX_SOLVER_FGMRES ? fgmres_host(s->op, s->prec, s->cfg, s->hv, x, b, info)
+                                      : gcr_host(s->op, s->prec, s->cfg, s->hv, x, b, info);
+    if (!rc) rc = lfx_ctx_check_device_error(ctx);
+    if (rc) {
+      info->status = rc;
+      return rc;
+    }
+    if (info->status == LFX_NAN_DETECTED) return fail(ctx, LFX_NAN_DETECTED, "NaN in residual");
+    const bool must_fail = s->kind == LFX_SOLVER_GCR || s->cfg.fail_on_non_converged;
+    if (!info->converged && s->cfg.monitor_convergence && must_fail) {
+      info->status = LFX_NOT_CONVERGED;
+      return fail(ctx, LFX_NOT_CONVERGED, "solver did not converge");
+    }
+    return LFX_OK;
+  }
   if (s->kind == 100) {
     rc = refined_run(s, x, b, info);
   } else {

@@ -35,7 +35,7 @@ STATUS = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN_DETECTED", 3: "OUT_OF_MEMORY",
           4: "INVALID_ARGUMENT", 5: "TYPE_MISMATCH", 6: "TIMEOUT", 7: "CUDA_ERROR",
           8: "NOT_SUPPORTED"}
 R64, R32 = 64, 32
-CG, BICGSTAB, GMRES_KIND = 1, 2, 3
+CG, BICGSTAB, GMRES_KIND, FGMRES_KIND, GCR_KIND = 1, 2, 3, 4, 5
 
 i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
@@ -648,6 +648,30 @@ class BiCGStab(_KrylovSolver):
 class GMRES(_KrylovSolver):
     """gmres_type(lin_op, prec, gcrk, r_tol, a_tol, max_iter, ...)"""
     KIND = GMRES_KIND
+
+    def __init__(self, lin_op, prec, gcrk, r_tol, a_tol, max_iter, monitor_convergence=True,
+                 fail_on_non_converged=False):
+        super().__init__(lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence,
+                         fail_on_non_converged, gcrk=gcrk)
+
+
+class FGMRES(_KrylovSolver):
+    """fgmres_type(lin_op, prec, gcrk, r_tol, a_tol, max_iter, ...): flexible
+    GMRES; like the reference it starts from b (zero initial guess assumed)
+    and adds the correction to x."""
+    KIND = FGMRES_KIND
+
+    def __init__(self, lin_op, prec, gcrk, r_tol, a_tol, max_iter, monitor_convergence=True,
+                 fail_on_non_converged=False):
+        super().__init__(lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence,
+                         fail_on_non_converged, gcrk=gcrk)
+
+
+class GCR(_KrylovSolver):
+    """gcr_type(lin_op, prec, gcrk, r_tol, a_tol, max_iter, ...): right
+    preconditioned GCR(gcrk); non-convergence (monitored) always raises, as
+    the reference logs it as an error in both branches."""
+    KIND = GCR_KIND
 
     def __init__(self, lin_op, prec, gcrk, r_tol, a_tol, max_iter, monitor_convergence=True,
                  fail_on_non_converged=False):

@@ -637,3 +637,194 @@ done:
   free(res);
   return 0;
 }
+
+/* Givens reduction of the (gcrk+1) x gcrk Hessenberg matrix and back
+ * substitution, shared by or_fgmres: sci_iterative_solver_mod.f90:1153-1182
+ * (the same steps as gmres_solve :931-960). */
+static void hessenberg_solve(double* h, double* g, double* u, int32_t gcrk) {
+#define H(i, j) h[((i) - 1) + (int64_t)(gcrk + 1) * ((j) - 1)]
+  for (int32_t iv = 1; iv <= gcrk; ++iv) {
+    const double nrm = sqrt(fma(H(iv, iv), H(iv, iv), H(iv + 1, iv) * H(iv + 1, iv)));
+    const double si = H(iv + 1, iv) / nrm;
+    const double ci = H(iv, iv) / nrm;
+    const double p = fma(ci, g[iv - 1], si * g[iv]);
+    const double q = fma(-si, g[iv - 1], ci * g[iv]);
+    g[iv - 1] = p;
+    g[iv] = q;
+    for (int32_t ivj = iv; ivj <= gcrk; ++ivj) {
+      const double h1 = fma(ci, H(iv, ivj), si * H(iv + 1, ivj));
+      const double h2 = fma(-si, H(iv, ivj), ci * H(iv + 1, ivj));
+      H(iv, ivj) = h1;
+      H(iv + 1, ivj) = h2;
+    }
+  }
+  u[gcrk - 1] = g[gcrk - 1] / H(gcrk, gcrk);
+  for (int32_t iv = gcrk - 1; iv >= 1; --iv) {
+    u[iv - 1] = g[iv - 1];
+    for (int32_t ivj = iv + 1; ivj <= gcrk; ++ivj) u[iv - 1] = fma(-H(iv, ivj), u[ivj - 1], u[iv - 1]);
+    u[iv - 1] = u[iv - 1] / H(iv, iv);
+  }
+#undef H
+}
+
+/* fgmres_solve, sci_iterative_solver_mod.f90:1055-1237, monitor_convergence on */
+int or_fgmres(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t gcrk,
+              double r_tol, double a_tol, int32_t max_iter, or_info* info) {
+  double *s = vnew(n), *w = vnew(n), *dx = vnew(n), *Ax = vnew(n), *res = vnew(n);
+  double** v = (double**)calloc((size_t)gcrk, sizeof(double*));
+  double** Pv = (double**)calloc((size_t)gcrk, sizeof(double*));
+  double* h = (double*)calloc((size_t)(gcrk + 1) * gcrk, sizeof(double));
+  double* g = (double*)calloc((size_t)gcrk + 1, sizeof(double));
+  double* u = (double*)calloc((size_t)gcrk, sizeof(double));
+#define H(i, j) h[((i) - 1) + (int64_t)(gcrk + 1) * ((j) - 1)]
+  double beta, err = 0.0, sc_err;
+  int32_t iv, ivj, iter;
+  memset(info, 0, sizeof *info);
+  for (iv = 0; iv < gcrk; ++iv) {
+    v[iv] = vnew(n);
+    Pv[iv] = vnew(n);
+  }
+  /* :1079-1087 dx = 0, Ax = 0, res = b */
+  or_setval_x(res, b, n);
+  sc_err = vnorm(res, n);
+  info->initial_norm = sc_err;
+  if (sc_err < EPS_RDEF) { /* :1092-1097, returns before x += dx */
+    info->converged = 1;
+    info->final_norm = sc_err;
+    goto done;
+  }
+  sc_err = fmax(sc_err, a_tol);
+  or_setval_x(s, res, n);
+  beta = vnorm(s, n);
+  or_setval_x(v[0], s, n);
+  or_inc_a_times_x(1.0 / beta, v[0], n);
+  for (iv = 0; iv <= gcrk; ++iv) g[iv] = 0.0;
+  g[0] = beta;
+  for (iter = 1; iter <= max_iter; ++iter) {
+    for (iv = 1; iv <= gcrk; ++iv) { /* :1134-1151 */
+      or_prec_apply(P, v[iv - 1], Pv[iv - 1]);
+      or_op_apply(A, Pv[iv - 1], s);
+      info->applies++;
+      or_setval_x(w, s, n);
+      for (ivj = 1; ivj <= iv; ++ivj) {
+        H(ivj, iv) = or_dot(v[ivj - 1], w, n);
+        or_inc_x_plus_by(w, -H(ivj, iv), v[ivj - 1], n);
+      }
+      H(iv + 1, iv) = vnorm(w, n);
+      if (iv < gcrk) {
+        or_setval_x(v[iv], w, n);
+        or_inc_a_times_x(1.0 / H(iv + 1, iv), v[iv], n);
+      }
+    }
+    hessenberg_solve(h, g, u, gcrk);
+    for (iv = 1; iv <= gcrk; ++iv) or_inc_x_plus_by(dx, u[iv - 1], Pv[iv - 1], n); /* :1185-1188 */
+    or_op_apply(A, dx, Ax); /* :1191-1193 */
+    info->applies++;
+    or_setval_x(res, Ax, n);
+    or_inc_ax_plus_y(-1.0, res, b, n);
+    beta = vnorm(res, n);
+    err = beta / sc_err;
+    info->iterations = iter;
+    info->final_norm = beta;
+    info->final_rel = err;
+    if (err < r_tol) {
+      info->converged = 1;
+      break;
+    }
+    or_setval_x(s, res, n); /* :1208-1213 */
+    or_setval_c(v[0], 0.0, n);
+    or_inc_x_plus_by(v[0], 1.0 / beta, s, n);
+    for (iv = 0; iv <= gcrk; ++iv) g[iv] = 0.0;
+    g[0] = beta;
+  }
+  or_inc_x_plus_by(x, 1.0, dx, n); /* :1228 */
+done:
+#undef H
+  for (iv = 0; iv < gcrk; ++iv) {
+    free(v[iv]);
+    free(Pv[iv]);
+  }
+  free(v);
+  free(Pv);
+  free(h);
+  free(g);
+  free(u);
+  free(s);
+  free(w);
+  free(dx);
+  free(Ax);
+  free(res);
+  return 0;
+}
+
+/* gcr_solve, sci_iterative_solver_mod.f90:1288-1408, monitor_convergence on */
+int or_gcr(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t gcrk,
+           double r_tol, double a_tol, int32_t max_iter, or_info* info, int32_t* iv_final) {
+  double *dx = vnew(n), *res = vnew(n), *Ax = vnew(n);
+  double** v = (double**)calloc((size_t)gcrk, sizeof(double*));
+  double** Pv = (double**)calloc((size_t)gcrk, sizeof(double*));
+  double alpha, beta, err = 0.0, sc_err, rn = 0.0;
+  int32_t iv, ivj, iter, ivf = 0;
+  memset(info, 0, sizeof *info);
+  for (iv = 0; iv < gcrk; ++iv) {
+    v[iv] = vnew(n);
+    Pv[iv] = vnew(n);
+  }
+  /* :1321-1327 dx = P b, res = b - A dx */
+  or_prec_apply(P, b, dx);
+  or_op_apply(A, dx, Ax);
+  info->applies++;
+  or_setval_x(res, b, n);
+  or_inc_x_plus_by(res, -1.0, Ax, n);
+  sc_err = vnorm(b, n); /* :1330 */
+  info->initial_norm = sc_err;
+  if (sc_err < EPS_RDEF) {
+    info->converged = 1;
+    info->final_norm = sc_err;
+    goto done;
+  }
+  sc_err = fmax(sc_err, a_tol);
+  for (iter = 1; iter <= max_iter; ++iter) {
+    for (iv = 1; iv <= gcrk; ++iv) { /* :1356-1380 */
+      or_prec_apply(P, res, Pv[iv - 1]);
+      or_op_apply(A, Pv[iv - 1], v[iv - 1]);
+      info->applies++;
+      for (ivj = 1; ivj <= iv - 1; ++ivj) {
+        alpha = or_dot(v[iv - 1], v[ivj - 1], n);
+        or_inc_x_plus_by(v[iv - 1], -alpha, v[ivj - 1], n);
+        or_inc_x_plus_by(Pv[iv - 1], -alpha, Pv[ivj - 1], n);
+      }
+      alpha = vnorm(v[iv - 1], n);
+      beta = 1.0 / alpha;
+      or_inc_a_times_x(beta, v[iv - 1], n);
+      or_inc_a_times_x(beta, Pv[iv - 1], n);
+      alpha = or_dot(res, v[iv - 1], n);
+      or_inc_x_plus_by(dx, alpha, Pv[iv - 1], n);
+      or_inc_x_plus_by(res, -alpha, v[iv - 1], n);
+      rn = vnorm(res, n);
+      err = rn / sc_err;
+      ivf = iv;
+      if (err < r_tol) break;
+    }
+    info->iterations = iter;
+    info->final_norm = rn;
+    info->final_rel = err;
+    if (err < r_tol) {
+      info->converged = 1;
+      break;
+    }
+  }
+  or_inc_x_plus_by(x, 1.0, dx, n); /* :1400 */
+done:
+  if (iv_final) *iv_final = ivf;
+  for (iv = 0; iv < gcrk; ++iv) {
+    free(v[iv]);
+    free(Pv[iv]);
+  }
+  free(v);
+  free(Pv);
+  free(dx);
+  free(res);
+  free(Ax);
+  return 0;
+}

@@ -120,6 +120,16 @@ int or_bicgstab(or_op* A, or_prec* P, double* x, const double* b, int64_t n, dou
                 double a_tol, int32_t max_iter, or_info* info);
 int or_gmres(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t gcrk,
              double r_tol, double a_tol, int32_t max_iter, or_info* info);
+/* fgmres_solve (sci_iterative_solver_mod.f90:1055-1237): flexible GMRES with
+ * the preconditioned basis Pv kept; the residual starts from b (the reference
+ * assumes a zero initial guess) and x += dx at the end. iterations = cycles. */
+int or_fgmres(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t gcrk,
+              double r_tol, double a_tol, int32_t max_iter, or_info* info);
+/* gcr_solve (sci_iterative_solver_mod.f90:1288-1408): right-preconditioned
+ * GCR(gcrk) with dx0 = P b, relative to ||b||. iterations = outer restarts;
+ * *iv_final = the inner step at the last check. */
+int or_gcr(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t gcrk,
+           double r_tol, double a_tol, int32_t max_iter, or_info* info, int32_t* iv_final);
 
 #ifdef __cplusplus
 }

@@ -78,6 +78,8 @@ def lib():
                                          C.c_double, C.c_int32, C.POINTER(Info)]
         L.or_gmres.argtypes = [C.c_void_p, C.c_void_p, f64p, f64p, C.c_int64, C.c_int32,
                                C.c_double, C.c_double, C.c_int32, C.POINTER(Info)]
+        L.or_fgmres.argtypes = L.or_gmres.argtypes
+        L.or_gcr.argtypes = L.or_gmres.argtypes + [C.POINTER(C.c_int32)]
         _lib = L
     return _lib
 
@@ -147,7 +149,8 @@ class Preconditioner:
 
 
 def solve(kind, op, prec, b, x0=None, r_tol=1e-8, a_tol=1e-16, max_iter=1000, gcrk=10):
-    """Run the oracle's cg / bicgstab / gmres; returns (x, Info)."""
+    """Run the oracle's cg / bicgstab / gmres / fgmres / gcr; returns (x, Info)
+    (for gcr, Info gains iv_final: the inner step of the last check)."""
     n = len(b)
     x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
     b = np.ascontiguousarray(b, dtype=np.float64)
@@ -159,6 +162,12 @@ def solve(kind, op, prec, b, x0=None, r_tol=1e-8, a_tol=1e-16, max_iter=1000, gc
         L.or_bicgstab(op.h, prec.h, x, b, n, r_tol, a_tol, max_iter, C.byref(info))
     elif kind == "gmres":
         L.or_gmres(op.h, prec.h, x, b, n, gcrk, r_tol, a_tol, max_iter, C.byref(info))
+    elif kind == "fgmres":
+        L.or_fgmres(op.h, prec.h, x, b, n, gcrk, r_tol, a_tol, max_iter, C.byref(info))
+    elif kind == "gcr":
+        ivf = C.c_int32()
+        L.or_gcr(op.h, prec.h, x, b, n, gcrk, r_tol, a_tol, max_iter, C.byref(info), C.byref(ivf))
+        info.iv_final = ivf.value
     else:
         raise ValueError(kind)
     return x, info

@@ -288,6 +288,53 @@ def test_gmres_w2_cma_parity(ctx, n, nl):
     assert same(X.export_field(), x_o)
 
 
+@pytest.mark.parametrize("kind", ["fgmres", "gcr"])
+@pytest.mark.parametrize("space", ["w0", "w2"])
+def test_flexible_solvers_parity(ctx, kind, space):
+    """FGMRES and GCR (device vector calls, host recurrences) equal the
+    oracle's restatements: same cycles, bit-identical solution."""
+    if space == "w0":
+        p = mg.w0_problem(10, 8, seed=5)
+        sysd = wl.device_w0(ctx, p)
+        op = o_lma(p)
+        P = orc.Preconditioner.diagonal(op.diagonal())
+    else:
+        p = mg.w2_problem(12, 15, seed=5)
+        sysd = wl.device_w2(ctx, p)
+        op = o_lma(p)
+        P, _ = o_w2_prec(p, op)
+    x0 = mg.normal(9, p.undf)
+    x_o, info_o = orc.solve(kind, op, P, p.rhs, x0=x0, r_tol=1e-9, a_tol=1e-16, max_iter=300,
+                            gcrk=8)
+    cls = lfx.FGMRES if kind == "fgmres" else lfx.GCR
+    s = cls(sysd.op, sysd.prec, 8, 1e-9, 1e-16, 300)
+    X, B = sysd.vector(x0), sysd.vector(p.rhs)
+    info = s.apply(X, B)
+    assert info.converged and info_o.converged
+    assert info.iterations == info_o.iterations
+    if kind == "gcr":
+        assert info.inner_iterations == info_o.iv_final
+    assert info.final_rel == info_o.final_rel
+    assert same(X.export_field(), x_o)
+
+
+def test_gcr_nonconvergence_always_fails(ctx):
+    """gcr_solve logs non-convergence as an error in both branches, so the
+    device GCR returns LFX_NOT_CONVERGED even without fail_on_non_converged;
+    FGMRES follows fail_on_non_converged."""
+    p = mg.w2_problem(8, 6, seed=3)
+    sysd = wl.device_w2(ctx, p)
+    X, B = sysd.vector(), sysd.vector(p.rhs)
+    with pytest.raises(lfx.LfxError) as e:
+        lfx.GCR(sysd.op, sysd.prec, 2, 1e-12, 0.0, 1).apply(X, B)
+    assert e.value.status == 1
+    X.set_scalar(0.0)
+    info = lfx.FGMRES(sysd.op, sysd.prec, 2, 1e-12, 0.0, 1).apply(X, B)
+    assert not info.converged
+    with pytest.raises(lfx.LfxError):
+        lfx.FGMRES(sysd.op, sysd.prec, 2, 1e-12, 0.0, 1, fail_on_non_converged=True).apply(X, B)
+
+
 def test_mixed_precision_refinement(ctx):
     """FP32 GMRES inside FP64 refinement reaches the 1e-8 true FP64 residual;
     the solution agrees with the FP64 oracle within the solve tolerance."""

@@ -116,3 +116,33 @@ def test_transpose_apply_is_adjoint():
     u = rng.standard_normal(q.undf)
     w = rng.standard_normal(u3)
     np.testing.assert_allclose(w @ D.apply(u), u @ Dt.apply(w), rtol=1e-12)
+
+
+@pytest.mark.parametrize("kind", ["fgmres", "gcr"])
+def test_oracle_flexible_solvers_converge(kind):
+    p, op, prec, _, _ = w2_setup(6, 7)
+    x, info = orc.solve(kind, op, prec, p.rhs, r_tol=1e-8, max_iter=200, gcrk=8)
+    assert info.converged
+    r = p.rhs - op.apply(x)
+    assert np.linalg.norm(r) / np.linalg.norm(p.rhs) < 2e-8
+    if kind == "gcr":
+        assert 1 <= info.iv_final <= 8
+
+
+def test_oracle_fgmres_adds_correction_to_initial_guess():
+    """fgmres_solve starts its residual from b (it assumes x0 = 0) and adds
+    the correction to x: with x0 != 0 the result is x0 + A^-1 b."""
+    p, op = w0_setup(5, 4)
+    P = orc.Preconditioner.diagonal(op.diagonal())
+    x_zero, _ = orc.solve("fgmres", op, P, p.rhs, r_tol=1e-10, max_iter=400, gcrk=10)
+    x0 = mg.normal(5, p.undf)
+    x_one, _ = orc.solve("fgmres", op, P, p.rhs, x0=x0, r_tol=1e-10, max_iter=400, gcrk=10)
+    np.testing.assert_allclose(x_one, x0 + x_zero, rtol=0, atol=1e-12)
+
+
+def test_oracle_gcr_relative_to_b_and_fgmres_zero_rhs():
+    p, op, prec, _, _ = w2_setup(4, 3)
+    z = np.zeros(p.undf)
+    for kind in ("fgmres", "gcr"):
+        x, info = orc.solve(kind, op, prec, z, r_tol=1e-8, max_iter=10, gcrk=4)
+        assert info.converged and info.iterations == 0 and np.all(x == 0.0)

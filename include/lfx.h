@@ -212,7 +212,11 @@ enum {
    * branches. iterations = restart cycles; GCR's inner_iterations = the inner
    * step of the last check. */
   LFX_SOLVER_FGMRES = 4,    /* fgmres_solve   :1055-1237 */
-  LFX_SOLVER_GCR = 5        /* gcr_solve      :1288-1408 */
+  LFX_SOLVER_GCR = 5,       /* gcr_solve      :1288-1408 */
+  /* made by their own constructors below */
+  LFX_SOLVER_PRECONDITION_ONLY = 6, /* precondition_only_solve :1664-1694 */
+  LFX_SOLVER_JACOBI = 7,            /* jacobi_solve            :1745-1815 */
+  LFX_SOLVER_CHEBYSHEV = 8          /* chebyshev_solve         :1868-1940 */
 };
 
 typedef struct {
@@ -241,6 +245,26 @@ int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
 /* x: initial guess on entry, solution on exit; b unchanged */
 int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info* info);
 int lfx_solver_destroy(lfx_solver* s);
+/* precondition_only_constructor (:1642-1657): x = P b; with monitoring the
+ * info reports ||b - A x|| against ||b||. */
+int lfx_precondition_only_solver_create(lfx_ctx* ctx, lfx_op* op, lfx_prec* prec,
+                                        int32_t monitor_convergence, lfx_solver** out);
+/* jacobi_constructor (:1715-1739): x += -rho_relax P (A x - b), converged when
+ * ||r||/||r_1|| <= r_tol or ||r|| <= a_tol (checked before each update);
+ * iterations = residual checks made. */
+int lfx_jacobi_solver_create(lfx_ctx* ctx, lfx_op* op, lfx_prec* prec, double r_tol, double a_tol,
+                             int32_t max_iter, int32_t monitor_convergence,
+                             int32_t fail_on_non_converged, double rho_relax, lfx_solver** out);
+/* chebyshev_constructor (:1836-1862): exactly max_iter steps from x = 0 (the
+ * initial guess is ignored, as in the reference) for eigenvalue bounds
+ * [lmin, lmax] of P A; with monitoring the info reports ||A x - b|| /
+ * max(1, ||b||). As in the reference, fail_on_non_converged with monitoring
+ * makes every solve return LFX_NOT_CONVERGED (it logs its result as an
+ * error). */
+int lfx_chebyshev_solver_create(lfx_ctx* ctx, lfx_op* op, lfx_prec* prec, double r_tol,
+                                double a_tol, int32_t max_iter, int32_t monitor_convergence,
+                                int32_t fail_on_non_converged, double lmin, double lmax,
+                                lfx_solver** out);
 /* change r_tol / a_tol for the next solves (keeps the solver's CUDA graphs) */
 int lfx_solver_set_tolerance(lfx_solver* s, double r_tol, double a_tol);
 

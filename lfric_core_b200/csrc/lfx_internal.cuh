@@ -361,6 +361,15 @@ int fgmres_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,
 int gcr_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,
              const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
              lfx_solve_info* info);
+int precondition_only_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,
+                           const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+                           lfx_solve_info* info);
+int jacobi_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg, double rho_relax,
+                const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+                lfx_solve_info* info);
+int chebyshev_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg, double lmin,
+                   double lmax, const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+                   lfx_solve_info* info);
 int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int64_t n,
                     const int* skip);
 void timing_begin(lfx_ctx* ctx, int32_t precision);

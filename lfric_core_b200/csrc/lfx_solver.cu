@@ -71,7 +71,8 @@ struct lfx_solver {
   double* d_gm = nullptr;       // gmres: H, negH, g, u, cs, sn
   bool inner_mode = false;      // GMRES used as the inner solve of a refinement
   std::vector<GraphEntry> graphs;
-  std::vector<lfx_vec*> hv;  // FGMRES / GCR work vectors
+  std::vector<lfx_vec*> hv;  // work vectors of the host-driven solvers
+  double rho_relax = 1.0, lmin = 0.0, lmax = 0.0;  // Jacobi / Chebyshev
   // refined solver
   lfx_solver* inner = nullptr;
   double inner_rtol = 0.0;
@@ -788,6 +789,37 @@ int free_solver(lfx_solver* s) {
   return LFX_OK;
 }
 
+// a solver whose scalar recurrences run on the host over the vector C ABI
+// (lfx_solver_flex.cu), with nvec work vectors
+int create_host_solver(lfx_ctx* ctx, int kind, lfx_op* op, lfx_prec* prec,
+                       const lfx_solver_cfg& cfg, int nvec, lfx_solver** out) {
+  if (op->lay->undf_to != op->lay->undf_from)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "Krylov solve needs a square operator");
+  if (prec->kind != PREC_NULL && prec->precision != op->precision)
+    return fail(ctx, LFX_TYPE_MISMATCH, "operator and preconditioner precision differ");
+  lfx_solver* s = new lfx_solver();
+  s->ctx = ctx;
+  s->kind = kind;
+  s->op = op;
+  s->prec = prec;
+  s->cfg = cfg;
+  s->precision = op->precision;
+  s->n = op->lay->undf_to;
+  int64_t n = s->n;
+  int rc = LFX_OK;
+  for (int i = 0; i < nvec && !rc; ++i) {
+    lfx_vec* v = nullptr;
+    rc = lfx_vec_create(ctx, 1, &n, s->precision, &v);
+    if (!rc) s->hv.push_back(v);
+  }
+  if (rc) {
+    free_solver(s);
+    return rc;
+  }
+  *out = s;
+  return LFX_OK;
+}
+
 int alloc_common(lfx_solver* s, int nwork) {
   lfx_ctx* ctx = s->ctx;
   int rc = dmalloc(ctx, (void**)&s->d_state, sizeof(DevState));
@@ -885,7 +917,7 @@ int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
                       const lfx_solver_cfg* cfg, lfx_solver** out) {
   if (!ctx || !op || !prec || !cfg || !out) return LFX_INVALID_ARGUMENT;
   *out = nullptr;
-  if (kind < LFX_SOLVER_CG || kind > LFX_SOLVER_GCR)
+  if (kind < LFX_SOLVER_CG || kind > LFX_SOLVER_CHEBYSHEV)
     return fail(ctx, LFX_INVALID_ARGUMENT, "unknown solver kind");
   if (op->lay->undf_to != op->lay->undf_from)
     return fail(ctx, LFX_INVALID_ARGUMENT, "Krylov solve needs a square operator");
@@ -899,30 +931,12 @@ int lfx_solver_create(lfx_ctx* ctx, int32_t kind, lfx_op* op, lfx_prec* prec,
   if (cfg->max_iter < 1) return fail(ctx, LFX_INVALID_ARGUMENT, "max_iter must be positive");
   if (kind >= LFX_SOLVER_GMRES && (cfg->gcrk < 1 || cfg->gcrk > MAX_GCRK))
     return fail(ctx, LFX_INVALID_ARGUMENT, "gcrk must be in 1..64");
-  if (kind == LFX_SOLVER_FGMRES || kind == LFX_SOLVER_GCR) {
-    lfx_solver* s = new lfx_solver();
-    s->ctx = ctx;
-    s->kind = kind;
-    s->op = op;
-    s->prec = prec;
-    s->cfg = *cfg;
-    s->precision = op->precision;
-    s->n = op->lay->undf_to;
-    const int nv = (kind == LFX_SOLVER_FGMRES ? 5 : 3) + 2 * cfg->gcrk;
-    int64_t n = s->n;
-    int rc = LFX_OK;
-    for (int i = 0; i < nv && !rc; ++i) {
-      lfx_vec* v = nullptr;
-      rc = lfx_vec_create(ctx, 1, &n, s->precision, &v);
-      if (!rc) s->hv.push_back(v);
-    }
-    if (rc) {
-      free_solver(s);
-      return rc;
-    }
-    *out = s;
-    return LFX_OK;
-  }
+  if (kind == LFX_SOLVER_FGMRES || kind == LFX_SOLVER_GCR)
+    return create_host_solver(ctx, kind, op, prec, *cfg,
+                              (kind == LFX_SOLVER_FGMRES ? 5 : 3) + 2 * cfg->gcrk, out);
+  if (kind > LFX_SOLVER_GCR)
+    return fail(ctx, LFX_INVALID_ARGUMENT,
+                "precondition-only, Jacobi and Chebyshev solvers have their own constructors");
   lfx_solver* s = new lfx_solver();
   s->ctx = ctx;
   s->kind = kind;
@@ -995,15 +1009,34 @@ int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info
     return fail(ctx, LFX_TYPE_MISMATCH, "vector length does not match the operator");
   if (x->data[0] == b->data[0]) return fail(ctx, LFX_INVALID_ARGUMENT, "x and b must differ");
   int rc;
-  if (s->kind == LFX_SOLVER_FGMRES || s->kind == LFX_SOLVER_GCR) {
-    rc = s->kind == LFX_SOLVER_FGMRES ? fgmres_host(s->op, s->prec, s->cfg, s->hv, x, b, info)
-                                      : gcr_host(s->op, s->prec, s->cfg, s->hv, x, b, info);
+  if (s->kind >= LFX_SOLVER_FGMRES && s->kind <= LFX_SOLVER_CHEBYSHEV) {
+    switch (s->kind) {
+      case LFX_SOLVER_FGMRES: rc = fgmres_host(s->op, s->prec, s->cfg, s->hv, x, b, info); break;
+      case LFX_SOLVER_GCR: rc = gcr_host(s->op, s->prec, s->cfg, s->hv, x, b, info); break;
+      case LFX_SOLVER_PRECONDITION_ONLY:
+        rc = precondition_only_host(s->op, s->prec, s->cfg, s->hv, x, b, info);
+        break;
+      case LFX_SOLVER_JACOBI:
+        rc = jacobi_host(s->op, s->prec, s->cfg, s->rho_relax, s->hv, x, b, info);
+        break;
+      default:
+        rc = chebyshev_host(s->op, s->prec, s->cfg, s->lmin, s->lmax, s->hv, x, b, info);
+        break;
+    }
     if (!rc) rc = lfx_ctx_check_device_error(ctx);
     if (rc) {
       info->status = rc;
       return rc;
     }
     if (info->status == LFX_NAN_DETECTED) return fail(ctx, LFX_NAN_DETECTED, "NaN in residual");
+    // as the reference: GCR logs non-convergence as an error in both branches;
+    // Chebyshev, which has no convergence test, logs its final residual as an
+    // error whenever fail_on_non_converged is set
+    if (s->kind == LFX_SOLVER_CHEBYSHEV && s->cfg.monitor_convergence &&
+        s->cfg.fail_on_non_converged) {
+      info->status = LFX_NOT_CONVERGED;
+      return fail(ctx, LFX_NOT_CONVERGED, "chebyshev with fail_on_non_converged");
+    }
     const bool must_fail = s->kind == LFX_SOLVER_GCR || s->cfg.fail_on_non_converged;
     if (!info->converged && s->cfg.monitor_convergence && must_fail) {
       info->status = LFX_NOT_CONVERGED;
@@ -1044,6 +1077,45 @@ int lfx_solver_apply(lfx_solver* s, lfx_vec* x, const lfx_vec* b, lfx_solve_info
 }
 
 int lfx_solver_destroy(lfx_solver* s) { return free_solver(s); }
+
+int lfx_precondition_only_solver_create(lfx_ctx* ctx, lfx_op* op, lfx_prec* prec,
+                                        int32_t monitor_convergence, lfx_solver** out) {
+  if (!ctx || !op || !prec || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  lfx_solver_cfg cfg{};
+  cfg.max_iter = 1;
+  cfg.monitor_convergence = monitor_convergence;
+  return create_host_solver(ctx, LFX_SOLVER_PRECONDITION_ONLY, op, prec, cfg, 2, out);
+}
+
+int lfx_jacobi_solver_create(lfx_ctx* ctx, lfx_op* op, lfx_prec* prec, double r_tol, double a_tol,
+                             int32_t max_iter, int32_t monitor_convergence,
+                             int32_t fail_on_non_converged, double rho_relax, lfx_solver** out) {
+  if (!ctx || !op || !prec || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (max_iter < 1) return fail(ctx, LFX_INVALID_ARGUMENT, "max_iter must be positive");
+  lfx_solver_cfg cfg{r_tol, a_tol, max_iter, 1, monitor_convergence, fail_on_non_converged};
+  int rc = create_host_solver(ctx, LFX_SOLVER_JACOBI, op, prec, cfg, 2, out);
+  if (!rc) (*out)->rho_relax = rho_relax;
+  return rc;
+}
+
+int lfx_chebyshev_solver_create(lfx_ctx* ctx, lfx_op* op, lfx_prec* prec, double r_tol,
+                                double a_tol, int32_t max_iter, int32_t monitor_convergence,
+                                int32_t fail_on_non_converged, double lmin, double lmax,
+                                lfx_solver** out) {
+  if (!ctx || !op || !prec || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (max_iter < 1) return fail(ctx, LFX_INVALID_ARGUMENT, "max_iter must be positive");
+  if (!(lmax > lmin)) return fail(ctx, LFX_INVALID_ARGUMENT, "lmax must exceed lmin");
+  lfx_solver_cfg cfg{r_tol, a_tol, max_iter, 1, monitor_convergence, fail_on_non_converged};
+  int rc = create_host_solver(ctx, LFX_SOLVER_CHEBYSHEV, op, prec, cfg, 4, out);
+  if (!rc) {
+    (*out)->lmin = lmin;
+    (*out)->lmax = lmax;
+  }
+  return rc;
+}
 
 // The tolerances are read from the solver's device state at every solve, so
 // changing them keeps the captured graphs valid.

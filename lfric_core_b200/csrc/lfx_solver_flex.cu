@@ -1,6 +1,8 @@
-// Flexible GMRES and GCR (sci_iterative_solver_mod.f90:1055-1237, 1288-1408).
+// Flexible GMRES and GCR (sci_iterative_solver_mod.f90:1055-1237, 1288-1408),
+// and the precondition-only, Jacobi and Chebyshev solves (:1664-1694,
+// 1745-1815, 1868-1940).
 //
-// Both are written against the abstract-vector operations of the C ABI --
+// All are written against the abstract-vector operations of the C ABI --
 // lfx_vec_{copy,axpy,aypx,scale,set_scalar,dot,norm}, lfx_op_apply and
 // lfx_prec_apply -- exactly as the reference writes them against
 // abstract_vector_type: every vector operation, apply and preconditioner runs
@@ -32,6 +34,9 @@ struct Vops {
   }
   void aypx(lfx_vec* y, double a, const lfx_vec* x) {
     if (!rc) rc = lfx_vec_aypx(y, a, x);
+  }
+  void axpby(lfx_vec* z, double a, const lfx_vec* x, double b, const lfx_vec* y) {
+    if (!rc) rc = lfx_vec_axpby(z, a, x, b, y);
   }
   void scale(lfx_vec* v, double a) {
     if (!rc) rc = lfx_vec_scale(v, a);
@@ -227,6 +232,103 @@ int gcr_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,
   if (o.rc) return o.rc;
   if (std::isnan(err)) info->status = LFX_NAN_DETECTED;
   o.axpy(x, 1.0, dx);  // :1400
+  return o.rc;
+}
+
+// work: res, Ax. x = P b; with monitoring, ||b - A x|| against ||b||.
+int precondition_only_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,
+                           const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+                           lfx_solve_info* info) {
+  lfx_vec *res = work[0], *Ax = work[1];
+  Vops o;
+  o.P(prec, b, x);
+  info->iterations = 1;
+  info->converged = 1;
+  if (cfg.monitor_convergence) {
+    o.copy(res, b);
+    const double e0 = o.norm(res);
+    o.A(op, x, Ax, &info->applies);
+    o.axpy(res, -1.0, Ax);
+    const double e = o.norm(res);
+    info->initial_norm = e0;
+    info->final_norm = e;
+    info->final_rel = e / e0;
+  }
+  return o.rc;
+}
+
+// work: r, z. x += -rho P (A x - b), the residual checked before each update.
+int jacobi_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg, double rho_relax,
+                const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+                lfx_solve_info* info) {
+  lfx_vec *r = work[0], *z = work[1];
+  Vops o;
+  o.set(r, 0.0);
+  o.set(z, 0.0);
+  const double cst = -rho_relax;
+  double r_nrm = 0.0, r_nrm_0 = 0.0;
+  for (int iter = 1; iter <= cfg.max_iter && !o.rc; ++iter) {
+    o.A(op, x, r, &info->applies);
+    o.axpy(r, -1.0, b);
+    info->iterations = iter;
+    if (cfg.monitor_convergence) {
+      r_nrm = o.norm(r);
+      if (iter == 1) r_nrm_0 = r_nrm;
+      info->final_norm = r_nrm;
+      info->final_rel = r_nrm / r_nrm_0;
+      if (r_nrm / r_nrm_0 <= cfg.r_tol || r_nrm <= cfg.a_tol) {
+        info->converged = 1;
+        break;
+      }
+    }
+    o.P(prec, r, z);
+    o.axpy(x, cst, z);
+  }
+  info->initial_norm = r_nrm_0;
+  if (std::isnan(r_nrm)) info->status = LFX_NAN_DETECTED;
+  return o.rc;
+}
+
+// work: xp, xo, z, r. max_iter Chebyshev steps from x = 0 for eigenvalue
+// bounds [lmin, lmax] of the preconditioned operator.
+int chebyshev_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg, double lmin,
+                   double lmax, const std::vector<lfx_vec*>& work, lfx_vec* x, const lfx_vec* b,
+                   lfx_solve_info* info) {
+  lfx_vec *xp = work[0], *xo = work[1], *z = work[2], *r = work[3];
+  Vops o;
+  o.set(x, 0.0);
+  o.set(xp, 0.0);
+  o.set(xo, 0.0);
+  double init_norm = 0.0;
+  if (cfg.monitor_convergence) init_norm = std::fmax(1.0, o.norm(b));
+  const double a1 = 2.0 / (lmax - lmin);
+  const double a2 = (lmax + lmin) / (lmax - lmin);
+  const double a_over_b = a1 / a2;
+  double w = 1.0;
+  for (int iter = 1; iter <= cfg.max_iter && !o.rc; ++iter) {
+    o.A(op, xo, z, &info->applies);
+    o.axpby(r, 1.0, b, -1.0, z);
+    o.P(prec, r, z);
+    w = 1.0 / (1.0 - w / (4.0 * (a2 * a2)));
+    const double wa_over_b = w * a_over_b;
+    o.axpby(x, wa_over_b, z, w, xo);
+    o.axpy(x, 1.0 - w, xp);
+    if (iter < cfg.max_iter) {
+      o.copy(xp, xo);
+      o.copy(xo, x);
+    }
+  }
+  info->iterations = cfg.max_iter;
+  info->converged = 1;
+  if (cfg.monitor_convergence) {
+    o.A(op, x, z, &info->applies);
+    o.axpy(z, -1.0, b);
+    const double fn = o.norm(z);
+    info->initial_norm = init_norm;
+    info->final_norm = fn;
+    info->final_rel = fn / init_norm;
+    if (std::isnan(fn)) info->status = LFX_NAN_DETECTED;
+  }
   return o.rc;
 }
 

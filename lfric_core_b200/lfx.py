@@ -143,6 +143,11 @@ _SIGS = [
     ("lfx_batch_slot_info", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                              C.POINTER(SolveInfo)], C.c_int),
     ("lfx_batch_retire", [vp, C.c_int32], C.c_int),
+    ("lfx_precondition_only_solver_create", [vp, vp, vp, C.c_int32, C.POINTER(vp)], C.c_int),
+    ("lfx_jacobi_solver_create", [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                  C.c_int32, C.c_double, C.POINTER(vp)], C.c_int),
+    ("lfx_chebyshev_solver_create", [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                     C.c_int32, C.c_double, C.c_double, C.POINTER(vp)], C.c_int),
     ("lfx_mrhs_create", [vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(vp)], C.c_int),
     ("lfx_mrhs_destroy", [vp], C.c_int),
     ("lfx_mrhs_info", [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
@@ -677,6 +682,51 @@ class GCR(_KrylovSolver):
                  fail_on_non_converged=False):
         super().__init__(lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence,
                          fail_on_non_converged, gcrk=gcrk)
+
+
+class PreconditionOnly(_Solver):
+    """precondition_only_type(lin_op, prec, monitor_convergence): x = P b."""
+
+    def __init__(self, lin_op, prec, monitor_convergence=True):
+        self.ctx = lin_op.ctx
+        self.precision = lin_op.precision
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_precondition_only_solver_create(
+            self.ctx.h, lin_op.h, prec.h, 1 if monitor_convergence else 0, C.byref(h)))
+        self.h = h
+        self._keep = (lin_op, prec)
+
+
+class Jacobi(_Solver):
+    """jacobi_type(lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence,
+    fail_on_non_converged, rho_relax): x += -rho_relax P (A x - b)."""
+
+    def __init__(self, lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence=True,
+                 fail_on_non_converged=False, rho_relax=1.0):
+        self.ctx = lin_op.ctx
+        self.precision = lin_op.precision
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_jacobi_solver_create(
+            self.ctx.h, lin_op.h, prec.h, r_tol, a_tol, max_iter, 1 if monitor_convergence else 0,
+            1 if fail_on_non_converged else 0, rho_relax, C.byref(h)))
+        self.h = h
+        self._keep = (lin_op, prec)
+
+
+class Chebyshev(_Solver):
+    """chebyshev_type(lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence,
+    fail_on_non_converged, lmin, lmax): max_iter Chebyshev steps from x = 0."""
+
+    def __init__(self, lin_op, prec, r_tol, a_tol, max_iter, monitor_convergence=True,
+                 fail_on_non_converged=False, lmin=0.0, lmax=2.0):
+        self.ctx = lin_op.ctx
+        self.precision = lin_op.precision
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_chebyshev_solver_create(
+            self.ctx.h, lin_op.h, prec.h, r_tol, a_tol, max_iter, 1 if monitor_convergence else 0,
+            1 if fail_on_non_converged else 0, lmin, lmax, C.byref(h)))
+        self.h = h
+        self._keep = (lin_op, prec)
 
 
 class RefinedSolver(_Solver):

@@ -828,3 +828,95 @@ done:
   free(Ax);
   return 0;
 }
+
+/* precondition_only_solve, sci_iterative_solver_mod.f90:1664-1694 (monitoring on) */
+int or_precondition_only(or_op* A, or_prec* P, double* x, const double* b, int64_t n,
+                         or_info* info) {
+  double *res = vnew(n), *Ax = vnew(n);
+  memset(info, 0, sizeof *info);
+  or_prec_apply(P, b, x);
+  or_setval_x(res, b, n);
+  const double e0 = vnorm(res, n);
+  or_op_apply(A, x, Ax);
+  info->applies = 1;
+  or_inc_x_plus_by(res, -1.0, Ax, n);
+  const double e = vnorm(res, n);
+  info->iterations = 1;
+  info->converged = 1;
+  info->initial_norm = e0;
+  info->final_norm = e;
+  info->final_rel = e / e0;
+  free(res);
+  free(Ax);
+  return 0;
+}
+
+/* jacobi_solve, sci_iterative_solver_mod.f90:1745-1815 (monitoring on) */
+int or_jacobi(or_op* A, or_prec* P, double* x, const double* b, int64_t n, double r_tol,
+              double a_tol, int32_t max_iter, double rho_relax, or_info* info) {
+  double *r = vnew(n), *z = vnew(n);
+  double r_nrm = 0.0, r_nrm_0 = 0.0;
+  const double cst = -rho_relax;
+  memset(info, 0, sizeof *info);
+  for (int32_t iter = 1; iter <= max_iter; ++iter) {
+    or_op_apply(A, x, r);
+    info->applies++;
+    or_inc_x_plus_by(r, -1.0, b, n);
+    r_nrm = vnorm(r, n);
+    if (iter == 1) r_nrm_0 = r_nrm;
+    info->iterations = iter;
+    info->final_norm = r_nrm;
+    info->final_rel = r_nrm / r_nrm_0;
+    if (r_nrm / r_nrm_0 <= r_tol || r_nrm <= a_tol) {
+      info->converged = 1;
+      break;
+    }
+    or_prec_apply(P, r, z);
+    or_inc_x_plus_by(x, cst, z, n);
+  }
+  info->initial_norm = r_nrm_0;
+  free(r);
+  free(z);
+  return 0;
+}
+
+/* chebyshev_solve, sci_iterative_solver_mod.f90:1868-1940 (monitoring on) */
+int or_chebyshev(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t max_iter,
+                 double lmin, double lmax, or_info* info) {
+  double *xp = vnew(n), *xo = vnew(n), *z = vnew(n), *r = vnew(n);
+  memset(info, 0, sizeof *info);
+  or_setval_c(x, 0.0, n);
+  const double init_norm = fmax(1.0, vnorm(b, n));
+  const double a1 = 2.0 / (lmax - lmin);
+  const double a2 = (lmax + lmin) / (lmax - lmin);
+  const double a_over_b = a1 / a2;
+  double w = 1.0;
+  for (int32_t iter = 1; iter <= max_iter; ++iter) {
+    or_op_apply(A, xo, z);
+    info->applies++;
+    or_ax_plus_by(r, 1.0, b, -1.0, z, n);
+    or_prec_apply(P, r, z);
+    w = 1.0 / (1.0 - w / (4.0 * (a2 * a2)));
+    const double wa_over_b = w * a_over_b;
+    or_ax_plus_by(x, wa_over_b, z, w, xo, n);
+    or_inc_x_plus_by(x, 1.0 - w, xp, n);
+    if (iter < max_iter) {
+      or_setval_x(xp, xo, n);
+      or_setval_x(xo, x, n);
+    }
+  }
+  or_op_apply(A, x, z);
+  info->applies++;
+  or_inc_x_plus_by(z, -1.0, b, n);
+  const double fn = vnorm(z, n);
+  info->iterations = max_iter;
+  info->converged = 1;
+  info->initial_norm = init_norm;
+  info->final_norm = fn;
+  info->final_rel = fn / init_norm;
+  free(xp);
+  free(xo);
+  free(z);
+  free(r);
+  return 0;
+}

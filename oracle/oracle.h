@@ -130,6 +130,18 @@ int or_fgmres(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32
  * *iv_final = the inner step at the last check. */
 int or_gcr(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t gcrk,
            double r_tol, double a_tol, int32_t max_iter, or_info* info, int32_t* iv_final);
+/* precondition_only_solve (:1664-1694): x = P b, then (monitoring) the
+ * residual ||b - A x|| against ||b||. */
+int or_precondition_only(or_op* A, or_prec* P, double* x, const double* b, int64_t n,
+                         or_info* info);
+/* jacobi_solve (:1745-1815): x += -rho P (A x - b) until ||r||/||r_1|| <= r_tol
+ * or ||r|| <= a_tol (checked before each update); iterations = checks made. */
+int or_jacobi(or_op* A, or_prec* P, double* x, const double* b, int64_t n, double r_tol,
+              double a_tol, int32_t max_iter, double rho_relax, or_info* info);
+/* chebyshev_solve (:1868-1940): max_iter steps from x = 0 with eigenvalue
+ * bounds lmin, lmax; final ||A x - b|| / max(1, ||b||). */
+int or_chebyshev(or_op* A, or_prec* P, double* x, const double* b, int64_t n, int32_t max_iter,
+                 double lmin, double lmax, or_info* info);
 
 #ifdef __cplusplus
 }

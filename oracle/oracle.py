@@ -80,6 +80,12 @@ def lib():
                                C.c_double, C.c_double, C.c_int32, C.POINTER(Info)]
         L.or_fgmres.argtypes = L.or_gmres.argtypes
         L.or_gcr.argtypes = L.or_gmres.argtypes + [C.POINTER(C.c_int32)]
+        L.or_precondition_only.argtypes = [C.c_void_p, C.c_void_p, f64p, f64p, C.c_int64,
+                                           C.POINTER(Info)]
+        L.or_jacobi.argtypes = [C.c_void_p, C.c_void_p, f64p, f64p, C.c_int64, C.c_double,
+                                C.c_double, C.c_int32, C.c_double, C.POINTER(Info)]
+        L.or_chebyshev.argtypes = [C.c_void_p, C.c_void_p, f64p, f64p, C.c_int64, C.c_int32,
+                                   C.c_double, C.c_double, C.POINTER(Info)]
         _lib = L
     return _lib
 
@@ -148,9 +154,11 @@ class Preconditioner:
             _lib.or_prec_destroy(self.h)
 
 
-def solve(kind, op, prec, b, x0=None, r_tol=1e-8, a_tol=1e-16, max_iter=1000, gcrk=10):
-    """Run the oracle's cg / bicgstab / gmres / fgmres / gcr; returns (x, Info)
-    (for gcr, Info gains iv_final: the inner step of the last check)."""
+def solve(kind, op, prec, b, x0=None, r_tol=1e-8, a_tol=1e-16, max_iter=1000, gcrk=10,
+          rho_relax=1.0, lmin=0.0, lmax=2.0):
+    """Run the oracle's cg / bicgstab / gmres / fgmres / gcr / precondition_only
+    / jacobi / chebyshev; returns (x, Info) (for gcr, Info gains iv_final: the
+    inner step of the last check)."""
     n = len(b)
     x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
     b = np.ascontiguousarray(b, dtype=np.float64)
@@ -168,6 +176,12 @@ def solve(kind, op, prec, b, x0=None, r_tol=1e-8, a_tol=1e-16, max_iter=1000, gc
         ivf = C.c_int32()
         L.or_gcr(op.h, prec.h, x, b, n, gcrk, r_tol, a_tol, max_iter, C.byref(info), C.byref(ivf))
         info.iv_final = ivf.value
+    elif kind == "precondition_only":
+        L.or_precondition_only(op.h, prec.h, x, b, n, C.byref(info))
+    elif kind == "jacobi":
+        L.or_jacobi(op.h, prec.h, x, b, n, r_tol, a_tol, max_iter, rho_relax, C.byref(info))
+    elif kind == "chebyshev":
+        L.or_chebyshev(op.h, prec.h, x, b, n, max_iter, lmin, lmax, C.byref(info))
     else:
         raise ValueError(kind)
     return x, info

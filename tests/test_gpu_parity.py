@@ -318,6 +318,35 @@ def test_flexible_solvers_parity(ctx, kind, space):
     assert same(X.export_field(), x_o)
 
 
+@pytest.mark.parametrize("kind", ["precondition_only", "jacobi", "chebyshev"])
+def test_stationary_solvers_parity(ctx, kind):
+    """Precondition-only, Jacobi and Chebyshev (device vector calls) equal the
+    oracle's restatements bit for bit."""
+    p = mg.w2_problem(10, 12, seed=6)
+    sysd = wl.device_w2(ctx, p)
+    op = o_lma(p)
+    P, _ = o_w2_prec(p, op)
+    x0 = mg.normal(4, p.undf)
+    it = 30 if kind == "chebyshev" else 400
+    args = dict(r_tol=1e-7, a_tol=0.0, max_iter=it, rho_relax=0.8, lmin=0.05, lmax=1.6)
+    x_o, info_o = orc.solve(kind, op, P, p.rhs, x0=x0, **args)
+    if kind == "precondition_only":
+        s = lfx.PreconditionOnly(sysd.op, sysd.prec)
+    elif kind == "jacobi":
+        s = lfx.Jacobi(sysd.op, sysd.prec, 1e-7, 0.0, 400, rho_relax=0.8)
+    else:
+        s = lfx.Chebyshev(sysd.op, sysd.prec, 1e-7, 0.0, 30, lmin=0.05, lmax=1.6)
+    X, B = sysd.vector(x0), sysd.vector(p.rhs)
+    info = s.apply(X, B)
+    assert info.iterations == info_o.iterations
+    assert info.final_rel == info_o.final_rel
+    assert same(X.export_field(), x_o)
+    if kind == "chebyshev":
+        with pytest.raises(lfx.LfxError):
+            lfx.Chebyshev(sysd.op, sysd.prec, 1e-7, 0.0, 5, fail_on_non_converged=True,
+                          lmin=0.05, lmax=1.6).apply(X, B)
+
+
 def test_gcr_nonconvergence_always_fails(ctx):
     """gcr_solve logs non-convergence as an error in both branches, so the
     device GCR returns LFX_NOT_CONVERGED even without fail_on_non_converged;

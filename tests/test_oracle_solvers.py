@@ -146,3 +146,24 @@ def test_oracle_gcr_relative_to_b_and_fgmres_zero_rhs():
     for kind in ("fgmres", "gcr"):
         x, info = orc.solve(kind, op, prec, z, r_tol=1e-8, max_iter=10, gcrk=4)
         assert info.converged and info.iterations == 0 and np.all(x == 0.0)
+
+
+def test_oracle_jacobi_and_chebyshev_and_precondition_only():
+    p, op = w0_setup(5, 4)
+    d = op.diagonal()
+    P = orc.Preconditioner.diagonal(d)
+    # Jacobi with a damping that converges for this diagonally dominant-ish operator
+    x, info = orc.solve("jacobi", op, P, p.rhs, r_tol=1e-6, a_tol=0.0, max_iter=5000,
+                        rho_relax=0.5)
+    assert info.converged
+    r = p.rhs - op.apply(x)
+    assert np.linalg.norm(r) <= 1e-6 * info.initial_norm * (1 + 1e-9)
+    # Chebyshev with the spectrum of D^-1 A from a dense eigensolve
+    A = dense_of(op, p.undf)
+    ev = np.linalg.eigvals(A / d[:, None]).real
+    x, info = orc.solve("chebyshev", op, P, p.rhs, max_iter=60, lmin=ev.min(), lmax=ev.max())
+    assert info.final_rel < 1e-3
+    # precondition only: x = D^-1 b
+    x, info = orc.solve("precondition_only", op, P, p.rhs)
+    np.testing.assert_array_equal(x, p.rhs / d)
+    assert info.final_norm == pytest.approx(np.linalg.norm(p.rhs - op.apply(x)), rel=1e-12)

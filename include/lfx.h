@@ -174,6 +174,38 @@ int lfx_cma_assemble_from_lma(const lfx_op* lma, int32_t nsub, const int32_t* df
                               int32_t beta, int32_t gamma_m, int32_t gamma_p,
                               int32_t bandwidth, int32_t nrow, const int32_t* first_dof,
                               const int32_t* indirection, lfx_cma** out);
+/* CMA set-up algebra (the Helmholtz column operators of the reference's
+ * pressure preconditioner are built this way). Operators made here have no
+ * dofmap (lfx_cma_set_dofmap attaches one to a square operator before
+ * lfx_cma_apply / lfx_cma_prec_create) and may be rectangular (nrow != ncol).
+ * Band parameters must satisfy bandwidth >= 1 + ceiling((g_m + g_p)/beta). */
+int lfx_cma_create_banded(lfx_ctx* ctx, int32_t ncell_2d, int32_t nrow, int32_t ncol,
+                          int32_t bandwidth, int32_t alpha, int32_t beta, int32_t gamma_m,
+                          int32_t gamma_p, const double* columnwise_matrix, lfx_cma** out);
+int lfx_cma_set_dofmap(lfx_cma* cma, const int32_t* first_dof, const int32_t* indirection);
+/* C += A B: columnwise_op_mul_kernel (sci_columnwise_op_mul_kernel_mod.F90) */
+int lfx_cma_mul(const lfx_cma* A, const lfx_cma* B, lfx_cma* C);
+/* new C = A B: columnwise_operator_product (columnwise_operator_mod.f90) + mul;
+ * alpha/beta/gamma from the product rule, divided by gcd(alpha, beta) */
+int lfx_cma_product(const lfx_cma* A, const lfx_cma* B, lfx_cma** C);
+/* C = alpha A + beta B: columnwise_op_scaledadd_kernel
+ * (sci_columnwise_op_scaledadd_kernel_mod.F90); C's band must hold A's and B's */
+int lfx_cma_scaledadd(const lfx_cma* A, const lfx_cma* B, lfx_cma* C, double alpha, double beta);
+/* new C = alpha A + beta B: columnwise_operator_sum + scaledadd */
+int lfx_cma_sum(const lfx_cma* A, const lfx_cma* B, double alpha, double beta, lfx_cma** C);
+/* columnwise_op_asm_m2v_lumped_inv_krnl (..._krnl_mod.F90:74-132): inverse of
+ * the lumped (diagonal) square FP64 LMA, in band entry 1 of each row;
+ * column_banded_dofmap Fortran (ndf, nlayers) */
+int lfx_cma_assemble_m2v_lumped_inv(const lfx_op* lma, const int32_t* column_banded_dofmap,
+                                    int32_t alpha, int32_t beta, int32_t gamma_m, int32_t gamma_p,
+                                    int32_t bandwidth, int32_t nrow, lfx_cma** out);
+/* columnwise_op_asm_diag_hmht_kernel (..._kernel_mod.F90:78-151): sum over the
+ * W2h dofs of Dh Dh^T / diag(M2h), Dh the FP64 W2h -> W3 LMA and M2h the FP64
+ * W2h mass LMA; column_banded_dofmap Fortran (ndf_w3, nlayers) */
+int lfx_cma_assemble_diag_hmht(const lfx_op* Dh, const lfx_op* M2h,
+                               const int32_t* column_banded_dofmap, int32_t alpha, int32_t beta,
+                               int32_t gamma_m, int32_t gamma_p, int32_t bandwidth, int32_t nrow,
+                               lfx_cma** out);
 /* copy of the band back to the host, Fortran (bandwidth, nrow, ncell_2d) */
 int lfx_cma_get_band(const lfx_cma* cma, double* band);
 /* y += A x (columnwise_op_app_kernel_mod.F90:73-124) */

@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
+#include <vector>
 
 #include "lfx_internal.cuh"
 
@@ -53,6 +55,114 @@ __global__ void cma_asm(int ncell, int nl, int ndf_full, int blk, const double* 
         if (j - jm < 0 || j - jm >= bw) continue;  // outside the band (host validates)
         double* e = &col[(j - jm) + (size_t)bw * (i - 1)];
         *e = *e + Mc[(size_t)dfs[a] * blk + (size_t)dfs[b] * nl + (k - 1)];
+      }
+    }
+}
+
+// Band of one columnwise operator as the set-up kernels see it.
+struct BandArg {
+  double* band;
+  int nrow, ncol, bw, alpha, beta, gm, gp;
+};
+
+// columnwise_op_mul_kernel_code (sci_columnwise_op_mul_kernel_mod.F90): C += A B,
+// one thread per column, the reference's loops and order (matrixentry as one fma chain)
+__global__ void cma_mul(int ncell, BandArg A, BandArg B, BandArg C) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const double* a = A.band + (size_t)c * A.bw * A.nrow;
+  const double* bb = B.band + (size_t)c * B.bw * B.nrow;
+  double* cc = C.band + (size_t)c * C.bw * C.nrow;
+  for (int i = 1; i <= C.nrow; ++i) {
+    const int jmA = ceil_div_i(A.alpha * i - A.gp, A.beta);
+    const int jpA = floor_div_i(A.alpha * i + A.gm, A.beta);
+    const int jmC = ceil_div_i(C.alpha * i - C.gp, C.beta);
+    const int jpC = floor_div_i(C.alpha * i + C.gm, C.beta);
+    for (int j = max(1, jmC); j <= min(C.ncol, jpC); ++j) {
+      double e = 0.0;
+      for (int l = max(1, jmA); l <= min(A.ncol, jpA); ++l) {
+        const int jmB = ceil_div_i(B.alpha * l - B.gp, B.beta);
+        const int jpB = floor_div_i(B.alpha * l + B.gm, B.beta);
+        if (jmB <= j && j <= jpB)
+          e = fma(a[(l - jmA) + (size_t)A.bw * (i - 1)], bb[(j - jmB) + (size_t)B.bw * (l - 1)], e);
+      }
+      double* t = &cc[(j - jmC) + (size_t)C.bw * (i - 1)];
+      *t = *t + e;
+    }
+  }
+}
+
+// columnwise_op_scaledadd_kernel_code (sci_columnwise_op_scaledadd_kernel_mod.F90):
+// C = alpha A + beta B over the rows of A
+__global__ void cma_scaledadd(int ncell, BandArg A, BandArg B, BandArg C, double alpha,
+                              double beta) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const double* a = A.band + (size_t)c * A.bw * A.nrow;
+  const double* bb = B.band + (size_t)c * B.bw * B.nrow;
+  double* cc = C.band + (size_t)c * C.bw * C.nrow;
+  for (int q = 0; q < C.bw * C.nrow; ++q) cc[q] = 0.0;
+  for (int i = 1; i <= A.nrow; ++i) {
+    const int jmA = ceil_div_i(A.alpha * i - A.gp, A.beta);
+    const int jpA = floor_div_i(A.alpha * i + A.gm, A.beta);
+    const int jmB = ceil_div_i(B.alpha * i - B.gp, B.beta);
+    const int jpB = floor_div_i(B.alpha * i + B.gm, B.beta);
+    const int jmC = ceil_div_i(C.alpha * i - C.gp, C.beta);
+    for (int j = max(1, jmA); j <= min(A.ncol, jpA); ++j) {
+      double* t = &cc[(j - jmC) + (size_t)C.bw * (i - 1)];
+      *t = fma(alpha, a[(j - jmA) + (size_t)A.bw * (i - 1)], *t);
+    }
+    for (int j = max(1, jmB); j <= min(A.ncol, jpB); ++j) {
+      double* t = &cc[(j - jmC) + (size_t)C.bw * (i - 1)];
+      *t = fma(beta, bb[(j - jmB) + (size_t)B.bw * (i - 1)], *t);
+    }
+  }
+}
+
+// columnwise_op_asm_m2v_lumped_inv_krnl_code (..._krnl_mod.F90:74-132): the
+// diagonal entries of the LMA summed into band entry 1 of each row, then
+// every nonzero band entry inverted. M: [c][df] blocks of blk, [df2][k] inside.
+__global__ void cma_m2v_lumped_inv(int ncell, int nl, int ndf, int blk, const double* __restrict__ M,
+                                   const int* __restrict__ cbd, BandArg C) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  double* cc = C.band + (size_t)c * C.bw * C.nrow;
+  for (int q = 0; q < C.bw * C.nrow; ++q) cc[q] = 0.0;
+  const double* Mc = M + (size_t)c * ndf * blk;
+  for (int k = 1; k <= nl; ++k)
+    for (int df = 0; df < ndf; ++df) {
+      const int i = cbd[df + ndf * (k - 1)];
+      double* t = &cc[(size_t)C.bw * (i - 1)];
+      *t = *t + Mc[(size_t)df * blk + (size_t)df * nl + (k - 1)];
+    }
+  for (int q = 0; q < C.bw * C.nrow; ++q)
+    if (cc[q] != 0.0) cc[q] = 1.0 / cc[q];
+}
+
+// columnwise_op_asm_diag_hmht_kernel_code (..._kernel_mod.F90:78-151):
+// sum_df3 Dh(df1, df3) Dh(df2, df3) / M2h(df3, df3) into the band.
+__global__ void cma_diag_hmht(int ncell, int nl, int ndf3, int ndfh, int blkD, int blkM,
+                              const double* __restrict__ Dh, const double* __restrict__ Mh,
+                              const int* __restrict__ cbd, BandArg C) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  double* cc = C.band + (size_t)c * C.bw * C.nrow;
+  for (int q = 0; q < C.bw * C.nrow; ++q) cc[q] = 0.0;
+  const double* Dc = Dh + (size_t)c * ndf3 * blkD;
+  const double* Mc = Mh + (size_t)c * ndfh * blkM;
+  for (int k = 1; k <= nl; ++k)
+    for (int d1 = 0; d1 < ndf3; ++d1) {
+      const int i = cbd[d1 + ndf3 * (k - 1)];
+      const int jm = ceil_div_i(C.alpha * i - C.gp, C.beta);
+      for (int d2 = 0; d2 < ndf3; ++d2) {
+        double tmp = 0.0;
+        for (int d3 = 0; d3 < ndfh; ++d3)
+          tmp = tmp + Dc[(size_t)d1 * blkD + (size_t)d3 * nl + (k - 1)] *
+                          Dc[(size_t)d2 * blkD + (size_t)d3 * nl + (k - 1)] /
+                          Mc[(size_t)d3 * blkM + (size_t)d3 * nl + (k - 1)];
+        const int j = cbd[d2 + ndf3 * (k - 1)];
+        double* t = &cc[(j - jm) + (size_t)C.bw * (i - 1)];
+        *t = *t + tmp;
       }
     }
 }
@@ -310,6 +420,8 @@ int lfx_cma_get_band(const lfx_cma* m, double* band) {
 int lfx_cma_apply(lfx_cma* m, const lfx_vec* x, lfx_vec* y) {
   if (!m || !x || !y) return LFX_INVALID_ARGUMENT;
   lfx_ctx* ctx = m->ctx;
+  if (!m->first_dof || m->nrow != m->ncol)
+    return fail(ctx, LFX_NOT_SUPPORTED, "apply needs a square CMA operator with a dofmap");
   if (x->precision != y->precision || x->undf != y->undf)
     return fail(ctx, LFX_TYPE_MISMATCH, "vectors differ in shape or precision");
   if (m->max_row >= x->undf[0])
@@ -336,6 +448,283 @@ int lfx_cma_destroy(lfx_cma* m) {
   dfree(m->ctx, m->band, 8 * (size_t)m->bw * m->nrow * m->ncell_2d);
   delete m;
   return LFX_OK;
+}
+
+// ------------------------------------------------------------------ CMA set-up
+namespace {
+
+bool band_consistent(int bw, int beta, int gm, int gp) {
+  return beta >= 1 && gm >= 0 && gp >= 0 && bw >= 1 + ceil_div_i(gm + gp, beta);
+}
+
+BandArg arg_of(const lfx_cma* m) {
+  return BandArg{m->band, m->nrow, m->ncol, m->bw, m->alpha, m->beta, m->gamma_m, m->gamma_p};
+}
+
+int gcd_i(int a, int b) {
+  while (b) {
+    const int t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// a map-free operator with a zero band: the parameters divided by
+// gcd(alpha, beta) and bandwidth 1 + ceiling((g_m + g_p)/beta), as
+// columnwise_operator_initialiser_custom (columnwise_operator_mod.f90:216-247)
+int cma_new(lfx_ctx* ctx, int ncell_2d, int nrow, int ncol, int alpha, int beta, int gm, int gp,
+            lfx_cma** out) {
+  const int g = gcd_i(alpha, beta);
+  if (g > 1) {
+    alpha /= g;
+    beta /= g;
+    gm /= g;
+    gp /= g;
+  }
+  const int bw = 1 + ceil_div_i(gm + gp, beta);
+  return lfx_cma_create_banded(ctx, ncell_2d, nrow, ncol, bw, alpha, beta, gm, gp, nullptr, out);
+}
+
+int run_sync(lfx_ctx* ctx, const char* what) {
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return fail(ctx, LFX_CUDA_ERROR, what);
+  return LFX_OK;
+}
+
+int upload_cbd(lfx_ctx* ctx, const int32_t* cbd, size_t n, int** d) {
+  int rc = dmalloc(ctx, (void**)d, 4 * n);
+  if (!rc && cudaMemcpy(*d, cbd, 4 * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(ctx, LFX_CUDA_ERROR, "upload of column_banded_dofmap failed");
+  return rc;
+}
+
+}  // namespace
+
+int lfx_cma_create_banded(lfx_ctx* ctx, int32_t ncell_2d, int32_t nrow, int32_t ncol,
+                          int32_t bandwidth, int32_t alpha, int32_t beta, int32_t gamma_m,
+                          int32_t gamma_p, const double* columnwise_matrix, lfx_cma** out) {
+  if (!ctx || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (ncell_2d < 1 || nrow < 1 || ncol < 1 || !band_consistent(bandwidth, beta, gamma_m, gamma_p))
+    return fail(ctx, LFX_INVALID_ARGUMENT, "bad CMA dimensions or band parameters");
+  lfx_cma* m = new lfx_cma();
+  m->ctx = ctx;
+  m->ncell_2d = ncell_2d;
+  m->nrow = nrow;
+  m->ncol = ncol;
+  m->bw = bandwidth;
+  m->alpha = alpha;
+  m->beta = beta;
+  m->gamma_m = gamma_m;
+  m->gamma_p = gamma_p;
+  const size_t bytes = 8 * (size_t)bandwidth * nrow * ncell_2d;
+  int rc = dmalloc(ctx, (void**)&m->band, bytes);
+  if (!rc) {
+    if (columnwise_matrix)
+      rc = cudaMemcpy(m->band, columnwise_matrix, bytes, cudaMemcpyHostToDevice) == cudaSuccess
+               ? LFX_OK
+               : fail(ctx, LFX_CUDA_ERROR, "band upload failed");
+    else
+      rc = cudaMemset(m->band, 0, bytes) == cudaSuccess ? LFX_OK
+                                                         : fail(ctx, LFX_CUDA_ERROR, "memset failed");
+  }
+  if (rc) {
+    lfx_cma_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return LFX_OK;
+}
+
+int lfx_cma_set_dofmap(lfx_cma* m, const int32_t* first_dof, const int32_t* indirection) {
+  if (!m || !first_dof || !indirection) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = m->ctx;
+  if (m->nrow != m->ncol) return fail(ctx, LFX_NOT_SUPPORTED, "dofmaps for square operators only");
+  std::vector<int32_t> f(m->ncell_2d), ind(m->nrow);
+  int32_t maxf = 0, maxi = 0;
+  for (int c = 0; c < m->ncell_2d; ++c) {
+    f[c] = first_dof[c] - 1;
+    if (f[c] < 0) return fail(ctx, LFX_INVALID_ARGUMENT, "first_dof must be >= 1");
+    maxf = std::max(maxf, f[c]);
+  }
+  for (int i = 0; i < m->nrow; ++i) {
+    ind[i] = indirection[i] - 1;
+    if (ind[i] < 0) return fail(ctx, LFX_INVALID_ARGUMENT, "indirection entries must be >= 1");
+    maxi = std::max(maxi, ind[i]);
+  }
+  if (!m->first_dof) {
+    int rc = dmalloc(ctx, (void**)&m->first_dof, 4 * (size_t)m->ncell_2d);
+    if (!rc) rc = dmalloc(ctx, (void**)&m->indirection, 4 * (size_t)m->nrow);
+    if (rc) return rc;
+  }
+  LFX_CK(ctx, cudaMemcpy(m->first_dof, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
+  LFX_CK(ctx, cudaMemcpy(m->indirection, ind.data(), 4 * ind.size(), cudaMemcpyHostToDevice));
+  m->h_first = f;
+  m->h_ind = ind;
+  m->max_row = (int64_t)maxf + maxi;
+  return LFX_OK;
+}
+
+// C += A B (columnwise_op_mul_kernel_code)
+int lfx_cma_mul(const lfx_cma* A, const lfx_cma* B, lfx_cma* C) {
+  if (!A || !B || !C) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = C->ctx;
+  if (A->ncell_2d != B->ncell_2d || A->ncell_2d != C->ncell_2d || A->ncol != B->nrow ||
+      C->nrow != A->nrow || C->ncol != B->ncol)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "operator shapes do not chain");
+  for (const lfx_cma* m : std::initializer_list<const lfx_cma*>{A, B, C})
+    if (!band_consistent(m->bw, m->beta, m->gamma_m, m->gamma_p))
+      return fail(ctx, LFX_INVALID_ARGUMENT, "inconsistent band parameters");
+  cma_mul<<<(C->ncell_2d + 127) / 128, 128, 0, ctx->stream>>>(C->ncell_2d, arg_of(A), arg_of(B),
+                                                               arg_of(C));
+  ctx->launches++;
+  return run_sync(ctx, "CMA product failed");
+}
+
+// columnwise_operator_product (columnwise_operator_mod.f90) followed by the
+// mul kernel: a new C = A B
+int lfx_cma_product(const lfx_cma* A, const lfx_cma* B, lfx_cma** out) {
+  if (!A || !B || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  lfx_cma* C = nullptr;
+  int rc = cma_new(A->ctx, A->ncell_2d, A->nrow, B->ncol, A->alpha * B->alpha, A->beta * B->beta,
+                   B->alpha * A->gamma_m + A->beta * B->gamma_m,
+                   B->alpha * A->gamma_p + A->beta * B->gamma_p, &C);
+  if (!rc) rc = lfx_cma_mul(A, B, C);
+  if (rc) {
+    lfx_cma_destroy(C);
+    return rc;
+  }
+  *out = C;
+  return LFX_OK;
+}
+
+// C = alpha A + beta B (columnwise_op_scaledadd_kernel_code); C's band must
+// hold the bands of A and B row by row
+int lfx_cma_scaledadd(const lfx_cma* A, const lfx_cma* B, lfx_cma* C, double alpha, double beta) {
+  if (!A || !B || !C) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = C->ctx;
+  if (A->ncell_2d != B->ncell_2d || A->ncell_2d != C->ncell_2d || C->nrow < A->nrow ||
+      B->nrow < A->nrow)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "operator shapes differ");
+  for (const lfx_cma* m : std::initializer_list<const lfx_cma*>{A, B, C})
+    if (!band_consistent(m->bw, m->beta, m->gamma_m, m->gamma_p))
+      return fail(ctx, LFX_INVALID_ARGUMENT, "inconsistent band parameters");
+  for (int i = 1; i <= A->nrow; ++i) {
+    const int jmC = ceil_div_i(C->alpha * i - C->gamma_p, C->beta);
+    for (const lfx_cma* m : std::initializer_list<const lfx_cma*>{A, B}) {
+      const int lo = std::max(1, ceil_div_i(m->alpha * i - m->gamma_p, m->beta));
+      const int hi = std::min(A->ncol, floor_div_i(m->alpha * i + m->gamma_m, m->beta));
+      if (lo <= hi && (lo - jmC < 0 || hi - jmC >= C->bw))
+        return fail(ctx, LFX_INVALID_ARGUMENT, "C's band does not cover A and B");
+    }
+  }
+  cma_scaledadd<<<(C->ncell_2d + 127) / 128, 128, 0, ctx->stream>>>(
+      C->ncell_2d, arg_of(A), arg_of(B), arg_of(C), alpha, beta);
+  ctx->launches++;
+  return run_sync(ctx, "CMA scaled add failed");
+}
+
+// columnwise_operator_sum followed by the scaledadd kernel: a new C = alpha A + beta B
+int lfx_cma_sum(const lfx_cma* A, const lfx_cma* B, double alpha, double beta, lfx_cma** out) {
+  if (!A || !B || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  lfx_ctx* ctx = A->ctx;
+  if (A->alpha != B->alpha || A->beta != B->beta)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "parameters alpha / beta of the operators differ");
+  if (A->nrow != B->nrow || A->ncol != B->ncol)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "operator shapes differ");
+  lfx_cma* C = nullptr;
+  int rc = cma_new(ctx, A->ncell_2d, A->nrow, A->ncol, A->alpha, A->beta,
+                   std::max(A->gamma_m, B->gamma_m), std::max(A->gamma_p, B->gamma_p), &C);
+  if (!rc) rc = lfx_cma_scaledadd(A, B, C, alpha, beta);
+  if (rc) {
+    lfx_cma_destroy(C);
+    return rc;
+  }
+  *out = C;
+  return LFX_OK;
+}
+
+int lfx_cma_assemble_m2v_lumped_inv(const lfx_op* lma, const int32_t* column_banded_dofmap,
+                                    int32_t alpha, int32_t beta, int32_t gamma_m, int32_t gamma_p,
+                                    int32_t bandwidth, int32_t nrow, lfx_cma** out) {
+  if (!lma || !column_banded_dofmap || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  lfx_ctx* ctx = lma->ctx;
+  const lfx_lma_layout* L = lma->lay;
+  if (lma->precision != LFX_R64 || L->ndf_to != L->ndf_from)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "lumped inverse needs a square FP64 LMA");
+  const size_t ncbd = (size_t)L->ndf_to * L->nlayers;
+  for (size_t q = 0; q < ncbd; ++q)
+    if (column_banded_dofmap[q] < 1 || column_banded_dofmap[q] > nrow)
+      return fail(ctx, LFX_INVALID_ARGUMENT, "column_banded_dofmap out of range");
+  int rc = lfx_cma_create_banded(ctx, L->ncell_2d, nrow, nrow, bandwidth, alpha, beta, gamma_m,
+                                 gamma_p, nullptr, out);
+  if (rc) return rc;
+  int* d_cbd = nullptr;
+  rc = upload_cbd(ctx, column_banded_dofmap, ncbd, &d_cbd);
+  if (!rc) {
+    cma_m2v_lumped_inv<<<(L->ncell_2d + 127) / 128, 128, 0, ctx->stream>>>(
+        L->ncell_2d, L->nlayers, L->ndf_to, lma->blk, (const double*)lma->mat, d_cbd,
+        arg_of(*out));
+    ctx->launches++;
+    rc = run_sync(ctx, "lumped inverse assembly failed");
+  }
+  dfree(ctx, d_cbd, 4 * ncbd);
+  if (rc) {
+    lfx_cma_destroy(*out);
+    *out = nullptr;
+  }
+  return rc;
+}
+
+int lfx_cma_assemble_diag_hmht(const lfx_op* Dh, const lfx_op* M2h,
+                               const int32_t* column_banded_dofmap, int32_t alpha, int32_t beta,
+                               int32_t gamma_m, int32_t gamma_p, int32_t bandwidth, int32_t nrow,
+                               lfx_cma** out) {
+  if (!Dh || !M2h || !column_banded_dofmap || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  lfx_ctx* ctx = Dh->ctx;
+  const lfx_lma_layout *LD = Dh->lay, *LM = M2h->lay;
+  if (Dh->precision != LFX_R64 || M2h->precision != LFX_R64)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "diag_hmht needs FP64 LMAs");
+  if (LM->ndf_to != LM->ndf_from || LD->ndf_from != LM->ndf_to || LD->ncell_2d != LM->ncell_2d ||
+      LD->nlayers != LM->nlayers)
+    return fail(ctx, LFX_INVALID_ARGUMENT, "Dh (W2h -> W3) and M2h (W2h) do not match");
+  const int ndf3 = LD->ndf_to, nl = LD->nlayers;
+  if (beta < 1) return fail(ctx, LFX_INVALID_ARGUMENT, "beta must be positive");
+  for (int k = 0; k < nl; ++k)
+    for (int a = 0; a < ndf3; ++a) {
+      const int i = column_banded_dofmap[a + ndf3 * k];
+      if (i < 1 || i > nrow) return fail(ctx, LFX_INVALID_ARGUMENT, "column_banded_dofmap out of range");
+      const int jm = ceil_div_i(alpha * i - gamma_p, beta);
+      for (int b = 0; b < ndf3; ++b) {
+        const int j = column_banded_dofmap[b + ndf3 * k];
+        if (j - jm < 0 || j - jm >= bandwidth)
+          return fail(ctx, LFX_INVALID_ARGUMENT, "entry falls outside the band");
+      }
+    }
+  int rc = lfx_cma_create_banded(ctx, LD->ncell_2d, nrow, nrow, bandwidth, alpha, beta, gamma_m,
+                                 gamma_p, nullptr, out);
+  if (rc) return rc;
+  int* d_cbd = nullptr;
+  const size_t ncbd = (size_t)ndf3 * nl;
+  rc = upload_cbd(ctx, column_banded_dofmap, ncbd, &d_cbd);
+  if (!rc) {
+    cma_diag_hmht<<<(LD->ncell_2d + 127) / 128, 128, 0, ctx->stream>>>(
+        LD->ncell_2d, nl, ndf3, LM->ndf_to, Dh->blk, M2h->blk, (const double*)Dh->mat,
+        (const double*)M2h->mat, d_cbd, arg_of(*out));
+    ctx->launches++;
+    rc = run_sync(ctx, "diag_hmht assembly failed");
+  }
+  dfree(ctx, d_cbd, 4 * ncbd);
+  if (rc) {
+    lfx_cma_destroy(*out);
+    *out = nullptr;
+  }
+  return rc;
 }
 
 int lfx_null_prec_create(lfx_ctx* ctx, lfx_prec** out) {
@@ -373,6 +762,8 @@ int lfx_cma_prec_create(lfx_ctx* ctx, const lfx_cma* m, const lfx_vec* diag, int
   if (!ctx || !m || !out) return LFX_INVALID_ARGUMENT;
   *out = nullptr;
   if (m->bw != 3) return fail(ctx, LFX_NOT_SUPPORTED, "column inverse needs a tridiagonal band");
+  if (!m->first_dof || m->nrow != m->ncol)
+    return fail(ctx, LFX_NOT_SUPPORTED, "column inverse needs a square CMA operator with a dofmap");
   if (precision != LFX_R64 && precision != LFX_R32) return LFX_INVALID_ARGUMENT;
   const size_t esz = precision == LFX_R64 ? 8 : 4;
   lfx_prec* p = new lfx_prec();

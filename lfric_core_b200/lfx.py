@@ -114,6 +114,15 @@ _SIGS = [
     ("lfx_cma_assemble_from_lma", [vp, C.c_int32, i32p, i32p, C.c_int32, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, C.c_int32, i32p, i32p, C.POINTER(vp)],
      C.c_int),
+    ("lfx_cma_create_banded", [vp] + [C.c_int32] * 8 + [vp, C.POINTER(vp)], C.c_int),
+    ("lfx_cma_set_dofmap", [vp, i32p, i32p], C.c_int),
+    ("lfx_cma_mul", [vp, vp, vp], C.c_int),
+    ("lfx_cma_product", [vp, vp, C.POINTER(vp)], C.c_int),
+    ("lfx_cma_scaledadd", [vp, vp, vp, C.c_double, C.c_double], C.c_int),
+    ("lfx_cma_sum", [vp, vp, C.c_double, C.c_double, C.POINTER(vp)], C.c_int),
+    ("lfx_cma_assemble_m2v_lumped_inv", [vp, i32p] + [C.c_int32] * 6 + [C.POINTER(vp)], C.c_int),
+    ("lfx_cma_assemble_diag_hmht", [vp, vp, i32p] + [C.c_int32] * 6 + [C.POINTER(vp)],
+     C.c_int),
     ("lfx_cma_get_band", [vp, f64p], C.c_int),
     ("lfx_cma_apply", [vp, vp, vp], C.c_int),
     ("lfx_cma_destroy", [vp], C.c_int),
@@ -533,9 +542,78 @@ class ColumnwiseOperator(_Handle):
 
     _destroy = "lfx_cma_destroy"
 
-    def __init__(self, ctx, h, ncell_2d, nrow, bandwidth):
+    def __init__(self, ctx, h, ncell_2d, nrow, bandwidth, ncol=None, params=None):
         self.ctx, self.h = ctx, h
         self.ncell_2d, self.nrow, self.bandwidth = ncell_2d, nrow, bandwidth
+        self.ncol = nrow if ncol is None else ncol
+        self.params = params  # (alpha, beta, gamma_m, gamma_p) when known
+
+    @staticmethod
+    def _gcd(a, b):
+        while b:
+            a, b = b, a % b
+        return a
+
+    @classmethod
+    def banded(cls, ctx, ncell_2d, nrow, ncol, bandwidth, alpha, beta, gamma_m, gamma_p,
+               band=None):
+        """A map-free (possibly rectangular) operator from a host band, for
+        the set-up algebra."""
+        h = vp()
+        b = None if band is None else np.ascontiguousarray(band, dtype=np.float64)
+        ctx.check(ctx.L.lfx_cma_create_banded(ctx.h, ncell_2d, nrow, ncol, bandwidth, alpha, beta,
+                                              gamma_m, gamma_p,
+                                              None if b is None else b.ctypes.data, C.byref(h)))
+        return cls(ctx, h, ncell_2d, nrow, bandwidth, ncol, (alpha, beta, gamma_m, gamma_p))
+
+    @staticmethod
+    def _derived(alpha, beta, gm, gp):
+        g = ColumnwiseOperator._gcd(alpha, beta)
+        if g > 1:
+            alpha, beta, gm, gp = alpha // g, beta // g, gm // g, gp // g
+        return (alpha, beta, gm, gp), 1 + -((-(gm + gp)) // beta)
+
+    def product(self, other: "ColumnwiseOperator") -> "ColumnwiseOperator":
+        """columnwise_operator_product + mul: self . other"""
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_cma_product(self.h, other.h, C.byref(h)))
+        (a1, b1, m1, p1), (a2, b2, m2, p2) = self.params, other.params
+        prm, bw = self._derived(a1 * a2, b1 * b2, a2 * m1 + b1 * m2, a2 * p1 + b1 * p2)
+        return ColumnwiseOperator(self.ctx, h, self.ncell_2d, self.nrow, bw, other.ncol, prm)
+
+    def sum(self, other: "ColumnwiseOperator", alpha, beta) -> "ColumnwiseOperator":
+        """columnwise_operator_sum + scaledadd: alpha self + beta other"""
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_cma_sum(self.h, other.h, alpha, beta, C.byref(h)))
+        (a1, b1, m1, p1), (_, _, m2, p2) = self.params, other.params
+        prm, bw = self._derived(a1, b1, max(m1, m2), max(p1, p2))
+        return ColumnwiseOperator(self.ctx, h, self.ncell_2d, self.nrow, bw, self.ncol, prm)
+
+    def set_dofmap(self, first_dof, indirection):
+        self.ctx.check(self.ctx.L.lfx_cma_set_dofmap(
+            self.h, np.ascontiguousarray(first_dof, dtype=np.int32),
+            np.ascontiguousarray(indirection, dtype=np.int32)))
+
+    @classmethod
+    def m2v_lumped_inv(cls, lma: "LmaOperator", column_banded_dofmap, params, bandwidth, nrow):
+        """columnwise_op_asm_m2v_lumped_inv from a square FP64 LMA."""
+        ctx = lma.ctx
+        h = vp()
+        cbd = np.ascontiguousarray(column_banded_dofmap, dtype=np.int32)
+        ctx.check(ctx.L.lfx_cma_assemble_m2v_lumped_inv(lma.h, cbd, *params, bandwidth, nrow,
+                                                        C.byref(h)))
+        return cls(ctx, h, lma._shape[0], nrow, bandwidth, nrow, tuple(params))
+
+    @classmethod
+    def diag_hmht(cls, dh: "LmaOperator", m2h: "LmaOperator", column_banded_dofmap, params,
+                  bandwidth, nrow):
+        """columnwise_op_asm_diag_hmht from the W2h -> W3 LMA and the W2h mass."""
+        ctx = dh.ctx
+        h = vp()
+        cbd = np.ascontiguousarray(column_banded_dofmap, dtype=np.int32)
+        ctx.check(ctx.L.lfx_cma_assemble_diag_hmht(dh.h, m2h.h, cbd, *params, bandwidth, nrow,
+                                                   C.byref(h)))
+        return cls(ctx, h, dh._shape[0], nrow, bandwidth, nrow, tuple(params))
 
     @classmethod
     def from_band(cls, ctx, ncell_2d, nrow, bandwidth, alpha, beta, gamma_m, gamma_p, first_dof,
@@ -561,6 +639,10 @@ class ColumnwiseOperator(_Handle):
             params["nrow"], np.ascontiguousarray(first_dof, dtype=np.int32),
             np.ascontiguousarray(params["indirection"], dtype=np.int32), C.byref(h)))
         return cls(ctx, h, lma._shape[0], params["nrow"], params["bandwidth"])
+
+    def mul_into(self, other: "ColumnwiseOperator", out: "ColumnwiseOperator"):
+        """out += self . other (columnwise_op_mul_kernel)"""
+        self.ctx.check(self.ctx.L.lfx_cma_mul(self.h, other.h, out.h))
 
     def band(self):
         out = np.empty(self.ncell_2d * self.nrow * self.bandwidth)

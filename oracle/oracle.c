@@ -286,6 +286,120 @@ struct or_op {
   const double* stencil;
 };
 
+/* columnwise_op_mul_kernel_code, sci_columnwise_op_mul_kernel_mod.F90 */
+#define BAND(M, b, i, bw, nrow, cell) (M)[((b) - 1) + (int64_t)(bw) * ((i) - 1) + (int64_t)(bw) * (nrow) * ((cell) - 1)]
+void or_columnwise_op_mul_code(int32_t cell, int32_t ncell_2d, const double* A, int32_t nrow_A,
+                               int32_t ncol_A, int32_t bw_A, int32_t alpha_A, int32_t beta_A,
+                               int32_t gm_A, int32_t gp_A, const double* B, int32_t nrow_B,
+                               int32_t ncol_B, int32_t bw_B, int32_t alpha_B, int32_t beta_B,
+                               int32_t gm_B, int32_t gp_B, double* C, int32_t nrow_C,
+                               int32_t ncol_C, int32_t bw_C, int32_t alpha_C, int32_t beta_C,
+                               int32_t gm_C, int32_t gp_C) {
+  (void)ncell_2d;
+  (void)ncol_B;
+  (void)gm_C;
+  for (int32_t i = 1; i <= nrow_C; ++i) {
+    const int32_t jmA = ceil_div_r(alpha_A * i - gp_A, beta_A);
+    const int32_t jpA = floor_div_r(alpha_A * i + gm_A, beta_A);
+    const int32_t jmC = ceil_div_r(alpha_C * i - gp_C, beta_C);
+    const int32_t jpC = floor_div_r(alpha_C * i + gm_C, beta_C);
+    for (int32_t j = (jmC > 1 ? jmC : 1); j <= (ncol_C < jpC ? ncol_C : jpC); ++j) {
+      double e = 0.0;
+      for (int32_t l = (jmA > 1 ? jmA : 1); l <= (ncol_A < jpA ? ncol_A : jpA); ++l) {
+        const int32_t jmB = ceil_div_r(alpha_B * l - gp_B, beta_B);
+        const int32_t jpB = floor_div_r(alpha_B * l + gm_B, beta_B);
+        if (jmB <= j && j <= jpB)
+          e = fma(BAND(A, l - jmA + 1, i, bw_A, nrow_A, cell),
+                  BAND(B, j - jmB + 1, l, bw_B, nrow_B, cell), e);
+      }
+      BAND(C, j - jmC + 1, i, bw_C, nrow_C, cell) = BAND(C, j - jmC + 1, i, bw_C, nrow_C, cell) + e;
+    }
+  }
+}
+
+/* columnwise_op_scaledadd_kernel_code, sci_columnwise_op_scaledadd_kernel_mod.F90 */
+void or_columnwise_op_scaledadd_code(int32_t cell, int32_t ncell_2d, const double* A,
+                                     int32_t nrow_A, int32_t ncol_A, int32_t bw_A, int32_t alpha_A,
+                                     int32_t beta_A, int32_t gm_A, int32_t gp_A, const double* B,
+                                     int32_t nrow_B, int32_t ncol_B, int32_t bw_B, int32_t alpha_B,
+                                     int32_t beta_B, int32_t gm_B, int32_t gp_B, double* C,
+                                     int32_t nrow_C, int32_t ncol_C, int32_t bw_C, int32_t alpha_C,
+                                     int32_t beta_C, int32_t gm_C, int32_t gp_C, double alpha,
+                                     double beta) {
+  (void)ncell_2d;
+  (void)ncol_B;
+  (void)ncol_C;
+  (void)gm_C;
+  for (int64_t q = 0; q < (int64_t)bw_C * nrow_C; ++q) C[q + (int64_t)bw_C * nrow_C * (cell - 1)] = 0.0;
+  for (int32_t i = 1; i <= nrow_A; ++i) {
+    const int32_t jmA = ceil_div_r(alpha_A * i - gp_A, beta_A);
+    const int32_t jpA = floor_div_r(alpha_A * i + gm_A, beta_A);
+    const int32_t jmB = ceil_div_r(alpha_B * i - gp_B, beta_B);
+    const int32_t jpB = floor_div_r(alpha_B * i + gm_B, beta_B);
+    const int32_t jmC = ceil_div_r(alpha_C * i - gp_C, beta_C);
+    for (int32_t j = (jmA > 1 ? jmA : 1); j <= (ncol_A < jpA ? ncol_A : jpA); ++j) {
+      double* e = &BAND(C, j - jmC + 1, i, bw_C, nrow_C, cell);
+      *e = fma(alpha, BAND(A, j - jmA + 1, i, bw_A, nrow_A, cell), *e);
+    }
+    for (int32_t j = (jmB > 1 ? jmB : 1); j <= (ncol_A < jpB ? ncol_A : jpB); ++j) {
+      double* e = &BAND(C, j - jmC + 1, i, bw_C, nrow_C, cell);
+      *e = fma(beta, BAND(B, j - jmB + 1, i, bw_B, nrow_B, cell), *e);
+    }
+  }
+}
+
+/* columnwise_op_asm_m2v_lumped_inv_krnl_code, ..._asm_m2v_lumped_inv_krnl_mod.F90:74-132 */
+void or_columnwise_op_asm_m2v_lumped_inv_code(int32_t cell, int32_t nlayers, int32_t ncell_2d,
+                                              int32_t ncell_3d, const double* local_stencil,
+                                              double* C, int32_t nrow, int32_t bw, int32_t ndf,
+                                              const int32_t* column_banded_dofmap) {
+  (void)ncell_2d;
+  double* col = C + (int64_t)bw * nrow * (cell - 1);
+  for (int64_t q = 0; q < (int64_t)bw * nrow; ++q) col[q] = 0.0;
+  for (int32_t k = 1; k <= nlayers; ++k) {
+    const int64_t ik = (int64_t)(cell - 1) * nlayers + k;
+    for (int32_t df1 = 1; df1 <= ndf; ++df1) {
+      const int32_t i = column_banded_dofmap[(df1 - 1) + (int64_t)ndf * (k - 1)];
+      col[(int64_t)bw * (i - 1)] = col[(int64_t)bw * (i - 1)] +
+          local_stencil[(ik - 1) + (int64_t)ncell_3d * ((df1 - 1) + (int64_t)ndf * (df1 - 1))];
+    }
+  }
+  for (int64_t q = 0; q < (int64_t)bw * nrow; ++q)
+    if (col[q] != 0.0) col[q] = 1.0 / col[q];
+}
+
+/* columnwise_op_asm_diag_hmht_kernel_code, ..._asm_diag_hmht_kernel_mod.F90:78-151 */
+void or_columnwise_op_asm_diag_hmht_code(int32_t cell, int32_t nlayers, int32_t ncell_2d,
+                                         int32_t ncell_3d, const double* Dh, const double* M2h,
+                                         double* C, int32_t nrow, int32_t bw, int32_t alpha,
+                                         int32_t beta, int32_t gamma_m, int32_t gamma_p,
+                                         int32_t ndf_w3, const int32_t* column_banded_dofmap,
+                                         int32_t ndf_w2h) {
+  (void)ncell_2d;
+  (void)gamma_m;
+  double* col = C + (int64_t)bw * nrow * (cell - 1);
+  for (int64_t q = 0; q < (int64_t)bw * nrow; ++q) col[q] = 0.0;
+#define DH(ik, a, b) Dh[((ik) - 1) + (int64_t)ncell_3d * (((a) - 1) + (int64_t)ndf_w3 * ((b) - 1))]
+#define MH(ik, a, b) M2h[((ik) - 1) + (int64_t)ncell_3d * (((a) - 1) + (int64_t)ndf_w2h * ((b) - 1))]
+  for (int32_t k = 1; k <= nlayers; ++k) {
+    const int64_t ik = (int64_t)(cell - 1) * nlayers + k;
+    for (int32_t df1 = 1; df1 <= ndf_w3; ++df1) {
+      const int32_t i = column_banded_dofmap[(df1 - 1) + (int64_t)ndf_w3 * (k - 1)];
+      const int32_t jm = ceil_div_r(alpha * i - gamma_p, beta);
+      for (int32_t df2 = 1; df2 <= ndf_w3; ++df2) {
+        double tmp = 0.0;
+        for (int32_t df3 = 1; df3 <= ndf_w2h; ++df3)
+          tmp = tmp + DH(ik, df1, df3) * DH(ik, df2, df3) / MH(ik, df3, df3);
+        const int32_t j = column_banded_dofmap[(df2 - 1) + (int64_t)ndf_w3 * (k - 1)];
+        col[(j - jm) + (int64_t)bw * (i - 1)] = col[(j - jm) + (int64_t)bw * (i - 1)] + tmp;
+      }
+    }
+  }
+#undef DH
+#undef MH
+}
+#undef BAND
+
 or_op* or_lma_create(int32_t ncell_2d, int32_t nlayers, int32_t ndf_to, int32_t ndf_from,
                      const int32_t* map_to, const int32_t* map_from, int64_t undf_to,
                      int64_t undf_from, const double* stencil, int32_t ncolours,

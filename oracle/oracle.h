@@ -81,6 +81,38 @@ void or_columnwise_op_appinv_code(int32_t cell, double* lhs, const double* x,
 typedef struct or_op or_op;
 typedef struct or_prec or_prec;
 
+/* CMA set-up kernels, one column (cell, 1-based) of Fortran band arrays
+ * (bw, nrow, ncell_2d) and local stencils (ncell_3d, ndf_to, ndf_from):
+ *   mul        sci_columnwise_op_mul_kernel_mod.F90 (C += A B)
+ *   scaledadd  sci_columnwise_op_scaledadd_kernel_mod.F90 (C = alpha A + beta B)
+ *   m2v_lumped_inv  sci_columnwise_op_asm_m2v_lumped_inv_krnl_mod.F90:74-132
+ *   diag_hmht  sci_columnwise_op_asm_diag_hmht_kernel_mod.F90:78-151 */
+void or_columnwise_op_mul_code(int32_t cell, int32_t ncell_2d, const double* A, int32_t nrow_A,
+                               int32_t ncol_A, int32_t bw_A, int32_t alpha_A, int32_t beta_A,
+                               int32_t gm_A, int32_t gp_A, const double* B, int32_t nrow_B,
+                               int32_t ncol_B, int32_t bw_B, int32_t alpha_B, int32_t beta_B,
+                               int32_t gm_B, int32_t gp_B, double* C, int32_t nrow_C,
+                               int32_t ncol_C, int32_t bw_C, int32_t alpha_C, int32_t beta_C,
+                               int32_t gm_C, int32_t gp_C);
+void or_columnwise_op_scaledadd_code(int32_t cell, int32_t ncell_2d, const double* A,
+                                     int32_t nrow_A, int32_t ncol_A, int32_t bw_A, int32_t alpha_A,
+                                     int32_t beta_A, int32_t gm_A, int32_t gp_A, const double* B,
+                                     int32_t nrow_B, int32_t ncol_B, int32_t bw_B, int32_t alpha_B,
+                                     int32_t beta_B, int32_t gm_B, int32_t gp_B, double* C,
+                                     int32_t nrow_C, int32_t ncol_C, int32_t bw_C, int32_t alpha_C,
+                                     int32_t beta_C, int32_t gm_C, int32_t gp_C, double alpha,
+                                     double beta);
+void or_columnwise_op_asm_m2v_lumped_inv_code(int32_t cell, int32_t nlayers, int32_t ncell_2d,
+                                              int32_t ncell_3d, const double* local_stencil,
+                                              double* C, int32_t nrow, int32_t bw, int32_t ndf,
+                                              const int32_t* column_banded_dofmap);
+void or_columnwise_op_asm_diag_hmht_code(int32_t cell, int32_t nlayers, int32_t ncell_2d,
+                                         int32_t ncell_3d, const double* Dh, const double* M2h,
+                                         double* C, int32_t nrow, int32_t bw, int32_t alpha,
+                                         int32_t beta, int32_t gamma_m, int32_t gamma_p,
+                                         int32_t ndf_w3, const int32_t* column_banded_dofmap,
+                                         int32_t ndf_w2h);
+
 /* LMA operator: y = A x, coloured loop over cell columns. maps [ncell_2d][ndf],
  * cells_in_colour Fortran (ncolours, maxc), 1-based. mode 0 = matrix_vector
  * (GH_INC after setval_c(y,0)), 1 = transpose_matrix_vector. */

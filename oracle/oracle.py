@@ -52,6 +52,15 @@ def lib():
                                                 f64p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                 C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p,
                                                 C.c_int32, i32p]
+        I = C.c_int32
+        band_args = [f64p, I, I, I, I, I, I, I]  # band, nrow, ncol, bw, alpha, beta, g_m, g_p
+        L.or_columnwise_op_mul_code.argtypes = [I, I] + band_args * 3
+        L.or_columnwise_op_scaledadd_code.argtypes = [I, I] + band_args * 3 + [C.c_double,
+                                                                               C.c_double]
+        L.or_columnwise_op_asm_m2v_lumped_inv_code.argtypes = [I, I, I, I, f64p, f64p, I, I, I,
+                                                               i32p]
+        L.or_columnwise_op_asm_diag_hmht_code.argtypes = [I, I, I, I, f64p, f64p, f64p, I, I, I,
+                                                          I, I, I, I, i32p, I]
         L.or_columnwise_op_app_code.argtypes = [C.c_int32, f64p, f64p, f64p, C.c_int32, C.c_int32,
                                                 C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                 C.c_int32, i32p, i32p, i32p, i32p]
@@ -200,3 +209,87 @@ def assemble_cma(lma_sub, ncell_2d, nlayers, params):
                                     ncol, bw, params["alpha"], params["beta"], params["gamma_m"],
                                     params["gamma_p"], ndf, cbd, ndf, cbd)
     return band
+
+
+# ------------------------------------------------------------------ CMA set-up
+class Band:
+    """A columnwise operator's band, Fortran (bw, nrow, ncell_2d) flattened,
+    with its parameters (columnwise_operator_mod.f90:42-114)."""
+
+    def __init__(self, ncell_2d, nrow, ncol, bw, alpha, beta, gamma_m, gamma_p, band=None):
+        self.ncell_2d, self.nrow, self.ncol, self.bw = ncell_2d, nrow, ncol, bw
+        self.alpha, self.beta, self.gamma_m, self.gamma_p = alpha, beta, gamma_m, gamma_p
+        self.band = (np.zeros(bw * nrow * ncell_2d) if band is None
+                     else np.ascontiguousarray(band, dtype=np.float64).reshape(-1))
+
+    def args(self):
+        return [self.band, self.nrow, self.ncol, self.bw, self.alpha, self.beta, self.gamma_m,
+                self.gamma_p]
+
+
+def _gcd(a, b):
+    while b:
+        a, b = b, a % b
+    return a
+
+
+def _ceil_div(a, b):
+    return -((-a) // b)
+
+
+def cma_params(alpha, beta, gamma_m, gamma_p):
+    """divide_by_gcd and the bandwidth 1 + ceiling((g_m + g_p)/beta)
+    (columnwise_operator_mod.f90:216-247, 316-332)."""
+    g = _gcd(alpha, beta)
+    if g > 1:
+        alpha, beta, gamma_m, gamma_p = alpha // g, beta // g, gamma_m // g, gamma_p // g
+    return alpha, beta, gamma_m, gamma_p, 1 + _ceil_div(gamma_m + gamma_p, beta)
+
+
+def cma_product(A: Band, B: Band) -> Band:
+    """columnwise_operator_product (columnwise_operator_mod.f90) + the mul kernel
+    over every column: C = A B."""
+    al, be, gm, gp, bw = cma_params(A.alpha * B.alpha, A.beta * B.beta,
+                                    B.alpha * A.gamma_m + A.beta * B.gamma_m,
+                                    B.alpha * A.gamma_p + A.beta * B.gamma_p)
+    Cb = Band(A.ncell_2d, A.nrow, B.ncol, bw, al, be, gm, gp)
+    for c in range(1, A.ncell_2d + 1):
+        lib().or_columnwise_op_mul_code(c, A.ncell_2d, *A.args(), *B.args(), *Cb.args())
+    return Cb
+
+
+def cma_scaledadd(A: Band, B: Band, alpha, beta) -> Band:
+    """columnwise_operator_sum + the scaledadd kernel: C = alpha A + beta B."""
+    al, be, gm, gp, bw = cma_params(A.alpha, A.beta, max(A.gamma_m, B.gamma_m),
+                                    max(A.gamma_p, B.gamma_p))
+    Cb = Band(A.ncell_2d, A.nrow, A.ncol, bw, al, be, gm, gp)
+    for c in range(1, A.ncell_2d + 1):
+        lib().or_columnwise_op_scaledadd_code(c, A.ncell_2d, *A.args(), *B.args(), *Cb.args(),
+                                              alpha, beta)
+    return Cb
+
+
+def cma_m2v_lumped_inv(local_stencil, ncell_2d, nlayers, ndf, cbd, nrow, bw, params):
+    """asm_m2v_lumped_inv over every column; cbd Fortran (ndf, nlayers) as a
+    (nlayers, ndf) C array."""
+    Cb = Band(ncell_2d, nrow, nrow, bw, *params)
+    cbd = np.ascontiguousarray(cbd, dtype=np.int32)
+    st = np.ascontiguousarray(local_stencil, dtype=np.float64).reshape(-1)
+    for c in range(1, ncell_2d + 1):
+        lib().or_columnwise_op_asm_m2v_lumped_inv_code(c, nlayers, ncell_2d, ncell_2d * nlayers,
+                                                       st, Cb.band, nrow, bw, ndf, cbd)
+    return Cb
+
+
+def cma_diag_hmht(Dh, M2h, ncell_2d, nlayers, ndf_w3, ndf_w2h, cbd, nrow, bw, params):
+    """asm_diag_hmht over every column (params = alpha, beta, gamma_m, gamma_p)."""
+    Cb = Band(ncell_2d, nrow, nrow, bw, *params)
+    cbd = np.ascontiguousarray(cbd, dtype=np.int32)
+    Dh = np.ascontiguousarray(Dh, dtype=np.float64).reshape(-1)
+    M2h = np.ascontiguousarray(M2h, dtype=np.float64).reshape(-1)
+    al, be, gm, gp = params
+    for c in range(1, ncell_2d + 1):
+        lib().or_columnwise_op_asm_diag_hmht_code(c, nlayers, ncell_2d, ncell_2d * nlayers, Dh, M2h,
+                                                  Cb.band, nrow, bw, al, be, gm, gp, ndf_w3, cbd,
+                                                  ndf_w2h)
+    return Cb

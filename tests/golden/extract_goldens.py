@@ -11,6 +11,8 @@ Sources (paths inside the reference project):
   components/science/unit-test/kernel/columnwise_operators/columnwise_op_appinv_kernel_mod_test.pf
   components/science/unit-test/kernel/columnwise_operators/columnwise_op_asm_kernel_mod_test.pf
   components/science/unit-test/kernel/columnwise_operators/columnwise_op_app_kernel_mod_test.pf
+  components/science/unit-test/kernel/columnwise_operators/columnwise_op_{mul,scaledadd,
+      asm_m2v_lumped_inv,asm_diag_hmht}_kernel_mod_test.pf
 """
 from __future__ import annotations
 
@@ -73,6 +75,48 @@ def cma_asm(text: str) -> dict:
             "reference_tol": fnum(re.search(r"tol\s*=\s*(" + NUM + ")", text).group(1))}
 
 
+def cma_mul(text: str) -> dict:
+    # D (W3 <- Wtheta) band entries 1, 2 and its transpose's, nlayers
+    nl = int(re.search(r"nlayers\s*=\s*(\d+)_i_def", text).group(1))
+    d1 = fnum(re.search(r"clm_mat_D\(1_i_def,i,cell\)\s*=\s*(" + NUM + ")", text).group(1))
+    d2 = fnum(re.search(r"clm_mat_D\(2_i_def,i,cell\)\s*=\s*(" + NUM + ")", text).group(1))
+    t1 = fnum(re.search(r"clm_mat_DT\(1_i_def,i,cell\)\s*=\s*(" + NUM + ")", text).group(1))
+    t2 = fnum(re.search(r"clm_mat_DT\(2_i_def,i,cell\)\s*=\s*(" + NUM + ")", text).group(1))
+    return {"nlayers": nl, "D_band": [d1, d2], "DT_band": [t1, t2],
+            "reference_tol": fnum(re.search(r"tol\s*=\s*(" + NUM + ")", text).group(1))}
+
+
+def cma_scaledadd(text: str) -> dict:
+    nl = int(re.search(r"nlayers\s*=\s*(\d+)_i_def", text).group(1))
+    mu = fnum(re.search(r"mu\s*=\s*(" + NUM + ")_r_solver", text).group(1))
+    nu = fnum(re.search(r"nu\s*=\s*(" + NUM + ")_r_solver", text).group(1))
+    dtd = [fnum(re.search(r"clm_mat_DTD\(%d,i,cell\)\s*=\s*(" % k + NUM + ")", text).group(1))
+           for k in (1, 2, 3)]
+    m1 = fnum(re.search(r"clm_mat_M\(1,i,cell\)\s*=\s*(" + NUM + ")", text).group(1))
+    return {"nlayers": nl, "mu": mu, "nu": nu, "DTD_band": dtd, "M_band": [m1],
+            "reference_tol": fnum(re.search(r"tol\s*=\s*(" + NUM + ")", text).group(1))}
+
+
+def cma_m2v_lumped_inv(text: str) -> dict:
+    nl = int(re.search(r"nlayers\s*=\s*(\d+)", text).group(1))
+    assert re.search(r"reshape\(\s*\(/\s*1\.0_r_solver/3\.0_r_solver,\s*1\.0_r_solver/6\.0_r_solver",
+                     text), "m2v stencil not found"
+    ends = fnum(re.search(r"answer\s*=\s*(" + NUM + r")_r_solver\s*\n", text).group(1))
+    inner = re.search(r"answer\s*=\s*\((" + NUM + r")_r_solver/(" + NUM + r")_r_solver\)", text)
+    return {"nlayers": nl, "local_stencil": [[1 / 3, 1 / 6], [1 / 6, 1 / 3]],
+            "answer_end_rows": ends, "answer_interior_rows": fnum(inner.group(1)) / fnum(inner.group(2)),
+            "reference_tol": fnum(re.search(r"tol\s*=\s*(" + NUM + ")", text).group(1))}
+
+
+def cma_diag_hmht(text: str) -> dict:
+    nl = int(re.search(r"nlayers\s*=\s*(\d+)", text).group(1))
+    rho = [fnum(re.search(r"rho\(%d\)\s*=\s*(" % k + NUM + ")", text).group(1)) for k in range(1, 5)]
+    sig = [fnum(re.search(r"sigma\(%d\)\s*=\s*(" % k + NUM + ")", text).group(1)) for k in range(1, 5)]
+    return {"nlayers": nl, "rho": rho, "sigma": sig,
+            "answer": sum(r * r / s for r, s in zip(rho, sig)),
+            "reference_tol": fnum(re.search(r"tol\s*=\s*(" + NUM + ")", text).group(1))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -85,6 +129,11 @@ def main():
         "cma_appinv": ut / "columnwise_operators/columnwise_op_appinv_kernel_mod_test.pf",
         "cma_app": ut / "columnwise_operators/columnwise_op_app_kernel_mod_test.pf",
         "cma_asm": ut / "columnwise_operators/columnwise_op_asm_kernel_mod_test.pf",
+        "cma_mul": ut / "columnwise_operators/columnwise_op_mul_kernel_mod_test.pf",
+        "cma_scaledadd": ut / "columnwise_operators/columnwise_op_scaledadd_kernel_mod_test.pf",
+        "cma_m2v_lumped_inv":
+            ut / "columnwise_operators/columnwise_op_asm_m2v_lumped_inv_kernel_mod_test.pf",
+        "cma_diag_hmht": ut / "columnwise_operators/columnwise_op_asm_diag_hmht_kernel_mod_test.pf",
     }
     out = {
         "matrix_vector": matrix_vector(src["matrix_vector"].read_text()),
@@ -92,6 +141,10 @@ def main():
         "cma_appinv": cma_band(src["cma_appinv"].read_text()),
         "cma_app": cma_band(src["cma_app"].read_text()),
         "cma_asm": cma_asm(src["cma_asm"].read_text()),
+        "cma_mul": cma_mul(src["cma_mul"].read_text()),
+        "cma_scaledadd": cma_scaledadd(src["cma_scaledadd"].read_text()),
+        "cma_m2v_lumped_inv": cma_m2v_lumped_inv(src["cma_m2v_lumped_inv"].read_text()),
+        "cma_diag_hmht": cma_diag_hmht(src["cma_diag_hmht"].read_text()),
     }
     for k, p in src.items():
         out[k]["source"] = str(p.relative_to(Path(a.ref)))

@@ -143,3 +143,75 @@ def test_blocked_sum_matches_exact(n):
     scale = math.fsum(np.abs(x * y).tolist()) if n else 1.0
     assert abs(blocked - exact) <= 1e-14 * max(scale, 1e-300) + 0.0
     assert abs(seq - exact) <= 1e-12 * max(scale, 1e-300) + 0.0
+
+
+def _dense_of_band(Cb, cell=1):
+    """Dense (nrow, ncol) matrix of one column of a band (zero outside the band)."""
+    D = np.zeros((Cb.nrow, Cb.ncol))
+    b = Cb.band.reshape(Cb.ncell_2d, Cb.nrow, Cb.bw)[cell - 1]
+    for i in range(1, Cb.nrow + 1):
+        jm = -((-(Cb.alpha * i - Cb.gamma_p)) // Cb.beta)
+        for q in range(Cb.bw):
+            j = jm + q
+            if 1 <= j <= Cb.ncol:
+                D[i - 1, j - 1] = b[i - 1, q]
+    return D
+
+
+def test_cma_mul_golden():
+    """columnwise_op_mul_kernel_mod_test.pf: D^T D of the W3 <- Wtheta
+    difference operator, against the dense product (sizes from get_cma_size)."""
+    g = G["cma_mul"]
+    nl = g["nlayers"]
+    # W3 <- Wtheta: nrow nl, ncol nl+1, alpha = beta = 1, g_m 1, g_p 0, bw 2
+    D = orc.Band(1, nl, nl + 1, 2, 1, 1, 1, 0, np.tile(g["D_band"], nl))
+    DT = orc.Band(1, nl + 1, nl, 2, 1, 1, 0, 1, np.tile(g["DT_band"], nl + 1))
+    C = orc.cma_product(DT, D)
+    assert (C.nrow, C.ncol, C.bw, C.gamma_m, C.gamma_p) == (nl + 1, nl + 1, 3, 1, 1)
+    Dd = np.zeros((nl, nl + 1))
+    for i in range(nl):
+        Dd[i, i], Dd[i, i + 1] = g["D_band"]
+    np.testing.assert_allclose(_dense_of_band(C), Dd.T @ Dd, atol=g["reference_tol"])
+    np.testing.assert_array_equal(_dense_of_band(C), Dd.T @ Dd)
+
+
+def test_cma_scaledadd_golden():
+    """columnwise_op_scaledadd_kernel_mod_test.pf: mu M + nu D^T D on W3."""
+    g = G["cma_scaledadd"]
+    nl = g["nlayers"]
+    M = orc.Band(1, nl, nl, 1, 1, 1, 0, 0, np.tile(g["M_band"], nl))
+    DTD = orc.Band(1, nl, nl, 3, 1, 1, 1, 1, np.tile(g["DTD_band"], nl))
+    C = orc.cma_scaledadd(M, DTD, g["mu"], g["nu"])
+    dense = g["mu"] * np.eye(nl) + g["nu"] * (2 * np.eye(nl) + np.eye(nl, k=1) + np.eye(nl, k=-1))
+    np.testing.assert_allclose(_dense_of_band(C), dense, atol=g["reference_tol"])
+
+
+def test_cma_m2v_lumped_inv_golden():
+    """columnwise_op_asm_m2v_lumped_inv_kernel_mod_test.pf: inverse lumped W2V
+    mass, 3 on the end rows and 3/2 inside (band index 1)."""
+    g = G["cma_m2v_lumped_inv"]
+    nl = g["nlayers"]
+    st = np.zeros((2, 2, nl))  # Fortran (ncell_3d, 2, 2) as [df2][df1][ik]
+    for k in range(nl):
+        st[:, :, k] = np.array(g["local_stencil"]).T
+    cbd = np.array([[k + 1, k + 2] for k in range(nl)], dtype=np.int32)  # col_bmap(df, k)
+    C = orc.cma_m2v_lumped_inv(st, 1, nl, 2, cbd, nl + 1, 3, (1, 1, 1, 1))
+    first = C.band.reshape(nl + 1, 3)[:, 0]
+    expect = [g["answer_end_rows"]] + [g["answer_interior_rows"]] * (nl - 1) + [g["answer_end_rows"]]
+    np.testing.assert_allclose(first, expect, rtol=0, atol=g["reference_tol"])
+    assert np.all(C.band.reshape(nl + 1, 3)[:, 1:] == 0.0)
+
+
+def test_cma_diag_hmht_golden():
+    """columnwise_op_asm_diag_hmht_kernel_mod_test.pf: sum_k rho_k^2 / sigma_k
+    on the W3 diagonal."""
+    g = G["cma_diag_hmht"]
+    nl = g["nlayers"]
+    Dh = np.zeros((4, 1, nl))  # Fortran (ncell_3d, 1, 4) as [df3][df1][ik]
+    M2h = np.zeros((4, 4, nl))
+    for k in range(nl):
+        Dh[:, 0, k] = g["rho"]
+        M2h[:, :, k] = np.diag(g["sigma"])
+    cbd = np.arange(1, nl + 1, dtype=np.int32).reshape(nl, 1)
+    C = orc.cma_diag_hmht(Dh, M2h, 1, nl, 1, 4, cbd, nl, 1, (1, 1, 0, 0))
+    np.testing.assert_allclose(C.band, g["answer"], rtol=0, atol=g["reference_tol"])

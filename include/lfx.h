@@ -212,6 +212,24 @@ int lfx_cma_get_band(const lfx_cma* cma, double* band);
 int lfx_cma_apply(lfx_cma* cma, const lfx_vec* x, lfx_vec* y);
 int lfx_cma_destroy(lfx_cma* cma);
 
+/* ------------------------------------------------------------------ W2 split / combine
+ * split_w2_field_kernel_mod.F90 / combine_w2_field_kernel_mod.F90 for the
+ * lowest-order spaces: W2 (6 dofs per cell, faces W S E N B T) to and from its
+ * horizontal part W2h (4) and vertical part W2v (2, one column of nlayers + 1
+ * dofs). Maps are Fortran (ndf, ncell_2d), 1-based; the face selectors
+ * (get_face_selector_ew / _ns: 1 or 2 per W3-2D dof) choose which cells copy
+ * their E and N faces, as in the reference. */
+typedef struct lfx_w2_split lfx_w2_split;
+int lfx_w2_split_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, const int32_t* map_w2,
+                        const int32_t* map_w2h, const int32_t* map_w2v, const int32_t* map_w3_2d,
+                        int64_t undf_w3_2d, const int32_t* face_selector_ew,
+                        const int32_t* face_selector_ns, lfx_w2_split** out);
+/* uv, w from uvw (split_w2_field) */
+int lfx_w2_split_field(lfx_w2_split* s, const lfx_vec* uvw, lfx_vec* uv, lfx_vec* w);
+/* uvw from uv, w (combine_w2_field) */
+int lfx_w2_combine_field(lfx_w2_split* s, const lfx_vec* uv, const lfx_vec* w, lfx_vec* uvw);
+int lfx_w2_split_destroy(lfx_w2_split* s);
+
 /* ------------------------------------------------------------------ preconditioners
  * apply writes y = P^{-1} x (sci_preconditioner_mod.f90:19-38). */
 int lfx_null_prec_create(lfx_ctx* ctx, lfx_prec** out);                 /* y = x        */

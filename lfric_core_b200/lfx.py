@@ -123,6 +123,11 @@ _SIGS = [
     ("lfx_cma_assemble_m2v_lumped_inv", [vp, i32p] + [C.c_int32] * 6 + [C.POINTER(vp)], C.c_int),
     ("lfx_cma_assemble_diag_hmht", [vp, vp, i32p] + [C.c_int32] * 6 + [C.POINTER(vp)],
      C.c_int),
+    ("lfx_w2_split_create", [vp, C.c_int32, C.c_int32, i32p, i32p, i32p, i32p, C.c_int64, i32p,
+                             i32p, C.POINTER(vp)], C.c_int),
+    ("lfx_w2_split_field", [vp, vp, vp, vp], C.c_int),
+    ("lfx_w2_combine_field", [vp, vp, vp, vp], C.c_int),
+    ("lfx_w2_split_destroy", [vp], C.c_int),
     ("lfx_cma_get_band", [vp, f64p], C.c_int),
     ("lfx_cma_apply", [vp, vp, vp], C.c_int),
     ("lfx_cma_destroy", [vp], C.c_int),
@@ -651,6 +656,30 @@ class ColumnwiseOperator(_Handle):
 
     def apply(self, x, y):
         self.ctx.check(self.ctx.L.lfx_cma_apply(self.h, x.h, y.h))
+
+
+class W2Split(_Handle):
+    """split_w2_field / combine_w2_field (lowest order): W2 <-> W2h + W2v.
+    Maps are (ncell_2d, ndf) 1-based arrays."""
+
+    _destroy = "lfx_w2_split_destroy"
+
+    def __init__(self, ctx, nlayers, map_w2, map_w2h, map_w2v, map_w3_2d, undf_w3_2d,
+                 face_selector_ew, face_selector_ns):
+        self.ctx = ctx
+        h = vp()
+        as_i = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        ctx.check(ctx.L.lfx_w2_split_create(ctx.h, len(map_w2), nlayers, as_i(map_w2),
+                                            as_i(map_w2h), as_i(map_w2v), as_i(map_w3_2d),
+                                            undf_w3_2d, as_i(face_selector_ew),
+                                            as_i(face_selector_ns), C.byref(h)))
+        self.h = h
+
+    def split(self, uvw, uv, w):
+        self.ctx.check(self.ctx.L.lfx_w2_split_field(self.h, uvw.h, uv.h, w.h))
+
+    def combine(self, uv, w, uvw):
+        self.ctx.check(self.ctx.L.lfx_w2_combine_field(self.h, uv.h, w.h, uvw.h))
 
 
 class _Prec(_Handle):

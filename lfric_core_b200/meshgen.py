@@ -204,3 +204,21 @@ def w2v_cma_params(nlayers: int):
     ind = np.arange(1, nrow + 1, dtype=np.int32)
     return dict(alpha=1, beta=1, gamma_m=1, gamma_p=1, bandwidth=3, nrow=nrow, ncol=nrow,
                 column_banded_dofmap=cbd, indirection=ind)
+
+
+def w2_subspace_maps(map_w2: np.ndarray, nlayers: int):
+    """Dofmaps of the W2h and W2v parts and of W3-2D for a lowest-order W2
+    dofmap (faces W S E N B T), column-contiguous as dofmap_setup numbers
+    them: each horizontal face column keeps its nlayers dofs, each vertical
+    face column its nlayers + 1, in the order of their W2 numbering. Returns
+    (map_w2h, undf_w2h, map_w2v, undf_w2v, map_w3_2d, undf_w3_2d)."""
+    m = np.asarray(map_w2)
+    hb = np.unique(m[:, :4])
+    hidx = {int(b): i for i, b in enumerate(hb)}
+    map_h = np.vectorize(lambda b: hidx[int(b)] * nlayers + 1)(m[:, :4]).astype(np.int32)
+    vb = np.unique(m[:, 4])
+    vidx = {int(b): i for i, b in enumerate(vb)}
+    bot = np.array([vidx[int(b)] * (nlayers + 1) + 1 for b in m[:, 4]], dtype=np.int32)
+    map_v = np.stack([bot, bot + 1], axis=1)
+    map_3 = np.arange(1, len(m) + 1, dtype=np.int32).reshape(-1, 1)
+    return map_h, len(hb) * nlayers, map_v, len(vb) * (nlayers + 1), map_3, len(m)

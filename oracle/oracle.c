@@ -400,6 +400,58 @@ void or_columnwise_op_asm_diag_hmht_code(int32_t cell, int32_t nlayers, int32_t 
 }
 #undef BAND
 
+/* face_selector_code, sci_face_selector_kernel_mod.F90: the first cell (in
+ * loop order) whose E (N) face a W2h face is marks it and selects 2 */
+void or_face_selector_code(int32_t* face_selector_ew, int32_t* face_selector_ns,
+                           int32_t* face_counter, const int32_t* map_w3, const int32_t* map_w2h) {
+  const int32_t e = map_w2h[2] - 1, nn = map_w2h[3] - 1, c3 = map_w3[0] - 1;
+  if (face_counter[e] == 0) {
+    face_selector_ew[c3] = 2;
+    face_counter[e] = 1;
+  }
+  if (face_counter[nn] == 0) {
+    face_selector_ns[c3] = 2;
+    face_counter[nn] = 1;
+  }
+}
+
+/* the horizontal faces a cell copies: W, S, then E or N (or both), as
+ * split_w2_field_code / combine_w2_field_code select them */
+static int32_t hori_faces(const int32_t* ew, const int32_t* ns, const int32_t* map_w3_2d,
+                          int32_t* dof3) {
+  const int32_t c = map_w3_2d[0] - 1;
+  *dof3 = (ns[c] == 2 && ew[c] == 1) ? 4 : 3; /* N = 4, E = 3 */
+  return ew[c] + ns[c];
+}
+
+/* split_w2_field_code_r_double, split_w2_field_kernel_mod.F90 (lowest order) */
+void or_split_w2_field_code(int32_t nlayers, double* uv, double* w, const double* uvw,
+                            const int32_t* face_selector_ew, const int32_t* face_selector_ns,
+                            const int32_t* map_w2h, const int32_t* map_w2v, const int32_t* map_w2,
+                            const int32_t* map_w3_2d) {
+  int32_t dof3;
+  const int32_t todo = hori_faces(face_selector_ew, face_selector_ns, map_w3_2d, &dof3);
+  for (int32_t j = 1; j <= todo; ++j) {
+    const int32_t df = (j == 3) ? dof3 : j;
+    for (int32_t k = 0; k <= nlayers - 1; ++k) uv[map_w2h[df - 1] - 1 + k] = uvw[map_w2[df - 1] - 1 + k];
+  }
+  for (int32_t k = 0; k <= nlayers; ++k) w[map_w2v[0] - 1 + k] = uvw[map_w2[4] - 1 + k];
+}
+
+/* combine_w2_field_code_r_double, combine_w2_field_kernel_mod.F90 (lowest order) */
+void or_combine_w2_field_code(int32_t nlayers, double* uvw, const double* uv, const double* w,
+                              const int32_t* face_selector_ew, const int32_t* face_selector_ns,
+                              const int32_t* map_w2, const int32_t* map_w2h,
+                              const int32_t* map_w2v, const int32_t* map_w3_2d) {
+  int32_t dof3;
+  const int32_t todo = hori_faces(face_selector_ew, face_selector_ns, map_w3_2d, &dof3);
+  for (int32_t j = 1; j <= todo; ++j) {
+    const int32_t df = (j == 3) ? dof3 : j;
+    for (int32_t k = 0; k <= nlayers - 1; ++k) uvw[map_w2[df - 1] - 1 + k] = uv[map_w2h[df - 1] - 1 + k];
+  }
+  for (int32_t k = 0; k <= nlayers; ++k) uvw[map_w2[4] - 1 + k] = w[map_w2v[0] - 1 + k];
+}
+
 or_op* or_lma_create(int32_t ncell_2d, int32_t nlayers, int32_t ndf_to, int32_t ndf_from,
                      const int32_t* map_to, const int32_t* map_from, int64_t undf_to,
                      int64_t undf_from, const double* stencil, int32_t ncolours,

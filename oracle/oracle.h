@@ -113,6 +113,23 @@ void or_columnwise_op_asm_diag_hmht_code(int32_t cell, int32_t nlayers, int32_t 
                                          int32_t ndf_w3, const int32_t* column_banded_dofmap,
                                          int32_t ndf_w2h);
 
+/* W2 split / combine for the lowest-order spaces (ndf_w2 6, ndf_w2h 4,
+ * ndf_w2v 2), one cell (maps of that cell, 1-based):
+ *   face_selector  sci_face_selector_kernel_mod.F90 (face_counter on W2h)
+ *   split          split_w2_field_kernel_mod.F90 (uvw -> uv, w)
+ *   combine        combine_w2_field_kernel_mod.F90 (uv, w -> uvw)
+ * Arrays are 0-based host arrays indexed by the 1-based map values minus 1. */
+void or_face_selector_code(int32_t* face_selector_ew, int32_t* face_selector_ns,
+                           int32_t* face_counter, const int32_t* map_w3, const int32_t* map_w2h);
+void or_split_w2_field_code(int32_t nlayers, double* uv, double* w, const double* uvw,
+                            const int32_t* face_selector_ew, const int32_t* face_selector_ns,
+                            const int32_t* map_w2h, const int32_t* map_w2v, const int32_t* map_w2,
+                            const int32_t* map_w3_2d);
+void or_combine_w2_field_code(int32_t nlayers, double* uvw, const double* uv, const double* w,
+                              const int32_t* face_selector_ew, const int32_t* face_selector_ns,
+                              const int32_t* map_w2, const int32_t* map_w2h,
+                              const int32_t* map_w2v, const int32_t* map_w3_2d);
+
 /* LMA operator: y = A x, coloured loop over cell columns. maps [ncell_2d][ndf],
  * cells_in_colour Fortran (ncolours, maxc), 1-based. mode 0 = matrix_vector
  * (GH_INC after setval_c(y,0)), 1 = transpose_matrix_vector. */

@@ -61,6 +61,11 @@ def lib():
                                                                i32p]
         L.or_columnwise_op_asm_diag_hmht_code.argtypes = [I, I, I, I, f64p, f64p, f64p, I, I, I,
                                                           I, I, I, I, i32p, I]
+        L.or_face_selector_code.argtypes = [i32p, i32p, i32p, i32p, i32p]
+        L.or_split_w2_field_code.argtypes = [C.c_int32, f64p, f64p, f64p, i32p, i32p, i32p, i32p,
+                                             i32p, i32p]
+        L.or_combine_w2_field_code.argtypes = [C.c_int32, f64p, f64p, f64p, i32p, i32p, i32p,
+                                               i32p, i32p, i32p]
         L.or_columnwise_op_app_code.argtypes = [C.c_int32, f64p, f64p, f64p, C.c_int32, C.c_int32,
                                                 C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                 C.c_int32, i32p, i32p, i32p, i32p]
@@ -293,3 +298,40 @@ def cma_diag_hmht(Dh, M2h, ncell_2d, nlayers, ndf_w3, ndf_w2h, cbd, nrow, bw, pa
                                                   Cb.band, nrow, bw, al, be, gm, gp, ndf_w3, cbd,
                                                   ndf_w2h)
     return Cb
+
+
+# ------------------------------------------------------------------ W2 split / combine
+def face_selectors(map_w3_2d, map_w2h, undf_w3_2d, undf_w2h):
+    """compute_face_selectors (sci_geometric_constants_mod.x90:203-253): both
+    selectors set to 1, then face_selector_code over the cells in order."""
+    ew = np.ones(undf_w3_2d, dtype=np.int32)
+    ns = np.ones(undf_w3_2d, dtype=np.int32)
+    cnt = np.zeros(undf_w2h, dtype=np.int32)
+    m3 = np.ascontiguousarray(map_w3_2d, dtype=np.int32)
+    mh = np.ascontiguousarray(map_w2h, dtype=np.int32)
+    for c in range(m3.shape[0]):
+        lib().or_face_selector_code(ew, ns, cnt, m3[c].copy(), mh[c].copy())
+    return ew, ns
+
+
+def split_w2(nlayers, uvw, maps, ew, ns, undf_w2h, undf_w2v):
+    """split_w2_field over every cell: returns (uv, w); maps = dict of
+    (ncell, ndf) 1-based maps w2, w2h, w2v, w3_2d."""
+    uv, w = np.zeros(undf_w2h), np.zeros(undf_w2v)
+    uvw = np.ascontiguousarray(uvw, dtype=np.float64)
+    m = {k: np.ascontiguousarray(v, dtype=np.int32) for k, v in maps.items()}
+    for c in range(m["w2"].shape[0]):
+        lib().or_split_w2_field_code(nlayers, uv, w, uvw, ew, ns, m["w2h"][c].copy(),
+                                     m["w2v"][c].copy(), m["w2"][c].copy(), m["w3_2d"][c].copy())
+    return uv, w
+
+
+def combine_w2(nlayers, uv, w, maps, ew, ns, undf_w2):
+    uvw = np.zeros(undf_w2)
+    uv = np.ascontiguousarray(uv, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    m = {k: np.ascontiguousarray(v, dtype=np.int32) for k, v in maps.items()}
+    for c in range(m["w2"].shape[0]):
+        lib().or_combine_w2_field_code(nlayers, uvw, uv, w, ew, ns, m["w2"][c].copy(),
+                                       m["w2h"][c].copy(), m["w2v"][c].copy(), m["w3_2d"][c].copy())
+    return uvw

@@ -581,7 +581,7 @@ def main():
     achieved = bytes32 / (avg32 / 1e3) / 1e9
     peak, peak_kind = measured_hbm_peak()
     traffic = profiled_traffic()
-    roof = {"kernel": "lma_gather<float,6> (FP32 LMA apply)", "bound": "hbm",
+    roof = {"kernel": f"{tuning['fp32']['kernel']} (FP32 LMA apply)", "bound": "hbm",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": traffic, "algorithmic_bytes_per_launch": bytes32,

@@ -114,14 +114,16 @@ int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y);
 int lfx_op_destroy(lfx_op* op);
 /* Apply autotuner (no counterpart in the reference, whose loop shape is fixed
  * by PSyclone): times each launch configuration of the apply on this
- * operator -- register gather with and without metadata lookahead, the
- * bulk-copy pipeline with 2..8 stages and 1..8 warps per block, and the
- * copy-staged pipeline with 2..6 stages and 2..8 warps, those that fit the
- * shared memory -- over `reps` launches and
- * keeps the fastest for later applies. Outputs (nullable) name the choice:
- * kernel 0 pipeline / 1 register gather / 2 generic / 3 register gather with
- * metadata lookahead / 4 copy-staged pipeline (matrix blocks and x values
- * both staged in shared memory), and its time per apply. */
+ * operator -- the register gather, the register gather with prefetched
+ * column descriptors (at two register caps, stages 0 and 1; columns reading
+ * at most two blocks from at most two cells, e.g. W2 and W3), the bulk-copy
+ * pipeline with 2..8 stages and 1..8 warps per block, and the copy-staged
+ * pipeline with 2..6 stages and 2..8 warps, those that fit the shared memory
+ * -- over `reps` launches and keeps the fastest for later applies. Outputs
+ * (nullable) name the choice: kernel 0 pipeline / 1 register gather / 2
+ * generic / 3 register gather with prefetched descriptors / 4 copy-staged
+ * pipeline (matrix blocks and x values both staged in shared memory), and its
+ * time per apply. */
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
                     float* us);
 /* time one configuration (as above) without keeping it */
@@ -339,7 +341,8 @@ int64_t lfx_ctx_launch_count(const lfx_ctx* ctx);
 /* LMA apply kernel for every operator of the context: -1 = each operator's
  * autotuned choice, else the register gather (default); 0 = force the
  * bulk-copy pipeline; 1 = force the register gather; 3 = force the register
- * gather with metadata lookahead; 4 = force the copy-staged pipeline. All give
+ * gather with prefetched descriptors (the register gather where the operator
+ * does not fit it); 4 = force the copy-staged pipeline. All give
  * bit-identical results. */
 int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which);
 /* LFX_TIMEOUT if a kernel's bounded device-side wait ran out since the last

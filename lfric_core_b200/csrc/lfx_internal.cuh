@@ -292,6 +292,11 @@ struct lfx_lma_layout {
   // blocks} then per group {cell, record, map_from row} (0 when not built)
   int32_t* desc = nullptr;
   int32_t desc_ipl = 0;
+  // per entity column fd_ints ints for the prefetching gather: {base, h,
+  // groups, 0} then per group {cell, record, map_from row} padded to 4 ints
+  // (built when a column reads at most two blocks from at most two cells)
+  int32_t* fdesc = nullptr;
+  int32_t fd_ints = 0;
   int32_t max_groups = 0;  // groups of one entity column, at most
   int32_t max_blocks = 0;  // (cell, df) matrix blocks one entity column reads, at most
   int refcount = 1;

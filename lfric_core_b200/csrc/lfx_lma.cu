@@ -40,12 +40,14 @@ struct LayoutArgs {
   const int32_t* grp_pack;
   int32_t gp_stride;
   const int32_t* desc;
+  const int32_t* fdesc;
 };
 
 LayoutArgs args_of(const lfx_lma_layout* L, int blk) {
   return LayoutArgs{L->nent,     L->nlayers,  L->ndf_to,   L->ndf_from, blk,
                     L->ent_base, L->ent_h,    L->ent_grp,  L->grp_cell, L->grp_rec,
-                    L->map_from, L->ent_pack, L->grp_pack, L->gp_stride, L->desc};
+                    L->map_from, L->ent_pack, L->grp_pack, L->gp_stride, L->desc,
+                    L->fdesc};
 }
 
 // packed group record: bits 0-1 nrec (1..3); record r at bit 2+9r: df (6 bits), off (3 bits)
@@ -265,82 +267,92 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
   }
 }
 
-// Group record as int4 vectors (NI of them) and its decoding.
-template <int NDF2>
-struct GroupRec {
-  static constexpr int NI = NDF2 > 6 ? 3 : (NDF2 > 2 ? 2 : 1);
-  int4 v[NI];
-  __device__ __forceinline__ void load(const LayoutArgs& A, int g) {
-    const int4* gp4 = reinterpret_cast<const int4*>(A.grp_pack + (size_t)g * A.gp_stride);
-#pragma unroll
-    for (int i = 0; i < NI; ++i) v[i] = __ldg(gp4 + i);
-  }
-  __device__ __forceinline__ void decode(int& c, uint32_t& pk, int* mf) const {
-    c = v[0].x;
-    pk = (uint32_t)v[0].y;
-    int tmp[12];
-    tmp[0] = v[0].z;
-    tmp[1] = v[0].w;
-    if (NI > 1) {
-      tmp[2] = v[NI > 1 ? 1 : 0].x;
-      tmp[3] = v[NI > 1 ? 1 : 0].y;
-      tmp[4] = v[NI > 1 ? 1 : 0].z;
-      tmp[5] = v[NI > 1 ? 1 : 0].w;
-    }
-    if (NI > 2) {
-      tmp[6] = v[NI > 2 ? 2 : 0].x;
-      tmp[7] = v[NI > 2 ? 2 : 0].y;
-    }
-#pragma unroll
-    for (int j = 0; j < NDF2; ++j) mf[j] = tmp[j];
-  }
-};
+// Per-column descriptor of lma_fetch (columns reading at most two (cell, df)
+// blocks from at most two cells): ints {base, h, groups, 0}, then per group
+// {cell, record, map_from row} padded to a multiple of 4 ints.
+__host__ __device__ constexpr int fd_group_ints(int ndf2) { return (2 + ndf2 + 3) / 4 * 4; }
+__host__ __device__ constexpr int fd_ints(int ndf2) { return 4 + 2 * fd_group_ints(ndf2); }
 
-// The register gather with metadata lookahead: while a warp computes entity
-// column e it already holds the pack of e + nwarp and loads the records of
-// its first two groups, and the pack of e + 2 nwarp, so only the matrix and x
-// loads of each column wait on memory. Same arithmetic (and bits) as
-// lma_gather2.
-template <class T, int NDF2>
-__global__ void __launch_bounds__(256) lma_gather3(LayoutArgs A, const T* __restrict__ M,
-                                                   const T* __restrict__ x, T* __restrict__ y,
-                                                   const T* __restrict__ b, const int* skip) {
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The register gather with its column descriptors prefetched: each warp keeps
+// the descriptors of its next kFetchDepth columns in flight (16-byte cp.async
+// into a per-warp ring in shared memory), so a column waits on memory once,
+// for its matrix rows and x values, which all lanes issue before the first
+// FMA. Columns of two one-record groups (horizontal W2 faces) load both
+// groups at once; a column of one group goes through group_acc. Same sums in
+// the same order (and bits) as lma_gather2.
+constexpr int kFetchDepth = 4;
+
+template <class T, int NDF2, int MINB>
+__global__ void __launch_bounds__(256, MINB) lma_fetch(LayoutArgs A, const T* __restrict__ M,
+                                                 const T* __restrict__ x, T* __restrict__ y,
+                                                 const T* __restrict__ b, const int* skip) {
+  constexpr int GS = fd_group_ints(NDF2), FS = fd_ints(NDF2), NV = FS / 4;
+  __shared__ __align__(16) int ring[8][kFetchDepth][FS];
   if (skip && *((volatile const int*)skip)) return;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nl = A.nlayers;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t e0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const size_t cell_stride = (size_t)A.ndf1 * A.blk;
-  const int4 zero = make_int4(0, 0, 0, 0);
-  int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (e >= A.nent) return;
-  int4 ep = __ldg(A.ent_pack + e);
-  int4 epn = e + nwarp < A.nent ? __ldg(A.ent_pack + e + nwarp) : zero;
-  GroupRec<NDF2> r0, r1;
-  if (ep.z < ep.w) r0.load(A, ep.z);
-  if (ep.z + 1 < ep.w) r1.load(A, ep.z + 1);
-  for (; e < A.nent; e += nwarp) {
-    // lookahead loads for the next two columns
-    GroupRec<NDF2> s0, s1;
-    if (epn.z < epn.w) s0.load(A, epn.z);
-    if (epn.z + 1 < epn.w) s1.load(A, epn.z + 1);
-    const int4 ep2 = e + 2 * nwarp < A.nent ? __ldg(A.ent_pack + e + 2 * nwarp) : zero;
-    const int base = ep.x, h = ep.y, g0 = ep.z, g1 = ep.w;
+  const int4* fd = reinterpret_cast<const int4*>(A.fdesc);
+#pragma unroll
+  for (int s = 0; s < kFetchDepth; ++s) {
+    const int64_t e = e0 + s * nwarp;
+    if (lane < NV && e < A.nent) cp_async16(&ring[wib][s][4 * lane], fd + e * NV + lane);
+    cp_async_commit();
+  }
+  int s = 0;
+  for (int64_t e = e0; e < A.nent; e += nwarp) {
+    cp_async_wait<kFetchDepth - 1>();
+    __syncwarp();
+    // fields are read from the ring where they are used (fewer live registers)
+    const int* d = ring[wib][s];
+    const int4 hd = *reinterpret_cast<const int4*>(d);
+    const int base = hd.x, h = hd.y, ng = hd.z;
     for (int l0 = 0; l0 < h; l0 += 32) {
       const int l = l0 + lane;
       T acc = T(0);
-      for (int g = g0; g < g1; ++g) {
-        int c;
-        uint32_t pk;
-        int mf[NDF2];
-        if (g == g0) {
-          r0.decode(c, pk, mf);
-        } else if (g == g0 + 1) {
-          r1.decode(c, pk, mf);
-        } else {
-          GroupRec<NDF2> rr;
-          rr.load(A, g);
-          rr.decode(c, pk, mf);
+      if (ng == 2) {
+        // two cells, one record each: every load of both before the FMAs
+        const uint32_t pk0 = (uint32_t)d[5], pk1 = (uint32_t)d[5 + GS];
+        const int k0 = l - rec_off(pk0, 0), k1 = l - rec_off(pk1, 0);
+        const bool v0 = (unsigned)k0 < (unsigned)nl, v1 = (unsigned)k1 < (unsigned)nl;
+        const T* M0 = M + (size_t)d[4] * cell_stride + (size_t)rec_df(pk0, 0) * A.blk + (v0 ? k0 : 0);
+        const T* M1 = M + (size_t)d[4 + GS] * cell_stride + (size_t)rec_df(pk1, 0) * A.blk + (v1 ? k1 : 0);
+        T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) {
+          a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+          a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
         }
-        acc = group_acc<T, NDF2>(A, M, x, cell_stride, l, lane, c, pk, mf, acc);
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) {
+          b0[j] = v0 ? __ldg(x + (d[6 + j] + k0)) : T(0);
+          b1[j] = v1 ? __ldg(x + (d[6 + GS + j] + k1)) : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j)
+          if (v0) acc = fmaT(a0[j], b0[j], acc);
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j)
+          if (v1) acc = fmaT(a1[j], b1[j], acc);
+      } else if (ng == 1) {
+        int mf[NDF2];
+#pragma unroll
+        for (int j = 0; j < NDF2; ++j) mf[j] = d[6 + j];
+        acc = group_acc<T, NDF2>(A, M, x, cell_stride, l, lane, d[4], (uint32_t)d[5], mf, acc);
       }
       if (l < h) {
         if (b)
@@ -349,11 +361,14 @@ __global__ void __launch_bounds__(256) lma_gather3(LayoutArgs A, const T* __rest
           y[base + l] = acc;
       }
     }
-    ep = epn;
-    epn = ep2;
-    r0 = s0;
-    r1 = s1;
+    __syncwarp();
+    // the slot is free again: fetch the descriptor kFetchDepth columns ahead
+    const int64_t en = e + kFetchDepth * nwarp;
+    if (lane < NV && en < A.nent) cp_async16(&ring[wib][s][4 * lane], fd + en * NV + lane);
+    cp_async_commit();
+    s = s + 1 == kFetchDepth ? 0 : s + 1;
   }
+  cp_async_wait<0>();
 }
 
 // Shared-memory layout of one warp in lma_tma: S stages, each holding up to
@@ -900,6 +915,26 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
       }
       up((void**)&L->desc, d.data(), d.size() * 4);
     }
+    // descriptors of the prefetching gather (at most two blocks from at most
+    // two cells per column)
+    if (max_blocks <= 2 && max_groups <= 2 && (ndf_from == 1 || ndf_from == 6 || ndf_from == 8)) {
+      const int gs = fd_group_ints(ndf_from), fs = fd_ints(ndf_from);
+      L->fd_ints = fs;
+      std::vector<int32_t> d((size_t)L->nent * fs, 0);
+      for (int32_t e = 0; e < L->nent; ++e) {
+        int32_t* row = &d[(size_t)e * fs];
+        row[0] = ent_base[e];
+        row[1] = ent_h[e];
+        row[2] = ent_grp[e + 1] - ent_grp[e];
+        for (int32_t g = ent_grp[e]; g < ent_grp[e + 1]; ++g) {
+          int32_t* gr = row + 4 + (g - ent_grp[e]) * gs;
+          gr[0] = grp_cell[g];
+          gr[1] = (int32_t)grp_rec[g];
+          for (int j = 0; j < ndf_from; ++j) gr[2 + j] = mf0[(size_t)grp_cell[g] * ndf_from + j];
+        }
+      }
+      up((void**)&L->fdesc, d.data(), d.size() * 4);
+    }
   }
   return rc;
 }
@@ -914,6 +949,7 @@ void free_layout(lfx_ctx* ctx, lfx_lma_layout* L) {
   dfree(ctx, L->ent_pack, (size_t)L->nent * sizeof(int4));
   dfree(ctx, L->grp_pack, (size_t)L->ngrp * L->gp_stride * 4);
   dfree(ctx, L->desc, (size_t)L->nent * 32 * L->desc_ipl * 4);
+  dfree(ctx, L->fdesc, (size_t)L->nent * L->fd_ints * 4);
   dfree(ctx, L->map_from, (size_t)L->ncell_2d * L->ndf_from * 4);
   dfree(ctx, L->map_to, (size_t)L->ncell_2d * L->ndf_to * 4);
   free_layout(ctx, L->tlay);
@@ -1096,8 +1132,41 @@ void launch_tma(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const TmaSh
       op->lay->max_blocks, ctx->d_err);
 }
 
+// descriptor-prefetch gather (kernel 3): columns of at most two blocks from
+// at most two cells, ndf_from 1, 6 or 8
+bool fetch_ok(const lfx_op* op) {
+  const lfx_lma_layout* L = op->lay;
+  return L->fdesc && L->max_blocks <= 2 && L->max_groups <= 2 &&
+         (L->ndf_from == 1 || L->ndf_from == 6 || L->ndf_from == 8);
+}
+
+// one resident wave of blocks: each warp walks its columns with the
+// descriptors of the next kFetchDepth in flight. variant 0 caps registers for
+// 3 blocks of 256 per SM, variant 1 for 4 (FP32) / 2 (FP64).
+template <class T, int N, int MINB>
+void launch_fetch_t(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, const void* x, void* y,
+                    const void* b, const int* skip) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_fetch<T, N, MINB>, 256, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int grid = (int)std::min<int64_t>(((int64_t)A.nent + 7) / 8, (int64_t)ctx->num_sms * per_sm);
+  lma_fetch<T, N, MINB><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y,
+                                                        (const T*)b, skip);
+}
+
+template <class T, int N>
+void launch_fetch(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, int variant, const void* x,
+                  void* y, const void* b, const int* skip) {
+  if (variant == 1)
+    launch_fetch_t<T, N, sizeof(T) == 8 ? 2 : 4>(ctx, op, A, x, y, b, skip);
+  else
+    launch_fetch_t<T, N, 3>(ctx, op, A, x, y, b, skip);
+}
+
 // kernel: 0 bulk-copy pipelined (shape ts), 1 register gather, 2 generic,
-// 3 register gather with metadata lookahead, 4 copy-staged pipeline (shape ts)
+// 3 register gather with prefetched descriptors, 4 copy-staged pipeline (shape ts)
 template <class T>
 void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& ts,
                     const void* x, void* y, const void* b, const int* skip) {
@@ -1124,9 +1193,9 @@ void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& 
   }
   if (kernel == 3) {
     switch (L->ndf_from) {
-      case 1: lma_gather3<T, 1><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
-      case 6: lma_gather3<T, 6><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
-      default: lma_gather3<T, 8><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y, (const T*)b, skip); return;
+      case 1: launch_fetch<T, 1>(ctx, op, A, ts.stages, x, y, b, skip); return;
+      case 6: launch_fetch<T, 6>(ctx, op, A, ts.stages, x, y, b, skip); return;
+      default: launch_fetch<T, 8>(ctx, op, A, ts.stages, x, y, b, skip); return;
     }
   }
   lma_gather<T><<<grid, 256, 0, ctx->stream>>>(A, (const T*)op->mat, (const T*)x, (T*)y,
@@ -1155,8 +1224,12 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     *ts = tma_default(op);
     if (ts->warps) return;
   }
+  if (ctx->lma_kernel == 3 && fetch_ok(op)) {
+    *kernel = 3;
+    return;
+  }
   if ((ctx->lma_kernel == 1 || ctx->lma_kernel == 3) && gather2_ok(op)) {
-    *kernel = ctx->lma_kernel;
+    *kernel = 1;
     return;
   }
   if (ctx->lma_kernel == 4 && pipe_ok(op)) {
@@ -1168,6 +1241,7 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     *kernel = op->tune_kernel;
     if (*kernel == 0) *ts = tma_shape(op, op->tune_stages, op->tune_warps);
     if (*kernel == 4) *ts = pipe_shape(op, op->tune_stages, op->tune_warps);
+    if (*kernel == 3) ts->stages = op->tune_stages;
     if ((*kernel != 0 && *kernel != 4) || ts->warps) return;
   }
   *kernel = gather2_ok(op) ? 1 : 2;
@@ -1324,8 +1398,13 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
     ts = kernel == 0 ? tma_shape(op, stages, warps) : pipe_shape(op, stages, warps);
     if (!ts.warps) return fail(ctx, LFX_NOT_SUPPORTED, "configuration does not fit this operator");
   }
-  if ((kernel == 1 || kernel == 3) && !gather2_ok(op))
+  if (kernel == 1 && !gather2_ok(op))
     return fail(ctx, LFX_NOT_SUPPORTED, "register gather does not fit this operator");
+  if (kernel == 3) {
+    if (!fetch_ok(op) || stages < 0 || stages > 1)
+      return fail(ctx, LFX_NOT_SUPPORTED, "prefetching gather does not fit this operator");
+    ts.stages = stages;
+  }
   const size_t esz = op->precision == LFX_R64 ? 8 : 4;
   void *x = nullptr, *y = nullptr;
   int rc = dmalloc(ctx, &x, L->undf_from * esz);
@@ -1354,7 +1433,7 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
 }
 
 // Picks the fastest apply configuration for this operator by timing the
-// candidates (register gather with and without metadata lookahead; bulk-copy
+// candidates (register gather, the prefetching gather at two register caps, bulk-copy
 // pipeline with 2..8 stages and 1..8 warps per block that fit the shared
 // memory) and keeps it for later applies.
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
@@ -1378,7 +1457,8 @@ int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, 
   int rc = LFX_OK;
   if (gather2_ok(op)) {
     rc = consider(1, 0, 0);
-    if (!rc) rc = consider(3, 0, 0);
+    if (!rc && fetch_ok(op)) rc = consider(3, 0, 0);
+    if (!rc && fetch_ok(op)) rc = consider(3, 1, 0);
   } else {
     rc = consider(2, 0, 0);
   }

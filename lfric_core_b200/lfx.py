@@ -246,7 +246,7 @@ class Context:
     def set_apply_kernel(self, which: int):
         """-1: per-operator choice (autotuned, else register gather), 0: bulk-copy
         pipelined LMA apply, 1: register gather, 3: register gather with
-        metadata lookahead, 4: copy-staged pipeline."""
+        prefetched column descriptors, 4: copy-staged pipeline."""
         self.check(self.L.lfx_ctx_set_apply_kernel(self.h, which))
 
     def check_device_error(self):
@@ -399,7 +399,7 @@ class LmaOperator(_Handle):
         self.ctx.check(self.ctx.L.lfx_op_autotune(self.h, reps, C.byref(k), C.byref(s),
                                                    C.byref(w), C.byref(us)))
         name = {0: "pipeline", 1: "register-gather", 2: "generic",
-                3: "register-gather-lookahead", 4: "staged-pipeline"}[k.value]
+                3: "register-gather-prefetch", 4: "staged-pipeline"}[k.value]
         return {"kernel": name, "stages": s.value, "warps": w.value, "us": round(us.value, 2)}
 
     def time_apply(self, kernel: int, stages: int = 0, warps: int = 0, reps: int = 10):

@@ -162,8 +162,12 @@ def _run_apply(args):
     op = _lma(ctx, p, prec)
     x = lfx.FieldVector.from_array(ctx, mg.normal(3, p.undf), prec)
     y = lfx.FieldVector(ctx, [p.undf], prec)
-    for k in [int(v) for v in args.kernels.split(",")]:
-        ctx.set_apply_kernel(k)
+    for v in args.kernels.split(","):
+        if v == "tuned":
+            print(op.autotune(reps=5), flush=True)
+            ctx.set_apply_kernel(-1)
+        else:
+            ctx.set_apply_kernel(int(v))
         for _ in range(args.reps):
             op.apply(x, y)
         ctx.synchronize()
@@ -221,9 +225,40 @@ def _run_batch_w2(args):
           flush=True)
 
 
+def _run_solve_w2(args):
+    """The C96x30 W2 Helmholtz solves of the headline benchmark (set-up,
+    autotuning and warm-up first); the solves themselves run inside an NVTX
+    range "timed" so a profiler can keep to them (ncu --nvtx --nvtx-include timed/)."""
+    import torch
+    p = mg.w2_problem(args.n, args.nl, seed=args.seed)
+    ctx = lfx.Context(0)
+    s64 = device_w2(ctx, p, lfx.R64)
+    s32 = device_w2(ctx, p, lfx.R32, op64=s64.op64, cma=s64.cma, diag64=s64.diag)
+    s32.op.autotune(reps=10)
+    s64.op.autotune(reps=10)
+    solvers = {"mixed": refined_gmres(s32, gcrk=10, inner_rtol=1e-4, r_tol=1e-8),
+               "fp64": lfx.GMRES(s64.op, s64.prec, 10, 1e-8, 1e-16, 200)}
+    b = lfx.FieldVector.from_array(ctx, p.rhs)
+    x = lfx.FieldVector(ctx, [p.undf])
+    runs = [solvers[k] for k in args.kinds.split(",")]
+    for sol in runs:
+        for _ in range(2):
+            x.set_scalar(0.0)
+            sol.apply(x, b)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    for sol in runs:
+        for _ in range(args.solves):
+            x.set_scalar(0.0)
+            info = sol.apply(x, b)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print("solves done", info.as_dict(), flush=True)
+
+
 def main(argv=None):
     """One named workload, run once, for profilers:
-    ``python -m lfric_core_b200.workloads apply|time-apply|mrhs|batch-w2 [options]``."""
+    ``python -m lfric_core_b200.workloads apply|time-apply|mrhs|batch-w2|solve-w2 [options]``."""
     import argparse
     ap = argparse.ArgumentParser(prog="python -m lfric_core_b200.workloads")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -232,7 +267,8 @@ def main(argv=None):
     a.add_argument("--n", type=int, default=96)
     a.add_argument("--nl", type=int, default=30)
     a.add_argument("--precision", type=int, choices=[32, 64], default=32)
-    a.add_argument("--kernels", default="1,4", help="comma-separated apply kernels (0,1,3,4)")
+    a.add_argument("--kernels", default="1,4",
+                   help="comma-separated apply kernels (0,1,3,4, or tuned: the autotuner's choice)")
     a.add_argument("--reps", type=int, default=2)
     t = sub.add_parser("time-apply", help="time LMA apply configurations (FP32 and FP64)")
     t.add_argument("--space", choices=["w0", "w2"], default="w2")
@@ -252,9 +288,15 @@ def main(argv=None):
     b.add_argument("--n", type=int, default=94)
     b.add_argument("--nl", type=int, default=64)
     b.add_argument("--seed", type=int, default=505)
+    w = sub.add_parser("solve-w2", help="headline W2 solves (mixed and/or FP64) after set-up")
+    w.add_argument("--n", type=int, default=96)
+    w.add_argument("--nl", type=int, default=30)
+    w.add_argument("--seed", type=int, default=2)
+    w.add_argument("--kinds", default="mixed,fp64", help="comma-separated: mixed, fp64")
+    w.add_argument("--solves", type=int, default=1)
     args = ap.parse_args(argv)
     {"apply": _run_apply, "time-apply": _run_time_apply, "mrhs": _run_mrhs,
-     "batch-w2": _run_batch_w2}[args.cmd](args)
+     "batch-w2": _run_batch_w2, "solve-w2": _run_solve_w2}[args.cmd](args)
     return 0
 
 

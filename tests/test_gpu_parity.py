@@ -123,7 +123,8 @@ def test_lma_apply_w2_bitwise(ctx, n, nl):
 
 @pytest.mark.parametrize("kernel", [0, 1, 3, 4])
 @pytest.mark.parametrize("space,n,nl,prec", [("w0", 6, 5, 64), ("w2", 8, 7, 64), ("w2", 8, 7, 32),
-                                             ("w2", 12, 30, 64), ("w0", 5, 21, 32)])
+                                             ("w2", 12, 30, 64), ("w0", 5, 21, 32),
+                                             ("w2", 6, 40, 64), ("w2", 7, 33, 32)])
 def test_apply_kernels_agree(ctx, kernel, space, n, nl, prec):
     """Both LMA apply kernels (bulk-copy pipelined and register gather) give
     the oracle's FP64 result bit for bit, and the same FP32 result."""
@@ -153,6 +154,23 @@ def test_apply_kernels_agree(ctx, kernel, space, n, nl, prec):
         assert same(got, other)
 
 
+@pytest.mark.parametrize("prec", [64, 32])
+def test_prefetch_gather_variants(ctx, prec):
+    """Both register caps of the prefetching gather time and give the register
+    gather's bits on W2; W0 (columns of four cells) is refused."""
+    p = mg.w2_problem(9, 12, seed=12)
+    npc, cic = p.mesh.colour_lookup()
+    op = lfx.LmaOperator(ctx, p.ncell_2d, 12, 6, 6, p.map, p.map, p.undf, p.undf, p.lma, npc, cic,
+                         precision=prec)
+    for stages in (0, 1):
+        assert op.time_apply(3, stages, 0, reps=2) > 0
+    assert op.time_apply(3, 2, 0, reps=1) is None     # no such variant
+    q = mg.w0_problem(5, 4, seed=1)
+    nq, cq = q.mesh.colour_lookup()
+    op0 = lfx.LmaOperator(ctx, q.ncell_2d, 4, 8, 8, q.map, q.map, q.undf, q.undf, q.lma, nq, cq)
+    assert op0.time_apply(3, 0, 0, reps=1) is None
+
+
 def test_autotune_keeps_results(ctx):
     p = mg.w2_problem(12, 10, seed=6)
     npc, cic = p.mesh.colour_lookup()
@@ -161,13 +179,14 @@ def test_autotune_keeps_results(ctx):
     X, Y = lfx.FieldVector.from_array(ctx, x), lfx.FieldVector(ctx, [p.undf])
     choice = op.autotune(reps=3)
     assert choice["us"] > 0 and choice["kernel"] in ("pipeline", "register-gather",
-                                                     "register-gather-lookahead",
+                                                     "register-gather-prefetch",
                                                      "staged-pipeline")
     op.apply(X, Y)
     assert same(Y.export_field(), o_lma(p).apply(x))
 
 
-def test_divergence_and_transpose_bitwise(ctx):
+@pytest.mark.parametrize("kernel", [1, 3])
+def test_divergence_and_transpose_bitwise(ctx, kernel):
     q = mg.w2_problem(6, 4, seed=3, keep_parts=True)
     npc, cic = q.mesh.colour_lookup()
     m3, u3 = q.extra["map_w3"], q.extra["undf_w3"]
@@ -179,7 +198,11 @@ def test_divergence_and_transpose_bitwise(ctx):
     w = mg.normal(6, u3)
     U = lfx.FieldVector.from_array(ctx, u)
     W = lfx.FieldVector(ctx, [u3])
-    D.apply(U, W)  # dg_matrix_vector: W2 -> W3
+    ctx.set_apply_kernel(kernel)
+    try:
+        D.apply(U, W)  # dg_matrix_vector: W2 -> W3
+    finally:
+        ctx.set_apply_kernel(-1)
     assert same(W.export_field(), oD.apply(u))
     W.import_field(w)
     U2 = lfx.FieldVector(ctx, [q.undf])

@@ -353,7 +353,8 @@ struct lfx_prec {
   int64_t rdiag_n = 0;
   size_t bytes = 0;
   int64_t max_row = -1;  // PREC_CMA: largest 0-based dof the columns touch
-  bool jacobi_zeroed = false;  // PREC_CMA: rdiag zeroed on the column rows (batched use)
+  bool jacobi_zeroed = false;  // PREC_CMA: rdiag zeroed on the column rows
+  bool zero_sentinel = false;  // ... and non-zero on every other row
 };
 
 namespace lfx {

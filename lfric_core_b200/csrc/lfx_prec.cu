@@ -231,6 +231,226 @@ __global__ void __launch_bounds__(128) cma_prec_apply(
   }
 }
 
+// The same Thomas sweeps with each block's kStageCols columns staged through
+// shared memory. The block's x rows are copied in by one warp per column
+// (a column's rows are contiguous dofs, so the copies coalesce) and, with SF,
+// its factor rows too ([row][column] in memory: one coalesced run of
+// kStageCols per row), all issued before the first sweep; each of the first
+// kStageCols threads then runs its column's recurrences on the staged copy
+// and the result is copied out the same way. Row i of column j sits at
+// [i * (kStageCols + 1) + j], conflict-free for the row-wise copies and the
+// column-wise sweeps. Same arithmetic as thomas_sweep, so the same bits.
+//
+// Rows the columns do not cover get y = x / diag: by a separate elementwise
+// launch where the diagonal carries zeros on the column rows (zero_sentinel;
+// its blocks then need no shared memory), else by runs of rows in the blocks
+// after the Thomas blocks.
+constexpr int kStageCols = 64;
+constexpr int kStageThreads = 128;
+
+template <class T, bool SF>
+__global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
+    int ncell, int nrow, const int* __restrict__ first, const int* __restrict__ ind,
+    const T* __restrict__ fa, const T* __restrict__ finv, const T* __restrict__ fc,
+    const T* __restrict__ x, T* __restrict__ y, int thomas_blocks, int nruns,
+    const int* __restrict__ run_start, const int* __restrict__ run_len, const T* __restrict__ diag,
+    const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  constexpr int LD = kStageCols + 1;
+  constexpr int NW = kStageThreads / 32;
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if ((int)blockIdx.x < thomas_blocks) {
+    T* xs = reinterpret_cast<T*>(stage_raw);
+    T* as = xs + (size_t)nrow * LD;
+    T* is = as + (size_t)nrow * LD;
+    T* cs = is + (size_t)nrow * LD;
+    __shared__ int fs[kStageCols];
+    const int c0 = blockIdx.x * kStageCols;
+    const int nc = min(kStageCols, ncell - c0);
+    if (threadIdx.x < nc) fs[threadIdx.x] = __ldg(first + c0 + threadIdx.x);
+    __syncthreads();
+    // lane l copies row r0 + l of the warp's columns warp, warp + NW, ...:
+    // the loads of all of them are issued before their shared-memory stores
+    constexpr int CPW = kStageCols / NW;
+    for (int r0 = 0; r0 < nrow; r0 += 32) {
+      const int i = r0 + lane;
+      const bool act = i < nrow;
+      const int il = act ? __ldg(ind + i) : 0;
+      T v[CPW];
+#pragma unroll
+      for (int k = 0; k < CPW; ++k) {
+        const int j = warp + NW * k;
+        v[k] = (act && j < nc) ? x[fs[j] + il] : T(0);
+      }
+#pragma unroll
+      for (int k = 0; k < CPW; ++k)
+        if (act) xs[i * LD + warp + NW * k] = v[k];
+    }
+    if (SF) {
+      // thread t copies column t % kStageCols of rows t / kStageCols + 2 m
+      const int j = threadIdx.x % kStageCols, i0 = threadIdx.x / kStageCols;
+      constexpr int RS = kStageThreads / kStageCols;
+      constexpr int U = 8;
+      for (int ib = i0; ib < nrow; ib += RS * U) {
+        T va[U], vi[U], vc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int i = ib + RS * u;
+          const bool ok = i < nrow && j < nc;
+          const size_t g = (size_t)i * ncell + c0 + j;
+          va[u] = ok ? __ldg(fa + g) : T(0);
+          vi[u] = ok ? __ldg(finv + g) : T(0);
+          vc[u] = ok ? __ldg(fc + g) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int i = ib + RS * u;
+          if (i < nrow) {
+            as[i * LD + j] = va[u];
+            is[i * LD + j] = vi[u];
+            cs[i * LD + j] = vc[u];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    const int j = threadIdx.x;
+    if (j < nc) {
+      const int c = c0 + j;
+      T* col = xs + j;
+      double d = 0.0;
+      if (SF) {
+        for (int i = 0; i < nrow; ++i) {
+          const double xv = (double)col[i * LD], iv = (double)is[i * LD + j];
+          d = (i == 0) ? iv * xv : iv * fma(-(double)as[i * LD + j], d, xv);
+          col[i * LD] = (T)d;
+        }
+        for (int i = nrow - 2; i >= 0; --i) {
+          d = fma(-(double)cs[i * LD + j], d, (double)col[i * LD]);
+          col[i * LD] = (T)d;
+        }
+      } else {
+        constexpr int R = 8;
+        for (int i0 = 0; i0 < nrow; i0 += R) {
+          double iv[R], av[R];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = i0 + r;
+            if (i < nrow) {
+              iv[r] = (double)__ldg(finv + (size_t)i * ncell + c);
+              av[r] = (double)__ldg(fa + (size_t)i * ncell + c);
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = i0 + r;
+            if (i < nrow) {
+              const double xv = (double)col[i * LD];
+              d = (i == 0) ? iv[r] * xv : iv[r] * fma(-av[r], d, xv);
+              col[i * LD] = (T)d;
+            }
+          }
+        }
+        for (int i0 = nrow - 2; i0 >= 0; i0 -= R) {
+          double cv[R];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = i0 - r;
+            if (i >= 0) cv[r] = (double)__ldg(fc + (size_t)i * ncell + c);
+          }
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = i0 - r;
+            if (i >= 0) {
+              d = fma(-cv[r], d, (double)col[i * LD]);
+              col[i * LD] = (T)d;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (int r0 = 0; r0 < nrow; r0 += 32) {
+      const int i = r0 + lane;
+      if (i < nrow) {
+        const int il = __ldg(ind + i);
+#pragma unroll
+        for (int k = 0; k < CPW; ++k) {
+          const int j = warp + NW * k;
+          if (j < nc) y[fs[j] + il] = xs[i * LD + j];
+        }
+      }
+    }
+  } else {
+    const int64_t w = ((int64_t)(blockIdx.x - thomas_blocks) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)(gridDim.x - thomas_blocks) * blockDim.x) >> 5;
+    for (int64_t r = w; r < nruns; r += nw) {
+      const int s0 = run_start[r], len = run_len[r];
+      for (int l = lane; l < len; l += 32) y[s0 + l] = x[s0 + l] / diag[s0 + l];
+    }
+  }
+}
+
+// y = x / diag on the rows whose diagonal is not zero (the diagonal carries
+// zeros on the column rows): eight rows per thread per pass, loads first
+template <class T>
+__global__ void __launch_bounds__(256) jacobi_sentinel(int64_t n, const T* __restrict__ x,
+                                                       T* __restrict__ y,
+                                                       const T* __restrict__ diag,
+                                                       const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  constexpr int U = 8;
+  for (int64_t b0 = (int64_t)blockIdx.x * U * 256; b0 < n; b0 += (int64_t)gridDim.x * U * 256) {
+    T dv[U], xv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = b0 + u * 256 + threadIdx.x;
+      dv[u] = i < n ? __ldg(diag + i) : T(0);
+      xv[u] = i < n ? x[i] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = b0 + u * 256 + threadIdx.x;
+      if (dv[u] != T(0)) y[i] = xv[u] / dv[u];
+    }
+  }
+}
+
+// shared memory of the staged sweeps (0: the column does not fit)
+constexpr size_t kStageSmemMax = 200 * 1024;
+size_t staged_smem(int nrow, size_t esz, bool sf) {
+  const size_t b = (size_t)nrow * (kStageCols + 1) * esz * (sf ? 4 : 1);
+  return b <= kStageSmemMax ? b : 0;
+}
+// factors are staged while the block's shared memory stays at most this
+constexpr size_t kStageFactorsMax = 100 * 1024;
+
+template <class T, bool SF>
+void launch_staged(lfx_ctx* ctx, const lfx_prec* p, const T* x, T* y, size_t smem,
+                   const int* skip) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(cma_prec_staged<T, SF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kStageSmemMax);
+    attr = true;
+  }
+  const int tb = (p->ncell_2d + kStageCols - 1) / kStageCols;
+  int jb = 0;
+  if (p->rdiag && p->zero_sentinel) {
+    const int g = (int)std::max<int64_t>(
+        1, std::min<int64_t>((p->rdiag_n + 8 * 256 - 1) / (8 * 256), (int64_t)ctx->num_sms * 8));
+    jacobi_sentinel<T><<<g, 256, 0, ctx->stream>>>(p->rdiag_n, x, y, (const T*)p->rdiag, skip);
+    ctx->launches++;
+  } else if (p->nruns) {
+    jb = (int)std::min<int64_t>(((int64_t)p->nruns + 3) / 4, (int64_t)ctx->num_sms * 8);
+  }
+  cma_prec_staged<T, SF><<<tb + jb, kStageThreads, smem, ctx->stream>>>(
+      p->ncell_2d, p->nrow, p->first_dof, p->indirection, (const T*)p->fa, (const T*)p->finv,
+      (const T*)p->fc, x, y, tb, p->nruns, p->run_start, p->run_len, (const T*)p->rdiag,
+      skip);
+}
+
 template <class T>
 int k_divide(lfx_ctx* ctx, T* y, const T* x, const T* d, int64_t n, const int* skip) {
   return launch_chunks<0>(
@@ -261,6 +481,27 @@ int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int6
                  : k_divide(ctx, (float*)y, (const float*)x, (const float*)p->rdiag, n, skip);
     case PREC_CMA: {
       ctx->launches++;
+      {
+        const size_t esz = r64 ? 8 : 4;
+        size_t smem = staged_smem(p->nrow, esz, true);
+        const bool sf = smem && smem <= kStageFactorsMax;
+        if (!sf) smem = staged_smem(p->nrow, esz, false);
+        if (smem) {
+          if (r64) {
+            if (sf)
+              launch_staged<double, true>(ctx, p, (const double*)x, (double*)y, smem, skip);
+            else
+              launch_staged<double, false>(ctx, p, (const double*)x, (double*)y, smem, skip);
+          } else {
+            if (sf)
+              launch_staged<float, true>(ctx, p, (const float*)x, (float*)y, smem, skip);
+            else
+              launch_staged<float, false>(ctx, p, (const float*)x, (float*)y, smem, skip);
+          }
+          LFX_CK(ctx, cudaGetLastError());
+          return LFX_OK;
+        }
+      }
       const int tb = (p->ncell_2d + 127) / 128;
       int rb = (int)std::min<int64_t>(((int64_t)p->nruns + 3) / 4, (int64_t)ctx->num_sms * 8);
       if (p->nruns == 0) rb = 0;
@@ -282,6 +523,30 @@ int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int6
 }
 
 }  // namespace lfx
+
+template <class T>
+static int zero_rows_t(lfx_ctx* ctx, lfx_prec* p, const std::vector<char>& cov) {
+  const int64_t n = p->rdiag_n;
+  std::vector<T> d((size_t)n);
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  LFX_CK(ctx, cudaMemcpy(d.data(), p->rdiag, n * sizeof(T), cudaMemcpyDeviceToHost));
+  bool ok = true;
+  for (int64_t i = 0; i < n; ++i) {
+    if (cov[i])
+      d[i] = T(0);
+    else if (d[i] == T(0))
+      ok = false;
+  }
+  LFX_CK(ctx, cudaMemcpy(p->rdiag, d.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+  p->jacobi_zeroed = true;
+  p->zero_sentinel = ok;
+  return LFX_OK;
+}
+
+static int zero_column_rows(lfx_ctx* ctx, lfx_prec* p, const std::vector<char>& cov) {
+  return p->precision == LFX_R64 ? zero_rows_t<double>(ctx, p, cov)
+                                 : zero_rows_t<float>(ctx, p, cov);
+}
 
 static int copy_diag(lfx_ctx* ctx, const lfx_vec* diag, int32_t precision, void** out) {
   const int64_t n = diag->undf[0];
@@ -838,6 +1103,9 @@ int lfx_cma_prec_create(lfx_ctx* ctx, const lfx_cma* m, const lfx_vec* diag, int
     }
     p->rdiag_n = n;
     if (!rc) rc = copy_diag(ctx, diag, precision, &p->rdiag);
+    // zeros on the column rows mark them for the elementwise Jacobi pass,
+    // unless an uncovered row has a zero diagonal of its own
+    if (!rc) rc = zero_column_rows(ctx, p, cov);
   }
   if (rc) {
     lfx_prec_destroy(p);

@@ -18,6 +18,8 @@
 #include <cstring>
 #include <functional>
 
+#include <type_traits>
+
 #include "lfx_internal.cuh"
 
 namespace lfx {
@@ -68,7 +70,7 @@ struct lfx_solver {
   std::vector<void*> work;  // owned device vectors of n elements
   DevState* d_state = nullptr;
   DevState* h_state = nullptr;  // pinned
-  double* d_gm = nullptr;       // gmres: H, negH, g, u, cs, sn
+  double* d_gm = nullptr;       // gmres: H, negH, g, u, cs, sn, basis scales
   bool inner_mode = false;      // GMRES used as the inner solve of a refinement
   std::vector<GraphEntry> graphs;
   std::vector<lfx_vec*> hv;  // work vectors of the host-driven solvers
@@ -83,7 +85,7 @@ struct lfx_solver {
 namespace {
 
 size_t esz(int32_t p) { return p == LFX_R64 ? 8 : 4; }
-size_t gm_doubles(int K) { return 2 * (size_t)(K + 1) * K + (K + 1) + 3 * (size_t)K + 8; }
+size_t gm_doubles(int K) { return 2 * (size_t)(K + 1) * K + 2 * (size_t)(K + 1) + 3 * (size_t)K + 8; }
 
 int read_state(lfx_solver* s) {
   lfx_ctx* ctx = s->ctx;
@@ -227,10 +229,198 @@ int cgs_update(lfx_ctx* ctx, int64_t n, const VecPtrs& vp, T* w, const double* n
       fin, skip);
 }
 
+// FP32 classical Gram-Schmidt of the inner solve, streamed as float4 quads:
+// every thread walks its quads of the NR basis vectors and w in a grid-stride
+// loop (all loads of a quad issued together), adds each quad's products,
+// formed in FP32, into FP64 running sums, and the block reduces once at the
+// end. The last block to finish sums the block partials warp by warp in block
+// order, so the result is fixed for a given grid (the grid depends only on n
+// and the GPU's SM count). The n % 4 tail goes to block 0.
+constexpr int kCgsThreads = 256;
+
+__device__ __forceinline__ float quad_dot(const float4& a, const float4& b) {
+  float s = a.x * b.x;
+  s = fmaf(a.y, b.y, s);
+  s = fmaf(a.z, b.z, s);
+  return fmaf(a.w, b.w, s);
+}
+
+// block sums of acc[0..NR) into partials[r * grid + block]; returns true in
+// every thread of the last block, whose tot[0..NR) (valid in all its threads)
+// then holds the grand totals
+template <int NR>
+__device__ __forceinline__ bool cgs_reduce(double (&acc)[NR], double* partials, unsigned* ticket,
+                                           double (&tot)[NR]) {
+  __shared__ double sm[kCgsThreads / 32][NR];
+  __shared__ double st[NR];
+  __shared__ int am_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const double v = warp_butterfly(acc[r]);
+    if (lane == 0) sm[warp][r] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NR) {
+    double t = sm[0][threadIdx.x];
+#pragma unroll
+    for (int q = 1; q < kCgsThreads / 32; ++q) t = t + sm[q][threadIdx.x];
+    partials[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  for (int r = warp; r < NR; r += kCgsThreads / 32) {
+    double a = 0.0;
+    for (int i = lane; i < (int)gridDim.x; i += 32) a = a + __ldcg(&partials[(int64_t)r * gridDim.x + i]);
+    a = warp_butterfly(a);
+    if (lane == 0) st[r] = a;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NR; ++r) tot[r] = st[r];
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+// sig (nullable): the basis is stored unnormalised, v_j = sig[j] u_j, and the
+// true vector is sig[prev] w; then hcol receives the true inner products
+// <v_j, sig[prev] w> and nhcol the update coefficients -sig[j]^2 <u_j, w>
+template <int NR>
+__global__ void __launch_bounds__(kCgsThreads) cgs_dots_f4(int64_t n, VecPtrs vp,
+                                                           const float* __restrict__ w,
+                                                           double* hcol, double* nhcol,
+                                                           const double* sig, int prev,
+                                                           double* partials, unsigned* ticket,
+                                                           const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  double acc[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+  const int64_t n4 = n >> 2;
+  const float4* w4 = reinterpret_cast<const float4*>(w);
+  for (int64_t q = (int64_t)blockIdx.x * kCgsThreads + threadIdx.x; q < n4;
+       q += (int64_t)gridDim.x * kCgsThreads) {
+    float4 v[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) v[r] = __ldg(reinterpret_cast<const float4*>(vp.p[r]) + q);
+    const float4 wq = __ldg(w4 + q);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] += (double)quad_dot(v[r], wq);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+    const int64_t i = 4 * n4 + threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] += (double)(((const float*)vp.p[r])[i] * w[i]);
+  }
+  double tot[NR];
+  if (cgs_reduce<NR>(acc, partials, ticket, tot) && threadIdx.x == 0) {
+    for (int r = 0; r < NR; ++r) {
+      if (sig) {
+        hcol[r] = sig[r] * sig[prev] * tot[r];
+        nhcol[r] = -(sig[r] * sig[r]) * tot[r];
+      } else {
+        hcol[r] = tot[r];
+        nhcol[r] = -tot[r];
+      }
+    }
+  }
+}
+
+// out = w + sum_j nhcol[j] v_j (out may be w) and fin(||out||^2)
+template <int NR, class Fin>
+__global__ void __launch_bounds__(kCgsThreads) cgs_update_f4(int64_t n, VecPtrs vp,
+                                                             const float* w, float* out,
+                                                             const double* nhcol, Fin fin,
+                                                             double* partials, unsigned* ticket,
+                                                             const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  float c[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) c[r] = (float)nhcol[r];
+  double acc[1] = {0.0};
+  const int64_t n4 = n >> 2;
+  const float4* w4 = reinterpret_cast<const float4*>(w);
+  float4* o4 = reinterpret_cast<float4*>(out);
+  for (int64_t q = (int64_t)blockIdx.x * kCgsThreads + threadIdx.x; q < n4;
+       q += (int64_t)gridDim.x * kCgsThreads) {
+    float4 v[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) v[r] = __ldg(reinterpret_cast<const float4*>(vp.p[r]) + q);
+    float4 wq = w4[q];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      wq.x = fmaf(c[r], v[r].x, wq.x);
+      wq.y = fmaf(c[r], v[r].y, wq.y);
+      wq.z = fmaf(c[r], v[r].z, wq.z);
+      wq.w = fmaf(c[r], v[r].w, wq.w);
+    }
+    o4[q] = wq;
+    acc[0] += (double)quad_dot(wq, wq);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+    const int64_t i = 4 * n4 + threadIdx.x;
+    float wi = w[i];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) wi = fmaf(c[r], ((const float*)vp.p[r])[i], wi);
+    out[i] = wi;
+    acc[0] += (double)(wi * wi);
+  }
+  double tot[1];
+  if (cgs_reduce<1>(acc, partials, ticket, tot) && threadIdx.x == 0) fin(tot);
+}
+
+// blocks of a float4 Gram-Schmidt kernel resident on the GPU at once
+template <class K>
+int resident_blocks(const lfx_ctx* ctx, K kernel) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kCgsThreads, 0);
+  return ctx->num_sms * std::max(per_sm, 1);
+}
+
+bool quad_aligned(const VecPtrs& vp, int nr, const void* w) {
+  if ((uintptr_t)w & 15) return false;
+  for (int r = 0; r < nr; ++r)
+    if ((uintptr_t)vp.p[r] & 15) return false;
+  return true;
+}
+
+template <int NR, class Fin>
+int cgs_step_f4(lfx_ctx* ctx, int64_t n, const VecPtrs& vp, float* w, float* out, double* hcol,
+                double* nhcol, const double* sig, int prev, Fin fin, const int* skip) {
+  // one resident wave, and at most one block per 2048 values (the partials
+  // scratch holds nchunks(n) values per sum)
+  static int gd = 0, gu = 0;
+  if (!gd) gd = resident_blocks(ctx, cgs_dots_f4<NR>);
+  if (!gu) gu = resident_blocks(ctx, cgs_update_f4<NR, Fin>);
+  const int64_t cap = std::max<int64_t>(1, nchunks(n));
+  cgs_dots_f4<NR><<<(int)std::min<int64_t>(gd, cap), kCgsThreads, 0, ctx->stream>>>(
+      n, vp, w, hcol, nhcol, sig, prev, ctx->d_partials, ctx->d_ticket, skip);
+  cgs_update_f4<NR, Fin><<<(int)std::min<int64_t>(gu, cap), kCgsThreads, 0, ctx->stream>>>(
+      n, vp, w, out, nhcol, fin, ctx->d_partials, ctx->d_ticket, skip);
+  ctx->launches += 2;
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
 template <class T, class Fin>
 int cgs_step(lfx_ctx* ctx, int64_t n, int nr, const VecPtrs& vp, T* w, double* hcol,
              double* nhcol, Fin fin, const int* skip) {
   int rc = LFX_INVALID_ARGUMENT;
+  if constexpr (std::is_same<T, float>::value) {
+    if (quad_aligned(vp, nr, w)) {
+      switch (nr) {
+#define CGS_F4(N) \
+  case N: return cgs_step_f4<N>(ctx, n, vp, w, w, hcol, nhcol, nullptr, 0, fin, skip);
+        CGS_F4(1) CGS_F4(2) CGS_F4(3) CGS_F4(4) CGS_F4(5) CGS_F4(6)
+        CGS_F4(7) CGS_F4(8) CGS_F4(9) CGS_F4(10) CGS_F4(11) CGS_F4(12)
+#undef CGS_F4
+      }
+    }
+  }
   switch (nr) {
 #define CGS_CASE(N)                                                          \
   case N:                                                                    \
@@ -244,6 +434,23 @@ int cgs_step(lfx_ctx* ctx, int64_t n, int nr, const VecPtrs& vp, T* w, double* h
   return rc;
 }
 constexpr int kMaxCgs = 12;
+
+// Gram-Schmidt step of the inner solve over an unnormalised FP32 basis
+// (v_j = sig[j] u_j; the true vector is sig[nr - 1] w): out = w - sum_j
+// sig[j]^2 <u_j, w> u_j, the next basis vector unnormalised, whose scale
+// sig[nr] = sig[nr - 1] / ||sig[nr - 1] out|| the norm's fin sets.
+template <class Fin>
+int cgs_step_lazy(lfx_ctx* ctx, int64_t n, int nr, const VecPtrs& vp, float* w, float* out,
+                  double* hcol, double* nhcol, const double* sig, Fin fin, const int* skip) {
+  switch (nr) {
+#define CGS_LZ(N) \
+  case N: return cgs_step_f4<N>(ctx, n, vp, w, out, hcol, nhcol, sig, N - 1, fin, skip);
+    CGS_LZ(1) CGS_LZ(2) CGS_LZ(3) CGS_LZ(4) CGS_LZ(5) CGS_LZ(6)
+    CGS_LZ(7) CGS_LZ(8) CGS_LZ(9) CGS_LZ(10) CGS_LZ(11) CGS_LZ(12)
+#undef CGS_LZ
+  }
+  return LFX_INVALID_ARGUMENT;
+}
 
 template <class T>
 int norm_kernel(lfx_ctx* ctx, int64_t n, const T* v, double* out, const int* skip) {
@@ -513,7 +720,8 @@ int bicgstab_run(lfx_solver* s, T* x, const T* b) {
 // Givens rotations and back substitution (:930-953) by one thread. In inner
 // mode the rotations were already applied column by column as the Arnoldi
 // process ran, and only the back substitution over the m vectors is left.
-__global__ void gmres_finish_cycle(DevState* S, double* gm, int K) {
+// sig (nullable): scales of an unnormalised basis, folded into u
+__global__ void gmres_finish_cycle(DevState* S, double* gm, int K, const double* sig) {
   if (S->done) return;
   double* h = gm;                  // H(i,j) at (i-1) + (K+1)(j-1)
   double* g = gm + 2 * (K + 1) * K;
@@ -543,6 +751,8 @@ __global__ void gmres_finish_cycle(DevState* S, double* gm, int K) {
     for (int ivj = iv + 1; ivj <= m; ++ivj) a = fma(-H(iv, ivj), u[ivj - 1], a);
     u[iv - 1] = a / H(iv, iv);
   }
+  if (sig)
+    for (int iv = 0; iv < m; ++iv) u[iv] = u[iv] * sig[iv];
   S->m = m;
 #undef H
 }
@@ -564,8 +774,17 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
   double* u = g + (K + 1);
   double* cs = u + K;
   double* sn = cs + K;
+  double* sig = sn + K;
   const int* done = &S->done;
   const int* askip = &S->askip;
+  // the inner solve's FP32 basis is kept unnormalised (v_j = sig[j] u_j), so
+  // no pass rescales it: the preconditioner writes u_0 and each Gram-Schmidt
+  // update writes the next u_j directly
+  bool lazy = false;
+  if constexpr (std::is_same<T, float>::value) {
+    lazy = s->inner_mode && K <= kMaxCgs && ((uintptr_t)w & 15) == 0;
+    for (int k = 0; k < K; ++k) lazy = lazy && ((uintptr_t)V[k] & 15) == 0;
+  }
   int rc;
   // res = b - A x ; sc_err = ||res||
   if ((rc = op_apply_impl(s->op, x, res, b, nullptr))) return rc;
@@ -591,21 +810,23 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
   auto cycle = [&]() -> int {
     int q;
     // s = P res ; beta = ||s|| ; v1 = s / beta ; g = (beta, 0, ...)
-    if ((q = prec_apply_impl(s->prec, s->precision, res, sv, n, done))) return q;
+    T* s0 = lazy ? V[0] : sv;
+    if ((q = prec_apply_impl(s->prec, s->precision, res, s0, n, done))) return q;
     q = launch_chunks<1>(
-        ctx, n, [=] __device__(int64_t i) { return V1<T>{sv[i]}; },
+        ctx, n, [=] __device__(int64_t i) { return V1<T>{s0[i]}; },
         [=] __device__(int64_t, const V1<T>& v, double* a) { a[0] = fma((double)v.a, (double)v.a, a[0]); },
         [=] __device__(const double* t) {
           S->gbeta = sqrt(t[0]);
           if (S->iter == 0) S->gbeta0 = S->gbeta;
           S->inv_beta = 1.0 / S->gbeta;
+          sig[0] = S->inv_beta;
           S->m = K;
           for (int k = 0; k <= K; ++k) g[k] = 0.0;
           g[0] = S->gbeta;
         },
         done);
     if (q) return q;
-    {
+    if (!lazy) {
       T* v0 = V[0];
       q = launch_chunks<0>(
           ctx, n, [=] __device__(int64_t i) { return V1<T>{sv[i]}; },
@@ -620,10 +841,12 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
       const int ivc = iv;
       // last step of the orthogonalisation: H(iv+1, iv) = ||w||, and in inner
       // mode the column's Givens rotation and the in-cycle convergence test
+      const bool lz = lazy;
       auto fin_norm = [=] __device__(const double* t) {
-        const double hn = sqrt(t[0]);
+        const double hn = lz ? sig[ivc - 1] * sqrt(t[0]) : sqrt(t[0]);
         col[ivc] = hn;  // H(iv+1, iv)
         S->inv_hn = 1.0 / hn;
+        sig[ivc] = lz ? sig[ivc - 1] * S->inv_hn : S->inv_hn;
         S->applies += 1;
         if (S->inner_mode) {
           for (int j = 1; j < ivc; ++j) {
@@ -648,7 +871,14 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
           }
         }
       };
-      if (s->inner_mode && K <= kMaxCgs) {
+      if (lazy) {
+        VecPtrs vpi{};
+        for (int k = 0; k < iv; ++k) vpi.p[k] = V[k];
+        float* out = (float*)(iv < K ? V[iv] : w);
+        q = cgs_step_lazy(ctx, n, iv, vpi, (float*)w, out, col, &nh[(K + 1) * (iv - 1)], sig,
+                          fin_norm, askip);
+        if (q) return q;
+      } else if (s->inner_mode && K <= kMaxCgs) {
         // inner solve: classical Gram-Schmidt, two passes per step
         VecPtrs vpi{};
         for (int k = 0; k < iv; ++k) vpi.p[k] = V[k];
@@ -706,7 +936,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
         if (q) return q;
       }
       }
-      if (iv < K) {
+      if (iv < K && !lazy) {
         T* vn = V[iv];
         q = launch_chunks<0>(
             ctx, n, [=] __device__(int64_t i) { return V1<T>{w[i]}; },
@@ -715,7 +945,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
         if (q) return q;
       }
     }
-    gmres_finish_cycle<<<1, 1, 0, ctx->stream>>>(S, h, K);
+    gmres_finish_cycle<<<1, 1, 0, ctx->stream>>>(S, h, K, lazy ? sig : nullptr);
     ctx->launches++;
     LFX_CK(ctx, cudaGetLastError());
     // x += sum_iv u(iv) v_iv over the m vectors of the cycle, one pass, the

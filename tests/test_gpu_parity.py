@@ -222,8 +222,12 @@ def test_lma_fp32_apply(ctx):
 
 
 # ------------------------------------------------------------------ CMA
-def test_cma_assembly_and_preconditioner_bitwise(ctx):
-    p = mg.w2_problem(12, 10, seed=5)
+@pytest.mark.parametrize("n,nl", [(12, 10), (5, 70)])
+def test_cma_assembly_and_preconditioner_bitwise(ctx, n, nl):
+    """Column assembly and Thomas sweeps equal the oracle bit for bit (5 x 70:
+    columns of 71 rows, a partial block of columns); the FP32 preconditioner
+    agrees to FP32 rounding."""
+    p = mg.w2_problem(n, nl, seed=5)
     sysd = wl.device_w2(ctx, p)
     op = o_lma(p)
     oprec, band = o_w2_prec(p, op)
@@ -231,7 +235,15 @@ def test_cma_assembly_and_preconditioner_bitwise(ctx):
     x = mg.normal(11, p.undf)
     X, Y = sysd.vector(x), sysd.vector()
     sysd.prec.apply(X, Y)
-    assert same(Y.export_field(), oprec.apply(x))
+    want = oprec.apply(x)
+    assert same(Y.export_field(), want)
+    s32 = wl.device_w2(ctx, p, lfx.R32, op64=sysd.op64, cma=sysd.cma, diag64=sysd.diag)
+    X32, Y32 = s32.vector(x), s32.vector()
+    s32.prec.apply(X32, Y32)
+    got32 = Y32.export_field()
+    assert np.linalg.norm(got32 - want) <= 1e-6 * np.linalg.norm(want)
+    if nl != 10:
+        return
     # y += A x on the column space (columnwise_op_app)
     prm = mg.w2v_cma_params(p.nlayers)
     y0 = mg.normal(12, p.undf)

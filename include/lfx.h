@@ -118,17 +118,24 @@ int lfx_op_destroy(lfx_op* op);
  * column descriptors (at two register caps, stages 0 and 1; columns reading
  * at most two blocks from at most two cells, e.g. W2 and W3), the bulk-copy
  * pipeline with 2..8 stages and 1..8 warps per block, and the copy-staged
- * pipeline with 2..6 stages and 2..8 warps, those that fit the shared memory
- * -- over `reps` launches and keeps the fastest for later applies. Outputs
+ * pipeline with 2..6 stages and 2..8 warps, those that fit the shared memory,
+ * and the cell scatter (square operators on one dofmap; one launch per
+ * colour, reading a symmetric operator's packed upper triangle) -- over
+ * `reps` launches and keeps the fastest for later applies. Outputs
  * (nullable) name the choice: kernel 0 pipeline / 1 register gather / 2
  * generic / 3 register gather with prefetched descriptors / 4 copy-staged
- * pipeline (matrix blocks and x values both staged in shared memory), and its
- * time per apply. */
+ * pipeline (matrix blocks and x values both staged in shared memory) / 5 cell
+ * scatter (residual applies y = b - A x then take a gather), and its time per
+ * apply. */
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
                     float* us);
 /* time one configuration (as above) without keeping it */
 int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps, int32_t reps,
                       float* us);
+/* keep one configuration (as above) for later applies, as the autotuner
+ * would; LFX_NOT_SUPPORTED if it does not fit the operator. Kernel 5 takes
+ * stages 0 (one cell per warp) or 2, 3 (cells staged ahead in shared memory). */
+int lfx_op_set_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps);
 /* diag(A) by mm_diagonal_kernel (sci_mm_diagonal_kernel_mod.F90:99-125) */
 int lfx_lma_diagonal(lfx_op* op, lfx_vec* diag);
 /* transpose apply y = A^T x for a matrix stored as (ncell_3d, ndf_to, ndf_from)
@@ -342,8 +349,8 @@ int64_t lfx_ctx_launch_count(const lfx_ctx* ctx);
  * autotuned choice, else the register gather (default); 0 = force the
  * bulk-copy pipeline; 1 = force the register gather; 3 = force the register
  * gather with prefetched descriptors (the register gather where the operator
- * does not fit it); 4 = force the copy-staged pipeline. All give
- * bit-identical results. */
+ * does not fit it); 4 = force the copy-staged pipeline; 5 = force the cell
+ * scatter where the operator fits it. All give bit-identical results. */
 int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which);
 /* LFX_TIMEOUT if a kernel's bounded device-side wait ran out since the last
  * check (the kernel then skipped its work); synchronises the stream */

@@ -201,7 +201,7 @@ int lfx_ctx_apply_timing(lfx_ctx* ctx, int32_t precision, int64_t* launches, dou
 int64_t lfx_ctx_launch_count(const lfx_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which) {
-  if (!ctx || which < -1 || which > 4 || which == 2) return LFX_INVALID_ARGUMENT;
+  if (!ctx || which < -1 || which > 5 || which == 2) return LFX_INVALID_ARGUMENT;
   ctx->lma_kernel = which;
   return LFX_OK;
 }

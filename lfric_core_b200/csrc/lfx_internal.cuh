@@ -302,6 +302,18 @@ struct lfx_lma_layout {
   int refcount = 1;
   std::vector<int32_t> rank;         // colour-loop position of every cell
   lfx_lma_layout* tlay = nullptr;    // from-space layout for the transpose apply
+  // cell-scatter plan (square operators on one dofmap whose dof columns each
+  // get the same records from every cell that touches them, at most two per
+  // cell at consecutive offsets): cells in colour-loop order with the start of
+  // each colour, and per cell {map row, flags, partners} padded to cs_ints
+  // ints. flags bit df: this cell is the first (in colour order) on the
+  // column of df; bit 8+df: df is the lower record of a pair; bit 16+df: the
+  // upper one. partners: 4 bits per df, the upper record of df's pair.
+  bool cs_ok = false;
+  int32_t cs_ints = 0;
+  std::vector<int32_t> colour_start;
+  int32_t* cs_cells = nullptr;
+  int32_t* cs_desc = nullptr;
 };
 
 struct lfx_op {
@@ -319,6 +331,12 @@ struct lfx_op {
   // kernel 1 register gather, kernel 2 generic gather
   int32_t tune_kernel = -1, tune_stages = 0, tune_warps = 0;
   float tune_us = 0.f;
+  // the upper triangle [cell][p][k] of bitwise symmetric local matrices
+  // (p = packed (df, df2), df <= df2), cell stride sblk elements; null when
+  // the operator is not square on one dofmap or not symmetric
+  void* smat = nullptr;
+  size_t smat_bytes = 0;
+  int32_t sblk = 0;
 };
 
 struct lfx_cma {

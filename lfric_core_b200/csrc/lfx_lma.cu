@@ -731,7 +731,7 @@ __global__ void lma_gather_t(LayoutArgs A, int max_off, int blk, const T* __rest
                              const T* __restrict__ x, const int32_t* __restrict__ map_to,
                              T* __restrict__ y) {
   // here A.ndf1 is the from-space ndf (output), A.ndf2 the to-space ndf
-  const int nl = A.nlayers, ndf_out = A.ndf1, ndf_in = A.ndf2;
+  const int nl = A.nlayers, ndf_in = A.ndf2;
   const int lane = threadIdx.x & 31;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const size_t cell_stride = (size_t)ndf_in * blk;  // stored as [c][j(to)][df(from)][k]
@@ -781,6 +781,228 @@ __global__ void relayout(const double* __restrict__ src, T* __restrict__ dst, in
   }
 }
 
+// ---------------------------------------------------------------- cell scatter
+// The reference's own loop shape, one colour at a time: a warp takes one cell
+// column (lane = level), loads the cell's local matrices and x values once,
+// and adds M(df, df2) x(df2) into every dof of the cell in the reference's
+// order (df2 outer, df inner), directly into y. The first cell on a dof
+// column (in colour order) starts from zero, later ones from the stored sum;
+// a column holding two records of the same cell at consecutive offsets (the
+// bottom and top faces or vertices of a cell column) is summed by the lane
+// of the output level, which takes the upper record's terms from the lane
+// below. Cells of one colour share no dof, so a launch per colour is
+// race-free, and every dof receives its terms in the coloured order of the
+// reference (the bits of the gather kernels). With a symmetric operator the
+// matrix is read from its packed upper triangle, so each entry crosses HBM
+// once.
+template <int NDF>
+__host__ __device__ constexpr int pidx(int i, int j) {
+  return i <= j ? i * NDF - i * (i - 1) / 2 + (j - i) : j * NDF - j * (j - 1) / 2 + (i - j);
+}
+
+struct CellArgs {
+  int nl, blk, cstride, dints;
+  const int* cells;
+  int ncells;
+  const int* desc;
+};
+
+template <class T, int NDF, bool SYM>
+__global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict__ M,
+                                                 const T* __restrict__ x, T* __restrict__ y,
+                                                 const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  const int lane = threadIdx.x & 31;
+  const int ci = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (ci >= C.ncells) return;  // whole warps
+  const int c = __ldg(C.cells + ci);
+  const int* dsc = C.desc + (size_t)c * C.dints;
+  int mf[NDF];
+#pragma unroll
+  for (int j = 0; j < NDF; ++j) mf[j] = __ldg(dsc + j);
+  const uint32_t flags = (uint32_t)__ldg(dsc + NDF), part = (uint32_t)__ldg(dsc + NDF + 1);
+  const int nl = C.nl;
+  const bool v = lane < nl;
+  const T* Mc = M + (size_t)c * C.cstride + (v ? lane : 0);
+  constexpr int NP = SYM ? NDF * (NDF + 1) / 2 : NDF * NDF;
+  T m[NP], xv[NDF], yo[NDF];
+#pragma unroll
+  for (int p = 0; p < NP; ++p)
+    m[p] = v ? __ldg(Mc + (SYM ? p * nl : (p / NDF) * C.blk + (p % NDF) * nl)) : T(0);
+#pragma unroll
+  for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldg(x + mf[j] + lane) : T(0);
+#pragma unroll
+  for (int df = 0; df < NDF; ++df) {
+    const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+    const bool opens = (flags >> df) & 1u;
+    const bool live = lower ? lane <= nl : v;
+    yo[df] = (!upper && !opens && live) ? y[mf[df] + lane] : T(0);
+  }
+#define MV(i, j) m[SYM ? pidx<NDF>(i, j) : (i) * NDF + (j)]
+#pragma unroll
+  for (int df = 0; df < NDF; ++df) {
+    if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
+    if ((flags >> (8 + df)) & 1u) {
+      const int bsel = (part >> (4 * df)) & 15u;
+#pragma unroll
+      for (int bb = df + 1; bb < NDF; ++bb) {
+        if (bb != bsel) continue;
+        T acc = yo[df];
+#pragma unroll
+        for (int j = 0; j < NDF; ++j) {
+          const T mb = __shfl_up_sync(0xffffffffu, MV(bb, j), 1);
+          const T xb = __shfl_up_sync(0xffffffffu, xv[j], 1);
+          if (v) acc = fmaT(MV(df, j), xv[j], acc);
+          if (lane >= 1 && lane <= nl) acc = fmaT(mb, xb, acc);
+        }
+        if (lane <= nl) y[mf[df] + lane] = acc;
+      }
+    } else {
+      T acc = yo[df];
+#pragma unroll
+      for (int j = 0; j < NDF; ++j) acc = fmaT(MV(df, j), xv[j], acc);
+      if (v) y[mf[df] + lane] = acc;
+    }
+  }
+#undef MV
+}
+
+// The cell scatter with each warp's next cells staged ahead: a warp walks
+// the colour's cells with stride (warps in the grid) and keeps the local
+// matrices and descriptors of its next S cells in flight (16-byte cp.async
+// into a per-warp ring in shared memory), so HBM sees every warp's upcoming
+// matrix blocks at once; lanes then read their level's entries from shared
+// memory. Same arithmetic as lma_cells.
+constexpr int kCellWarps = 4;
+
+template <class T, int NDF, bool SYM, int S>
+__global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, const T* __restrict__ M,
+                                                                 const T* __restrict__ x,
+                                                                 T* __restrict__ y, int stage_bytes,
+                                                                 const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  extern __shared__ __align__(16) unsigned char cell_ring[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned char* ring = cell_ring + (size_t)wib * S * stage_bytes;
+  const int mat_bytes = C.cstride * (int)sizeof(T);
+  const int nq = mat_bytes / 16, dq = C.dints / 4;
+  auto issue = [&](int64_t i, int s) {
+    if (i < C.ncells) {
+      const int c = __ldg(C.cells + i);
+      const char* src = reinterpret_cast<const char*>(M + (size_t)c * C.cstride);
+      unsigned char* dst = ring + (size_t)s * stage_bytes;
+      for (int q = lane; q < nq; q += 32) cp_async16(dst + 16 * q, src + 16 * q);
+      const char* ds = reinterpret_cast<const char*>(C.desc + (size_t)c * C.dints);
+      if (lane < dq) cp_async16(dst + mat_bytes + 16 * lane, ds + 16 * lane);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < S; ++s) issue(gw + s * nw, s);
+  const int nl = C.nl;
+  const bool v = lane < nl;
+  int s = 0;
+  for (int64_t i = gw; i < C.ncells; i += nw) {
+    cp_async_wait<S - 1>();
+    __syncwarp();
+    const unsigned char* st = ring + (size_t)s * stage_bytes;
+    const T* sm = reinterpret_cast<const T*>(st) + (v ? lane : 0);
+    const int* dsc = reinterpret_cast<const int*>(st + mat_bytes);
+    int mf[NDF];
+#pragma unroll
+    for (int j = 0; j < NDF; ++j) mf[j] = dsc[j];
+    const uint32_t flags = (uint32_t)dsc[NDF], part = (uint32_t)dsc[NDF + 1];
+    constexpr int NP = SYM ? NDF * (NDF + 1) / 2 : NDF * NDF;
+    T m[NP], xv[NDF], yo[NDF];
+#pragma unroll
+    for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldg(x + mf[j] + lane) : T(0);
+#pragma unroll
+    for (int df = 0; df < NDF; ++df) {
+      const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+      const bool opens = (flags >> df) & 1u;
+      const bool live = lower ? lane <= nl : v;
+      yo[df] = (!upper && !opens && live) ? y[mf[df] + lane] : T(0);
+    }
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+      m[p] = v ? sm[SYM ? p * nl : (p / NDF) * C.blk + (p % NDF) * nl] : T(0);
+    __syncwarp();
+    // the stage is free again: fetch the cell S ahead
+    issue(i + (int64_t)S * nw, s);
+    s = s + 1 == S ? 0 : s + 1;
+#define MV(i, j) m[SYM ? pidx<NDF>(i, j) : (i) * NDF + (j)]
+#pragma unroll
+    for (int df = 0; df < NDF; ++df) {
+      if ((flags >> (16 + df)) & 1u) continue;
+      if ((flags >> (8 + df)) & 1u) {
+        const int bsel = (part >> (4 * df)) & 15u;
+#pragma unroll
+        for (int bb = df + 1; bb < NDF; ++bb) {
+          if (bb != bsel) continue;
+          T acc = yo[df];
+#pragma unroll
+          for (int j = 0; j < NDF; ++j) {
+            const T mb = __shfl_up_sync(0xffffffffu, MV(bb, j), 1);
+            const T xb = __shfl_up_sync(0xffffffffu, xv[j], 1);
+            if (v) acc = fmaT(MV(df, j), xv[j], acc);
+            if (lane >= 1 && lane <= nl) acc = fmaT(mb, xb, acc);
+          }
+          if (lane <= nl) y[mf[df] + lane] = acc;
+        }
+      } else {
+        T acc = yo[df];
+#pragma unroll
+        for (int j = 0; j < NDF; ++j) acc = fmaT(MV(df, j), xv[j], acc);
+        if (v) y[mf[df] + lane] = acc;
+      }
+    }
+#undef MV
+  }
+  cp_async_wait<0>();
+}
+
+// packed upper triangle [c][p][k] (cell stride sblk) from the Fortran
+// (nc3, ndf, ndf) FP64 stencil
+template <class T>
+__global__ void relayout_sym(const double* __restrict__ src, T* __restrict__ dst, int64_t ncell,
+                             int nl, int ndf, int sblk) {
+  const int np = ndf * (ndf + 1) / 2;
+  const int64_t total = ncell * sblk;
+  const int64_t nc3 = ncell * nl;
+  for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < total;
+       d += (int64_t)gridDim.x * blockDim.x) {
+    const int in = (int)(d % sblk);
+    const int64_t c = d / sblk;
+    if (in >= np * nl) {
+      dst[d] = T(0);
+      continue;
+    }
+    int p = in / nl, i = 0;
+    const int k = in % nl;
+    while (p >= ndf - i) {
+      p -= ndf - i;
+      ++i;
+    }
+    const int j = i + p;
+    dst[d] = (T)src[(c * nl + k) + nc3 * (i + (int64_t)ndf * j)];
+  }
+}
+
+// *bad = 1 unless every local matrix equals its transpose bit for bit
+__global__ void sym_check(const double* __restrict__ src, int64_t nc3, int ndf, int* bad) {
+  const int64_t total = nc3 * ndf * ndf;
+  for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < total;
+       d += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = d % nc3;
+    const int ij = (int)(d / nc3), i = ij % ndf, j = ij / ndf;
+    if (i < j && __double_as_longlong(src[r + nc3 * (i + (int64_t)ndf * j)]) !=
+                     __double_as_longlong(src[r + nc3 * (j + (int64_t)ndf * i)]))
+      *bad = 1;
+  }
+}
+
 struct HostRec {
   int32_t start, cell, df;
 };
@@ -791,7 +1013,7 @@ struct HostRec {
 // the fast kernels are built too.
 int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int32_t ndf,
                  const int32_t* map, int64_t undf, const std::vector<int32_t>& rank,
-                 const int32_t* mf0, int32_t ndf_from) {
+                 const int32_t* mf0, int32_t ndf_from, const std::vector<int32_t>* colour) {
   std::vector<HostRec> recs;
   recs.reserve((size_t)ncell * ndf);
   for (int32_t c = 0; c < ncell; ++c)
@@ -805,6 +1027,9 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
                    [](const HostRec& a, const HostRec& b) { return a.start < b.start; });
   std::vector<int32_t> ent_base, ent_h, ent_grp, grp_cell;
   std::vector<uint32_t> grp_rec;
+  // cell-scatter plan: only for square operators on one dofmap (colour given)
+  bool cs = colour != nullptr && ndf <= 8 && nl + 1 <= 32;
+  std::vector<uint32_t> cs_flags(cs ? (size_t)ncell : 0, 0u), cs_part(cs ? (size_t)ncell : 0, 0u);
   size_t i = 0;
   int64_t covered = 0;
   int max_off = 0, max_h = 0, max_groups = 0, max_blocks = 0;
@@ -847,6 +1072,29 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
       }
       pk |= (uint32_t)n;
       L->max_nrec = std::max(L->max_nrec, n);
+      if (cs) {
+        // every cell on the column must carry the first cell's record pattern
+        // (one record, or two at consecutive offsets), in distinct colours
+        const uint32_t pat = pk & ~((63u << 2) | (63u << 11) | (63u << 20));
+        const uint32_t pat0 = grp_cell.size() > (size_t)ent_grp.back()
+                                  ? grp_rec[ent_grp.back()] & ~((63u << 2) | (63u << 11) | (63u << 20))
+                                  : pat;
+        if (n > 2 || pat != pat0 || (n == 2 && rec_off(pk, 1) != rec_off(pk, 0) + 1)) cs = false;
+        for (int32_t g = ent_grp.back(); cs && g < (int32_t)grp_cell.size(); ++g)
+          if ((*colour)[grp_cell[g]] == (*colour)[er[q].cell]) cs = false;
+        if (cs) {
+          const int32_t c = er[q].cell;
+          const bool first = (int32_t)grp_cell.size() == ent_grp.back();
+          const int a = rec_df(pk, 0);
+          if (first) cs_flags[c] |= 1u << a;
+          if (n == 2) {
+            const int bb = rec_df(pk, 1);
+            if (first) cs_flags[c] |= 1u << bb;
+            cs_flags[c] |= (1u << (8 + a)) | (1u << (16 + bb));
+            cs_part[c] |= (uint32_t)bb << (4 * a);
+          }
+        }
+      }
       grp_cell.push_back(er[q].cell);
       grp_rec.push_back(pk);
       ++ng;
@@ -877,6 +1125,27 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
   up((void**)&L->ent_grp, ent_grp.data(), ent_grp.size() * 4);
   up((void**)&L->grp_cell, grp_cell.data(), grp_cell.size() * 4);
   up((void**)&L->grp_rec, grp_rec.data(), grp_rec.size() * 4);
+  if (cs && mf0) {
+    // cells in colour-loop order, the start of each colour, per cell descriptors
+    std::vector<int32_t> order(ncell);
+    for (int32_t c = 0; c < ncell; ++c) order[rank[c]] = c;
+    int32_t ncol = 0;
+    for (int32_t c = 0; c < ncell; ++c) ncol = std::max(ncol, (*colour)[c] + 1);
+    L->colour_start.assign(ncol + 1, 0);
+    for (int32_t c = 0; c < ncell; ++c) L->colour_start[(*colour)[c] + 1]++;
+    for (int32_t k = 0; k < ncol; ++k) L->colour_start[k + 1] += L->colour_start[k];
+    L->cs_ints = (ndf + 2 + 3) / 4 * 4;
+    std::vector<int32_t> d((size_t)ncell * L->cs_ints, 0);
+    for (int32_t c = 0; c < ncell; ++c) {
+      int32_t* row = &d[(size_t)c * L->cs_ints];
+      for (int j = 0; j < ndf; ++j) row[j] = mf0[(size_t)c * ndf + j];
+      row[ndf] = (int32_t)cs_flags[c];
+      row[ndf + 1] = (int32_t)cs_part[c];
+    }
+    up((void**)&L->cs_cells, order.data(), order.size() * 4);
+    up((void**)&L->cs_desc, d.data(), d.size() * 4);
+    L->cs_ok = rc == 0;
+  }
   if (mf0) {
     std::vector<int4> ep(L->nent);
     for (int32_t e = 0; e < L->nent; ++e) ep[e] = make_int4(ent_base[e], ent_h[e], ent_grp[e], ent_grp[e + 1]);
@@ -950,6 +1219,8 @@ void free_layout(lfx_ctx* ctx, lfx_lma_layout* L) {
   dfree(ctx, L->grp_pack, (size_t)L->ngrp * L->gp_stride * 4);
   dfree(ctx, L->desc, (size_t)L->nent * 32 * L->desc_ipl * 4);
   dfree(ctx, L->fdesc, (size_t)L->nent * L->fd_ints * 4);
+  dfree(ctx, L->cs_cells, (size_t)L->ncell_2d * 4);
+  dfree(ctx, L->cs_desc, (size_t)L->ncell_2d * L->cs_ints * 4);
   dfree(ctx, L->map_from, (size_t)L->ncell_2d * L->ndf_from * 4);
   dfree(ctx, L->map_to, (size_t)L->ncell_2d * L->ndf_to * 4);
   free_layout(ctx, L->tlay);
@@ -981,9 +1252,41 @@ int upload_matrix(lfx_ctx* ctx, lfx_op* op, const double* stencil) {
     relayout<float><<<grid, 256, 0, ctx->stream>>>(raw, (float*)op->mat, L->ncell_2d, L->nlayers,
                                                     L->ndf_to, L->ndf_from, op->blk);
   LFX_CK(ctx, cudaGetLastError());
+  if (L->cs_ok) {
+    // bitwise symmetric local matrices: keep the packed upper triangle too
+    int* bad = nullptr;
+    int hbad = 1;
+    rc = dmalloc(ctx, (void**)&bad, 4);
+    if (!rc) {
+      cudaMemsetAsync(bad, 0, 4, ctx->stream);
+      sym_check<<<grid, 256, 0, ctx->stream>>>(raw, (int64_t)L->ncell_2d * L->nlayers, L->ndf_to, bad);
+      LFX_CK(ctx, cudaGetLastError());
+      LFX_CK(ctx, cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
+      LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+      dfree(ctx, bad, 4);
+    }
+    if (!rc && !hbad) {
+      const int np = L->ndf_to * (L->ndf_to + 1) / 2;
+      const size_t b = (size_t)np * L->nlayers * esz;
+      op->sblk = (int)(((b + 15) / 16 * 16) / esz);
+      op->smat_bytes = (size_t)L->ncell_2d * op->sblk * esz;
+      rc = dmalloc(ctx, &op->smat, op->smat_bytes);
+      if (!rc) {
+        if (op->precision == LFX_R64)
+          relayout_sym<double><<<grid, 256, 0, ctx->stream>>>(raw, (double*)op->smat, L->ncell_2d,
+                                                               L->nlayers, L->ndf_to, op->sblk);
+        else
+          relayout_sym<float><<<grid, 256, 0, ctx->stream>>>(raw, (float*)op->smat, L->ncell_2d,
+                                                              L->nlayers, L->ndf_to, op->sblk);
+        LFX_CK(ctx, cudaGetLastError());
+      } else {
+        op->smat_bytes = 0;
+      }
+    }
+  }
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
   dfree(ctx, raw, (size_t)total_in * 8);
-  return LFX_OK;
+  return rc;
 }
 
 int gather_grid(const lfx_ctx* ctx, int32_t nent) {
@@ -1165,13 +1468,100 @@ void launch_fetch(lfx_ctx* ctx, const lfx_op* op, const LayoutArgs& A, int varia
     launch_fetch_t<T, N, 3>(ctx, op, A, x, y, b, skip);
 }
 
+// cell scatter (kernel 5): one dofmap, the plan built, ndf 1, 6 or 8
+bool cells_ok(const lfx_op* op) {
+  const lfx_lma_layout* L = op->lay;
+  return L->cs_ok && (L->ndf_to == 1 || L->ndf_to == 6 || L->ndf_to == 8);
+}
+
+// shared memory of one stage of lma_cells_pipe: a cell's matrix block and
+// its descriptor
+size_t cells_stage_bytes(const lfx_op* op) {
+  const size_t esz = op->precision == LFX_R64 ? 8 : 4;
+  const size_t m = op->smat ? (size_t)op->sblk * esz : (size_t)op->lay->ndf_to * op->blk * esz;
+  return m + (size_t)op->lay->cs_ints * 4;
+}
+constexpr size_t kCellSmemMax = 200 * 1024;
+
+// stages: 0 one cell per warp (lma_cells), 2 or 3 the staged pipeline
+template <class T, int N, bool SYM, int S>
+void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const int* skip) {
+  const lfx_lma_layout* L = op->lay;
+  CellArgs C{L->nlayers, op->blk, SYM ? op->sblk : N * op->blk, L->cs_ints, nullptr, 0, L->cs_desc};
+  const T* M = (const T*)(SYM ? op->smat : op->mat);
+  const int sb = (int)cells_stage_bytes(op);
+  const size_t smem = (size_t)kCellWarps * S * sb;
+  int per_sm = 1;
+  if constexpr (S > 0) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(lma_cells_pipe<T, N, SYM, S>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellSmemMax);
+      attr = true;
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_cells_pipe<T, N, SYM, S>,
+                                                  32 * kCellWarps, smem);
+    if (per_sm < 1) per_sm = 1;
+  }
+  // one launch per colour, in the reference's colour order
+  for (size_t k = 0; k + 1 < L->colour_start.size(); ++k) {
+    C.cells = L->cs_cells + L->colour_start[k];
+    C.ncells = L->colour_start[k + 1] - L->colour_start[k];
+    if (C.ncells <= 0) continue;
+    if constexpr (S > 0) {
+      const int grid = (int)std::min<int64_t>(((int64_t)C.ncells + kCellWarps - 1) / kCellWarps,
+                                              (int64_t)ctx->num_sms * per_sm);
+      lma_cells_pipe<T, N, SYM, S><<<grid, 32 * kCellWarps, smem, ctx->stream>>>(
+          C, M, (const T*)x, (T*)y, sb, skip);
+    } else {
+      const int grid = (int)(((int64_t)C.ncells * 32 + 255) / 256);
+      lma_cells<T, N, SYM><<<grid, 256, 0, ctx->stream>>>(C, M, (const T*)x, (T*)y, skip);
+    }
+    ctx->launches++;
+  }
+  ctx->launches--;  // counted once by the caller
+}
+
+template <class T, int N, int S>
+void launch_cells_s(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const int* skip) {
+  if (op->smat)
+    launch_cells_t<T, N, true, S>(ctx, op, x, y, skip);
+  else
+    launch_cells_t<T, N, false, S>(ctx, op, x, y, skip);
+}
+
+template <class T, int N>
+void launch_cells(lfx_ctx* ctx, const lfx_op* op, int stages, const void* x, void* y,
+                  const int* skip) {
+  switch (stages) {
+    case 2: launch_cells_s<T, N, 2>(ctx, op, x, y, skip); return;
+    case 3: launch_cells_s<T, N, 3>(ctx, op, x, y, skip); return;
+    default: launch_cells_s<T, N, 0>(ctx, op, x, y, skip); return;
+  }
+}
+
+// a staged cell scatter with `stages` stages fits the shared memory
+bool cells_stages_ok(const lfx_op* op, int stages) {
+  if (stages == 0) return true;
+  if (stages != 2 && stages != 3) return false;
+  return (size_t)kCellWarps * stages * cells_stage_bytes(op) <= kCellSmemMax;
+}
+
 // kernel: 0 bulk-copy pipelined (shape ts), 1 register gather, 2 generic,
-// 3 register gather with prefetched descriptors, 4 copy-staged pipeline (shape ts)
+// 3 register gather with prefetched descriptors, 4 copy-staged pipeline (shape ts),
+// 5 cell scatter (y = A x only)
 template <class T>
 void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& ts,
                     const void* x, void* y, const void* b, const int* skip) {
   const lfx_lma_layout* L = op->lay;
   const LayoutArgs A = args_of(L, op->blk);
+  if (kernel == 5) {
+    switch (L->ndf_to) {
+      case 1: launch_cells<T, 1>(ctx, op, ts.stages, x, y, skip); return;
+      case 6: launch_cells<T, 6>(ctx, op, ts.stages, x, y, skip); return;
+      default: launch_cells<T, 8>(ctx, op, ts.stages, x, y, skip); return;
+    }
+  }
   if (kernel == 4) {
     launch_pipe<T>(ctx, op, A, ts, x, y, b, skip);
     return;
@@ -1228,6 +1618,10 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     *kernel = 3;
     return;
   }
+  if (ctx->lma_kernel == 5 && cells_ok(op)) {
+    *kernel = 5;
+    return;
+  }
   if ((ctx->lma_kernel == 1 || ctx->lma_kernel == 3) && gather2_ok(op)) {
     *kernel = 1;
     return;
@@ -1241,7 +1635,7 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     *kernel = op->tune_kernel;
     if (*kernel == 0) *ts = tma_shape(op, op->tune_stages, op->tune_warps);
     if (*kernel == 4) *ts = pipe_shape(op, op->tune_stages, op->tune_warps);
-    if (*kernel == 3) ts->stages = op->tune_stages;
+    if (*kernel == 3 || *kernel == 5) ts->stages = op->tune_stages;
     if ((*kernel != 0 && *kernel != 4) || ts->warps) return;
   }
   *kernel = gather2_ok(op) ? 1 : 2;
@@ -1266,6 +1660,11 @@ int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* 
   int kernel = 2;
   TmaShape ts;
   pick_apply(ctx, op, &kernel, &ts);
+  if (kernel == 5 && b) {
+    // the cell scatter computes y = A x only; residuals take a gather
+    ts = TmaShape{};
+    kernel = fetch_ok(op) ? 3 : (gather2_ok(op) ? 1 : 2);
+  }
   timing_begin(ctx, op->precision);
   ctx->launches++;
   launch_apply(ctx, op, kernel, ts, x, y, b, skip);
@@ -1296,7 +1695,7 @@ int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_
     return fail(ctx, LFX_INVALID_ARGUMENT, "precision must be 64 or 32");
   // colour rank of every cell: the position of its kernel call in the
   // reference's colour loop
-  std::vector<int32_t> rank(ncell_2d, -1);
+  std::vector<int32_t> rank(ncell_2d, -1), colour(ncell_2d, -1);
   int32_t pos = 0;
   for (int32_t col = 0; col < ncolours; ++col) {
     if (ncells_per_colour[col] < 0 || ncells_per_colour[col] > max_cells_per_colour)
@@ -1306,6 +1705,7 @@ int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_
       if (cell < 1 || cell > ncell_2d || rank[cell - 1] >= 0)
         return fail(ctx, LFX_INVALID_ARGUMENT, "colouring does not list every cell exactly once");
       rank[cell - 1] = pos++;
+      colour[cell - 1] = col;
     }
   }
   if (pos != ncell_2d)
@@ -1325,8 +1725,11 @@ int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_
   L->ndf_from = ndf_from;
   L->undf_to = undf_to;
   L->undf_from = undf_from;
+  // one dofmap on both sides: the cell-scatter plan can be built
+  const bool one_map = ndf_to == ndf_from && undf_to == undf_from &&
+                       std::equal(map_to, map_to + (size_t)ncell_2d * ndf_to, map_from);
   int rc = build_layout(ctx, L, ncell_2d, nlayers, ndf_to, map_to, undf_to, rank, mf.data(),
-                        ndf_from);
+                        ndf_from, one_map ? &colour : nullptr);
   if (!rc) rc = dmalloc(ctx, (void**)&L->map_from, mf.size() * 4);
   if (!rc) rc = dmalloc(ctx, (void**)&L->map_to, mt.size() * 4);
   if (!rc) cudaMemcpy(L->map_from, mf.data(), mf.size() * 4, cudaMemcpyHostToDevice);
@@ -1371,6 +1774,7 @@ int lfx_op_destroy(lfx_op* op) {
   if (!op) return LFX_OK;
   lfx_ctx* ctx = op->ctx;
   dfree(ctx, op->mat, op->mat_bytes);
+  dfree(ctx, op->smat, op->smat_bytes);
   if (op->lay && --op->lay->refcount == 0) free_layout(ctx, op->lay);
   delete op;
   return LFX_OK;
@@ -1390,7 +1794,7 @@ int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y) {
 // Times `reps` applies of one launch configuration on scratch vectors.
 int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps, int32_t reps,
                       float* us) {
-  if (!op || !us || reps < 1 || kernel < 0 || kernel > 4) return LFX_INVALID_ARGUMENT;
+  if (!op || !us || reps < 1 || kernel < 0 || kernel > 5) return LFX_INVALID_ARGUMENT;
   lfx_ctx* ctx = op->ctx;
   const lfx_lma_layout* L = op->lay;
   TmaShape ts;
@@ -1403,6 +1807,11 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
   if (kernel == 3) {
     if (!fetch_ok(op) || stages < 0 || stages > 1)
       return fail(ctx, LFX_NOT_SUPPORTED, "prefetching gather does not fit this operator");
+    ts.stages = stages;
+  }
+  if (kernel == 5) {
+    if (!cells_ok(op) || !cells_stages_ok(op, stages))
+      return fail(ctx, LFX_NOT_SUPPORTED, "cell scatter does not fit this operator");
     ts.stages = stages;
   }
   const size_t esz = op->precision == LFX_R64 ? 8 : 4;
@@ -1432,8 +1841,31 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
   return rc;
 }
 
+// Keeps one launch configuration for later applies of this operator (as the
+// autotuner would), after checking that it fits.
+int lfx_op_set_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps) {
+  if (!op) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = op->ctx;
+  bool ok = false;
+  switch (kernel) {
+    case 0: ok = tma_shape(op, stages, warps).warps > 0; break;
+    case 1: ok = gather2_ok(op); break;
+    case 2: ok = true; break;
+    case 3: ok = fetch_ok(op) && (stages == 0 || stages == 1); break;
+    case 4: ok = pipe_shape(op, stages, warps).warps > 0; break;
+    case 5: ok = cells_ok(op) && cells_stages_ok(op, stages); break;
+    default: return fail(ctx, LFX_INVALID_ARGUMENT, "no such apply kernel");
+  }
+  if (!ok) return fail(ctx, LFX_NOT_SUPPORTED, "configuration does not fit this operator");
+  op->tune_kernel = kernel;
+  op->tune_stages = stages;
+  op->tune_warps = warps;
+  return LFX_OK;
+}
+
 // Picks the fastest apply configuration for this operator by timing the
-// candidates (register gather, the prefetching gather at two register caps, bulk-copy
+// candidates (register gather, the prefetching gather at two register caps, the
+// cell scatter, bulk-copy
 // pipeline with 2..8 stages and 1..8 warps per block that fit the shared
 // memory) and keeps it for later applies.
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
@@ -1459,6 +1891,8 @@ int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, 
     rc = consider(1, 0, 0);
     if (!rc && fetch_ok(op)) rc = consider(3, 0, 0);
     if (!rc && fetch_ok(op)) rc = consider(3, 1, 0);
+    for (int st : {0, 2, 3})
+      if (!rc && cells_ok(op) && cells_stages_ok(op, st)) rc = consider(5, st, 0);
   } else {
     rc = consider(2, 0, 0);
   }
@@ -1525,7 +1959,7 @@ int lfx_op_apply_transpose(lfx_op* op, const lfx_vec* x, lfx_vec* y) {
     T->undf_to = L->undf_from;
     T->undf_from = L->undf_to;
     int rc = build_layout(ctx, T, L->ncell_2d, L->nlayers, L->ndf_from, mf.data(), L->undf_from,
-                          L->rank, nullptr, 0);
+                          L->rank, nullptr, 0, nullptr);
     if (rc) {
       free_layout(ctx, T);
       return rc;

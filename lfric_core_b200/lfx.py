@@ -104,6 +104,7 @@ _SIGS = [
     ("lfx_op_apply", [vp, vp, vp], C.c_int),
     ("lfx_op_autotune", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                          C.POINTER(C.c_int32), C.POINTER(C.c_float)], C.c_int),
+    ("lfx_op_set_apply", [vp, C.c_int32, C.c_int32, C.c_int32], C.c_int),
     ("lfx_op_time_apply", [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                            C.POINTER(C.c_float)], C.c_int),
     ("lfx_op_apply_transpose", [vp, vp, vp], C.c_int),
@@ -246,7 +247,8 @@ class Context:
     def set_apply_kernel(self, which: int):
         """-1: per-operator choice (autotuned, else register gather), 0: bulk-copy
         pipelined LMA apply, 1: register gather, 3: register gather with
-        prefetched column descriptors, 4: copy-staged pipeline."""
+        prefetched column descriptors, 4: copy-staged pipeline, 5: cell scatter
+        (one launch per colour)."""
         self.check(self.L.lfx_ctx_set_apply_kernel(self.h, which))
 
     def check_device_error(self):
@@ -399,8 +401,14 @@ class LmaOperator(_Handle):
         self.ctx.check(self.ctx.L.lfx_op_autotune(self.h, reps, C.byref(k), C.byref(s),
                                                    C.byref(w), C.byref(us)))
         name = {0: "pipeline", 1: "register-gather", 2: "generic",
-                3: "register-gather-prefetch", 4: "staged-pipeline"}[k.value]
+                3: "register-gather-prefetch", 4: "staged-pipeline",
+                5: "cell-scatter"}[k.value]
         return {"kernel": name, "stages": s.value, "warps": w.value, "us": round(us.value, 2)}
+
+    def set_apply(self, kernel: int, stages: int = 0, warps: int = 0):
+        """Keep one apply launch configuration for this operator (as the
+        autotuner would); raises if it does not fit."""
+        self.ctx.check(self.ctx.L.lfx_op_set_apply(self.h, kernel, stages, warps))
 
     def time_apply(self, kernel: int, stages: int = 0, warps: int = 0, reps: int = 10):
         us = C.c_float()

@@ -121,7 +121,7 @@ def test_lma_apply_w2_bitwise(ctx, n, nl):
     assert same(sysd.diag.export_field(), op.diagonal())
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 3, 4])
+@pytest.mark.parametrize("kernel", [0, 1, 3, 4, 5])
 @pytest.mark.parametrize("space,n,nl,prec", [("w0", 6, 5, 64), ("w2", 8, 7, 64), ("w2", 8, 7, 32),
                                              ("w2", 12, 30, 64), ("w0", 5, 21, 32),
                                              ("w2", 6, 40, 64), ("w2", 7, 33, 32)])
@@ -152,6 +152,77 @@ def test_apply_kernels_agree(ctx, kernel, space, n, nl, prec):
         finally:
             ctx.set_apply_kernel(-1)
         assert same(got, other)
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("space", ["w2", "w0"])
+def test_cell_scatter_nonsymmetric(ctx, prec, space):
+    """The cell scatter on local matrices that are not symmetric (full
+    storage) gives the oracle's FP64 bits and the register gather's FP32 bits;
+    forced inside a GMRES solve (whose residuals take a gather) the FP64 solve
+    still matches the oracle bit for bit."""
+    p = mg.w2_problem(7, 9, seed=21) if space == "w2" else mg.w0_problem(7, 9, seed=21)
+    rng = np.random.default_rng(4)
+    lma = p.lma * (1.0 + 0.01 * rng.standard_normal(p.lma.shape))
+    npc, cic = p.mesh.colour_lookup()
+    op = lfx.LmaOperator(ctx, p.ncell_2d, 9, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf, lma,
+                         npc, cic, precision=prec)
+    assert op.time_apply(5, 0, 0, reps=1) is not None
+    x = mg.normal(8, p.undf)
+    X = lfx.FieldVector.from_array(ctx, x, prec)
+    Y = lfx.FieldVector(ctx, [p.undf], prec)
+    got = {}
+    for k, st in ((5, 0), (5, 2), (5, 3), (1, 0)):
+        op.set_apply(k, st)
+        op.apply(X, Y)
+        got[(k, st)] = Y.export_field()
+    for st in (0, 2, 3):
+        assert same(got[(5, st)], got[(1, 0)])
+    if prec == 64:
+        oop = orc.LmaOperator(p.ncell_2d, 9, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf, lma,
+                              npc, cic)
+        assert same(got[(5, 0)], oop.apply(x))
+
+
+@pytest.mark.parametrize("space,n,nl", [("w2", 9, 30), ("w0", 6, 20), ("w2", 5, 31)])
+@pytest.mark.parametrize("prec", [64, 32])
+def test_cell_scatter_stages_symmetric(ctx, space, n, nl, prec):
+    """Symmetric operators (packed upper triangle) in every cell-scatter
+    configuration: FP64 equals the oracle, FP32 the register gather, bit for
+    bit; 31 levels fill the warp (the top dof of a column on lane 31)."""
+    p = mg.w2_problem(n, nl, seed=5) if space == "w2" else mg.w0_problem(n, nl, seed=5)
+    npc, cic = p.mesh.colour_lookup()
+    op = lfx.LmaOperator(ctx, p.ncell_2d, nl, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf, p.lma,
+                         npc, cic, precision=prec)
+    x = mg.normal(9, p.undf)
+    X = lfx.FieldVector.from_array(ctx, x, prec)
+    Y = lfx.FieldVector(ctx, [p.undf], prec)
+    op.set_apply(1)
+    op.apply(X, Y)
+    ref = o_lma(p).apply(x) if prec == 64 else Y.export_field()
+    for st in (0, 2, 3):
+        op.set_apply(5, st)
+        Y.set_scalar(7.0)
+        op.apply(X, Y)
+        assert same(Y.export_field(), ref)
+
+
+def test_cell_scatter_in_gmres(ctx):
+    p = mg.w2_problem(16, 12, seed=2)
+    sysd = wl.device_w2(ctx, p)
+    op = o_lma(p)
+    oprec, _ = o_w2_prec(p, op)
+    x_o, info_o = orc.solve("gmres", op, oprec, p.rhs, r_tol=1e-8, a_tol=1e-16, max_iter=200,
+                            gcrk=10)
+    ctx.set_apply_kernel(5)
+    try:
+        g = lfx.GMRES(sysd.op, sysd.prec, 10, 1e-8, 1e-16, 200)
+        X, B = sysd.vector(), sysd.vector(p.rhs)
+        info = g.apply(X, B)
+    finally:
+        ctx.set_apply_kernel(-1)
+    assert info.converged and info.iterations == info_o.iterations
+    assert same(X.export_field(), x_o)
 
 
 @pytest.mark.parametrize("prec", [64, 32])

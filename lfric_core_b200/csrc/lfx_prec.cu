@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
     const T* __restrict__ fa, const T* __restrict__ finv, const T* __restrict__ fc,
     const T* __restrict__ x, T* __restrict__ y, int thomas_blocks, int nruns,
     const int* __restrict__ run_start, const int* __restrict__ run_len, const T* __restrict__ diag,
-    const int* skip) {
+    int64_t sentinel_n, const int* skip) {
   if (skip && *((volatile const int*)skip)) return;
   constexpr int LD = kStageCols + 1;
   constexpr int NW = kStageThreads / 32;
@@ -382,6 +382,25 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
         }
       }
     }
+  } else if (sentinel_n > 0) {
+    // the other rows, elementwise: eight per thread per pass, loads first
+    constexpr int U = 8;
+    const int64_t nb = gridDim.x - thomas_blocks;
+    for (int64_t b0 = (int64_t)(blockIdx.x - thomas_blocks) * U * kStageThreads; b0 < sentinel_n;
+         b0 += nb * U * kStageThreads) {
+      T dv[U], xv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t i = b0 + u * kStageThreads + threadIdx.x;
+        dv[u] = i < sentinel_n ? __ldg(diag + i) : T(0);
+        xv[u] = i < sentinel_n ? x[i] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t i = b0 + u * kStageThreads + threadIdx.x;
+        if (dv[u] != T(0)) y[i] = xv[u] / dv[u];
+      }
+    }
   } else {
     const int64_t w = ((int64_t)(blockIdx.x - thomas_blocks) * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)(gridDim.x - thomas_blocks) * blockDim.x) >> 5;
@@ -425,6 +444,9 @@ size_t staged_smem(int nrow, size_t esz, bool sf) {
 }
 // factors are staged while the block's shared memory stays at most this
 constexpr size_t kStageFactorsMax = 100 * 1024;
+// the elementwise Jacobi rows join the Thomas launch up to this much shared
+// memory per block
+constexpr size_t kFuseSmemMax = 40 * 1024;
 
 template <class T, bool SF>
 void launch_staged(lfx_ctx* ctx, const lfx_prec* p, const T* x, T* y, size_t smem,
@@ -437,18 +459,28 @@ void launch_staged(lfx_ctx* ctx, const lfx_prec* p, const T* x, T* y, size_t sme
   }
   const int tb = (p->ncell_2d + kStageCols - 1) / kStageCols;
   int jb = 0;
+  int64_t sentinel_n = 0;
   if (p->rdiag && p->zero_sentinel) {
-    const int g = (int)std::max<int64_t>(
-        1, std::min<int64_t>((p->rdiag_n + 8 * 256 - 1) / (8 * 256), (int64_t)ctx->num_sms * 8));
-    jacobi_sentinel<T><<<g, 256, 0, ctx->stream>>>(p->rdiag_n, x, y, (const T*)p->rdiag, skip);
-    ctx->launches++;
+    if (smem <= kFuseSmemMax) {
+      // small stages: the elementwise rows share the launch (their blocks
+      // still fit several per SM beside the Thomas blocks)
+      sentinel_n = p->rdiag_n;
+      jb = (int)std::max<int64_t>(
+          1, std::min<int64_t>((p->rdiag_n + 8 * kStageThreads - 1) / (8 * kStageThreads),
+                               (int64_t)ctx->num_sms * 16));
+    } else {
+      const int g = (int)std::max<int64_t>(
+          1, std::min<int64_t>((p->rdiag_n + 8 * 256 - 1) / (8 * 256), (int64_t)ctx->num_sms * 8));
+      jacobi_sentinel<T><<<g, 256, 0, ctx->stream>>>(p->rdiag_n, x, y, (const T*)p->rdiag, skip);
+      ctx->launches++;
+    }
   } else if (p->nruns) {
     jb = (int)std::min<int64_t>(((int64_t)p->nruns + 3) / 4, (int64_t)ctx->num_sms * 8);
   }
   cma_prec_staged<T, SF><<<tb + jb, kStageThreads, smem, ctx->stream>>>(
       p->ncell_2d, p->nrow, p->first_dof, p->indirection, (const T*)p->fa, (const T*)p->finv,
       (const T*)p->fc, x, y, tb, p->nruns, p->run_start, p->run_len, (const T*)p->rdiag,
-      skip);
+      sentinel_n, skip);
 }
 
 template <class T>

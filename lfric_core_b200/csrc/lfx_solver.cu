@@ -570,9 +570,11 @@ int cg_run(lfx_solver* s, T* x, const T* b) {
     }
     return LFX_OK;
   };
-  if ((rc = read_state(s))) return rc;
-  while (!s->h_state->done)
+  // no host round trip before the first graph: its kernels idle if the
+  // initial residual already ended the solve (device flags)
+  do {
     if ((rc = run_graph(s, x, b, batch))) return rc;
+  } while (!s->h_state->done);
   return LFX_OK;
 }
 
@@ -710,9 +712,11 @@ int bicgstab_run(lfx_solver* s, T* x, const T* b) {
     }
     return LFX_OK;
   };
-  if ((rc = read_state(s))) return rc;
-  while (!s->h_state->done)
+  // no host round trip before the first graph: its kernels idle if the
+  // initial residual already ended the solve (device flags)
+  do {
     if ((rc = run_graph(s, x, b, batch))) return rc;
+  } while (!s->h_state->done);
   return LFX_OK;
 }
 
@@ -720,6 +724,43 @@ int bicgstab_run(lfx_solver* s, T* x, const T* b) {
 // Givens rotations and back substitution (:930-953) by one thread. In inner
 // mode the rotations were already applied column by column as the Arnoldi
 // process ran, and only the back substitution over the m vectors is left.
+// x += sum_k u[k] v_k over the cycle's m basis vectors, 16 bytes per thread
+// per pass (the reference's order per element, so the same bits as the
+// scalar form); all pointers 16-byte aligned; the n % W tail in block 0
+template <class T>
+__global__ void __launch_bounds__(256) gmres_xupdate(int64_t n, VecPtrs vp, const double* u,
+                                                     const int* mptr, T* x, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  using Q = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+  constexpr int W = 16 / sizeof(T);
+  const int m = *mptr;
+  const int64_t nq = n / W;
+  Q* xq = reinterpret_cast<Q*>(x);
+  for (int64_t q = (int64_t)blockIdx.x * 256 + threadIdx.x; q < nq; q += (int64_t)gridDim.x * 256) {
+    T xv[W];
+    const Q a = xq[q];
+    memcpy(xv, &a, 16);
+#pragma unroll 4
+    for (int k = 0; k < m; ++k) {
+      const Q b = __ldg(reinterpret_cast<const Q*>(vp.p[k]) + q);
+      T vv[W];
+      memcpy(vv, &b, 16);
+      const T uk = (T)u[k];
+#pragma unroll
+      for (int e = 0; e < W; ++e) xv[e] = fmaT(uk, vv[e], xv[e]);
+    }
+    Q o;
+    memcpy(&o, xv, 16);
+    xq[q] = o;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - nq * W) {
+    const int64_t i = nq * W + threadIdx.x;
+    T xi = x[i];
+    for (int k = 0; k < m; ++k) xi = fmaT((T)u[k], ((const T*)vp.p[k])[i], xi);
+    x[i] = xi;
+  }
+}
+
 // sig (nullable): scales of an unnormalised basis, folded into u
 __global__ void gmres_finish_cycle(DevState* S, double* gm, int K, const double* sig) {
   if (S->done) return;
@@ -950,6 +991,15 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
     LFX_CK(ctx, cudaGetLastError());
     // x += sum_iv u(iv) v_iv over the m vectors of the cycle, one pass, the
     // reference's order per element
+    bool al = ((uintptr_t)x & 15) == 0;
+    for (int k = 0; k < K; ++k) al = al && ((uintptr_t)V[k] & 15) == 0;
+    if (al) {
+      const int grid = (int)std::max<int64_t>(
+          1, std::min<int64_t>((n + 256 * 4 - 1) / (256 * 4), (int64_t)ctx->num_sms * 8));
+      gmres_xupdate<T><<<grid, 256, 0, ctx->stream>>>(n, vp, u, &S->m, x, done);
+      ctx->launches++;
+      LFX_CK(ctx, cudaGetLastError());
+    } else {
     q = launch_chunks<0>(
         ctx, n, [=] __device__(int64_t i) { return V1<T>{x[i]}; },
         [=] __device__(int64_t i, const V1<T>& v, double*) {
@@ -960,6 +1010,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
         },
         NoFin{}, done);
     if (q) return q;
+    }
     if ((q = op_apply_impl(s->op, x, res, b, done))) return q;  // res = b - A x
     q = launch_chunks<1>(
         ctx, n, [=] __device__(int64_t i) { return V1<T>{res[i]}; },
@@ -985,9 +1036,11 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
         done);
     return q;
   };
-  if ((rc = read_state(s))) return rc;
-  while (!s->h_state->done)
+  // no host round trip before the first graph: its kernels idle if the
+  // initial residual already ended the solve (device flags)
+  do {
     if ((rc = run_graph(s, x, b, cycle))) return rc;
+  } while (!s->h_state->done);
   return LFX_OK;
 }
 

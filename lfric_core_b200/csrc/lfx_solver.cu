@@ -72,6 +72,7 @@ struct lfx_solver {
   DevState* h_state = nullptr;  // pinned
   double* d_gm = nullptr;       // gmres: H, negH, g, u, cs, sn, basis scales
   bool inner_mode = false;      // GMRES used as the inner solve of a refinement
+  bool zero_x0 = false;         // the next apply starts from x = 0 (set by the refinement)
   std::vector<GraphEntry> graphs;
   std::vector<lfx_vec*> hv;  // work vectors of the host-driven solvers
   double rho_relax = 1.0, lmin = 0.0, lmax = 0.0;  // Jacobi / Chebyshev
@@ -827,13 +828,20 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
     for (int k = 0; k < K; ++k) lazy = lazy && ((uintptr_t)V[k] & 15) == 0;
   }
   int rc;
-  // res = b - A x ; sc_err = ||res||
-  if ((rc = op_apply_impl(s->op, x, res, b, nullptr))) return rc;
+  // res = b - A x ; sc_err = ||res||. When the refinement's inner solve
+  // starts from x = 0, res = b exactly and the apply is skipped.
+  const bool zero_x0 = s->zero_x0;
+  s->zero_x0 = false;
+  if (!zero_x0 && (rc = op_apply_impl(s->op, x, res, b, nullptr))) return rc;
+  const T* r0src = zero_x0 ? b : res;
   rc = launch_chunks<1>(
-      ctx, n, [=] __device__(int64_t i) { return V1<T>{res[i]}; },
-      [=] __device__(int64_t, const V1<T>& q, double* a) { a[0] = fma((double)q.a, (double)q.a, a[0]); },
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{r0src[i]}; },
+      [=] __device__(int64_t i, const V1<T>& q, double* a) {
+        if (zero_x0) res[i] = q.a;
+        a[0] = fma((double)q.a, (double)q.a, a[0]);
+      },
       [=] __device__(const double* t) {
-        S->applies = 1;
+        S->applies = zero_x0 ? 0 : 1;
         S->r_nrm_0 = sqrt(t[0]);
         S->sc_err = S->r_nrm_0;
         if (S->sc_err < EPS_RDEF) {  // :866
@@ -1163,6 +1171,7 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
         NoFin{});
     if (rc) return rc;
     lfx_solve_info ii{};
+    s->inner->zero_x0 = s->inner->kind == LFX_SOLVER_GMRES;  // d32 was just zeroed
     rc = lfx_solver_apply(s->inner, s->d32, s->r32, &ii);
     if (rc && rc != LFX_NOT_CONVERGED) return rc;
     info->inner_iterations += ii.iterations;

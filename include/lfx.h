@@ -346,7 +346,8 @@ int lfx_ctx_apply_timing(lfx_ctx* ctx, int32_t precision, int64_t* launches, dou
 /* number of kernels this context has launched so far */
 int64_t lfx_ctx_launch_count(const lfx_ctx* ctx);
 /* LMA apply kernel for every operator of the context: -1 = each operator's
- * autotuned choice, else the register gather (default); 0 = force the
+ * autotuned choice, else the register gather with prefetched descriptors
+ * where it fits, else the register gather (default); 0 = force the
  * bulk-copy pipeline; 1 = force the register gather; 3 = force the register
  * gather with prefetched descriptors (the register gather where the operator
  * does not fit it); 4 = force the copy-staged pipeline; 5 = force the cell

@@ -47,11 +47,12 @@ struct BSlot {
   const float *fa, *finv, *fc;
   const int32_t *first, *ind;
   int32_t ncol, nrow;
-  // vectors
+  // vectors: x (FP64) moves only at true residuals; between them the FP32
+  // xc accumulates the steps, x += xc then (a reliable update)
   const double* b;
   double* x;
   double* r64;
-  float *r, *p, *z;
+  float *r, *p, *z, *xc;
 };
 
 struct BState {
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
       const int64_t i = base + (int64_t)m * RT;
       if (i < D.n) v[m] = ld(D, i);
     }
-    double acc[NR];
+    double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = 0.0;
 #pragma unroll
@@ -109,6 +110,7 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
       const int64_t i = base + (int64_t)m * RT;
       if (i < D.n) op(D, S, i, v[m], acc);
     }
+    if constexpr (NR > 0) {
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       const double t = block_sum(acc[r], sm);
@@ -120,7 +122,7 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
     __syncthreads();
     if (am_last) {
       __threadfence();
-      double tot[NR];
+      double tot[NR > 0 ? NR : 1];
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
         double a = 0.0;
@@ -133,6 +135,7 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
         tickets[w.x] = 0u;
       }
       __syncthreads();
+    }
     }
   }
 }
@@ -148,8 +151,12 @@ __global__ void __launch_bounds__(256) bapply(const int2* list, const int* len, 
   const int lane = threadIdx.x & 31;
   const int L = *len;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < L; u += nwarp) {
-    const int2 w = list[u];
+  int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int2 wn = u < L ? list[u] : make_int2(-1, -1);
+  for (; u < L; u += nwarp) {
+    // the next item's list entry is loaded while this one is computed
+    const int2 w = wn;
+    wn = u + nwarp < L ? list[u + nwarp] : make_int2(-1, -1);
     if (w.x < 0) continue;
     if (RESID ? !ph_resid(st[w.x]) : !ph_run(st[w.x])) continue;
     // local copy: the stores below cannot alias it, so the pointers stay in
@@ -246,16 +253,272 @@ __global__ void __launch_bounds__(256) bapply(const int2* list, const int* len, 
   }
 }
 
-// Batched column-tridiagonal sweeps (items (slot, column)); the Jacobi part
-// of the line preconditioner runs in the fused prec+dot chunk kernel.
-__global__ void bthomas(const int2* list, const int* len, const BSlot* slots, const BState* st) {
+// 16-byte asynchronous copies global -> shared and their groups
+__device__ __forceinline__ void bcp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bcp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bcp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Batched apply for 6-dof cells whose columns read at most two blocks from
+// at most two cells (W2): the per-item column descriptors sit in list order
+// in the batch's own pool (copied at admission), so each warp keeps the
+// descriptors of its next kBFetchDepth items in flight (cp.async ring in
+// shared memory) and an item waits on memory once, for its matrix rows and x
+// values. Same sums in the same order as bapply.
+constexpr int kBFetchDepth = 4;
+
+template <bool RESID>
+__global__ void __launch_bounds__(256, RESID ? 2 : 3) bapply_fetch(const int2* list, const int* len,
+                                                                   const BSlot* slots,
+                                                                   const BState* st, const int* gate,
+                                                                   const int* bdesc) {
+  using T = typename std::conditional<RESID, double, float>::type;
+  constexpr int NDF2 = 6, GS = fd_group_ints(NDF2), FS = fd_ints(NDF2), NV = FS / 4;
+  __shared__ __align__(16) int ring[8][kBFetchDepth][FS];
+  if (gate && !*((volatile const int*)gate)) return;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int L = *len;
-  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < L; u += gridDim.x * blockDim.x) {
-    const int2 w = list[u];
-    if (w.x < 0 || !ph_active(st[w.x])) continue;
-    const BSlot D = slots[w.x];  // local copy: the z stores cannot alias it
-    thomas_sweep<8>(__ldg(D.first + w.y), D.ind, D.nrow, D.ncol, w.y, D.fa, D.finv, D.fc,
-                    (const float*)D.r, D.z);
+  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t e0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+#pragma unroll
+  for (int q = 0; q < kBFetchDepth; ++q) {
+    const int64_t e = e0 + q * nwarp;
+    if (lane < NV && e < L) bcp_async16(&ring[wib][q][4 * lane], bdesc + e * FS + 4 * lane);
+    bcp_commit();
+  }
+  int2 wn = e0 < L ? list[e0] : make_int2(-1, -1);
+  int sl = 0;
+  for (int64_t e = e0; e < L; e += nwarp) {
+    bcp_wait<kBFetchDepth - 1>();
+    __syncwarp();
+    const int2 w = wn;
+    wn = e + nwarp < L ? list[e + nwarp] : make_int2(-1, -1);
+    const int* d = ring[wib][sl];
+    if (w.x >= 0 && (RESID ? ph_resid(st[w.x]) : ph_run(st[w.x]))) {
+      const BSlot* P = slots + w.x;
+      const T* __restrict__ M = RESID ? (const T*)P->M64 : (const T*)P->M32;
+      const int blk = RESID ? P->blk64 : P->blk32;
+      const T* __restrict__ x = RESID ? (const T*)P->x : (const T*)P->p;
+      T* __restrict__ y = RESID ? (T*)P->r64 : (T*)P->z;
+      const double* __restrict__ bv = P->b;
+      const int nl = P->nl;
+      const size_t cell_stride = (size_t)NDF2 * blk;
+      const int base = d[0], h = d[1], ng = d[2];
+      for (int l0 = 0; l0 < h; l0 += 32) {
+        const int l = l0 + lane;
+        T acc = T(0);
+        const uint32_t pk0 = (uint32_t)d[5];
+        const int o0 = (pk0 >> 8) & 7u;
+        const int k0 = l - o0;
+        const bool v0 = (unsigned)k0 < (unsigned)nl;
+        const T* M0 = M + (size_t)d[4] * cell_stride + (size_t)((pk0 >> 2) & 63u) * blk + (v0 ? k0 : 0);
+        if (ng == 2) {
+          const uint32_t pk1 = (uint32_t)d[5 + GS];
+          const int k1 = l - (int)((pk1 >> 8) & 7u);
+          const bool v1 = (unsigned)k1 < (unsigned)nl;
+          const T* M1 = M + (size_t)d[4 + GS] * cell_stride + (size_t)((pk1 >> 2) & 63u) * blk +
+                        (v1 ? k1 : 0);
+          T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+            a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+          }
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
+            b1[j] = v1 ? __ldg(x + d[6 + GS + j] + k1) : T(0);
+          }
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j)
+            if (v0) acc = fmaT(a0[j], b0[j], acc);
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j)
+            if (v1) acc = fmaT(a1[j], b1[j], acc);
+        } else if ((pk0 & 3u) == 1) {
+          T a0[NDF2], b0[NDF2];
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+            b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
+          }
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j)
+            if (v0) acc = fmaT(a0[j], b0[j], acc);
+        } else {
+          // one cell, two records (bottom and top of a column)
+          const int o1 = (pk0 >> 17) & 7u;
+          const int k1 = l - o1;
+          const bool v1 = (unsigned)k1 < (unsigned)nl;
+          const bool pair = o1 == o0 + 1;
+          const T* M1 = M + (size_t)d[4] * cell_stride + (size_t)((pk0 >> 11) & 63u) * blk +
+                        (v1 ? k1 : 0);
+          T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+            b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
+            a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+          }
+          if (pair) {
+#pragma unroll
+            for (int j = 0; j < NDF2; ++j) {
+              const T up = __shfl_up_sync(0xffffffffu, b0[j], 1);
+              b1[j] = (lane == 0) ? (v1 ? __ldg(x + d[6 + j] + k1) : T(0)) : up;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < NDF2; ++j) b1[j] = v1 ? __ldg(x + d[6 + j] + k1) : T(0);
+          }
+#pragma unroll
+          for (int j = 0; j < NDF2; ++j) {
+            if (v0) acc = fmaT(a0[j], b0[j], acc);
+            if (v1) acc = fmaT(a1[j], b1[j], acc);
+          }
+        }
+        if (l < h) {
+          const int row = base + l;
+          if (RESID)
+            y[row] = (T)bv[row] - acc;
+          else
+            y[row] = acc;
+        }
+      }
+    }
+    __syncwarp();
+    // the slot is free again: fetch the descriptor kBFetchDepth items ahead
+    const int64_t en = e + kBFetchDepth * nwarp;
+    if (lane < NV && en < L) bcp_async16(&ring[wib][sl][4 * lane], bdesc + en * FS + 4 * lane);
+    bcp_commit();
+    sl = sl + 1 == kBFetchDepth ? 0 : sl + 1;
+  }
+  bcp_wait<0>();
+}
+
+// Batched column-tridiagonal sweeps (the Jacobi part of the line
+// preconditioner runs in the fused prec+dot chunk kernel), the rows of 64
+// consecutive list items (columns, of any slots) staged through shared memory: one warp per column copies its
+// rows in and out (a column's rows are contiguous dofs, so the copies
+// coalesce), and each thread sweeps its column on the staged copy with the
+// factors read from global memory (coalesced: [row][column]); same arithmetic
+// as thomas_sweep. Admission refuses columns of more than kBRows rows.
+constexpr int kBCols = 64, kBRows = 160, kBThreads = 128;
+
+__global__ void __launch_bounds__(kBThreads) bthomas_staged(const int2* list, const int* len,
+                                                             const BSlot* slots, const BState* st) {
+  constexpr int LD = kBCols + 1, NW = kBThreads / 32, CPW = kBCols / NW;
+  __shared__ float xs[kBRows * LD];
+  // per column of the chunk: rows (0: nothing to do), first dof, indirection
+  // and the slot's r and z (read once, so the copies below do not wait on
+  // the list and slot records column by column)
+  __shared__ int s_nrow[kBCols], s_f[kBCols];
+  __shared__ const int* s_ind[kBCols];
+  __shared__ const float* s_r[kBCols];
+  __shared__ float* s_z[kBCols];
+  __shared__ int s_maxrow;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int L = *len;
+  for (int u0 = blockIdx.x * kBCols; u0 < L; u0 += gridDim.x * kBCols) {
+    if (threadIdx.x == 0) s_maxrow = 0;
+    __syncthreads();
+    if (threadIdx.x < kBCols) {
+      const int t = threadIdx.x, u = u0 + t;
+      int nrow = 0;
+      if (u < L) {
+        const int2 w = list[u];
+        if (w.x >= 0 && ph_active(st[w.x])) {
+          const BSlot* D = slots + w.x;
+          nrow = D->nrow;
+          s_f[t] = __ldg(D->first + w.y);
+          s_ind[t] = D->ind;
+          s_r[t] = D->r;
+          s_z[t] = D->z;
+        }
+      }
+      s_nrow[t] = nrow;
+      atomicMax(&s_maxrow, nrow);
+    }
+    __syncthreads();
+    const int maxrow = s_maxrow;
+    // stage: lane l copies row r0 + l of the warp's columns, loads first
+    for (int r0 = 0; r0 < maxrow; r0 += 32) {
+      const int i = r0 + lane;
+      float v[CPW];
+#pragma unroll
+      for (int k = 0; k < CPW; ++k) {
+        const int j = warp + NW * k;
+        v[k] = i < s_nrow[j] ? s_r[j][s_f[j] + __ldg(s_ind[j] + i)] : 0.0f;
+      }
+#pragma unroll
+      for (int k = 0; k < CPW; ++k) {
+        const int j = warp + NW * k;
+        if (i < s_nrow[j]) xs[i * LD + j] = v[k];
+      }
+    }
+    __syncthreads();
+    const int j = threadIdx.x;
+    if (j < kBCols && s_nrow[j] > 0) {
+      const int2 w = list[u0 + j];
+      const BSlot* D = slots + w.x;
+      const int nrow = s_nrow[j], nc = D->ncol, c = w.y;
+      const float *fa = D->fa, *finv = D->finv, *fc = D->fc;
+      float* col = xs + j;
+      double d = 0.0;
+      constexpr int R = 8;
+      for (int i0 = 0; i0 < nrow; i0 += R) {
+        double iv[R], av[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int i = i0 + q;
+          if (i < nrow) {
+            iv[q] = (double)__ldg(finv + (size_t)i * nc + c);
+            av[q] = (double)__ldg(fa + (size_t)i * nc + c);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int i = i0 + q;
+          if (i < nrow) {
+            const double xv = (double)col[i * LD];
+            d = (i == 0) ? iv[q] * xv : iv[q] * fma(-av[q], d, xv);
+            col[i * LD] = (float)d;
+          }
+        }
+      }
+      for (int i0 = nrow - 2; i0 >= 0; i0 -= R) {
+        double cv[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int i = i0 - q;
+          if (i >= 0) cv[q] = (double)__ldg(fc + (size_t)i * nc + c);
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int i = i0 - q;
+          if (i >= 0) {
+            d = fma(-cv[q], d, (double)col[i * LD]);
+            col[i * LD] = (float)d;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (int r0 = 0; r0 < maxrow; r0 += 32) {
+      const int i = r0 + lane;
+#pragma unroll
+      for (int k = 0; k < CPW; ++k) {
+        const int jj = warp + NW * k;
+        if (i < s_nrow[jj]) s_z[jj][s_f[jj] + __ldg(s_ind[jj] + i)] = xs[i * LD + jj];
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -285,7 +548,10 @@ struct lfx_batch {
   double* d_partials = nullptr;
   unsigned* d_tickets = nullptr;
   double* pool64 = nullptr;  // r64 per slot
-  float* pool32 = nullptr;   // r, p, z per slot (3 per dof)
+  float* pool32 = nullptr;   // r, p, z, xc per slot (4 per dof)
+  // per entity-list item, the column descriptor of the prefetching gather
+  // (6-dof cells), copied from the slot's operator at admission
+  int* d_bdesc = nullptr;
   std::vector<SlotHost> slots;
   cudaGraphExec_t graph = nullptr;
   int64_t graph_kernels = 0;
@@ -353,7 +619,11 @@ int launch_super(lfx_batch* B) {
   auto resid = [] __device__(const BState& s) { return ph_resid(s); };
   auto active = [] __device__(const BState& s) { return ph_active(s); };
   // 1. z = A32 p
-  bapply<NDF2, false><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, nullptr);
+  if constexpr (NDF2 == 6)
+    bapply_fetch<false><<<ctx->num_sms * 3, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, nullptr,
+                                                                    B->d_bdesc);
+  else
+    bapply<NDF2, false><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, nullptr);
   // 2. alpha = rz / <p, z>
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
       B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, run,
@@ -362,15 +632,15 @@ int launch_super(lfx_batch* B) {
         a[0] = fma((double)v.a, (double)v.b, a[0]);
       },
       [] __device__(const BSlot&, BState& S, const double* t) { S.alpha = S.rz / t[0]; });
-  // 3. x += alpha p (FP64); r -= alpha z (FP32); ||r||; decide on a true residual
+  // 3. xc += alpha p, r -= alpha z (FP32); ||r||; decide on a true residual
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
       B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, run,
       [] __device__(const BSlot& D, int64_t i) {
-        return V4<double>{D.x[i], (double)D.p[i], (double)D.r[i], (double)D.z[i]};
+        return V4<float>{D.xc[i], D.p[i], D.r[i], D.z[i]};
       },
-      [] __device__(const BSlot& D, const BState& S, int64_t i, const V4<double>& v, double* a) {
-        D.x[i] = fma(S.alpha, v.b, v.a);
-        const float ri = fmaf((float)(-S.alpha), (float)v.d, (float)v.c);
+      [] __device__(const BSlot& D, const BState& S, int64_t i, const V4<float>& v, double* a) {
+        D.xc[i] = fmaf((float)S.alpha, v.b, v.a);
+        const float ri = fmaf((float)(-S.alpha), v.d, v.c);
         D.r[i] = ri;
         a[0] = fma((double)ri, (double)ri, a[0]);
       },
@@ -383,8 +653,21 @@ int launch_super(lfx_batch* B) {
           *need = 1;
         }
       });
+  // 3b. reliable update: x += xc (FP64), xc = 0 (new slots: xc = 0)
+  bchunk<0><<<gridc, RT, 0, ctx->stream>>>(
+      B->d_ch, lc, sl, st, pa, tk, need, nullptr, resid,
+      [] __device__(const BSlot& D, int64_t i) { return V2<double>{D.x[i], (double)D.xc[i]}; },
+      [] __device__(const BSlot& D, const BState& S, int64_t i, const V2<double>& v, double*) {
+        if (S.phase != PH_INIT) D.x[i] = v.a + v.b;
+        D.xc[i] = 0.0f;
+      },
+      [] __device__(const BSlot&, BState&, const double*) {});
   // 4. r64 = b - A64 x (new slots, and slots taking a true residual)
-  bapply<NDF2, true><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, need);
+  if constexpr (NDF2 == 6)
+    bapply_fetch<true><<<ctx->num_sms * 2, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, need,
+                                                                   B->d_bdesc);
+  else
+    bapply<NDF2, true><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, need);
   // 5. ||r64||, r = r64 (FP32); convergence on the true residual
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
       B->d_ch, lc, sl, st, pa, tk, need, nullptr, resid,
@@ -420,7 +703,8 @@ int launch_super(lfx_batch* B) {
       });
   // 6. z = P r (column sweeps for the line kind), then the Jacobi rows fused
   //    with rz_new = <r, z> and beta
-  if (B->cap_col > 0) bthomas<<<ctx->num_sms * 8, 128, 0, ctx->stream>>>(B->d_col, lk, sl, st);
+  if (B->cap_col > 0)
+    bthomas_staged<<<ctx->num_sms * 8, kBThreads, 0, ctx->stream>>>(B->d_col, lk, sl, st);
   bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
       B->d_ch, lc, sl, st, pa, tk, nullptr, need, active,
       [] __device__(const BSlot& D, int64_t i) { return V3<float>{D.r[i], D.diag[i], D.z[i]}; },
@@ -468,7 +752,7 @@ int capture(lfx_batch* B) {
   e = cudaGraphInstantiate(&B->graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
-  B->graph_kernels = (B->cap_col > 0 ? 8 : 7) * (int64_t)B->iters;
+  B->graph_kernels = (B->cap_col > 0 ? 9 : 8) * (int64_t)B->iters;
   return LFX_OK;
 }
 
@@ -503,7 +787,9 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t max_d
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_partials, sizeof(double) * B->cap_part);
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_tickets, sizeof(unsigned) * max_slots);
   if (!rc) rc = dmalloc(ctx, (void**)&B->pool64, sizeof(double) * max_dofs);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->pool32, sizeof(float) * 3 * max_dofs);
+  if (!rc) rc = dmalloc(ctx, (void**)&B->pool32, sizeof(float) * 4 * max_dofs);
+  if (!rc && ndf == 6)
+    rc = dmalloc(ctx, (void**)&B->d_bdesc, sizeof(int) * fd_ints(6) * B->cap_ent);
   if (!rc && cudaMallocHost((void**)&B->h_state, sizeof(BState) * max_slots) != cudaSuccess)
     rc = LFX_OUT_OF_MEMORY;
   B->h_slots = new BSlot[max_slots];
@@ -542,7 +828,8 @@ int lfx_batch_destroy(lfx_batch* B) {
   dfree(ctx, B->d_partials, sizeof(double) * B->cap_part);
   dfree(ctx, B->d_tickets, sizeof(unsigned) * B->max_slots);
   dfree(ctx, B->pool64, sizeof(double) * B->cap_dofs);
-  dfree(ctx, B->pool32, sizeof(float) * 3 * B->cap_dofs);
+  dfree(ctx, B->pool32, sizeof(float) * 4 * B->cap_dofs);
+  if (B->d_bdesc) dfree(ctx, B->d_bdesc, sizeof(int) * fd_ints(6) * B->cap_ent);
   if (B->h_state) cudaFreeHost(B->h_state);
   delete[] B->h_slots;
   delete B;
@@ -563,9 +850,14 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
     return fail(ctx, LFX_TYPE_MISMATCH, "batch needs FP64 and FP32 copies of one operator");
   if (L->ndf_from != B->ndf || L->ndf_to != B->ndf || L->max_nrec > 2 || !L->ent_pack)
     return fail(ctx, LFX_NOT_SUPPORTED, "operator shape does not match the batch");
+  if (B->ndf == 6 && (!L->fdesc || L->fd_ints != fd_ints(6)))
+    return fail(ctx, LFX_NOT_SUPPORTED,
+                "batch of 6-dof cells needs columns reading at most two blocks from two cells");
   if (prec32->precision != LFX_R32 || (prec32->kind != PREC_DIAG && prec32->kind != PREC_CMA) ||
       !prec32->rdiag || prec32->rdiag_n != L->undf_to)
     return fail(ctx, LFX_NOT_SUPPORTED, "batch needs an FP32 Jacobi or column preconditioner with a diagonal");
+  if (prec32->kind == PREC_CMA && prec32->nrow > kBRows)
+    return fail(ctx, LFX_NOT_SUPPORTED, "batch column preconditioner: at most 160 rows per column");
   if (b->precision != LFX_R64 || x->precision != LFX_R64 || b->undf[0] != L->undf_to ||
       x->undf[0] != L->undf_to)
     return fail(ctx, LFX_TYPE_MISMATCH, "b and x must be FP64 vectors of the operator's space");
@@ -626,9 +918,10 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   D.b = (const double*)b->data[0];
   D.x = (double*)x->data[0];
   D.r64 = B->pool64 + H.vec_off;
-  D.r = B->pool32 + 3 * H.vec_off;
+  D.r = B->pool32 + 4 * H.vec_off;
   D.p = D.r + n;
   D.z = D.p + n;
+  D.xc = D.z + n;
   B->h_slots[s] = D;
   BState S{};
   S.phase = PH_INIT;
@@ -656,6 +949,10 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   for (int64_t c = 0; c < nch; ++c) ch[c] = make_int2(s, (int)c);
   for (int64_t c = 0; c < ncol; ++c) col[c] = make_int2(s, (int)c);
   rc = upload_region(ctx, B->d_ent + H.ent_off, ent);
+  if (!rc && B->d_bdesc)
+    LFX_CK(ctx, cudaMemcpyAsync(B->d_bdesc + (size_t)H.ent_off * fd_ints(6), L->fdesc,
+                                sizeof(int) * fd_ints(6) * H.ent_len, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
   if (!rc) rc = upload_region(ctx, B->d_ch + H.ch_off, ch);
   if (!rc && ncol) rc = upload_region(ctx, B->d_col + H.col_off, col);
   if (!rc) LFX_CK(ctx, cudaMemcpyAsync(B->d_slots + s, &B->h_slots[s], sizeof(BSlot),

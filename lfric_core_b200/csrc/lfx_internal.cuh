@@ -194,6 +194,11 @@ int launch_chunks(lfx_ctx* ctx, int64_t n, Ld ld, Op op, Fin fin, const int* ski
   return LFX_OK;
 }
 
+// ints of one group and of one column in the per-column descriptors of the
+// prefetching gather (fdesc of lfx_lma_layout)
+__host__ __device__ constexpr int fd_group_ints(int ndf2) { return (2 + ndf2 + 3) / 4 * 4; }
+__host__ __device__ constexpr int fd_ints(int ndf2) { return 4 + 2 * fd_group_ints(ndf2); }
+
 // Thomas sweeps of one column with x-independent factors stored [row][column]
 // (nc columns): y = T^{-1} x on rows f + ind[i], i < nrow, in FP64 with the
 // forward result rounded to TX between the sweeps. The loads of R rows are

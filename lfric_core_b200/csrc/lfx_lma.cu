@@ -270,8 +270,6 @@ __global__ void __launch_bounds__(256) lma_gather2(LayoutArgs A, const T* __rest
 // Per-column descriptor of lma_fetch (columns reading at most two (cell, df)
 // blocks from at most two cells): ints {base, h, groups, 0}, then per group
 // {cell, record, map_from row} padded to a multiple of 4 ints.
-__host__ __device__ constexpr int fd_group_ints(int ndf2) { return (2 + ndf2 + 3) / 4 * 4; }
-__host__ __device__ constexpr int fd_ints(int ndf2) { return 4 + 2 * fd_group_ints(ndf2); }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
@@ -1638,7 +1636,9 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     if (*kernel == 3 || *kernel == 5) ts->stages = op->tune_stages;
     if ((*kernel != 0 && *kernel != 4) || ts->warps) return;
   }
-  *kernel = gather2_ok(op) ? 1 : 2;
+  // untuned: the prefetching gather where it fits (fastest measured on W2
+  // and W3 columns), else the register gather, else the generic one
+  *kernel = fetch_ok(op) ? 3 : (gather2_ok(op) ? 1 : 2);
 }
 
 }  // namespace

@@ -74,6 +74,7 @@ struct lfx_solver {
   bool inner_mode = false;      // GMRES used as the inner solve of a refinement
   bool zero_x0 = false;         // the next apply starts from x = 0 (set by the refinement)
   std::vector<GraphEntry> graphs;
+  int pending = -1;  // graph launched last, whose timings are not collected yet
   std::vector<lfx_vec*> hv;  // work vectors of the host-driven solvers
   double rho_relax = 1.0, lmin = 0.0, lmax = 0.0;  // Jacobi / Chebyshev
   // refined solver
@@ -111,8 +112,28 @@ int init_state(lfx_solver* s) {
 }
 
 // Runs `body` (a fixed sequence of launches on the context stream) through a
-// CUDA graph cached per (x, b) pair, then reads the device state.
-int run_graph(lfx_solver* s, const void* x, const void* b, const std::function<int()>& body) {
+// CUDA graph cached per (x, b) pair, then reads the device state (wait) or
+// leaves the graph queued (!wait: the caller reads the state later and then
+// calls collect_timing).
+// adds the apply timings of the last launched graph (finished) to the context
+void collect_timing(lfx_solver* s) {
+  lfx_ctx* ctx = s->ctx;
+  const int pi = s->pending;
+  s->pending = -1;
+  if (pi < 0 || pi >= (int)s->graphs.size() || !ctx->time_applies) return;
+  GraphEntry* ge = &s->graphs[pi];
+  for (auto& p : ge->ev) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      const int k = p.prec == LFX_R32 ? 1 : 0;
+      ctx->timed_ms[k] += ms;
+      ctx->timed_launches[k] += 1;
+    }
+  }
+}
+
+int run_graph(lfx_solver* s, const void* x, const void* b, const std::function<int()>& body,
+              bool wait = true) {
   lfx_ctx* ctx = s->ctx;
   GraphEntry* ge = nullptr;
   for (auto& g : s->graphs)
@@ -149,18 +170,11 @@ int run_graph(lfx_solver* s, const void* x, const void* b, const std::function<i
   }
   LFX_CK(ctx, cudaGraphLaunch(ge->exec, ctx->stream));
   ctx->launches += ge->kernels;
+  s->pending = (int)(ge - s->graphs.data());
+  if (!wait) return LFX_OK;
   int rc = read_state(s);
   if (rc) return rc;
-  if (ctx->time_applies) {
-    for (auto& p : ge->ev) {
-      float ms = 0.f;
-      if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
-        const int k = p.prec == LFX_R32 ? 1 : 0;
-        ctx->timed_ms[k] += ms;
-        ctx->timed_launches[k] += 1;
-      }
-    }
-  }
+  collect_timing(s);
   return LFX_OK;
 }
 
@@ -173,6 +187,7 @@ void free_graphs(lfx_solver* s) {
     }
   }
   s->graphs.clear();
+  s->pending = -1;
 }
 
 template <class T, int N>
@@ -799,8 +814,11 @@ __global__ void gmres_finish_cycle(DevState* S, double* gm, int K, const double*
 #undef H
 }
 
+// one_cycle: queue the initial residual and exactly one restart cycle and
+// return without waiting (the refinement reads the state after its own
+// residual, in the same synchronisation)
 template <class T>
-int gmres_run(lfx_solver* s, T* x, const T* b) {
+int gmres_run(lfx_solver* s, T* x, const T* b, bool one_cycle = false) {
   lfx_ctx* ctx = s->ctx;
   DevState* S = s->d_state;
   const int64_t n = s->n;
@@ -1044,6 +1062,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b) {
         done);
     return q;
   };
+  if (one_cycle) return run_graph(s, x, b, cycle, false);
   // no host round trip before the first graph: its kernels idle if the
   // initial residual already ended the solve (device flags)
   do {
@@ -1148,6 +1167,10 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
     *out = ctx->h_scalars[0];
     return LFX_OK;
   };
+  // an FP32 GMRES inner solve runs one restart cycle per refinement step,
+  // queued with the step's FP64 residual (one host round trip per step)
+  const bool fast = s->inner->kind == LFX_SOLVER_GMRES && s->inner->inner_mode &&
+                    s->inner->precision == LFX_R32;
   double r0 = 0.0, rn = 0.0;
   if ((rc = resid_norm(&r0))) return rc;
   memset(info, 0, sizeof *info);
@@ -1171,11 +1194,22 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
         NoFin{});
     if (rc) return rc;
     lfx_solve_info ii{};
-    s->inner->zero_x0 = s->inner->kind == LFX_SOLVER_GMRES;  // d32 was just zeroed
-    rc = lfx_solver_apply(s->inner, s->d32, s->r32, &ii);
-    if (rc && rc != LFX_NOT_CONVERGED) return rc;
-    info->inner_iterations += ii.iterations;
-    info->applies += ii.applies;
+    lfx_solver* in = s->inner;
+    if (fast) {
+      // one inner GMRES cycle, queued; its state comes back with the
+      // residual norm below, in one synchronisation
+      if ((rc = init_state(in))) return rc;
+      in->zero_x0 = true;  // d32 was just zeroed
+      if ((rc = gmres_run<float>(in, d32, r32, true))) return rc;
+      LFX_CK(ctx, cudaMemcpyAsync(in->h_state, in->d_state, sizeof(DevState),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    } else {
+      in->zero_x0 = in->kind == LFX_SOLVER_GMRES;  // d32 was just zeroed
+      rc = lfx_solver_apply(in, s->d32, s->r32, &ii);
+      if (rc && rc != LFX_NOT_CONVERGED) return rc;
+      info->inner_iterations += ii.iterations;
+      info->applies += ii.applies;
+    }
     // x += ||r|| d
     const double scale = rn;
     rc = launch_chunks<0>(
@@ -1184,6 +1218,16 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
         NoFin{});
     if (rc) return rc;
     if ((rc = resid_norm(&rn))) return rc;
+    if (fast) {
+      collect_timing(in);
+      fill_info(in, &ii);
+      if (ii.status == LFX_NAN_DETECTED) {
+        info->status = LFX_NAN_DETECTED;
+        return fail(ctx, LFX_NAN_DETECTED, "NaN in the inner solve");
+      }
+      info->inner_iterations += ii.iterations;
+      info->applies += ii.applies;
+    }
     info->applies += 1;
     info->outer_iterations = k;
     info->iterations = k;

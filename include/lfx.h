@@ -136,6 +136,10 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
  * would; LFX_NOT_SUPPORTED if it does not fit the operator. Kernel 5 takes
  * stages 0 (one cell per warp) or 2, 3 (cells staged ahead in shared memory). */
 int lfx_op_set_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps);
+/* bytes of the stored local matrices: the full copy every kernel can read
+ * and the packed upper triangle of a bitwise symmetric operator on one
+ * dofmap (0 when there is none), which the cell scatter reads instead */
+int lfx_op_storage(const lfx_op* op, int64_t* full_bytes, int64_t* packed_bytes);
 /* diag(A) by mm_diagonal_kernel (sci_mm_diagonal_kernel_mod.F90:99-125) */
 int lfx_lma_diagonal(lfx_op* op, lfx_vec* diag);
 /* transpose apply y = A^T x for a matrix stored as (ncell_3d, ndf_to, ndf_from)

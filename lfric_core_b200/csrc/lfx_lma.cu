@@ -1841,6 +1841,16 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
   return rc;
 }
 
+// Storage of the local matrices: bytes of the full [cell][df][df2][k] copy
+// and of the packed upper triangle (0 when the operator is not symmetric or
+// not on one dofmap); the cell scatter reads the packed copy when it exists.
+int lfx_op_storage(const lfx_op* op, int64_t* full_bytes, int64_t* packed_bytes) {
+  if (!op) return LFX_INVALID_ARGUMENT;
+  if (full_bytes) *full_bytes = (int64_t)op->mat_bytes;
+  if (packed_bytes) *packed_bytes = op->smat ? (int64_t)op->smat_bytes : 0;
+  return LFX_OK;
+}
+
 // Keeps one launch configuration for later applies of this operator (as the
 // autotuner would), after checking that it fits.
 int lfx_op_set_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps) {

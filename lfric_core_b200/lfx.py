@@ -105,6 +105,7 @@ _SIGS = [
     ("lfx_op_autotune", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                          C.POINTER(C.c_int32), C.POINTER(C.c_float)], C.c_int),
     ("lfx_op_set_apply", [vp, C.c_int32, C.c_int32, C.c_int32], C.c_int),
+    ("lfx_op_storage", [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     ("lfx_op_time_apply", [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                            C.POINTER(C.c_float)], C.c_int),
     ("lfx_op_apply_transpose", [vp, vp, vp], C.c_int),
@@ -404,6 +405,13 @@ class LmaOperator(_Handle):
                 3: "register-gather-prefetch", 4: "staged-pipeline",
                 5: "cell-scatter"}[k.value]
         return {"kernel": name, "stages": s.value, "warps": w.value, "us": round(us.value, 2)}
+
+    def storage(self) -> dict:
+        """Bytes of the full local-matrix copy and of the packed upper
+        triangle (0 unless the operator is symmetric on one dofmap)."""
+        f, p = C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.L.lfx_op_storage(self.h, C.byref(f), C.byref(p)))
+        return {"full_bytes": f.value, "packed_bytes": p.value}
 
     def set_apply(self, kernel: int, stages: int = 0, warps: int = 0):
         """Keep one apply launch configuration for this operator (as the

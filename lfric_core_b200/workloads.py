@@ -234,8 +234,16 @@ def _run_solve_w2(args):
     ctx = lfx.Context(0)
     s64 = device_w2(ctx, p, lfx.R64)
     s32 = device_w2(ctx, p, lfx.R32, op64=s64.op64, cma=s64.cma, diag64=s64.diag)
-    s32.op.autotune(reps=10)
-    s64.op.autotune(reps=10)
+    if args.apply:
+        # a pinned configuration per precision, e.g. "5:0,5:2" (FP32, FP64),
+        # so a profiler sees the configuration an unprofiled run tunes to
+        (k32, st32), (k64, st64) = [tuple(int(v) for v in c.split(":"))
+                                    for c in args.apply.split(",")]
+        s32.op.set_apply(k32, st32)
+        s64.op.set_apply(k64, st64)
+    else:
+        s32.op.autotune(reps=10)
+        s64.op.autotune(reps=10)
     solvers = {"mixed": refined_gmres(s32, gcrk=10, inner_rtol=1e-4, r_tol=1e-8),
                "fp64": lfx.GMRES(s64.op, s64.prec, 10, 1e-8, 1e-16, 200)}
     b = lfx.FieldVector.from_array(ctx, p.rhs)
@@ -294,6 +302,8 @@ def main(argv=None):
     w.add_argument("--seed", type=int, default=2)
     w.add_argument("--kinds", default="mixed,fp64", help="comma-separated: mixed, fp64")
     w.add_argument("--solves", type=int, default=1)
+    w.add_argument("--apply", default="",
+                   help="pinned apply kernel:stages for FP32,FP64 (default: autotune)")
     args = ap.parse_args(argv)
     {"apply": _run_apply, "time-apply": _run_time_apply, "mrhs": _run_mrhs,
      "batch-w2": _run_batch_w2, "solve-w2": _run_solve_w2}[args.cmd](args)

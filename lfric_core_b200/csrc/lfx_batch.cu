@@ -271,7 +271,8 @@ __device__ __forceinline__ void bcp_wait() {
 // in the batch's own pool (copied at admission), so each warp keeps the
 // descriptors of its next kBFetchDepth items in flight (cp.async ring in
 // shared memory) and an item waits on memory once, for its matrix rows and x
-// values. Same sums in the same order as bapply.
+// values (matrix rows with streaming, evict-first loads). Same sums in the
+// same order as bapply.
 constexpr int kBFetchDepth = 4;
 
 template <bool RESID>
@@ -328,8 +329,8 @@ __global__ void __launch_bounds__(256, RESID ? 2 : 3) bapply_fetch(const int2* l
           T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
 #pragma unroll
           for (int j = 0; j < NDF2; ++j) {
-            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
-            a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+            a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
+            a1[j] = v1 ? __ldcs(M1 + j * nl) : T(0);
           }
 #pragma unroll
           for (int j = 0; j < NDF2; ++j) {
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(256, RESID ? 2 : 3) bapply_fetch(const int2* l
           T a0[NDF2], b0[NDF2];
 #pragma unroll
           for (int j = 0; j < NDF2; ++j) {
-            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+            a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
             b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
           }
 #pragma unroll
@@ -363,9 +364,9 @@ __global__ void __launch_bounds__(256, RESID ? 2 : 3) bapply_fetch(const int2* l
           T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
 #pragma unroll
           for (int j = 0; j < NDF2; ++j) {
-            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+            a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
             b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
-            a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+            a1[j] = v1 ? __ldcs(M1 + j * nl) : T(0);
           }
           if (pair) {
 #pragma unroll

@@ -179,7 +179,9 @@ __device__ __forceinline__ void gather_record(const LayoutArgs& A, int g, int& c
 
 // One cell group's contribution to output row l of an entity column (groups of
 // at most two records): all loads of the group are issued before the FMA
-// chain that consumes them. The warp must be converged (pair shuffles).
+// chain that consumes them; matrix rows, read once per apply, with streaming
+// (evict-first) loads so that x stays in L2. The warp must be converged (pair
+// shuffles).
 template <class T, int NDF2>
 __device__ __forceinline__ T group_acc(const LayoutArgs& A, const T* __restrict__ M,
                                        const T* __restrict__ x, size_t cell_stride, int l,
@@ -193,7 +195,7 @@ __device__ __forceinline__ T group_acc(const LayoutArgs& A, const T* __restrict_
     T a0[NDF2], b0[NDF2];
 #pragma unroll
     for (int j = 0; j < NDF2; ++j) {
-      a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+      a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
       b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
     }
 #pragma unroll
@@ -211,9 +213,9 @@ __device__ __forceinline__ T group_acc(const LayoutArgs& A, const T* __restrict_
   T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
 #pragma unroll
   for (int j = 0; j < NDF2; ++j) {
-    a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
+    a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
     b0[j] = v0 ? __ldg(x + mf[j] + k0) : T(0);
-    a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+    a1[j] = v1 ? __ldcs(M1 + j * nl) : T(0);
   }
   if (pair) {
 #pragma unroll
@@ -332,8 +334,8 @@ __global__ void __launch_bounds__(256, MINB) lma_fetch(LayoutArgs A, const T* __
         T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
 #pragma unroll
         for (int j = 0; j < NDF2; ++j) {
-          a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
-          a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
+          a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
+          a1[j] = v1 ? __ldcs(M1 + j * nl) : T(0);
         }
 #pragma unroll
         for (int j = 0; j < NDF2; ++j) {
@@ -824,9 +826,11 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
   const T* Mc = M + (size_t)c * C.cstride + (v ? lane : 0);
   constexpr int NP = SYM ? NDF * (NDF + 1) / 2 : NDF * NDF;
   T m[NP], xv[NDF], yo[NDF];
+  // the matrix is read once per apply: streaming (evict-first) loads keep x
+  // and the partial sums of y in L2 for the later colours
 #pragma unroll
   for (int p = 0; p < NP; ++p)
-    m[p] = v ? __ldg(Mc + (SYM ? p * nl : (p / NDF) * C.blk + (p % NDF) * nl)) : T(0);
+    m[p] = v ? __ldcs(Mc + (SYM ? p * nl : (p / NDF) * C.blk + (p % NDF) * nl)) : T(0);
 #pragma unroll
   for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldg(x + mf[j] + lane) : T(0);
 #pragma unroll

@@ -580,8 +580,7 @@ def main():
     # (the packed upper triangle for the cell scatter of this symmetric
     # operator), x read once, y written once, the map rows. The average is
     # over every FP32 apply of the timed solves (events around each apply in
-    # the solver graphs), residual-form applies (which read the full copy)
-    # included, so the fraction is a lower bound.
+    # the solver graphs), residual-form applies included.
     nc3 = p.mesh.ncell_3d
 
     def apply_bytes(op, esz, kernel):

@@ -125,7 +125,7 @@ int lfx_op_destroy(lfx_op* op);
  * (nullable) name the choice: kernel 0 pipeline / 1 register gather / 2
  * generic / 3 register gather with prefetched descriptors / 4 copy-staged
  * pipeline (matrix blocks and x values both staged in shared memory) / 5 cell
- * scatter (residual applies y = b - A x then take a gather), and its time per
+ * scatter, and its time per
  * apply. */
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
                     float* us);

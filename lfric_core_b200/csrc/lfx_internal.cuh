@@ -313,7 +313,8 @@ struct lfx_lma_layout {
   // each colour, and per cell {map row, flags, partners} padded to cs_ints
   // ints. flags bit df: this cell is the first (in colour order) on the
   // column of df; bit 8+df: df is the lower record of a pair; bit 16+df: the
-  // upper one. partners: 4 bits per df, the upper record of df's pair.
+  // upper one; bit 24+df: this cell is the last on the column of df.
+  // partners: 4 bits per df, the upper record of df's pair.
   bool cs_ok = false;
   int32_t cs_ints = 0;
   std::vector<int32_t> colour_start;

@@ -786,7 +786,8 @@ __global__ void relayout(const double* __restrict__ src, T* __restrict__ dst, in
 // column (lane = level), loads the cell's local matrices and x values once,
 // and adds M(df, df2) x(df2) into every dof of the cell in the reference's
 // order (df2 outer, df inner), directly into y. The first cell on a dof
-// column (in colour order) starts from zero, later ones from the stored sum;
+// column (in colour order) starts from zero, later ones from the stored sum,
+// and in the residual form (b given) the last one writes b - sum;
 // a column holding two records of the same cell at consecutive offsets (the
 // bottom and top faces or vertices of a cell column) is summed by the lane
 // of the output level, which takes the upper record's terms from the lane
@@ -807,10 +808,10 @@ struct CellArgs {
   const int* desc;
 };
 
-template <class T, int NDF, bool SYM>
+template <class T, int NDF, bool SYM, bool RESID>
 __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict__ M,
                                                  const T* __restrict__ x, T* __restrict__ y,
-                                                 const int* skip) {
+                                                 const T* __restrict__ b, const int* skip) {
   if (skip && *((volatile const int*)skip)) return;
   const int lane = threadIdx.x & 31;
   const int ci = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -857,13 +858,21 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
           if (v) acc = fmaT(MV(df, j), xv[j], acc);
           if (lane >= 1 && lane <= nl) acc = fmaT(mb, xb, acc);
         }
-        if (lane <= nl) y[mf[df] + lane] = acc;
+        if (lane <= nl) {
+          // the last cell on the column writes b - A x in the residual form
+          const int row = mf[df] + lane;
+          y[row] = (RESID && ((flags >> (24 + df)) & 1u)) ? b[row] - acc : acc;
+        }
       }
     } else {
       T acc = yo[df];
 #pragma unroll
       for (int j = 0; j < NDF; ++j) acc = fmaT(MV(df, j), xv[j], acc);
-      if (v) y[mf[df] + lane] = acc;
+      if (v) {
+        // the last cell on the column writes b - A x in the residual form
+        const int row = mf[df] + lane;
+        y[row] = (RESID && ((flags >> (24 + df)) & 1u)) ? b[row] - acc : acc;
+      }
     }
   }
 #undef MV
@@ -877,10 +886,12 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
 // memory. Same arithmetic as lma_cells.
 constexpr int kCellWarps = 4;
 
-template <class T, int NDF, bool SYM, int S>
+template <class T, int NDF, bool SYM, int S, bool RESID>
 __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, const T* __restrict__ M,
                                                                  const T* __restrict__ x,
-                                                                 T* __restrict__ y, int stage_bytes,
+                                                                 T* __restrict__ y,
+                                                                 const T* __restrict__ b,
+                                                                 int stage_bytes,
                                                                  const int* skip) {
   if (skip && *((volatile const int*)skip)) return;
   extern __shared__ __align__(16) unsigned char cell_ring[];
@@ -951,13 +962,21 @@ __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, co
             if (v) acc = fmaT(MV(df, j), xv[j], acc);
             if (lane >= 1 && lane <= nl) acc = fmaT(mb, xb, acc);
           }
-          if (lane <= nl) y[mf[df] + lane] = acc;
+          if (lane <= nl) {
+            // the last cell on the column writes b - A x in the residual form
+            const int row = mf[df] + lane;
+            y[row] = (RESID && ((flags >> (24 + df)) & 1u)) ? b[row] - acc : acc;
+          }
         }
       } else {
         T acc = yo[df];
 #pragma unroll
         for (int j = 0; j < NDF; ++j) acc = fmaT(MV(df, j), xv[j], acc);
-        if (v) y[mf[df] + lane] = acc;
+        if (v) {
+          // the last cell on the column writes b - A x in the residual form
+          const int row = mf[df] + lane;
+          y[row] = (RESID && ((flags >> (24 + df)) & 1u)) ? b[row] - acc : acc;
+        }
       }
     }
 #undef MV
@@ -1087,11 +1106,14 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
         if (cs) {
           const int32_t c = er[q].cell;
           const bool first = (int32_t)grp_cell.size() == ent_grp.back();
+          const bool last = r == er.size();
           const int a = rec_df(pk, 0);
           if (first) cs_flags[c] |= 1u << a;
+          if (last) cs_flags[c] |= 1u << (24 + a);
           if (n == 2) {
             const int bb = rec_df(pk, 1);
             if (first) cs_flags[c] |= 1u << bb;
+            if (last) cs_flags[c] |= 1u << (24 + bb);
             cs_flags[c] |= (1u << (8 + a)) | (1u << (16 + bb));
             cs_part[c] |= (uint32_t)bb << (4 * a);
           }
@@ -1486,8 +1508,9 @@ size_t cells_stage_bytes(const lfx_op* op) {
 constexpr size_t kCellSmemMax = 200 * 1024;
 
 // stages: 0 one cell per warp (lma_cells), 2 or 3 the staged pipeline
-template <class T, int N, bool SYM, int S>
-void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const int* skip) {
+template <class T, int N, bool SYM, int S, bool RESID>
+void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const void* b,
+                    const int* skip) {
   const lfx_lma_layout* L = op->lay;
   CellArgs C{L->nlayers, op->blk, SYM ? op->sblk : N * op->blk, L->cs_ints, nullptr, 0, L->cs_desc};
   const T* M = (const T*)(SYM ? op->smat : op->mat);
@@ -1497,11 +1520,11 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
   if constexpr (S > 0) {
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(lma_cells_pipe<T, N, SYM, S>,
+      cudaFuncSetAttribute(lma_cells_pipe<T, N, SYM, S, RESID>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellSmemMax);
       attr = true;
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_cells_pipe<T, N, SYM, S>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_cells_pipe<T, N, SYM, S, RESID>,
                                                   32 * kCellWarps, smem);
     if (per_sm < 1) per_sm = 1;
   }
@@ -1513,11 +1536,12 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
     if constexpr (S > 0) {
       const int grid = (int)std::min<int64_t>(((int64_t)C.ncells + kCellWarps - 1) / kCellWarps,
                                               (int64_t)ctx->num_sms * per_sm);
-      lma_cells_pipe<T, N, SYM, S><<<grid, 32 * kCellWarps, smem, ctx->stream>>>(
-          C, M, (const T*)x, (T*)y, sb, skip);
+      lma_cells_pipe<T, N, SYM, S, RESID><<<grid, 32 * kCellWarps, smem, ctx->stream>>>(
+          C, M, (const T*)x, (T*)y, (const T*)b, sb, skip);
     } else {
       const int grid = (int)(((int64_t)C.ncells * 32 + 255) / 256);
-      lma_cells<T, N, SYM><<<grid, 256, 0, ctx->stream>>>(C, M, (const T*)x, (T*)y, skip);
+      lma_cells<T, N, SYM, RESID><<<grid, 256, 0, ctx->stream>>>(C, M, (const T*)x, (T*)y, (const T*)b,
+                                                           skip);
     }
     ctx->launches++;
   }
@@ -1525,20 +1549,30 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
 }
 
 template <class T, int N, int S>
-void launch_cells_s(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const int* skip) {
-  if (op->smat)
-    launch_cells_t<T, N, true, S>(ctx, op, x, y, skip);
-  else
-    launch_cells_t<T, N, false, S>(ctx, op, x, y, skip);
+void launch_cells_s(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const void* b,
+                    const int* skip) {
+  // the residual form is its own instantiation: the plain apply keeps its
+  // register count (and occupancy)
+  if (op->smat) {
+    if (b)
+      launch_cells_t<T, N, true, S, true>(ctx, op, x, y, b, skip);
+    else
+      launch_cells_t<T, N, true, S, false>(ctx, op, x, y, b, skip);
+  } else {
+    if (b)
+      launch_cells_t<T, N, false, S, true>(ctx, op, x, y, b, skip);
+    else
+      launch_cells_t<T, N, false, S, false>(ctx, op, x, y, b, skip);
+  }
 }
 
 template <class T, int N>
 void launch_cells(lfx_ctx* ctx, const lfx_op* op, int stages, const void* x, void* y,
-                  const int* skip) {
+                  const void* b, const int* skip) {
   switch (stages) {
-    case 2: launch_cells_s<T, N, 2>(ctx, op, x, y, skip); return;
-    case 3: launch_cells_s<T, N, 3>(ctx, op, x, y, skip); return;
-    default: launch_cells_s<T, N, 0>(ctx, op, x, y, skip); return;
+    case 2: launch_cells_s<T, N, 2>(ctx, op, x, y, b, skip); return;
+    case 3: launch_cells_s<T, N, 3>(ctx, op, x, y, b, skip); return;
+    default: launch_cells_s<T, N, 0>(ctx, op, x, y, b, skip); return;
   }
 }
 
@@ -1551,7 +1585,7 @@ bool cells_stages_ok(const lfx_op* op, int stages) {
 
 // kernel: 0 bulk-copy pipelined (shape ts), 1 register gather, 2 generic,
 // 3 register gather with prefetched descriptors, 4 copy-staged pipeline (shape ts),
-// 5 cell scatter (y = A x only)
+// 5 cell scatter
 template <class T>
 void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& ts,
                     const void* x, void* y, const void* b, const int* skip) {
@@ -1559,9 +1593,9 @@ void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& 
   const LayoutArgs A = args_of(L, op->blk);
   if (kernel == 5) {
     switch (L->ndf_to) {
-      case 1: launch_cells<T, 1>(ctx, op, ts.stages, x, y, skip); return;
-      case 6: launch_cells<T, 6>(ctx, op, ts.stages, x, y, skip); return;
-      default: launch_cells<T, 8>(ctx, op, ts.stages, x, y, skip); return;
+      case 1: launch_cells<T, 1>(ctx, op, ts.stages, x, y, b, skip); return;
+      case 6: launch_cells<T, 6>(ctx, op, ts.stages, x, y, b, skip); return;
+      default: launch_cells<T, 8>(ctx, op, ts.stages, x, y, b, skip); return;
     }
   }
   if (kernel == 4) {
@@ -1664,11 +1698,6 @@ int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* 
   int kernel = 2;
   TmaShape ts;
   pick_apply(ctx, op, &kernel, &ts);
-  if (kernel == 5 && b) {
-    // the cell scatter computes y = A x only; residuals take a gather
-    ts = TmaShape{};
-    kernel = fetch_ok(op) ? 3 : (gather2_ok(op) ? 1 : 2);
-  }
   timing_begin(ctx, op->precision);
   ctx->launches++;
   launch_apply(ctx, op, kernel, ts, x, y, b, skip);

@@ -240,11 +240,13 @@ __global__ void __launch_bounds__(128) cma_prec_apply(
 // and the result is copied out the same way. Row i of column j sits at
 // [i * (kStageCols + 1) + j], conflict-free for the row-wise copies and the
 // column-wise sweeps. Same arithmetic as thomas_sweep, so the same bits.
+// Factors, read once per application, come through streaming (evict-first)
+// loads so that x and y stay in L2.
 //
-// Rows the columns do not cover get y = x / diag: by a separate elementwise
-// launch where the diagonal carries zeros on the column rows (zero_sentinel;
-// its blocks then need no shared memory), else by runs of rows in the blocks
-// after the Thomas blocks.
+// Rows the columns do not cover get y = x / diag: elementwise, in the same
+// launch for small stages or in a launch of their own, where the diagonal
+// carries zeros on the column rows (zero_sentinel), else by runs of rows in
+// the blocks after the Thomas blocks.
 constexpr int kStageCols = 64;
 constexpr int kStageThreads = 128;
 
@@ -299,9 +301,9 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
           const int i = ib + RS * u;
           const bool ok = i < nrow && j < nc;
           const size_t g = (size_t)i * ncell + c0 + j;
-          va[u] = ok ? __ldg(fa + g) : T(0);
-          vi[u] = ok ? __ldg(finv + g) : T(0);
-          vc[u] = ok ? __ldg(fc + g) : T(0);
+          va[u] = ok ? __ldcs(fa + g) : T(0);
+          vi[u] = ok ? __ldcs(finv + g) : T(0);
+          vc[u] = ok ? __ldcs(fc + g) : T(0);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -338,8 +340,8 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
           for (int r = 0; r < R; ++r) {
             const int i = i0 + r;
             if (i < nrow) {
-              iv[r] = (double)__ldg(finv + (size_t)i * ncell + c);
-              av[r] = (double)__ldg(fa + (size_t)i * ncell + c);
+              iv[r] = (double)__ldcs(finv + (size_t)i * ncell + c);
+              av[r] = (double)__ldcs(fa + (size_t)i * ncell + c);
             }
           }
 #pragma unroll
@@ -357,7 +359,7 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const int i = i0 - r;
-            if (i >= 0) cv[r] = (double)__ldg(fc + (size_t)i * ncell + c);
+            if (i >= 0) cv[r] = (double)__ldcs(fc + (size_t)i * ncell + c);
           }
 #pragma unroll
           for (int r = 0; r < R; ++r) {
@@ -392,7 +394,7 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int64_t i = b0 + u * kStageThreads + threadIdx.x;
-        dv[u] = i < sentinel_n ? __ldg(diag + i) : T(0);
+        dv[u] = i < sentinel_n ? __ldcs(diag + i) : T(0);
         xv[u] = i < sentinel_n ? x[i] : T(0);
       }
 #pragma unroll
@@ -425,7 +427,7 @@ __global__ void __launch_bounds__(256) jacobi_sentinel(int64_t n, const T* __res
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t i = b0 + u * 256 + threadIdx.x;
-      dv[u] = i < n ? __ldg(diag + i) : T(0);
+      dv[u] = i < n ? __ldcs(diag + i) : T(0);
       xv[u] = i < n ? x[i] : T(0);
     }
 #pragma unroll

@@ -35,7 +35,8 @@ constexpr double EPS_RDEF = DBL_EPSILON;  // constants_mod.F90:167
 struct DevState {
   int done, converged, iter, status;
   int applies, monitor, max_iter, askip;  // askip: skip the rest of a GMRES cycle
-  int m, inner_mode, pad0, pad1;          // m: Krylov vectors used by the cycle
+  int m, inner_mode;                      // m: Krylov vectors used by the cycle
+  int x_zero, x_nonzero;                  // initial guess all zero / not (residual skip flags)
   double r_tol, a_tol;
   double r_nrm_0, r_nrm, rz, alpha, neg_alpha, beta;
   // bicgstab
@@ -115,6 +116,42 @@ int init_state(lfx_solver* s) {
 // CUDA graph cached per (x, b) pair, then reads the device state (wait) or
 // leaves the graph queued (!wait: the caller reads the state later and then
 // calls collect_timing).
+// flags[0] (nonzero = true) stays set and flags[1] stays clear while every
+// x[i] is zero; any nonzero entry clears the first and sets the second
+template <class T>
+__global__ void __launch_bounds__(256) zero_check(int64_t n, const T* __restrict__ x, int* flags) {
+  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
+    if (x[i] != T(0)) {
+      flags[0] = 0;
+      flags[1] = 1;
+    }
+}
+
+// r = b - A x, where a zero initial guess (checked on the device) skips the
+// apply and copies b: b - A 0 = b exactly, so the bits are those of the
+// apply; a nonzero x costs one extra read of x
+template <class T>
+int residual_from(lfx_solver* s, lfx_op* op, const T* x, T* r, const T* b, int* flags) {
+  lfx_ctx* ctx = s->ctx;
+  const int64_t n = s->n;
+  LFX_CK(ctx, cudaMemsetAsync(flags, 0x01, sizeof(int), ctx->stream));
+  LFX_CK(ctx, cudaMemsetAsync(flags + 1, 0, sizeof(int), ctx->stream));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 1023) / 1024, ctx->num_sms * 8));
+  zero_check<T><<<grid, 256, 0, ctx->stream>>>(n, x, flags);
+  ctx->launches++;
+  LFX_CK(ctx, cudaGetLastError());
+  // (not in the per-apply timings: it may idle)
+  const bool timed = ctx->time_applies;
+  ctx->time_applies = false;
+  int rc = op_apply_impl(op, x, r, b, flags);  // idles when x == 0
+  ctx->time_applies = timed;
+  if (rc) return rc;
+  return launch_chunks<0>(
+      ctx, n, [=] __device__(int64_t i) { return V1<T>{b[i]}; },
+      [=] __device__(int64_t i, const V1<T>& v, double*) { r[i] = v.a; }, NoFin{},
+      flags + 1);  // idles when x != 0
+}
+
 // adds the apply timings of the last launched graph (finished) to the context
 void collect_timing(lfx_solver* s) {
   lfx_ctx* ctx = s->ctx;
@@ -850,7 +887,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b, bool one_cycle = false) {
   // starts from x = 0, res = b exactly and the apply is skipped.
   const bool zero_x0 = s->zero_x0;
   s->zero_x0 = false;
-  if (!zero_x0 && (rc = op_apply_impl(s->op, x, res, b, nullptr))) return rc;
+  if (!zero_x0 && (rc = residual_from<T>(s, s->op, x, res, b, &S->x_zero))) return rc;
   const T* r0src = zero_x0 ? b : res;
   rc = launch_chunks<1>(
       ctx, n, [=] __device__(int64_t i) { return V1<T>{r0src[i]}; },
@@ -1172,7 +1209,15 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
   const bool fast = s->inner->kind == LFX_SOLVER_GMRES && s->inner->inner_mode &&
                     s->inner->precision == LFX_R32;
   double r0 = 0.0, rn = 0.0;
-  if ((rc = resid_norm(&r0))) return rc;
+  {
+    // the first residual skips its apply when x starts at zero
+    int q = residual_from<double>(s, s->op, x, r, b, &s->d_state->x_zero);
+    if (!q) q = norm_kernel(ctx, n, (const double*)r, sc, nullptr);
+    if (q) return q;
+    LFX_CK(ctx, cudaMemcpyAsync(ctx->h_scalars, sc, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    r0 = ctx->h_scalars[0];
+  }
   memset(info, 0, sizeof *info);
   info->initial_norm = r0;
   info->applies = 1;

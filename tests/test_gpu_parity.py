@@ -394,6 +394,23 @@ def test_gmres_w2_cma_parity(ctx, n, nl):
     assert same(X.export_field(), x_o)
 
 
+def test_gmres_nonzero_initial_guess(ctx):
+    """A nonzero initial guess takes the full residual apply (a zero one skips
+    it, since b - A 0 = b): both equal the oracle bit for bit."""
+    p = mg.w2_problem(12, 10, seed=7)
+    sysd = wl.device_w2(ctx, p)
+    op = o_lma(p)
+    oprec, _ = o_w2_prec(p, op)
+    x0 = 1e-3 * mg.normal(21, p.undf)
+    x_o, info_o = orc.solve("gmres", op, oprec, p.rhs, x0=x0, r_tol=1e-8, a_tol=1e-16,
+                            max_iter=200, gcrk=10)
+    g = lfx.GMRES(sysd.op, sysd.prec, 10, 1e-8, 1e-16, 200)
+    X, B = sysd.vector(x0), sysd.vector(p.rhs)
+    info = g.apply(X, B)
+    assert info.converged and info.iterations == info_o.iterations
+    assert same(X.export_field(), x_o)
+
+
 @pytest.mark.parametrize("kind", ["fgmres", "gcr"])
 @pytest.mark.parametrize("space", ["w0", "w2"])
 def test_flexible_solvers_parity(ctx, kind, space):

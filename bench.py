@@ -435,6 +435,23 @@ def cpu_baseline(problem, nsolves):
             "p50_ms": 1e3 * statistics.median(times)}
 
 
+def max_over_ranks(v, dist=None, device="cuda"):
+    """The largest v over the ranks of the process group (v itself when there
+    is no group): timings are the slowest rank's."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, steps, ms):
+    """Whole-job solves/s of `world` replicas that each ran `steps` solves in
+    `ms` milliseconds (the slowest rank's time)."""
+    return world * steps / (ms / 1e3)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -529,13 +546,6 @@ def main():
         return {"ms": t_all[0].elapsed_time(t_all[1]), "wall_ms": 1e3 * wall, "lat": lat,
                 "infos": infos, "launches": ctx.launch_count() - l0}
 
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # warm-up (also checks both paths reach the tolerance)
     for _ in range(max(args.warmup, 3)):
         X.set_scalar(0.0)
@@ -563,12 +573,12 @@ def main():
     host["rhs"][:] = p.rhs
     e = timed(mixed, K, e2e=True, host=host)
 
-    t_mx = max_over_ranks(mx["ms"])
-    t_64 = max_over_ranks(f["ms"])
-    t_e2e = max_over_ranks(e["ms"])
-    value = world * K / (t_mx / 1e3)
-    fp64_value = world * K / (t_64 / 1e3)
-    e2e_value = world * K / (t_e2e / 1e3)
+    t_mx = max_over_ranks(mx["ms"], dist)
+    t_64 = max_over_ranks(f["ms"], dist)
+    t_e2e = max_over_ranks(e["ms"], dist)
+    value = replica_throughput(world, K, t_mx)
+    fp64_value = replica_throughput(world, K, t_64)
+    e2e_value = replica_throughput(world, K, t_e2e)
 
     if rank != 0:
         if dist:

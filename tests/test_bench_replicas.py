@@ -1,0 +1,62 @@
+"""The multi-GPU bench path (replicas) with two gloo ranks on the CPU: the
+slowest rank's time sets the whole-job throughput, and the reference arm does
+its work on rank 0 only."""
+import os
+import socket
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import bench
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        ms = 100.0 + 50.0 * rank          # rank 1 is the slow one
+        t = bench.max_over_ranks(ms, dist, device="cpu")
+        dist.barrier()
+        q.put((rank, t, bench.replica_throughput(world, 20, t), bench.dist_env()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_take_the_slowest_time():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, t, value, env in out:
+        assert t == 150.0                       # max over ranks
+        assert value == pytest.approx(2 * 20 / 0.150)  # both replicas' solves
+        assert env == (rank, world, rank)
+
+
+def test_single_process_keeps_its_own_time():
+    assert bench.max_over_ranks(42.0) == 42.0
+    assert bench.replica_throughput(1, 10, 1000.0) == pytest.approx(10.0)
+
+
+def test_reference_arm_runs_on_rank0_only(monkeypatch):
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    import argparse
+    ns = argparse.Namespace(gpus=2, steps=2, warmup=1, impl="reference", cpu_sample=1,
+                            no_cpu=False, quick=True)
+    assert bench.run_reference(ns) == 0     # returns at once, no solve, no output

@@ -86,6 +86,16 @@ int lfx_vec_size(const lfx_vec* v, int32_t* nfields);
  * data of field `position` (1-based); converts to/from FP32 storage. */
 int lfx_vec_import_field(lfx_vec* v, int32_t position, const double* host, int64_t n);
 int lfx_vec_export_field(const lfx_vec* v, int32_t position, double* host, int64_t n);
+/* the same transfers for an FP64 field, queued on `stream` (a cudaStream_t;
+ * NULL = the context's stream) without waiting: with pinned host memory they
+ * overlap work on other streams (e.g. the next request's right-hand side
+ * arriving while a solve runs). The caller orders `stream` against the
+ * context's stream (lfx_ctx_stream, events) and keeps `host` alive until the
+ * copy is done. No counterpart in the reference (its fields live on the host). */
+int lfx_vec_import_field_async(lfx_vec* v, int32_t position, const double* host, int64_t n,
+                               void* stream);
+int lfx_vec_export_field_async(const lfx_vec* v, int32_t position, double* host, int64_t n,
+                               void* stream);
 /* raw device pointer of a field (for zero-copy callers); precision tells the type */
 int lfx_vec_field_device_ptr(const lfx_vec* v, int32_t position, void** out);
 

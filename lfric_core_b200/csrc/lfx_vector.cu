@@ -292,6 +292,41 @@ int lfx_vec_import_field(lfx_vec* v, int32_t position, const double* host, int64
   return rc;
 }
 
+// Asynchronous transfers of an FP64 field on a caller's stream (null: the
+// context's); with pinned host memory they overlap work on other streams.
+// The caller orders the stream against the context's stream.
+static int field_async(const lfx_vec* v, int32_t position, void* dst, const void* src, int64_t n,
+                       void* stream, cudaMemcpyKind kind) {
+  lfx_ctx* ctx = v->ctx;
+  if (position < 1 || position > (int32_t)v->data.size())
+    return fail(ctx, LFX_INVALID_ARGUMENT, "field position bigger than nfields");
+  if (!dst || !src || n != v->undf[position - 1])
+    return fail(ctx, LFX_INVALID_ARGUMENT, "field length mismatch");
+  if (v->precision != LFX_R64)
+    return fail(ctx, LFX_NOT_SUPPORTED, "asynchronous transfers take FP64 fields");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  LFX_CK(ctx, cudaMemcpyAsync(dst, src, n * 8, kind, s));
+  return LFX_OK;
+}
+
+int lfx_vec_import_field_async(lfx_vec* v, int32_t position, const double* host, int64_t n,
+                               void* stream) {
+  VEC_CHECK(v);
+  if (!host) return LFX_INVALID_ARGUMENT;
+  if (position < 1 || position > (int32_t)v->data.size())
+    return fail(v->ctx, LFX_INVALID_ARGUMENT, "field position bigger than nfields");
+  return field_async(v, position, v->data[position - 1], host, n, stream, cudaMemcpyHostToDevice);
+}
+
+int lfx_vec_export_field_async(const lfx_vec* v, int32_t position, double* host, int64_t n,
+                               void* stream) {
+  VEC_CHECK(v);
+  if (!host) return LFX_INVALID_ARGUMENT;
+  if (position < 1 || position > (int32_t)v->data.size())
+    return fail(v->ctx, LFX_INVALID_ARGUMENT, "field position bigger than nfields");
+  return field_async(v, position, host, v->data[position - 1], n, stream, cudaMemcpyDeviceToHost);
+}
+
 int lfx_vec_export_field(const lfx_vec* v, int32_t position, double* host, int64_t n) {
   VEC_CHECK(v);
   lfx_ctx* ctx = v->ctx;

@@ -96,6 +96,8 @@ _SIGS = [
     ("lfx_vec_size", [vp, C.POINTER(C.c_int32)], C.c_int),
     ("lfx_vec_import_field", [vp, C.c_int32, f64p, C.c_int64], C.c_int),
     ("lfx_vec_export_field", [vp, C.c_int32, f64p, C.c_int64], C.c_int),
+    ("lfx_vec_import_field_async", [vp, C.c_int32, vp, C.c_int64, vp], C.c_int),
+    ("lfx_vec_export_field_async", [vp, C.c_int32, vp, C.c_int64, vp], C.c_int),
     ("lfx_vec_field_device_ptr", [vp, C.c_int32, C.POINTER(vp)], C.c_int),
     ("lfx_lma_create", [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p, C.c_int64,
                         C.c_int64, f64p, C.c_int32, i32p, i32p, C.c_int32, C.c_int32,
@@ -350,6 +352,21 @@ class FieldVector(_Handle):
             out = np.empty(self.undf[position - 1], dtype=np.float64)
         self.ctx.check(self.ctx.L.lfx_vec_export_field(self.h, position, out, len(out)))
         return out
+
+    def import_field_async(self, host, stream: int = 0, position=1):
+        """Queue the copy of FP64 host data (a pinned, contiguous float64
+        array kept alive by the caller) into field `position` on `stream`
+        (a cudaStream_t handle; 0 = the context's stream); returns at once."""
+        assert host.dtype == np.float64 and host.flags["C_CONTIGUOUS"]
+        self.ctx.check(self.ctx.L.lfx_vec_import_field_async(
+            self.h, position, C.c_void_p(host.ctypes.data), len(host), C.c_void_p(stream)))
+
+    def export_field_async(self, host, stream: int = 0, position=1):
+        """Queue the copy of field `position` into FP64 host memory (pinned,
+        contiguous, kept alive by the caller) on `stream`; returns at once."""
+        assert host.dtype == np.float64 and host.flags["C_CONTIGUOUS"]
+        self.ctx.check(self.ctx.L.lfx_vec_export_field_async(
+            self.h, position, C.c_void_p(host.ctypes.data), len(host), C.c_void_p(stream)))
 
     def device_ptr(self, position=1) -> int:
         p = vp()

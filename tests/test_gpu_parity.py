@@ -77,6 +77,38 @@ def test_fp32_vector_semantics(ctx):
                                rtol=1e-6)
 
 
+def test_async_field_transfers(ctx):
+    """Asynchronous FP64 imports/exports on a caller stream (torch side
+    stream, ordered with events) give back exactly the data; FP32 fields are
+    refused."""
+    import torch
+    n = 100003
+    src = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    dst = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    src[:] = mg.normal(5, n)
+    v = lfx.FieldVector(ctx, [n])
+    cs = torch.cuda.Stream()
+    v.import_field_async(src, cs.cuda_stream)
+    done = torch.cuda.Event()
+    done.record(cs)
+    main = torch.cuda.ExternalStream(ctx.stream)
+    main.wait_event(done)
+    v.scale(2.0)                                   # on the context's stream
+    back = torch.cuda.Event()
+    back.record(main)
+    cs.wait_event(back)
+    v.export_field_async(dst, cs.cuda_stream)
+    cs.synchronize()
+    assert same(dst, 2.0 * src)
+    v.import_field_async(src)                      # the context's stream
+    v.export_field_async(dst)
+    ctx.synchronize()
+    assert same(dst, src)
+    w = lfx.FieldVector(ctx, [n], lfx.R32)
+    with pytest.raises(lfx.LfxError):
+        w.import_field_async(src)
+
+
 def test_multifield_vector(ctx):
     undf = [1000, 3001]
     rng = np.random.default_rng(4)

@@ -834,6 +834,11 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
     m[p] = v ? __ldcs(Mc + (SYM ? p * nl : (p / NDF) * C.blk + (p % NDF) * nl)) : T(0);
 #pragma unroll
   for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldg(x + mf[j] + lane) : T(0);
+  // the launch of colour k > 0 may start while colour k - 1 finishes
+  // (programmatic dependent launch): its matrix and x loads above overlap that
+  // tail, and it waits here, before touching y, until colour k - 1 has
+  // completed (a no-op for a launch without the dependency)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 #pragma unroll
   for (int df = 0; df < NDF; ++df) {
     const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
@@ -1539,9 +1544,20 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
       lma_cells_pipe<T, N, SYM, S, RESID><<<grid, 32 * kCellWarps, smem, ctx->stream>>>(
           C, M, (const T*)x, (T*)y, (const T*)b, sb, skip);
     } else {
-      const int grid = (int)(((int64_t)C.ncells * 32 + 255) / 256);
-      lma_cells<T, N, SYM, RESID><<<grid, 256, 0, ctx->stream>>>(C, M, (const T*)x, (T*)y, (const T*)b,
-                                                           skip);
+      // colours after the first launch as programmatic dependents of the
+      // previous colour (they wait in the kernel before reading y)
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(((int64_t)C.ncells * 32 + 255) / 256));
+      cfg.blockDim = dim3(256);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = ctx->stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = k > 0 ? 1 : 0;
+      cudaLaunchKernelEx(&cfg, lma_cells<T, N, SYM, RESID>, C, M, (const T*)x, (T*)y,
+                         (const T*)b, skip);
     }
     ctx->launches++;
   }

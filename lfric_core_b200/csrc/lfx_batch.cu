@@ -71,6 +71,10 @@ __device__ __forceinline__ bool ph_active(const BState& s) {
   return s.phase == PH_INIT || s.phase == PH_RUN;
 }
 
+// values of one batched chunk item: kBSub chunks of RCHUNK
+constexpr int kBSub = 4;
+inline int64_t bchunks(int64_t n) { return (n + (int64_t)kBSub * RCHUNK - 1) / ((int64_t)kBSub * RCHUNK); }
+
 // Batched chunk kernel: items are (slot, chunk); ld/op as in chunk_kernel but
 // with the slot's descriptor; fin(slot desc, state, tot) runs once per slot
 // after all its chunks. A non-null gate that reads zero skips the launch; a
@@ -94,21 +98,27 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
     // and scalars stay in registers
     const BSlot D = slots[w.x];
     const BState S = Sg;
-    const int64_t base = (int64_t)w.y * RCHUNK + threadIdx.x;
     using V = decltype(ld(D, int64_t(0)));
-    V v[RPER];
-#pragma unroll
-    for (int m = 0; m < RPER; ++m) {
-      const int64_t i = base + (int64_t)m * RT;
-      if (i < D.n) v[m] = ld(D, i);
-    }
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+    // an item is kBSub consecutive 2048-value chunks, taken in order, each
+    // with all its loads issued before its stores (one block reduction per
+    // item: the fixed cost of an item is spread over more values)
+    for (int sub = 0; sub < kBSub; ++sub) {
+      const int64_t base = ((int64_t)w.y * kBSub + sub) * RCHUNK + threadIdx.x;
+      if (base - threadIdx.x >= D.n) break;
+      V v[RPER];
 #pragma unroll
-    for (int m = 0; m < RPER; ++m) {
-      const int64_t i = base + (int64_t)m * RT;
-      if (i < D.n) op(D, S, i, v[m], acc);
+      for (int m = 0; m < RPER; ++m) {
+        const int64_t i = base + (int64_t)m * RT;
+        if (i < D.n) v[m] = ld(D, i);
+      }
+#pragma unroll
+      for (int m = 0; m < RPER; ++m) {
+        const int64_t i = base + (int64_t)m * RT;
+        if (i < D.n) op(D, S, i, v[m], acc);
+      }
     }
     if constexpr (NR > 0) {
 #pragma unroll
@@ -870,7 +880,7 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
     }
   if (s < 0) return fail(ctx, LFX_OUT_OF_MEMORY, "no free batch slot");
   const int64_t n = L->undf_to;
-  const int64_t nch = nchunks(n);
+  const int64_t nch = bchunks(n);
   const int64_t ncol = prec32->kind == PREC_CMA ? prec32->ncell_2d : 0;
   SlotHost& H = B->slots[s];
   H = SlotHost();

@@ -3,18 +3,19 @@
 // with SPD Jacobi / column-tridiagonal preconditioners).
 //
 // Algorithm per slot: preconditioned CG whose recurrences, operator apply and
-// preconditioner run in FP32, with the solution accumulated in FP64 and
-// reliable updates: when the FP32 recursive residual has fallen by a factor
-// delta since the last true residual (or reaches the tolerance), the true
-// residual b - A x is recomputed with the FP64 operator and replaces it. A
-// slot converges only on that FP64 true residual, ||b - A x|| / ||b - A x0||.
+// preconditioner run in FP32, with reliable updates: the steps accumulate in
+// an FP32 correction; when the FP32 recursive residual has fallen by a factor
+// delta since the last true residual (or reaches the tolerance), the
+// correction is added to the FP64 solution and the true residual b - A x is
+// recomputed with the FP64 operator and replaces it. A slot converges only on
+// that FP64 true residual, ||b - A x|| / ||b - A x0||.
 //
-// Batching: every kernel covers all slots -- entity columns, 2048-element
+// Batching: every kernel covers all slots -- entity columns, 8192-element
 // chunks and CMA columns come from device work lists of (slot, item) pairs --
 // and reads per-slot pointers and state from device tables, so one CUDA graph
 // of `iters` super-iterations serves any set of admitted slots. Slots whose
-// phase does not call for a kernel skip its items. Per-slot reductions keep
-// the fixed chunk order of lfx_internal.cuh, with a completion ticket per
+// phase does not call for a kernel skip its items. Per-slot reductions sum in
+// a fixed order (lanes, then warps, then chunks), with a completion ticket per
 // slot, so a slot's result is bit-identical whatever else is in the batch.
 // Vectors and list regions come from pools sized at creation: admitting a
 // request allocates nothing, and is refused when the pools are full.

@@ -139,7 +139,10 @@ int lfx_op_destroy(lfx_op* op);
  * apply. */
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
                     float* us);
-/* time one configuration (as above) without keeping it */
+/* time one configuration (as above) without keeping it. Both time on
+ * scratch vectors allocated for the call: consecutive applies take different
+ * x and y (pairs enough to hold twice the L2), so the vectors travel to and
+ * from HBM on every apply, as the local matrices do. */
 int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps, int32_t reps,
                       float* us);
 /* keep one configuration (as above) for later applies, as the autotuner

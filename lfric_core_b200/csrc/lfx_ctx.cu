@@ -111,6 +111,7 @@ int lfx_ctx_create(int device, lfx_ctx** out) {
   lfx_ctx* ctx = new lfx_ctx();
   ctx->device = device;
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&ctx->l2_bytes, cudaDevAttrL2CacheSize, device);
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete ctx;
     return LFX_CUDA_ERROR;

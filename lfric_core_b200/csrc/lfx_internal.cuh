@@ -27,6 +27,7 @@ struct TimedPair {
 struct lfx_ctx {
   int device = 0;
   int num_sms = 148;
+  int l2_bytes = 126 << 20;  // the device's L2 size (queried at creation)
   cudaStream_t stream = nullptr;
   std::string err;
   // reduction scratch: partials of up to 4 simultaneous sums, one ticket

@@ -1864,17 +1864,28 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
     ts.stages = stages;
   }
   const size_t esz = op->precision == LFX_R64 ? 8 : 4;
-  void *x = nullptr, *y = nullptr;
-  int rc = dmalloc(ctx, &x, L->undf_from * esz);
-  if (!rc) rc = dmalloc(ctx, &y, L->undf_to * esz);
+  // consecutive applies take different x and y (enough pairs to hold twice
+  // the L2), so each apply reads x from and writes y to HBM as in a solve
+  // whose vectors change, rather than finding them in L2
+  const size_t pair = (L->undf_from + L->undf_to) * esz;
+  const size_t l2 = (size_t)std::max(ctx->l2_bytes, 1);
+  const int npair = (int)std::min<size_t>(8, std::max<size_t>(2, (2 * l2 + pair - 1) / pair));
+  void* x[8] = {};
+  void* y[8] = {};
+  int rc = LFX_OK;
+  for (int i = 0; i < npair && !rc; ++i) {
+    rc = dmalloc(ctx, &x[i], L->undf_from * esz);
+    if (!rc) rc = dmalloc(ctx, &y[i], L->undf_to * esz);
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (!rc) {
-    cudaMemsetAsync(x, 0, L->undf_from * esz, ctx->stream);
+    for (int i = 0; i < npair; ++i) cudaMemsetAsync(x[i], 0, L->undf_from * esz, ctx->stream);
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    launch_apply(ctx, op, kernel, ts, x, y, nullptr, nullptr);  // warm
+    launch_apply(ctx, op, kernel, ts, x[0], y[0], nullptr, nullptr);  // warm
     cudaEventRecord(e0, ctx->stream);
-    for (int r = 0; r < reps; ++r) launch_apply(ctx, op, kernel, ts, x, y, nullptr, nullptr);
+    for (int r = 0; r < reps; ++r)
+      launch_apply(ctx, op, kernel, ts, x[(r + 1) % npair], y[(r + 1) % npair], nullptr, nullptr);
     cudaEventRecord(e1, ctx->stream);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
       rc = fail(ctx, LFX_CUDA_ERROR, "apply timing failed");
@@ -1884,8 +1895,10 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
-  dfree(ctx, x, L->undf_from * esz);
-  dfree(ctx, y, L->undf_to * esz);
+  for (int i = 0; i < npair; ++i) {
+    if (x[i]) dfree(ctx, x[i], L->undf_from * esz);
+    if (y[i]) dfree(ctx, y[i], L->undf_to * esz);
+  }
   if (!rc) rc = lfx_ctx_check_device_error(ctx);
   return rc;
 }

@@ -53,6 +53,7 @@ struct GraphEntry {
   const void* x = nullptr;
   const void* b = nullptr;
   bool timed = false;
+  int variant = 0;  // bodies that differ for the same vectors (one-cycle runs)
   cudaGraphExec_t exec = nullptr;
   std::vector<TimedPair> ev;  // apply-timing events recorded by the graph
   int64_t kernels = 0;
@@ -170,13 +171,14 @@ void collect_timing(lfx_solver* s) {
 }
 
 int run_graph(lfx_solver* s, const void* x, const void* b, const std::function<int()>& body,
-              bool wait = true) {
+              bool wait = true, int variant = 0) {
   lfx_ctx* ctx = s->ctx;
   GraphEntry* ge = nullptr;
   for (auto& g : s->graphs)
-    if (g.x == x && g.b == b && g.timed == ctx->time_applies) ge = &g;
+    if (g.x == x && g.b == b && g.timed == ctx->time_applies && g.variant == variant) ge = &g;
   if (!ge) {
     GraphEntry g;
+    g.variant = variant;
     g.x = x;
     g.b = b;
     g.timed = ctx->time_applies;
@@ -815,7 +817,8 @@ __global__ void __launch_bounds__(256) gmres_xupdate(int64_t n, VecPtrs vp, cons
 }
 
 // sig (nullable): scales of an unnormalised basis, folded into u
-__global__ void gmres_finish_cycle(DevState* S, double* gm, int K, const double* sig) {
+__global__ void gmres_finish_cycle(DevState* S, double* gm, int K, const double* sig,
+                                   int count_cycle) {
   if (S->done) return;
   double* h = gm;                  // H(i,j) at (i-1) + (K+1)(j-1)
   double* g = gm + 2 * (K + 1) * K;
@@ -848,12 +851,14 @@ __global__ void gmres_finish_cycle(DevState* S, double* gm, int K, const double*
   if (sig)
     for (int iv = 0; iv < m; ++iv) u[iv] = u[iv] * sig[iv];
   S->m = m;
+  if (count_cycle) S->iter += 1;  // the cycle ends without its own residual
 #undef H
 }
 
-// one_cycle: queue the initial residual and exactly one restart cycle and
-// return without waiting (the refinement reads the state after its own
-// residual, in the same synchronisation)
+// one_cycle: queue the initial residual and exactly one restart cycle, without
+// the cycle's closing residual, and return without waiting (the refinement
+// reads the state after its own residual, in the same synchronisation; a NaN
+// in the cycle reaches that FP64 residual through the solution update)
 template <class T>
 int gmres_run(lfx_solver* s, T* x, const T* b, bool one_cycle = false) {
   lfx_ctx* ctx = s->ctx;
@@ -1049,7 +1054,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b, bool one_cycle = false) {
         if (q) return q;
       }
     }
-    gmres_finish_cycle<<<1, 1, 0, ctx->stream>>>(S, h, K, lazy ? sig : nullptr);
+    gmres_finish_cycle<<<1, 1, 0, ctx->stream>>>(S, h, K, lazy ? sig : nullptr, one_cycle);
     ctx->launches++;
     LFX_CK(ctx, cudaGetLastError());
     // x += sum_iv u(iv) v_iv over the m vectors of the cycle, one pass, the
@@ -1074,6 +1079,9 @@ int gmres_run(lfx_solver* s, T* x, const T* b, bool one_cycle = false) {
         NoFin{}, done);
     if (q) return q;
     }
+    // a single queued cycle is followed at once by the caller's own (FP64)
+    // residual, the only one it reads: this cycle's residual is not formed
+    if (one_cycle) return LFX_OK;
     if ((q = op_apply_impl(s->op, x, res, b, done))) return q;  // res = b - A x
     q = launch_chunks<1>(
         ctx, n, [=] __device__(int64_t i) { return V1<T>{res[i]}; },
@@ -1099,7 +1107,7 @@ int gmres_run(lfx_solver* s, T* x, const T* b, bool one_cycle = false) {
         done);
     return q;
   };
-  if (one_cycle) return run_graph(s, x, b, cycle, false);
+  if (one_cycle) return run_graph(s, x, b, cycle, false, 1);
   // no host round trip before the first graph: its kernels idle if the
   // initial residual already ended the solve (device flags)
   do {

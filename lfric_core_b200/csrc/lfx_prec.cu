@@ -235,20 +235,38 @@ __global__ void __launch_bounds__(128) cma_prec_apply(
 // shared memory. The block's x rows are copied in by one warp per column
 // (a column's rows are contiguous dofs, so the copies coalesce) and, with SF,
 // its factor rows too ([row][column] in memory: one coalesced run of
-// kStageCols per row), all issued before the first sweep; each of the first
-// kStageCols threads then runs its column's recurrences on the staged copy
-// and the result is copied out the same way. Row i of column j sits at
-// [i * (kStageCols + 1) + j], conflict-free for the row-wise copies and the
-// column-wise sweeps. Same arithmetic as thomas_sweep, so the same bits.
-// Factors, read once per application, come through streaming (evict-first)
-// loads so that x and y stay in L2.
+// kStageCols per row), all by asynchronous copies issued before any is waited
+// for; each of the first kStageCols threads then runs its column's
+// recurrences on the staged copy and the result is copied out the same way.
+// Row i of column j sits at [i * (kStageCols + 1) + j], conflict-free for the
+// row-wise copies and the column-wise sweeps. Same arithmetic as
+// thomas_sweep, so the same bits. Factors, read once per application, carry
+// an evict-first L2 policy so that x and y stay in L2.
 //
-// Rows the columns do not cover get y = x / diag: elementwise, in the same
-// launch for small stages or in a launch of their own, where the diagonal
-// carries zeros on the column rows (zero_sentinel), else by runs of rows in
+// Rows the columns do not cover get y = x / diag: where the diagonal carries
+// zeros on the column rows (zero_sentinel), elementwise in a launch of its
+// own that runs beside the sweeps (jacobi_sentinel), else by runs of rows in
 // the blocks after the Thomas blocks.
 constexpr int kStageCols = 64;
 constexpr int kStageThreads = 128;
+
+// asynchronous global -> shared copy of one element (the thread holds no
+// register for it while it is in flight); the factor copies carry an L2
+// evict-first policy, as they are read once per application
+__device__ __forceinline__ uint32_t stage_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+template <int B>
+__device__ __forceinline__ void stage_copy(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(stage_addr(dst)), "l"(src), "n"(B)
+               : "memory");
+}
+template <int B>
+__device__ __forceinline__ void stage_copy_once(void* dst, const void* src, uint64_t pol) {
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], %2, %3;" ::"r"(stage_addr(dst)),
+               "l"(src), "n"(B), "l"(pol)
+               : "memory");
+}
 
 template <class T, bool SF>
 __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
@@ -256,7 +274,10 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
     const T* __restrict__ fa, const T* __restrict__ finv, const T* __restrict__ fc,
     const T* __restrict__ x, T* __restrict__ y, int thomas_blocks, int nruns,
     const int* __restrict__ run_start, const int* __restrict__ run_len, const T* __restrict__ diag,
-    int64_t sentinel_n, const int* skip) {
+    const int* skip) {
+  // a programmatic dependent launch after this one (the Jacobi rows) may
+  // start at once and run beside the sweeps
+  asm volatile("griddepcontrol.launch_dependents;");
   if (skip && *((volatile const int*)skip)) return;
   constexpr int LD = kStageCols + 1;
   constexpr int NW = kStageThreads / 32;
@@ -272,50 +293,37 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
     const int nc = min(kStageCols, ncell - c0);
     if (threadIdx.x < nc) fs[threadIdx.x] = __ldg(first + c0 + threadIdx.x);
     __syncthreads();
-    // lane l copies row r0 + l of the warp's columns warp, warp + NW, ...:
-    // the loads of all of them are issued before their shared-memory stores
+    // every staging copy of the block is in flight before any is waited for:
+    // lane l copies row r0 + l of the warp's columns warp, warp + NW, ...
+    // (one contiguous run of rows per column), and with SF thread t copies
+    // column t % kStageCols of the factor rows t / kStageCols + RS m (one
+    // contiguous run of kStageCols per row)
     constexpr int CPW = kStageCols / NW;
     for (int r0 = 0; r0 < nrow; r0 += 32) {
       const int i = r0 + lane;
-      const bool act = i < nrow;
-      const int il = act ? __ldg(ind + i) : 0;
-      T v[CPW];
+      if (i < nrow) {
+        const int il = __ldg(ind + i);
 #pragma unroll
-      for (int k = 0; k < CPW; ++k) {
-        const int j = warp + NW * k;
-        v[k] = (act && j < nc) ? x[fs[j] + il] : T(0);
+        for (int k = 0; k < CPW; ++k) {
+          const int j = warp + NW * k;
+          if (j < nc) stage_copy<sizeof(T)>(&xs[i * LD + j], x + fs[j] + il);
+        }
       }
-#pragma unroll
-      for (int k = 0; k < CPW; ++k)
-        if (act) xs[i * LD + warp + NW * k] = v[k];
     }
     if (SF) {
-      // thread t copies column t % kStageCols of rows t / kStageCols + 2 m
+      uint64_t pol;
+      asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
       const int j = threadIdx.x % kStageCols, i0 = threadIdx.x / kStageCols;
       constexpr int RS = kStageThreads / kStageCols;
-      constexpr int U = 8;
-      for (int ib = i0; ib < nrow; ib += RS * U) {
-        T va[U], vi[U], vc[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int i = ib + RS * u;
-          const bool ok = i < nrow && j < nc;
+      if (j < nc)
+        for (int i = i0; i < nrow; i += RS) {
           const size_t g = (size_t)i * ncell + c0 + j;
-          va[u] = ok ? __ldcs(fa + g) : T(0);
-          vi[u] = ok ? __ldcs(finv + g) : T(0);
-          vc[u] = ok ? __ldcs(fc + g) : T(0);
+          stage_copy_once<sizeof(T)>(&as[i * LD + j], fa + g, pol);
+          stage_copy_once<sizeof(T)>(&is[i * LD + j], finv + g, pol);
+          stage_copy_once<sizeof(T)>(&cs[i * LD + j], fc + g, pol);
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int i = ib + RS * u;
-          if (i < nrow) {
-            as[i * LD + j] = va[u];
-            is[i * LD + j] = vi[u];
-            cs[i * LD + j] = vc[u];
-          }
-        }
-      }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     const int j = threadIdx.x;
     if (j < nc) {
@@ -384,25 +392,6 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
         }
       }
     }
-  } else if (sentinel_n > 0) {
-    // the other rows, elementwise: eight per thread per pass, loads first
-    constexpr int U = 8;
-    const int64_t nb = gridDim.x - thomas_blocks;
-    for (int64_t b0 = (int64_t)(blockIdx.x - thomas_blocks) * U * kStageThreads; b0 < sentinel_n;
-         b0 += nb * U * kStageThreads) {
-      T dv[U], xv[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int64_t i = b0 + u * kStageThreads + threadIdx.x;
-        dv[u] = i < sentinel_n ? __ldcs(diag + i) : T(0);
-        xv[u] = i < sentinel_n ? x[i] : T(0);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int64_t i = b0 + u * kStageThreads + threadIdx.x;
-        if (dv[u] != T(0)) y[i] = xv[u] / dv[u];
-      }
-    }
   } else {
     const int64_t w = ((int64_t)(blockIdx.x - thomas_blocks) * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)(gridDim.x - thomas_blocks) * blockDim.x) >> 5;
@@ -414,13 +403,18 @@ __global__ void __launch_bounds__(kStageThreads) cma_prec_staged(
 }
 
 // y = x / diag on the rows whose diagonal is not zero (the diagonal carries
-// zeros on the column rows): eight rows per thread per pass, loads first
+// zeros on the column rows): eight rows per thread per pass, loads first.
+// Launched as a programmatic dependent of the column sweeps (it shares no
+// row of y with them), it waits for them only before it completes.
 template <class T>
 __global__ void __launch_bounds__(256) jacobi_sentinel(int64_t n, const T* __restrict__ x,
                                                        T* __restrict__ y,
                                                        const T* __restrict__ diag,
                                                        const int* skip) {
-  if (skip && *((volatile const int*)skip)) return;
+  if (skip && *((volatile const int*)skip)) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    return;
+  }
   constexpr int U = 8;
   for (int64_t b0 = (int64_t)blockIdx.x * U * 256; b0 < n; b0 += (int64_t)gridDim.x * U * 256) {
     T dv[U], xv[U];
@@ -436,6 +430,9 @@ __global__ void __launch_bounds__(256) jacobi_sentinel(int64_t n, const T* __res
       if (dv[u] != T(0)) y[i] = xv[u] / dv[u];
     }
   }
+  // launched beside the column sweeps: this grid completes only after them,
+  // so work queued after it sees both
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // shared memory of the staged sweeps (0: the column does not fit)
@@ -446,9 +443,9 @@ size_t staged_smem(int nrow, size_t esz, bool sf) {
 }
 // factors are staged while the block's shared memory stays at most this
 constexpr size_t kStageFactorsMax = 100 * 1024;
-// the elementwise Jacobi rows join the Thomas launch up to this much shared
-// memory per block
-constexpr size_t kFuseSmemMax = 40 * 1024;
+// resident blocks per SM given to the elementwise Jacobi rows beside the
+// column sweeps (each loops over its share of the rows)
+constexpr int kJacobiBlocksPerSm = 4;
 
 template <class T, bool SF>
 void launch_staged(lfx_ctx* ctx, const lfx_prec* p, const T* x, T* y, size_t smem,
@@ -460,29 +457,35 @@ void launch_staged(lfx_ctx* ctx, const lfx_prec* p, const T* x, T* y, size_t sme
     attr = true;
   }
   const int tb = (p->ncell_2d + kStageCols - 1) / kStageCols;
-  int jb = 0;
-  int64_t sentinel_n = 0;
   if (p->rdiag && p->zero_sentinel) {
-    if (smem <= kFuseSmemMax) {
-      // small stages: the elementwise rows share the launch (their blocks
-      // still fit several per SM beside the Thomas blocks)
-      sentinel_n = p->rdiag_n;
-      jb = (int)std::max<int64_t>(
-          1, std::min<int64_t>((p->rdiag_n + 8 * kStageThreads - 1) / (8 * kStageThreads),
-                               (int64_t)ctx->num_sms * 16));
-    } else {
-      const int g = (int)std::max<int64_t>(
-          1, std::min<int64_t>((p->rdiag_n + 8 * 256 - 1) / (8 * 256), (int64_t)ctx->num_sms * 8));
-      jacobi_sentinel<T><<<g, 256, 0, ctx->stream>>>(p->rdiag_n, x, y, (const T*)p->rdiag, skip);
-      ctx->launches++;
-    }
-  } else if (p->nruns) {
-    jb = (int)std::min<int64_t>(((int64_t)p->nruns + 3) / 4, (int64_t)ctx->num_sms * 8);
+    // the column sweeps, then the Jacobi rows as a programmatic dependent
+    // launch: its blocks start as soon as every sweep block has started and
+    // fill the SMs beside them (the two write disjoint rows of y)
+    cma_prec_staged<T, SF><<<tb, kStageThreads, smem, ctx->stream>>>(
+        p->ncell_2d, p->nrow, p->first_dof, p->indirection, (const T*)p->fa, (const T*)p->finv,
+        (const T*)p->fc, x, y, tb, 0, nullptr, nullptr, nullptr, skip);
+    const int g = (int)std::max<int64_t>(
+        1, std::min<int64_t>((p->rdiag_n + 8 * 256 - 1) / (8 * 256),
+                             (int64_t)ctx->num_sms * kJacobiBlocksPerSm));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3((unsigned)g);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, jacobi_sentinel<T>, p->rdiag_n, x, y, (const T*)p->rdiag, skip);
+    ctx->launches++;
+    return;
   }
+  const int jb =
+      p->nruns ? (int)std::min<int64_t>(((int64_t)p->nruns + 3) / 4, (int64_t)ctx->num_sms * 8) : 0;
   cma_prec_staged<T, SF><<<tb + jb, kStageThreads, smem, ctx->stream>>>(
       p->ncell_2d, p->nrow, p->first_dof, p->indirection, (const T*)p->fa, (const T*)p->finv,
-      (const T*)p->fc, x, y, tb, p->nruns, p->run_start, p->run_len, (const T*)p->rdiag,
-      sentinel_n, skip);
+      (const T*)p->fc, x, y, tb, p->nruns, p->run_start, p->run_len, (const T*)p->rdiag, skip);
 }
 
 template <class T>

@@ -225,6 +225,33 @@ def _run_batch_w2(args):
           flush=True)
 
 
+def _run_prec(args):
+    """Column preconditioner applies of the C96x30 W2 system (FP32 or FP64),
+    consecutive applies on different vectors (four pairs, past L2), timed by
+    CUDA events on the library's stream after one warm-up apply."""
+    import torch
+    p = mg.w2_problem(args.n, args.nl, seed=2)
+    ctx = lfx.Context(0)
+    prec_bits = lfx.R32 if args.precision == 32 else lfx.R64
+    s64 = device_w2(ctx, p, lfx.R64)
+    sysd = s64 if prec_bits == lfx.R64 else device_w2(ctx, p, lfx.R32, op64=s64.op64,
+                                                      cma=s64.cma, diag64=s64.diag)
+    xs = [lfx.FieldVector.from_array(ctx, mg.normal(3 + i, p.undf), prec_bits) for i in range(4)]
+    ys = [lfx.FieldVector(ctx, [p.undf], prec_bits) for _ in range(4)]
+    sysd.prec.apply(xs[0], ys[0])
+    ctx.synchronize()
+    st = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for r in range(args.reps):
+        sysd.prec.apply(xs[(r + 1) % 4], ys[(r + 1) % 4])
+    e1.record(st)
+    ctx.synchronize()
+    ctx.check_device_error()
+    print(f"fp{args.precision} column preconditioner: {1e3 * e0.elapsed_time(e1) / args.reps:.2f} us "
+          f"per apply ({args.reps} applies)", flush=True)
+
+
 def _run_solve_w2(args):
     """The C96x30 W2 Helmholtz solves of the headline benchmark (set-up,
     autotuning and warm-up first); the solves themselves run inside an NVTX
@@ -266,7 +293,7 @@ def _run_solve_w2(args):
 
 def main(argv=None):
     """One named workload, run once, for profilers:
-    ``python -m lfric_core_b200.workloads apply|time-apply|mrhs|batch-w2|solve-w2 [options]``."""
+    ``python -m lfric_core_b200.workloads apply|time-apply|prec|mrhs|batch-w2|solve-w2 [options]``."""
     import argparse
     ap = argparse.ArgumentParser(prog="python -m lfric_core_b200.workloads")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -296,6 +323,11 @@ def main(argv=None):
     b.add_argument("--n", type=int, default=94)
     b.add_argument("--nl", type=int, default=64)
     b.add_argument("--seed", type=int, default=505)
+    q = sub.add_parser("prec", help="column preconditioner applies of the W2 system")
+    q.add_argument("--n", type=int, default=96)
+    q.add_argument("--nl", type=int, default=30)
+    q.add_argument("--precision", type=int, choices=[32, 64], default=32)
+    q.add_argument("--reps", type=int, default=50)
     w = sub.add_parser("solve-w2", help="headline W2 solves (mixed and/or FP64) after set-up")
     w.add_argument("--n", type=int, default=96)
     w.add_argument("--nl", type=int, default=30)
@@ -306,7 +338,7 @@ def main(argv=None):
                    help="pinned apply kernel:stages for FP32,FP64 (default: autotune)")
     args = ap.parse_args(argv)
     {"apply": _run_apply, "time-apply": _run_time_apply, "mrhs": _run_mrhs,
-     "batch-w2": _run_batch_w2, "solve-w2": _run_solve_w2}[args.cmd](args)
+     "batch-w2": _run_batch_w2, "solve-w2": _run_solve_w2, "prec": _run_prec}[args.cmd](args)
     return 0
 
 

@@ -82,6 +82,35 @@ void timing_begin(lfx_ctx* ctx, int32_t precision) {
   cudaEventRecord(ctx->ev_pool[ctx->ev_used++], ctx->stream);
 }
 
+__global__ void small_copy(const unsigned* __restrict__ src, unsigned* dst, int words) {
+  for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+}
+
+int host_alloc_mapped(lfx_ctx* ctx, void** host, void** dev, size_t bytes) {
+  *host = *dev = nullptr;
+  if (cudaHostAlloc(host, bytes, cudaHostAllocMapped) != cudaSuccess) {
+    cudaGetLastError();
+    *host = nullptr;
+    return fail(ctx, LFX_OUT_OF_MEMORY, "pinned host allocation failed");
+  }
+  if (cudaHostGetDevicePointer(dev, *host, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeHost(*host);
+    *host = nullptr;
+    return fail(ctx, LFX_CUDA_ERROR, "pinned host memory is not mapped into the device");
+  }
+  return LFX_OK;
+}
+
+// bytes: a multiple of 4, both addresses 4-byte aligned
+int to_host_small(lfx_ctx* ctx, void* host_dev, const void* dev, size_t bytes) {
+  small_copy<<<1, 64, 0, ctx->stream>>>((const unsigned*)dev, (unsigned*)host_dev,
+                                        (int)(bytes / 4));
+  ctx->launches++;
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
 void timing_end(lfx_ctx* ctx) {
   if (!ctx->time_applies) return;
   if (ctx->capture_ev) {
@@ -121,8 +150,9 @@ int lfx_ctx_create(int device, lfx_ctx** out) {
   if (!rc) rc = dmalloc(ctx, (void**)&ctx->d_err, sizeof(int) * 4);
   if (!rc && cudaMemset(ctx->d_ticket, 0, sizeof(unsigned) * 4) != cudaSuccess) rc = LFX_CUDA_ERROR;
   if (!rc && cudaMemset(ctx->d_err, 0, sizeof(int) * 4) != cudaSuccess) rc = LFX_CUDA_ERROR;
-  if (!rc && cudaMallocHost((void**)&ctx->h_scalars, sizeof(double) * 64) != cudaSuccess)
-    rc = LFX_OUT_OF_MEMORY;
+  if (!rc)
+    rc = host_alloc_mapped(ctx, (void**)&ctx->h_scalars, (void**)&ctx->h_scalars_dev,
+                           sizeof(double) * 64);
   if (!rc) rc = ensure_partials(ctx, (int64_t)RCHUNK * 4096, 1);
   if (rc) {
     lfx_ctx_destroy(ctx);

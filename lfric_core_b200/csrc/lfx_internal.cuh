@@ -36,7 +36,8 @@ struct lfx_ctx {
   unsigned* d_ticket = nullptr;
   // small device scratch for scalar results of the C-ABI reductions
   double* d_scalars = nullptr;
-  double* h_scalars = nullptr;  // pinned
+  double* h_scalars = nullptr;      // pinned, mapped into the device's address space
+  double* h_scalars_dev = nullptr;  // its device address
   int64_t device_bytes = 0;
   // operator-apply timing: event pairs, the precision of each timed apply,
   // and running totals per precision (index 0: FP64, 1: FP32)
@@ -403,6 +404,11 @@ int chebyshev_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg, double
                    lfx_solve_info* info);
 int prec_apply_impl(lfx_prec* p, int32_t precision, const void* x, void* y, int64_t n,
                     const int* skip);
+// Small device -> host results go through pinned, device-mapped host memory
+// written by a one-block kernel, not a copy engine: they never queue behind
+// large field copies that other streams have in flight.
+int host_alloc_mapped(lfx_ctx* ctx, void** host, void** dev, size_t bytes);
+int to_host_small(lfx_ctx* ctx, void* host_dev, const void* dev, size_t bytes);
 void timing_begin(lfx_ctx* ctx, int32_t precision);
 void timing_end(lfx_ctx* ctx);
 }  // namespace lfx

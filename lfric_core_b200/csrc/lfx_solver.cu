@@ -71,7 +71,8 @@ struct lfx_solver {
   int64_t n = 0;
   std::vector<void*> work;  // owned device vectors of n elements
   DevState* d_state = nullptr;
-  DevState* h_state = nullptr;  // pinned
+  DevState* h_state = nullptr;      // pinned, mapped into the device's address space
+  DevState* h_state_dev = nullptr;  // its device address
   double* d_gm = nullptr;       // gmres: H, negH, g, u, cs, sn, basis scales
   bool inner_mode = false;      // GMRES used as the inner solve of a refinement
   bool zero_x0 = false;         // the next apply starts from x = 0 (set by the refinement)
@@ -93,11 +94,14 @@ size_t gm_doubles(int K) { return 2 * (size_t)(K + 1) * K + 2 * (size_t)(K + 1) 
 
 int read_state(lfx_solver* s) {
   lfx_ctx* ctx = s->ctx;
-  LFX_CK(ctx, cudaMemcpyAsync(s->h_state, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
-                              ctx->stream));
+  int rc = to_host_small(ctx, s->h_state_dev, s->d_state, sizeof(DevState));
+  if (rc) return rc;
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
   return LFX_OK;
 }
+
+// the initial state travels as a kernel argument (no copy engine involved)
+__global__ void put_state(DevState* d, DevState h) { *d = h; }
 
 int init_state(lfx_solver* s) {
   DevState h{};
@@ -108,8 +112,9 @@ int init_state(lfx_solver* s) {
   h.inner_mode = s->inner_mode ? 1 : 0;
   h.m = s->cfg.gcrk;
   *s->h_state = h;
-  LFX_CK(s->ctx, cudaMemcpyAsync(s->d_state, s->h_state, sizeof(DevState), cudaMemcpyHostToDevice,
-                                 s->ctx->stream));
+  put_state<<<1, 1, 0, s->ctx->stream>>>(s->d_state, h);
+  s->ctx->launches++;
+  LFX_CK(s->ctx, cudaGetLastError());
   return LFX_OK;
 }
 
@@ -1179,8 +1184,8 @@ int alloc_common(lfx_solver* s, int nwork) {
   lfx_ctx* ctx = s->ctx;
   int rc = dmalloc(ctx, (void**)&s->d_state, sizeof(DevState));
   if (rc) return rc;
-  if (cudaMallocHost((void**)&s->h_state, sizeof(DevState)) != cudaSuccess)
-    return fail(ctx, LFX_OUT_OF_MEMORY, "pinned allocation failed");
+  rc = host_alloc_mapped(ctx, (void**)&s->h_state, (void**)&s->h_state_dev, sizeof(DevState));
+  if (rc) return rc;
   for (int k = 0; k < nwork; ++k) {
     void* p = nullptr;
     rc = dmalloc(ctx, &p, s->n * esz(s->precision));
@@ -1206,8 +1211,8 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
     int q = op_apply_impl(s->op, x, r, b, nullptr);
     if (q) return q;
     q = norm_kernel(ctx, n, (const double*)r, sc, nullptr);
+    if (!q) q = to_host_small(ctx, ctx->h_scalars_dev, sc, 8);
     if (q) return q;
-    LFX_CK(ctx, cudaMemcpyAsync(ctx->h_scalars, sc, 8, cudaMemcpyDeviceToHost, ctx->stream));
     LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
     *out = ctx->h_scalars[0];
     return LFX_OK;
@@ -1221,8 +1226,8 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
     // the first residual skips its apply when x starts at zero
     int q = residual_from<double>(s, s->op, x, r, b, &s->d_state->x_zero);
     if (!q) q = norm_kernel(ctx, n, (const double*)r, sc, nullptr);
+    if (!q) q = to_host_small(ctx, ctx->h_scalars_dev, sc, 8);
     if (q) return q;
-    LFX_CK(ctx, cudaMemcpyAsync(ctx->h_scalars, sc, 8, cudaMemcpyDeviceToHost, ctx->stream));
     LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
     r0 = ctx->h_scalars[0];
   }
@@ -1254,8 +1259,7 @@ int refined_run(lfx_solver* s, lfx_vec* xv, const lfx_vec* bv, lfx_solve_info* i
       if ((rc = init_state(in))) return rc;
       in->zero_x0 = true;  // d32 was just zeroed
       if ((rc = gmres_run<float>(in, d32, r32, true))) return rc;
-      LFX_CK(ctx, cudaMemcpyAsync(in->h_state, in->d_state, sizeof(DevState),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
+      if ((rc = to_host_small(ctx, in->h_state_dev, in->d_state, sizeof(DevState)))) return rc;
     } else {
       in->zero_x0 = in->kind == LFX_SOLVER_GMRES;  // d32 was just zeroed
       rc = lfx_solver_apply(in, s->d32, s->r32, &ii);
@@ -1367,8 +1371,8 @@ int lfx_refined_solver_create(lfx_ctx* ctx, lfx_op* op64, lfx_solver* inner, dou
   if (!rc) rc = lfx_vec_create(ctx, 1, &n, LFX_R32, &s->r32);
   if (!rc) rc = lfx_vec_create(ctx, 1, &n, LFX_R32, &s->d32);
   if (!rc) rc = dmalloc(ctx, (void**)&s->d_state, sizeof(DevState));
-  if (!rc && cudaMallocHost((void**)&s->h_state, sizeof(DevState)) != cudaSuccess)
-    rc = LFX_OUT_OF_MEMORY;
+  if (!rc)
+    rc = host_alloc_mapped(ctx, (void**)&s->h_state, (void**)&s->h_state_dev, sizeof(DevState));
   if (!rc) rc = ensure_partials(ctx, n, 4);
   if (rc) {
     free_solver(s);

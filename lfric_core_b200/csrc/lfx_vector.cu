@@ -83,8 +83,8 @@ static bool same_shape(const lfx_vec* a, const lfx_vec* b) {
 // result of NF per-field sums combined left to right on the host, as the
 // field loops of sci_field_vector_mod.x90:132-182 do
 static int read_sums(lfx_ctx* ctx, int nf, double* out_sum) {
-  LFX_CK(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, sizeof(double) * nf,
-                              cudaMemcpyDeviceToHost, ctx->stream));
+  int rc = to_host_small(ctx, ctx->h_scalars_dev, ctx->d_scalars, sizeof(double) * nf);
+  if (rc) return rc;
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
   double s = 0.0;
   for (int f = 0; f < nf; ++f) s = s + ctx->h_scalars[f];

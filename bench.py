@@ -432,10 +432,30 @@ def cpu_baseline(problem, nsolves):
         _, info = orc.solve("gmres", op, P, p.rhs, r_tol=RTOL, max_iter=200, gcrk=GCRK)
         times.append(time.perf_counter() - t0)
     cores = os.cpu_count()
+    # and one solve on a single thread
+    orc.lib().or_set_threads(1)
+    t0 = time.perf_counter()
+    orc.solve("gmres", op, P, p.rhs, r_tol=RTOL, max_iter=200, gcrk=GCRK)
+    t1 = time.perf_counter() - t0
+    orc.lib().or_set_threads(cores)
     return {"value": nsolves / sum(times), "unit": "solves/s", "cores": cores, "kind": "port",
             "sample": f"{nsolves} full FP64 GMRES(10) solves of the same C96x30 system "
-                      f"({info.iterations} cycles each), OpenMP on {cores} threads",
-            "p50_ms": 1e3 * statistics.median(times)}
+                      f"({info.iterations} cycles each), OpenMP on {cores} threads; one more "
+                      "on 1 thread",
+            "p50_ms": 1e3 * statistics.median(times),
+            "one_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1},
+            "cpu_model": cpu_model()}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def max_over_ranks(v, dist=None, device="cuda"):

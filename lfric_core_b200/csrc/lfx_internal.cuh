@@ -313,7 +313,7 @@ struct lfx_lma_layout {
   // get the same records from every cell that touches them, at most two per
   // cell at consecutive offsets): cells in colour-loop order with the start of
   // each colour, and per cell {map row, flags, partners} padded to cs_ints
-  // ints. flags bit df: this cell is the first (in colour order) on the
+  // ints, stored in the same colour-loop order. flags bit df: this cell is the first (in colour order) on the
   // column of df; bit 8+df: df is the lower record of a pair; bit 16+df: the
   // upper one; bit 24+df: this cell is the last on the column of df.
   // partners: 4 bits per df, the upper record of df's pair.
@@ -339,9 +339,10 @@ struct lfx_op {
   // kernel 1 register gather, kernel 2 generic gather
   int32_t tune_kernel = -1, tune_stages = 0, tune_warps = 0;
   float tune_us = 0.f;
-  // the upper triangle [cell][p][k] of bitwise symmetric local matrices
-  // (p = packed (df, df2), df <= df2), cell stride sblk elements; null when
-  // the operator is not square on one dofmap or not symmetric
+  // the upper triangle [q][p][k] of bitwise symmetric local matrices
+  // (p = packed (df, df2), df <= df2), blocks in the colour-loop order of
+  // the cell scatter (block q: cell cs_cells[q]), stride sblk elements; null
+  // when the operator is not square on one dofmap or not symmetric
   void* smat = nullptr;
   size_t smat_bytes = 0;
   int32_t sblk = 0;

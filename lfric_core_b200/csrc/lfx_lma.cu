@@ -801,11 +801,16 @@ __host__ __device__ constexpr int pidx(int i, int j) {
   return i <= j ? i * NDF - i * (i - 1) / 2 + (j - i) : j * NDF - j * (j - 1) / 2 + (i - j);
 }
 
+// cells: the launch's colour in the colour-loop order (cell ids); q0: the
+// position of its first cell in that order. Descriptors and the packed
+// matrix copy are stored in that order (so a colour's launch streams one
+// contiguous run of each); the full matrix copy stays in cell order.
 struct CellArgs {
   int nl, blk, cstride, dints;
   const int* cells;
   int ncells;
   const int* desc;
+  int q0;
 };
 
 template <class T, int NDF, bool SYM, bool RESID>
@@ -816,8 +821,9 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
   const int lane = threadIdx.x & 31;
   const int ci = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (ci >= C.ncells) return;  // whole warps
-  const int c = __ldg(C.cells + ci);
-  const int* dsc = C.desc + (size_t)c * C.dints;
+  const int q = C.q0 + ci;
+  const int c = SYM ? q : __ldg(C.cells + ci);  // the matrix block
+  const int* dsc = C.desc + (size_t)q * C.dints;
   int mf[NDF];
 #pragma unroll
   for (int j = 0; j < NDF; ++j) mf[j] = __ldg(dsc + j);
@@ -908,11 +914,12 @@ __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, co
   const int nq = mat_bytes / 16, dq = C.dints / 4;
   auto issue = [&](int64_t i, int s) {
     if (i < C.ncells) {
-      const int c = __ldg(C.cells + i);
+      const int cq = C.q0 + (int)i;
+      const int c = SYM ? cq : __ldg(C.cells + i);  // the matrix block
       const char* src = reinterpret_cast<const char*>(M + (size_t)c * C.cstride);
       unsigned char* dst = ring + (size_t)s * stage_bytes;
       for (int q = lane; q < nq; q += 32) cp_async16(dst + 16 * q, src + 16 * q);
-      const char* ds = reinterpret_cast<const char*>(C.desc + (size_t)c * C.dints);
+      const char* ds = reinterpret_cast<const char*>(C.desc + (size_t)cq * C.dints);
       if (lane < dq) cp_async16(dst + mat_bytes + 16 * lane, ds + 16 * lane);
     }
     cp_async_commit();
@@ -989,18 +996,19 @@ __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, co
   cp_async_wait<0>();
 }
 
-// packed upper triangle [c][p][k] (cell stride sblk) from the Fortran
-// (nc3, ndf, ndf) FP64 stencil
+// packed upper triangle [q][p][k] (block stride sblk; block q holds the q-th
+// cell of the colour loop, order[q]) from the Fortran (nc3, ndf, ndf) FP64
+// stencil
 template <class T>
 __global__ void relayout_sym(const double* __restrict__ src, T* __restrict__ dst, int64_t ncell,
-                             int nl, int ndf, int sblk) {
+                             int nl, int ndf, int sblk, const int* __restrict__ order) {
   const int np = ndf * (ndf + 1) / 2;
   const int64_t total = ncell * sblk;
   const int64_t nc3 = ncell * nl;
   for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < total;
        d += (int64_t)gridDim.x * blockDim.x) {
     const int in = (int)(d % sblk);
-    const int64_t c = d / sblk;
+    const int64_t c = order[d / sblk];  // block q holds the q-th cell of the colour loop
     if (in >= np * nl) {
       dst[d] = T(0);
       continue;
@@ -1166,7 +1174,7 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
     L->cs_ints = (ndf + 2 + 3) / 4 * 4;
     std::vector<int32_t> d((size_t)ncell * L->cs_ints, 0);
     for (int32_t c = 0; c < ncell; ++c) {
-      int32_t* row = &d[(size_t)c * L->cs_ints];
+      int32_t* row = &d[(size_t)rank[c] * L->cs_ints];  // in colour-loop order
       for (int j = 0; j < ndf; ++j) row[j] = mf0[(size_t)c * ndf + j];
       row[ndf] = (int32_t)cs_flags[c];
       row[ndf + 1] = (int32_t)cs_part[c];
@@ -1303,10 +1311,12 @@ int upload_matrix(lfx_ctx* ctx, lfx_op* op, const double* stencil) {
       if (!rc) {
         if (op->precision == LFX_R64)
           relayout_sym<double><<<grid, 256, 0, ctx->stream>>>(raw, (double*)op->smat, L->ncell_2d,
-                                                               L->nlayers, L->ndf_to, op->sblk);
+                                                               L->nlayers, L->ndf_to, op->sblk,
+                                                               L->cs_cells);
         else
           relayout_sym<float><<<grid, 256, 0, ctx->stream>>>(raw, (float*)op->smat, L->ncell_2d,
-                                                              L->nlayers, L->ndf_to, op->sblk);
+                                                              L->nlayers, L->ndf_to, op->sblk,
+                                                              L->cs_cells);
         LFX_CK(ctx, cudaGetLastError());
       } else {
         op->smat_bytes = 0;
@@ -1517,7 +1527,7 @@ template <class T, int N, bool SYM, int S, bool RESID>
 void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const void* b,
                     const int* skip) {
   const lfx_lma_layout* L = op->lay;
-  CellArgs C{L->nlayers, op->blk, SYM ? op->sblk : N * op->blk, L->cs_ints, nullptr, 0, L->cs_desc};
+  CellArgs C{L->nlayers, op->blk, SYM ? op->sblk : N * op->blk, L->cs_ints, nullptr, 0, L->cs_desc, 0};
   const T* M = (const T*)(SYM ? op->smat : op->mat);
   const int sb = (int)cells_stage_bytes(op);
   const size_t smem = (size_t)kCellWarps * S * sb;
@@ -1536,6 +1546,7 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
   // one launch per colour, in the reference's colour order
   for (size_t k = 0; k + 1 < L->colour_start.size(); ++k) {
     C.cells = L->cs_cells + L->colour_start[k];
+    C.q0 = L->colour_start[k];
     C.ncells = L->colour_start[k + 1] - L->colour_start[k];
     if (C.ncells <= 0) continue;
     if constexpr (S > 0) {

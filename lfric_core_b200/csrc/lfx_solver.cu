@@ -349,6 +349,13 @@ __device__ __forceinline__ bool cgs_reduce(double (&acc)[NR], double* partials, 
 // sig (nullable): the basis is stored unnormalised, v_j = sig[j] u_j, and the
 // true vector is sig[prev] w; then hcol receives the true inner products
 // <v_j, sig[prev] w> and nhcol the update coefficients -sig[j]^2 <u_j, w>
+// grid-stride steps per loop trip of the float4 Gram-Schmidt kernels: with
+// few basis vectors a thread has too few loads in flight per step
+template <int NR>
+struct CgsUnroll {
+  static constexpr int U = NR <= 2 ? 4 : (NR <= 5 ? 2 : 1);
+};
+
 template <int NR>
 __global__ void __launch_bounds__(kCgsThreads) cgs_dots_f4(int64_t n, VecPtrs vp,
                                                            const float* __restrict__ w,
@@ -362,14 +369,27 @@ __global__ void __launch_bounds__(kCgsThreads) cgs_dots_f4(int64_t n, VecPtrs vp
   for (int r = 0; r < NR; ++r) acc[r] = 0.0;
   const int64_t n4 = n >> 2;
   const float4* w4 = reinterpret_cast<const float4*>(w);
-  for (int64_t q = (int64_t)blockIdx.x * kCgsThreads + threadIdx.x; q < n4;
-       q += (int64_t)gridDim.x * kCgsThreads) {
-    float4 v[NR];
+  // CgsUnroll<NR>::U grid-stride steps per trip, loads first (the same
+  // element order per thread as one step per trip)
+  constexpr int U = CgsUnroll<NR>::U;
+  const int64_t stride = (int64_t)gridDim.x * kCgsThreads;
+  for (int64_t q0 = (int64_t)blockIdx.x * kCgsThreads + threadIdx.x; q0 < n4; q0 += U * stride) {
+    float4 v[U][NR], wq[U];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) v[r] = __ldg(reinterpret_cast<const float4*>(vp.p[r]) + q);
-    const float4 wq = __ldg(w4 + q);
+    for (int u = 0; u < U; ++u) {
+      const int64_t q = q0 + u * stride;
+      if (q < n4) {
 #pragma unroll
-    for (int r = 0; r < NR; ++r) acc[r] += (double)quad_dot(v[r], wq);
+        for (int r = 0; r < NR; ++r) v[u][r] = __ldg(reinterpret_cast<const float4*>(vp.p[r]) + q);
+        wq[u] = __ldg(w4 + q);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (q0 + u * stride < n4) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] += (double)quad_dot(v[u][r], wq[u]);
+      }
   }
   if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
     const int64_t i = 4 * n4 + threadIdx.x;
@@ -405,21 +425,35 @@ __global__ void __launch_bounds__(kCgsThreads) cgs_update_f4(int64_t n, VecPtrs 
   const int64_t n4 = n >> 2;
   const float4* w4 = reinterpret_cast<const float4*>(w);
   float4* o4 = reinterpret_cast<float4*>(out);
-  for (int64_t q = (int64_t)blockIdx.x * kCgsThreads + threadIdx.x; q < n4;
-       q += (int64_t)gridDim.x * kCgsThreads) {
-    float4 v[NR];
+  constexpr int U = CgsUnroll<NR>::U;
+  const int64_t stride = (int64_t)gridDim.x * kCgsThreads;
+  for (int64_t q0 = (int64_t)blockIdx.x * kCgsThreads + threadIdx.x; q0 < n4; q0 += U * stride) {
+    float4 v[U][NR], wq[U];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) v[r] = __ldg(reinterpret_cast<const float4*>(vp.p[r]) + q);
-    float4 wq = w4[q];
+    for (int u = 0; u < U; ++u) {
+      const int64_t q = q0 + u * stride;
+      if (q < n4) {
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      wq.x = fmaf(c[r], v[r].x, wq.x);
-      wq.y = fmaf(c[r], v[r].y, wq.y);
-      wq.z = fmaf(c[r], v[r].z, wq.z);
-      wq.w = fmaf(c[r], v[r].w, wq.w);
+        for (int r = 0; r < NR; ++r) v[u][r] = __ldg(reinterpret_cast<const float4*>(vp.p[r]) + q);
+        wq[u] = w4[q];
+      }
     }
-    o4[q] = wq;
-    acc[0] += (double)quad_dot(wq, wq);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t q = q0 + u * stride;
+      if (q < n4) {
+        float4 o = wq[u];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          o.x = fmaf(c[r], v[u][r].x, o.x);
+          o.y = fmaf(c[r], v[u][r].y, o.y);
+          o.z = fmaf(c[r], v[u][r].z, o.z);
+          o.w = fmaf(c[r], v[u][r].w, o.w);
+        }
+        o4[q] = o;
+        acc[0] += (double)quad_dot(o, o);
+      }
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
     const int64_t i = 4 * n4 + threadIdx.x;

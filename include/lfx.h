@@ -348,7 +348,12 @@ int lfx_solver_set_tolerance(lfx_solver* s, double r_tol, double a_tol);
  * b - A x and the solution update stay FP64 (op64, FP64 vectors); each
  * correction comes from `inner` (typically an FP32 GMRES on an FP32 copy of
  * the operator) solved to inner_rtol. Converged when ||b - A x||/||b - A x0||
- * <= cfg->r_tol, with at most cfg->max_iter refinement steps. */
+ * <= cfg->r_tol, with at most cfg->max_iter refinement steps. When `inner`
+ * is an FP32 GMRES, each refinement step runs one of its restart cycles
+ * (stopping early once the cycle's own estimate reaches inner_rtol), queued
+ * with the step's FP64 residual so that a step costs one host round trip;
+ * the cycle forms no FP32 residual of its own. Other inner solvers run their
+ * full solve per step. */
 int lfx_refined_solver_create(lfx_ctx* ctx, lfx_op* op64, lfx_solver* inner,
                               double inner_rtol, const lfx_solver_cfg* cfg,
                               lfx_solver** out);

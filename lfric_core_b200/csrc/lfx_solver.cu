@@ -346,9 +346,6 @@ __device__ __forceinline__ bool cgs_reduce(double (&acc)[NR], double* partials, 
   return true;
 }
 
-// sig (nullable): the basis is stored unnormalised, v_j = sig[j] u_j, and the
-// true vector is sig[prev] w; then hcol receives the true inner products
-// <v_j, sig[prev] w> and nhcol the update coefficients -sig[j]^2 <u_j, w>
 // grid-stride steps per loop trip of the float4 Gram-Schmidt kernels: with
 // few basis vectors a thread has too few loads in flight per step
 template <int NR>
@@ -356,6 +353,9 @@ struct CgsUnroll {
   static constexpr int U = NR <= 2 ? 4 : (NR <= 5 ? 2 : 1);
 };
 
+// sig (nullable): the basis is stored unnormalised, v_j = sig[j] u_j, and the
+// true vector is sig[prev] w; then hcol receives the true inner products
+// <v_j, sig[prev] w> and nhcol the update coefficients -sig[j]^2 <u_j, w>
 template <int NR>
 __global__ void __launch_bounds__(kCgsThreads) cgs_dots_f4(int64_t n, VecPtrs vp,
                                                            const float* __restrict__ w,

@@ -60,3 +60,19 @@ def test_reference_arm_runs_on_rank0_only(monkeypatch):
     ns = argparse.Namespace(gpus=2, steps=2, warmup=1, impl="reference", cpu_sample=1,
                             no_cpu=False, quick=True)
     assert bench.run_reference(ns) == 0     # returns at once, no solve, no output
+
+
+def test_solve_bytes_counts_every_pass():
+    """Per-solve algorithmic bytes: with unit-sized vectors and applies the
+    count reduces to the passes of each solve, term by term."""
+    n, nc, nrow = 1, 0, 0             # vectors of 4 / 8 bytes, no factors
+    mixed, fp64 = bench.solve_bytes(n, nc, nrow, a32=0, a64=0, gcrk=2, steps=1, inner_iters=2,
+                                    fp64_cycles=1)
+    # mixed: initial 4*8; step: r32 (8+8) + res (8) + prec (12) + norm (4)
+    # + iterations j=1,2: prec 12 + dots 4(j+1) + update 4(j+2) + xupdate 16
+    # + x update 20 + residual 8 + norm 8
+    it = sum(12 + 4 * (j + 1) + 4 * (j + 2) for j in (1, 2))
+    assert mixed == 32 + 16 + 8 + 12 + 4 + it + 16 + 20 + 8 + 8
+    # fp64: initial 32; cycle: prec 24 + norm 8 + scale 16 + 2 precs 48
+    # + MGS (j=1: 16+24+16, j=2: 16+32+24) + xupdate 32 + residual 8 + norm 8
+    assert fp64 == 32 + 24 + 8 + 16 + 48 + (16 + 24 + 16) + (16 + 32 + 24) + 32 + 8 + 8

@@ -76,3 +76,14 @@ def test_solve_bytes_counts_every_pass():
     # fp64: initial 32; cycle: prec 24 + norm 8 + scale 16 + 2 precs 48
     # + MGS (j=1: 16+24+16, j=2: 16+32+24) + xupdate 32 + residual 8 + norm 8
     assert fp64 == 32 + 24 + 8 + 16 + 48 + (16 + 24 + 16) + (16 + 32 + 24) + 32 + 8 + 8
+
+
+def test_solve_bytes_counts_only_executed_iterations():
+    """A cycle that stops early does not count its skipped step: with three
+    iterations over two cycles (2 + 1) the count is one step j = 2 (prec 12,
+    dots 12, update 16) and one x-update vector (4) below four (2 + 2)."""
+    full, _ = bench.solve_bytes(1, 0, 0, a32=0, a64=0, gcrk=2, steps=2, inner_iters=4,
+                                fp64_cycles=1)
+    short, _ = bench.solve_bytes(1, 0, 0, a32=0, a64=0, gcrk=2, steps=2, inner_iters=3,
+                                 fp64_cycles=1)
+    assert full - short == 12 + 12 + 16 + 4

@@ -61,6 +61,10 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=3, help="oracle solves timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the batched and serving legs")
+    ap.add_argument("--apply", default="",
+                    help="pin the LMA apply configuration kernel:stages for FP32,FP64, e.g. 5:0,5:0 "
+                         "(default: the autotuner's choice; a profiler's replays can move that "
+                         "choice, so profiled runs pin the one an unprofiled run tunes to)")
     return ap.parse_args()
 
 
@@ -558,7 +562,15 @@ def main():
     s64 = wl.device_w2(ctx, p, lfx.R64)
     s32 = wl.device_w2(ctx, p, lfx.R32, op64=s64.op64, cma=s64.cma, diag64=s64.diag)
     # apply autotuner (set-up, untimed): fastest launch configuration per operator
-    tuning = {"fp32": s32.op.autotune(reps=10), "fp64": s64.op.autotune(reps=10)}
+    if args.apply:
+        tuning = {}
+        for name, sys_, spec in zip(("fp32", "fp64"), (s32, s64), args.apply.split(",")):
+            k, st = (int(v) for v in spec.split(":"))
+            sys_.op.set_apply(k, st)
+            tuning[name] = {"kernel": lfx.APPLY_KERNEL_NAMES[k], "stages": st, "warps": 0,
+                            "us": round(sys_.op.time_apply(k, st, 0, 10), 2), "pinned": True}
+    else:
+        tuning = {"fp32": s32.op.autotune(reps=10), "fp64": s64.op.autotune(reps=10)}
     fp64 = lfx.GMRES(s64.op, s64.prec, GCRK, RTOL, 1e-16, 200)
     mixed = wl.refined_gmres(s32, gcrk=GCRK, inner_rtol=INNER_RTOL, r_tol=RTOL)
     B = lfx.FieldVector.from_array(ctx, p.rhs)
@@ -662,8 +674,12 @@ def main():
 
     K = args.steps
     # mixed precision: the headline, uninstrumented
+    # (an NVTX range "timed" lets a profiler keep to these solves:
+    # ncu --nvtx --nvtx-include "timed/")
     with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("timed")
         mx = timed(mixed, K)
+        torch.cuda.nvtx.range_pop()
     rel_mixed = true_rel()
     # the same K solves again with CUDA events around every apply inside the
     # solver graphs (the roofline's kernel times; the event nodes themselves
@@ -723,7 +739,8 @@ def main():
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": traffic, "algorithmic_bytes_per_launch": bytes32,
-            "launch": "one apply (the cell scatter: one kernel per colour)",
+            "launch": ("one apply (the cell scatter: one kernel per colour)"
+                       if tuning["fp32"]["kernel"] == "cell-scatter" else "one apply (one launch)"),
             "launches_timed": n32, "applies_executed": K * exec32,
             "avg_launch_us": round(1e3 * avg32, 2),
             "timed_pass": "a second pass of the same solves with events around each apply "

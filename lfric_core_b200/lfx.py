@@ -374,6 +374,11 @@ class FieldVector(_Handle):
         return p.value
 
 
+# LMA apply kernels by number (lfx_op_autotune / lfx_op_set_apply)
+APPLY_KERNEL_NAMES = {0: "pipeline", 1: "register-gather", 2: "generic",
+                      3: "register-gather-prefetch", 4: "staged-pipeline", 5: "cell-scatter"}
+
+
 class LmaOperator(_Handle):
     """operator_type applied by the coloured matrix_vector_kernel: y = A x."""
 
@@ -418,10 +423,8 @@ class LmaOperator(_Handle):
         k, s, w, us = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
         self.ctx.check(self.ctx.L.lfx_op_autotune(self.h, reps, C.byref(k), C.byref(s),
                                                    C.byref(w), C.byref(us)))
-        name = {0: "pipeline", 1: "register-gather", 2: "generic",
-                3: "register-gather-prefetch", 4: "staged-pipeline",
-                5: "cell-scatter"}[k.value]
-        return {"kernel": name, "stages": s.value, "warps": w.value, "us": round(us.value, 2)}
+        return {"kernel": APPLY_KERNEL_NAMES[k.value], "stages": s.value, "warps": w.value,
+                "us": round(us.value, 2)}
 
     def storage(self) -> dict:
         """Bytes of the full local-matrix copy and of the packed upper

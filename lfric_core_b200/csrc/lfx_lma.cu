@@ -889,6 +889,85 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
 #undef MV
 }
 
+// The cell scatter for columns of more than 31 levels: a cell column is split
+// into nseg segments of L <= 31 levels, one warp each. In segment sg, lane l
+// (1 <= l <= L) holds level k = sg * L + l - 1 and writes the dofs of that
+// level (and the bottom face of a pair, whose upper-record terms come from
+// the lane below); lane 0 holds the level just below the segment only to
+// supply those terms to lane 1 and writes nothing. Every dof therefore gets
+// the terms of lma_cells in the same order (the same bits).
+template <class T, int NDF, bool SYM, bool RESID>
+__global__ void __launch_bounds__(256) lma_cells_seg(CellArgs C, int nseg, int L,
+                                                     const T* __restrict__ M,
+                                                     const T* __restrict__ x, T* __restrict__ y,
+                                                     const T* __restrict__ b, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (wg >= (int64_t)C.ncells * nseg) return;  // whole warps
+  const int ci = (int)(wg / nseg), sg = (int)(wg % nseg);
+  const int q = C.q0 + ci;
+  const int c = SYM ? q : __ldg(C.cells + ci);  // the matrix block
+  const int* dsc = C.desc + (size_t)q * C.dints;
+  int mf[NDF];
+#pragma unroll
+  for (int j = 0; j < NDF; ++j) mf[j] = __ldg(dsc + j);
+  const uint32_t flags = (uint32_t)__ldg(dsc + NDF), part = (uint32_t)__ldg(dsc + NDF + 1);
+  const int nl = C.nl;
+  const int k = sg * L + lane - 1;           // this lane's level
+  const bool own = lane >= 1 && lane <= L;   // lanes that write
+  const bool v = k >= 0 && k < nl && lane <= L;  // a cell level this warp needs
+  const T* Mc = M + (size_t)c * C.cstride + (v ? k : 0);
+  constexpr int NP = SYM ? NDF * (NDF + 1) / 2 : NDF * NDF;
+  T m[NP], xv[NDF], yo[NDF];
+#pragma unroll
+  for (int p = 0; p < NP; ++p)
+    m[p] = v ? __ldcs(Mc + (SYM ? p * nl : (p / NDF) * C.blk + (p % NDF) * nl)) : T(0);
+#pragma unroll
+  for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldg(x + mf[j] + k) : T(0);
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#pragma unroll
+  for (int df = 0; df < NDF; ++df) {
+    const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+    const bool opens = (flags >> df) & 1u;
+    const bool live = own && (lower ? k <= nl : v);
+    yo[df] = (!upper && !opens && live) ? y[mf[df] + k] : T(0);
+  }
+#define MV(i, j) m[SYM ? pidx<NDF>(i, j) : (i) * NDF + (j)]
+#pragma unroll
+  for (int df = 0; df < NDF; ++df) {
+    if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
+    if ((flags >> (8 + df)) & 1u) {
+      const int bsel = (part >> (4 * df)) & 15u;
+#pragma unroll
+      for (int bb = df + 1; bb < NDF; ++bb) {
+        if (bb != bsel) continue;
+        T acc = yo[df];
+#pragma unroll
+        for (int j = 0; j < NDF; ++j) {
+          const T mb = __shfl_up_sync(0xffffffffu, MV(bb, j), 1);
+          const T xb = __shfl_up_sync(0xffffffffu, xv[j], 1);
+          if (v) acc = fmaT(MV(df, j), xv[j], acc);
+          if (own && k >= 1 && k <= nl) acc = fmaT(mb, xb, acc);
+        }
+        if (own && k <= nl) {
+          const int row = mf[df] + k;
+          y[row] = (RESID && ((flags >> (24 + df)) & 1u)) ? b[row] - acc : acc;
+        }
+      }
+    } else {
+      T acc = yo[df];
+#pragma unroll
+      for (int j = 0; j < NDF; ++j) acc = fmaT(MV(df, j), xv[j], acc);
+      if (own && v) {
+        const int row = mf[df] + k;
+        y[row] = (RESID && ((flags >> (24 + df)) & 1u)) ? b[row] - acc : acc;
+      }
+    }
+  }
+#undef MV
+}
+
 // The cell scatter with each warp's next cells staged ahead: a warp walks
 // the colour's cells with stride (warps in the grid) and keeps the local
 // matrices and descriptors of its next S cells in flight (16-byte cp.async
@@ -1062,7 +1141,7 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
   std::vector<int32_t> ent_base, ent_h, ent_grp, grp_cell;
   std::vector<uint32_t> grp_rec;
   // cell-scatter plan: only for square operators on one dofmap (colour given)
-  bool cs = colour != nullptr && ndf <= 8 && nl + 1 <= 32;
+  bool cs = colour != nullptr && ndf <= 8;
   std::vector<uint32_t> cs_flags(cs ? (size_t)ncell : 0, 0u), cs_part(cs ? (size_t)ncell : 0, 0u);
   size_t i = 0;
   int64_t covered = 0;
@@ -1556,9 +1635,13 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
           C, M, (const T*)x, (T*)y, (const T*)b, sb, skip);
     } else {
       // colours after the first launch as programmatic dependents of the
-      // previous colour (they wait in the kernel before reading y)
+      // previous colour (they wait in the kernel before reading y); a column
+      // of more than 31 levels takes nseg warps of L levels each
+      const int nl = L->nlayers;
+      const int nseg = nl + 1 <= 32 ? 1 : (nl + 1 + 30) / 31;
+      const int seg_l = (nl + 1 + nseg - 1) / nseg;
       cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3((unsigned)(((int64_t)C.ncells * 32 + 255) / 256));
+      cfg.gridDim = dim3((unsigned)(((int64_t)C.ncells * nseg * 32 + 255) / 256));
       cfg.blockDim = dim3(256);
       cfg.dynamicSmemBytes = 0;
       cfg.stream = ctx->stream;
@@ -1567,8 +1650,12 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
       at[0].val.programmaticStreamSerializationAllowed = 1;
       cfg.attrs = at;
       cfg.numAttrs = k > 0 ? 1 : 0;
-      cudaLaunchKernelEx(&cfg, lma_cells<T, N, SYM, RESID>, C, M, (const T*)x, (T*)y,
-                         (const T*)b, skip);
+      if (nseg == 1)
+        cudaLaunchKernelEx(&cfg, lma_cells<T, N, SYM, RESID>, C, M, (const T*)x, (T*)y,
+                           (const T*)b, skip);
+      else
+        cudaLaunchKernelEx(&cfg, lma_cells_seg<T, N, SYM, RESID>, C, nseg, seg_l, M,
+                           (const T*)x, (T*)y, (const T*)b, skip);
     }
     ctx->launches++;
   }
@@ -1607,6 +1694,7 @@ void launch_cells(lfx_ctx* ctx, const lfx_op* op, int stages, const void* x, voi
 bool cells_stages_ok(const lfx_op* op, int stages) {
   if (stages == 0) return true;
   if (stages != 2 && stages != 3) return false;
+  if (op->lay->nlayers + 1 > 32) return false;  // the staged walk keeps one warp per column
   return (size_t)kCellWarps * stages * cells_stage_bytes(op) <= kCellSmemMax;
 }
 

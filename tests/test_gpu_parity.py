@@ -239,6 +239,55 @@ def test_cell_scatter_stages_symmetric(ctx, space, n, nl, prec):
         assert same(Y.export_field(), ref)
 
 
+@pytest.mark.parametrize("space,n,nl", [("w2", 5, 32), ("w2", 4, 40), ("w0", 4, 63),
+                                         ("w2", 3, 70), ("w0", 3, 70)])
+@pytest.mark.parametrize("prec", [64, 32])
+def test_cell_scatter_long_columns(ctx, space, n, nl, prec):
+    """Columns of more than 31 levels take several warps per cell column
+    (segments whose lane 0 supplies the face shared with the segment below):
+    FP64 equals the oracle and FP32 the register gather, bit for bit, for the
+    packed symmetric and the full (non-symmetric) storage."""
+    p = mg.w2_problem(n, nl, seed=6) if space == "w2" else mg.w0_problem(n, nl, seed=6)
+    npc, cic = p.mesh.colour_lookup()
+    rng = np.random.default_rng(8)
+    x = mg.normal(10, p.undf)
+    for lma in (p.lma, p.lma * (1.0 + 0.01 * rng.standard_normal(p.lma.shape))):
+        op = lfx.LmaOperator(ctx, p.ncell_2d, nl, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf,
+                             lma, npc, cic, precision=prec)
+        X = lfx.FieldVector.from_array(ctx, x, prec)
+        Y = lfx.FieldVector(ctx, [p.undf], prec)
+        op.set_apply(1)
+        op.apply(X, Y)
+        gather = Y.export_field()
+        op.set_apply(5, 0)
+        Y.set_scalar(3.0)
+        op.apply(X, Y)
+        got = Y.export_field()
+        ctx.check_device_error()
+        if prec == 64:
+            oop = orc.LmaOperator(p.ncell_2d, nl, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf,
+                                  lma, npc, cic)
+            assert same(got, oop.apply(x))
+        assert same(got, gather)
+
+
+def test_cell_scatter_long_columns_in_gmres(ctx):
+    """A 40-level W2 GMRES solve through the segmented cell scatter (plain and
+    residual-form applies) equals the oracle's solve bit for bit."""
+    p = mg.w2_problem(6, 40, seed=2)
+    sysd = wl.device_w2(ctx, p)
+    op = o_lma(p)
+    oprec, _ = o_w2_prec(p, op)
+    x_o, info_o = orc.solve("gmres", op, oprec, p.rhs, r_tol=1e-8, a_tol=1e-16, max_iter=200,
+                            gcrk=10)
+    sysd.op.set_apply(5, 0)
+    g = lfx.GMRES(sysd.op, sysd.prec, 10, 1e-8, 1e-16, 200)
+    X, B = sysd.vector(), sysd.vector(p.rhs)
+    info = g.apply(X, B)
+    assert info.converged and info.iterations == info_o.iterations
+    assert same(X.export_field(), x_o)
+
+
 def test_cell_scatter_in_gmres(ctx):
     p = mg.w2_problem(16, 12, seed=2)
     sysd = wl.device_w2(ctx, p)

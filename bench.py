@@ -86,6 +86,7 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self._first = threading.Event()
 
     def __enter__(self):
         try:
@@ -95,6 +96,9 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            # nvidia-smi takes a moment to start sampling: the timed region
+            # begins once the first sample is in (or after 5 s without one)
+            self._first.wait(timeout=5.0)
         except OSError:
             self.proc = None
         return self
@@ -102,6 +106,7 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self._first.set()
 
     def __exit__(self, *a):
         if self.proc:

@@ -457,9 +457,8 @@ int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double*
 /* ------------------------------------------------------------------ no allocation
  * Allocation-free inner product (no counterpart in the reference): for
  * callers that cannot allocate device memory where they need a dot product --
- * device memory owned by another runtime's pool, a CUDA graph capture open on
- * their stream, or a loop that must not take cudaMalloc's implicit
- * synchronisation. x, y (n FP64 values) and result (one FP64 value) are device
+ * device memory owned by another runtime's pool, or a loop that must not take
+ * cudaMalloc's implicit synchronisation. x, y (n FP64 values) and result (one FP64 value) are device
  * pointers owned by the caller; the work is queued on `stream` (a
  * cudaStream_t, NULL for the default stream) and *result is valid once it
  * completes. The reduction scratch is a fixed array built into the library
@@ -467,7 +466,9 @@ int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double*
  * to lfx_dot_noalloc_max_n() (16 Mi) values; larger n is rejected with
  * LFX_INVALID_ARGUMENT and a message from lfx_noalloc_last_error(). The first
  * call on each device looks up the array's device address; make that first
- * call before any stream capture. All calls share the array: calls that
+ * call before any stream capture. A device reset (cudaDeviceReset) may move
+ * the array; do not call this again in a process after one. n = 0 gives 0.0.
+ * All calls share the array: calls that
  * overlap on the GPU (different streams, or concurrent host threads) race and
  * must be serialised by the caller. The result equals lfx_vec_dot's bit for
  * bit. */

@@ -7,6 +7,7 @@ Both land in lfric_core_b200/lib/ so that they travel with the source tree.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import subprocess
 import sys
@@ -24,11 +25,31 @@ CU_SOURCES = sorted(CSRC.glob("*.cu"))
 CU_HEADERS = sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
 
 
-def _stale(target: Path, deps) -> bool:
-    if not target.exists():
+def _digest(deps, cmd=()) -> str:
+    h = hashlib.sha256()
+    for d in sorted(str(x) for x in deps):
+        h.update(Path(d).name.encode())
+        h.update(Path(d).read_bytes())
+    h.update(" ".join(str(c) for c in cmd).encode())
+    return h.hexdigest()
+
+
+def _stamp(target: Path) -> Path:
+    return target.with_name(target.name + ".stamp")
+
+
+def _stale(target: Path, deps, cmd=()) -> bool:
+    """True unless `target` exists and was built from sources with these
+    exact contents (a digest stamp beside it: copying the tree, which moves
+    modification times, does not force a rebuild; editing a source does)."""
+    st = _stamp(target)
+    if not target.exists() or not st.exists():
         return True
-    t = target.stat().st_mtime
-    return any(Path(d).stat().st_mtime > t for d in deps)
+    return st.read_text().strip() != _digest(deps, cmd)
+
+
+def _mark(target: Path, deps, cmd=()) -> None:
+    _stamp(target).write_text(_digest(deps, cmd) + "\n")
 
 
 def _run(cmd):
@@ -39,10 +60,12 @@ def _run(cmd):
 def build_meshgen(force: bool = False) -> Path:
     out = LIB / "liblfx_meshgen.so"
     src = CSRC / "meshgen.c"
-    if force or _stale(out, [src, INCLUDE / "lfx_meshgen.h"]):
+    deps = [src, INCLUDE / "lfx_meshgen.h"]
+    if force or _stale(out, deps):
         LIB.mkdir(exist_ok=True)
         _run(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
               f"-I{INCLUDE}", src, "-o", out, "-lm"])
+        _mark(out, deps)
     return out
 
 
@@ -63,9 +86,11 @@ def build_lfx(force: bool = False) -> Path:
                       "-Xcompiler", "-fPIC,-ffp-contract=off",
                       "-Xptxas", "-v" if os.environ.get("LFX_PTXAS_V") else "-O3",
                       f"-I{INCLUDE}", f"-I{CSRC}", "-c", src, "-o", obj])
+                _mark(obj, [src] + CU_HEADERS)
             objs.append(obj)
         _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", out,
               "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
+        _mark(out, CU_SOURCES + CU_HEADERS)
     return out
 
 

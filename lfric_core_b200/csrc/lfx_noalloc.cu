@@ -2,10 +2,10 @@
 //
 // Some callers cannot allocate device memory at the point where they need an
 // inner product: a host model whose device memory belongs to another
-// allocator (a Fortran runtime's OpenMP/OpenACC pool, say), code running while
-// somebody else's CUDA graph capture is open on its stream (an allocation
-// there is illegal), or a latency-critical loop that must not take the
-// implicit synchronisation of cudaMalloc/cudaFree. lfx_dot_noalloc serves them:
+// allocator (a Fortran runtime's OpenMP/OpenACC pool, say, which must stay
+// the only owner of the device's memory), or a latency-critical loop that must
+// not take the implicit synchronisation of cudaMalloc/cudaFree. lfx_dot_noalloc
+// serves them:
 // the caller passes the inputs and the (device) output, and the only scratch
 // the reduction needs -- one partial sum per 2048-element chunk plus a
 // completion ticket -- lives in the file-scope array below, which every GPU
@@ -13,6 +13,11 @@
 //
 // The sum is computed in the same fixed order as lfx_vec_dot, so the two give
 // bit-identical results.
+//
+// The array's device address is looked up once per device and kept for the
+// life of the process. A cudaDeviceReset (or any reset of the device's primary
+// context) unloads the module, which may come back at another address: after
+// one, this entry point must not be called again in the same process.
 #include <mutex>
 #include <string>
 

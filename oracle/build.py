@@ -8,6 +8,7 @@ environment (no Fortran compiler, no PSyclone), so there is no oracle/_ref.
 """
 from __future__ import annotations
 
+import hashlib
 import subprocess
 import sys
 from pathlib import Path
@@ -21,14 +22,25 @@ CFLAGS = ["-O3", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
           "-march=x86-64-v3", "-fno-math-errno"]
 
 
+def _digest() -> str:
+    h = hashlib.sha256()
+    for f in ("oracle.c", "oracle.h"):
+        h.update((HERE / f).read_bytes())
+    h.update(" ".join(CFLAGS).encode())
+    return h.hexdigest()
+
+
 def build(force: bool = False) -> Path:
-    src = HERE / "oracle.c"
-    hdr = HERE / "oracle.h"
-    if force or not OUT.exists() or max(src.stat().st_mtime, hdr.stat().st_mtime) > OUT.stat().st_mtime:
+    """Compiles the oracle unless the library beside its digest stamp was
+    built from these exact sources."""
+    stamp = OUT.with_name(OUT.name + ".stamp")
+    dg = _digest()
+    if force or not OUT.exists() or not stamp.exists() or stamp.read_text().strip() != dg:
         OUT.parent.mkdir(exist_ok=True)
-        cmd = ["gcc", *CFLAGS, str(src), "-o", str(OUT), "-lm"]
+        cmd = ["gcc", *CFLAGS, str(HERE / "oracle.c"), "-o", str(OUT), "-lm"]
         print("+", " ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+        stamp.write_text(dg + "\n")
     return OUT
 
 

@@ -13,16 +13,14 @@ def pytest_configure(config):
 
 
 def _ensure_built():
-    """Build whatever native library is missing (no rebuild when present, so
-    prebuilt libraries shipped with the tree are used as they are)."""
+    """Rebuild every native library whose sources changed since it was built
+    (each library carries a digest of the sources it was built from, so a
+    stale library is never tested, and a prebuilt tree whose sources match
+    is used as it is)."""
     from lfric_core_b200 import build as pkg_build
     from oracle import build as oracle_build
-    if not (pkg_build.LIB / "liblfx_meshgen.so").exists():
-        pkg_build.build_meshgen()
-    if not oracle_build.OUT.exists():
-        oracle_build.build()
-    if not (pkg_build.LIB / "liblfx.so").exists():
-        pkg_build.build_lfx()
+    pkg_build.build_all()
+    oracle_build.build()
 
 
 _ensure_built()

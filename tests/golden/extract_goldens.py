@@ -1,9 +1,8 @@
 """Extract the known-answer data of the reference's pFUnit kernel tests into
 tests/golden/kernel_goldens.json.
 
-Run in a checkout that has the reference tree (default location given by
---ref). The tests read only the JSON; the reference is not needed at test
-time. Each entry records the .pf file it came from.
+Run with --ref pointing at a checkout of the reference tree. The tests read
+only the JSON; the reference is not needed at test time. Each entry records the .pf file it came from.
 
 Sources (paths inside the reference project):
   components/science/unit-test/kernel/algebra/matrix_vector_mod_test.pf
@@ -119,7 +118,7 @@ def cma_diag_hmht(text: str) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference checkout")
     ap.add_argument("--out", default=str(Path(__file__).with_name("kernel_goldens.json")))
     a = ap.parse_args()
     ut = Path(a.ref) / "components/science/unit-test/kernel"

@@ -1,12 +1,14 @@
 """GPU test of the allocation-free inner product (lfx_dot_noalloc).
 
 Callers that cannot allocate device memory where they need a dot product (a
-pool owned by another runtime, an open graph capture, a loop that must not
-synchronise) use lfx_dot_noalloc, whose reduction scratch is a fixed array
-inside the library. This checks it through the C ABI against the allocating
-entry point, lfx_vec_dot, on two calls in a row (the second reuses the scratch
-the first left behind), and that an oversized input is refused before any
-work is queued. The file is named to run after the other tests.
+pool owned by another runtime, a loop that must not synchronise) use
+lfx_dot_noalloc, whose reduction scratch is a fixed array inside the library.
+This checks it through the C ABI against the allocating entry point,
+lfx_vec_dot, on two calls in a row (the second reuses the scratch the first
+left behind): the header promises the same bits, and the parity tests'
+relative tolerance is checked as well. An empty input gives 0.0, and an
+oversized one is refused before any work is queued. The file is named to run
+after the other tests.
 """
 import numpy as np
 import pytest
@@ -34,10 +36,22 @@ def test_dot_noalloc_matches_vec_dot_on_two_calls(ctx):
         rc = L.lfx_dot_noalloc(X.device_ptr(), Y.device_ptr(), n, R.device_ptr(), ctx.stream)
         assert rc == 0, L.lfx_noalloc_last_error().decode()
         ctx.synchronize()
-        got = float(R.export_field()[0])
+        got = R.export_field()[0]
         assert abs(got - want) <= REL_TOL * abs(want), (call, got, want)
-        results.append(got)
+        assert np.float64(got).view(np.int64) == np.float64(want).view(np.int64), (call, got, want)
+        results.append(float(got))
     assert results[0] != results[1]
+
+
+def test_dot_noalloc_empty_input_gives_zero(ctx):
+    L = lfx.load_library()
+    X = lfx.FieldVector(ctx, [4])
+    R = lfx.FieldVector(ctx, [1])
+    R.set_scalar(7.0)
+    rc = L.lfx_dot_noalloc(X.device_ptr(), X.device_ptr(), 0, R.device_ptr(), ctx.stream)
+    assert rc == 0, L.lfx_noalloc_last_error().decode()
+    ctx.synchronize()
+    assert R.export_field()[0] == 0.0
 
 
 def test_dot_noalloc_rejects_oversized_input(ctx):

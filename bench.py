@@ -50,6 +50,9 @@ N_EDGE, NLAYERS, GCRK, RTOL, SEED = 96, 30, 10, 1e-8, 2
 WORKLOAD = ("C96x30 W2-W3 Helmholtz A=M2+0.1*D^T*D, GMRES(10) + column-tridiagonal(W2V)"
             " / Jacobi(W2H) preconditioner, solve to 1e-8 rel. residual")
 INNER_RTOL = 1e-4
+# a solution at 1e-8 relative residual lies within cond(A) * 2e-8 of another;
+# cond(A) of the C96x30 Helmholtz system is below 50 (mass-dominated, tau 0.1)
+E2E_TOL = 1e-6
 
 
 def parse():
@@ -204,15 +207,16 @@ def leg_batched(ctx, lfx, mg, wl, torch, stream):
     systems = [wl.batch_system(ctx, n, l, sd, mg.W0) for n, l, _, sd in specs]
     setup_s = time.perf_counter() - t0
     tot = sum(s.undf for s in systems)
-    ent = sum(s.entities for s in systems)
-    B = lfx.Batch(ctx, 8, len(systems), tot, ent, 0, 8)
+    B = lfx.Batch(ctx, 8, len(systems), reserve_bytes=2 << 30, iters=16)
     xs = [lfx.FieldVector(ctx, [s.undf]) for s in systems]
 
-    def batched():
+    def batched(tune=False):
         slots = []
         for s, x, (_, _, tol, _) in zip(systems, xs, specs):
             x.set_scalar(0.0)
             slots.append(B.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x, tol, 20000))
+        if tune:
+            B.autotune(iters=4)
         steps = 0
         while B.step() < len(systems):
             steps += 1
@@ -221,7 +225,8 @@ def leg_batched(ctx, lfx, mg, wl, torch, stream):
             B.retire(sl)
         return infos, steps
 
-    batched()  # warm-up (graph already captured; pages the pools in)
+    batched(tune=True)  # warm-up with the launch-shape autotuner (pages the pool in)
+    r0 = B.tuning()["replays"]
     ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     ctx.synchronize()
     ev[0].record(stream)
@@ -233,6 +238,7 @@ def leg_batched(ctx, lfx, mg, wl, torch, stream):
     wall_batch = time.perf_counter() - w0
     ok = all(i["status"] == 0 and i["final_rel"] <= tol * 1.0001
              for i, (_, _, tol, _) in zip(infos, specs))
+    x_batch = [x.export_field() for x in xs]
     # plain FP64 serial solves of the same systems (graphs warmed first)
     cgs = [s.cg64(tol) for s, (_, _, tol, _) in zip(systems, specs)]
     for c, s, x in zip(cgs, systems, xs):
@@ -248,14 +254,39 @@ def leg_batched(ctx, lfx, mg, wl, torch, stream):
     ctx.synchronize()
     t_serial = ev[0].elapsed_time(ev[1]) / 1e3
     cells = sum(6 * n * n * l for n, l, _, _ in specs)
+    tune = B.tuning()
+    err = []
+    for xb, x in zip(x_batch, xs):
+        x64 = x.export_field()
+        err.append(float(np.linalg.norm(xb - x64) / np.linalg.norm(x64)))
+    # two systems against the oracle's own FP64 CG on the host (the smallest
+    # and a mid-size one; the parity tests pin the device CG to it bit for bit)
+    from oracle import oracle as orc
+    sample = {}
+    for i in sorted(range(len(specs)), key=lambda i: 6 * specs[i][0] ** 2 * specs[i][1])[:2]:
+        n, l, tol, sd = specs[i]
+        p = mg.w0_problem(n, l, seed=sd)
+        npc, cic = p.mesh.colour_lookup()
+        o = orc.LmaOperator(p.ncell_2d, l, 8, 8, p.map, p.map, p.undf, p.undf, p.lma, npc, cic)
+        xo, _ = orc.solve("cg", o, orc.Preconditioner.diagonal(o.diagonal()),
+                          systems[i].b.export_field(), r_tol=tol, a_tol=0.0, max_iter=20000)
+        sample[f"C{n}x{l}"] = float(np.linalg.norm(x_batch[i] - xo) / np.linalg.norm(xo))
     return {
         "workload": "256 uneven W0 mass+diffusion solves, C12-C48 x 10-70 levels, tol 1e-10..1e-6 "
                     "(seeded), FP32 PCG + FP64 reliable updates, one batch",
         "cells_total": cells, "dofs_total": tot,
         "batched_solves_per_s": round(len(specs) / t_batch, 2),
         "batched_s": round(t_batch, 4), "batched_wall_s": round(wall_batch, 4),
-        "graph_replays": steps + 1, "iterations_max": max(i["iterations"] for i in infos),
+        "graph_replays": tune["replays"] - r0, "kernel_launches_per_replay": 1,
+        "launch_shape": {k: tune[k] for k in ("cells_per_item", "blocks_per_sm", "grid",
+                                              "group_bytes", "cooperative")},
+        "tuned_us_per_iteration": round(tune["us_per_iteration"], 2),
+        "iterations_max": max(i["iterations"] for i in infos),
         "all_converged_on_fp64_residual": ok,
+        "error_vs_fp64_max": max(err), "error_vs_fp64_median": float(np.median(err)),
+        "error_reference": "each system's serial FP64 device CG solution at the same tolerance "
+                           "(that solve equals the oracle's bit for bit in the parity tests)",
+        "error_vs_fp64_oracle_sample": sample,
         "serial_fp64_solves_per_s": round(len(specs) / t_serial, 2), "serial_fp64_s": round(t_serial, 4),
         "serial_fp64_iterations_max": max(it64),
         "speedup_vs_serial_fp64": round(t_serial / t_batch, 3), "setup_s": round(setup_s, 1),
@@ -377,84 +408,135 @@ def leg_multi_rhs(ctx, lfx, mg, wl, torch, stream, n=48, nl=30, nrhs=64):
     return out
 
 
-def leg_serving(ctx, lfx, mg, wl, nreq=200):
-    """Poisson stream (2000 requests/s, seeded) of W2 Helmholtz solves of
-    mixed size (a pool of 12 operators, C12-C96 x 20-70 levels; right-hand
-    sides staged in HBM), tolerances 1e-10..1e-6: continuous batching against
-    serial plain FP64 solves of the same request list."""
-    shapes, reqs = wl.config4_stream(nreq=nreq)
+def leg_serving(ctx, lfx, mg, wl, torch, nreq=200, npool=48):
+    """Poisson stream (2000 requests/s, seeded) of W2 Helmholtz solves, each
+    request with its own operator and right-hand side: the operators are 48
+    distinct seeded geometries C12-C96 x 20-70 levels (assembled on the device
+    before the stream starts, as the client model hands them over), the
+    right-hand side of every request is its own N(0,1) vector in pinned host
+    memory, copied to the device at admission, and the solution is copied
+    back at completion; tolerances 1e-10..1e-6. Continuous batching: a request
+    is admitted as soon as it has arrived, a slot is free and the device keeps
+    its memory reserve; its Krylov state lives on the device until it is
+    retired. Against serial plain FP64 device CG solves of the same request
+    list (same copies)."""
+    shapes, reqs = wl.config4_stream(nreq=nreq, pool=npool)
+    t0 = time.perf_counter()
     systems = [wl.batch_system(ctx, n, l, 500 + i, mg.W2) for i, (n, l) in enumerate(shapes)]
-    big = max(s.undf for s in systems)
-    B = lfx.Batch(ctx, 6, 32, 6 * big, 6 * max(s.entities for s in systems),
-                  6 * max(s.columns for s in systems), 4)
-    free_x = {i: [lfx.FieldVector(ctx, [s.undf]) for _ in range(4)] for i, s in enumerate(systems)}
-    # serial FP64 service times: one device-resident CG per operator, warmed
-    # (graphs captured) before timing; each request sets its tolerance
+    setup_s = time.perf_counter() - t0
+    # every request's right-hand side, in pinned host memory (its own seed)
+    tot = sum(systems[w].undf for _, w, _ in reqs)
+    pin = torch.empty(2 * tot, dtype=torch.float64, pin_memory=True).numpy()
+    off, bh, xh = 0, [], []
+    for r, (_, w, _) in enumerate(reqs):
+        n = systems[w].undf
+        pin[off:off + n] = mg.normal(7000 + r, n)
+        bh.append(pin[off:off + n])
+        xh.append(pin[tot + off:tot + off + n])
+        off += n
+    free = {}  # device (b, x) pairs by operator, reused; a new pair when none is free
+
+    def pair(w):
+        lst = free.setdefault(w, [])
+        if lst:
+            return lst.pop()
+        n = systems[w].undf
+        return lfx.FieldVector(ctx, [n]), lfx.FieldVector(ctx, [n])
+
+    # serial plain FP64: one device-resident CG per request (graphs warmed)
     cgs = {}
-    for i, s in enumerate(systems):
-        cgs[i] = s.cg64(1e-10)
-        x = free_x[i][0]
-        x.set_scalar(0.0)
-        cgs[i].apply(x, s.b)
-    service = []
-    for _, w, tol in reqs:
-        s, x = systems[w], free_x[w][0]
-        cgs[w].set_tolerance(tol)
-        x.set_scalar(0.0)
+    for w, sy in enumerate(systems):
+        cgs[w] = sy.cg64(1e-10)
+        bv, xv = pair(w)
+        xv.set_scalar(0.0)
+        cgs[w].apply(xv, sy.b)
+        free[w].append((bv, xv))
+    service, x64 = [], []
+    for r, (_, w, tol) in enumerate(reqs):
+        bv, xv = pair(w)
         ctx.synchronize()
         t = time.perf_counter()
-        cgs[w].apply(x, s.b)
+        bv.import_field_async(bh[r])
+        xv.set_scalar(0.0)
+        cgs[w].set_tolerance(tol)
+        cgs[w].apply(xv, bv)
+        xv.export_field(out=xh[r])
         service.append(time.perf_counter() - t)
+        x64.append(xh[r].copy())
+        free[w].append((bv, xv))
     fin, lat_serial = 0.0, []
     for (arr, _, _), sv in zip(reqs, service):
         fin = max(fin, arr) + sv
         lat_serial.append(fin - arr)
     serial_makespan = fin - reqs[0][0]
-    # continuous batching
-    pending, inflight, lat, done = list(range(nreq)), {}, [0.0] * nreq, 0
-    occupancy = []
-    ctx.synchronize()
-    t0 = time.perf_counter()
-    while done < nreq:
-        now = time.perf_counter() - t0
-        while pending and reqs[pending[0]][0] <= now and free_x[reqs[pending[0]][1]]:
-            r = pending[0]
-            _, w, tol = reqs[r]
-            s = systems[w]
-            x = free_x[w].pop()
-            x.set_scalar(0.0)
-            slot = B.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x, tol, 20000, r)
-            if slot is None:
-                free_x[w].append(x)
-                break
-            inflight[slot] = (r, w, x)
-            pending.pop(0)
-        if not inflight:
-            if pending:
-                time.sleep(max(0.0, reqs[pending[0]][0] - (time.perf_counter() - t0)))
-            continue
-        occupancy.append(len(inflight))
-        B.step()
-        now = time.perf_counter() - t0
-        for slot in B.done_slots():
-            r, w, x = inflight.pop(slot)
-            ph, tag, info = B.slot(slot)
-            lat[r] = now - reqs[r][0]
-            B.retire(slot)
-            free_x[w].append(x)
-            done += 1
-    makespan = time.perf_counter() - t0 - reqs[0][0]
+
+    B = lfx.Batch(ctx, 6, 64, reserve_bytes=4 << 30, iters=4)
+
+    def serve():
+        pending, inflight, lat, lat_adm, done = list(range(nreq)), {}, [0.0] * nreq, [0.0] * nreq, 0
+        occupancy, refused = [], 0
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        while done < nreq:
+            now = time.perf_counter() - t0
+            while pending and reqs[pending[0]][0] <= now:
+                r = pending[0]
+                _, w, tol = reqs[r]
+                sy = systems[w]
+                bv, xv = pair(w)
+                bv.import_field_async(bh[r])
+                xv.set_scalar(0.0)
+                slot = B.admit(sy.ops[lfx.R64], sy.ops[lfx.R32], sy.prec32, bv, xv, tol, 20000, r)
+                if slot is None:  # no slot or no memory: wait for a retirement
+                    free[w].append((bv, xv))
+                    refused += 1
+                    break
+                inflight[slot] = (r, w, bv, xv, time.perf_counter() - t0)
+                pending.pop(0)
+            if not inflight:
+                if pending:
+                    time.sleep(max(0.0, reqs[pending[0]][0] - (time.perf_counter() - t0)))
+                continue
+            occupancy.append(len(inflight))
+            B.step()
+            for slot in B.done_slots():
+                r, w, bv, xv, t_adm = inflight.pop(slot)
+                ph, tag, info = B.slot(slot)
+                assert info.status == 0, info.as_dict()
+                xv.export_field(out=xh[r])
+                now = time.perf_counter() - t0
+                lat[r] = now - reqs[r][0]
+                lat_adm[r] = now - t_adm
+                B.retire(slot)
+                free[w].append((bv, xv))
+                done += 1
+        return time.perf_counter() - t0 - reqs[0][0], lat, lat_adm, occupancy, refused
+
+    serve()  # warm-up: the device vectors of the busiest moment exist afterwards
+    makespan, lat, lat_adm, occupancy, refused = serve()
+    err = [float(np.linalg.norm(xh[r] - x64[r]) / np.linalg.norm(x64[r])) for r in range(nreq)]
     pct = lambda v, q: round(1e3 * float(np.percentile(v, q)), 3)
     return {
-        "workload": f"{nreq} W2 Helmholtz requests, Poisson 2000/s, 12-operator pool C12-C96 x "
-                    "20-70 levels, tol 1e-10..1e-6, continuous batching (FP32 PCG + FP64 "
-                    "reliable updates, column preconditioner)",
-        "solves_per_s": round(nreq / makespan, 2), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+        "workload": f"{nreq} W2 Helmholtz requests, Poisson 2000/s, each with its own operator "
+                    f"({npool} distinct seeded geometries C12-C96 x 20-70 levels) and right-hand "
+                    "side (copied in at admission, solution copied out at completion), tol "
+                    "1e-10..1e-6, continuous batching (FP32 PCG + FP64 reliable updates, column "
+                    "preconditioner), admission by free device memory (4 GiB reserve)",
+        "solves_per_s": round(nreq / makespan, 2),
+        "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+        "admission_to_completion_p50_ms": pct(lat_adm, 50),
+        "admission_to_completion_p99_ms": pct(lat_adm, 99),
         "mean_inflight": round(float(np.mean(occupancy)), 2) if occupancy else 0,
+        "max_inflight": int(max(occupancy)) if occupancy else 0,
+        "admissions_deferred": refused,
         "serial_fp64_solves_per_s": round(nreq / serial_makespan, 2),
         "serial_fp64_p50_ms": pct(lat_serial, 50), "serial_fp64_p99_ms": pct(lat_serial, 99),
         "serial_fp64_mean_service_ms": round(1e3 * float(np.mean(service)), 3),
         "speedup_vs_serial_fp64": round(serial_makespan / makespan, 3),
+        "error_vs_fp64_max": max(err), "error_vs_fp64_median": float(np.median(err)),
+        "error_reference": "each request's serial FP64 device CG solution (that solve equals "
+                           "the oracle's bit for bit in the parity tests)",
+        "setup_s": round(setup_s, 1),
     }
 
 
@@ -471,10 +553,10 @@ def cpu_baseline(problem, nsolves):
                             p.nlayers, prm)
     P = orc.Preconditioner.cma(p.ncell_2d, prm["nrow"], 3, p.map[:, 4], prm["indirection"], band,
                                op.diagonal(), p.undf)
-    times, info = [], None
+    times, info, x_oracle = [], None, None
     for _ in range(nsolves):
         t0 = time.perf_counter()
-        _, info = orc.solve("gmres", op, P, p.rhs, r_tol=RTOL, max_iter=200, gcrk=GCRK)
+        x_oracle, info = orc.solve("gmres", op, P, p.rhs, r_tol=RTOL, max_iter=200, gcrk=GCRK)
         times.append(time.perf_counter() - t0)
     cores = os.cpu_count()
     # and one solve on a single thread
@@ -489,7 +571,7 @@ def cpu_baseline(problem, nsolves):
                       "on 1 thread",
             "p50_ms": 1e3 * statistics.median(times),
             "one_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1},
-            "cpu_model": cpu_model()}
+            "cpu_model": cpu_model(), "_x": x_oracle}
 
 
 def cpu_model():
@@ -531,6 +613,7 @@ def run_reference(args):
     steps = min(steps, 20)
     cb = cpu_baseline(p, warm) if warm else None
     cb = cpu_baseline(p, steps)
+    cb.pop("_x", None)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "solves/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": 1e3 / cb["value"], "higher_is_better": True, "scaling": "weak",
@@ -774,15 +857,34 @@ def main():
                               "avg_launch_us": round(1e3 * avg64, 2), "launches_timed": n64m,
                               "algorithmic_bytes": bytes64}
 
-    cb = None
+    cb, x_oracle = None, None
     if world == 1 and not args.no_cpu:
         cb = cpu_baseline(p, args.cpu_sample)
+        x_oracle = cb.pop("_x")
+    # the headline's solutions against the oracle's FP64 GMRES solution of the
+    # same system (the mixed one within its 1e-8 residual; the plain FP64 one
+    # bit for bit)
+    oracle_check = None
+    if x_oracle is not None:
+        X.set_scalar(0.0)
+        mixed.apply(X, B)
+        xm = X.export_field()
+        X.set_scalar(0.0)
+        fp64.apply(X, B)
+        xf = X.export_field()
+        on = np.linalg.norm(x_oracle)
+        oracle_check = {
+            "mixed_error_vs_fp64_oracle": float(np.linalg.norm(xm - x_oracle) / on),
+            "fp64_bitwise_equal_to_oracle": bool(np.array_equal(xf.view(np.int64),
+                                                                x_oracle.view(np.int64))),
+            "e2e_error_vs_fp64_oracle": float(np.linalg.norm(host["x"] - x_oracle) / on),
+            "e2e_tolerance": E2E_TOL}
     extra = {}
     if not args.quick:
         extra["plain_cg_w0"] = leg_plain_cg(ctx, lfx, mg, wl, torch, stream)
         extra["multi_rhs_w0"] = leg_multi_rhs(ctx, lfx, mg, wl, torch, stream)
         extra["batched_uneven_w0"] = leg_batched(ctx, lfx, mg, wl, torch, stream)
-        extra["serving_w2"] = leg_serving(ctx, lfx, mg, wl)
+        extra["serving_w2"] = leg_serving(ctx, lfx, mg, wl, torch)
 
     def pct(v, q):
         return float(np.percentile(np.array(v), q))
@@ -814,7 +916,10 @@ def main():
                 "h2d_bytes_per_step": p.undf * 8, "d2h_bytes_per_step": p.undf * 8,
                 "p50_ms": round(pct(e["lat"], 50), 4),
                 "copies": "async on a copy stream, double-buffered (overlap the neighbouring solves)",
-                "solution_checked": bool(np.allclose(host["x"], host["x2"], rtol=1e-6, atol=1e-12))},
+                "solution_checked": (None if oracle_check is None else
+                                     oracle_check["e2e_error_vs_fp64_oracle"] <= E2E_TOL),
+                "solution_reference": "the oracle's FP64 GMRES solution of the same system"},
+        "error_vs_fp64_oracle": oracle_check,
         "gpu_launches": mx["launches"],
         "clocks": clk.summary(),
         "workloads": extra,

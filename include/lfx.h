@@ -122,6 +122,13 @@ int lfx_lma_create_like(const lfx_op* src, const double* local_stencil, int32_t 
                         lfx_op** out);
 int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y);
 int lfx_op_destroy(lfx_op* op);
+/* operator_x_plus_ay (components/science/source/kernel/algebra/
+ * sci_operator_algebra_kernel_mod.F90:92-119): a new operator x + a y, entry
+ * by entry (each entry one fma, as the oracle computes it), for two operators
+ * of one precision sharing one layout (made from one another by
+ * lfx_lma_create_like, e.g. the mass matrix and tau D^T D); the result shares
+ * that layout. An FP32 pair sums in FP32. */
+int lfx_lma_sum(const lfx_op* x, double a, const lfx_op* y, lfx_op** out);
 /* Apply autotuner (no counterpart in the reference, whose loop shape is fixed
  * by PSyclone): times each launch configuration of the apply on this
  * operator -- the register gather, the register gather with prefetched
@@ -381,33 +388,67 @@ int lfx_ctx_check_device_error(lfx_ctx* ctx);
 
 /* ------------------------------------------------------------------ batched solves
  * Continuous batching of many independent SPD solves (no counterpart in the
- * reference, which solves one system per call). Each slot runs preconditioned
- * CG in FP32 with the solution accumulated in FP64 and reliable updates: the
- * true residual b - A x is recomputed with the FP64 operator whenever the
- * FP32 residual has dropped by 1e-3 since the last one, and a slot converges
- * only when ||b - A x|| / ||b - A x0|| <= tol. Every kernel covers all
- * admitted slots, and one CUDA graph replays `iters_per_launch`
- * super-iterations for the whole batch; a slot's result does not depend on
- * the other slots. The pools (max_dofs unknowns in total, max_entities dof
- * columns, max_columns preconditioner columns) are allocated at creation:
- * admission allocates nothing and fails with LFX_OUT_OF_MEMORY when they are
- * full. ndf is 8 (W0) or 6 (W2) for every slot of a batch. */
+ * reference, which solves one system per call: each slot replaces one
+ * cg_solve of sci_iterative_solver_mod.f90:495-592). Each slot runs
+ * preconditioned CG in FP32 with the solution accumulated in FP64 and
+ * reliable updates: the true residual b - A x is recomputed with the FP64
+ * operator whenever the FP32 residual has dropped by 1e-3 since the last one,
+ * and a slot converges only when ||b - A x|| / ||b - A x0|| <= tol.
+ * One CUDA graph replay is ONE persistent (cooperative) kernel launch that
+ * runs `iters_per_launch` super-iterations of every admitted slot, phase by
+ * phase with grid-wide barriers; the operator apply is the reference's
+ * coloured cell loop over each slot's packed FP32 local matrices (the FP64
+ * ones for the true residuals). A slot's result does not depend on the other
+ * slots or on the launch shape. Admission allocates the slot's Krylov state
+ * (28 bytes per dof) from the device's stream-ordered memory pool and is
+ * refused (LFX_OUT_OF_MEMORY) while it would leave less than reserve_bytes of
+ * device memory free, or when all max_slots slots are taken. Every slot of a
+ * batch has ndf 8 (W0) or 6 (W2) dofs per cell. A bounded wait that runs out
+ * returns LFX_TIMEOUT from lfx_batch_step; the batch must then be destroyed. */
 typedef struct lfx_batch lfx_batch;
-int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t max_dofs,
-                     int64_t max_entities, int64_t max_columns, int32_t iters_per_launch,
-                     lfx_batch** out);
+int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t reserve_bytes,
+                     int32_t iters_per_launch, lfx_batch** out);
 int lfx_batch_destroy(lfx_batch* b);
-/* op64/op32: FP64 and FP32 copies of one operator (lfx_lma_create_like);
- * prec32: its FP32 Jacobi or column preconditioner; b, x: FP64 vectors kept
- * alive until the slot is retired (x: initial guess in, solution out). */
+/* op64/op32: FP64 and FP32 copies of one symmetric operator on one dofmap
+ * (lfx_lma_create_like), which therefore carry the packed cell-scatter
+ * copies; prec32: its FP32 Jacobi or column preconditioner; b, x: FP64
+ * vectors kept alive, with the operators, until the slot is retired (x:
+ * initial guess in, solution out). */
 int lfx_batch_admit(lfx_batch* b, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, const lfx_vec* rhs,
                     lfx_vec* x, double tol, int32_t max_iter, int64_t tag, int32_t* slot);
-/* one graph replay for every slot; *ndone = slots done and not yet retired */
+/* one graph replay (one kernel launch) for every slot; *ndone = slots done
+ * and not yet retired */
 int lfx_batch_step(lfx_batch* b, int32_t* ndone);
-/* phase: 0 empty, 1 starting, 2 iterating, 3 done; info as lfx_solve_info */
+/* phase: 0 empty, 1 starting, 2 iterating, 3 done; info as lfx_solve_info
+ * (iterations = CG iterations, outer_iterations = true residuals taken) */
 int lfx_batch_slot_info(const lfx_batch* b, int32_t slot, int32_t* phase, int64_t* tag,
                         lfx_solve_info* info);
 int lfx_batch_retire(lfx_batch* b, int32_t slot);
+/* launch shape of the persistent kernel: cell columns per apply work item
+ * (the colour block), blocks per SM, and the bytes of vectors of one L2 group
+ * of slots (slots of a group run their colour phases together, so their
+ * vectors stay in L2 across the colours) */
+typedef struct {
+  int32_t cells_per_item;
+  int32_t blocks_per_sm;
+  int32_t grid;
+  int32_t cooperative;      /* 1: cooperative launch inside the graph      */
+  int64_t group_bytes;
+  int64_t replays;          /* graph replays (kernel launches) so far       */
+  float us_per_iteration;   /* the tuner's best time per super-iteration   */
+} lfx_batch_tuning;
+/* Batch autotuner: times one replay of `iters` super-iterations per candidate
+ * shape on the admitted slots (these replays advance the solves, which do not
+ * depend on the shape) -- blocks per SM, then 32/64/128 columns per item,
+ * then L2 groups of a quarter, half, all of L2 or one group -- and keeps the
+ * fastest. */
+int lfx_batch_autotune(lfx_batch* b, int32_t iters, lfx_batch_tuning* out);
+int lfx_batch_get_tuning(const lfx_batch* b, lfx_batch_tuning* out);
+/* pin a launch shape (cells_per_item a multiple of 32, at most 128) */
+int lfx_batch_set_tuning(lfx_batch* b, int32_t cells_per_item, int32_t blocks_per_sm,
+                         int64_t group_bytes);
+/* upper bound in seconds of one grid-barrier wait (default 2) */
+int lfx_batch_set_wait_limit(lfx_batch* b, double seconds);
 
 /* ------------------------------------------------------------------ many right-hand sides
  * One operator applied to, and solved for, nrhs right-hand sides at once (no

@@ -1,29 +1,55 @@
 // Batched, continuously admitted mixed-precision solves of many independent
 // SPD systems (the W0 mass+diffusion and W2 Helmholtz operators are both SPD,
-// with SPD Jacobi / column-tridiagonal preconditioners).
+// with SPD Jacobi / column-tridiagonal preconditioners), run by ONE persistent
+// kernel per CUDA graph replay.
 //
 // Algorithm per slot: preconditioned CG whose recurrences, operator apply and
 // preconditioner run in FP32, with reliable updates: the steps accumulate in
 // an FP32 correction; when the FP32 recursive residual has fallen by a factor
-// delta since the last true residual (or reaches the tolerance), the
+// kDelta since the last true residual (or reaches the tolerance), the
 // correction is added to the FP64 solution and the true residual b - A x is
 // recomputed with the FP64 operator and replaces it. A slot converges only on
 // that FP64 true residual, ||b - A x|| / ||b - A x0||.
 //
-// Batching: every kernel covers all slots -- entity columns, 8192-element
-// chunks and CMA columns come from device work lists of (slot, item) pairs --
-// and reads per-slot pointers and state from device tables, so one CUDA graph
-// of `iters` super-iterations serves any set of admitted slots. Slots whose
-// phase does not call for a kernel skip its items. Per-slot reductions sum in
-// a fixed order (lanes, then warps, then chunks), with a completion ticket per
-// slot, so a slot's result is bit-identical whatever else is in the batch.
-// Vectors and list regions come from pools sized at creation: admitting a
-// request allocates nothing, and is refused when the pools are full.
+// One launch (cooperative: every block resident, so the grid-wide phase
+// barriers cannot wait on a block that never runs) loops over `iters`
+// super-iterations. Each super-iteration is a fixed sequence of phases, every
+// phase covering all admitted slots through host-built work lists and ending
+// at a grid barrier whose spin is bounded in time (a run-out sets an error
+// flag, and every block leaves at its next barrier):
+//   A   z = A32 p: the cell scatter of the reference's colour loop
+//       (matrix_vector_kernel_mod.F90:107-140) over each slot's packed FP32
+//       upper triangles, one phase per colour and per L2 group of slots (the
+//       slots of one group keep p and the partial sums of z in L2 across
+//       their four colours); the last writer of every dof adds p_i z_i to the
+//       slot's <p, z>, whose last item sets alpha
+//   U   xc += alpha p, r -= alpha z, ||r||^2 (and, for a Jacobi slot, <r, r/d>
+//       and beta); a slot whose residual fell by kDelta, reached its
+//       tolerance or its iteration limit asks for a true residual
+//   R   (only when some slot asked, or was just admitted) x += xc; the FP64
+//       residual b - A64 x by the same cell scatter on the FP64 packed
+//       triangles; r = r64, ||r64||, convergence
+//   C   (slots with a column preconditioner) Thomas sweeps of the columns,
+//       then z = r / d on the other rows with <r, z> and beta
+//   P   p = z + beta p
+// Work items: apply items of up to `cells_per_item` cell columns of one
+// colour of one slot; 8192-value chunk items (slot, chunk) for the vector
+// phases; 64-column items for the sweeps. Per-slot sums are reduced in an
+// order fixed by the slot alone (32-column dot blocks, 8192-value chunks,
+// then in index order), so a slot's result is bit-identical whatever else is
+// in the batch and whatever launch shape the autotuner picks.
+//
+// Memory: a slot's Krylov state (r64 FP64; r, p, z, xc FP32; its partial
+// sums) is allocated at admission from the device's stream-ordered memory
+// pool, and admission is refused while the device's free memory would drop
+// under the batch's reserve. The operators, preconditioners and b, x belong
+// to the caller and stay alive until the slot is retired.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
-#include <type_traits>
+#include <map>
+#include <vector>
 
 #include "lfx_internal.cuh"
 
@@ -33,23 +59,41 @@ namespace {
 
 enum { PH_EMPTY = 0, PH_INIT = 1, PH_RUN = 2, PH_DONE = 3 };
 
+constexpr double kDelta = 1e-3;  // reliable update when ||r|| drops by this factor
+constexpr int kBT = 256;         // threads per block of the persistent kernel
+constexpr int kBW = kBT / 32;    // warps per block
+constexpr int kBSub = 4;         // a chunk item: kBSub chunks of RCHUNK values
+constexpr int kDotCols = 32;     // cell columns per partial sum of <p, A p>
+constexpr int kMaxIters = 64;    // super-iterations per launch, at most
+constexpr int kMaxSeg = 4;       // warps (segments of <= 31 levels) per cell column, at most
+constexpr int kMaxCB = 128;      // cell columns per apply item, at most
+constexpr int kMaxUnits = kMaxCB * kMaxSeg;
+constexpr int kBCols = 64;       // columns per sweep item
+constexpr int kBRows = 160;      // rows per preconditioner column, at most
+
+inline int64_t bchunks(int64_t n) {
+  return (n + (int64_t)kBSub * RCHUNK - 1) / ((int64_t)kBSub * RCHUNK);
+}
+
 struct BSlot {
-  // operator (gather layout shared by the FP32 and FP64 copies)
-  const int4* ent_pack;
-  const int32_t* grp_pack;
-  const float* M32;
-  const double* M64;
-  int32_t gp_stride, nent, nl, ndf1;
-  int32_t blk32, blk64, nch, part_off;
+  // cell scatter: packed upper triangles [q][p][k] in the colour-loop order
+  // (block stride sblk elements) and the per-cell descriptors {map row,
+  // flags, partners} in the same order
+  const float* S32;
+  const double* S64;
+  const int* cdesc;
+  int32_t sblk32, sblk64, cdints, nl;
+  int32_t nseg, segL, nch, ndot;
+  int32_t nitem32, cma, ncol, nrow;
   int64_t n;
-  // preconditioner: Jacobi diag (all rows) and, for the line kind, Thomas
-  // factors [row][column] on the columns
+  double* part;  // [0, 2 nch): chunk sums; [2 nch, 2 nch + ndot): apply dots
+  // preconditioner: FP32 Jacobi diagonal (zero on the column rows of a
+  // column preconditioner) and the Thomas factors [row][column]
   const float* diag;
   const float *fa, *finv, *fc;
-  const int32_t *first, *ind;
-  int32_t ncol, nrow;
-  // vectors: x (FP64) moves only at true residuals; between them the FP32
-  // xc accumulates the steps, x += xc then (a reliable update)
+  const int *first, *ind;
+  // vectors: x (FP64, the caller's) moves only at true residuals; between
+  // them the FP32 xc accumulates the steps
   const double* b;
   double* x;
   double* r64;
@@ -58,56 +102,335 @@ struct BSlot {
 
 struct BState {
   int phase, flag, iter, status;
-  int max_iter, fresh, pad0, pad1;
+  int max_iter, fresh, resid, pad;
   double tol, r0, rlast, rnorm, rz, alpha, beta, true_rel;
 };
 
-constexpr double kDelta = 1e-3;  // reliable update when ||r|| drops by this factor
+// device-resident launch parameters (the graph's kernel takes their address,
+// so lists can be rebuilt and reallocated between replays)
+struct BParams {
+  const int4* items32;  // FP32 apply items {slot, q0, columns, first dot block}
+  const int* off32;     // [4 * ngr32 + 1]: items of group g, colour c from off32[4g + c]
+  const int4* items64;  // FP64 residual items {slot, q0, columns, 0}
+  const int* off64;
+  const int2* chunks;   // {slot, chunk}
+  const int2* cols;     // {slot, column}
+  const BSlot* slots;
+  BState* st;
+  unsigned* tickets;
+  int* need;            // [kMaxIters]: a slot takes a true residual in super-iteration it
+  unsigned* bar;        // grid barrier {count, generation}
+  int* err;             // LFX_TIMEOUT when a wait ran out
+  int ngr32, ngr64, nchunk, ncolitem;
+  int iters, max_slots, any_cma, pad;
+  unsigned long long timeout_ns;
+};
 
-__device__ __forceinline__ bool ph_run(const BState& s) { return s.phase == PH_RUN; }
-__device__ __forceinline__ bool ph_resid(const BState& s) {
-  return s.phase == PH_INIT || (s.phase == PH_RUN && s.flag);
+struct BShared {
+  BSlot slot;
+  BState state;
+  int skip, last, s;
+  int4 item;
+  double unit[kMaxUnits];
+  double red[kBT / 32];
+  int ok;
+};
+
+__device__ __forceinline__ bool ph_run(int ph) { return ph == PH_RUN; }
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
-__device__ __forceinline__ bool ph_active(const BState& s) {
-  return s.phase == PH_INIT || s.phase == PH_RUN;
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acqrel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
 }
 
-// values of one batched chunk item: kBSub chunks of RCHUNK
-constexpr int kBSub = 4;
-inline int64_t bchunks(int64_t n) { return (n + (int64_t)kBSub * RCHUNK - 1) / ((int64_t)kBSub * RCHUNK); }
+// (each phase below is a separate, non-inlined function: the kernel's loop
+// then keeps nothing of one phase live across the others, and no phase
+// spills registers)
+//
+// Grid-wide barrier of a cooperative launch. Thread 0 of each block reads the
+// generation, arrives, and the last to arrive resets the count and releases
+// the next generation; the others spin on it for at most timeout_ns (and stop
+// at once when another block has reported an error). Returns false when the
+// block must leave the kernel.
+__device__ bool grid_sync(const BParams& P, BShared& sh) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned gen = ld_acquire(P.bar + 1);
+    __threadfence();
+    const unsigned arrived = atom_add_acqrel(P.bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      P.bar[0] = 0u;
+      st_release(P.bar + 1, gen + 1u);
+    } else {
+      const unsigned long long t0 = gtimer();
+      while (ld_acquire(P.bar + 1) == gen) {
+        if (*(volatile int*)P.err) {
+          ok = 0;
+          break;
+        }
+        if (gtimer() - t0 > P.timeout_ns) {
+          atomicExch(P.err, (int)LFX_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+    if (*(volatile int*)P.err) ok = 0;
+    sh.ok = ok;
+  }
+  __syncthreads();
+  return sh.ok != 0;
+}
 
-// Batched chunk kernel: items are (slot, chunk); ld/op as in chunk_kernel but
-// with the slot's descriptor; fin(slot desc, state, tot) runs once per slot
-// after all its chunks. A non-null gate that reads zero skips the launch; a
-// non-null reset is cleared by the first thread.
+// block sum in a fixed order (lane butterfly, then warps left to right);
+// result valid in thread 0
+__device__ __forceinline__ double bsum(double acc, double* red) {
+  acc = warp_butterfly(acc);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = acc;
+  __syncthreads();
+  double tot = 0.0;
+  if (threadIdx.x == 0) {
+    tot = red[0];
+#pragma unroll
+    for (int i = 1; i < kBW; ++i) tot = tot + red[i];
+  }
+  __syncthreads();
+  return tot;
+}
+
+// the slot record and state of a work item, copied to shared memory by the
+// block (the record is read-only during a launch; the state is read through
+// L2, since other blocks write it)
+__device__ __forceinline__ void load_item(const BParams& P, BShared& sh, int s) {
+  const int* src = reinterpret_cast<const int*>(P.slots + s);
+  int* dst = reinterpret_cast<int*>(&sh.slot);
+  constexpr int NW = sizeof(BSlot) / 4;
+  for (int i = threadIdx.x; i < NW; i += kBT) dst[i] = __ldg(src + i);
+  const int* ss = reinterpret_cast<const int*>(P.st + s);
+  int* sd = reinterpret_cast<int*>(&sh.state);
+  constexpr int NS = sizeof(BState) / 4;
+  for (int i = threadIdx.x; i < NS; i += kBT) sd[i] = __ldcg(ss + i);
+}
+
+// a slot's state as one thread sees it in L2 (other blocks write it)
+__device__ __forceinline__ void copy_state_in(BState* d, const BState* s) {
+  const int* a = reinterpret_cast<const int*>(s);
+  int* b = reinterpret_cast<int*>(d);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(BState) / 4); ++i) b[i] = __ldcg(a + i);
+}
+__device__ __forceinline__ void copy_state_out(BState* d, const BState& s) {
+  const int* a = reinterpret_cast<const int*>(&s);
+  int* b = reinterpret_cast<int*>(d);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(BState) / 4); ++i) __stcg(b + i, a[i]);
+}
+
+template <int N>
+__host__ __device__ constexpr int pidx(int i, int j) {
+  return i <= j ? i * N - i * (i - 1) / 2 + (j - i) : j * N - j * (j - 1) / 2 + (i - j);
+}
+
+// One warp's share of the cell scatter: segment sg (L <= 31 output levels)
+// of the cell column at colour-loop position q. Lane l (1 <= l <= L) holds
+// level k = sg L + l - 1 and writes the dofs of that level (and the bottom
+// dof of a pair, whose upper-record terms come from the lane below); lane 0
+// holds the level below the segment only to supply those terms. A dof gets
+// its terms in the reference's colour order: the first cell on its column
+// starts from zero, later ones from the stored sum, and in the residual form
+// the last writes b - sum. With DOT the lane returns the sum of p_i y_i over
+// the dofs it finished (the last writer of each dof).
+template <class T, int NDF, bool RESID, bool DOT>
+__device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const int* __restrict__ dsc,
+                                               int nl, int L, int sg, int lane,
+                                               const T* x, T* y, const double* __restrict__ b) {
+  int mf[NDF];
+#pragma unroll
+  for (int j = 0; j < NDF; ++j) mf[j] = __ldg(dsc + j);
+  const uint32_t flags = (uint32_t)__ldg(dsc + NDF), part = (uint32_t)__ldg(dsc + NDF + 1);
+  const int k = sg * L + lane - 1;
+  const bool own = lane >= 1 && lane <= L;
+  const bool v = k >= 0 && k < nl && lane <= L;
+  const T* Mc = Mq + (v ? k : 0);
+  constexpr int NP = NDF * (NDF + 1) / 2;
+  T m[NP], xv[NDF], yo[NDF];
+  // the matrix is read once per apply (streaming loads); x and the partial
+  // sums of y are written during the launch, so they are read through L2
+#pragma unroll
+  for (int p = 0; p < NP; ++p) m[p] = v ? __ldcs(Mc + p * nl) : T(0);
+#pragma unroll
+  for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldcg(x + mf[j] + k) : T(0);
+#pragma unroll
+  for (int df = 0; df < NDF; ++df) {
+    const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+    const bool opens = (flags >> df) & 1u;
+    const bool live = own && (lower ? k <= nl : v);
+    yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + k) : T(0);
+  }
+  double dot = 0.0;
+#define MV(i, j) m[pidx<NDF>(i, j)]
+#pragma unroll
+  for (int df = 0; df < NDF; ++df) {
+    if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
+    const bool last = (flags >> (24 + df)) & 1u;
+    if ((flags >> (8 + df)) & 1u) {
+      const int bsel = (part >> (4 * df)) & 15u;
+#pragma unroll
+      for (int bb = df + 1; bb < NDF; ++bb) {
+        if (bb != bsel) continue;
+        T acc = yo[df];
+#pragma unroll
+        for (int j = 0; j < NDF; ++j) {
+          const T mb = __shfl_up_sync(0xffffffffu, MV(bb, j), 1);
+          const T xb = __shfl_up_sync(0xffffffffu, xv[j], 1);
+          if (v) acc = fmaT(MV(df, j), xv[j], acc);
+          if (own && k >= 1 && k <= nl) acc = fmaT(mb, xb, acc);
+        }
+        if (own && k <= nl) {
+          const int row = mf[df] + k;
+          if (RESID && last)
+            __stcg(y + row, (T)(b[row] - (double)acc));
+          else
+            __stcg(y + row, acc);
+          if (DOT && last) {
+            const T pr = k < nl ? xv[df] : __ldcg(x + row);
+            dot = fma((double)pr, (double)acc, dot);
+          }
+        }
+      }
+    } else {
+      T acc = yo[df];
+#pragma unroll
+      for (int j = 0; j < NDF; ++j) acc = fmaT(MV(df, j), xv[j], acc);
+      if (own && v) {
+        const int row = mf[df] + k;
+        if (RESID && last)
+          __stcg(y + row, (T)(b[row] - (double)acc));
+        else
+          __stcg(y + row, acc);
+        if (DOT && last) dot = fma((double)xv[df], (double)acc, dot);
+      }
+    }
+  }
+#undef MV
+  return dot;
+}
+
+// The apply items [i0, i1) of one (group, colour) phase. FP32 (DOT): z = A32 p
+// for running slots, with <p, z> per 32-column block and alpha from the
+// slot's last item. FP64 (RESID): r64 = b - A64 x for slots taking a true
+// residual.
+template <int NDF, bool FP64>
+__device__ __noinline__ void apply_phase(const BParams& P, BShared& sh, const int4* __restrict__ items, int i0,
+                            int i1) {
+  using T = typename std::conditional<FP64, double, float>::type;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int u = i0 + blockIdx.x; u < i1; u += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int4 it = __ldg(items + u);
+      sh.item = it;
+      const int ph = __ldcg(&P.st[it.x].phase), fl = __ldcg(&P.st[it.x].flag);
+      sh.skip = FP64 ? !(ph == PH_INIT || (ph == PH_RUN && fl)) : !ph_run(ph);
+    }
+    __syncthreads();
+    if (sh.skip) continue;
+    const int s = sh.item.x;
+    load_item(P, sh, s);
+    __syncthreads();
+    const BSlot& D = sh.slot;
+    const int q0 = sh.item.y, nq = sh.item.z;
+    const int nseg = D.nseg, L = D.segL, nl = D.nl;
+    const int nunits = nq * nseg;
+    const T* M = FP64 ? (const T*)D.S64 : (const T*)D.S32;
+    const int sblk = FP64 ? D.sblk64 : D.sblk32;
+    const T* x = FP64 ? (const T*)D.x : (const T*)D.p;
+    T* y = FP64 ? (T*)D.r64 : (T*)D.z;
+    for (int w = warp; w < nunits; w += kBW) {
+      const int q = q0 + w / nseg, sg = w % nseg;
+      const double c = scatter_unit<T, NDF, FP64, !FP64>(M + (size_t)q * sblk,
+                                                         D.cdesc + (size_t)q * D.cdints, nl, L, sg,
+                                                         lane, x, y, D.b);
+      if (!FP64) {
+        const double cw = warp_butterfly(c);
+        if (lane == 0) sh.unit[w] = cw;
+      }
+    }
+    if (!FP64) {
+      __syncthreads();
+      // one partial per 32-column block, units in order
+      const int ndb = (nq + kDotCols - 1) / kDotCols;
+      if (threadIdx.x < ndb) {
+        const int a0 = threadIdx.x * kDotCols * nseg;
+        const int a1 = min((threadIdx.x + 1) * kDotCols, nq) * nseg;
+        double a = 0.0;
+        for (int w = a0; w < a1; ++w) a = a + sh.unit[w];
+        __stcg(D.part + 2 * (int64_t)D.nch + sh.item.w + threadIdx.x, a);
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) sh.last = (atomicAdd(&P.tickets[s], 1u) == (unsigned)D.nitem32 - 1u);
+      __syncthreads();
+      if (sh.last) {
+        __threadfence();
+        double a = 0.0;
+        for (int i = threadIdx.x; i < D.ndot; i += kBT) a = a + __ldcg(&D.part[2 * (int64_t)D.nch + i]);
+        const double pz = bsum(a, sh.red);
+        if (threadIdx.x == 0) {
+          BState S;
+          copy_state_in(&S, P.st + s);
+          S.alpha = S.rz / pz;
+          S.fresh = 0;
+          copy_state_out(P.st + s, S);
+          P.tickets[s] = 0u;
+        }
+      }
+    }
+  }
+}
+
+// Chunk phase: items (slot, chunk); ld/op as in chunk_kernel with the slot's
+// record and state; fin(state, tot) runs once per slot after all its chunks.
 template <int NR, class Pred, class Ld, class Op, class Fin>
-__global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, const BSlot* slots,
-                                            BState* st, double* partials, unsigned* tickets,
-                                            const int* gate, int* reset, Pred pred, Ld ld, Op op,
-                                            Fin fin) {
-  __shared__ double sm[RT / 32];
-  __shared__ int am_last;
-  if (gate && !*((volatile const int*)gate)) return;
-  if (reset && blockIdx.x == 0 && threadIdx.x == 0) *reset = 0;
-  const int L = *len;
-  for (int u = blockIdx.x; u < L; u += gridDim.x) {
-    const int2 w = list[u];
-    if (w.x < 0) continue;
-    BState& Sg = st[w.x];
-    if (!pred(Sg)) continue;
-    // local copies: the element loop's stores cannot alias them, so pointers
-    // and scalars stay in registers
-    const BSlot D = slots[w.x];
-    const BState S = Sg;
+__device__ __noinline__ void chunk_phase(const BParams& P, BShared& sh, Pred pred, Ld ld, Op op, Fin fin) {
+  for (int u = blockIdx.x; u < P.nchunk; u += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int2 w = __ldg(P.chunks + u);
+      sh.item = make_int4(w.x, w.y, 0, 0);
+      sh.skip = !pred(__ldcg(&P.st[w.x].phase), __ldcg(&P.st[w.x].flag));
+    }
+    __syncthreads();
+    if (sh.skip) continue;
+    const int s = sh.item.x, ch = sh.item.y;
+    load_item(P, sh, s);
+    __syncthreads();
+    const BSlot& D = sh.slot;
+    const BState& S = sh.state;
     using V = decltype(ld(D, int64_t(0)));
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-    // an item is kBSub consecutive 2048-value chunks, taken in order, each
-    // with all its loads issued before its stores (one block reduction per
-    // item: the fixed cost of an item is spread over more values)
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
     for (int sub = 0; sub < kBSub; ++sub) {
-      const int64_t base = ((int64_t)w.y * kBSub + sub) * RCHUNK + threadIdx.x;
+      const int64_t base = ((int64_t)ch * kBSub + sub) * RCHUNK + threadIdx.x;
       if (base - threadIdx.x >= D.n) break;
       V v[RPER];
 #pragma unroll
@@ -123,363 +446,94 @@ __global__ void __launch_bounds__(RT) bchunk(const int2* list, const int* len, c
     }
     if constexpr (NR > 0) {
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      const double t = block_sum(acc[r], sm);
-      if (threadIdx.x == 0) partials[D.part_off + (int64_t)r * D.nch + w.y] = t;
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) am_last = (atomicAdd(&tickets[w.x], 1u) == (unsigned)D.nch - 1);
-    __syncthreads();
-    if (am_last) {
-      __threadfence();
-      double tot[NR > 0 ? NR : 1];
-#pragma unroll
       for (int r = 0; r < NR; ++r) {
-        double a = 0.0;
-        for (int i = threadIdx.x; i < D.nch; i += RT)
-          a = a + __ldcg(&partials[D.part_off + (int64_t)r * D.nch + i]);
-        tot[r] = block_sum(a, sm);
+        const double t = bsum(acc[r], sh.red);
+        if (threadIdx.x == 0) __stcg(D.part + (int64_t)r * D.nch + ch, t);
       }
-      if (threadIdx.x == 0) {
-        fin(D, Sg, tot);
-        tickets[w.x] = 0u;
-      }
+      __threadfence();
       __syncthreads();
-    }
-    }
-  }
-}
-
-// Batched LMA apply (register gather), items (slot, entity). RESID: y = b - A64 x
-// with x = slot.x, y = slot.r64; else z = A32 p. A non-null gate that reads
-// zero skips the launch.
-template <int NDF2, bool RESID>
-__global__ void __launch_bounds__(256) bapply(const int2* list, const int* len, const BSlot* slots,
-                                              const BState* st, const int* gate) {
-  using T = typename std::conditional<RESID, double, float>::type;
-  if (gate && !*((volatile const int*)gate)) return;
-  const int lane = threadIdx.x & 31;
-  const int L = *len;
-  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int2 wn = u < L ? list[u] : make_int2(-1, -1);
-  for (; u < L; u += nwarp) {
-    // the next item's list entry is loaded while this one is computed
-    const int2 w = wn;
-    wn = u + nwarp < L ? list[u + nwarp] : make_int2(-1, -1);
-    if (w.x < 0) continue;
-    if (RESID ? !ph_resid(st[w.x]) : !ph_run(st[w.x])) continue;
-    // local copy: the stores below cannot alias it, so the pointers stay in
-    // registers across the column loop
-    const BSlot D = slots[w.x];
-    const T* __restrict__ M = RESID ? (const T*)D.M64 : (const T*)D.M32;
-    const int blk = RESID ? D.blk64 : D.blk32;
-    const T* __restrict__ x = RESID ? (const T*)D.x : (const T*)D.p;
-    T* __restrict__ y = RESID ? (T*)D.r64 : (T*)D.z;
-    const int nl = D.nl;
-    const size_t cell_stride = (size_t)D.ndf1 * blk;
-    const int4 ep = __ldg(D.ent_pack + w.y);
-    // all 32 lanes run every pass so the shuffles below see a converged warp
-    for (int l0 = 0; l0 < ep.y; l0 += 32) {
-      const int l = l0 + lane;
-      T acc = T(0);
-      for (int g = ep.z; g < ep.w; ++g) {
-        // group record {cell, records, map_from row} as 16-byte vectors
-        // (gp_stride is a multiple of 4 ints)
-        const int4* gp4 = reinterpret_cast<const int4*>(D.grp_pack + (size_t)g * D.gp_stride);
-        const int4 h0 = __ldg(gp4);
-        const int c = h0.x;
-        const uint32_t pk = (uint32_t)h0.y;
-        int tmp[8];
-        tmp[0] = h0.z;
-        tmp[1] = h0.w;
-        if (NDF2 > 2) {
-          const int4 h1 = __ldg(gp4 + 1);
-          tmp[2] = h1.x;
-          tmp[3] = h1.y;
-          tmp[4] = h1.z;
-          tmp[5] = h1.w;
+      if (threadIdx.x == 0) sh.last = (atomicAdd(&P.tickets[s], 1u) == (unsigned)D.nch - 1u);
+      __syncthreads();
+      if (sh.last) {
+        __threadfence();
+        double tot[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          double a = 0.0;
+          for (int i = threadIdx.x; i < D.nch; i += kBT) a = a + __ldcg(&D.part[(int64_t)r * D.nch + i]);
+          tot[r] = bsum(a, sh.red);
         }
-        if (NDF2 > 6) {
-          const int4 h2 = __ldg(gp4 + 2);
-          tmp[6] = h2.x;
-          tmp[7] = h2.y;
-        }
-        const int o0 = (pk >> 8) & 7u, o1 = (pk >> 17) & 7u;
-        const int k0 = l - o0, k1 = l - o1;
-        const bool v0 = (unsigned)k0 < (unsigned)nl;
-        if ((pk & 3u) == 1) {
-          // one record (warp-uniform branch): no second-record instructions
-          const T* M0 = M + (size_t)c * cell_stride + (size_t)((pk >> 2) & 63u) * blk + (v0 ? k0 : 0);
-          T a0[NDF2], b0[NDF2];
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
-            b0[j] = v0 ? __ldg(x + tmp[j] + k0) : T(0);
-          }
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j)
-            if (v0) acc = fmaT(a0[j], b0[j], acc);
-          continue;
-        }
-        const bool v1 = (pk & 3u) > 1 && (unsigned)k1 < (unsigned)nl;
-        // second record one level above the first: its x values are the
-        // neighbouring lane's first-record values
-        const bool pair = (pk & 3u) == 2 && o1 == o0 + 1;
-        const T* Mc = M + (size_t)c * cell_stride;
-        const T* M0 = Mc + (size_t)((pk >> 2) & 63u) * blk + (v0 ? k0 : 0);
-        const T* M1 = Mc + (size_t)((pk >> 11) & 63u) * blk + (v1 ? k1 : 0);
-        T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
-#pragma unroll
-        for (int j = 0; j < NDF2; ++j) {
-          a0[j] = v0 ? __ldg(M0 + j * nl) : T(0);
-          b0[j] = v0 ? __ldg(x + tmp[j] + k0) : T(0);
-          a1[j] = v1 ? __ldg(M1 + j * nl) : T(0);
-        }
-        if (pair) {
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            const T up = __shfl_up_sync(0xffffffffu, b0[j], 1);
-            b1[j] = (lane == 0) ? (v1 ? __ldg(x + tmp[j] + k1) : T(0)) : up;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) b1[j] = v1 ? __ldg(x + tmp[j] + k1) : T(0);
-        }
-#pragma unroll
-        for (int j = 0; j < NDF2; ++j) {
-          if (v0) acc = fmaT(a0[j], b0[j], acc);
-          if (v1) acc = fmaT(a1[j], b1[j], acc);
-        }
-      }
-      if (l < ep.y) {
-        const int row = ep.x + l;
-        if (RESID)
-          y[row] = (T)D.b[row] - acc;
-        else
-          y[row] = acc;
-      }
-    }
-  }
-}
-
-// 16-byte asynchronous copies global -> shared and their groups
-__device__ __forceinline__ void bcp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                   (unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void bcp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void bcp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Batched apply for 6-dof cells whose columns read at most two blocks from
-// at most two cells (W2): the per-item column descriptors sit in list order
-// in the batch's own pool (copied at admission), so each warp keeps the
-// descriptors of its next kBFetchDepth items in flight (cp.async ring in
-// shared memory) and an item waits on memory once, for its matrix rows and x
-// values (matrix rows with streaming, evict-first loads). Same sums in the
-// same order as bapply.
-constexpr int kBFetchDepth = 4;
-
-template <bool RESID>
-__global__ void __launch_bounds__(256, RESID ? 2 : 3) bapply_fetch(const int2* list, const int* len,
-                                                                   const BSlot* slots,
-                                                                   const BState* st, const int* gate,
-                                                                   const int* bdesc) {
-  using T = typename std::conditional<RESID, double, float>::type;
-  constexpr int NDF2 = 6, GS = fd_group_ints(NDF2), FS = fd_ints(NDF2), NV = FS / 4;
-  __shared__ __align__(16) int ring[8][kBFetchDepth][FS];
-  if (gate && !*((volatile const int*)gate)) return;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int L = *len;
-  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t e0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-#pragma unroll
-  for (int q = 0; q < kBFetchDepth; ++q) {
-    const int64_t e = e0 + q * nwarp;
-    if (lane < NV && e < L) bcp_async16(&ring[wib][q][4 * lane], bdesc + e * FS + 4 * lane);
-    bcp_commit();
-  }
-  int2 wn = e0 < L ? list[e0] : make_int2(-1, -1);
-  int sl = 0;
-  for (int64_t e = e0; e < L; e += nwarp) {
-    bcp_wait<kBFetchDepth - 1>();
-    __syncwarp();
-    const int2 w = wn;
-    wn = e + nwarp < L ? list[e + nwarp] : make_int2(-1, -1);
-    const int* d = ring[wib][sl];
-    if (w.x >= 0 && (RESID ? ph_resid(st[w.x]) : ph_run(st[w.x]))) {
-      const BSlot* P = slots + w.x;
-      const T* __restrict__ M = RESID ? (const T*)P->M64 : (const T*)P->M32;
-      const int blk = RESID ? P->blk64 : P->blk32;
-      const T* __restrict__ x = RESID ? (const T*)P->x : (const T*)P->p;
-      T* __restrict__ y = RESID ? (T*)P->r64 : (T*)P->z;
-      const double* __restrict__ bv = P->b;
-      const int nl = P->nl;
-      const size_t cell_stride = (size_t)NDF2 * blk;
-      const int base = d[0], h = d[1], ng = d[2];
-      for (int l0 = 0; l0 < h; l0 += 32) {
-        const int l = l0 + lane;
-        T acc = T(0);
-        const uint32_t pk0 = (uint32_t)d[5];
-        const int o0 = (pk0 >> 8) & 7u;
-        const int k0 = l - o0;
-        const bool v0 = (unsigned)k0 < (unsigned)nl;
-        const T* M0 = M + (size_t)d[4] * cell_stride + (size_t)((pk0 >> 2) & 63u) * blk + (v0 ? k0 : 0);
-        if (ng == 2) {
-          const uint32_t pk1 = (uint32_t)d[5 + GS];
-          const int k1 = l - (int)((pk1 >> 8) & 7u);
-          const bool v1 = (unsigned)k1 < (unsigned)nl;
-          const T* M1 = M + (size_t)d[4 + GS] * cell_stride + (size_t)((pk1 >> 2) & 63u) * blk +
-                        (v1 ? k1 : 0);
-          T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
-            a1[j] = v1 ? __ldcs(M1 + j * nl) : T(0);
-          }
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
-            b1[j] = v1 ? __ldg(x + d[6 + GS + j] + k1) : T(0);
-          }
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j)
-            if (v0) acc = fmaT(a0[j], b0[j], acc);
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j)
-            if (v1) acc = fmaT(a1[j], b1[j], acc);
-        } else if ((pk0 & 3u) == 1) {
-          T a0[NDF2], b0[NDF2];
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
-            b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
-          }
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j)
-            if (v0) acc = fmaT(a0[j], b0[j], acc);
-        } else {
-          // one cell, two records (bottom and top of a column)
-          const int o1 = (pk0 >> 17) & 7u;
-          const int k1 = l - o1;
-          const bool v1 = (unsigned)k1 < (unsigned)nl;
-          const bool pair = o1 == o0 + 1;
-          const T* M1 = M + (size_t)d[4] * cell_stride + (size_t)((pk0 >> 11) & 63u) * blk +
-                        (v1 ? k1 : 0);
-          T a0[NDF2], b0[NDF2], a1[NDF2], b1[NDF2];
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            a0[j] = v0 ? __ldcs(M0 + j * nl) : T(0);
-            b0[j] = v0 ? __ldg(x + d[6 + j] + k0) : T(0);
-            a1[j] = v1 ? __ldcs(M1 + j * nl) : T(0);
-          }
-          if (pair) {
-#pragma unroll
-            for (int j = 0; j < NDF2; ++j) {
-              const T up = __shfl_up_sync(0xffffffffu, b0[j], 1);
-              b1[j] = (lane == 0) ? (v1 ? __ldg(x + d[6 + j] + k1) : T(0)) : up;
-            }
-          } else {
-#pragma unroll
-            for (int j = 0; j < NDF2; ++j) b1[j] = v1 ? __ldg(x + d[6 + j] + k1) : T(0);
-          }
-#pragma unroll
-          for (int j = 0; j < NDF2; ++j) {
-            if (v0) acc = fmaT(a0[j], b0[j], acc);
-            if (v1) acc = fmaT(a1[j], b1[j], acc);
-          }
-        }
-        if (l < h) {
-          const int row = base + l;
-          if (RESID)
-            y[row] = (T)bv[row] - acc;
-          else
-            y[row] = acc;
+        if (threadIdx.x == 0) {
+          BState S;
+          copy_state_in(&S, P.st + s);
+          fin(D, S, tot);
+          copy_state_out(P.st + s, S);
+          P.tickets[s] = 0u;
         }
       }
     }
-    __syncwarp();
-    // the slot is free again: fetch the descriptor kBFetchDepth items ahead
-    const int64_t en = e + kBFetchDepth * nwarp;
-    if (lane < NV && en < L) bcp_async16(&ring[wib][sl][4 * lane], bdesc + en * FS + 4 * lane);
-    bcp_commit();
-    sl = sl + 1 == kBFetchDepth ? 0 : sl + 1;
   }
-  bcp_wait<0>();
 }
 
-// Batched column-tridiagonal sweeps (the Jacobi part of the line
-// preconditioner runs in the fused prec+dot chunk kernel), the rows of 64
-// consecutive list items (columns, of any slots) staged through shared memory: one warp per column copies its
-// rows in and out (a column's rows are contiguous dofs, so the copies
-// coalesce), and each thread sweeps its column on the staged copy with the
-// factors read from global memory (coalesced: [row][column]); same arithmetic
-// as thomas_sweep. Admission refuses columns of more than kBRows rows.
-constexpr int kBCols = 64, kBRows = 160, kBThreads = 128;
+// Column sweeps of the line preconditioner for running slots: z = T^{-1} r on
+// the rows of 64 consecutive list items (columns of any slots), staged in
+// shared memory (one warp copies a column's contiguous rows in and out, one
+// thread sweeps a column with the factors read coalesced from [row][column]);
+// the arithmetic of thomas_sweep.
+struct SweepShared {
+  int nrow[kBCols], f[kBCols], maxrow;
+  const int* ind[kBCols];
+  const float* r[kBCols];
+  float* z[kBCols];
+};
 
-__global__ void __launch_bounds__(kBThreads) bthomas_staged(const int2* list, const int* len,
-                                                             const BSlot* slots, const BState* st) {
-  constexpr int LD = kBCols + 1, NW = kBThreads / 32, CPW = kBCols / NW;
-  __shared__ float xs[kBRows * LD];
-  // per column of the chunk: rows (0: nothing to do), first dof, indirection
-  // and the slot's r and z (read once, so the copies below do not wait on
-  // the list and slot records column by column)
-  __shared__ int s_nrow[kBCols], s_f[kBCols];
-  __shared__ const int* s_ind[kBCols];
-  __shared__ const float* s_r[kBCols];
-  __shared__ float* s_z[kBCols];
-  __shared__ int s_maxrow;
+__device__ __noinline__ void sweep_phase(const BParams& P, float* xs, SweepShared& ss) {
+  constexpr int LD = kBCols + 1, CPW = kBCols / kBW;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int L = *len;
-  for (int u0 = blockIdx.x * kBCols; u0 < L; u0 += gridDim.x * kBCols) {
-    if (threadIdx.x == 0) s_maxrow = 0;
+  for (int u0 = blockIdx.x * kBCols; u0 < P.ncolitem; u0 += gridDim.x * kBCols) {
+    __syncthreads();
+    if (threadIdx.x == 0) ss.maxrow = 0;
     __syncthreads();
     if (threadIdx.x < kBCols) {
       const int t = threadIdx.x, u = u0 + t;
       int nrow = 0;
-      if (u < L) {
-        const int2 w = list[u];
-        if (w.x >= 0 && ph_active(st[w.x])) {
-          const BSlot* D = slots + w.x;
+      if (u < P.ncolitem) {
+        const int2 w = __ldg(P.cols + u);
+        if (ph_run(__ldcg(&P.st[w.x].phase))) {
+          // slot records are read-only during a launch
+          const BSlot* D = P.slots + w.x;
           nrow = D->nrow;
-          s_f[t] = __ldg(D->first + w.y);
-          s_ind[t] = D->ind;
-          s_r[t] = D->r;
-          s_z[t] = D->z;
+          ss.f[t] = __ldg(D->first + w.y);
+          ss.ind[t] = D->ind;
+          ss.r[t] = D->r;
+          ss.z[t] = D->z;
         }
       }
-      s_nrow[t] = nrow;
-      atomicMax(&s_maxrow, nrow);
+      ss.nrow[t] = nrow;
+      atomicMax(&ss.maxrow, nrow);
     }
     __syncthreads();
-    const int maxrow = s_maxrow;
-    // stage: lane l copies row r0 + l of the warp's columns, loads first
+    const int maxrow = ss.maxrow;
     for (int r0 = 0; r0 < maxrow; r0 += 32) {
       const int i = r0 + lane;
       float v[CPW];
 #pragma unroll
       for (int k = 0; k < CPW; ++k) {
-        const int j = warp + NW * k;
-        v[k] = i < s_nrow[j] ? s_r[j][s_f[j] + __ldg(s_ind[j] + i)] : 0.0f;
+        const int j = warp + kBW * k;
+        v[k] = i < ss.nrow[j] ? __ldcg(ss.r[j] + ss.f[j] + __ldg(ss.ind[j] + i)) : 0.0f;
       }
 #pragma unroll
       for (int k = 0; k < CPW; ++k) {
-        const int j = warp + NW * k;
-        if (i < s_nrow[j]) xs[i * LD + j] = v[k];
+        const int j = warp + kBW * k;
+        if (i < ss.nrow[j]) xs[i * LD + j] = v[k];
       }
     }
     __syncthreads();
     const int j = threadIdx.x;
-    if (j < kBCols && s_nrow[j] > 0) {
-      const int2 w = list[u0 + j];
-      const BSlot* D = slots + w.x;
-      const int nrow = s_nrow[j], nc = D->ncol, c = w.y;
+    if (j < kBCols && ss.nrow[j] > 0) {
+      const int2 w = __ldg(P.cols + u0 + j);
+      const BSlot* D = P.slots + w.x;
+      const int nrow = ss.nrow[j], nc = D->ncol, c = w.y;
       const float *fa = D->fa, *finv = D->finv, *fc = D->fc;
       float* col = xs + j;
       double d = 0.0;
@@ -526,12 +580,187 @@ __global__ void __launch_bounds__(kBThreads) bthomas_staged(const int2* list, co
       const int i = r0 + lane;
 #pragma unroll
       for (int k = 0; k < CPW; ++k) {
-        const int jj = warp + NW * k;
-        if (i < s_nrow[jj]) s_z[jj][s_f[jj] + __ldg(s_ind[jj] + i)] = xs[i * LD + jj];
+        const int jj = warp + kBW * k;
+        if (i < ss.nrow[jj]) __stcg(ss.z[jj] + ss.f[jj] + __ldg(ss.ind[jj] + i), xs[i * LD + jj]);
       }
     }
-    __syncthreads();
   }
+}
+
+template <class T> struct W5 { T a, b, c, d, e; };
+
+// The persistent kernel: `iters` super-iterations of every admitted slot.
+template <int NDF, bool CMA>
+__global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict__ PP) {
+  __shared__ BShared sh;
+  __shared__ BParams sp;
+  constexpr int XS = CMA ? kBRows * (kBCols + 1) : 1;
+  __shared__ float xs[XS];
+  __shared__ SweepShared ss;
+  {
+    const int* src = reinterpret_cast<const int*>(PP);
+    int* dst = reinterpret_cast<int*>(&sp);
+    for (int i = threadIdx.x; i < (int)(sizeof(BParams) / 4); i += kBT) dst[i] = src[i];
+  }
+  __syncthreads();
+  const BParams& P = sp;
+  // slots admitted since the last launch take their first residual in
+  // super-iteration 0; later flags are raised by the iterations themselves
+  if (blockIdx.x == 0 && threadIdx.x < 32) {
+    int any = 0;
+    for (int s = threadIdx.x; s < P.max_slots; s += 32) any |= (__ldcg(&P.st[s].phase) == PH_INIT);
+    any = __any_sync(0xffffffffu, any);
+    if (threadIdx.x == 0) {
+      P.need[0] = any;
+      for (int i = 1; i < P.iters; ++i) P.need[i] = 0;
+    }
+  }
+  if (!grid_sync(P, sh)) return;
+
+  for (int it = 0; it < P.iters; ++it) {
+    // ---- A: z = A32 p, alpha
+    for (int g = 0; g < P.ngr32; ++g)
+      for (int c = 0; c < 4; ++c) {
+        apply_phase<NDF, false>(P, sh, P.items32, __ldg(P.off32 + 4 * g + c),
+                                __ldg(P.off32 + 4 * g + c + 1));
+        if (!grid_sync(P, sh)) return;
+      }
+    // ---- U: xc += alpha p, r -= alpha z, ||r||^2 (+ <r, r/d>, beta for Jacobi slots)
+    int* need = P.need + it;
+    chunk_phase<2>(
+        P, sh, [](int ph, int) { return ph_run(ph); },
+        [](const BSlot& D, int64_t i) {
+          return W5<float>{__ldcg(D.xc + i), __ldcg(D.p + i), __ldcg(D.r + i), __ldcg(D.z + i),
+                           D.cma ? 1.0f : __ldg(D.diag + i)};
+        },
+        [](const BSlot& D, const BState& S, int64_t i, const W5<float>& v, double* a) {
+          __stcg(D.xc + i, fmaf((float)S.alpha, v.b, v.a));
+          const float ri = fmaf((float)(-S.alpha), v.d, v.c);
+          __stcg(D.r + i, ri);
+          a[0] = fma((double)ri, (double)ri, a[0]);
+          if (!D.cma) a[1] = fma((double)ri, (double)(ri / v.e), a[1]);
+        },
+        [need](const BSlot& D, BState& S, const double* t) {
+          S.iter += 1;
+          S.rnorm = sqrt(t[0]);
+          if (S.rnorm <= kDelta * S.rlast || S.rnorm <= S.tol * S.r0 || S.iter >= S.max_iter ||
+              !(S.rnorm == S.rnorm)) {
+            S.flag = 1;
+            *need = 1;
+          } else if (!D.cma) {
+            S.beta = t[1] / S.rz;
+            S.rz = t[1];
+          }
+        });
+    if (!grid_sync(P, sh)) return;
+    // ---- R: reliable update and FP64 true residual
+    if (__ldcg(need)) {
+      auto resid = [](int ph, int fl) { return ph == PH_INIT || (ph == PH_RUN && fl); };
+      chunk_phase<0>(
+          P, sh, resid,
+          [](const BSlot& D, int64_t i) { return V2<double>{__ldcg(D.x + i), (double)__ldcg(D.xc + i)}; },
+          [](const BSlot& D, const BState& S, int64_t i, const V2<double>& v, double*) {
+            if (S.phase != PH_INIT) __stcg(D.x + i, v.a + v.b);
+            __stcg(D.xc + i, 0.0f);
+          },
+          [](const BSlot&, BState&, const double*) {});
+      if (!grid_sync(P, sh)) return;
+      for (int g = 0; g < P.ngr64; ++g)
+        for (int c = 0; c < 4; ++c) {
+          apply_phase<NDF, true>(P, sh, P.items64, __ldg(P.off64 + 4 * g + c),
+                                 __ldg(P.off64 + 4 * g + c + 1));
+          if (!grid_sync(P, sh)) return;
+        }
+      chunk_phase<2>(
+          P, sh, resid,
+          [](const BSlot& D, int64_t i) { return V2<double>{__ldcg(D.r64 + i), (double)__ldg(D.diag + i)}; },
+          [](const BSlot& D, const BState&, int64_t i, const V2<double>& v, double* a) {
+            const float ri = (float)v.a;
+            __stcg(D.r + i, ri);
+            a[0] = fma(v.a, v.a, a[0]);
+            if (!D.cma) a[1] = fma((double)ri, (double)(ri / (float)v.b), a[1]);
+          },
+          [](const BSlot& D, BState& S, const double* t) {
+            const double nr = sqrt(t[0]);
+            S.resid += 1;
+            if (S.phase == PH_INIT) {
+              S.r0 = nr;
+              S.rlast = nr;
+              S.true_rel = nr > 0.0 ? 1.0 : 0.0;
+              if (nr < DBL_EPSILON) {
+                S.phase = PH_DONE;
+                S.true_rel = 0.0;
+                return;
+              }
+              S.phase = PH_RUN;
+              S.flag = 0;
+              if (!D.cma) S.rz = t[1];
+              return;
+            }
+            S.flag = 0;
+            S.rlast = nr;
+            S.true_rel = nr / S.r0;
+            if (S.true_rel <= S.tol) {
+              S.phase = PH_DONE;
+            } else if (!(nr == nr)) {
+              S.phase = PH_DONE;
+              S.status = LFX_NAN_DETECTED;
+            } else if (S.iter >= S.max_iter) {
+              S.phase = PH_DONE;
+              S.status = LFX_NOT_CONVERGED;
+            } else if (!D.cma) {
+              S.beta = t[1] / S.rz;
+              S.rz = t[1];
+            }
+          });
+      if (!grid_sync(P, sh)) return;
+    }
+    // ---- C: column sweeps, then the Jacobi rows with <r, z> and beta
+    if (CMA && P.any_cma) {
+      sweep_phase(P, xs, ss);
+      if (!grid_sync(P, sh)) return;
+      chunk_phase<1>(
+          P, sh, [](int ph, int) { return ph_run(ph); },
+          [](const BSlot& D, int64_t i) {
+            return V3<float>{__ldcg(D.r + i), D.cma ? __ldg(D.diag + i) : 1.0f, D.cma ? __ldcg(D.z + i) : 0.0f};
+          },
+          [](const BSlot& D, const BState&, int64_t i, const V3<float>& v, double* a) {
+            if (!D.cma) return;
+            // rows with a non-zero diagonal are Jacobi rows; the column rows
+            // (written by the sweeps) carry a zero in the Jacobi diagonal
+            float zi = v.c;
+            if (v.b != 0.0f) {
+              zi = v.a / v.b;
+              __stcg(D.z + i, zi);
+            }
+            a[0] = fma((double)v.a, (double)zi, a[0]);
+          },
+          [](const BSlot& D, BState& S, const double* t) {
+            if (!D.cma) return;
+            S.beta = S.fresh ? 0.0 : t[0] / S.rz;
+            S.rz = t[0];
+          });
+      if (!grid_sync(P, sh)) return;
+    }
+    // ---- P: p = z + beta p (p = z for a slot that just started)
+    chunk_phase<0>(
+        P, sh, [](int ph, int) { return ph_run(ph); },
+        [](const BSlot& D, int64_t i) {
+          return V3<float>{__ldcg(D.p + i), D.cma ? __ldcg(D.z + i) : __ldcg(D.r + i),
+                           D.cma ? 1.0f : __ldg(D.diag + i)};
+        },
+        [](const BSlot& D, const BState& S, int64_t i, const V3<float>& v, double*) {
+          const float zi = D.cma ? v.b : v.b / v.c;
+          __stcg(D.p + i, S.fresh ? zi : fmaf((float)S.beta, v.a, zi));
+        },
+        [](const BSlot&, BState&, const double*) {});
+    if (!grid_sync(P, sh)) return;
+  }
+}
+
+template <int NDF, bool CMA>
+const void* kernel_ptr() {
+  return reinterpret_cast<const void*>(&batch_kernel<NDF, CMA>);
 }
 
 }  // namespace
@@ -539,244 +768,304 @@ __global__ void __launch_bounds__(kBThreads) bthomas_staged(const int2* list, co
 // host-side record of one slot
 struct SlotHost {
   bool used = false;
-  int64_t vec_off = 0, vec_len = 0;  // in the vector pools (elements)
-  int64_t ent_off = 0, ent_len = 0, ch_off = 0, ch_len = 0, col_off = 0, col_len = 0;
-  int64_t part_off = 0, part_len = 0;
+  void* mem = nullptr;
+  size_t mem_bytes = 0;
   lfx_vec* x = nullptr;
   int64_t tag = 0;
+  int64_t n = 0;
+  int nch = 0, ndot = 0, nl = 0, ncol = 0;
+  bool cma = false;
+  std::vector<int32_t> cstart;  // colour starts in the colour-loop order
+  int last_phase = PH_EMPTY;
 };
 
 struct lfx_batch {
   lfx_ctx* ctx = nullptr;
-  int max_slots = 0, ndf = 0, iters = 4;
-  int64_t cap_dofs = 0, cap_ent = 0, cap_ch = 0, cap_col = 0, cap_part = 0;
+  int ndf = 8, max_slots = 0, iters = 8;
+  int64_t reserve = 0;
   BSlot* d_slots = nullptr;
-  BSlot* h_slots = nullptr;
+  std::vector<BSlot> h_slots;
   BState* d_state = nullptr;
   BState* h_state = nullptr;  // pinned
-  int2 *d_ent = nullptr, *d_ch = nullptr, *d_col = nullptr;
-  int* d_len = nullptr;  // [3]: ent, chunk, col list lengths (high-water marks)
-  int h_len[3] = {0, 0, 0};
-  double* d_partials = nullptr;
   unsigned* d_tickets = nullptr;
-  double* pool64 = nullptr;  // r64 per slot
-  float* pool32 = nullptr;   // r, p, z, xc per slot (4 per dof)
-  // per entity-list item, the column descriptor of the prefetching gather
-  // (6-dof cells), copied from the slot's operator at admission
-  int* d_bdesc = nullptr;
+  int* d_need = nullptr;
+  unsigned* d_bar = nullptr;
+  int* d_err = nullptr;
+  int* h_err = nullptr;  // pinned
+  BParams* d_params = nullptr;
+  BParams h_params{};
+  // work lists (device, grown on demand)
+  int4 *d_items32 = nullptr, *d_items64 = nullptr;
+  int *d_off32 = nullptr, *d_off64 = nullptr;
+  int2 *d_chunks = nullptr, *d_cols = nullptr;
+  size_t cap_items32 = 0, cap_items64 = 0, cap_off32 = 0, cap_off64 = 0, cap_chunks = 0,
+         cap_cols = 0;
   std::vector<SlotHost> slots;
-  cudaGraphExec_t graph = nullptr;
-  int64_t graph_kernels = 0;
-  size_t bytes = 0;
+  bool dirty = true;
+  int nactive = 0;
+  // launch shape (autotuned) and its graphs
+  int cells_per_item = 64, blocks_per_sm = 2, max_bps = 2;
+  int64_t group_bytes = 64 << 20;
+  float tuned_us = 0.f;
+  std::map<int, cudaGraphExec_t> graphs;  // by blocks per SM
+  bool cooperative = true;
+  int64_t replays = 0;
+  double timeout_s = 2.0;
 };
 
 namespace {
 
-// first fit in [0, cap) among the used ranges given by (off, len) of the slots
-int64_t first_fit(const std::vector<SlotHost>& s, int64_t SlotHost::*off, int64_t SlotHost::*len,
-                  int64_t need, int64_t cap) {
-  std::vector<std::pair<int64_t, int64_t>> used;
-  for (auto& x : s)
-    if (x.used && x.*len) used.push_back({x.*off, x.*len});
-  std::sort(used.begin(), used.end());
-  int64_t at = 0;
-  for (auto& u : used) {
-    if (u.first - at >= need) return at;
-    at = std::max(at, u.first + u.second);
-  }
-  return cap - at >= need ? at : -1;
+template <class T>
+int grow(lfx_ctx* ctx, T** p, size_t* cap, size_t need) {
+  if (need <= *cap && *p) return LFX_OK;
+  size_t c = std::max<size_t>(need, *cap * 2);
+  if (c < 64) c = 64;
+  if (*p) LFX_CK(ctx, cudaFreeAsync(*p, ctx->stream));
+  *p = nullptr;
+  LFX_CK(ctx, cudaMallocAsync((void**)p, c * sizeof(T), ctx->stream));
+  *cap = c;
+  return LFX_OK;
 }
 
 template <class T>
-int upload_region(lfx_ctx* ctx, T* dst, const std::vector<T>& src) {
+int upload(lfx_ctx* ctx, T* dst, const std::vector<T>& src) {
   if (src.empty()) return LFX_OK;
   LFX_CK(ctx, cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
                               ctx->stream));
   return LFX_OK;
 }
 
-int set_lengths(lfx_batch* B) {
-  int64_t e = 0, c = 0, k = 0;
-  for (auto& s : B->slots)
-    if (s.used) {
-      e = std::max(e, s.ent_off + s.ent_len);
-      c = std::max(c, s.ch_off + s.ch_len);
-      k = std::max(k, s.col_off + s.col_len);
+const void* pick_kernel(int ndf, bool cma) {
+  if (ndf == 8) return cma ? kernel_ptr<8, true>() : kernel_ptr<8, false>();
+  return cma ? kernel_ptr<6, true>() : kernel_ptr<6, false>();
+}
+
+// apply items of one precision: slots greedily grouped so that a group's
+// vectors (bytes_per_dof per dof) stay within group_bytes; per group and
+// colour the slots' runs of cells_per_item cell columns
+void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int bytes_per_dof,
+                       bool dots, std::vector<int4>& items, std::vector<int>& off,
+                       std::vector<int>* nitem) {
+  items.clear();
+  off.clear();
+  std::vector<std::vector<int>> groups;
+  int64_t acc = 0;
+  for (int s : act) {
+    const int64_t b = (int64_t)bytes_per_dof * B->slots[s].n;
+    if (groups.empty() || (acc + b > B->group_bytes && !groups.back().empty())) {
+      groups.emplace_back();
+      acc = 0;
     }
-  B->h_len[0] = (int)e;
-  B->h_len[1] = (int)c;
-  B->h_len[2] = (int)k;
-  LFX_CK(B->ctx, cudaMemcpyAsync(B->d_len, B->h_len, sizeof(int) * 3, cudaMemcpyHostToDevice,
-                                 B->ctx->stream));
-  return LFX_OK;
-}
-
-// one super-iteration for every slot
-template <int NDF2>
-int launch_super(lfx_batch* B) {
-  lfx_ctx* ctx = B->ctx;
-  const int gridc = ctx->num_sms * 16;
-  const int grida = ctx->num_sms * 16;
-  BSlot* sl = B->d_slots;
-  BState* st = B->d_state;
-  const int* le = B->d_len;
-  const int* lc = B->d_len + 1;
-  const int* lk = B->d_len + 2;
-  // nonzero while some slot needs a true residual this super-iteration: set
-  // by admission and by step 3, cleared by step 6
-  int* need = B->d_len + 3;
-  double* pa = B->d_partials;
-  unsigned* tk = B->d_tickets;
-  auto run = [] __device__(const BState& s) { return ph_run(s); };
-  auto resid = [] __device__(const BState& s) { return ph_resid(s); };
-  auto active = [] __device__(const BState& s) { return ph_active(s); };
-  // 1. z = A32 p
-  if constexpr (NDF2 == 6)
-    bapply_fetch<false><<<ctx->num_sms * 3, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, nullptr,
-                                                                    B->d_bdesc);
-  else
-    bapply<NDF2, false><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, nullptr);
-  // 2. alpha = rz / <p, z>
-  bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, run,
-      [] __device__(const BSlot& D, int64_t i) { return V2<float>{D.p[i], D.z[i]}; },
-      [] __device__(const BSlot&, const BState&, int64_t, const V2<float>& v, double* a) {
-        a[0] = fma((double)v.a, (double)v.b, a[0]);
-      },
-      [] __device__(const BSlot&, BState& S, const double* t) { S.alpha = S.rz / t[0]; });
-  // 3. xc += alpha p, r -= alpha z (FP32); ||r||; decide on a true residual
-  bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, run,
-      [] __device__(const BSlot& D, int64_t i) {
-        return V4<float>{D.xc[i], D.p[i], D.r[i], D.z[i]};
-      },
-      [] __device__(const BSlot& D, const BState& S, int64_t i, const V4<float>& v, double* a) {
-        D.xc[i] = fmaf((float)S.alpha, v.b, v.a);
-        const float ri = fmaf((float)(-S.alpha), v.d, v.c);
-        D.r[i] = ri;
-        a[0] = fma((double)ri, (double)ri, a[0]);
-      },
-      [need] __device__(const BSlot&, BState& S, const double* t) {
-        S.iter += 1;
-        S.rnorm = sqrt(t[0]);
-        if (S.rnorm <= kDelta * S.rlast || S.rnorm <= S.tol * S.r0 || S.iter >= S.max_iter ||
-            !(S.rnorm == S.rnorm)) {
-          S.flag = 1;
-          *need = 1;
-        }
-      });
-  // 3b. reliable update: x += xc (FP64), xc = 0 (new slots: xc = 0)
-  bchunk<0><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, need, nullptr, resid,
-      [] __device__(const BSlot& D, int64_t i) { return V2<double>{D.x[i], (double)D.xc[i]}; },
-      [] __device__(const BSlot& D, const BState& S, int64_t i, const V2<double>& v, double*) {
-        if (S.phase != PH_INIT) D.x[i] = v.a + v.b;
-        D.xc[i] = 0.0f;
-      },
-      [] __device__(const BSlot&, BState&, const double*) {});
-  // 4. r64 = b - A64 x (new slots, and slots taking a true residual)
-  if constexpr (NDF2 == 6)
-    bapply_fetch<true><<<ctx->num_sms * 2, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, need,
-                                                                   B->d_bdesc);
-  else
-    bapply<NDF2, true><<<grida, 256, 0, ctx->stream>>>(B->d_ent, le, sl, st, need);
-  // 5. ||r64||, r = r64 (FP32); convergence on the true residual
-  bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, need, nullptr, resid,
-      [] __device__(const BSlot& D, int64_t i) { return V1<double>{D.r64[i]}; },
-      [] __device__(const BSlot& D, const BState&, int64_t i, const V1<double>& v, double* a) {
-        D.r[i] = (float)v.a;
-        a[0] = fma(v.a, v.a, a[0]);
-      },
-      [] __device__(const BSlot&, BState& S, const double* t) {
-        const double nr = sqrt(t[0]);
-        if (S.phase == PH_INIT) {
-          S.r0 = nr;
-          S.rlast = nr;
-          S.true_rel = nr > 0.0 ? 1.0 : 0.0;
-          if (nr < DBL_EPSILON) {
-            S.phase = PH_DONE;
-            S.true_rel = 0.0;
-          }
-          return;
-        }
-        S.flag = 0;
-        S.rlast = nr;
-        S.true_rel = nr / S.r0;
-        if (S.true_rel <= S.tol) {
-          S.phase = PH_DONE;
-        } else if (!(nr == nr)) {
-          S.phase = PH_DONE;
-          S.status = LFX_NAN_DETECTED;
-        } else if (S.iter >= S.max_iter) {
-          S.phase = PH_DONE;
-          S.status = LFX_NOT_CONVERGED;
-        }
-      });
-  // 6. z = P r (column sweeps for the line kind), then the Jacobi rows fused
-  //    with rz_new = <r, z> and beta
-  if (B->cap_col > 0)
-    bthomas_staged<<<ctx->num_sms * 8, kBThreads, 0, ctx->stream>>>(B->d_col, lk, sl, st);
-  bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, nullptr, need, active,
-      [] __device__(const BSlot& D, int64_t i) { return V3<float>{D.r[i], D.diag[i], D.z[i]}; },
-      [] __device__(const BSlot& D, const BState&, int64_t i, const V3<float>& v, double* a) {
-        // rows with a positive diagonal entry are Jacobi rows; the column rows
-        // (written by the sweeps) carry a zero in the Jacobi diagonal
-        float zi = v.c;
-        if (v.b != 0.0f) {
-          zi = v.a / v.b;
-          D.z[i] = zi;
-        }
-        a[0] = fma((double)v.a, (double)zi, a[0]);
-      },
-      [] __device__(const BSlot&, BState& S, const double* t) {
-        S.beta = S.fresh ? 0.0 : t[0] / S.rz;
-        S.rz = t[0];
-      });
-  // 7. p = z + beta p (p = z for a new slot); new slots start iterating
-  bchunk<1><<<gridc, RT, 0, ctx->stream>>>(
-      B->d_ch, lc, sl, st, pa, tk, nullptr, nullptr, active,
-      [] __device__(const BSlot& D, int64_t i) { return V2<float>{D.p[i], D.z[i]}; },
-      [] __device__(const BSlot& D, const BState& S, int64_t i, const V2<float>& v, double*) {
-        D.p[i] = S.fresh ? v.b : fmaf((float)S.beta, v.a, v.b);
-      },
-      [] __device__(const BSlot&, BState& S, const double*) {
-        S.fresh = 0;
-        if (S.phase == PH_INIT) S.phase = PH_RUN;
-      });
-  LFX_CK(ctx, cudaGetLastError());
-  return LFX_OK;
-}
-
-int capture(lfx_batch* B) {
-  lfx_ctx* ctx = B->ctx;
-  cudaGraph_t g = nullptr;
-  LFX_CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = LFX_OK;
-  for (int it = 0; it < B->iters && !rc; ++it)
-    rc = B->ndf == 8 ? launch_super<8>(B) : launch_super<6>(B);
-  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-  if (rc || e != cudaSuccess) {
-    if (g) cudaGraphDestroy(g);
-    return rc ? rc : cuda_fail(ctx, e, "cudaStreamEndCapture");
+    groups.back().push_back(s);
+    acc += b;
   }
-  e = cudaGraphInstantiate(&B->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
-  B->graph_kernels = (B->cap_col > 0 ? 9 : 8) * (int64_t)B->iters;
+  const int cb = B->cells_per_item;
+  for (auto& g : groups)
+    for (int c = 0; c < 4; ++c) {
+      off.push_back((int)items.size());
+      for (int s : g) {
+        const SlotHost& H = B->slots[s];
+        int dotbase = 0;
+        for (int cc = 0; cc < c; ++cc)
+          dotbase += (H.cstart[cc + 1] - H.cstart[cc] + kDotCols - 1) / kDotCols;
+        if (c + 1 >= (int)H.cstart.size()) continue;
+        const int a = H.cstart[c], e = H.cstart[c + 1];
+        for (int q = a; q < e; q += cb) {
+          items.push_back(make_int4(s, q, std::min(cb, e - q), dots ? dotbase + (q - a) / kDotCols : 0));
+          if (nitem) (*nitem)[s]++;
+        }
+      }
+    }
+  off.push_back((int)items.size());
+}
+
+int rebuild(lfx_batch* B) {
+  lfx_ctx* ctx = B->ctx;
+  std::vector<int> act;
+  bool any_cma = false;
+  for (int s = 0; s < B->max_slots; ++s) {
+    const SlotHost& H = B->slots[s];
+    if (H.used && H.last_phase != PH_DONE) {
+      act.push_back(s);
+      any_cma |= H.cma;
+    }
+  }
+  B->nactive = (int)act.size();
+  std::vector<int4> it32, it64;
+  std::vector<int> off32, off64, nitem(B->max_slots, 0);
+  build_apply_items(B, act, 8, true, it32, off32, &nitem);
+  build_apply_items(B, act, 16, false, it64, off64, nullptr);
+  std::vector<int2> ch, col;
+  for (int s : act) {
+    const SlotHost& H = B->slots[s];
+    for (int c = 0; c < H.nch; ++c) ch.push_back(make_int2(s, c));
+    if (H.cma)
+      for (int c = 0; c < H.ncol; ++c) col.push_back(make_int2(s, c));
+  }
+  int rc = grow(ctx, &B->d_items32, &B->cap_items32, it32.size());
+  if (!rc) rc = grow(ctx, &B->d_items64, &B->cap_items64, it64.size());
+  if (!rc) rc = grow(ctx, &B->d_off32, &B->cap_off32, off32.size());
+  if (!rc) rc = grow(ctx, &B->d_off64, &B->cap_off64, off64.size());
+  if (!rc) rc = grow(ctx, &B->d_chunks, &B->cap_chunks, ch.size());
+  if (!rc) rc = grow(ctx, &B->d_cols, &B->cap_cols, col.size());
+  if (rc) return rc;
+  rc = upload(ctx, B->d_items32, it32);
+  if (!rc) rc = upload(ctx, B->d_items64, it64);
+  if (!rc) rc = upload(ctx, B->d_off32, off32);
+  if (!rc) rc = upload(ctx, B->d_off64, off64);
+  if (!rc) rc = upload(ctx, B->d_chunks, ch);
+  if (!rc) rc = upload(ctx, B->d_cols, col);
+  if (rc) return rc;
+  for (int s : act) {
+    B->h_slots[s].nitem32 = nitem[s];
+    LFX_CK(ctx, cudaMemcpyAsync(B->d_slots + s, &B->h_slots[s], sizeof(BSlot),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  }
+  BParams& P = B->h_params;
+  P.items32 = B->d_items32;
+  P.off32 = B->d_off32;
+  P.items64 = B->d_items64;
+  P.off64 = B->d_off64;
+  P.chunks = B->d_chunks;
+  P.cols = B->d_cols;
+  P.slots = B->d_slots;
+  P.st = B->d_state;
+  P.tickets = B->d_tickets;
+  P.need = B->d_need;
+  P.bar = B->d_bar;
+  P.err = B->d_err;
+  P.ngr32 = (int)off32.size() / 4;
+  P.ngr64 = (int)off64.size() / 4;
+  P.nchunk = (int)ch.size();
+  P.ncolitem = (int)col.size();
+  P.iters = B->iters;
+  P.max_slots = B->max_slots;
+  P.any_cma = any_cma ? 1 : 0;
+  P.timeout_ns = (unsigned long long)(B->timeout_s * 1e9);
+  LFX_CK(ctx, cudaMemcpyAsync(B->d_params, &P, sizeof(BParams), cudaMemcpyHostToDevice,
+                              ctx->stream));
+  B->dirty = false;
   return LFX_OK;
+}
+
+// the graph of one launch shape: reset the barrier, then the persistent
+// kernel (cooperative where the graph takes it)
+int graph_for(lfx_batch* B, int bps, cudaGraphExec_t* out) {
+  auto f = B->graphs.find(bps);
+  if (f != B->graphs.end()) {
+    *out = f->second;
+    return LFX_OK;
+  }
+  lfx_ctx* ctx = B->ctx;
+  const void* k = pick_kernel(B->ndf, B->ndf == 6);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ctx->num_sms * bps));
+  cfg.blockDim = dim3(kBT);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  void* args[] = {(void*)&B->d_params};
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    cfg.attrs = B->cooperative ? at : nullptr;
+    cfg.numAttrs = B->cooperative ? 1 : 0;
+    cudaGraph_t g = nullptr;
+    LFX_CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1 = cudaMemsetAsync(B->d_bar, 0, 2 * sizeof(unsigned), ctx->stream);
+    cudaError_t e2 = cudaLaunchKernelExC(&cfg, k, args);
+    cudaError_t e3 = cudaStreamEndCapture(ctx->stream, &g);
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e4 = cudaErrorUnknown;
+    if (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && g)
+      e4 = cudaGraphInstantiate(&ex, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e4 == cudaSuccess) {
+      B->graphs[bps] = ex;
+      *out = ex;
+      return LFX_OK;
+    }
+    cudaGetLastError();
+    if (!B->cooperative) {
+      cudaError_t e = e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3 != cudaSuccess ? e3 : e4;
+      return cuda_fail(ctx, e, "batch graph capture");
+    }
+    // graphs that do not take a cooperative kernel: the grid is sized to
+    // what the device holds at once, and every barrier wait is bounded
+    B->cooperative = false;
+  }
+  return fail(ctx, LFX_CUDA_ERROR, "batch graph capture");
+}
+
+int replay(lfx_batch* B) {
+  lfx_ctx* ctx = B->ctx;
+  cudaGraphExec_t g = nullptr;
+  int rc = graph_for(B, B->blocks_per_sm, &g);
+  if (rc) return rc;
+  LFX_CK(ctx, cudaGraphLaunch(g, ctx->stream));
+  ctx->launches += 1;
+  B->replays += 1;
+  return LFX_OK;
+}
+
+// reads the slot states and the error flag back (synchronises)
+int read_back(lfx_batch* B) {
+  lfx_ctx* ctx = B->ctx;
+  LFX_CK(ctx, cudaMemcpyAsync(B->h_state, B->d_state, sizeof(BState) * B->max_slots,
+                              cudaMemcpyDeviceToHost, ctx->stream));
+  LFX_CK(ctx, cudaMemcpyAsync(B->h_err, B->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  if (*B->h_err) {
+    const int e = *B->h_err;
+    *B->h_err = 0;
+    cudaMemsetAsync(B->d_err, 0, sizeof(int), ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return fail(ctx, e, "batch: a grid barrier wait ran out (the batch state is undefined)");
+  }
+  for (int s = 0; s < B->max_slots; ++s) {
+    SlotHost& H = B->slots[s];
+    if (!H.used) continue;
+    if (B->h_state[s].phase == PH_DONE && H.last_phase != PH_DONE) B->dirty = true;
+    H.last_phase = B->h_state[s].phase;
+  }
+  return LFX_OK;
+}
+
+// device memory the batch may still take: free memory plus what the
+// stream-ordered pool holds unused
+int64_t available_bytes(lfx_ctx* ctx) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int64_t avail = (int64_t)fr;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+    uint64_t res = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        res > used)
+      avail += (int64_t)(res - used);
+  }
+  cudaGetLastError();
+  return avail;
+}
+
+// device bytes a slot of this operator takes at admission
+int64_t slot_bytes(int64_t n, int64_t nch, int64_t ndot) {
+  const int64_t v = ((8 * n + 255) / 256 + 4 * ((4 * n + 255) / 256)) * 256;
+  return v + ((2 * nch + ndot) * 8 + 255) / 256 * 256;
 }
 
 }  // namespace
 
 extern "C" {
 
-int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t max_dofs,
-                     int64_t max_entities, int64_t max_columns, int32_t iters_per_launch,
-                     lfx_batch** out) {
-  if (!ctx || !out || (ndf != 6 && ndf != 8) || max_slots < 1 || max_dofs < 1 ||
-      max_entities < 1 || iters_per_launch < 1)
+int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t reserve_bytes,
+                     int32_t iters_per_launch, lfx_batch** out) {
+  if (!ctx || !out || (ndf != 6 && ndf != 8) || max_slots < 1 || reserve_bytes < 0 ||
+      iters_per_launch < 1 || iters_per_launch > kMaxIters)
     return LFX_INVALID_ARGUMENT;
   *out = nullptr;
   lfx_batch* B = new lfx_batch();
@@ -784,41 +1073,49 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t max_d
   B->ndf = ndf;
   B->max_slots = max_slots;
   B->iters = iters_per_launch;
-  B->cap_dofs = max_dofs;
-  B->cap_ent = max_entities;
-  B->cap_ch = nchunks(max_dofs) + max_slots;
-  B->cap_col = max_columns;
-  B->cap_part = 2 * B->cap_ch;
+  B->reserve = reserve_bytes;
   B->slots.resize(max_slots);
+  B->h_slots.assign(max_slots, BSlot{});
   int rc = dmalloc(ctx, (void**)&B->d_slots, sizeof(BSlot) * max_slots);
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_state, sizeof(BState) * max_slots);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->d_ent, sizeof(int2) * B->cap_ent);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->d_ch, sizeof(int2) * B->cap_ch);
-  if (!rc && B->cap_col) rc = dmalloc(ctx, (void**)&B->d_col, sizeof(int2) * B->cap_col);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->d_len, sizeof(int) * 4);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->d_partials, sizeof(double) * B->cap_part);
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_tickets, sizeof(unsigned) * max_slots);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->pool64, sizeof(double) * max_dofs);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->pool32, sizeof(float) * 4 * max_dofs);
-  if (!rc && ndf == 6)
-    rc = dmalloc(ctx, (void**)&B->d_bdesc, sizeof(int) * fd_ints(6) * B->cap_ent);
+  if (!rc) rc = dmalloc(ctx, (void**)&B->d_need, sizeof(int) * kMaxIters);
+  if (!rc) rc = dmalloc(ctx, (void**)&B->d_bar, sizeof(unsigned) * 2);
+  if (!rc) rc = dmalloc(ctx, (void**)&B->d_err, sizeof(int));
+  if (!rc) rc = dmalloc(ctx, (void**)&B->d_params, sizeof(BParams));
   if (!rc && cudaMallocHost((void**)&B->h_state, sizeof(BState) * max_slots) != cudaSuccess)
     rc = LFX_OUT_OF_MEMORY;
-  B->h_slots = new BSlot[max_slots];
+  if (!rc && cudaMallocHost((void**)&B->h_err, sizeof(int)) != cudaSuccess) rc = LFX_OUT_OF_MEMORY;
   if (!rc) {
-    memset(B->h_slots, 0, sizeof(BSlot) * max_slots);
     memset(B->h_state, 0, sizeof(BState) * max_slots);
+    *B->h_err = 0;
+    cudaMemsetAsync(B->d_slots, 0, sizeof(BSlot) * max_slots, ctx->stream);
     cudaMemsetAsync(B->d_state, 0, sizeof(BState) * max_slots, ctx->stream);
     cudaMemsetAsync(B->d_tickets, 0, sizeof(unsigned) * max_slots, ctx->stream);
-    cudaMemsetAsync(B->d_len, 0, sizeof(int) * 4, ctx->stream);
-    cudaMemsetAsync(B->d_slots, 0, sizeof(BSlot) * max_slots, ctx->stream);
-    // list entries start out as "no slot"
-    cudaMemsetAsync(B->d_ent, 0xff, sizeof(int2) * B->cap_ent, ctx->stream);
-    cudaMemsetAsync(B->d_ch, 0xff, sizeof(int2) * B->cap_ch, ctx->stream);
-    if (B->cap_col) cudaMemsetAsync(B->d_col, 0xff, sizeof(int2) * B->cap_col, ctx->stream);
+    cudaMemsetAsync(B->d_need, 0, sizeof(int) * kMaxIters, ctx->stream);
+    cudaMemsetAsync(B->d_bar, 0, sizeof(unsigned) * 2, ctx->stream);
+    cudaMemsetAsync(B->d_err, 0, sizeof(int), ctx->stream);
+    // memory returned by retired slots stays in the pool for the next ones
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    // the kernel holds at most two blocks per SM (launch bounds); fewer if
+    // the device says so
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(ndf, ndf == 6), kBT, 0);
+    B->max_bps = std::max(1, std::min(per_sm, 2));
+    B->blocks_per_sm = B->max_bps;
+    B->group_bytes = ctx->l2_bytes / 2;
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = LFX_CUDA_ERROR;
+    cudaGetLastError();
   }
-  if (!rc) rc = capture(B);
+  if (!rc) rc = rebuild(B);
+  if (!rc) {
+    cudaGraphExec_t g;
+    rc = graph_for(B, B->blocks_per_sm, &g);
+  }
   if (rc) {
     lfx_batch_destroy(B);
     return rc;
@@ -830,46 +1127,53 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t max_d
 int lfx_batch_destroy(lfx_batch* B) {
   if (!B) return LFX_OK;
   lfx_ctx* ctx = B->ctx;
-  if (B->graph) cudaGraphExecDestroy(B->graph);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& H : B->slots)
+    if (H.mem) cudaFreeAsync(H.mem, ctx->stream);
+  for (void* p : {(void*)B->d_items32, (void*)B->d_items64, (void*)B->d_off32, (void*)B->d_off64,
+                  (void*)B->d_chunks, (void*)B->d_cols})
+    if (p) cudaFreeAsync(p, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
   dfree(ctx, B->d_slots, sizeof(BSlot) * B->max_slots);
   dfree(ctx, B->d_state, sizeof(BState) * B->max_slots);
-  dfree(ctx, B->d_ent, sizeof(int2) * B->cap_ent);
-  dfree(ctx, B->d_ch, sizeof(int2) * B->cap_ch);
-  dfree(ctx, B->d_col, sizeof(int2) * B->cap_col);
-  dfree(ctx, B->d_len, sizeof(int) * 4);
-  dfree(ctx, B->d_partials, sizeof(double) * B->cap_part);
   dfree(ctx, B->d_tickets, sizeof(unsigned) * B->max_slots);
-  dfree(ctx, B->pool64, sizeof(double) * B->cap_dofs);
-  dfree(ctx, B->pool32, sizeof(float) * 4 * B->cap_dofs);
-  if (B->d_bdesc) dfree(ctx, B->d_bdesc, sizeof(int) * fd_ints(6) * B->cap_ent);
+  dfree(ctx, B->d_need, sizeof(int) * kMaxIters);
+  dfree(ctx, B->d_bar, sizeof(unsigned) * 2);
+  dfree(ctx, B->d_err, sizeof(int));
+  dfree(ctx, B->d_params, sizeof(BParams));
   if (B->h_state) cudaFreeHost(B->h_state);
-  delete[] B->h_slots;
+  if (B->h_err) cudaFreeHost(B->h_err);
+  cudaGetLastError();
   delete B;
   return LFX_OK;
 }
 
-// Admits one solve A x = b into a free slot: op64 / op32 the FP64 and FP32
-// copies of one operator (same layout), prec32 its FP32 Jacobi or column
-// preconditioner, b and x FP64 vectors (x is the initial guess and receives
-// the solution; both must stay alive until the slot is retired).
 int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, const lfx_vec* b,
                     lfx_vec* x, double tol, int32_t max_iter, int64_t tag, int32_t* slot_out) {
-  if (!B || !op64 || !op32 || !prec32 || !b || !x || !slot_out) return LFX_INVALID_ARGUMENT;
+  if (!B || !op64 || !op32 || !prec32 || !b || !x || !slot_out || !(tol > 0.0) || max_iter < 1)
+    return LFX_INVALID_ARGUMENT;
   lfx_ctx* ctx = B->ctx;
   *slot_out = -1;
   const lfx_lma_layout* L = op64->lay;
   if (op32->lay != L || op64->precision != LFX_R64 || op32->precision != LFX_R32)
     return fail(ctx, LFX_TYPE_MISMATCH, "batch needs FP64 and FP32 copies of one operator");
-  if (L->ndf_from != B->ndf || L->ndf_to != B->ndf || L->max_nrec > 2 || !L->ent_pack)
-    return fail(ctx, LFX_NOT_SUPPORTED, "operator shape does not match the batch");
-  if (B->ndf == 6 && (!L->fdesc || L->fd_ints != fd_ints(6)))
+  if (L->ndf_from != B->ndf || L->ndf_to != B->ndf || !L->cs_ok || !op32->smat || !op64->smat)
     return fail(ctx, LFX_NOT_SUPPORTED,
-                "batch of 6-dof cells needs columns reading at most two blocks from two cells");
-  if (prec32->precision != LFX_R32 || (prec32->kind != PREC_DIAG && prec32->kind != PREC_CMA) ||
-      !prec32->rdiag || prec32->rdiag_n != L->undf_to)
-    return fail(ctx, LFX_NOT_SUPPORTED, "batch needs an FP32 Jacobi or column preconditioner with a diagonal");
-  if (prec32->kind == PREC_CMA && prec32->nrow > kBRows)
-    return fail(ctx, LFX_NOT_SUPPORTED, "batch column preconditioner: at most 160 rows per column");
+                "batch needs a symmetric operator on one dofmap of the batch's cell size "
+                "(the packed cell scatter)");
+  const int nl = L->nlayers;
+  const int nseg = nl + 1 <= 32 ? 1 : (nl + 1 + 30) / 31;
+  if (nseg > kMaxSeg)
+    return fail(ctx, LFX_NOT_SUPPORTED, "batch: at most 123 levels per column");
+  const bool cma = prec32->kind == PREC_CMA;
+  if (prec32->precision != LFX_R32 || (prec32->kind != PREC_DIAG && !cma) || !prec32->rdiag ||
+      prec32->rdiag_n != L->undf_to || (cma && !prec32->jacobi_zeroed))
+    return fail(ctx, LFX_NOT_SUPPORTED,
+                "batch needs an FP32 Jacobi or column preconditioner with a diagonal");
+  if (cma && (B->ndf != 6 || prec32->nrow > kBRows))
+    return fail(ctx, LFX_NOT_SUPPORTED,
+                "batch column preconditioner: 6-dof cells, at most 160 rows per column");
   if (b->precision != LFX_R64 || x->precision != LFX_R64 || b->undf[0] != L->undf_to ||
       x->undf[0] != L->undf_to)
     return fail(ctx, LFX_TYPE_MISMATCH, "b and x must be FP64 vectors of the operator's space");
@@ -882,43 +1186,68 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   if (s < 0) return fail(ctx, LFX_OUT_OF_MEMORY, "no free batch slot");
   const int64_t n = L->undf_to;
   const int64_t nch = bchunks(n);
-  const int64_t ncol = prec32->kind == PREC_CMA ? prec32->ncell_2d : 0;
+  int ndot = 0;
+  for (size_t c = 0; c + 1 < L->colour_start.size(); ++c)
+    ndot += (L->colour_start[c + 1] - L->colour_start[c] + kDotCols - 1) / kDotCols;
+  if (L->colour_start.size() != 5)
+    return fail(ctx, LFX_NOT_SUPPORTED, "batch: four colours");
+  // admission by free device memory: the slot's state, its share of the
+  // work lists, and the batch's reserve must fit
+  const int64_t need = slot_bytes(n, nch, ndot);
+  const int64_t lists = 16 * (2 * ((int64_t)L->ncell_2d / 32 + 8) + nch) + 8 * (cma ? prec32->ncell_2d : 0);
+  if (available_bytes(ctx) - need - 2 * lists < B->reserve)
+    return fail(ctx, LFX_OUT_OF_MEMORY, "batch: not enough free device memory for the solve");
   SlotHost& H = B->slots[s];
   H = SlotHost();
-  H.vec_len = n;
-  H.ent_len = L->nent;
-  H.ch_len = nch;
-  H.col_len = ncol;
-  H.part_len = 2 * nch;
-  H.vec_off = first_fit(B->slots, &SlotHost::vec_off, &SlotHost::vec_len, n, B->cap_dofs);
-  H.ent_off = first_fit(B->slots, &SlotHost::ent_off, &SlotHost::ent_len, H.ent_len, B->cap_ent);
-  H.ch_off = first_fit(B->slots, &SlotHost::ch_off, &SlotHost::ch_len, nch, B->cap_ch);
-  H.col_off = ncol ? first_fit(B->slots, &SlotHost::col_off, &SlotHost::col_len, ncol, B->cap_col) : 0;
-  H.part_off = first_fit(B->slots, &SlotHost::part_off, &SlotHost::part_len, 2 * nch, B->cap_part);
-  if (H.vec_off < 0 || H.ent_off < 0 || H.ch_off < 0 || H.col_off < 0 || H.part_off < 0) {
-    H = SlotHost();
-    return fail(ctx, LFX_OUT_OF_MEMORY, "batch pools are full");
+  void* mem = nullptr;
+  cudaError_t e = cudaMallocAsync(&mem, (size_t)need, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, LFX_OUT_OF_MEMORY, "batch: slot state allocation failed");
   }
   H.used = true;
+  H.mem = mem;
+  H.mem_bytes = (size_t)need;
   H.x = x;
   H.tag = tag;
-  // descriptor
+  H.n = n;
+  H.nch = (int)nch;
+  H.ndot = ndot;
+  H.nl = nl;
+  H.cma = cma;
+  H.ncol = cma ? prec32->ncell_2d : 0;
+  H.cstart = L->colour_start;
+  H.last_phase = PH_INIT;
   BSlot D{};
-  D.ent_pack = L->ent_pack;
-  D.grp_pack = L->grp_pack;
-  D.M32 = (const float*)op32->mat;
-  D.M64 = (const double*)op64->mat;
-  D.gp_stride = L->gp_stride;
-  D.nent = L->nent;
-  D.nl = L->nlayers;
-  D.ndf1 = L->ndf_to;
-  D.blk32 = op32->blk;
-  D.blk64 = op64->blk;
-  D.nch = (int32_t)nch;
-  D.part_off = (int32_t)H.part_off;
+  D.S32 = (const float*)op32->smat;
+  D.S64 = (const double*)op64->smat;
+  D.cdesc = L->cs_desc;
+  D.sblk32 = op32->sblk;
+  D.sblk64 = op64->sblk;
+  D.cdints = L->cs_ints;
+  D.nl = nl;
+  D.nseg = nseg;
+  D.segL = (nl + 1 + nseg - 1) / nseg;
+  D.nch = (int)nch;
+  D.ndot = ndot;
+  D.nitem32 = 0;
+  D.cma = cma ? 1 : 0;
   D.n = n;
+  char* m = (char*)mem;
+  D.r64 = (double*)m;
+  m += (8 * n + 255) / 256 * 256;
+  float* f[4];
+  for (int i = 0; i < 4; ++i) {
+    f[i] = (float*)m;
+    m += (4 * n + 255) / 256 * 256;
+  }
+  D.r = f[0];
+  D.p = f[1];
+  D.z = f[2];
+  D.xc = f[3];
+  D.part = (double*)m;
   D.diag = (const float*)prec32->rdiag;
-  if (prec32->kind == PREC_CMA) {
+  if (cma) {
     D.fa = (const float*)prec32->fa;
     D.finv = (const float*)prec32->finv;
     D.fc = (const float*)prec32->fc;
@@ -929,11 +1258,6 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   }
   D.b = (const double*)b->data[0];
   D.x = (double*)x->data[0];
-  D.r64 = B->pool64 + H.vec_off;
-  D.r = B->pool32 + 4 * H.vec_off;
-  D.p = D.r + n;
-  D.z = D.p + n;
-  D.xc = D.z + n;
   B->h_slots[s] = D;
   BState S{};
   S.phase = PH_INIT;
@@ -941,43 +1265,23 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   S.tol = tol;
   S.max_iter = max_iter;
   B->h_state[s] = S;
-  // the line preconditioner's Jacobi diagonal must carry zeros on the column
-  // rows (the fused kernel tells the two kinds of row apart by it)
   int rc = LFX_OK;
-  if (prec32->kind == PREC_CMA && !prec32->jacobi_zeroed) {
-    std::vector<float> d(n);
-    LFX_CK(ctx, cudaMemcpy(d.data(), prec32->rdiag, n * 4, cudaMemcpyDeviceToHost));
-    std::vector<int32_t> f(prec32->ncell_2d), ind(prec32->nrow);
-    LFX_CK(ctx, cudaMemcpy(f.data(), prec32->first_dof, f.size() * 4, cudaMemcpyDeviceToHost));
-    LFX_CK(ctx, cudaMemcpy(ind.data(), prec32->indirection, ind.size() * 4, cudaMemcpyDeviceToHost));
-    // (the single-solve preconditioner reads this diagonal on the other rows only)
-    for (size_t c = 0; c < f.size(); ++c)
-      for (size_t i = 0; i < ind.size(); ++i) d[(size_t)f[c] + ind[i]] = 0.0f;
-    LFX_CK(ctx, cudaMemcpy(prec32->rdiag, d.data(), n * 4, cudaMemcpyHostToDevice));
-    prec32->jacobi_zeroed = true;
-  }
-  std::vector<int2> ent(H.ent_len), ch(nch), col(ncol);
-  for (int64_t e = 0; e < H.ent_len; ++e) ent[e] = make_int2(s, (int)e);
-  for (int64_t c = 0; c < nch; ++c) ch[c] = make_int2(s, (int)c);
-  for (int64_t c = 0; c < ncol; ++c) col[c] = make_int2(s, (int)c);
-  rc = upload_region(ctx, B->d_ent + H.ent_off, ent);
-  if (!rc && B->d_bdesc)
-    LFX_CK(ctx, cudaMemcpyAsync(B->d_bdesc + (size_t)H.ent_off * fd_ints(6), L->fdesc,
-                                sizeof(int) * fd_ints(6) * H.ent_len, cudaMemcpyDeviceToDevice,
-                                ctx->stream));
-  if (!rc) rc = upload_region(ctx, B->d_ch + H.ch_off, ch);
-  if (!rc && ncol) rc = upload_region(ctx, B->d_col + H.col_off, col);
-  if (!rc) LFX_CK(ctx, cudaMemcpyAsync(B->d_slots + s, &B->h_slots[s], sizeof(BSlot),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-  if (!rc) LFX_CK(ctx, cudaMemcpyAsync(B->d_state + s, &B->h_state[s], sizeof(BState),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-  // the new slot takes its first residual in the next super-iteration
-  if (!rc) LFX_CK(ctx, cudaMemsetAsync(B->d_len + 3, 1, sizeof(int), ctx->stream));
-  if (!rc) rc = set_lengths(B);
+  // xc starts at zero (the first true residual leaves x as given)
+  e = cudaMemsetAsync(D.xc, 0, 4 * n, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(B->d_slots + s, &B->h_slots[s], sizeof(BSlot), cudaMemcpyHostToDevice,
+                        ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(B->d_state + s, &B->h_state[s], sizeof(BState), cudaMemcpyHostToDevice,
+                        ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(B->d_tickets + s, 0, sizeof(unsigned), ctx->stream);
+  if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch admission");
   if (rc) {
+    cudaFreeAsync(mem, ctx->stream);
     H = SlotHost();
     return rc;
   }
+  B->dirty = true;
   *slot_out = s;
   return LFX_OK;
 }
@@ -987,15 +1291,17 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
 // (converged or failed) and not yet retired.
 int lfx_batch_step(lfx_batch* B, int32_t* ndone) {
   if (!B) return LFX_INVALID_ARGUMENT;
-  lfx_ctx* ctx = B->ctx;
-  LFX_CK(ctx, cudaGraphLaunch(B->graph, ctx->stream));
-  ctx->launches += B->graph_kernels;
-  LFX_CK(ctx, cudaMemcpyAsync(B->h_state, B->d_state, sizeof(BState) * B->max_slots,
-                              cudaMemcpyDeviceToHost, ctx->stream));
-  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  int rc = LFX_OK;
+  if (B->dirty) rc = rebuild(B);
+  if (rc) return rc;
+  if (B->nactive > 0) {
+    rc = replay(B);
+    if (!rc) rc = read_back(B);
+    if (rc) return rc;
+  }
   int nd = 0;
   for (int s = 0; s < B->max_slots; ++s)
-    if (B->slots[s].used && B->h_state[s].phase == PH_DONE) ++nd;
+    if (B->slots[s].used && B->slots[s].last_phase == PH_DONE) ++nd;
   if (ndone) *ndone = nd;
   return LFX_OK;
 }
@@ -1014,30 +1320,136 @@ int lfx_batch_slot_info(const lfx_batch* B, int32_t slot, int32_t* phase, int64_
     info->initial_norm = S.r0;
     info->final_norm = S.rlast;
     info->final_rel = S.true_rel;
+    info->applies = S.iter + S.resid;
     info->status = S.status;
+    info->outer_iterations = S.resid;
+    info->inner_iterations = S.iter;
   }
   return LFX_OK;
 }
 
-// Frees a done (or any) slot for new admissions.
+// Frees a done (or any) slot for new admissions; its state returns to the
+// device's memory pool.
 int lfx_batch_retire(lfx_batch* B, int32_t slot) {
   if (!B || slot < 0 || slot >= B->max_slots) return LFX_INVALID_ARGUMENT;
   lfx_ctx* ctx = B->ctx;
   SlotHost& H = B->slots[slot];
   if (!H.used) return LFX_OK;
-  // mark its list items and state empty on the device
-  std::vector<int2> none_e(H.ent_len, make_int2(-1, -1)), none_c(H.ch_len, make_int2(-1, -1)),
-      none_k(H.col_len, make_int2(-1, -1));
-  int rc = upload_region(ctx, B->d_ent + H.ent_off, none_e);
-  if (!rc) rc = upload_region(ctx, B->d_ch + H.ch_off, none_c);
-  if (!rc && H.col_len) rc = upload_region(ctx, B->d_col + H.col_off, none_k);
   B->h_state[slot] = BState{};
-  if (!rc) LFX_CK(ctx, cudaMemcpyAsync(B->d_state + slot, &B->h_state[slot], sizeof(BState),
-                                       cudaMemcpyHostToDevice, ctx->stream));
+  LFX_CK(ctx, cudaMemcpyAsync(B->d_state + slot, &B->h_state[slot], sizeof(BState),
+                              cudaMemcpyHostToDevice, ctx->stream));
+  if (H.mem) LFX_CK(ctx, cudaFreeAsync(H.mem, ctx->stream));
   H = SlotHost();
-  if (!rc) rc = set_lengths(B);
-  if (!rc) LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  B->dirty = true;
+  return LFX_OK;
+}
+
+int lfx_batch_get_tuning(const lfx_batch* B, lfx_batch_tuning* t) {
+  if (!B || !t) return LFX_INVALID_ARGUMENT;
+  t->cells_per_item = B->cells_per_item;
+  t->blocks_per_sm = B->blocks_per_sm;
+  t->grid = B->ctx->num_sms * B->blocks_per_sm;
+  t->group_bytes = B->group_bytes;
+  t->us_per_iteration = B->tuned_us;
+  t->cooperative = B->cooperative ? 1 : 0;
+  t->replays = B->replays;
+  return LFX_OK;
+}
+
+int lfx_batch_set_tuning(lfx_batch* B, int32_t cells_per_item, int32_t blocks_per_sm,
+                         int64_t group_bytes) {
+  if (!B) return LFX_INVALID_ARGUMENT;
+  if (cells_per_item < kDotCols || cells_per_item > kMaxCB || cells_per_item % kDotCols ||
+      blocks_per_sm < 1 || blocks_per_sm > B->max_bps || group_bytes < 1)
+    return fail(B->ctx, LFX_INVALID_ARGUMENT, "batch tuning out of range");
+  B->cells_per_item = cells_per_item;
+  B->blocks_per_sm = blocks_per_sm;
+  B->group_bytes = group_bytes;
+  B->dirty = true;
+  return LFX_OK;
+}
+
+// Batch autotuner: times one replay of `iters` super-iterations per
+// candidate launch shape on the admitted slots (the replays advance the
+// solves; results do not depend on the shape) and keeps the fastest:
+// blocks per SM, then cell columns per apply item, then the L2 group size.
+int lfx_batch_autotune(lfx_batch* B, int32_t iters, lfx_batch_tuning* out) {
+  if (!B || iters < 1 || iters > kMaxIters) return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = B->ctx;
+  const int keep_iters = B->iters;
+  cudaEvent_t e0, e1;
+  LFX_CK(ctx, cudaEventCreate(&e0));
+  LFX_CK(ctx, cudaEventCreate(&e1));
+  int rc = LFX_OK;
+  auto trial = [&](float* us) -> int {
+    int r = rebuild(B);
+    if (r) return r;
+    if (B->nactive == 0) {
+      *us = 0.f;
+      return LFX_OK;
+    }
+    cudaGraphExec_t g = nullptr;
+    r = graph_for(B, B->blocks_per_sm, &g);  // captured before the timed replay
+    if (r) return r;
+    LFX_CK(ctx, cudaEventRecord(e0, ctx->stream));
+    r = replay(B);
+    if (r) return r;
+    LFX_CK(ctx, cudaEventRecord(e1, ctx->stream));
+    r = read_back(B);
+    if (r) return r;
+    float ms = 0.f;
+    LFX_CK(ctx, cudaEventElapsedTime(&ms, e0, e1));
+    *us = 1e3f * ms / iters;
+    return LFX_OK;
+  };
+  B->iters = iters;
+  float t = 0.f, best = 0.f;
+  // one warm-up replay (first residuals of new slots)
+  rc = trial(&t);
+  int bb = B->blocks_per_sm, bc = B->cells_per_item;
+  int64_t bg = B->group_bytes;
+  const int64_t l2 = ctx->l2_bytes;
+  for (int stage = 0; stage < 3 && !rc; ++stage) {
+    std::vector<int64_t> cand;
+    if (stage == 0)
+      for (int v = 1; v <= B->max_bps; ++v) cand.push_back(v);
+    if (stage == 1) cand = {32, 64, 128};
+    if (stage == 2) cand = {l2 / 4, l2 / 2, l2, int64_t(1) << 40};
+    best = 0.f;
+    for (int64_t c : cand) {
+      B->blocks_per_sm = stage == 0 ? (int)c : bb;
+      B->cells_per_item = stage == 1 ? (int)c : bc;
+      B->group_bytes = stage == 2 ? c : bg;
+      B->dirty = true;
+      rc = trial(&t);
+      if (rc) break;
+      if (best == 0.f || t < best) {
+        best = t;
+        if (stage == 0) bb = (int)c;
+        if (stage == 1) bc = (int)c;
+        if (stage == 2) bg = c;
+      }
+    }
+  }
+  B->blocks_per_sm = bb;
+  B->cells_per_item = bc;
+  B->group_bytes = bg;
+  B->tuned_us = best;
+  B->iters = keep_iters;
+  B->dirty = true;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc && out) rc = lfx_batch_get_tuning(B, out);
   return rc;
+}
+
+// Upper bound on one grid-barrier wait (seconds) before the kernel gives up
+// with LFX_TIMEOUT.
+int lfx_batch_set_wait_limit(lfx_batch* B, double seconds) {
+  if (!B || !(seconds > 0.0)) return LFX_INVALID_ARGUMENT;
+  B->timeout_s = seconds;
+  B->dirty = true;
+  return LFX_OK;
 }
 
 }  // extern "C"

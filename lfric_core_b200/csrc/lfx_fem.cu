@@ -97,8 +97,10 @@ __global__ void assemble_w0(int64_t nc3, int nl, const int* vc, const double* xy
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b)
           G[a][b] = Ji[a][0] * Ji[b][0] + Ji[a][1] * Ji[b][1] + Ji[a][2] * Ji[b][2];
+      /* the upper triangle; the lower one is its mirror image, so the
+       * local matrix is symmetric bit for bit */
       for (int i = 0; i < 8; ++i)
-        for (int j = 0; j < 8; ++j) {
+        for (int j = i; j < 8; ++j) {
           double kij = 0.0;
           for (int a = 0; a < 3; ++a)
             for (int b = 0; b < 3; ++b) kij += dphi[i][a] * G[a][b] * dphi[j][b];
@@ -106,7 +108,7 @@ __global__ void assemble_w0(int64_t nc3, int nl, const int* vc, const double* xy
         }
     }
     for (int i = 0; i < 8; ++i)
-      for (int j = 0; j < 8; ++j) lma[ik + nc3 * (i + 8 * j)] = A[i][j];
+      for (int j = 0; j < 8; ++j) lma[ik + nc3 * (i + 8 * j)] = i <= j ? A[i][j] : A[j][i];
   }
 }
 

@@ -1823,6 +1823,32 @@ int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* 
 
 }  // namespace lfx
 
+// out = fma(a, y, x) elementwise: operator_x_plus_ay on the stored copies
+// (the padding between blocks is zero in both, and stays zero)
+template <class T>
+__global__ void lma_x_plus_ay(int64_t n, const T* __restrict__ x, T a, const T* __restrict__ y,
+                              T* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = fmaT(a, y[i], x[i]);
+}
+
+int x_plus_ay_copy(lfx_ctx* ctx, int32_t precision, const void* x, double a, const void* y,
+                   void* out, size_t bytes) {
+  const size_t esz = precision == LFX_R64 ? 8 : 4;
+  const int64_t n = (int64_t)(bytes / esz);
+  const int grid = ctx->num_sms * 8;
+  if (precision == LFX_R64)
+    lma_x_plus_ay<double><<<grid, 256, 0, ctx->stream>>>(n, (const double*)x, a, (const double*)y,
+                                                          (double*)out);
+  else
+    lma_x_plus_ay<float><<<grid, 256, 0, ctx->stream>>>(n, (const float*)x, (float)a,
+                                                         (const float*)y, (float*)out);
+  ctx->launches++;
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
 extern "C" {
 
 int lfx_lma_create(lfx_ctx* ctx, int32_t ncell_2d, int32_t nlayers, int32_t ndf_to,
@@ -1910,6 +1936,42 @@ int lfx_lma_create_like(const lfx_op* src, const double* local_stencil, int32_t 
   op->lay->refcount++;
   op->precision = precision;
   int rc = upload_matrix(src->ctx, op, local_stencil);
+  if (rc) {
+    lfx_op_destroy(op);
+    return rc;
+  }
+  *out = op;
+  return LFX_OK;
+}
+
+int lfx_lma_sum(const lfx_op* x, double a, const lfx_op* y, lfx_op** out) {
+  if (!x || !y || !out) return LFX_INVALID_ARGUMENT;
+  *out = nullptr;
+  lfx_ctx* ctx = x->ctx;
+  if (y->ctx != ctx || y->lay != x->lay || y->precision != x->precision)
+    return fail(ctx, LFX_TYPE_MISMATCH,
+                "lfx_lma_sum: operators must share one layout (lfx_lma_create_like) and precision");
+  lfx_op* op = new lfx_op();
+  op->ctx = ctx;
+  op->lay = x->lay;
+  op->lay->refcount++;
+  op->precision = x->precision;
+  op->blk = x->blk;
+  int rc = dmalloc(ctx, &op->mat, x->mat_bytes);
+  if (!rc) {
+    op->mat_bytes = x->mat_bytes;
+    rc = x_plus_ay_copy(ctx, x->precision, x->mat, a, y->mat, op->mat, x->mat_bytes);
+  }
+  // the packed upper triangles, when both operators have them (the sum of
+  // two bitwise symmetric operators is bitwise symmetric)
+  if (!rc && x->smat && y->smat && x->sblk == y->sblk) {
+    rc = dmalloc(ctx, &op->smat, x->smat_bytes);
+    if (!rc) {
+      op->smat_bytes = x->smat_bytes;
+      op->sblk = x->sblk;
+      rc = x_plus_ay_copy(ctx, x->precision, x->smat, a, y->smat, op->smat, x->smat_bytes);
+    }
+  }
   if (rc) {
     lfx_op_destroy(op);
     return rc;

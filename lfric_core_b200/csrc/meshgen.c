@@ -536,8 +536,10 @@ int lfx_mg_lma_w0(int32_t ncell, int32_t nlayers, const int32_t* verts_on_cell,
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b)
           G[a][b] = Ji[a][0] * Ji[b][0] + Ji[a][1] * Ji[b][1] + Ji[a][2] * Ji[b][2];
+      /* the upper triangle; the lower one is its mirror image, so the
+       * local matrix is symmetric bit for bit */
       for (int i = 0; i < 8; ++i)
-        for (int j = 0; j < 8; ++j) {
+        for (int j = i; j < 8; ++j) {
           double kij = 0.0;
           for (int a = 0; a < 3; ++a)
             for (int b = 0; b < 3; ++b) kij += dphi[i][a] * G[a][b] * dphi[j][b];
@@ -545,7 +547,7 @@ int lfx_mg_lma_w0(int32_t ncell, int32_t nlayers, const int32_t* verts_on_cell,
         }
     }
     for (int i = 0; i < 8; ++i)
-      for (int j = 0; j < 8; ++j) LMA(lma, ik, i, j, 8, ncell3d) = A[i][j];
+      for (int j = 0; j < 8; ++j) LMA(lma, ik, i, j, 8, ncell3d) = i <= j ? A[i][j] : A[j][i];
   }
   return 0;
 }

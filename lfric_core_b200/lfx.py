@@ -67,6 +67,15 @@ class MrhsCfg(C.Structure):
 MRHS_TF32, MRHS_BF16 = 1, 2
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("cells_per_item", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("grid", C.c_int32), ("cooperative", C.c_int32), ("group_bytes", C.c_int64),
+                ("replays", C.c_int64), ("us_per_iteration", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # (name, argtypes, restype)
 _SIGS = [
     ("lfx_ctx_create", [C.c_int, C.POINTER(vp)], C.c_int),
@@ -103,6 +112,7 @@ _SIGS = [
                         C.c_int64, f64p, C.c_int32, i32p, i32p, C.c_int32, C.c_int32,
                         C.POINTER(vp)], C.c_int),
     ("lfx_lma_create_like", [vp, f64p, C.c_int32, C.POINTER(vp)], C.c_int),
+    ("lfx_lma_sum", [vp, C.c_double, vp, C.POINTER(vp)], C.c_int),
     ("lfx_op_apply", [vp, vp, vp], C.c_int),
     ("lfx_op_autotune", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                          C.POINTER(C.c_int32), C.POINTER(C.c_float)], C.c_int),
@@ -152,8 +162,12 @@ _SIGS = [
     ("lfx_fem_w2_operator", [vp, C.c_int32, C.c_int32, i32p, i32p, C.c_int64, f64p, C.c_double,
                              i32p, C.c_int64, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(vp),
                              C.POINTER(vp)], C.c_int),
-    ("lfx_batch_create", [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int32,
-                          C.POINTER(vp)], C.c_int),
+    ("lfx_batch_create", [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int32, C.POINTER(vp)],
+     C.c_int),
+    ("lfx_batch_autotune", [vp, C.c_int32, C.POINTER(BatchTuning)], C.c_int),
+    ("lfx_batch_get_tuning", [vp, C.POINTER(BatchTuning)], C.c_int),
+    ("lfx_batch_set_tuning", [vp, C.c_int32, C.c_int32, C.c_int64], C.c_int),
+    ("lfx_batch_set_wait_limit", [vp, C.c_double], C.c_int),
     ("lfx_batch_destroy", [vp], C.c_int),
     ("lfx_batch_admit", [vp, vp, vp, vp, vp, vp, C.c_double, C.c_int32, C.c_int64,
                          C.POINTER(C.c_int32)], C.c_int),
@@ -266,11 +280,15 @@ class Context:
 class _Handle:
     _destroy = None
 
-    def __del__(self):
+    def close(self):
+        """Destroys the device object now (otherwise when collected)."""
         h = getattr(self, "h", None)
         if h and self._destroy and _lib is not None:
             getattr(_lib, self._destroy)(h)
-            self.h = None
+        self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 class FieldVector(_Handle):
@@ -414,6 +432,16 @@ class LmaOperator(_Handle):
         op._parent = self
         return op
 
+    def x_plus_ay(self, a, y: "LmaOperator") -> "LmaOperator":
+        """operator_x_plus_ay: a new operator self + a y on the same layout
+        (y made from self, or self from y, by like())."""
+        h = vp()
+        self.ctx.check(self.ctx.L.lfx_lma_sum(self.h, float(a), y.h, C.byref(h)))
+        op = LmaOperator(self.ctx, *self._shape, None, None, self.undf_to, self.undf_from, None,
+                         None, None, precision=self.precision, _h=h)
+        op._parent = self
+        return op
+
     def apply(self, x, y):
         self.ctx.check(self.ctx.L.lfx_op_apply(self.h, x.h, y.h))
 
@@ -536,15 +564,19 @@ class MultiRhsOperator(_Handle):
 
 
 class Batch(_Handle):
-    """Continuous batching of independent SPD solves (lfx_batch)."""
+    """Continuous batching of independent SPD solves (lfx_batch): one
+    persistent kernel launch per step runs `iters` CG iterations of every
+    admitted slot. Admission takes the slot's Krylov state from free device
+    memory and is refused (admit returns None) while it would leave less than
+    reserve_bytes free or when every slot is taken."""
 
     _destroy = "lfx_batch_destroy"
 
-    def __init__(self, ctx, ndf, max_slots, max_dofs, max_entities, max_columns=0, iters=4):
+    def __init__(self, ctx, ndf, max_slots, reserve_bytes=2 << 30, iters=8):
         self.ctx = ctx
         h = vp()
-        ctx.check(ctx.L.lfx_batch_create(ctx.h, ndf, max_slots, max_dofs, max_entities,
-                                         max_columns, iters, C.byref(h)))
+        ctx.check(ctx.L.lfx_batch_create(ctx.h, ndf, max_slots, int(reserve_bytes), iters,
+                                         C.byref(h)))
         self.h = h
         self.max_slots = max_slots
         self._keep = {}
@@ -553,11 +585,28 @@ class Batch(_Handle):
         s = C.c_int32()
         rc = self.ctx.L.lfx_batch_admit(self.h, op64.h, op32.h, prec32.h, b.h, x.h, tol, max_iter,
                                         tag, C.byref(s))
-        if rc == 3:  # pools or slots full
+        if rc == 3:  # memory or slots full
             return None
         self.ctx.check(rc)
         self._keep[s.value] = (op64, op32, prec32, b, x)
         return s.value
+
+    def autotune(self, iters=4):
+        t = BatchTuning()
+        self.ctx.check(self.ctx.L.lfx_batch_autotune(self.h, iters, C.byref(t)))
+        return t.as_dict()
+
+    def tuning(self):
+        t = BatchTuning()
+        self.ctx.check(self.ctx.L.lfx_batch_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, cells_per_item, blocks_per_sm, group_bytes):
+        self.ctx.check(self.ctx.L.lfx_batch_set_tuning(self.h, cells_per_item, blocks_per_sm,
+                                                       int(group_bytes)))
+
+    def set_wait_limit(self, seconds):
+        self.ctx.check(self.ctx.L.lfx_batch_set_wait_limit(self.h, float(seconds)))
 
     def step(self):
         nd = C.c_int32()

@@ -214,7 +214,7 @@ def _run_batch_w2(args):
     x = lfx.FieldVector(ctx, [s.undf])
     x.set_scalar(0.0)
     info = cg.apply(x, s.b)
-    b = lfx.Batch(ctx, 6, 1, s.undf, s.entities, s.columns, 4)
+    b = lfx.Batch(ctx, 6, 1, reserve_bytes=1 << 30, iters=4)
     x2 = lfx.FieldVector(ctx, [s.undf])
     x2.set_scalar(0.0)
     slot = b.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x2, 1e-10, 20000)

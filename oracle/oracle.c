@@ -177,6 +177,24 @@ void or_dg_matrix_vector_code(int32_t cell, int32_t nlayers, double* lhs, const 
   or_matrix_vector_code(cell, nlayers, lhs, x, ncell_3d, matrix, ndf1, map1, ndf2, map2);
 }
 
+/* sci_operator_algebra_kernel_mod.F90:92-119 (operator_x_plus_ay_kernel_code):
+ *   do k = 0, nlayers - 1
+ *     ik = k + 1 + (cell-1)*nlayers
+ *     x_plus_ay(ik,:,:) = x(ik,:,:) + a*y(ik,:,:)
+ * the a*y + x of each entry is one fma, as everywhere in this restatement */
+void or_operator_x_plus_ay_code(int32_t cell, int32_t nlayers, int64_t ncell_3d, double* x_plus_ay,
+                                const double* x, double a, const double* y, int32_t ndf1,
+                                int32_t ndf2) {
+  for (int32_t k = 0; k < nlayers; ++k) {
+    const int64_t ik = k + (int64_t)(cell - 1) * nlayers; /* 0-based */
+    for (int32_t j = 0; j < ndf2; ++j)
+      for (int32_t i = 0; i < ndf1; ++i) {
+        const int64_t e = ik + ncell_3d * (i + (int64_t)ndf1 * j);
+        x_plus_ay[e] = fma(a, y[e], x[e]);
+      }
+  }
+}
+
 /* sci_tri_solve_kernel_mod.f90:125-154 */
 void or_tri_solve_code(int32_t nlayers, double* y, const double* x, const double* tri_0,
                        const double* tri_plus, const double* tri_minus, const int32_t* map) {

@@ -17,6 +17,7 @@
  *   CMA asm/app/appinv      components/science/source/kernel/columnwise_operators/sci_columnwise_op_{asm,app,appinv}_kernel_mod.F90
  *   tri_solve               components/science/source/kernel/solver/sci_tri_solve_kernel_mod.f90:72-156
  *   cg/bicgstab/gmres       components/science/source/solver/sci_iterative_solver_mod.f90:495-592, 645-779, 830-1003
+ *   operator_x_plus_ay      components/science/source/kernel/algebra/sci_operator_algebra_kernel_mod.F90:92-119
  *
  * Arithmetic conventions (shared with the device path so FP64 results can be
  * compared bit for bit): every "a = a + b*c" of the reference is one fused
@@ -57,6 +58,12 @@ void or_transpose_matrix_vector_code(int32_t cell, int32_t nlayers, double* lhs,
 void or_dg_matrix_vector_code(int32_t cell, int32_t nlayers, double* lhs, const double* x,
                               int64_t ncell_3d, const double* matrix, int32_t ndf1,
                               const int32_t* map1, int32_t ndf2, const int32_t* map2);
+/* operator_x_plus_ay_kernel_code for one cell column: x_plus_ay(ik,:,:) =
+ * x(ik,:,:) + a*y(ik,:,:), ik = k + 1 + (cell-1)*nlayers, k = 0..nlayers-1,
+ * on (ncell_3d, ndf1, ndf2) operators */
+void or_operator_x_plus_ay_code(int32_t cell, int32_t nlayers, int64_t ncell_3d, double* x_plus_ay,
+                                const double* x, double a, const double* y, int32_t ndf1,
+                                int32_t ndf2);
 void or_tri_solve_code(int32_t nlayers, double* y, const double* x, const double* tri_0,
                        const double* tri_plus, const double* tri_minus, const int32_t* map);
 void or_columnwise_op_asm_code(int32_t cell, int32_t nlayers, int32_t ncell_2d,

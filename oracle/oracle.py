@@ -47,6 +47,8 @@ def lib():
                                             C.c_int32, i32p, C.c_int32, i32p]
         L.or_transpose_matrix_vector_code.argtypes = L.or_matrix_vector_code.argtypes
         L.or_dg_matrix_vector_code.argtypes = L.or_matrix_vector_code.argtypes
+        L.or_operator_x_plus_ay_code.argtypes = [C.c_int32, C.c_int32, C.c_int64, f64p, f64p,
+                                                 C.c_double, f64p, C.c_int32, C.c_int32]
         L.or_tri_solve_code.argtypes = [C.c_int32, f64p, f64p, f64p, f64p, f64p, i32p]
         L.or_columnwise_op_asm_code.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, f64p,
                                                 f64p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
@@ -240,6 +242,19 @@ def _gcd(a, b):
 
 def _ceil_div(a, b):
     return -((-a) // b)
+
+
+def operator_x_plus_ay(x, a, y, ncell_2d, nlayers, ndf1, ndf2):
+    """x + a y of two (ncell_2d*nlayers, ndf1, ndf2) Fortran-order operators,
+    cell by cell as the reference's kernel loop."""
+    nc3 = ncell_2d * nlayers
+    out = np.zeros(nc3 * ndf1 * ndf2)
+    xa = np.ascontiguousarray(x, dtype=np.float64)
+    ya = np.ascontiguousarray(y, dtype=np.float64)
+    L = lib()
+    for cell in range(1, ncell_2d + 1):
+        L.or_operator_x_plus_ay_code(cell, nlayers, nc3, out, xa, float(a), ya, ndf1, ndf2)
+    return out
 
 
 def cma_params(alpha, beta, gamma_m, gamma_p):

@@ -12,6 +12,7 @@ Sources (paths inside the reference project):
   components/science/unit-test/kernel/columnwise_operators/columnwise_op_app_kernel_mod_test.pf
   components/science/unit-test/kernel/columnwise_operators/columnwise_op_{mul,scaledadd,
       asm_m2v_lumped_inv,asm_diag_hmht}_kernel_mod_test.pf
+  components/science/unit-test/kernel/algebra/operator_algebra_kernel_mod_test.pf
 """
 from __future__ import annotations
 
@@ -116,6 +117,21 @@ def cma_diag_hmht(text: str) -> dict:
             "reference_tol": fnum(re.search(r"tol\s*=\s*(" + NUM + ")", text).group(1))}
 
 
+def operator_x_plus_ay(text: str) -> dict:
+    # test_x_plus_ay: x(1,:,j) and y(1,:,j) constant per column j, scalar a,
+    # answers per column
+    body = text.split("subroutine test_x_plus_ay")[1].split("end subroutine test_x_plus_ay")[0]
+    ndf1 = int(re.search(r"ndf1\s*=\s*(\d+)", body).group(1))
+    ndf2 = int(re.search(r"ndf2\s*=\s*(\d+)", body).group(1))
+    xs = {int(j): fnum(v) for j, v in re.findall(r"\bx\(1,:,(\d)\)\s*=\s*(" + NUM + ")", body)}
+    ys = {int(j): fnum(v) for j, v in re.findall(r"\by\(1,:,(\d)\)\s*=\s*(" + NUM + ")", body)}
+    a = fnum(re.search(r"::\s*a\s*=\s*(" + NUM + ")", body).group(1))
+    ans = [fnum(v) for v in re.findall(r"answer\s*=\s*(" + NUM + ")", body)]
+    return {"ndf1": ndf1, "ndf2": ndf2, "x": [xs[j + 1] for j in range(ndf2)],
+            "y": [ys[j + 1] for j in range(ndf2)], "a": a, "answer": ans,
+            "tol": fnum(re.search(r"tol\s*=\s*(" + NUM + ")", body).group(1))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True, help="root of the reference checkout")
@@ -133,6 +149,7 @@ def main():
         "cma_m2v_lumped_inv":
             ut / "columnwise_operators/columnwise_op_asm_m2v_lumped_inv_kernel_mod_test.pf",
         "cma_diag_hmht": ut / "columnwise_operators/columnwise_op_asm_diag_hmht_kernel_mod_test.pf",
+        "operator_x_plus_ay": ut / "algebra/operator_algebra_kernel_mod_test.pf",
     }
     out = {
         "matrix_vector": matrix_vector(src["matrix_vector"].read_text()),
@@ -144,6 +161,7 @@ def main():
         "cma_scaledadd": cma_scaledadd(src["cma_scaledadd"].read_text()),
         "cma_m2v_lumped_inv": cma_m2v_lumped_inv(src["cma_m2v_lumped_inv"].read_text()),
         "cma_diag_hmht": cma_diag_hmht(src["cma_diag_hmht"].read_text()),
+        "operator_x_plus_ay": operator_x_plus_ay(src["operator_x_plus_ay"].read_text()),
     }
     for k, p in src.items():
         out[k]["source"] = str(p.relative_to(Path(a.ref)))

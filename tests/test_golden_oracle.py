@@ -215,3 +215,15 @@ def test_cma_diag_hmht_golden():
     cbd = np.arange(1, nl + 1, dtype=np.int32).reshape(nl, 1)
     C = orc.cma_diag_hmht(Dh, M2h, 1, nl, 1, 4, cbd, nl, 1, (1, 1, 0, 0))
     np.testing.assert_allclose(C.band, g["answer"], rtol=0, atol=g["reference_tol"])
+
+
+def test_operator_x_plus_ay_golden():
+    # operator_algebra_kernel_mod_test.pf test_x_plus_ay: one cell, one layer,
+    # 3x2 operators constant per column, a = 2
+    g = G["operator_x_plus_ay"]
+    ndf1, ndf2 = g["ndf1"], g["ndf2"]
+    x = np.array([[g["x"][j]] * ndf1 for j in range(ndf2)]).ravel()  # Fortran (1, ndf1, ndf2)
+    y = np.array([[g["y"][j]] * ndf1 for j in range(ndf2)]).ravel()
+    out = orc.operator_x_plus_ay(x, g["a"], y, 1, 1, ndf1, ndf2).reshape(ndf2, ndf1)
+    for j in range(ndf2):
+        assert np.all(np.abs(out[j] - g["answer"][j]) <= g["tol"])

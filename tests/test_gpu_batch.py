@@ -42,10 +42,10 @@ def w0_system(ctx, n, nl, seed):
     return dict(mesh=mesh, ops=ops, prec=prec, b=b, undf=undf, map=m)
 
 
-def run_batch(ctx, systems, tols, ndf=8, iters=4):
-    tot = sum(s["undf"] for s in systems)
-    ent = sum(len(np.unique(s["map"][:, :4])) if ndf == 8 else s["undf"] for s in systems) * 2
-    B = lfx.Batch(ctx, ndf, len(systems), tot, ent, 0, iters)
+def run_batch(ctx, systems, tols, ndf=8, iters=4, shape=None):
+    B = lfx.Batch(ctx, ndf, len(systems), reserve_bytes=1 << 30, iters=iters)
+    if shape:
+        B.set_tuning(*shape)
     xs = []
     for i, (s, tol) in enumerate(zip(systems, tols)):
         x = lfx.FieldVector(ctx, [s["undf"]])
@@ -84,12 +84,48 @@ def test_batch_results_same_alone_and_in_the_mix(ctx):
         assert rel <= tol * 1.0001, (rel, tol, info)
 
 
+def test_batch_results_do_not_depend_on_the_launch_shape(ctx):
+    """Columns per work item, blocks per SM and L2 group size change how the
+    persistent kernel splits the work, not the sums: the same bits."""
+    specs = [(5, 33, 1, 1e-9), (7, 12, 2, 1e-8), (4, 40, 3, 1e-10)]
+    systems = [w0_system(ctx, n, nl, sd) for n, nl, sd, _ in specs]
+    tols = [t for *_, t in specs]
+    ref = run_batch(ctx, systems, tols, shape=(64, 2, 1 << 40))
+    for shape in ((32, 1, 1 << 40), (128, 2, 1), (32, 2, 40_000)):
+        got = run_batch(ctx, systems, tols, iters=3, shape=shape)
+        for (xa, ia), (xb, ib) in zip(ref, got):
+            assert same(xa, xb) and ia["iterations"] == ib["iterations"], shape
+
+
+def test_batch_autotune_keeps_results(ctx):
+    """The autotuner's timed replays advance the solves; the results are the
+    bits of an untuned run."""
+    specs = [(6, 20, 4, 1e-9), (5, 45, 5, 1e-8)]
+    systems = [w0_system(ctx, n, nl, sd) for n, nl, sd, _ in specs]
+    tols = [t for *_, t in specs]
+    ref = run_batch(ctx, systems, tols)
+    B = lfx.Batch(ctx, 8, 2, reserve_bytes=1 << 30, iters=4)
+    xs = []
+    for s, tol in zip(systems, tols):
+        x = lfx.FieldVector(ctx, [s["undf"]])
+        x.set_scalar(0.0)
+        xs.append((B.admit(s["ops"][lfx.R64], s["ops"][lfx.R32], s["prec"], s["b"], x, tol, 5000), x))
+    t = B.autotune(iters=2)
+    assert t["cells_per_item"] in (32, 64, 128) and t["us_per_iteration"] > 0
+    for _ in range(2000):
+        if B.step() == 2:
+            break
+    for (slot, x), (xr, ir) in zip(xs, ref):
+        ph, _, info = B.slot(slot)
+        assert ph == 3 and info.iterations == ir["iterations"]
+        assert same(x.export_field(), xr)
+
+
 def test_batch_admission_while_running(ctx):
     """Slots admitted while others are iterating: results are unchanged."""
     systems = [w0_system(ctx, 6, 5, 10 + i) for i in range(3)]
     ref = [run_batch(ctx, [s], [1e-8])[0][0] for s in systems]
-    tot = sum(s["undf"] for s in systems)
-    B = lfx.Batch(ctx, 8, 2, tot, tot, 0, 2)
+    B = lfx.Batch(ctx, 8, 2, reserve_bytes=1 << 30, iters=2)
     xs = {}
     pending = list(range(3))
     finished = {}
@@ -127,8 +163,7 @@ def test_batch_w2_line_preconditioner(ctx):
     col = sum(s.columns for s in systems)
 
     def run(idx):
-        B = lfx.Batch(ctx, 6, len(idx), sum(systems[i].undf for i in idx),
-                      sum(systems[i].entities for i in idx), sum(systems[i].columns for i in idx), 3)
+        B = lfx.Batch(ctx, 6, len(idx), reserve_bytes=1 << 30, iters=3)
         xs = []
         for i in idx:
             s = systems[i]
@@ -147,19 +182,60 @@ def test_batch_w2_line_preconditioner(ctx):
 
     assert tot and ent and col
     mixed = run([0, 1, 2])
-    for i in range(3):
+    for (n, nl, sd), i in zip(((4, 6, 1), (6, 5, 2), (5, 9, 3)), range(3)):
         assert same(run([i])[0], mixed[i])
-        s = systems[i]
-        X = lfx.FieldVector.from_array(ctx, mixed[i])
-        R = lfx.FieldVector(ctx, [s.undf])
-        s.ops[lfx.R64].apply(X, R)
-        R.aypx(-1.0, s.b)
-        assert R.norm() / s.b.norm() <= tols[i] * 1.0001
+        # the true residual with the oracle's FP64 apply of the same system
+        # (the device assembly equals the host generator's matrices)
+        p = mg.w2_problem(n, nl, seed=sd)
+        npc, cic = p.mesh.colour_lookup()
+        op = orc.LmaOperator(p.ncell_2d, nl, 6, 6, p.map, p.map, p.undf, p.undf, p.lma, npc, cic)
+        b = systems[i].b.export_field()
+        rel = np.linalg.norm(b - op.apply(mixed[i])) / np.linalg.norm(b)
+        assert rel <= tols[i] * 1.0001, (i, rel)
 
 
 def test_batch_refuses_when_full(ctx):
     s = w0_system(ctx, 4, 3, 5)
-    B = lfx.Batch(ctx, 8, 1, s["undf"], s["undf"], 0, 2)
+    B = lfx.Batch(ctx, 8, 1, reserve_bytes=1 << 30, iters=2)
     x1, x2 = lfx.FieldVector(ctx, [s["undf"]]), lfx.FieldVector(ctx, [s["undf"]])
     assert B.admit(s["ops"][lfx.R64], s["ops"][lfx.R32], s["prec"], s["b"], x1, 1e-8) is not None
     assert B.admit(s["ops"][lfx.R64], s["ops"][lfx.R32], s["prec"], s["b"], x2, 1e-8) is None
+
+
+def test_batch_admission_by_free_device_memory(ctx):
+    """A reserve larger than the device's memory refuses every admission; a
+    small one admits."""
+    import torch
+    s = w0_system(ctx, 4, 3, 6)
+    total = torch.cuda.get_device_properties(0).total_memory
+    x = lfx.FieldVector(ctx, [s["undf"]])
+    full = lfx.Batch(ctx, 8, 4, reserve_bytes=total, iters=2)
+    assert full.admit(s["ops"][lfx.R64], s["ops"][lfx.R32], s["prec"], s["b"], x, 1e-8) is None
+    ok = lfx.Batch(ctx, 8, 4, reserve_bytes=1 << 20, iters=2)
+    x.set_scalar(0.0)
+    slot = ok.admit(s["ops"][lfx.R64], s["ops"][lfx.R32], s["prec"], s["b"], x, 1e-8)
+    assert slot is not None
+    for _ in range(1000):
+        if ok.step() == 1:
+            break
+    assert ok.slot(slot)[0] == 3
+
+
+def test_batch_barrier_wait_limit_runs_out_and_context_survives(ctx):
+    """With a wait limit of one nanosecond every grid-barrier wait of the
+    persistent kernel gives up at its first poll: the kernel sets LFX_TIMEOUT
+    and every block leaves at its next barrier (no copy is in flight in that
+    kernel). The step reports the timeout, and the context then runs a fresh
+    batch to the same bits as before."""
+    s = w0_system(ctx, 5, 6, 31)
+    ref = run_batch(ctx, [s], [1e-8])[0][0]
+    B = lfx.Batch(ctx, 8, 1, reserve_bytes=1 << 30, iters=2)
+    B.set_wait_limit(1e-9)
+    x = lfx.FieldVector(ctx, [s["undf"]])
+    x.set_scalar(0.0)
+    assert B.admit(s["ops"][lfx.R64], s["ops"][lfx.R32], s["prec"], s["b"], x, 1e-8) is not None
+    with pytest.raises(lfx.LfxError) as e:
+        B.step()
+    assert e.value.status == 6  # LFX_TIMEOUT
+    B.close()
+    assert same(run_batch(ctx, [s], [1e-8])[0][0], ref)

@@ -630,3 +630,39 @@ def test_argument_errors(ctx):
     with pytest.raises(lfx.LfxError) as e:
         lfx.LmaOperator(ctx, p.ncell_2d, 2, 8, 8, p.map, p.map, p.undf, p.undf, p.lma, npc, cic_bad)
     assert e.value.status == 4
+
+
+def test_lma_sum_operator_x_plus_ay_bitwise(ctx):
+    """A = M2 + tau D^T D formed on the device from two operators on one
+    layout (operator_x_plus_ay) applies bit for bit like the oracle's operator
+    built from the oracle's own sum, with every apply kernel; the FP32 pair
+    agrees to FP32 rounding."""
+    q = mg.w2_problem(6, 5, seed=9, keep_parts=True)
+    nc3, tau = q.mesh.ncell_3d, q.extra["tau"]
+    D = q.extra["div"].reshape(6, nc3)          # Fortran (nc3, 1, 6): [j][ik]
+    dtd = (D[None, :, :] * D[:, None, :]).ravel()  # Fortran (nc3, 6, 6): [j][i][ik] = D_i D_j
+    m2 = q.extra["m2"]
+    npc, cic = q.mesh.colour_lookup()
+    opM = lfx.LmaOperator(ctx, q.ncell_2d, 5, 6, 6, q.map, q.map, q.undf, q.undf, m2, npc, cic)
+    opA = opM.x_plus_ay(tau, opM.like(dtd, lfx.R64))
+    host = orc.operator_x_plus_ay(m2, tau, dtd, q.ncell_2d, 5, 6, 6)
+    assert np.allclose(host, q.lma, rtol=1e-12, atol=1e-15)
+    oA = orc.LmaOperator(q.ncell_2d, 5, 6, 6, q.map, q.map, q.undf, q.undf, host, npc, cic)
+    x = mg.normal(17, q.undf)
+    want = oA.apply(x)
+    X, Y = lfx.FieldVector.from_array(ctx, x), lfx.FieldVector(ctx, [q.undf])
+    for kernel in (1, 3, 5):
+        ctx.set_apply_kernel(kernel)
+        try:
+            opA.apply(X, Y)
+        finally:
+            ctx.set_apply_kernel(-1)
+        assert same(Y.export_field(), want), kernel
+    op32 = opM.like(m2, lfx.R32).x_plus_ay(tau, opM.like(dtd, lfx.R32))
+    X32, Y32 = lfx.FieldVector.from_array(ctx, x, lfx.R32), lfx.FieldVector(ctx, [q.undf], lfx.R32)
+    op32.apply(X32, Y32)
+    err = np.linalg.norm(Y32.export_field() - want) / np.linalg.norm(want)
+    assert err < 1e-6
+    with pytest.raises(lfx.LfxError) as e:
+        opM.x_plus_ay(1.0, op32)  # precisions differ
+    assert e.value.status == 5

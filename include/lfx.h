@@ -479,15 +479,23 @@ int lfx_mrhs_time_apply(lfx_mrhs* m, const float* x, float* y, int32_t reps, flo
  * that fit) over reps applies and keeps the fastest; outputs (nullable) the
  * choice and its time per apply in microseconds */
 int lfx_mrhs_autotune(lfx_mrhs* m, int32_t reps, int32_t* levels_per_block, float* us);
+enum { LFX_MRHS_PER_RHS_CG = 0, LFX_MRHS_BLOCK_CG = 1 };
 typedef struct {
   double r_tol;      /* per right-hand side: ||b - A x|| <= r_tol ||b - A x0|| */
   double inner_tol;  /* each inner FP32 solve reduces its residual by this */
   int32_t max_outer; /* refinement steps, at most */
   int32_t max_inner; /* iterations of one inner solve, at most */
+  /* inner solver: LFX_MRHS_PER_RHS_CG, CG on every right-hand side with its
+   * own step lengths; LFX_MRHS_BLOCK_CG, breakdown-free block CG over the
+   * 64 right-hand sides together (64 only): one search space for all of
+   * them, directions that become dependent dropped by a pivoted Cholesky
+   * orthonormalisation (the block Krylov idea of block_gcr_solve,
+   * sci_iterative_solver_mod.f90:1461-1628, in CG form) */
+  int32_t method;
 } lfx_mrhs_cfg;
 /* FP64 iterative refinement around an FP32 Jacobi-preconditioned CG run on
- * all right-hand sides together (each with its own step lengths), with the
- * tensor-core apply. op64: the FP64 operator (residuals); diag: its FP64
+ * all right-hand sides together (cfg->method: each with its own step
+ * lengths, or one block CG), with the tensor-core apply. op64: the FP64 operator (residuals); diag: its FP64
  * diagonal (lfx_lma_diagonal). b, x: device arrays of nrhs FP64 vectors,
  * right-hand side r at b + r * ld (x: initial guess in, solution out). info:
  * nrhs entries; iterations = inner iterations of that right-hand side,

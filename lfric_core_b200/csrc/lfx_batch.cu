@@ -68,6 +68,7 @@ constexpr int kMaxIters = 64;    // super-iterations per launch, at most
 constexpr int kMaxSeg = 4;       // warps (segments of <= 31 levels) per cell column, at most
 constexpr int kMaxCB = 128;      // cell columns per apply item, at most
 constexpr int kMaxUnits = kMaxCB * kMaxSeg;
+constexpr int kMaxColours = 8;   // cell colours of a slot, at most
 constexpr int kBCols = 64;       // columns per sweep item
 constexpr int kBRows = 160;      // rows per preconditioner column, at most
 
@@ -110,7 +111,7 @@ struct BState {
 // so lists can be rebuilt and reallocated between replays)
 struct BParams {
   const int4* items32;  // FP32 apply items {slot, q0, columns, first dot block}
-  const int* off32;     // [4 * ngr32 + 1]: items of group g, colour c from off32[4g + c]
+  const int* off32;     // [ncolour * ngr32 + 1]: items of group g, colour c from off32[g ncolour + c]
   const int4* items64;  // FP64 residual items {slot, q0, columns, 0}
   const int* off64;
   const int2* chunks;   // {slot, chunk}
@@ -122,7 +123,7 @@ struct BParams {
   unsigned* bar;        // grid barrier {count, generation}
   int* err;             // LFX_TIMEOUT when a wait ran out
   int ngr32, ngr64, nchunk, ncolitem;
-  int iters, max_slots, any_cma, pad;
+  int iters, max_slots, any_cma, ncolour;
   unsigned long long timeout_ns;
 };
 
@@ -620,9 +621,9 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
   for (int it = 0; it < P.iters; ++it) {
     // ---- A: z = A32 p, alpha
     for (int g = 0; g < P.ngr32; ++g)
-      for (int c = 0; c < 4; ++c) {
-        apply_phase<NDF, false>(P, sh, P.items32, __ldg(P.off32 + 4 * g + c),
-                                __ldg(P.off32 + 4 * g + c + 1));
+      for (int c = 0; c < P.ncolour; ++c) {
+        const int o = g * P.ncolour + c;
+        apply_phase<NDF, false>(P, sh, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1));
         if (!grid_sync(P, sh)) return;
       }
     // ---- U: xc += alpha p, r -= alpha z, ||r||^2 (+ <r, r/d>, beta for Jacobi slots)
@@ -666,9 +667,9 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
           [](const BSlot&, BState&, const double*) {});
       if (!grid_sync(P, sh)) return;
       for (int g = 0; g < P.ngr64; ++g)
-        for (int c = 0; c < 4; ++c) {
-          apply_phase<NDF, true>(P, sh, P.items64, __ldg(P.off64 + 4 * g + c),
-                                 __ldg(P.off64 + 4 * g + c + 1));
+        for (int c = 0; c < P.ncolour; ++c) {
+          const int o = g * P.ncolour + c;
+          apply_phase<NDF, true>(P, sh, P.items64, __ldg(P.off64 + o), __ldg(P.off64 + o + 1));
           if (!grid_sync(P, sh)) return;
         }
       chunk_phase<2>(
@@ -843,9 +844,9 @@ const void* pick_kernel(int ndf, bool cma) {
 // apply items of one precision: slots greedily grouped so that a group's
 // vectors (bytes_per_dof per dof) stay within group_bytes; per group and
 // colour the slots' runs of cells_per_item cell columns
-void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int bytes_per_dof,
-                       bool dots, std::vector<int4>& items, std::vector<int>& off,
-                       std::vector<int>* nitem) {
+void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int ncolour,
+                       int bytes_per_dof, bool dots, std::vector<int4>& items,
+                       std::vector<int>& off, std::vector<int>* nitem) {
   items.clear();
   off.clear();
   std::vector<std::vector<int>> groups;
@@ -861,7 +862,7 @@ void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int byte
   }
   const int cb = B->cells_per_item;
   for (auto& g : groups)
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < ncolour; ++c) {
       off.push_back((int)items.size());
       for (int s : g) {
         const SlotHost& H = B->slots[s];
@@ -891,10 +892,13 @@ int rebuild(lfx_batch* B) {
     }
   }
   B->nactive = (int)act.size();
+  // colour phases: as many as the slot with the most colours has
+  int ncolour = 1;
+  for (int s : act) ncolour = std::max(ncolour, (int)B->slots[s].cstart.size() - 1);
   std::vector<int4> it32, it64;
   std::vector<int> off32, off64, nitem(B->max_slots, 0);
-  build_apply_items(B, act, 8, true, it32, off32, &nitem);
-  build_apply_items(B, act, 16, false, it64, off64, nullptr);
+  build_apply_items(B, act, ncolour, 8, true, it32, off32, &nitem);
+  build_apply_items(B, act, ncolour, 16, false, it64, off64, nullptr);
   std::vector<int2> ch, col;
   for (int s : act) {
     const SlotHost& H = B->slots[s];
@@ -934,8 +938,9 @@ int rebuild(lfx_batch* B) {
   P.need = B->d_need;
   P.bar = B->d_bar;
   P.err = B->d_err;
-  P.ngr32 = (int)off32.size() / 4;
-  P.ngr64 = (int)off64.size() / 4;
+  P.ngr32 = (int)(off32.size() - 1) / ncolour;
+  P.ngr64 = (int)(off64.size() - 1) / ncolour;
+  P.ncolour = ncolour;
   P.nchunk = (int)ch.size();
   P.ncolitem = (int)col.size();
   P.iters = B->iters;
@@ -1189,8 +1194,8 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   int ndot = 0;
   for (size_t c = 0; c + 1 < L->colour_start.size(); ++c)
     ndot += (L->colour_start[c + 1] - L->colour_start[c] + kDotCols - 1) / kDotCols;
-  if (L->colour_start.size() != 5)
-    return fail(ctx, LFX_NOT_SUPPORTED, "batch: four colours");
+  if (L->colour_start.size() < 2 || (int)L->colour_start.size() - 1 > kMaxColours)
+    return fail(ctx, LFX_NOT_SUPPORTED, "batch: at most 8 cell colours");
   // admission by free device memory: the slot's state, its share of the
   // work lists, and the batch's reserve must fit
   const int64_t need = slot_bytes(n, nch, ndot);

@@ -549,6 +549,368 @@ __global__ void k_dinv(int64_t n, const double* __restrict__ d, float* __restric
   if (i < n) dinv[i] = (float)(1.0 / d[i]);
 }
 
+// ------------------------------------------------ block CG
+// Breakdown-free block preconditioned CG on all 64 right-hand sides at once
+// (the block Krylov method of the reference's block_gcr_solve family,
+// sci_iterative_solver_mod.f90:1461-1628, in its CG form):
+//   Z = D^-1 R, P = orth(Z)
+//   loop: Q = A P; alpha = (P^T Q)^-1 P^T R; X += P alpha; R -= Q alpha;
+//         beta = -(P^T Q)^-1 Q^T D^-1 R; P = orth(D^-1 R + P beta)
+// orth(W) = W T with T from a pivoted Cholesky factorisation of W^T W that
+// stops at pivots below kBcgDrop times the largest one: directions the block
+// no longer spans (right-hand sides that have converged, or become
+// dependent) are dropped, so the method does not break down. The products
+// with the tall n x 64 blocks run as 32-row chunks staged in shared memory,
+// each thread holding a 4 x 4 (Gram) or 2 x 4 (update) register tile; the
+// Gram sums are FP32 within a chunk, FP64 across chunks and blocks, in a
+// fixed order; the 64 x 64 algebra runs in FP64 in one block.
+constexpr int kBS = 64;          // right-hand sides of a block solve
+constexpr int kBcgRows = 32;     // rows per staged chunk
+constexpr double kBcgDrop = 1e-10;
+
+struct BcgSmall {
+  double C[2 * kBS * kBS];  // [v][i][j]: v = 0 P^T Q, v = 1 P^T R (gram of P with Q, R)
+  double E[kBS * kBS];      // Q^T D^-1 R
+  double G[kBS * kBS];      // W^T W
+  double L1[kBS * kBS];     // Cholesky factor of the active block of P^T Q
+  double r0[kBS], rn[kBS];
+  float coef[kBS * kBS];    // alpha, beta or T [k][j] for the next row update
+  int active[kBS];          // right-hand sides the solve works on
+  int rank, done, iters, fail;
+};
+
+// stage rows [row0, row0 + rows) of an n x 64 row-major block into smem,
+// rows scaled by scale[row] when given; rows past n read as zero
+__device__ __forceinline__ void bcg_stage(float (*dst)[kBS], const float* __restrict__ src,
+                                          int64_t row0, int rows, const float* __restrict__ scale) {
+  for (int e = threadIdx.x; e < kBcgRows * (kBS / 4); e += blockDim.x) {
+    const int r = e / (kBS / 4), c4 = e % (kBS / 4);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (r < rows) {
+      v = ld4(src + (size_t)(row0 + r) * kBS + 4 * c4);
+      if (scale) {
+        const float sc = scale[row0 + r];
+        v.x *= sc; v.y *= sc; v.z *= sc; v.w *= sc;
+      }
+    }
+    *reinterpret_cast<float4*>(&dst[r][4 * c4]) = v;
+  }
+}
+
+// partials[block][v][i][j] = sum over the block's rows of U[row][i] V_v[row][j]
+// (V_v rows scaled by vscale[row] when given); 256 threads, 4 x 4 tiles
+template <int NV>
+__global__ void __launch_bounds__(256) bcg_gram(int64_t n, const float* __restrict__ U,
+                                                const float* __restrict__ V0,
+                                                const float* __restrict__ V1,
+                                                const float* __restrict__ vscale,
+                                                double* __restrict__ partials,
+                                                const BcgSmall* st) {
+  __shared__ __align__(16) float Us[kBcgRows][kBS];
+  __shared__ __align__(16) float Vs[NV][kBcgRows][kBS];
+  if (st->done) return;
+  const int i0 = 4 * (threadIdx.x / 16), j0 = 4 * (threadIdx.x % 16);
+  double acc[NV][4][4];
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[v][a][b] = 0.0;
+  for (int64_t c = blockIdx.x; c * kBcgRows < n; c += gridDim.x) {
+    const int64_t row0 = c * kBcgRows;
+    const int rows = (int)(n - row0 < (int64_t)kBcgRows ? n - row0 : (int64_t)kBcgRows);
+    __syncthreads();
+    bcg_stage(Us, U, row0, rows, nullptr);
+    bcg_stage(Vs[0], V0, row0, rows, vscale);
+    if (NV > 1) bcg_stage(Vs[NV - 1], V1, row0, rows, vscale);
+    __syncthreads();
+    float a[NV][4][4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) a[v][x][y] = 0.f;
+#pragma unroll 4
+    for (int r = 0; r < kBcgRows; ++r) {
+      const float4 u = *reinterpret_cast<const float4*>(&Us[r][i0]);
+      const float uu[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const float4 w = *reinterpret_cast<const float4*>(&Vs[v][r][j0]);
+        const float ww[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) a[v][x][y] = fmaf(uu[x], ww[y], a[v][x][y]);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[v][x][y] += (double)a[v][x][y];
+  }
+  double* out = partials + (size_t)blockIdx.x * NV * kBS * kBS;
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) out[((size_t)v * kBS + i0 + x) * kBS + j0 + y] = acc[v][x][y];
+}
+
+// out[e] = sum over the blocks, in block order, of partials[b][e]
+__global__ void bcg_reduce(int nb, int ne, const double* __restrict__ partials,
+                           double* __restrict__ out, const BcgSmall* st) {
+  if (st->done) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s = s + partials[(size_t)b * ne + e];
+  out[e] = s;
+}
+
+// Y (+)= B C for one or two row blocks: mode 0: X += P C, R -= Q C and the
+// column sums of R^2 into partials[block][64]; mode 1: W = D^-1 R + P C;
+// mode 2: P = W C. With skip_p the products are left out (taken as zero,
+// whatever the blocks hold): mode 0 then only sums R^2, mode 1 sets
+// W = D^-1 R.
+template <int MODE>
+__global__ void __launch_bounds__(256) bcg_update(int64_t n, const float* __restrict__ A0,
+                                                  const float* __restrict__ A1, float* Y0,
+                                                  float* Y1, const float* __restrict__ dinv,
+                                                  const BcgSmall* st, int skip_p,
+                                                  double* __restrict__ partials) {
+  __shared__ __align__(16) float Cs[kBS][kBS];
+  __shared__ __align__(16) float As[2][kBcgRows][kBS];
+  __shared__ double red[16][kBS];
+  if (st->done) return;
+  for (int e = threadIdx.x; e < kBS * kBS; e += blockDim.x) Cs[e / kBS][e % kBS] = st->coef[e];
+  const int r0 = 2 * (threadIdx.x / 16), c0 = 4 * (threadIdx.x % 16);
+  double nrm[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t c = blockIdx.x; c * kBcgRows < n; c += gridDim.x) {
+    const int64_t row0 = c * kBcgRows;
+    const int rows = (int)(n - row0 < (int64_t)kBcgRows ? n - row0 : (int64_t)kBcgRows);
+    __syncthreads();
+    if (!skip_p) bcg_stage(As[0], A0, row0, rows, nullptr);
+    if (MODE == 0 && !skip_p) bcg_stage(As[1], A1, row0, rows, nullptr);
+    __syncthreads();
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+      const int r = r0 + rr;
+      if (r >= rows) continue;
+      const size_t o = (size_t)(row0 + r) * kBS + c0;
+      float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f};
+      if (!skip_p) {
+#pragma unroll 8
+        for (int k = 0; k < kBS; ++k) {
+          const float4 cf = *reinterpret_cast<const float4*>(&Cs[k][c0]);
+          const float a0 = As[0][r][k];
+          d0[0] = fmaf(a0, cf.x, d0[0]); d0[1] = fmaf(a0, cf.y, d0[1]);
+          d0[2] = fmaf(a0, cf.z, d0[2]); d0[3] = fmaf(a0, cf.w, d0[3]);
+          if (MODE == 0) {
+            const float a1 = As[1][r][k];
+            d1[0] = fmaf(a1, cf.x, d1[0]); d1[1] = fmaf(a1, cf.y, d1[1]);
+            d1[2] = fmaf(a1, cf.z, d1[2]); d1[3] = fmaf(a1, cf.w, d1[3]);
+          }
+        }
+      }
+      if (MODE == 0) {
+        const float4 x = ld4(Y0 + o), rv = ld4(Y1 + o);
+        st4(Y0 + o, make_float4(x.x + d0[0], x.y + d0[1], x.z + d0[2], x.w + d0[3]));
+        const float rn[4] = {rv.x - d1[0], rv.y - d1[1], rv.z - d1[2], rv.w - d1[3]};
+        st4(Y1 + o, make_float4(rn[0], rn[1], rn[2], rn[3]));
+#pragma unroll
+        for (int j = 0; j < 4; ++j) nrm[j] = fma((double)rn[j], (double)rn[j], nrm[j]);
+      } else if (MODE == 1) {
+        const float4 rv = ld4(A1 + o);
+        const float dv = dinv[row0 + r];
+        st4(Y0 + o, make_float4(fmaf(rv.x, dv, d0[0]), fmaf(rv.y, dv, d0[1]),
+                                fmaf(rv.z, dv, d0[2]), fmaf(rv.w, dv, d0[3])));
+      } else {
+        st4(Y0 + o, make_float4(d0[0], d0[1], d0[2], d0[3]));
+      }
+    }
+  }
+  if (MODE == 0) {
+    // column sums of R^2: threads with the same c0 (16 of them, one per row
+    // pair) in a fixed order
+#pragma unroll
+    for (int j = 0; j < 4; ++j) red[threadIdx.x / 16][c0 + j] = nrm[j];
+    __syncthreads();
+    if (threadIdx.x < kBS) {
+      double s = 0.0;
+      for (int q = 0; q < 16; ++q) s = s + red[q][threadIdx.x];
+      partials[(size_t)blockIdx.x * kBS + threadIdx.x] = s;
+    }
+  }
+}
+
+// column norms ||R_j|| of the initial residual (r0) and, for the columns not
+// active, R_j = 0 so the block leaves them alone
+__global__ void __launch_bounds__(256) bcg_mask(int64_t n, float* R, const int* act) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * kBS;
+       e += (int64_t)gridDim.x * blockDim.x)
+    if (!act[e % kBS]) R[e] = 0.f;
+}
+
+// The 64 x 64 algebra of one step, in FP64, one block of 256 threads.
+// mode 0 (alpha): L1 = chol(active block of P^T Q); alpha = L1^-T L1^-1 P^T R
+// mode 1 (beta): rn = sqrt(column sums) (convergence: done when every active
+//   right-hand side has rn <= tol r0); beta = -(P^T Q)^-1 Q^T D^-1 R
+// mode 2 (orth): pivoted Cholesky of W^T W -> rank and T (P = W T)
+// mode 3 (norms of the initial residual into r0)
+constexpr size_t kBcgSmallSmem = 2 * sizeof(double) * kBS * (kBS + 1);
+
+__global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double tol) {
+  // two 64 x 65 FP64 matrices in dynamic shared memory (kBcgSmallSmem)
+  extern __shared__ double bcg_dyn[];
+  double (*M)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn);
+  double (*Bm)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn + kBS * (kBS + 1));
+  __shared__ int perm[kBS];
+  __shared__ int s_r, s_stop;
+  const int t = threadIdx.x;
+  if (st->done) return;
+  if (mode == 3) {
+    // the column sums of R^2 were reduced into rn
+    if (t < kBS) {
+      st->r0[t] = sqrt(st->rn[t]);
+      st->rn[t] = st->r0[t];
+    }
+    return;
+  }
+  if (mode == 0 || mode == 1) {
+    const int r = st->rank;
+    if (mode == 0) {
+      // Cholesky of the r x r active block of P^T Q (column by column)
+      for (int e = t; e < kBS * kBS; e += blockDim.x) M[e / kBS][e % kBS] = st->C[e];
+      if (t == 0) s_stop = 0;
+      __syncthreads();
+      for (int k = 0; k < r; ++k) {
+        if (t == 0) {
+          const double d = M[k][k];
+          if (!(d > 0.0)) s_stop = 1;
+          M[k][k] = d > 0.0 ? sqrt(d) : 1.0;
+        }
+        __syncthreads();
+        if (s_stop) break;
+        for (int i = k + 1 + t; i < r; i += blockDim.x) M[i][k] /= M[k][k];
+        __syncthreads();
+        for (int e = t; e < (r - k - 1) * (r - k - 1); e += blockDim.x) {
+          const int i = k + 1 + e / (r - k - 1), j = k + 1 + e % (r - k - 1);
+          if (j <= i) M[i][j] -= M[i][k] * M[j][k];
+        }
+        __syncthreads();
+      }
+      if (s_stop) {
+        if (t == 0) { st->fail = 1; st->done = 1; }
+        return;
+      }
+      for (int e = t; e < kBS * kBS; e += blockDim.x) st->L1[e] = M[e / kBS][e % kBS];
+      // right-hand sides: P^T R
+      for (int e = t; e < kBS * kBS; e += blockDim.x) Bm[e / kBS][e % kBS] = st->C[kBS * kBS + e];
+    } else {
+      if (t < kBS) st->rn[t] = sqrt(st->rn[t]);
+      __syncthreads();
+      if (t == 0) {
+        int done = 1;
+        for (int j = 0; j < kBS; ++j)
+          if (st->active[j] && st->rn[j] > tol * st->r0[j]) done = 0;
+        st->iters += 1;
+        s_stop = done;
+      }
+      __syncthreads();
+      if (s_stop) {
+        if (t == 0) st->done = 1;
+        return;
+      }
+      for (int e = t; e < kBS * kBS; e += blockDim.x) {
+        M[e / kBS][e % kBS] = st->L1[e];
+        Bm[e / kBS][e % kBS] = -st->E[e];
+      }
+    }
+    __syncthreads();
+    // solve L L^T Y = B on the first r rows, column j per thread
+    if (t < kBS) {
+      const int j = t;
+      for (int i = 0; i < r; ++i) {
+        double v = Bm[i][j];
+        for (int k = 0; k < i; ++k) v -= M[i][k] * Bm[k][j];
+        Bm[i][j] = v / M[i][i];
+      }
+      for (int i = r - 1; i >= 0; --i) {
+        double v = Bm[i][j];
+        for (int k = i + 1; k < r; ++k) v -= M[k][i] * Bm[k][j];
+        Bm[i][j] = v / M[i][i];
+      }
+      for (int i = 0; i < kBS; ++i) st->coef[i * kBS + j] = i < r ? (float)Bm[i][j] : 0.f;
+    }
+    return;
+  }
+  // mode 2: pivoted Cholesky of G = W^T W, stopping at pivots below
+  // kBcgDrop times the largest diagonal entry
+  for (int e = t; e < kBS * kBS; e += blockDim.x) M[e / kBS][e % kBS] = st->G[e];
+  if (t < kBS) perm[t] = t;
+  if (t == 0) s_r = 0;
+  __syncthreads();
+  double dmax = 0.0;
+  for (int i = 0; i < kBS; ++i) dmax = fmax(dmax, M[i][i]);
+  for (int k = 0; k < kBS; ++k) {
+    if (t == 0) {
+      int p = k;
+      for (int i = k + 1; i < kBS; ++i)
+        if (M[i][i] > M[p][p]) p = i;
+      s_stop = !(M[p][p] > kBcgDrop * dmax) || !(dmax > 0.0);
+      if (!s_stop && p != k) {
+        for (int j = 0; j < kBS; ++j) { const double tmp = M[k][j]; M[k][j] = M[p][j]; M[p][j] = tmp; }
+        for (int i = 0; i < kBS; ++i) { const double tmp = M[i][k]; M[i][k] = M[i][p]; M[i][p] = tmp; }
+        const int tp = perm[k]; perm[k] = perm[p]; perm[p] = tp;
+      }
+      if (!s_stop) {
+        M[k][k] = sqrt(M[k][k]);
+        s_r = k + 1;
+      }
+    }
+    __syncthreads();
+    if (s_stop) break;
+    for (int i = k + 1 + t; i < kBS; i += blockDim.x) M[i][k] /= M[k][k];
+    __syncthreads();
+    const int m = kBS - k - 1;
+    for (int e = t; e < m * m; e += blockDim.x) {
+      const int i = k + 1 + e / m, j = k + 1 + e % m;
+      M[i][j] -= M[i][k] * M[j][k];
+    }
+    __syncthreads();
+  }
+  const int r = s_r;
+  // Linv = L^-1 (r x r, lower): column j per thread
+  if (t < r) {
+    const int j = t;
+    for (int i = 0; i < r; ++i) Bm[i][j] = 0.0;
+    Bm[j][j] = 1.0 / M[j][j];
+    for (int i = j + 1; i < r; ++i) {
+      double v = 0.0;
+      for (int k = j; k < i; ++k) v -= M[i][k] * Bm[k][j];
+      Bm[i][j] = v / M[i][i];
+    }
+  }
+  __syncthreads();
+  // T[perm[i]][j] = Linv[j][i] (i <= j < r), zero elsewhere
+  for (int e = t; e < kBS * kBS; e += blockDim.x) st->coef[e] = 0.f;
+  __syncthreads();
+  for (int e = t; e < r * r; e += blockDim.x) {
+    const int i = e / r, j = e % r;
+    if (i <= j) st->coef[perm[i] * kBS + j] = (float)Bm[j][i];
+  }
+  if (t == 0) {
+    st->rank = r;
+    if (r == 0) st->done = 1;
+  }
+}
+
 }  // namespace
 
 struct lfx_mrhs {
@@ -577,6 +939,12 @@ struct lfx_mrhs {
   unsigned* ticket = nullptr;
   int grid = 0;
   size_t work_bytes = 0;
+  // block CG: W, the small algebra state and the Gram partials
+  float* w32 = nullptr;
+  BcgSmall* bcg = nullptr;
+  BcgSmall* h_bcg = nullptr;  // pinned
+  double* bpart = nullptr;
+  int bgrid = 0;
 };
 
 namespace {
@@ -641,6 +1009,10 @@ void mrhs_free(lfx_mrhs* m) {
   dfree(ctx, m->ticket, sizeof(unsigned));
   if (m->h_nrm) cudaFreeHost(m->h_nrm);
   if (m->h_S) cudaFreeHost(m->h_S);
+  dfree(ctx, m->w32, v32);
+  dfree(ctx, m->bcg, sizeof(BcgSmall));
+  dfree(ctx, m->bpart, sizeof(double) * 2 * kBS * kBS * m->bgrid);
+  if (m->h_bcg) cudaFreeHost(m->h_bcg);
 }
 
 }  // namespace
@@ -1039,6 +1411,88 @@ int inner_solve(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inn
   return LFX_OK;
 }
 
+int ensure_bcg(lfx_mrhs* m) {
+  if (m->bcg) return LFX_OK;
+  lfx_ctx* ctx = m->ctx;
+  LFX_CK(ctx, cudaFuncSetAttribute(bcg_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kBcgSmallSmem));
+  m->bgrid = ctx->num_sms * 2;
+  int rc = dmalloc(ctx, (void**)&m->w32, (size_t)m->undf * m->nrhs * 4);
+  if (!rc) rc = dmalloc(ctx, (void**)&m->bcg, sizeof(BcgSmall));
+  if (!rc) rc = dmalloc(ctx, (void**)&m->bpart, sizeof(double) * 2 * kBS * kBS * m->bgrid);
+  if (!rc && cudaMallocHost((void**)&m->h_bcg, sizeof(BcgSmall)) != cudaSuccess)
+    rc = fail(ctx, LFX_OUT_OF_MEMORY, "pinned allocation failed");
+  return rc;
+}
+
+// One inner block-CG solve of A X = R (R from the outer residual, X = 0),
+// each active right-hand side reduced by tol, at most max_inner iterations.
+int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner_its,
+              int* failed) {
+  lfx_ctx* ctx = m->ctx;
+  const int64_t n = m->undf;
+  const int G = m->bgrid;
+  BcgSmall* st = m->bcg;
+  const dim3 tb(32, 8), tg((unsigned)((n + 31) / 32), kBS / 32);
+  mv_from_rhs_major<kBS><<<tg, tb, 0, ctx->stream>>>(n, m->R64, n, m->r32);
+  LFX_CK(ctx, cudaMemsetAsync(st, 0, sizeof(BcgSmall), ctx->stream));
+  LFX_CK(ctx, cudaMemcpyAsync(st->active, act, sizeof(int) * kBS, cudaMemcpyHostToDevice,
+                              ctx->stream));
+  LFX_CK(ctx, cudaMemsetAsync(m->x32, 0, (size_t)n * kBS * 4, ctx->stream));
+  bcg_mask<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(n, m->r32, st->active);
+  const int nred = (kBS * kBS + 255) / 256;
+  // r0: column norms of R (the update kernel's norm pass, products left out)
+  bcg_update<0><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 1,
+                                            m->bpart);
+  bcg_reduce<<<1, kBS, 0, ctx->stream>>>(G, kBS, m->bpart, st->rn, st);
+  bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(3, st, tol);
+  // P = orth(D^-1 R)
+  bcg_update<1><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 1,
+                                            nullptr);
+  bcg_gram<1><<<G, 256, 0, ctx->stream>>>(n, m->w32, m->w32, nullptr, nullptr, m->bpart, st);
+  bcg_reduce<<<nred, 256, 0, ctx->stream>>>(G, kBS * kBS, m->bpart, st->G, st);
+  bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(2, st, tol);
+  bcg_update<2><<<G, 256, 0, ctx->stream>>>(n, m->w32, nullptr, m->p32, nullptr, nullptr, st, 0,
+                                            nullptr);
+  ctx->launches += 10;
+  LFX_CK(ctx, cudaGetLastError());
+  int it = 0;
+  while (it < max_inner) {
+    // Q = A P; alpha
+    int rc = mrhs_launch(m, m->p32, m->q32);
+    if (rc) return rc;
+    bcg_gram<2><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->r32, nullptr, m->bpart, st);
+    bcg_reduce<<<2 * nred, 256, 0, ctx->stream>>>(G, 2 * kBS * kBS, m->bpart, st->C, st);
+    bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(0, st, tol);
+    // X += P alpha, R -= Q alpha, ||R_j||
+    bcg_update<0><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 0,
+                                              m->bpart);
+    bcg_reduce<<<1, kBS, 0, ctx->stream>>>(G, kBS, m->bpart, st->rn, st);
+    // beta (and convergence)
+    bcg_gram<1><<<G, 256, 0, ctx->stream>>>(n, m->q32, m->r32, nullptr, m->dinv, m->bpart, st);
+    bcg_reduce<<<nred, 256, 0, ctx->stream>>>(G, kBS * kBS, m->bpart, st->E, st);
+    bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(1, st, tol);
+    // P = orth(D^-1 R + P beta)
+    bcg_update<1><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 0,
+                                              nullptr);
+    bcg_gram<1><<<G, 256, 0, ctx->stream>>>(n, m->w32, m->w32, nullptr, nullptr, m->bpart, st);
+    bcg_reduce<<<nred, 256, 0, ctx->stream>>>(G, kBS * kBS, m->bpart, st->G, st);
+    bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(2, st, tol);
+    bcg_update<2><<<G, 256, 0, ctx->stream>>>(n, m->w32, nullptr, m->p32, nullptr, nullptr, st,
+                                              0, nullptr);
+    ctx->launches += 13;
+    LFX_CK(ctx, cudaGetLastError());
+    ++it;
+    LFX_CK(ctx, cudaMemcpyAsync(&m->h_bcg->rank, &st->rank, 4 * sizeof(int),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (m->h_bcg->done) break;
+  }
+  *inner_its = m->h_bcg->iters;
+  *failed = m->h_bcg->fail;
+  return LFX_OK;
+}
+
 template <int NR>
 int add_correction(lfx_mrhs* m, double* x, int64_t ld) {
   lfx_ctx* ctx = m->ctx;
@@ -1062,10 +1516,16 @@ int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double*
     return fail(ctx, LFX_INVALID_ARGUMENT, "diag must be one FP64 field of undf values");
   if (ld < m->undf) return fail(ctx, LFX_INVALID_ARGUMENT, "ld must be at least undf");
   if (!(cfg->r_tol > 0.0) || !(cfg->inner_tol > 0.0) || !(cfg->inner_tol < 1.0) ||
-      cfg->max_outer < 1 || cfg->max_inner < 1)
-    return fail(ctx, LFX_INVALID_ARGUMENT, "bad tolerances or iteration limits");
+      cfg->max_outer < 1 || cfg->max_inner < 1 ||
+      (cfg->method != LFX_MRHS_PER_RHS_CG && cfg->method != LFX_MRHS_BLOCK_CG))
+    return fail(ctx, LFX_INVALID_ARGUMENT, "bad tolerances, iteration limits or method");
+  const bool block = cfg->method == LFX_MRHS_BLOCK_CG;
+  if (block && m->nrhs != kBS)
+    return fail(ctx, LFX_NOT_SUPPORTED, "block CG runs 64 right-hand sides");
   int rc = ensure_work(m);
+  if (!rc && block) rc = ensure_bcg(m);
   if (rc) return rc;
+  std::vector<int> bcg_its(m->nrhs, 0);
   const int nr = m->nrhs;
   const int64_t n = m->undf;
   k_dinv<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, (const double*)diag->data[0],
@@ -1086,10 +1546,16 @@ int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double*
       nact += act[r];
     }
     if (nact == 0 || outer >= cfg->max_outer) break;
-    int its = 0;
-    rc = nr == 16 ? inner_solve<16>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its)
-         : nr == 32 ? inner_solve<32>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its)
-                    : inner_solve<64>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its);
+    int its = 0, bfail = 0;
+    if (block) {
+      rc = bcg_inner(m, act.data(), cfg->inner_tol, cfg->max_inner, &its, &bfail);
+      for (int r = 0; r < nr; ++r)
+        if (act[r]) bcg_its[r] += its;
+    } else {
+      rc = nr == 16 ? inner_solve<16>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its)
+           : nr == 32 ? inner_solve<32>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its)
+                      : inner_solve<64>(m, act.data(), cfg->inner_tol, cfg->max_inner, &its);
+    }
     if (!rc) rc = nr == 16 ? add_correction<16>(m, x, ld)
                   : nr == 32 ? add_correction<32>(m, x, ld)
                              : add_correction<64>(m, x, ld);
@@ -1112,8 +1578,8 @@ int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double*
     I.final_rel = r0[r] > 0.0 ? rn[r] / r0[r] : 0.0;
     I.converged = r0[r] == 0.0 || rn[r] <= cfg->r_tol * r0[r];
     I.outer_iterations = outer_n[r];
-    I.inner_iterations = m->h_S->iters[r];
-    I.iterations = m->h_S->iters[r];
+    I.inner_iterations = block ? bcg_its[r] : m->h_S->iters[r];
+    I.iterations = I.inner_iterations;
     I.applies = inner_total;
     I.status = I.converged ? LFX_OK : (std::isfinite(rn[r]) ? LFX_NOT_CONVERGED : LFX_NAN_DETECTED);
   }

@@ -61,10 +61,11 @@ class SolveInfo(C.Structure):
 
 class MrhsCfg(C.Structure):
     _fields_ = [("r_tol", C.c_double), ("inner_tol", C.c_double), ("max_outer", C.c_int32),
-                ("max_inner", C.c_int32)]
+                ("max_inner", C.c_int32), ("method", C.c_int32)]
 
 
 MRHS_TF32, MRHS_BF16 = 1, 2
+MRHS_PER_RHS_CG, MRHS_BLOCK_CG = 0, 1
 
 
 class BatchTuning(C.Structure):
@@ -552,11 +553,12 @@ class MultiRhsOperator(_Handle):
         return {"levels_per_block": lb.value, "us": us.value}
 
     def solve(self, op64: "LmaOperator", diag: "FieldVector", b_ptr: int, x_ptr: int, ld: int,
-              r_tol=1e-8, inner_tol=1e-2, max_outer=20, max_inner=5000):
+              r_tol=1e-8, inner_tol=1e-2, max_outer=20, max_inner=5000, method=MRHS_PER_RHS_CG):
         """FP64 refinement around the FP32 tensor-core CG for all right-hand
-        sides; b, x: device FP64 arrays, right-hand side r at offset r * ld.
+        sides (method: MRHS_PER_RHS_CG, or MRHS_BLOCK_CG for 64 right-hand
+        sides); b, x: device FP64 arrays, right-hand side r at offset r * ld.
         Returns one SolveInfo per right-hand side."""
-        cfg = MrhsCfg(r_tol, inner_tol, max_outer, max_inner)
+        cfg = MrhsCfg(r_tol, inner_tol, max_outer, max_inner, method)
         info = (SolveInfo * self.nrhs)()
         self.ctx.check(self.ctx.L.lfx_mrhs_solve(self.h, op64.h, diag.h, b_ptr, x_ptr, ld,
                                                  C.byref(cfg), info))

@@ -370,7 +370,15 @@ def leg_multi_rhs(ctx, lfx, mg, wl, torch, stream, n=48, nl=30, nrhs=64):
     peak, _ = measured_hbm_peak()
     xr = torch.randn(p.undf, nrhs, device="cuda", dtype=torch.float32)
     yr = torch.empty_like(xr)
-    for kind, name in ((lfx.MRHS_TF32, "tf32"), (lfx.MRHS_BF16, "bf16")):
+    from oracle import oracle as orc
+    npc, cic = p.mesh.colour_lookup()
+    o = orc.LmaOperator(p.ncell_2d, nl, 8, 8, p.map, p.map, p.undf, p.undf, p.lma, npc, cic)
+    x_or, _ = orc.solve("cg", o, orc.Preconditioner.diagonal(o.diagonal()), Bh[0], r_tol=RTOL,
+                        a_tol=0.0, max_iter=20000)
+    runs = [(lfx.MRHS_TF32, "tf32", lfx.MRHS_PER_RHS_CG), (lfx.MRHS_BF16, "bf16", lfx.MRHS_PER_RHS_CG),
+            (lfx.MRHS_TF32, "tf32_block_cg", lfx.MRHS_BLOCK_CG),
+            (lfx.MRHS_BF16, "bf16_block_cg", lfx.MRHS_BLOCK_CG)]
+    for kind, name, method in runs:
         M = lfx.MultiRhsOperator(s.op, kind, nrhs)
         inf = M.info()
         tune = M.autotune(10)
@@ -379,18 +387,21 @@ def leg_multi_rhs(ctx, lfx, mg, wl, torch, stream, n=48, nl=30, nrhs=64):
         algo = inf["matrix_bytes"] + 2 * p.undf * nrhs * 4
         x.zero_()
         torch.cuda.synchronize()
-        M.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=RTOL)  # warm-up
+        M.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=RTOL, method=method)  # warm-up
         x.zero_()
         torch.cuda.synchronize()
         l0 = ctx.launch_count()
         ev[0].record(stream)
-        info = M.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=RTOL)
+        info = M.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=RTOL, method=method)
         ev[1].record(stream)
         ctx.synchronize()
         t = ev[0].elapsed_time(ev[1]) / 1e3
         X2 = x.cpu().numpy()
         err = [float(np.linalg.norm(X2[r] - x64[r]) / np.linalg.norm(x64[r])) for r in range(nrhs)]
         out[name] = {
+            "method": "block CG (one search space for the 64 right-hand sides)"
+                      if method == lfx.MRHS_BLOCK_CG else "CG per right-hand side",
+            "error_vs_fp64_oracle_rhs0": float(np.linalg.norm(X2[0] - x_or) / np.linalg.norm(x_or)),
             "solves_per_s": round(nrhs / t, 2), "s": round(t, 4),
             "speedup_vs_serial_fp64": round(t64 / t, 3),
             "all_converged": all(i.converged for i in info),
@@ -826,7 +837,11 @@ def main():
     roof = {"kernel": f"{tuning['fp32']['kernel']} (FP32 LMA apply)", "bound": "hbm",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": traffic, "algorithmic_bytes_per_launch": bytes32,
+            "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one apply, from "
+                               "the committed capture profiles/lma_apply_fp32_c96x30.json (not "
+                               "measured in this run)") if traffic else None,
+            "algorithmic_bytes_per_launch": bytes32,
             "launch": ("one apply (the cell scatter: one kernel per colour)"
                        if tuning["fp32"]["kernel"] == "cell-scatter" else "one apply (one launch)"),
             "launches_timed": n32, "applies_executed": K * exec32,

@@ -425,7 +425,7 @@ int lfx_batch_slot_info(const lfx_batch* b, int32_t slot, int32_t* phase, int64_
                         lfx_solve_info* info);
 int lfx_batch_retire(lfx_batch* b, int32_t slot);
 /* launch shape of the persistent kernel: cell columns per apply work item
- * (the colour block), blocks per SM, and the bytes of vectors of one L2 group
+ * (the colour block one warp takes), blocks per SM, and the bytes of vectors of one L2 group
  * of slots (slots of a group run their colour phases together, so their
  * vectors stay in L2 across the colours) */
 typedef struct {
@@ -439,12 +439,12 @@ typedef struct {
 } lfx_batch_tuning;
 /* Batch autotuner: times one replay of `iters` super-iterations per candidate
  * shape on the admitted slots (these replays advance the solves, which do not
- * depend on the shape) -- blocks per SM, then 32/64/128 columns per item,
+ * depend on the shape) -- blocks per SM, then 1/2/4/8 columns per item,
  * then L2 groups of a quarter, half, all of L2 or one group -- and keeps the
  * fastest. */
 int lfx_batch_autotune(lfx_batch* b, int32_t iters, lfx_batch_tuning* out);
 int lfx_batch_get_tuning(const lfx_batch* b, lfx_batch_tuning* out);
-/* pin a launch shape (cells_per_item a multiple of 32, at most 128) */
+/* pin a launch shape (cells_per_item 1 to 128) */
 int lfx_batch_set_tuning(lfx_batch* b, int32_t cells_per_item, int32_t blocks_per_sm,
                          int64_t group_bytes);
 /* upper bound in seconds of one grid-barrier wait (default 2) */
@@ -502,6 +502,17 @@ typedef struct {
  * outer_iterations = refinement steps it took part in. */
 int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double* b, double* x,
                    int64_t ld, const lfx_mrhs_cfg* cfg, lfx_solve_info* info);
+/* Where the block CG's Gram products U^T V (n x 64 blocks) run: tensor = 1
+ * on the tcgen05 tensor cores, each FP32 value split into two TF32 parts
+ * (three MMAs per step, about FP32 accuracy, FP32 accumulation in tensor
+ * memory per block, FP64 across blocks); 0 (default) on the FP32 cores. */
+int lfx_mrhs_set_gram(lfx_mrhs* m, int32_t tensor);
+/* One Gram product with either path: out (device, nv x 64 x 64 FP64,
+ * [v][i][j]) = sum over rows of U[row][i] V_v[row][j], for device arrays U,
+ * V0, V1 of undf x 64 FP32 values, dof-major. LFX_TIMEOUT if a bounded
+ * tensor-core wait ran out. */
+int lfx_mrhs_gram(lfx_mrhs* m, const float* U, const float* V0, const float* V1, int32_t nv,
+                  int32_t tensor, double* out);
 
 /* ------------------------------------------------------------------ no allocation
  * Allocation-free inner product (no counterpart in the reference): for

@@ -21,8 +21,9 @@
 //       (matrix_vector_kernel_mod.F90:107-140) over each slot's packed FP32
 //       upper triangles, one phase per colour and per L2 group of slots (the
 //       slots of one group keep p and the partial sums of z in L2 across
-//       their four colours); the last writer of every dof adds p_i z_i to the
-//       slot's <p, z>, whose last item sets alpha
+//       their colours); the last writer of every dof adds p_i z_i to its cell
+//       column's share of <p, z>
+//   F   alpha = rz / <p, z> per slot, the column shares summed in order
 //   U   xc += alpha p, r -= alpha z, ||r||^2 (and, for a Jacobi slot, <r, r/d>
 //       and beta); a slot whose residual fell by kDelta, reached its
 //       tolerance or its iteration limit asks for a true residual
@@ -33,11 +34,12 @@
 //       then z = r / d on the other rows with <r, z> and beta
 //   P   p = z + beta p
 // Work items: apply items of up to `cells_per_item` cell columns of one
-// colour of one slot; 8192-value chunk items (slot, chunk) for the vector
+// colour of one slot, one warp each (a column's segments in order);
+// 16384-value chunk items (slot, chunk), one block each, for the vector
 // phases; 64-column items for the sweeps. Per-slot sums are reduced in an
-// order fixed by the slot alone (32-column dot blocks, 8192-value chunks,
-// then in index order), so a slot's result is bit-identical whatever else is
-// in the batch and whatever launch shape the autotuner picks.
+// order fixed by the slot alone (per cell column, per 16384-value chunk, then
+// in index order), so a slot's result is bit-identical whatever else is in
+// the batch and whatever launch shape the autotuner picks.
 //
 // Memory: a slot's Krylov state (r64 FP64; r, p, z, xc FP32; its partial
 // sums) is allocated at admission from the device's stream-ordered memory
@@ -62,12 +64,10 @@ enum { PH_EMPTY = 0, PH_INIT = 1, PH_RUN = 2, PH_DONE = 3 };
 constexpr double kDelta = 1e-3;  // reliable update when ||r|| drops by this factor
 constexpr int kBT = 256;         // threads per block of the persistent kernel
 constexpr int kBW = kBT / 32;    // warps per block
-constexpr int kBSub = 4;         // a chunk item: kBSub chunks of RCHUNK values
-constexpr int kDotCols = 32;     // cell columns per partial sum of <p, A p>
+constexpr int kBSub = 8;         // a chunk item: kBSub chunks of RCHUNK values (16384)
 constexpr int kMaxIters = 64;    // super-iterations per launch, at most
 constexpr int kMaxSeg = 4;       // warps (segments of <= 31 levels) per cell column, at most
 constexpr int kMaxCB = 128;      // cell columns per apply item, at most
-constexpr int kMaxUnits = kMaxCB * kMaxSeg;
 constexpr int kMaxColours = 8;   // cell colours of a slot, at most
 constexpr int kBCols = 64;       // columns per sweep item
 constexpr int kBRows = 160;      // rows per preconditioner column, at most
@@ -84,10 +84,10 @@ struct BSlot {
   const double* S64;
   const int* cdesc;
   int32_t sblk32, sblk64, cdints, nl;
-  int32_t nseg, segL, nch, ndot;
-  int32_t nitem32, cma, ncol, nrow;
+  int32_t nseg, segL, nch, ncell;
+  int32_t pad0, cma, ncol, nrow;
   int64_t n;
-  double* part;  // [0, 2 nch): chunk sums; [2 nch, 2 nch + ndot): apply dots
+  double* part;  // [0, 2 nch): chunk sums; [2 nch, 2 nch + ncell): <p, z> per cell column
   // preconditioner: FP32 Jacobi diagonal (zero on the column rows of a
   // column preconditioner) and the Thomas factors [row][column]
   const float* diag;
@@ -110,12 +110,13 @@ struct BState {
 // device-resident launch parameters (the graph's kernel takes their address,
 // so lists can be rebuilt and reallocated between replays)
 struct BParams {
-  const int4* items32;  // FP32 apply items {slot, q0, columns, first dot block}
+  const int4* items32;  // FP32 apply items {slot, q0, columns, 0}
   const int* off32;     // [ncolour * ngr32 + 1]: items of group g, colour c from off32[g ncolour + c]
   const int4* items64;  // FP64 residual items {slot, q0, columns, 0}
   const int* off64;
   const int2* chunks;   // {slot, chunk}
   const int2* cols;     // {slot, column}
+  const int* slotlist;  // the slots the lists cover
   const BSlot* slots;
   BState* st;
   unsigned* tickets;
@@ -124,6 +125,7 @@ struct BParams {
   int* err;             // LFX_TIMEOUT when a wait ran out
   int ngr32, ngr64, nchunk, ncolitem;
   int iters, max_slots, any_cma, ncolour;
+  int nslot, pad1;
   unsigned long long timeout_ns;
 };
 
@@ -132,7 +134,6 @@ struct BShared {
   BState state;
   int skip, last, s;
   int4 item;
-  double unit[kMaxUnits];
   double red[kBT / 32];
   int ok;
 };
@@ -335,75 +336,73 @@ __device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const i
   return dot;
 }
 
-// The apply items [i0, i1) of one (group, colour) phase. FP32 (DOT): z = A32 p
-// for running slots, with <p, z> per 32-column block and alpha from the
-// slot's last item. FP64 (RESID): r64 = b - A64 x for slots taking a true
-// residual.
+// The apply items [i0, i1) of one (group, colour) phase, one warp per item
+// (no block-wide barrier: each warp walks its item's cell columns, and each
+// column's segments, in order). FP32: z = A32 p for running slots, each
+// column's share of <p, z> (lanes over the column's segments in order, then
+// the lane butterfly) stored at its colour-loop position. FP64: r64 = b -
+// A64 x for slots taking a true residual. An item's packed matrices are one
+// contiguous run, which lane 0 asks the L2 to fetch in bulk
+// (cp.async.bulk.prefetch) before the warp's first loads.
 template <int NDF, bool FP64>
-__device__ __noinline__ void apply_phase(const BParams& P, BShared& sh, const int4* __restrict__ items, int i0,
-                            int i1) {
+__device__ __noinline__ void apply_phase(const BParams& P, const int4* __restrict__ items, int i0,
+                                         int i1) {
   using T = typename std::conditional<FP64, double, float>::type;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int u = i0 + blockIdx.x; u < i1; u += gridDim.x) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int4 it = __ldg(items + u);
-      sh.item = it;
-      const int ph = __ldcg(&P.st[it.x].phase), fl = __ldcg(&P.st[it.x].flag);
-      sh.skip = FP64 ? !(ph == PH_INIT || (ph == PH_RUN && fl)) : !ph_run(ph);
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kBW + (threadIdx.x >> 5), nw = gridDim.x * kBW;
+  for (int u = i0 + gw; u < i1; u += nw) {
+    const int4 it = __ldg(items + u);
+    const int s = it.x;
+    const int ph = __ldcg(&P.st[s].phase), fl = __ldcg(&P.st[s].flag);
+    if (FP64 ? !(ph == PH_INIT || (ph == PH_RUN && fl)) : !ph_run(ph)) continue;
+    const BSlot* D = P.slots + s;
+    const T* M = FP64 ? (const T*)D->S64 : (const T*)D->S32;
+    const int sblk = FP64 ? D->sblk64 : D->sblk32;
+    const int* cdesc = D->cdesc;
+    const int cdints = D->cdints, nl = D->nl, nseg = D->nseg, L = D->segL;
+    const T* x = FP64 ? (const T*)D->x : (const T*)D->p;
+    T* y = FP64 ? (T*)D->r64 : (T*)D->z;
+    const double* bb = D->b;
+    const int q0 = it.y, nq = it.z;
+    if (lane == 0) {
+      const T* run = M + (size_t)q0 * sblk;
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(run),
+                   "r"((unsigned)((size_t)nq * sblk * sizeof(T)))
+                   : "memory");
     }
-    __syncthreads();
-    if (sh.skip) continue;
-    const int s = sh.item.x;
-    load_item(P, sh, s);
-    __syncthreads();
-    const BSlot& D = sh.slot;
-    const int q0 = sh.item.y, nq = sh.item.z;
-    const int nseg = D.nseg, L = D.segL, nl = D.nl;
-    const int nunits = nq * nseg;
-    const T* M = FP64 ? (const T*)D.S64 : (const T*)D.S32;
-    const int sblk = FP64 ? D.sblk64 : D.sblk32;
-    const T* x = FP64 ? (const T*)D.x : (const T*)D.p;
-    T* y = FP64 ? (T*)D.r64 : (T*)D.z;
-    for (int w = warp; w < nunits; w += kBW) {
-      const int q = q0 + w / nseg, sg = w % nseg;
-      const double c = scatter_unit<T, NDF, FP64, !FP64>(M + (size_t)q * sblk,
-                                                         D.cdesc + (size_t)q * D.cdints, nl, L, sg,
-                                                         lane, x, y, D.b);
+    double* part = FP64 ? nullptr : D->part + 2 * (int64_t)D->nch;
+    for (int c = 0; c < nq; ++c) {
+      const int q = q0 + c;
+      double dot = 0.0;
+      for (int sg = 0; sg < nseg; ++sg)
+        dot += scatter_unit<T, NDF, FP64, !FP64>(M + (size_t)q * sblk, cdesc + (size_t)q * cdints,
+                                                 nl, L, sg, lane, x, y, bb);
       if (!FP64) {
-        const double cw = warp_butterfly(c);
-        if (lane == 0) sh.unit[w] = cw;
+        const double w = warp_butterfly(dot);
+        if (lane == 0) __stcg(part + q, w);
       }
     }
-    if (!FP64) {
-      __syncthreads();
-      // one partial per 32-column block, units in order
-      const int ndb = (nq + kDotCols - 1) / kDotCols;
-      if (threadIdx.x < ndb) {
-        const int a0 = threadIdx.x * kDotCols * nseg;
-        const int a1 = min((threadIdx.x + 1) * kDotCols, nq) * nseg;
-        double a = 0.0;
-        for (int w = a0; w < a1; ++w) a = a + sh.unit[w];
-        __stcg(D.part + 2 * (int64_t)D.nch + sh.item.w + threadIdx.x, a);
-      }
-      __threadfence();
-      __syncthreads();
-      if (threadIdx.x == 0) sh.last = (atomicAdd(&P.tickets[s], 1u) == (unsigned)D.nitem32 - 1u);
-      __syncthreads();
-      if (sh.last) {
-        __threadfence();
-        double a = 0.0;
-        for (int i = threadIdx.x; i < D.ndot; i += kBT) a = a + __ldcg(&D.part[2 * (int64_t)D.nch + i]);
-        const double pz = bsum(a, sh.red);
-        if (threadIdx.x == 0) {
-          BState S;
-          copy_state_in(&S, P.st + s);
-          S.alpha = S.rz / pz;
-          S.fresh = 0;
-          copy_state_out(P.st + s, S);
-          P.tickets[s] = 0u;
-        }
-      }
+  }
+}
+
+// alpha = rz / <p, z> for every running slot: one block per slot sums the
+// slot's per-column shares in a fixed order
+__device__ __noinline__ void alpha_phase(const BParams& P, BShared& sh) {
+  for (int k = blockIdx.x; k < P.nslot; k += gridDim.x) {
+    const int s = __ldg(P.slotlist + k);
+    if (!ph_run(__ldcg(&P.st[s].phase))) continue;  // block-uniform
+    const BSlot* D = P.slots + s;
+    const double* part = D->part + 2 * (int64_t)D->nch;
+    const int nc = D->ncell;
+    double a = 0.0;
+    for (int i = threadIdx.x; i < nc; i += kBT) a = a + __ldcg(part + i);
+    const double pz = bsum(a, sh.red);
+    if (threadIdx.x == 0) {
+      BState S;
+      copy_state_in(&S, P.st + s);
+      S.alpha = S.rz / pz;
+      S.fresh = 0;
+      copy_state_out(P.st + s, S);
     }
   }
 }
@@ -623,9 +622,11 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
     for (int g = 0; g < P.ngr32; ++g)
       for (int c = 0; c < P.ncolour; ++c) {
         const int o = g * P.ncolour + c;
-        apply_phase<NDF, false>(P, sh, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1));
+        apply_phase<NDF, false>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1));
         if (!grid_sync(P, sh)) return;
       }
+    alpha_phase(P, sh);
+    if (!grid_sync(P, sh)) return;
     // ---- U: xc += alpha p, r -= alpha z, ||r||^2 (+ <r, r/d>, beta for Jacobi slots)
     int* need = P.need + it;
     chunk_phase<2>(
@@ -669,7 +670,7 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
       for (int g = 0; g < P.ngr64; ++g)
         for (int c = 0; c < P.ncolour; ++c) {
           const int o = g * P.ncolour + c;
-          apply_phase<NDF, true>(P, sh, P.items64, __ldg(P.off64 + o), __ldg(P.off64 + o + 1));
+          apply_phase<NDF, true>(P, P.items64, __ldg(P.off64 + o), __ldg(P.off64 + o + 1));
           if (!grid_sync(P, sh)) return;
         }
       chunk_phase<2>(
@@ -774,7 +775,7 @@ struct SlotHost {
   lfx_vec* x = nullptr;
   int64_t tag = 0;
   int64_t n = 0;
-  int nch = 0, ndot = 0, nl = 0, ncol = 0;
+  int nch = 0, nl = 0, ncol = 0;
   bool cma = false;
   std::vector<int32_t> cstart;  // colour starts in the colour-loop order
   int last_phase = PH_EMPTY;
@@ -799,13 +800,14 @@ struct lfx_batch {
   int4 *d_items32 = nullptr, *d_items64 = nullptr;
   int *d_off32 = nullptr, *d_off64 = nullptr;
   int2 *d_chunks = nullptr, *d_cols = nullptr;
+  int* d_slotlist = nullptr;
   size_t cap_items32 = 0, cap_items64 = 0, cap_off32 = 0, cap_off64 = 0, cap_chunks = 0,
-         cap_cols = 0;
+         cap_cols = 0, cap_slotlist = 0;
   std::vector<SlotHost> slots;
   bool dirty = true;
   int nactive = 0;
   // launch shape (autotuned) and its graphs
-  int cells_per_item = 64, blocks_per_sm = 2, max_bps = 2;
+  int cells_per_item = 2, blocks_per_sm = 2, max_bps = 2;
   int64_t group_bytes = 64 << 20;
   float tuned_us = 0.f;
   std::map<int, cudaGraphExec_t> graphs;  // by blocks per SM
@@ -845,8 +847,7 @@ const void* pick_kernel(int ndf, bool cma) {
 // vectors (bytes_per_dof per dof) stay within group_bytes; per group and
 // colour the slots' runs of cells_per_item cell columns
 void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int ncolour,
-                       int bytes_per_dof, bool dots, std::vector<int4>& items,
-                       std::vector<int>& off, std::vector<int>* nitem) {
+                       int bytes_per_dof, std::vector<int4>& items, std::vector<int>& off) {
   items.clear();
   off.clear();
   std::vector<std::vector<int>> groups;
@@ -866,14 +867,10 @@ void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int ncol
       off.push_back((int)items.size());
       for (int s : g) {
         const SlotHost& H = B->slots[s];
-        int dotbase = 0;
-        for (int cc = 0; cc < c; ++cc)
-          dotbase += (H.cstart[cc + 1] - H.cstart[cc] + kDotCols - 1) / kDotCols;
         if (c + 1 >= (int)H.cstart.size()) continue;
         const int a = H.cstart[c], e = H.cstart[c + 1];
         for (int q = a; q < e; q += cb) {
-          items.push_back(make_int4(s, q, std::min(cb, e - q), dots ? dotbase + (q - a) / kDotCols : 0));
-          if (nitem) (*nitem)[s]++;
+          items.push_back(make_int4(s, q, std::min(cb, e - q), 0));
         }
       }
     }
@@ -896,9 +893,9 @@ int rebuild(lfx_batch* B) {
   int ncolour = 1;
   for (int s : act) ncolour = std::max(ncolour, (int)B->slots[s].cstart.size() - 1);
   std::vector<int4> it32, it64;
-  std::vector<int> off32, off64, nitem(B->max_slots, 0);
-  build_apply_items(B, act, ncolour, 8, true, it32, off32, &nitem);
-  build_apply_items(B, act, ncolour, 16, false, it64, off64, nullptr);
+  std::vector<int> off32, off64;
+  build_apply_items(B, act, ncolour, 8, it32, off32);
+  build_apply_items(B, act, ncolour, 16, it64, off64);
   std::vector<int2> ch, col;
   for (int s : act) {
     const SlotHost& H = B->slots[s];
@@ -920,11 +917,9 @@ int rebuild(lfx_batch* B) {
   if (!rc) rc = upload(ctx, B->d_chunks, ch);
   if (!rc) rc = upload(ctx, B->d_cols, col);
   if (rc) return rc;
-  for (int s : act) {
-    B->h_slots[s].nitem32 = nitem[s];
-    LFX_CK(ctx, cudaMemcpyAsync(B->d_slots + s, &B->h_slots[s], sizeof(BSlot),
-                                cudaMemcpyHostToDevice, ctx->stream));
-  }
+  rc = grow(ctx, &B->d_slotlist, &B->cap_slotlist, act.size());
+  if (!rc) rc = upload(ctx, B->d_slotlist, act);
+  if (rc) return rc;
   BParams& P = B->h_params;
   P.items32 = B->d_items32;
   P.off32 = B->d_off32;
@@ -932,6 +927,8 @@ int rebuild(lfx_batch* B) {
   P.off64 = B->d_off64;
   P.chunks = B->d_chunks;
   P.cols = B->d_cols;
+  P.slotlist = B->d_slotlist;
+  P.nslot = (int)act.size();
   P.slots = B->d_slots;
   P.st = B->d_state;
   P.tickets = B->d_tickets;
@@ -1058,9 +1055,9 @@ int64_t available_bytes(lfx_ctx* ctx) {
 }
 
 // device bytes a slot of this operator takes at admission
-int64_t slot_bytes(int64_t n, int64_t nch, int64_t ndot) {
+int64_t slot_bytes(int64_t n, int64_t nch, int64_t ncell) {
   const int64_t v = ((8 * n + 255) / 256 + 4 * ((4 * n + 255) / 256)) * 256;
-  return v + ((2 * nch + ndot) * 8 + 255) / 256 * 256;
+  return v + ((2 * nch + ncell) * 8 + 255) / 256 * 256;
 }
 
 }  // namespace
@@ -1137,7 +1134,7 @@ int lfx_batch_destroy(lfx_batch* B) {
   for (auto& H : B->slots)
     if (H.mem) cudaFreeAsync(H.mem, ctx->stream);
   for (void* p : {(void*)B->d_items32, (void*)B->d_items64, (void*)B->d_off32, (void*)B->d_off64,
-                  (void*)B->d_chunks, (void*)B->d_cols})
+                  (void*)B->d_chunks, (void*)B->d_cols, (void*)B->d_slotlist})
     if (p) cudaFreeAsync(p, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   dfree(ctx, B->d_slots, sizeof(BSlot) * B->max_slots);
@@ -1168,7 +1165,8 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
                 "batch needs a symmetric operator on one dofmap of the batch's cell size "
                 "(the packed cell scatter)");
   const int nl = L->nlayers;
-  const int nseg = nl + 1 <= 32 ? 1 : (nl + 1 + 30) / 31;
+  // segments of at most 31 rows: lane 0 of a segment holds the row below it
+  const int nseg = (nl + 1 + 30) / 31;
   if (nseg > kMaxSeg)
     return fail(ctx, LFX_NOT_SUPPORTED, "batch: at most 123 levels per column");
   const bool cma = prec32->kind == PREC_CMA;
@@ -1191,14 +1189,11 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   if (s < 0) return fail(ctx, LFX_OUT_OF_MEMORY, "no free batch slot");
   const int64_t n = L->undf_to;
   const int64_t nch = bchunks(n);
-  int ndot = 0;
-  for (size_t c = 0; c + 1 < L->colour_start.size(); ++c)
-    ndot += (L->colour_start[c + 1] - L->colour_start[c] + kDotCols - 1) / kDotCols;
   if (L->colour_start.size() < 2 || (int)L->colour_start.size() - 1 > kMaxColours)
     return fail(ctx, LFX_NOT_SUPPORTED, "batch: at most 8 cell colours");
   // admission by free device memory: the slot's state, its share of the
   // work lists, and the batch's reserve must fit
-  const int64_t need = slot_bytes(n, nch, ndot);
+  const int64_t need = slot_bytes(n, nch, L->ncell_2d);
   const int64_t lists = 16 * (2 * ((int64_t)L->ncell_2d / 32 + 8) + nch) + 8 * (cma ? prec32->ncell_2d : 0);
   if (available_bytes(ctx) - need - 2 * lists < B->reserve)
     return fail(ctx, LFX_OUT_OF_MEMORY, "batch: not enough free device memory for the solve");
@@ -1217,7 +1212,6 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   H.tag = tag;
   H.n = n;
   H.nch = (int)nch;
-  H.ndot = ndot;
   H.nl = nl;
   H.cma = cma;
   H.ncol = cma ? prec32->ncell_2d : 0;
@@ -1234,8 +1228,7 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   D.nseg = nseg;
   D.segL = (nl + 1 + nseg - 1) / nseg;
   D.nch = (int)nch;
-  D.ndot = ndot;
-  D.nitem32 = 0;
+  D.ncell = L->ncell_2d;
   D.cma = cma ? 1 : 0;
   D.n = n;
   char* m = (char*)mem;
@@ -1364,7 +1357,7 @@ int lfx_batch_get_tuning(const lfx_batch* B, lfx_batch_tuning* t) {
 int lfx_batch_set_tuning(lfx_batch* B, int32_t cells_per_item, int32_t blocks_per_sm,
                          int64_t group_bytes) {
   if (!B) return LFX_INVALID_ARGUMENT;
-  if (cells_per_item < kDotCols || cells_per_item > kMaxCB || cells_per_item % kDotCols ||
+  if (cells_per_item < 1 || cells_per_item > kMaxCB ||
       blocks_per_sm < 1 || blocks_per_sm > B->max_bps || group_bytes < 1)
     return fail(B->ctx, LFX_INVALID_ARGUMENT, "batch tuning out of range");
   B->cells_per_item = cells_per_item;
@@ -1418,7 +1411,7 @@ int lfx_batch_autotune(lfx_batch* B, int32_t iters, lfx_batch_tuning* out) {
     std::vector<int64_t> cand;
     if (stage == 0)
       for (int v = 1; v <= B->max_bps; ++v) cand.push_back(v);
-    if (stage == 1) cand = {32, 64, 128};
+    if (stage == 1) cand = {1, 2, 4, 8};
     if (stage == 2) cand = {l2 / 4, l2 / 2, l2, int64_t(1) << 40};
     best = 0.f;
     for (int64_t c : cand) {

@@ -662,6 +662,220 @@ __global__ void __launch_bounds__(256) bcg_gram(int64_t n, const float* __restri
       for (int y = 0; y < 4; ++y) out[((size_t)v * kBS + i0 + x) * kBS + j0 + y] = acc[v][x][y];
 }
 
+// ---- The same Gram on the 5th-generation tensor cores (tcgen05).
+// D (64 x 64 NV) = U^T [V_0 .. V_NV-1] accumulates in tensor memory (TMEM,
+// FP32): A = U^T and B = V are both MN-major in shared memory, in the
+// canonical no-swizzle layout (core matrices of 8 K-rows x 16 bytes, K-rows
+// 16 bytes apart, MN groups 128 bytes apart, K groups G x 128 bytes apart).
+// Each FP32 value is split into TF32 parts hi + lo and a product taken as
+// hi hi + hi lo + lo hi (three kind::tf32 MMAs of M = 64, K = 8 per K step),
+// which keeps about FP32 accuracy. Two 32-row stages: the block stages the
+// next chunk while the tensor core works on the last one; one elected thread
+// issues the MMAs and commits them to the stage's mbarrier. Every mbarrier
+// wait is bounded; a wait that runs out sets st->fail = 2 and the block
+// stops issuing work (the final wait is bounded too before TMEM is freed).
+constexpr int kTcRows = 32;
+constexpr int kTcThreads = 128;
+constexpr unsigned long long kTcWaitNs = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+// shared-memory matrix descriptor: start, leading (K group) and stride (MN
+// group) byte offsets, version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor: FP32 accumulate, A and B TF32, both MN-major, M = 64
+template <int N>
+__host__ __device__ constexpr uint32_t idesc_tf32_mn() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(64 >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ unsigned long long tc_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// wait for the mbarrier phase of the given parity, for at most kTcWaitNs
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+  const unsigned long long t0 = tc_clock();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (tc_clock() - t0 > kTcWaitNs) return false;
+  }
+}
+__device__ __forceinline__ float tf32_round(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+// stage 32 rows of G column groups (4 floats each) of an n x (4 G) block made
+// of `nsrc` 64-column row-major sources into the canonical layout, as TF32
+// hi and lo parts; rows past n are zero
+__device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, int G,
+                                         const float* s0, const float* s1, int64_t row0,
+                                         int64_t n, const float* __restrict__ scale) {
+  for (int e = threadIdx.x; e < kTcRows * G; e += kTcThreads) {
+    const int k8 = e & 7, g = (e >> 3) % G, kg = e / (8 * G);
+    const int k = kg * 8 + k8;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (row0 + k < n) {
+      const float* src = g < kBS / 4 ? s0 + (size_t)(row0 + k) * kBS + 4 * g
+                                     : s1 + (size_t)(row0 + k) * kBS + 4 * (g - kBS / 4);
+      v = ld4(src);
+      if (scale) {
+        const float sc = scale[row0 + k];
+        v.x *= sc; v.y *= sc; v.z *= sc; v.w *= sc;
+      }
+    }
+    const float4 h = make_float4(tf32_round(v.x), tf32_round(v.y), tf32_round(v.z), tf32_round(v.w));
+    const float4 l = make_float4(tf32_round(v.x - h.x), tf32_round(v.y - h.y),
+                                 tf32_round(v.z - h.z), tf32_round(v.w - h.w));
+    const size_t off = ((size_t)(kg * G + g) * 8 + k8) * 16;
+    *reinterpret_cast<float4*>(hi + off) = h;
+    *reinterpret_cast<float4*>(lo + off) = l;
+  }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kTcThreads) bcg_gram_tc(int64_t n, const float* __restrict__ U,
+                                                         const float* __restrict__ V0,
+                                                         const float* __restrict__ V1,
+                                                         const float* __restrict__ vscale,
+                                                         double* __restrict__ partials,
+                                                         BcgSmall* st) {
+  constexpr int N = kBS * NV, GA = kBS / 4, GB = N / 4;
+  constexpr int ABYTES = kTcRows * kBS * 4, BBYTES = kTcRows * N * 4;
+  constexpr int STAGE = 2 * ABYTES + 2 * BBYTES;
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_abort;
+  if (st->done) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base)),
+                 "r"((uint32_t)N)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+    s_abort = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t IDESC = idesc_tf32_mn<N>();
+  int j = 0;  // chunks of this block so far
+  for (int64_t c = blockIdx.x; c * kTcRows < n; c += gridDim.x, ++j) {
+    const int sidx = j & 1;
+    unsigned char* base = tc_smem + (size_t)sidx * STAGE;
+    if (j >= 2) {
+      // the MMAs that last read this stage have completed
+      if (threadIdx.x == 0 && !tc_wait(smem_u32(&mbar[sidx]), (uint32_t)((j / 2 - 1) & 1))) {
+        s_abort = 1;
+        st->fail = 2;
+      }
+      __syncthreads();
+      if (s_abort) break;
+    }
+    tc_stage(base, base + ABYTES, GA, U, U, c * kTcRows, n, nullptr);
+    tc_stage(base + 2 * ABYTES, base + 2 * ABYTES + BBYTES, GB, V0, NV > 1 ? V1 : V0,
+             c * kTcRows, n, vscale);
+    // generic-proxy writes of the operands become visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_hi = smem_u32(base), a_lo = a_hi + ABYTES;
+      const uint32_t b_hi = a_hi + 2 * ABYTES, b_lo = b_hi + BBYTES;
+#pragma unroll
+      for (int kg = 0; kg < kTcRows / 8; ++kg) {
+        const uint64_t ah = umma_desc(a_hi + kg * GA * 128, GA * 128, 128);
+        const uint64_t al = umma_desc(a_lo + kg * GA * 128, GA * 128, 128);
+        const uint64_t bh = umma_desc(b_hi + kg * GB * 128, GB * 128, 128);
+        const uint64_t bl = umma_desc(b_lo + kg * GB * 128, GB * 128, 128);
+        tc_mma(tmem, ah, bh, IDESC, (j > 0 || kg > 0) ? 1u : 0u);
+        tc_mma(tmem, ah, bl, IDESC, 1u);
+        tc_mma(tmem, al, bh, IDESC, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[sidx]))
+                   : "memory");
+    }
+  }
+  // the last commit covers every MMA of the block
+  if (j > 0 && threadIdx.x == 0 &&
+      !tc_wait(smem_u32(&mbar[(j - 1) & 1]), (uint32_t)(((j - 1) / 2) & 1))) {
+    s_abort = 1;
+    st->fail = 2;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  double* out = partials + (size_t)blockIdx.x * NV * kBS * kBS;
+  // M = 64: row m sits in TMEM lane (m % 16) + 32 (m / 16); warp w reads
+  // lanes 32 w .. 32 w + 31, whose first 16 hold rows 16 w .. 16 w + 15
+#pragma unroll
+  for (int c0 = 0; c0 < N; c0 += 32) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+        "%28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (lane < 16) {
+      const int m = 16 * warp + lane;
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        const int jj = c0 + q, v = jj / kBS, jc = jj % kBS;
+        out[((size_t)v * kBS + m) * kBS + jc] =
+            (j > 0 && !s_abort) ? (double)__uint_as_float(r[q]) : 0.0;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"((uint32_t)N)
+                 : "memory");
+}
+
+template <int NV>
+constexpr size_t tc_gram_smem() {
+  return 2 * (2 * (size_t)kTcRows * kBS * 4 + 2 * (size_t)kTcRows * kBS * NV * 4);
+}
+
 // out[e] = sum over the blocks, in block order, of partials[b][e]
 __global__ void bcg_reduce(int nb, int ne, const double* __restrict__ partials,
                            double* __restrict__ out, const BcgSmall* st) {
@@ -945,6 +1159,7 @@ struct lfx_mrhs {
   BcgSmall* h_bcg = nullptr;  // pinned
   double* bpart = nullptr;
   int bgrid = 0;
+  int gram_tc = 0;  // block CG Gram products on the tcgen05 tensor cores (1) or the FP32 cores (0)
 };
 
 namespace {
@@ -1411,6 +1626,32 @@ int inner_solve(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inn
   return LFX_OK;
 }
 
+// partials of U^T [V0 (V1)] (rows of V scaled by vscale when given) on the
+// tensor cores or the FP32 cores, then the fixed-order reduction into out
+template <int NV>
+int gram(lfx_mrhs* m, const float* U, const float* V0, const float* V1, const float* vscale,
+         BcgSmall* st, double* out) {
+  lfx_ctx* ctx = m->ctx;
+  const int64_t n = m->undf;
+  if (m->gram_tc) {
+    static bool attr = false;
+    if (!attr) {
+      LFX_CK(ctx, cudaFuncSetAttribute(bcg_gram_tc<NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)tc_gram_smem<NV>()));
+      attr = true;
+    }
+    bcg_gram_tc<NV><<<m->bgrid, kTcThreads, tc_gram_smem<NV>(), ctx->stream>>>(n, U, V0, V1,
+                                                                               vscale, m->bpart, st);
+  } else {
+    bcg_gram<NV><<<m->bgrid, 256, 0, ctx->stream>>>(n, U, V0, V1, vscale, m->bpart, st);
+  }
+  const int ne = NV * kBS * kBS;
+  bcg_reduce<<<(ne + 255) / 256, 256, 0, ctx->stream>>>(m->bgrid, ne, m->bpart, out, st);
+  ctx->launches += 2;
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
 int ensure_bcg(lfx_mrhs* m) {
   if (m->bcg) return LFX_OK;
   lfx_ctx* ctx = m->ctx;
@@ -1440,7 +1681,6 @@ int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner
                               ctx->stream));
   LFX_CK(ctx, cudaMemsetAsync(m->x32, 0, (size_t)n * kBS * 4, ctx->stream));
   bcg_mask<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(n, m->r32, st->active);
-  const int nred = (kBS * kBS + 255) / 256;
   // r0: column norms of R (the update kernel's norm pass, products left out)
   bcg_update<0><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 1,
                                             m->bpart);
@@ -1449,8 +1689,8 @@ int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner
   // P = orth(D^-1 R)
   bcg_update<1><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 1,
                                             nullptr);
-  bcg_gram<1><<<G, 256, 0, ctx->stream>>>(n, m->w32, m->w32, nullptr, nullptr, m->bpart, st);
-  bcg_reduce<<<nred, 256, 0, ctx->stream>>>(G, kBS * kBS, m->bpart, st->G, st);
+  int rc = gram<1>(m, m->w32, m->w32, nullptr, nullptr, st, st->G);
+  if (rc) return rc;
   bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(2, st, tol);
   bcg_update<2><<<G, 256, 0, ctx->stream>>>(n, m->w32, nullptr, m->p32, nullptr, nullptr, st, 0,
                                             nullptr);
@@ -1459,24 +1699,23 @@ int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner
   int it = 0;
   while (it < max_inner) {
     // Q = A P; alpha
-    int rc = mrhs_launch(m, m->p32, m->q32);
+    rc = mrhs_launch(m, m->p32, m->q32);
+    if (!rc) rc = gram<2>(m, m->p32, m->q32, m->r32, nullptr, st, st->C);
     if (rc) return rc;
-    bcg_gram<2><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->r32, nullptr, m->bpart, st);
-    bcg_reduce<<<2 * nred, 256, 0, ctx->stream>>>(G, 2 * kBS * kBS, m->bpart, st->C, st);
     bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(0, st, tol);
     // X += P alpha, R -= Q alpha, ||R_j||
     bcg_update<0><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 0,
                                               m->bpart);
     bcg_reduce<<<1, kBS, 0, ctx->stream>>>(G, kBS, m->bpart, st->rn, st);
     // beta (and convergence)
-    bcg_gram<1><<<G, 256, 0, ctx->stream>>>(n, m->q32, m->r32, nullptr, m->dinv, m->bpart, st);
-    bcg_reduce<<<nred, 256, 0, ctx->stream>>>(G, kBS * kBS, m->bpart, st->E, st);
+    rc = gram<1>(m, m->q32, m->r32, nullptr, m->dinv, st, st->E);
+    if (rc) return rc;
     bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(1, st, tol);
     // P = orth(D^-1 R + P beta)
     bcg_update<1><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 0,
                                               nullptr);
-    bcg_gram<1><<<G, 256, 0, ctx->stream>>>(n, m->w32, m->w32, nullptr, nullptr, m->bpart, st);
-    bcg_reduce<<<nred, 256, 0, ctx->stream>>>(G, kBS * kBS, m->bpart, st->G, st);
+    rc = gram<1>(m, m->w32, m->w32, nullptr, nullptr, st, st->G);
+    if (rc) return rc;
     bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(2, st, tol);
     bcg_update<2><<<G, 256, 0, ctx->stream>>>(n, m->w32, nullptr, m->p32, nullptr, nullptr, st,
                                               0, nullptr);
@@ -1505,6 +1744,36 @@ int add_correction(lfx_mrhs* m, double* x, int64_t ld) {
 }
 
 }  // namespace
+
+int lfx_mrhs_set_gram(lfx_mrhs* m, int32_t tensor) {
+  if (!m || (tensor != 0 && tensor != 1)) return LFX_INVALID_ARGUMENT;
+  m->gram_tc = tensor;
+  return LFX_OK;
+}
+
+int lfx_mrhs_gram(lfx_mrhs* m, const float* U, const float* V0, const float* V1, int32_t nv,
+                  int32_t tensor, double* out) {
+  if (!m || !U || !V0 || !out || (nv != 1 && nv != 2) || (nv == 2 && !V1) ||
+      (tensor != 0 && tensor != 1))
+    return LFX_INVALID_ARGUMENT;
+  lfx_ctx* ctx = m->ctx;
+  if (m->nrhs != kBS) return fail(ctx, LFX_NOT_SUPPORTED, "Gram products of 64 columns only");
+  int rc = ensure_work(m);
+  if (!rc) rc = ensure_bcg(m);
+  if (rc) return rc;
+  LFX_CK(ctx, cudaMemsetAsync(m->bcg, 0, sizeof(BcgSmall), ctx->stream));
+  const int keep = m->gram_tc;
+  m->gram_tc = tensor;
+  rc = nv == 1 ? gram<1>(m, U, V0, nullptr, nullptr, m->bcg, out)
+               : gram<2>(m, U, V0, V1, nullptr, m->bcg, out);
+  m->gram_tc = keep;
+  if (rc) return rc;
+  LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  int h_fail = 0;
+  LFX_CK(ctx, cudaMemcpy(&h_fail, &m->bcg->fail, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h_fail) return fail(ctx, LFX_TIMEOUT, "a tensor-core wait ran out");
+  return LFX_OK;
+}
 
 int lfx_mrhs_solve(lfx_mrhs* m, lfx_op* op64, const lfx_vec* diag, const double* b, double* x,
                    int64_t ld, const lfx_mrhs_cfg* cfg, lfx_solve_info* info) {

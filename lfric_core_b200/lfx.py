@@ -190,6 +190,8 @@ _SIGS = [
     ("lfx_mrhs_autotune", [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_float)], C.c_int),
     ("lfx_mrhs_solve", [vp, vp, vp, vp, vp, C.c_int64, C.POINTER(MrhsCfg), C.POINTER(SolveInfo)],
      C.c_int),
+    ("lfx_mrhs_set_gram", [vp, C.c_int32], C.c_int),
+    ("lfx_mrhs_gram", [vp, vp, vp, vp, C.c_int32, C.c_int32, vp], C.c_int),
     ("lfx_dot_noalloc", [vp, vp, C.c_int64, vp, vp], C.c_int),
     ("lfx_dot_noalloc_max_n", [], C.c_int64),
     ("lfx_noalloc_last_error", [], C.c_char_p),
@@ -551,6 +553,16 @@ class MultiRhsOperator(_Handle):
         lb, us = C.c_int32(), C.c_float()
         self.ctx.check(self.ctx.L.lfx_mrhs_autotune(self.h, reps, C.byref(lb), C.byref(us)))
         return {"levels_per_block": lb.value, "us": us.value}
+
+    def set_gram(self, tensor: bool):
+        """Block CG Gram products on the tcgen05 tensor cores (True) or the
+        FP32 cores."""
+        self.ctx.check(self.ctx.L.lfx_mrhs_set_gram(self.h, 1 if tensor else 0))
+
+    def gram(self, u_ptr: int, v0_ptr: int, v1_ptr: int, nv: int, tensor: bool, out_ptr: int):
+        """out (device nv x 64 x 64 FP64) = U^T V_v for device FP32 blocks."""
+        self.ctx.check(self.ctx.L.lfx_mrhs_gram(self.h, u_ptr, v0_ptr, v1_ptr or None, nv,
+                                                1 if tensor else 0, out_ptr))
 
     def solve(self, op64: "LmaOperator", diag: "FieldVector", b_ptr: int, x_ptr: int, ld: int,
               r_tol=1e-8, inner_tol=1e-2, max_outer=20, max_inner=5000, method=MRHS_PER_RHS_CG):

@@ -87,7 +87,8 @@ def test_batch_results_same_alone_and_in_the_mix(ctx):
 def test_batch_results_do_not_depend_on_the_launch_shape(ctx):
     """Columns per work item, blocks per SM and L2 group size change how the
     persistent kernel splits the work, not the sums: the same bits."""
-    specs = [(5, 33, 1, 1e-9), (7, 12, 2, 1e-8), (4, 40, 3, 1e-10)]
+    specs = [(5, 33, 1, 1e-9), (7, 12, 2, 1e-8), (4, 40, 3, 1e-10), (6, 31, 4, 1e-9),
+             (5, 30, 5, 1e-8)]
     systems = [w0_system(ctx, n, nl, sd) for n, nl, sd, _ in specs]
     tols = [t for *_, t in specs]
     ref = run_batch(ctx, systems, tols, shape=(64, 2, 1 << 40))
@@ -111,7 +112,7 @@ def test_batch_autotune_keeps_results(ctx):
         x.set_scalar(0.0)
         xs.append((B.admit(s["ops"][lfx.R64], s["ops"][lfx.R32], s["prec"], s["b"], x, tol, 5000), x))
     t = B.autotune(iters=2)
-    assert t["cells_per_item"] in (32, 64, 128) and t["us_per_iteration"] > 0
+    assert t["cells_per_item"] in (1, 2, 4, 8) and t["us_per_iteration"] > 0
     for _ in range(2000):
         if B.step() == 2:
             break

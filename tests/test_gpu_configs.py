@@ -49,8 +49,9 @@ def rel_err(x, xo):
     return float(np.linalg.norm(x - xo) / np.linalg.norm(xo))
 
 
+@pytest.mark.parametrize("method", [lfx.MRHS_PER_RHS_CG, lfx.MRHS_BLOCK_CG])
 @pytest.mark.parametrize("kind", [lfx.MRHS_TF32, lfx.MRHS_BF16])
-def test_multi_rhs_c48x30_64rhs_against_oracle(ctx, kind):
+def test_multi_rhs_c48x30_64rhs_against_oracle(ctx, kind, method):
     p = mg.w0_problem(48, 30, seed=1, rhs="normal")
     s = wl.device_w0(ctx, p)
     nrhs, rtol = 64, 1e-8
@@ -59,7 +60,7 @@ def test_multi_rhs_c48x30_64rhs_against_oracle(ctx, kind):
     x = torch.zeros_like(b)
     M = lfx.MultiRhsOperator(s.op, kind, nrhs)
     torch.cuda.synchronize()
-    info = M.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=rtol)
+    info = M.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=rtol, method=method)
     ctx.synchronize()
     X = x.cpu().numpy()
     o = o_lma(p)
@@ -74,11 +75,13 @@ def test_multi_rhs_c48x30_64rhs_against_oracle(ctx, kind):
         assert rel_err(X[r], xo) <= ERR_FACTOR * rtol, (r, rel_err(X[r], xo))
 
 
-# (N, levels, tolerance, seed): the corners of the uneven batch's ranges and
-# points between them
+# (N, levels, tolerance, seed): the corners of the uneven batch's ranges,
+# points between them, and the level counts at a segment boundary (30, 31,
+# 32 levels: one or two 31-row segments per cell column)
 CONFIG3_SUBSET = [(12, 10, 1e-6, 101), (48, 70, 1e-10, 102), (20, 33, 1e-8, 103),
                   (36, 12, 1e-9, 104), (16, 64, 1e-7, 105), (30, 47, 1e-10, 106),
-                  (44, 25, 1e-6, 107), (25, 58, 1e-9, 108)]
+                  (44, 25, 1e-6, 107), (25, 58, 1e-9, 108), (47, 31, 1e-8, 109),
+                  (17, 30, 1e-9, 110), (13, 32, 1e-7, 111), (40, 62, 1e-8, 112)]
 
 
 def test_batch_uneven_w0_subset_against_oracle(ctx):
@@ -108,7 +111,8 @@ def test_batch_uneven_w0_subset_against_oracle(ctx):
         assert rel_err(xv, xo) <= ERR_FACTOR * tol, (n, nl, rel_err(xv, xo))
 
 
-CONFIG4_SUBSET = [(12, 20, 1e-6, 501), (24, 45, 1e-10, 502), (32, 70, 1e-8, 503)]
+CONFIG4_SUBSET = [(12, 20, 1e-6, 501), (24, 45, 1e-10, 502), (32, 70, 1e-8, 503),
+                  (21, 31, 1e-9, 504)]
 
 
 def test_batch_w2_requests_against_oracle(ctx):

@@ -148,3 +148,73 @@ def test_mrhs_solve_nonzero_initial_guess_and_converged_rhs(ctx):
             continue
         r0 = np.linalg.norm(B[r] - o.apply(X0[r]))
         assert np.linalg.norm(B[r] - o.apply(X[r])) <= 1e-9 * r0 * (1 + 1e-9)
+
+
+@pytest.mark.parametrize("kind", [TF32, BF16])
+def test_mrhs_block_cg_reaches_fp64_tolerance(ctx, kind):
+    """Block CG over the 64 right-hand sides: every right-hand side reaches
+    the FP64 tolerance on the oracle's residual, in fewer inner iterations
+    than CG run on each right-hand side alone, and its solutions agree with
+    the oracle's FP64 CG."""
+    p = mg.w0_problem(8, 6, seed=3)
+    s = wl.device_w0(ctx, p)
+    nrhs = 64
+    M = lfx.MultiRhsOperator(s.op, kind, nrhs)
+    B = np.stack([mg.normal(900 + r, p.undf) for r in range(nrhs)])
+    B[5] = 0.0  # a zero right-hand side: converged at once, left out of the block
+    b = torch.from_numpy(B).cuda()
+    out = {}
+    for method in (lfx.MRHS_PER_RHS_CG, lfx.MRHS_BLOCK_CG):
+        x = torch.zeros_like(b)
+        torch.cuda.synchronize()
+        info = M.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=1e-8,
+                       inner_tol=1e-3, method=method)
+        ctx.synchronize()
+        out[method] = (x.cpu().numpy(), info)
+    X, info = out[lfx.MRHS_BLOCK_CG]
+    o = o_lma(p)
+    od = orc.Preconditioner.diagonal(o.diagonal())
+    assert info[5].converged and np.all(X[5] == 0.0)
+    for r in range(nrhs):
+        assert info[r].converged and info[r].status == 0, r
+        if r == 5:
+            continue
+        rel = np.linalg.norm(B[r] - o.apply(X[r])) / np.linalg.norm(B[r])
+        assert rel <= 1e-8, (r, rel)
+    for r in (0, 33):
+        xo, _ = orc.solve("cg", o, od, B[r], r_tol=1e-10, max_iter=5000)
+        assert np.linalg.norm(X[r] - xo) <= 1e-5 * np.linalg.norm(xo)
+    per = max(i.inner_iterations for i in out[lfx.MRHS_PER_RHS_CG][1])
+    blk = max(i.inner_iterations for i in info)
+    assert blk < per, (blk, per)
+
+
+@pytest.mark.parametrize("nv", [1, 2])
+def test_block_cg_gram_products_match_fp64(ctx, nv):
+    """The block CG's Gram products U^T [V0 V1] of n x 64 blocks: on the
+    tcgen05 tensor cores (FP32 split into TF32 hi + lo, three MMAs per step,
+    FP32 accumulation in tensor memory) and on the FP32 cores, each within
+    5e-5 of |U|^T |V| of the FP64 product entry by entry (n = 72 618 rows,
+    not a multiple of the 32-row chunk), and run to run the same bits."""
+    p = mg.w0_problem(24, 20, seed=1)
+    s = wl.device_w0(ctx, p)
+    M = lfx.MultiRhsOperator(s.op, TF32, 64)
+    n = p.undf
+    g = torch.Generator(device="cpu").manual_seed(77)
+    U = torch.randn(n, 64, generator=g).cuda()
+    V = [torch.randn(n, 64, generator=g).cuda() for _ in range(nv)]
+    Vc = torch.cat(V, dim=1).double()
+    want = (U.double().T @ Vc).cpu().numpy()
+    bound = 5e-5 * (U.double().abs().T @ Vc.abs()).cpu().numpy()
+    out = torch.empty(nv, 64, 64, dtype=torch.float64, device="cuda")
+    for tensor in (True, False):
+        got = []
+        for _ in range(2):
+            out.fill_(float("nan"))
+            torch.cuda.synchronize()
+            M.gram(U.data_ptr(), V[0].data_ptr(), V[-1].data_ptr() if nv == 2 else 0, nv, tensor,
+                   out.data_ptr())
+            got.append(out.cpu().numpy().copy())
+        assert np.array_equal(got[0], got[1]), tensor
+        G = np.concatenate(list(got[0]), axis=1)  # 64 x 64 nv
+        assert np.all(np.abs(G - want) <= bound), (tensor, float(np.max(np.abs(G - want) / bound)))

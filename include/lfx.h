@@ -444,7 +444,7 @@ typedef struct {
  * fastest. */
 int lfx_batch_autotune(lfx_batch* b, int32_t iters, lfx_batch_tuning* out);
 int lfx_batch_get_tuning(const lfx_batch* b, lfx_batch_tuning* out);
-/* pin a launch shape (cells_per_item 1 to 128) */
+/* pin a launch shape (cells_per_item 1 to 8) */
 int lfx_batch_set_tuning(lfx_batch* b, int32_t cells_per_item, int32_t blocks_per_sm,
                          int64_t group_bytes);
 /* upper bound in seconds of one grid-barrier wait (default 2) */

@@ -67,7 +67,6 @@ constexpr int kBW = kBT / 32;    // warps per block
 constexpr int kBSub = 8;         // a chunk item: kBSub chunks of RCHUNK values (16384)
 constexpr int kMaxIters = 64;    // super-iterations per launch, at most
 constexpr int kMaxSeg = 4;       // warps (segments of <= 31 levels) per cell column, at most
-constexpr int kMaxCB = 128;      // cell columns per apply item, at most
 constexpr int kMaxColours = 8;   // cell colours of a slot, at most
 constexpr int kBCols = 64;       // columns per sweep item
 constexpr int kBRows = 160;      // rows per preconditioner column, at most
@@ -385,6 +384,164 @@ __device__ __noinline__ void apply_phase(const BParams& P, const int4* __restric
   }
 }
 
+// ---- The FP32 apply with its inputs staged through shared memory.
+// A warp walks its items' cell-column segments (units) in order and keeps
+// the next unit's inputs in flight while it computes the current one: each
+// lane copies its level's packed matrix entries, x values and partial sums
+// of y with 4-byte cp.async into a two-stage per-warp buffer, so the bytes
+// in flight do not cost registers (the persistent kernel runs at 128
+// registers a thread, 16 warps an SM). A lane reads back only what it copied
+// itself. An item's cell descriptors are read into shared memory once.
+constexpr int kPipeCols = 8;  // cell columns per item, at most, in this path
+constexpr int kDescInts = 12;  // cell descriptor ints, at most
+
+template <int NDF>
+struct PipeShape {
+  static constexpr int NP = NDF * (NDF + 1) / 2;
+  static constexpr int STAGE = (NP + 2 * NDF) * 32;  // floats: M[p][lane], X[j][lane], Y[df][lane]
+  static constexpr int WARP_FLOATS = 2 * STAGE + kPipeCols * kDescInts;
+  static constexpr size_t BLOCK_BYTES = (size_t)kBW * WARP_FLOATS * 4;
+};
+
+__device__ __forceinline__ void cp4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+
+template <int NDF>
+__device__ __noinline__ void apply_phase32_pipe(const BParams& P, const int4* __restrict__ items,
+                                                int i0, int i1, float* wsm) {
+  using S = PipeShape<NDF>;
+  constexpr int NP = S::NP;
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kBW + (threadIdx.x >> 5), nw = gridDim.x * kBW;
+  float* st0 = wsm;
+  int* dsm = reinterpret_cast<int*>(wsm + 2 * S::STAGE);
+  for (int u = i0 + gw; u < i1; u += nw) {
+    const int4 it = __ldg(items + u);
+    const int s = it.x;
+    if (!ph_run(__ldcg(&P.st[s].phase))) continue;  // warp-uniform
+    const BSlot* D = P.slots + s;
+    const float* M = D->S32;
+    const int sblk = D->sblk32, cdints = D->cdints, nl = D->nl, nseg = D->nseg, L = D->segL;
+    const float* x = D->p;
+    float* y = D->z;
+    double* part = D->part + 2 * (int64_t)D->nch;
+    const int q0 = it.y, nq = it.z;
+    if (lane == 0)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(M + (size_t)q0 * sblk),
+                   "r"((unsigned)((size_t)nq * sblk * 4))
+                   : "memory");
+    __syncwarp();
+    for (int i = lane; i < nq * cdints; i += 32) dsm[i] = __ldg(D->cdesc + (size_t)q0 * cdints + i);
+    __syncwarp();
+    // unit j = (column j / nseg, segment j % nseg)
+    const int nunit = nq * nseg;
+    auto issue = [&](int j) {
+      float* stg = st0 + (j & 1) * S::STAGE;
+      const int c = j / nseg, sg = j % nseg;
+      const int* dsc = dsm + c * cdints;
+      const uint32_t flags = (uint32_t)dsc[NDF];
+      const int k = sg * L + lane - 1;
+      const bool own = lane >= 1 && lane <= L;
+      const bool v = k >= 0 && k < nl && lane <= L;
+      if (v) {
+        const float* Mc = M + (size_t)(q0 + c) * sblk + k;
+#pragma unroll
+        for (int pp = 0; pp < NP; ++pp) cp4(stg + pp * 32 + lane, Mc + pp * nl);
+#pragma unroll
+        for (int jj = 0; jj < NDF; ++jj) cp4(stg + (NP + jj) * 32 + lane, x + dsc[jj] + k);
+      }
+#pragma unroll
+      for (int df = 0; df < NDF; ++df) {
+        const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+        const bool opens = (flags >> df) & 1u;
+        const bool live = own && (lower ? k <= nl : v);
+        if (!upper && !opens && live) cp4(stg + (NP + NDF + df) * 32 + lane, y + dsc[df] + k);
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    issue(0);
+    double dot = 0.0;
+    for (int j = 0; j < nunit; ++j) {
+      if (j + 1 < nunit)
+        issue(j + 1);
+      else
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+      const float* stg = st0 + (j & 1) * S::STAGE;
+      const int c = j / nseg, sg = j % nseg;
+      const int* dsc = dsm + c * cdints;
+      int mf[NDF];
+#pragma unroll
+      for (int jj = 0; jj < NDF; ++jj) mf[jj] = dsc[jj];
+      const uint32_t flags = (uint32_t)dsc[NDF], prt = (uint32_t)dsc[NDF + 1];
+      const int k = sg * L + lane - 1;
+      const bool own = lane >= 1 && lane <= L;
+      const bool v = k >= 0 && k < nl && lane <= L;
+      float m[NP], xv[NDF], yo[NDF];
+#pragma unroll
+      for (int pp = 0; pp < NP; ++pp) m[pp] = v ? stg[pp * 32 + lane] : 0.f;
+#pragma unroll
+      for (int jj = 0; jj < NDF; ++jj) xv[jj] = v ? stg[(NP + jj) * 32 + lane] : 0.f;
+#pragma unroll
+      for (int df = 0; df < NDF; ++df) {
+        const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+        const bool opens = (flags >> df) & 1u;
+        const bool live = own && (lower ? k <= nl : v);
+        yo[df] = (!upper && !opens && live) ? stg[(NP + NDF + df) * 32 + lane] : 0.f;
+      }
+#define MV(i, jx) m[pidx<NDF>(i, jx)]
+#pragma unroll
+      for (int df = 0; df < NDF; ++df) {
+        if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
+        const bool last = (flags >> (24 + df)) & 1u;
+        if ((flags >> (8 + df)) & 1u) {
+          const int bsel = (prt >> (4 * df)) & 15u;
+#pragma unroll
+          for (int bb = df + 1; bb < NDF; ++bb) {
+            if (bb != bsel) continue;
+            float acc = yo[df];
+#pragma unroll
+            for (int jj = 0; jj < NDF; ++jj) {
+              const float mb = __shfl_up_sync(0xffffffffu, MV(bb, jj), 1);
+              const float xb = __shfl_up_sync(0xffffffffu, xv[jj], 1);
+              if (v) acc = fmaf(MV(df, jj), xv[jj], acc);
+              if (own && k >= 1 && k <= nl) acc = fmaf(mb, xb, acc);
+            }
+            if (own && k <= nl) {
+              const int row = mf[df] + k;
+              __stcg(y + row, acc);
+              if (last) {
+                const float pr = k < nl ? xv[df] : __ldcg(x + row);
+                dot = fma((double)pr, (double)acc, dot);
+              }
+            }
+          }
+        } else {
+          float acc = yo[df];
+#pragma unroll
+          for (int jj = 0; jj < NDF; ++jj) acc = fmaf(MV(df, jj), xv[jj], acc);
+          if (own && v) {
+            __stcg(y + mf[df] + k, acc);
+            if (last) dot = fma((double)xv[df], (double)acc, dot);
+          }
+        }
+      }
+#undef MV
+      if (sg == nseg - 1) {
+        const double w = warp_butterfly(dot);
+        if (lane == 0) __stcg(part + q0 + c, w);
+        dot = 0.0;
+      }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
+  }
+}
+
 // alpha = rz / <p, z> for every running slot: one block per slot sums the
 // slot's per-column shares in a fixed order
 __device__ __noinline__ void alpha_phase(const BParams& P, BShared& sh) {
@@ -592,10 +749,13 @@ template <class T> struct W5 { T a, b, c, d, e; };
 // The persistent kernel: `iters` super-iterations of every admitted slot.
 template <int NDF, bool CMA>
 __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict__ PP) {
+  // per warp: the two stages and the item descriptors of the FP32 apply
+  // (the column sweeps of phase C stage their rows in the same memory)
+  extern __shared__ __align__(16) float pipe_smem[];
+  static_assert(PipeShape<NDF>::BLOCK_BYTES >= sizeof(float) * kBRows * (kBCols + 1),
+                "the sweeps' staging fits the apply's shared memory");
   __shared__ BShared sh;
   __shared__ BParams sp;
-  constexpr int XS = CMA ? kBRows * (kBCols + 1) : 1;
-  __shared__ float xs[XS];
   __shared__ SweepShared ss;
   {
     const int* src = reinterpret_cast<const int*>(PP);
@@ -622,7 +782,8 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
     for (int g = 0; g < P.ngr32; ++g)
       for (int c = 0; c < P.ncolour; ++c) {
         const int o = g * P.ncolour + c;
-        apply_phase<NDF, false>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1));
+        apply_phase32_pipe<NDF>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1),
+                                pipe_smem + (threadIdx.x >> 5) * PipeShape<NDF>::WARP_FLOATS);
         if (!grid_sync(P, sh)) return;
       }
     alpha_phase(P, sh);
@@ -719,7 +880,7 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
     }
     // ---- C: column sweeps, then the Jacobi rows with <r, z> and beta
     if (CMA && P.any_cma) {
-      sweep_phase(P, xs, ss);
+      sweep_phase(P, pipe_smem, ss);
       if (!grid_sync(P, sh)) return;
       chunk_phase<1>(
           P, sh, [](int ph, int) { return ph_run(ph); },
@@ -836,6 +997,10 @@ int upload(lfx_ctx* ctx, T* dst, const std::vector<T>& src) {
   LFX_CK(ctx, cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
                               ctx->stream));
   return LFX_OK;
+}
+
+size_t pipe_bytes(int ndf) {
+  return ndf == 8 ? PipeShape<8>::BLOCK_BYTES : PipeShape<6>::BLOCK_BYTES;
 }
 
 const void* pick_kernel(int ndf, bool cma) {
@@ -963,7 +1128,7 @@ int graph_for(lfx_batch* B, int bps, cudaGraphExec_t* out) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(ctx->num_sms * bps));
   cfg.blockDim = dim3(kBT);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = pipe_bytes(B->ndf);
   cfg.stream = ctx->stream;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeCooperative;
@@ -1106,7 +1271,10 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t reser
     // the kernel holds at most two blocks per SM (launch bounds); fewer if
     // the device says so
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(ndf, ndf == 6), kBT, 0);
+    cudaFuncSetAttribute(pick_kernel(ndf, ndf == 6), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pipe_bytes(ndf));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(ndf, ndf == 6), kBT,
+                                                  pipe_bytes(ndf));
     B->max_bps = std::max(1, std::min(per_sm, 2));
     B->blocks_per_sm = B->max_bps;
     B->group_bytes = ctx->l2_bytes / 2;
@@ -1169,6 +1337,8 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   const int nseg = (nl + 1 + 30) / 31;
   if (nseg > kMaxSeg)
     return fail(ctx, LFX_NOT_SUPPORTED, "batch: at most 123 levels per column");
+  if (L->cs_ints > kDescInts)
+    return fail(ctx, LFX_NOT_SUPPORTED, "batch: cell descriptors of at most 12 ints");
   const bool cma = prec32->kind == PREC_CMA;
   if (prec32->precision != LFX_R32 || (prec32->kind != PREC_DIAG && !cma) || !prec32->rdiag ||
       prec32->rdiag_n != L->undf_to || (cma && !prec32->jacobi_zeroed))
@@ -1357,7 +1527,7 @@ int lfx_batch_get_tuning(const lfx_batch* B, lfx_batch_tuning* t) {
 int lfx_batch_set_tuning(lfx_batch* B, int32_t cells_per_item, int32_t blocks_per_sm,
                          int64_t group_bytes) {
   if (!B) return LFX_INVALID_ARGUMENT;
-  if (cells_per_item < 1 || cells_per_item > kMaxCB ||
+  if (cells_per_item < 1 || cells_per_item > kPipeCols ||
       blocks_per_sm < 1 || blocks_per_sm > B->max_bps || group_bytes < 1)
     return fail(B->ctx, LFX_INVALID_ARGUMENT, "batch tuning out of range");
   B->cells_per_item = cells_per_item;

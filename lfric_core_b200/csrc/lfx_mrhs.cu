@@ -566,7 +566,11 @@ __global__ void k_dinv(int64_t n, const double* __restrict__ d, float* __restric
 // fixed order; the 64 x 64 algebra runs in FP64 in one block.
 constexpr int kBS = 64;          // right-hand sides of a block solve
 constexpr int kBcgRows = 32;     // rows per staged chunk
-constexpr double kBcgDrop = 1e-10;
+// W is FP32 and its Gram sums carry relative errors near 1e-6 of the largest
+// entry, so directions whose pivot falls below 1e-5 of the largest are noise
+// and are dropped (the kept part of W then has a condition number under
+// about 300, and W T is orthonormal to a few parts in a thousand)
+constexpr double kBcgDrop = 1e-5;
 
 struct BcgSmall {
   double C[2 * kBS * kBS];  // [v][i][j]: v = 0 P^T Q, v = 1 P^T R (gram of P with Q, R)

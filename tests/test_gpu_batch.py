@@ -91,8 +91,8 @@ def test_batch_results_do_not_depend_on_the_launch_shape(ctx):
              (5, 30, 5, 1e-8)]
     systems = [w0_system(ctx, n, nl, sd) for n, nl, sd, _ in specs]
     tols = [t for *_, t in specs]
-    ref = run_batch(ctx, systems, tols, shape=(64, 2, 1 << 40))
-    for shape in ((32, 1, 1 << 40), (128, 2, 1), (32, 2, 40_000)):
+    ref = run_batch(ctx, systems, tols, shape=(4, 2, 1 << 40))
+    for shape in ((1, 1, 1 << 40), (8, 2, 1), (2, 2, 40_000)):
         got = run_batch(ctx, systems, tols, iters=3, shape=shape)
         for (xa, ia), (xb, ib) in zip(ref, got):
             assert same(xa, xb) and ia["iterations"] == ib["iterations"], shape

@@ -225,6 +225,28 @@ def _run_batch_w2(args):
           flush=True)
 
 
+def _run_batch_w0(args):
+    """The first `count` systems of the uneven W0 batch through the batch
+    engine (one persistent kernel per step), `steps` steps after one untimed
+    step, with a pinned launch shape (columns per item, blocks per SM)."""
+    ctx = lfx.Context(0)
+    specs = config3_specs()[:args.count]
+    systems = [batch_system(ctx, n, l, sd, mg.W0) for n, l, _, sd in specs]
+    b = lfx.Batch(ctx, 8, len(systems), reserve_bytes=1 << 30, iters=args.iters)
+    b.set_tuning(args.cells_per_item, args.blocks_per_sm, 1 << 40)
+    xs = []
+    for s, (_, _, tol, _) in zip(systems, specs):
+        x = lfx.FieldVector(ctx, [s.undf])
+        x.set_scalar(0.0)
+        b.admit(s.ops[lfx.R64], s.ops[lfx.R32], s.prec32, s.b, x, tol, 20000)
+        xs.append(x)
+    b.step()
+    for _ in range(args.steps):
+        b.step()
+    ctx.synchronize()
+    print("batch steps done", b.tuning(), flush=True)
+
+
 def _run_prec(args):
     """Column preconditioner applies of the C96x30 W2 system (FP32 or FP64),
     consecutive applies on different vectors (four pairs, past L2), timed by
@@ -293,7 +315,7 @@ def _run_solve_w2(args):
 
 def main(argv=None):
     """One named workload, run once, for profilers:
-    ``python -m lfric_core_b200.workloads apply|time-apply|prec|mrhs|batch-w2|solve-w2 [options]``."""
+    ``python -m lfric_core_b200.workloads apply|time-apply|prec|mrhs|batch-w0|batch-w2|solve-w2 [options]``."""
     import argparse
     ap = argparse.ArgumentParser(prog="python -m lfric_core_b200.workloads")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -323,6 +345,12 @@ def main(argv=None):
     b.add_argument("--n", type=int, default=94)
     b.add_argument("--nl", type=int, default=64)
     b.add_argument("--seed", type=int, default=505)
+    bw = sub.add_parser("batch-w0", help="a subset of the uneven W0 batch through the batch engine")
+    bw.add_argument("--count", type=int, default=16)
+    bw.add_argument("--iters", type=int, default=4)
+    bw.add_argument("--steps", type=int, default=1)
+    bw.add_argument("--cells-per-item", type=int, default=2)
+    bw.add_argument("--blocks-per-sm", type=int, default=2)
     q = sub.add_parser("prec", help="column preconditioner applies of the W2 system")
     q.add_argument("--n", type=int, default=96)
     q.add_argument("--nl", type=int, default=30)
@@ -338,7 +366,8 @@ def main(argv=None):
                    help="pinned apply kernel:stages for FP32,FP64 (default: autotune)")
     args = ap.parse_args(argv)
     {"apply": _run_apply, "time-apply": _run_time_apply, "mrhs": _run_mrhs,
-     "batch-w2": _run_batch_w2, "solve-w2": _run_solve_w2, "prec": _run_prec}[args.cmd](args)
+     "batch-w2": _run_batch_w2, "batch-w0": _run_batch_w0, "solve-w2": _run_solve_w2,
+     "prec": _run_prec}[args.cmd](args)
     return 0
 
 

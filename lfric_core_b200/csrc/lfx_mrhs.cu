@@ -668,9 +668,11 @@ __global__ void __launch_bounds__(256) bcg_gram(int64_t n, const float* __restri
 
 // ---- The same Gram on the 5th-generation tensor cores (tcgen05).
 // D (64 x 64 NV) = U^T [V_0 .. V_NV-1] accumulates in tensor memory (TMEM,
-// FP32): A = U^T and B = V are both MN-major in shared memory, in the
-// canonical no-swizzle layout (core matrices of 8 K-rows x 16 bytes, K-rows
-// 16 bytes apart, MN groups 128 bytes apart, K groups G x 128 bytes apart).
+// FP32): A = U^T (64 x K) and B = V^T (64 NV x K) are both K-major in shared
+// memory (kind::tf32 takes K-major operands only), in the canonical
+// no-swizzle layout: core matrices of 8 MN-rows x 16 bytes (4 K values),
+// MN-rows 16 bytes apart, MN groups of 8 rows 128 bytes apart (stride byte
+// offset), K groups of 4 values MN/8 x 128 bytes apart (leading byte offset).
 // Each FP32 value is split into TF32 parts hi + lo and a product taken as
 // hi hi + hi lo + lo hi (three kind::tf32 MMAs of M = 64, K = 8 per K step),
 // which keeps about FP32 accuracy. Two 32-row stages: the block stages the
@@ -691,11 +693,11 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
-// instruction descriptor: FP32 accumulate, A and B TF32, both MN-major, M = 64
+// instruction descriptor: FP32 accumulate, A and B TF32, both K-major, M = 64
 template <int N>
-__host__ __device__ constexpr uint32_t idesc_tf32_mn() {
-  return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
-         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(64 >> 4) << 24);
+__host__ __device__ constexpr uint32_t idesc_tf32_k() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(64 >> 4) << 24);
 }
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
                                        uint32_t acc) {
@@ -730,29 +732,31 @@ __device__ __forceinline__ float tf32_round(float x) {
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
 }
-// stage 32 rows of G column groups (4 floats each) of an n x (4 G) block made
-// of `nsrc` 64-column row-major sources into the canonical layout, as TF32
-// hi and lo parts; rows past n are zero
-__device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, int G,
+// stage rows row0 .. row0 + 31 (the K dimension) of an n x MN block made of
+// 64-column row-major sources (columns 0..63 from s0, 64.. from s1) as the
+// K-major operand (MN x 32), TF32 hi and lo parts; rows past n are zero. A
+// thread takes four consecutive rows of one column: the warp's loads of a row
+// are coalesced and its 16-byte stores fill 512 contiguous bytes.
+__device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, int MN,
                                          const float* s0, const float* s1, int64_t row0,
                                          int64_t n, const float* __restrict__ scale) {
-  for (int e = threadIdx.x; e < kTcRows * G; e += kTcThreads) {
-    const int k8 = e & 7, g = (e >> 3) % G, kg = e / (8 * G);
-    const int k = kg * 8 + k8;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (row0 + k < n) {
-      const float* src = g < kBS / 4 ? s0 + (size_t)(row0 + k) * kBS + 4 * g
-                                     : s1 + (size_t)(row0 + k) * kBS + 4 * (g - kBS / 4);
-      v = ld4(src);
-      if (scale) {
-        const float sc = scale[row0 + k];
-        v.x *= sc; v.y *= sc; v.z *= sc; v.w *= sc;
+  for (int e = threadIdx.x; e < (kTcRows / 4) * MN; e += kTcThreads) {
+    const int m = e % MN, kq = e / MN;
+    const float* src = m < kBS ? s0 + m : s1 + (m - kBS);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t k = row0 + 4 * kq + q;
+      v[q] = 0.f;
+      if (k < n) {
+        v[q] = __ldg(src + (size_t)k * kBS);
+        if (scale) v[q] *= __ldg(scale + k);
       }
     }
-    const float4 h = make_float4(tf32_round(v.x), tf32_round(v.y), tf32_round(v.z), tf32_round(v.w));
-    const float4 l = make_float4(tf32_round(v.x - h.x), tf32_round(v.y - h.y),
-                                 tf32_round(v.z - h.z), tf32_round(v.w - h.w));
-    const size_t off = ((size_t)(kg * G + g) * 8 + k8) * 16;
+    const float4 h = make_float4(tf32_round(v[0]), tf32_round(v[1]), tf32_round(v[2]), tf32_round(v[3]));
+    const float4 l = make_float4(tf32_round(v[0] - h.x), tf32_round(v[1] - h.y),
+                                 tf32_round(v[2] - h.z), tf32_round(v[3] - h.w));
+    const size_t off = ((size_t)kq * (MN / 8) + m / 8) * 128 + (size_t)(m % 8) * 16;
     *reinterpret_cast<float4*>(hi + off) = h;
     *reinterpret_cast<float4*>(lo + off) = l;
   }
@@ -765,7 +769,7 @@ __global__ void __launch_bounds__(kTcThreads) bcg_gram_tc(int64_t n, const float
                                                          const float* __restrict__ vscale,
                                                          double* __restrict__ partials,
                                                          BcgSmall* st) {
-  constexpr int N = kBS * NV, GA = kBS / 4, GB = N / 4;
+  constexpr int N = kBS * NV, LBA = kBS / 8 * 128, LBB = N / 8 * 128;
   constexpr int ABYTES = kTcRows * kBS * 4, BBYTES = kTcRows * N * 4;
   constexpr int STAGE = 2 * ABYTES + 2 * BBYTES;
   extern __shared__ __align__(1024) unsigned char tc_smem[];
@@ -790,7 +794,7 @@ __global__ void __launch_bounds__(kTcThreads) bcg_gram_tc(int64_t n, const float
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  constexpr uint32_t IDESC = idesc_tf32_mn<N>();
+  constexpr uint32_t IDESC = idesc_tf32_k<N>();
   int j = 0;  // chunks of this block so far
   for (int64_t c = blockIdx.x; c * kTcRows < n; c += gridDim.x, ++j) {
     const int sidx = j & 1;
@@ -804,8 +808,8 @@ __global__ void __launch_bounds__(kTcThreads) bcg_gram_tc(int64_t n, const float
       __syncthreads();
       if (s_abort) break;
     }
-    tc_stage(base, base + ABYTES, GA, U, U, c * kTcRows, n, nullptr);
-    tc_stage(base + 2 * ABYTES, base + 2 * ABYTES + BBYTES, GB, V0, NV > 1 ? V1 : V0,
+    tc_stage(base, base + ABYTES, kBS, U, U, c * kTcRows, n, nullptr);
+    tc_stage(base + 2 * ABYTES, base + 2 * ABYTES + BBYTES, N, V0, NV > 1 ? V1 : V0,
              c * kTcRows, n, vscale);
     // generic-proxy writes of the operands become visible to the tensor core
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -816,10 +820,11 @@ __global__ void __launch_bounds__(kTcThreads) bcg_gram_tc(int64_t n, const float
       const uint32_t b_hi = a_hi + 2 * ABYTES, b_lo = b_hi + BBYTES;
 #pragma unroll
       for (int kg = 0; kg < kTcRows / 8; ++kg) {
-        const uint64_t ah = umma_desc(a_hi + kg * GA * 128, GA * 128, 128);
-        const uint64_t al = umma_desc(a_lo + kg * GA * 128, GA * 128, 128);
-        const uint64_t bh = umma_desc(b_hi + kg * GB * 128, GB * 128, 128);
-        const uint64_t bl = umma_desc(b_lo + kg * GB * 128, GB * 128, 128);
+        // K step kg: K groups 2 kg and 2 kg + 1
+        const uint64_t ah = umma_desc(a_hi + 2 * kg * LBA, LBA, 128);
+        const uint64_t al = umma_desc(a_lo + 2 * kg * LBA, LBA, 128);
+        const uint64_t bh = umma_desc(b_hi + 2 * kg * LBB, LBB, 128);
+        const uint64_t bl = umma_desc(b_lo + 2 * kg * LBB, LBB, 128);
         tc_mma(tmem, ah, bh, IDESC, (j > 0 || kg > 0) ? 1u : 0u);
         tc_mma(tmem, ah, bl, IDESC, 1u);
         tc_mma(tmem, al, bh, IDESC, 1u);

@@ -82,9 +82,11 @@ struct BSlot {
   const float* S32;
   const double* S64;
   const int* cdesc;
+  // the FP32 triangles level-major: [q][k][4 npv] (npv float4 per level)
+  const float4* L32;
   int32_t sblk32, sblk64, cdints, nl;
   int32_t nseg, segL, nch, ncell;
-  int32_t pad0, cma, ncol, nrow;
+  int32_t npv, cma, ncol, nrow;
   int64_t n;
   double* part;  // [0, 2 nch): chunk sums; [2 nch, 2 nch + ncell): <p, z> per cell column
   // preconditioner: FP32 Jacobi diagonal (zero on the column rows of a
@@ -129,11 +131,9 @@ struct BParams {
 };
 
 struct BShared {
-  BSlot slot;
-  BState state;
-  int skip, last, s;
-  int4 item;
+  int last;
   double red[kBT / 32];
+  double red2[2][kBT / 32];
   int ok;
 };
 
@@ -215,20 +215,6 @@ __device__ __forceinline__ double bsum(double acc, double* red) {
   }
   __syncthreads();
   return tot;
-}
-
-// the slot record and state of a work item, copied to shared memory by the
-// block (the record is read-only during a launch; the state is read through
-// L2, since other blocks write it)
-__device__ __forceinline__ void load_item(const BParams& P, BShared& sh, int s) {
-  const int* src = reinterpret_cast<const int*>(P.slots + s);
-  int* dst = reinterpret_cast<int*>(&sh.slot);
-  constexpr int NW = sizeof(BSlot) / 4;
-  for (int i = threadIdx.x; i < NW; i += kBT) dst[i] = __ldg(src + i);
-  const int* ss = reinterpret_cast<const int*>(P.st + s);
-  int* sd = reinterpret_cast<int*>(&sh.state);
-  constexpr int NS = sizeof(BState) / 4;
-  for (int i = threadIdx.x; i < NS; i += kBT) sd[i] = __ldcg(ss + i);
 }
 
 // a slot's state as one thread sees it in L2 (other blocks write it)
@@ -337,10 +323,12 @@ __device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const i
 
 // The apply items [i0, i1) of one (group, colour) phase, one warp per item
 // (no block-wide barrier: each warp walks its item's cell columns, and each
-// column's segments, in order). FP32: z = A32 p for running slots, each
-// column's share of <p, z> (lanes over the column's segments in order, then
-// the lane butterfly) stored at its colour-loop position. FP64: r64 = b -
-// A64 x for slots taking a true residual. An item's packed matrices are one
+// column's segments, in order). FP32 (the form apply_phase32_lm restates on
+// the level-major copy): z = A32 p for running slots, each column's share of
+// <p, z> (lanes over the column's segments in order, then the lane
+// butterfly) stored at its colour-loop position. FP64 (the form the kernel
+// runs): r64 = b - A64 x for slots taking a true residual. An item's packed
+// matrices are one
 // contiguous run, which lane 0 asks the L2 to fetch in bulk
 // (cp.async.bulk.prefetch) before the warp's first loads.
 template <int NDF, bool FP64>
@@ -384,163 +372,108 @@ __device__ __noinline__ void apply_phase(const BParams& P, const int4* __restric
   }
 }
 
-// ---- The FP32 apply with its inputs staged through shared memory.
-// A warp walks its items' cell-column segments (units) in order and keeps
-// the next unit's inputs in flight while it computes the current one: each
-// lane copies its level's packed matrix entries, x values and partial sums
-// of y with 4-byte cp.async into a two-stage per-warp buffer, so the bytes
-// in flight do not cost registers (the persistent kernel runs at 128
-// registers a thread, 16 warps an SM). A lane reads back only what it copied
-// itself. An item's cell descriptors are read into shared memory once.
-constexpr int kPipeCols = 8;  // cell columns per item, at most, in this path
-constexpr int kDescInts = 12;  // cell descriptor ints, at most
-
+// ---- The FP32 apply from the level-major triangles. One warp per item,
+// items' cell columns and each column's segments in order, as apply_phase;
+// lane l of segment sg holds level k = sg L + l - 1 and loads its level's
+// packed entries with npv 16-byte streaming loads (the warp's levels are one
+// contiguous run), then the x values and partial sums of y through L2. The
+// arithmetic is scatter_unit's (same terms, same order).
 template <int NDF>
-struct PipeShape {
-  static constexpr int NP = NDF * (NDF + 1) / 2;
-  static constexpr int STAGE = (NP + 2 * NDF) * 32;  // floats: M[p][lane], X[j][lane], Y[df][lane]
-  static constexpr int WARP_FLOATS = 2 * STAGE + kPipeCols * kDescInts;
-  static constexpr size_t BLOCK_BYTES = (size_t)kBW * WARP_FLOATS * 4;
-};
-
-__device__ __forceinline__ void cp4(float* dst, const float* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
-                   (unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
-
-template <int NDF>
-__device__ __noinline__ void apply_phase32_pipe(const BParams& P, const int4* __restrict__ items,
-                                                int i0, int i1, float* wsm) {
-  using S = PipeShape<NDF>;
-  constexpr int NP = S::NP;
+__device__ __noinline__ void apply_phase32_lm(const BParams& P, const int4* __restrict__ items,
+                                              int i0, int i1) {
+  constexpr int NP = NDF * (NDF + 1) / 2, NPV = (NP + 3) / 4;
   const int lane = threadIdx.x & 31;
   const int gw = blockIdx.x * kBW + (threadIdx.x >> 5), nw = gridDim.x * kBW;
-  float* st0 = wsm;
-  int* dsm = reinterpret_cast<int*>(wsm + 2 * S::STAGE);
   for (int u = i0 + gw; u < i1; u += nw) {
     const int4 it = __ldg(items + u);
     const int s = it.x;
     if (!ph_run(__ldcg(&P.st[s].phase))) continue;  // warp-uniform
-    const BSlot* D = P.slots + s;
-    const float* M = D->S32;
-    const int sblk = D->sblk32, cdints = D->cdints, nl = D->nl, nseg = D->nseg, L = D->segL;
-    const float* x = D->p;
-    float* y = D->z;
-    double* part = D->part + 2 * (int64_t)D->nch;
+    const BSlot& D = P.slots[s];
+    const float4* M4 = D.L32;
+    const int* cdesc = D.cdesc;
+    const int cdints = D.cdints, nl = D.nl, nseg = D.nseg, L = D.segL;
+    const float* x = D.p;
+    float* y = D.z;
+    double* part = D.part + 2 * (int64_t)D.nch;
     const int q0 = it.y, nq = it.z;
     if (lane == 0)
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(M + (size_t)q0 * sblk),
-                   "r"((unsigned)((size_t)nq * sblk * 4))
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(M4 + (size_t)q0 * nl * NPV),
+                   "r"((unsigned)((size_t)nq * nl * NPV * 16))
                    : "memory");
-    __syncwarp();
-    for (int i = lane; i < nq * cdints; i += 32) dsm[i] = __ldg(D->cdesc + (size_t)q0 * cdints + i);
-    __syncwarp();
-    // unit j = (column j / nseg, segment j % nseg)
-    const int nunit = nq * nseg;
-    auto issue = [&](int j) {
-      float* stg = st0 + (j & 1) * S::STAGE;
-      const int c = j / nseg, sg = j % nseg;
-      const int* dsc = dsm + c * cdints;
-      const uint32_t flags = (uint32_t)dsc[NDF];
-      const int k = sg * L + lane - 1;
-      const bool own = lane >= 1 && lane <= L;
-      const bool v = k >= 0 && k < nl && lane <= L;
-      if (v) {
-        const float* Mc = M + (size_t)(q0 + c) * sblk + k;
-#pragma unroll
-        for (int pp = 0; pp < NP; ++pp) cp4(stg + pp * 32 + lane, Mc + pp * nl);
-#pragma unroll
-        for (int jj = 0; jj < NDF; ++jj) cp4(stg + (NP + jj) * 32 + lane, x + dsc[jj] + k);
-      }
-#pragma unroll
-      for (int df = 0; df < NDF; ++df) {
-        const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
-        const bool opens = (flags >> df) & 1u;
-        const bool live = own && (lower ? k <= nl : v);
-        if (!upper && !opens && live) cp4(stg + (NP + NDF + df) * 32 + lane, y + dsc[df] + k);
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-    issue(0);
-    double dot = 0.0;
-    for (int j = 0; j < nunit; ++j) {
-      if (j + 1 < nunit)
-        issue(j + 1);
-      else
-        asm volatile("cp.async.commit_group;" ::: "memory");
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-      const float* stg = st0 + (j & 1) * S::STAGE;
-      const int c = j / nseg, sg = j % nseg;
-      const int* dsc = dsm + c * cdints;
+    for (int c = 0; c < nq; ++c) {
+      const int q = q0 + c;
+      const int* dsc = cdesc + (size_t)q * cdints;
       int mf[NDF];
 #pragma unroll
-      for (int jj = 0; jj < NDF; ++jj) mf[jj] = dsc[jj];
-      const uint32_t flags = (uint32_t)dsc[NDF], prt = (uint32_t)dsc[NDF + 1];
-      const int k = sg * L + lane - 1;
-      const bool own = lane >= 1 && lane <= L;
-      const bool v = k >= 0 && k < nl && lane <= L;
-      float m[NP], xv[NDF], yo[NDF];
+      for (int j = 0; j < NDF; ++j) mf[j] = __ldg(dsc + j);
+      const uint32_t flags = (uint32_t)__ldg(dsc + NDF), prt = (uint32_t)__ldg(dsc + NDF + 1);
+      double dot = 0.0;
+      for (int sg = 0; sg < nseg; ++sg) {
+        const int k = sg * L + lane - 1;
+        const bool own = lane >= 1 && lane <= L;
+        const bool v = k >= 0 && k < nl && lane <= L;
+        const float4* Mk = M4 + ((size_t)q * nl + (v ? k : 0)) * NPV;
+        float m[NPV * 4], xv[NDF], yo[NDF];
 #pragma unroll
-      for (int pp = 0; pp < NP; ++pp) m[pp] = v ? stg[pp * 32 + lane] : 0.f;
+        for (int pv = 0; pv < NPV; ++pv) {
+          const float4 t = v ? __ldcs(Mk + pv) : make_float4(0.f, 0.f, 0.f, 0.f);
+          m[4 * pv] = t.x; m[4 * pv + 1] = t.y; m[4 * pv + 2] = t.z; m[4 * pv + 3] = t.w;
+        }
 #pragma unroll
-      for (int jj = 0; jj < NDF; ++jj) xv[jj] = v ? stg[(NP + jj) * 32 + lane] : 0.f;
+        for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldcg(x + mf[j] + k) : 0.f;
 #pragma unroll
-      for (int df = 0; df < NDF; ++df) {
-        const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
-        const bool opens = (flags >> df) & 1u;
-        const bool live = own && (lower ? k <= nl : v);
-        yo[df] = (!upper && !opens && live) ? stg[(NP + NDF + df) * 32 + lane] : 0.f;
-      }
+        for (int df = 0; df < NDF; ++df) {
+          const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+          const bool opens = (flags >> df) & 1u;
+          const bool live = own && (lower ? k <= nl : v);
+          yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + k) : 0.f;
+        }
 #define MV(i, jx) m[pidx<NDF>(i, jx)]
 #pragma unroll
-      for (int df = 0; df < NDF; ++df) {
-        if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
-        const bool last = (flags >> (24 + df)) & 1u;
-        if ((flags >> (8 + df)) & 1u) {
-          const int bsel = (prt >> (4 * df)) & 15u;
+        for (int df = 0; df < NDF; ++df) {
+          if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
+          const bool last = (flags >> (24 + df)) & 1u;
+          if ((flags >> (8 + df)) & 1u) {
+            const int bsel = (prt >> (4 * df)) & 15u;
 #pragma unroll
-          for (int bb = df + 1; bb < NDF; ++bb) {
-            if (bb != bsel) continue;
-            float acc = yo[df];
+            for (int bb = df + 1; bb < NDF; ++bb) {
+              if (bb != bsel) continue;
+              float acc = yo[df];
 #pragma unroll
-            for (int jj = 0; jj < NDF; ++jj) {
-              const float mb = __shfl_up_sync(0xffffffffu, MV(bb, jj), 1);
-              const float xb = __shfl_up_sync(0xffffffffu, xv[jj], 1);
-              if (v) acc = fmaf(MV(df, jj), xv[jj], acc);
-              if (own && k >= 1 && k <= nl) acc = fmaf(mb, xb, acc);
-            }
-            if (own && k <= nl) {
-              const int row = mf[df] + k;
-              __stcg(y + row, acc);
-              if (last) {
-                const float pr = k < nl ? xv[df] : __ldcg(x + row);
-                dot = fma((double)pr, (double)acc, dot);
+              for (int jj = 0; jj < NDF; ++jj) {
+                const float mb = __shfl_up_sync(0xffffffffu, MV(bb, jj), 1);
+                const float xb = __shfl_up_sync(0xffffffffu, xv[jj], 1);
+                if (v) acc = fmaf(MV(df, jj), xv[jj], acc);
+                if (own && k >= 1 && k <= nl) acc = fmaf(mb, xb, acc);
+              }
+              if (own && k <= nl) {
+                const int row = mf[df] + k;
+                __stcg(y + row, acc);
+                if (last) {
+                  const float pr = k < nl ? xv[df] : __ldcg(x + row);
+                  dot = fma((double)pr, (double)acc, dot);
+                }
               }
             }
-          }
-        } else {
-          float acc = yo[df];
+          } else {
+            float acc = yo[df];
 #pragma unroll
-          for (int jj = 0; jj < NDF; ++jj) acc = fmaf(MV(df, jj), xv[jj], acc);
-          if (own && v) {
-            __stcg(y + mf[df] + k, acc);
-            if (last) dot = fma((double)xv[df], (double)acc, dot);
+            for (int jj = 0; jj < NDF; ++jj) acc = fmaf(MV(df, jj), xv[jj], acc);
+            if (own && v) {
+              __stcg(y + mf[df] + k, acc);
+              if (last) dot = fma((double)xv[df], (double)acc, dot);
+            }
           }
         }
-      }
 #undef MV
-      if (sg == nseg - 1) {
-        const double w = warp_butterfly(dot);
-        if (lane == 0) __stcg(part + q0 + c, w);
-        dot = 0.0;
       }
+      const double w = warp_butterfly(dot);
+      if (lane == 0) __stcg(part + q, w);
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    __syncwarp();
   }
 }
+
+constexpr int kItemCols = 8;  // cell columns per apply item, at most
 
 // alpha = rz / <p, z> for every running slot: one block per slot sums the
 // slot's per-column shares in a fixed order
@@ -564,69 +497,162 @@ __device__ __noinline__ void alpha_phase(const BParams& P, BShared& sh) {
   }
 }
 
-// Chunk phase: items (slot, chunk); ld/op as in chunk_kernel with the slot's
-// record and state; fin(state, tot) runs once per slot after all its chunks.
+// ---- Vector phases. An item is (slot, chunk of kBSub * RCHUNK = 16384
+// values). The block takes an item; each thread takes four consecutive
+// values per step (16-byte accesses, masked at the vector's end), with the
+// loads of two steps in flight before any store. The slot record is read
+// where it lies (read-only during a launch: broadcast loads); the state
+// words the elementwise work needs are read through L2 (written by other
+// blocks in earlier phases). A slot's item is skipped or taken by the whole
+// block alike: its state changes in this phase only in fin, which runs after
+// every item of the slot. Sums: FP64 per thread, then the block sum in a
+// fixed order (lanes by butterfly, warps left to right) into the chunk's
+// partial; the last block to finish a slot's chunks (ticket) sums the
+// partials in chunk order and runs fin(record, state, totals).
+constexpr int kVStep = kBT * 4;                   // values per block step
+constexpr int kVSteps = kBSub * RCHUNK / kVStep;  // steps per chunk (16)
+static_assert(kVSteps % 2 == 0, "two steps per pass");
+
+struct VState {
+  int phase, fresh;
+  float alpha, beta;
+};
+
+// four consecutive values from i (zeros past n); RO: read-only during the
+// launch (non-coherent cache), else read through L2
+template <bool RO>
+__device__ __forceinline__ float4 vld(const float* a, int64_t i, int64_t n) {
+  if (i + 3 < n)
+    return RO ? __ldg(reinterpret_cast<const float4*>(a + i))
+              : __ldcg(reinterpret_cast<const float4*>(a + i));
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (i < n) v.x = RO ? __ldg(a + i) : __ldcg(a + i);
+  if (i + 1 < n) v.y = RO ? __ldg(a + i + 1) : __ldcg(a + i + 1);
+  if (i + 2 < n) v.z = RO ? __ldg(a + i + 2) : __ldcg(a + i + 2);
+  return v;
+}
+__device__ __forceinline__ void vst(float* a, int64_t i, int64_t n, float4 v) {
+  if (i + 3 < n) {
+    __stcg(reinterpret_cast<float4*>(a + i), v);
+    return;
+  }
+  if (i < n) __stcg(a + i, v.x);
+  if (i + 1 < n) __stcg(a + i + 1, v.y);
+  if (i + 2 < n) __stcg(a + i + 2, v.z);
+}
+struct D4 {
+  double v[4];
+};
+struct DF4 {
+  D4 d;
+  float4 f;
+};
+template <bool RO>
+__device__ __forceinline__ D4 vldd(const double* a, int64_t i, int64_t n) {
+  D4 r;
+  if (i + 3 < n) {
+    const double2 lo = RO ? __ldg(reinterpret_cast<const double2*>(a + i))
+                          : __ldcg(reinterpret_cast<const double2*>(a + i));
+    const double2 hi = RO ? __ldg(reinterpret_cast<const double2*>(a + i + 2))
+                          : __ldcg(reinterpret_cast<const double2*>(a + i + 2));
+    r.v[0] = lo.x; r.v[1] = lo.y; r.v[2] = hi.x; r.v[3] = hi.y;
+    return r;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) r.v[c] = i + c < n ? (RO ? __ldg(a + i + c) : __ldcg(a + i + c)) : 0.0;
+  return r;
+}
+__device__ __forceinline__ void vstd(double* a, int64_t i, int64_t n, const D4& r) {
+  if (i + 3 < n) {
+    __stcg(reinterpret_cast<double2*>(a + i), make_double2(r.v[0], r.v[1]));
+    __stcg(reinterpret_cast<double2*>(a + i + 2), make_double2(r.v[2], r.v[3]));
+    return;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    if (i + c < n) __stcg(a + i + c, r.v[c]);
+}
+__device__ __forceinline__ void f4a(float4 v, float* o) {
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ float4 a4f(const float* o) { return make_float4(o[0], o[1], o[2], o[3]); }
+
+// ld(record, i, n) loads the four values at i; op(record, state, i, n,
+// values, acc) computes and stores them (components past n left alone)
 template <int NR, class Pred, class Ld, class Op, class Fin>
-__device__ __noinline__ void chunk_phase(const BParams& P, BShared& sh, Pred pred, Ld ld, Op op, Fin fin) {
+__device__ __noinline__ void vec_phase(const BParams& P, BShared& sh, Pred pred, Ld ld, Op op, Fin fin) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int u = blockIdx.x; u < P.nchunk; u += gridDim.x) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int2 w = __ldg(P.chunks + u);
-      sh.item = make_int4(w.x, w.y, 0, 0);
-      sh.skip = !pred(__ldcg(&P.st[w.x].phase), __ldcg(&P.st[w.x].flag));
-    }
-    __syncthreads();
-    if (sh.skip) continue;
-    const int s = sh.item.x, ch = sh.item.y;
-    load_item(P, sh, s);
-    __syncthreads();
-    const BSlot& D = sh.slot;
-    const BState& S = sh.state;
-    using V = decltype(ld(D, int64_t(0)));
+    const int2 item = __ldg(P.chunks + u);
+    const int s = item.x, ch = item.y;
+    const BState* Sg = P.st + s;
+    if (!pred(__ldcg(&Sg->phase), __ldcg(&Sg->flag))) continue;  // block-uniform
+    const BSlot& D = P.slots[s];
+    VState V;
+    V.phase = __ldcg(&Sg->phase);
+    V.fresh = __ldcg(&Sg->fresh);
+    V.alpha = (float)__ldcg(&Sg->alpha);
+    V.beta = (float)__ldcg(&Sg->beta);
+    const int64_t n = D.n;
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
-    for (int sub = 0; sub < kBSub; ++sub) {
-      const int64_t base = ((int64_t)ch * kBSub + sub) * RCHUNK + threadIdx.x;
-      if (base - threadIdx.x >= D.n) break;
-      V v[RPER];
-#pragma unroll
-      for (int m = 0; m < RPER; ++m) {
-        const int64_t i = base + (int64_t)m * RT;
-        if (i < D.n) v[m] = ld(D, i);
-      }
-#pragma unroll
-      for (int m = 0; m < RPER; ++m) {
-        const int64_t i = base + (int64_t)m * RT;
-        if (i < D.n) op(D, S, i, v[m], acc);
-      }
+    const int64_t c0 = (int64_t)ch * (kBSub * RCHUNK);
+    for (int stp = 0; stp < kVSteps; stp += 2) {
+      if (c0 + (int64_t)stp * kVStep >= n) break;  // block-uniform
+      const int64_t i0 = c0 + (int64_t)stp * kVStep + 4 * threadIdx.x, i1 = i0 + kVStep;
+      const auto a = ld(D, i0, n);
+      const auto b = ld(D, i1, n);
+      if (i0 < n) op(D, V, i0, n, a, acc);
+      if (i1 < n) op(D, V, i1, n, b, acc);
     }
     if constexpr (NR > 0) {
+      const int nch = D.nch;
+      double* part = D.part;
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const double t = bsum(acc[r], sh.red);
-        if (threadIdx.x == 0) __stcg(D.part + (int64_t)r * D.nch + ch, t);
+        const double t = warp_butterfly(acc[r]);
+        if (lane == 0) sh.red2[r][w] = t;
       }
-      __threadfence();
       __syncthreads();
-      if (threadIdx.x == 0) sh.last = (atomicAdd(&P.tickets[s], 1u) == (unsigned)D.nch - 1u);
+      if (threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          double t = sh.red2[r][0];
+#pragma unroll
+          for (int q = 1; q < kBW; ++q) t = t + sh.red2[r][q];
+          __stcg(part + (int64_t)r * nch + ch, t);
+        }
+        __threadfence();
+        sh.last = atomicAdd(&P.tickets[s], 1u) == (unsigned)nch - 1u;
+      }
       __syncthreads();
       if (sh.last) {
         __threadfence();
-        double tot[NR];
+        double a[NR];
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-          double a = 0.0;
-          for (int i = threadIdx.x; i < D.nch; i += kBT) a = a + __ldcg(&D.part[(int64_t)r * D.nch + i]);
-          tot[r] = bsum(a, sh.red);
+          a[r] = 0.0;
+          for (int i = threadIdx.x; i < nch; i += kBT) a[r] = a[r] + __ldcg(part + (int64_t)r * nch + i);
+          const double t = warp_butterfly(a[r]);
+          if (lane == 0) sh.red2[r][w] = t;
         }
+        __syncthreads();
         if (threadIdx.x == 0) {
+          double tot[NR];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            tot[r] = sh.red2[r][0];
+#pragma unroll
+            for (int q = 1; q < kBW; ++q) tot[r] = tot[r] + sh.red2[r][q];
+          }
           BState S;
           copy_state_in(&S, P.st + s);
           fin(D, S, tot);
           copy_state_out(P.st + s, S);
           P.tickets[s] = 0u;
         }
+        __syncthreads();
       }
     }
   }
@@ -749,11 +775,8 @@ template <class T> struct W5 { T a, b, c, d, e; };
 // The persistent kernel: `iters` super-iterations of every admitted slot.
 template <int NDF, bool CMA>
 __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict__ PP) {
-  // per warp: the two stages and the item descriptors of the FP32 apply
-  // (the column sweeps of phase C stage their rows in the same memory)
-  extern __shared__ __align__(16) float pipe_smem[];
-  static_assert(PipeShape<NDF>::BLOCK_BYTES >= sizeof(float) * kBRows * (kBCols + 1),
-                "the sweeps' staging fits the apply's shared memory");
+  // the column sweeps of phase C stage their rows here (sweep_bytes())
+  extern __shared__ __align__(16) float sweep_smem[];
   __shared__ BShared sh;
   __shared__ BParams sp;
   __shared__ SweepShared ss;
@@ -782,26 +805,34 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
     for (int g = 0; g < P.ngr32; ++g)
       for (int c = 0; c < P.ncolour; ++c) {
         const int o = g * P.ncolour + c;
-        apply_phase32_pipe<NDF>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1),
-                                pipe_smem + (threadIdx.x >> 5) * PipeShape<NDF>::WARP_FLOATS);
+        apply_phase32_lm<NDF>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1));
         if (!grid_sync(P, sh)) return;
       }
     alpha_phase(P, sh);
     if (!grid_sync(P, sh)) return;
     // ---- U: xc += alpha p, r -= alpha z, ||r||^2 (+ <r, r/d>, beta for Jacobi slots)
     int* need = P.need + it;
-    chunk_phase<2>(
+    vec_phase<2>(
         P, sh, [](int ph, int) { return ph_run(ph); },
-        [](const BSlot& D, int64_t i) {
-          return W5<float>{__ldcg(D.xc + i), __ldcg(D.p + i), __ldcg(D.r + i), __ldcg(D.z + i),
-                           D.cma ? 1.0f : __ldg(D.diag + i)};
+        [](const BSlot& D, int64_t i, int64_t n) {
+          return W5<float4>{vld<false>(D.xc, i, n), vld<false>(D.p, i, n), vld<false>(D.r, i, n),
+                            vld<false>(D.z, i, n),
+                            D.cma ? make_float4(1.f, 1.f, 1.f, 1.f) : vld<true>(D.diag, i, n)};
         },
-        [](const BSlot& D, const BState& S, int64_t i, const W5<float>& v, double* a) {
-          __stcg(D.xc + i, fmaf((float)S.alpha, v.b, v.a));
-          const float ri = fmaf((float)(-S.alpha), v.d, v.c);
-          __stcg(D.r + i, ri);
-          a[0] = fma((double)ri, (double)ri, a[0]);
-          if (!D.cma) a[1] = fma((double)ri, (double)(ri / v.e), a[1]);
+        [](const BSlot& D, const VState& S, int64_t i, int64_t n, const W5<float4>& v, double* a) {
+          float xc[4], p[4], r[4], z[4], d[4];
+          f4a(v.a, xc); f4a(v.b, p); f4a(v.c, r); f4a(v.d, z); f4a(v.e, d);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            xc[c] = fmaf(S.alpha, p[c], xc[c]);
+            r[c] = fmaf(-S.alpha, z[c], r[c]);
+            if (i + c < n) {
+              a[0] = fma((double)r[c], (double)r[c], a[0]);
+              if (!D.cma) a[1] = fma((double)r[c], (double)(r[c] / d[c]), a[1]);
+            }
+          }
+          vst(D.xc, i, n, a4f(xc));
+          vst(D.r, i, n, a4f(r));
         },
         [need](const BSlot& D, BState& S, const double* t) {
           S.iter += 1;
@@ -819,12 +850,21 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
     // ---- R: reliable update and FP64 true residual
     if (__ldcg(need)) {
       auto resid = [](int ph, int fl) { return ph == PH_INIT || (ph == PH_RUN && fl); };
-      chunk_phase<0>(
+      vec_phase<0>(
           P, sh, resid,
-          [](const BSlot& D, int64_t i) { return V2<double>{__ldcg(D.x + i), (double)__ldcg(D.xc + i)}; },
-          [](const BSlot& D, const BState& S, int64_t i, const V2<double>& v, double*) {
-            if (S.phase != PH_INIT) __stcg(D.x + i, v.a + v.b);
-            __stcg(D.xc + i, 0.0f);
+          [](const BSlot& D, int64_t i, int64_t n) {
+            return DF4{vldd<false>(D.x, i, n), vld<false>(D.xc, i, n)};
+          },
+          [](const BSlot& D, const VState& S, int64_t i, int64_t n, const DF4& v, double*) {
+            if (S.phase != PH_INIT) {
+              float xc[4];
+              f4a(v.f, xc);
+              D4 x = v.d;
+#pragma unroll
+              for (int c = 0; c < 4; ++c) x.v[c] = x.v[c] + (double)xc[c];
+              vstd(D.x, i, n, x);
+            }
+            vst(D.xc, i, n, make_float4(0.f, 0.f, 0.f, 0.f));
           },
           [](const BSlot&, BState&, const double*) {});
       if (!grid_sync(P, sh)) return;
@@ -834,14 +874,23 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
           apply_phase<NDF, true>(P, P.items64, __ldg(P.off64 + o), __ldg(P.off64 + o + 1));
           if (!grid_sync(P, sh)) return;
         }
-      chunk_phase<2>(
+      vec_phase<2>(
           P, sh, resid,
-          [](const BSlot& D, int64_t i) { return V2<double>{__ldcg(D.r64 + i), (double)__ldg(D.diag + i)}; },
-          [](const BSlot& D, const BState&, int64_t i, const V2<double>& v, double* a) {
-            const float ri = (float)v.a;
-            __stcg(D.r + i, ri);
-            a[0] = fma(v.a, v.a, a[0]);
-            if (!D.cma) a[1] = fma((double)ri, (double)(ri / (float)v.b), a[1]);
+          [](const BSlot& D, int64_t i, int64_t n) {
+            return DF4{vldd<false>(D.r64, i, n), vld<true>(D.diag, i, n)};
+          },
+          [](const BSlot& D, const VState&, int64_t i, int64_t n, const DF4& v, double* a) {
+            float d[4], r[4];
+            f4a(v.f, d);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              r[c] = (float)v.d.v[c];
+              if (i + c < n) {
+                a[0] = fma(v.d.v[c], v.d.v[c], a[0]);
+                if (!D.cma) a[1] = fma((double)r[c], (double)(r[c] / d[c]), a[1]);
+              }
+            }
+            vst(D.r, i, n, a4f(r));
           },
           [](const BSlot& D, BState& S, const double* t) {
             const double nr = sqrt(t[0]);
@@ -880,23 +929,30 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
     }
     // ---- C: column sweeps, then the Jacobi rows with <r, z> and beta
     if (CMA && P.any_cma) {
-      sweep_phase(P, pipe_smem, ss);
+      sweep_phase(P, sweep_smem, ss);
       if (!grid_sync(P, sh)) return;
-      chunk_phase<1>(
+      vec_phase<1>(
           P, sh, [](int ph, int) { return ph_run(ph); },
-          [](const BSlot& D, int64_t i) {
-            return V3<float>{__ldcg(D.r + i), D.cma ? __ldg(D.diag + i) : 1.0f, D.cma ? __ldcg(D.z + i) : 0.0f};
+          [](const BSlot& D, int64_t i, int64_t n) {
+            if (!D.cma) return V3<float4>{};
+            return V3<float4>{vld<false>(D.r, i, n), vld<true>(D.diag, i, n), vld<false>(D.z, i, n)};
           },
-          [](const BSlot& D, const BState&, int64_t i, const V3<float>& v, double* a) {
+          [](const BSlot& D, const VState&, int64_t i, int64_t n, const V3<float4>& v, double* a) {
             if (!D.cma) return;
             // rows with a non-zero diagonal are Jacobi rows; the column rows
             // (written by the sweeps) carry a zero in the Jacobi diagonal
-            float zi = v.c;
-            if (v.b != 0.0f) {
-              zi = v.a / v.b;
-              __stcg(D.z + i, zi);
+            float r[4], d[4], z[4];
+            f4a(v.a, r); f4a(v.b, d); f4a(v.c, z);
+            bool jac = false;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              if (d[c] != 0.0f) {
+                z[c] = r[c] / d[c];
+                jac = true;
+              }
+              if (i + c < n) a[0] = fma((double)r[c], (double)z[c], a[0]);
             }
-            a[0] = fma((double)v.a, (double)zi, a[0]);
+            if (jac) vst(D.z, i, n, a4f(z));
           },
           [](const BSlot& D, BState& S, const double* t) {
             if (!D.cma) return;
@@ -906,15 +962,21 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
       if (!grid_sync(P, sh)) return;
     }
     // ---- P: p = z + beta p (p = z for a slot that just started)
-    chunk_phase<0>(
+    vec_phase<0>(
         P, sh, [](int ph, int) { return ph_run(ph); },
-        [](const BSlot& D, int64_t i) {
-          return V3<float>{__ldcg(D.p + i), D.cma ? __ldcg(D.z + i) : __ldcg(D.r + i),
-                           D.cma ? 1.0f : __ldg(D.diag + i)};
+        [](const BSlot& D, int64_t i, int64_t n) {
+          return V3<float4>{vld<false>(D.p, i, n), D.cma ? vld<false>(D.z, i, n) : vld<false>(D.r, i, n),
+                            D.cma ? make_float4(1.f, 1.f, 1.f, 1.f) : vld<true>(D.diag, i, n)};
         },
-        [](const BSlot& D, const BState& S, int64_t i, const V3<float>& v, double*) {
-          const float zi = D.cma ? v.b : v.b / v.c;
-          __stcg(D.p + i, S.fresh ? zi : fmaf((float)S.beta, v.a, zi));
+        [](const BSlot& D, const VState& S, int64_t i, int64_t n, const V3<float4>& v, double*) {
+          float p[4], zr[4], d[4];
+          f4a(v.a, p); f4a(v.b, zr); f4a(v.c, d);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const float zi = D.cma ? zr[c] : zr[c] / d[c];
+            p[c] = S.fresh ? zi : fmaf(S.beta, p[c], zi);
+          }
+          vst(D.p, i, n, a4f(p));
         },
         [](const BSlot&, BState&, const double*) {});
     if (!grid_sync(P, sh)) return;
@@ -999,9 +1061,7 @@ int upload(lfx_ctx* ctx, T* dst, const std::vector<T>& src) {
   return LFX_OK;
 }
 
-size_t pipe_bytes(int ndf) {
-  return ndf == 8 ? PipeShape<8>::BLOCK_BYTES : PipeShape<6>::BLOCK_BYTES;
-}
+size_t sweep_bytes() { return sizeof(float) * kBRows * (kBCols + 1); }
 
 const void* pick_kernel(int ndf, bool cma) {
   if (ndf == 8) return cma ? kernel_ptr<8, true>() : kernel_ptr<8, false>();
@@ -1128,7 +1188,7 @@ int graph_for(lfx_batch* B, int bps, cudaGraphExec_t* out) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(ctx->num_sms * bps));
   cfg.blockDim = dim3(kBT);
-  cfg.dynamicSmemBytes = pipe_bytes(B->ndf);
+  cfg.dynamicSmemBytes = sweep_bytes();
   cfg.stream = ctx->stream;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeCooperative;
@@ -1272,9 +1332,9 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t reser
     // the device says so
     int per_sm = 0;
     cudaFuncSetAttribute(pick_kernel(ndf, ndf == 6), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pipe_bytes(ndf));
+                         (int)sweep_bytes());
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(ndf, ndf == 6), kBT,
-                                                  pipe_bytes(ndf));
+                                                  sweep_bytes());
     B->max_bps = std::max(1, std::min(per_sm, 2));
     B->blocks_per_sm = B->max_bps;
     B->group_bytes = ctx->l2_bytes / 2;
@@ -1337,8 +1397,6 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   const int nseg = (nl + 1 + 30) / 31;
   if (nseg > kMaxSeg)
     return fail(ctx, LFX_NOT_SUPPORTED, "batch: at most 123 levels per column");
-  if (L->cs_ints > kDescInts)
-    return fail(ctx, LFX_NOT_SUPPORTED, "batch: cell descriptors of at most 12 ints");
   const bool cma = prec32->kind == PREC_CMA;
   if (prec32->precision != LFX_R32 || (prec32->kind != PREC_DIAG && !cma) || !prec32->rdiag ||
       prec32->rdiag_n != L->undf_to || (cma && !prec32->jacobi_zeroed))
@@ -1363,10 +1421,14 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
     return fail(ctx, LFX_NOT_SUPPORTED, "batch: at most 8 cell colours");
   // admission by free device memory: the slot's state, its share of the
   // work lists, and the batch's reserve must fit
-  const int64_t need = slot_bytes(n, nch, L->ncell_2d);
+  const int64_t need = slot_bytes(n, nch, L->ncell_2d) + (int64_t)(op32->lmat ? 0 : op_level_major_bytes(op32));
   const int64_t lists = 16 * (2 * ((int64_t)L->ncell_2d / 32 + 8) + nch) + 8 * (cma ? prec32->ncell_2d : 0);
   if (available_bytes(ctx) - need - 2 * lists < B->reserve)
     return fail(ctx, LFX_OUT_OF_MEMORY, "batch: not enough free device memory for the solve");
+  {
+    const int rcl = op_level_major(op32);
+    if (rcl) return rcl;
+  }
   SlotHost& H = B->slots[s];
   H = SlotHost();
   void* mem = nullptr;
@@ -1390,6 +1452,8 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   BSlot D{};
   D.S32 = (const float*)op32->smat;
   D.S64 = (const double*)op64->smat;
+  D.L32 = (const float4*)op32->lmat;
+  D.npv = op32->lnpv;
   D.cdesc = L->cs_desc;
   D.sblk32 = op32->sblk;
   D.sblk64 = op64->sblk;
@@ -1527,7 +1591,7 @@ int lfx_batch_get_tuning(const lfx_batch* B, lfx_batch_tuning* t) {
 int lfx_batch_set_tuning(lfx_batch* B, int32_t cells_per_item, int32_t blocks_per_sm,
                          int64_t group_bytes) {
   if (!B) return LFX_INVALID_ARGUMENT;
-  if (cells_per_item < 1 || cells_per_item > kPipeCols ||
+  if (cells_per_item < 1 || cells_per_item > kItemCols ||
       blocks_per_sm < 1 || blocks_per_sm > B->max_bps || group_bytes < 1)
     return fail(B->ctx, LFX_INVALID_ARGUMENT, "batch tuning out of range");
   B->cells_per_item = cells_per_item;

@@ -346,6 +346,13 @@ struct lfx_op {
   void* smat = nullptr;
   size_t smat_bytes = 0;
   int32_t sblk = 0;
+  // FP32 only, made on first use by the batch engine: the same upper
+  // triangles level-major, [q][k][p] with each level's entries padded to a
+  // multiple of four (lnpv float4 per level), so a lane loads its level with
+  // 16-byte loads and a warp's levels are one contiguous run
+  void* lmat = nullptr;
+  size_t lmat_bytes = 0;
+  int32_t lnpv = 0;
 };
 
 struct lfx_cma {
@@ -386,6 +393,11 @@ struct lfx_prec {
 
 namespace lfx {
 int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* skip);
+// bytes of the level-major copy an FP32 operator with a packed copy would
+// take, and its creation (a no-op when it exists); both LFX_NOT_SUPPORTED
+// without an FP32 packed copy
+size_t op_level_major_bytes(const lfx_op* op);
+int op_level_major(lfx_op* op);
 // flexible GMRES / GCR over the C ABI's vector calls (lfx_solver_flex.cu);
 // work: FGMRES s, w, dx, Ax, res, v[gcrk], Pv[gcrk]; GCR dx, res, Ax, v, Pv
 int fgmres_host(lfx_op* op, lfx_prec* prec, const lfx_solver_cfg& cfg,

@@ -1075,6 +1075,22 @@ __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, co
   cp_async_wait<0>();
 }
 
+// level-major copy of the FP32 packed triangles: dst[(q nl + k) 4 npv + p]
+// = src[q sblk + p nl + k], zero in the padding p >= np
+__global__ void relayout_level_major(const float* __restrict__ src, float* __restrict__ dst,
+                                     int64_t ncol, int nl, int np, int npv, int sblk) {
+  const int w = 4 * npv;
+  const int64_t total = ncol * nl * w;
+  for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < total;
+       d += (int64_t)gridDim.x * blockDim.x) {
+    const int p = (int)(d % w);
+    const int64_t qk = d / w;
+    const int k = (int)(qk % nl);
+    const int64_t q = qk / nl;
+    dst[d] = p < np ? src[q * sblk + (int64_t)p * nl + k] : 0.f;
+  }
+}
+
 // packed upper triangle [q][p][k] (block stride sblk; block q holds the q-th
 // cell of the colour loop, order[q]) from the Fortran (nc3, ndf, ndf) FP64
 // stencil
@@ -1821,6 +1837,33 @@ int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* 
   return LFX_OK;
 }
 
+size_t op_level_major_bytes(const lfx_op* op) {
+  if (op->precision != LFX_R32 || !op->smat) return 0;
+  const int np = op->lay->ndf_to * (op->lay->ndf_to + 1) / 2;
+  return (size_t)op->lay->ncell_2d * op->lay->nlayers * ((np + 3) / 4) * 16;
+}
+
+int op_level_major(lfx_op* op) {
+  lfx_ctx* ctx = op->ctx;
+  if (op->precision != LFX_R32 || !op->smat)
+    return fail(ctx, LFX_NOT_SUPPORTED, "level-major copy: FP32 operators with a packed copy only");
+  if (op->lmat) return LFX_OK;
+  const lfx_lma_layout* L = op->lay;
+  const int np = L->ndf_to * (L->ndf_to + 1) / 2;
+  const size_t bytes = op_level_major_bytes(op);
+  int rc = dmalloc(ctx, &op->lmat, bytes);
+  if (rc) return rc;
+  op->lmat_bytes = bytes;
+  op->lnpv = (np + 3) / 4;
+  const int64_t total = (int64_t)(bytes / 4);
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 16);
+  relayout_level_major<<<grid, 256, 0, ctx->stream>>>((const float*)op->smat, (float*)op->lmat,
+                                                      L->ncell_2d, L->nlayers, np, op->lnpv,
+                                                      op->sblk);
+  LFX_CK(ctx, cudaGetLastError());
+  return LFX_OK;
+}
+
 }  // namespace lfx
 
 // out = fma(a, y, x) elementwise: operator_x_plus_ay on the stored copies
@@ -1985,6 +2028,7 @@ int lfx_op_destroy(lfx_op* op) {
   lfx_ctx* ctx = op->ctx;
   dfree(ctx, op->mat, op->mat_bytes);
   dfree(ctx, op->smat, op->smat_bytes);
+  dfree(ctx, op->lmat, op->lmat_bytes);
   if (op->lay && --op->lay->refcount == 0) free_layout(ctx, op->lay);
   delete op;
   return LFX_OK;

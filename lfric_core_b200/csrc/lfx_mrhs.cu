@@ -986,15 +986,19 @@ __global__ void __launch_bounds__(256) bcg_mask(int64_t n, float* R, const int* 
 //   right-hand side has rn <= tol r0); beta = -(P^T Q)^-1 Q^T D^-1 R
 // mode 2 (orth): pivoted Cholesky of W^T W -> rank and T (P = W T)
 // mode 3 (norms of the initial residual into r0)
-constexpr size_t kBcgSmallSmem = 2 * sizeof(double) * kBS * (kBS + 1);
+// The kernel's whole shared state is one dynamic buffer laid out here (no
+// static shared variables beside it): two 64 x 65 FP64 matrices, then the
+// pivot order and two flags.
+constexpr size_t kBcgMatBytes = sizeof(double) * kBS * (kBS + 1);
+constexpr size_t kBcgSmallSmem = 2 * kBcgMatBytes + sizeof(int) * (kBS + 4);
 
 __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double tol) {
-  // two 64 x 65 FP64 matrices in dynamic shared memory (kBcgSmallSmem)
-  extern __shared__ double bcg_dyn[];
+  extern __shared__ __align__(16) unsigned char bcg_dyn[];
   double (*M)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn);
-  double (*Bm)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn + kBS * (kBS + 1));
-  __shared__ int perm[kBS];
-  __shared__ int s_r, s_stop;
+  double (*Bm)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn + kBcgMatBytes);
+  int* perm = reinterpret_cast<int*>(bcg_dyn + 2 * kBcgMatBytes);
+  int& s_r = perm[kBS];
+  int& s_stop = perm[kBS + 1];
   const int t = threadIdx.x;
   if (st->done) return;
   if (mode == 3) {
@@ -1074,7 +1078,13 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
     return;
   }
   // mode 2: pivoted Cholesky of G = W^T W, stopping at pivots below
-  // kBcgDrop times the largest diagonal entry
+  // kBcgDrop times the largest diagonal entry. The pivoting is by index:
+  // rows and columns stay where they are and perm[i] names the row of step
+  // i, so L[i][j] = M[perm[i]][perm[j]] (i >= j) once the loop is done. (A
+  // form that swapped rows and columns in place, in one thread inside the
+  // loop over steps, lost the pivot's square root on the B200 while the same
+  // statements with a constant step index did not; the index form has no
+  // such swaps.)
   for (int e = t; e < kBS * kBS; e += blockDim.x) M[e / kBS][e % kBS] = st->G[e];
   if (t < kBS) perm[t] = t;
   if (t == 0) s_r = 0;
@@ -1085,39 +1095,41 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
     if (t == 0) {
       int p = k;
       for (int i = k + 1; i < kBS; ++i)
-        if (M[i][i] > M[p][p]) p = i;
-      s_stop = !(M[p][p] > kBcgDrop * dmax) || !(dmax > 0.0);
-      if (!s_stop && p != k) {
-        for (int j = 0; j < kBS; ++j) { const double tmp = M[k][j]; M[k][j] = M[p][j]; M[p][j] = tmp; }
-        for (int i = 0; i < kBS; ++i) { const double tmp = M[i][k]; M[i][k] = M[i][p]; M[i][p] = tmp; }
-        const int tp = perm[k]; perm[k] = perm[p]; perm[p] = tp;
-      }
-      if (!s_stop) {
-        M[k][k] = sqrt(M[k][k]);
+        if (M[perm[i]][perm[i]] > M[perm[p]][perm[p]]) p = i;
+      const int pk = perm[p];
+      const int stop = !(M[pk][pk] > kBcgDrop * dmax) || !(dmax > 0.0);
+      if (!stop) {
+        perm[p] = perm[k];
+        perm[k] = pk;
+        M[pk][pk] = sqrt(M[pk][pk]);
         s_r = k + 1;
       }
+      s_stop = stop;
     }
     __syncthreads();
     if (s_stop) break;
-    for (int i = k + 1 + t; i < kBS; i += blockDim.x) M[i][k] /= M[k][k];
+    const int pk = perm[k];
+    for (int i = k + 1 + t; i < kBS; i += blockDim.x) M[perm[i]][pk] /= M[pk][pk];
     __syncthreads();
     const int m = kBS - k - 1;
     for (int e = t; e < m * m; e += blockDim.x) {
-      const int i = k + 1 + e / m, j = k + 1 + e % m;
-      M[i][j] -= M[i][k] * M[j][k];
+      const int pi = perm[k + 1 + e / m], pj = perm[k + 1 + e % m];
+      M[pi][pj] -= M[pi][pk] * M[pj][pk];
     }
     __syncthreads();
   }
   const int r = s_r;
-  // Linv = L^-1 (r x r, lower): column j per thread
+  // Linv = L^-1 (r x r, lower; L[i][k] = M[perm[i]][perm[k]]): column j per
+  // thread
   if (t < r) {
     const int j = t;
     for (int i = 0; i < r; ++i) Bm[i][j] = 0.0;
-    Bm[j][j] = 1.0 / M[j][j];
+    Bm[j][j] = 1.0 / M[perm[j]][perm[j]];
     for (int i = j + 1; i < r; ++i) {
+      const int pi = perm[i];
       double v = 0.0;
-      for (int k = j; k < i; ++k) v -= M[i][k] * Bm[k][j];
-      Bm[i][j] = v / M[i][i];
+      for (int k = j; k < i; ++k) v -= M[pi][perm[k]] * Bm[k][j];
+      Bm[i][j] = v / M[pi][pi];
     }
   }
   __syncthreads();

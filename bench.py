@@ -375,11 +375,14 @@ def leg_multi_rhs(ctx, lfx, mg, wl, torch, stream, n=48, nl=30, nrhs=64):
     o = orc.LmaOperator(p.ncell_2d, nl, 8, 8, p.map, p.map, p.undf, p.undf, p.lma, npc, cic)
     x_or, _ = orc.solve("cg", o, orc.Preconditioner.diagonal(o.diagonal()), Bh[0], r_tol=RTOL,
                         a_tol=0.0, max_iter=20000)
-    runs = [(lfx.MRHS_TF32, "tf32", lfx.MRHS_PER_RHS_CG), (lfx.MRHS_BF16, "bf16", lfx.MRHS_PER_RHS_CG),
-            (lfx.MRHS_TF32, "tf32_block_cg", lfx.MRHS_BLOCK_CG),
-            (lfx.MRHS_BF16, "bf16_block_cg", lfx.MRHS_BLOCK_CG)]
-    for kind, name, method in runs:
+    runs = [(lfx.MRHS_TF32, "tf32", lfx.MRHS_PER_RHS_CG, False),
+            (lfx.MRHS_BF16, "bf16", lfx.MRHS_PER_RHS_CG, False),
+            (lfx.MRHS_TF32, "tf32_block_cg", lfx.MRHS_BLOCK_CG, False),
+            (lfx.MRHS_BF16, "bf16_block_cg", lfx.MRHS_BLOCK_CG, False),
+            (lfx.MRHS_BF16, "bf16_block_cg_tcgen05_gram", lfx.MRHS_BLOCK_CG, True)]
+    for kind, name, method, tc_gram in runs:
         M = lfx.MultiRhsOperator(s.op, kind, nrhs)
+        M.set_gram(tc_gram)
         inf = M.info()
         tune = M.autotune(10)
         torch.cuda.synchronize()
@@ -399,7 +402,8 @@ def leg_multi_rhs(ctx, lfx, mg, wl, torch, stream, n=48, nl=30, nrhs=64):
         X2 = x.cpu().numpy()
         err = [float(np.linalg.norm(X2[r] - x64[r]) / np.linalg.norm(x64[r])) for r in range(nrhs)]
         out[name] = {
-            "method": "block CG (one search space for the 64 right-hand sides)"
+            "method": ("block CG (one search space for the 64 right-hand sides)"
+                       + (", Gram products on tcgen05 (3xTF32)" if tc_gram else ""))
                       if method == lfx.MRHS_BLOCK_CG else "CG per right-hand side",
             "error_vs_fp64_oracle_rhs0": float(np.linalg.norm(X2[0] - x_or) / np.linalg.norm(x_or)),
             "solves_per_s": round(nrhs / t, 2), "s": round(t, 4),

@@ -64,6 +64,7 @@ enum { PH_EMPTY = 0, PH_INIT = 1, PH_RUN = 2, PH_DONE = 3 };
 constexpr double kDelta = 1e-3;  // reliable update when ||r|| drops by this factor
 constexpr int kBT = 256;         // threads per block of the persistent kernel
 constexpr int kBW = kBT / 32;    // warps per block
+constexpr int kMaxBps = 3;       // blocks per SM the kernel is built for (launch bounds)
 constexpr int kBSub = 8;         // a chunk item: kBSub chunks of RCHUNK values (16384)
 constexpr int kMaxIters = 64;    // super-iterations per launch, at most
 constexpr int kMaxSeg = 4;       // warps (segments of <= 31 levels) per cell column, at most
@@ -236,6 +237,26 @@ __host__ __device__ constexpr int pidx(int i, int j) {
   return i <= j ? i * N - i * (i - 1) / 2 + (j - i) : j * N - j * (j - 1) / 2 + (i - j);
 }
 
+// row and column (row <= column) of packed upper-triangle entry p
+template <int N>
+__host__ __device__ constexpr int prow(int p) {
+  int i = 0;
+  while (p >= N - i) {
+    p -= N - i;
+    ++i;
+  }
+  return i;
+}
+template <int N>
+__host__ __device__ constexpr int pcol(int p) {
+  int i = 0;
+  while (p >= N - i) {
+    p -= N - i;
+    ++i;
+  }
+  return i + p;
+}
+
 // One warp's share of the cell scatter: segment sg (L <= 31 output levels)
 // of the cell column at colour-loop position q. Lane l (1 <= l <= L) holds
 // level k = sg L + l - 1 and writes the dofs of that level (and the bottom
@@ -372,16 +393,110 @@ __device__ __noinline__ void apply_phase(const BParams& P, const int4* __restric
   }
 }
 
-// ---- The FP32 apply from the level-major triangles. One warp per item,
-// items' cell columns and each column's segments in order, as apply_phase;
-// lane l of segment sg holds level k = sg L + l - 1 and loads its level's
-// packed entries with npv 16-byte streaming loads (the warp's levels are one
-// contiguous run), then the x values and partial sums of y through L2. The
-// arithmetic is scatter_unit's (same terms, same order).
+// ---- The FP32 apply with each warp's matrix stream on the bulk-copy
+// engine. A warp walks its items' units (cell column, segment) in order; a
+// unit's levels are one contiguous run of the level-major copy, which lane 0
+// moves into the warp's ring in shared memory with one cp.async.bulk
+// completing on the stage's mbarrier, kRing units ahead, so the bytes in
+// flight cost no registers. The lanes gather x and the partial sums of y
+// through L2 before they wait for the unit's matrix, then read their level's
+// entries from the ring. Each lane forms the eight (six) row sums of its own
+// cell; a dof on a vertical pair (bottom of level k, top of level k - 1)
+// takes the row sum of the lane below with one shuffle, so the FP32 sums are
+// grouped per cell (the FP64 form keeps the reference's term order; the FP64
+// true residuals fix the accuracy of the solve). A wait is
+// bounded by the batch's wait limit: on a time-out the warp records
+// LFX_TIMEOUT, waits (bounded again) for the copies it still has in flight,
+// and returns; the kernel leaves at its next grid barrier.
+constexpr int kRing = 2;  // ring stages per warp
+
 template <int NDF>
-__device__ __noinline__ void apply_phase32_lm(const BParams& P, const int4* __restrict__ items,
-                                              int i0, int i1) {
-  constexpr int NP = NDF * (NDF + 1) / 2, NPV = (NP + 3) / 4;
+struct Ring {
+  static constexpr int NP = NDF * (NDF + 1) / 2, NPV = (NP + 3) / 4;
+  static constexpr int LEVEL = NPV * 16;           // bytes of one level
+  static constexpr int STAGE = 32 * LEVEL;         // a segment: at most 32 levels
+  static constexpr int WARP = kRing * STAGE;
+};
+
+// dynamic shared memory: the rings (or the sweeps' staging, which the
+// phases never hold at once), then kRing mbarriers per warp past both
+__host__ __device__ constexpr size_t ring_bar_offset(int ndf) {
+  return ((ndf == 8 ? (size_t)kBW * Ring<8>::WARP : (size_t)kBW * Ring<6>::WARP) >
+                  sizeof(float) * kBRows * (kBCols + 1)
+              ? (ndf == 8 ? (size_t)kBW * Ring<8>::WARP : (size_t)kBW * Ring<6>::WARP)
+              : sizeof(float) * kBRows * (kBCols + 1)) +
+         15 & ~(size_t)15;
+}
+__host__ __device__ constexpr size_t dyn_bytes(int ndf) {
+  return ring_bar_offset(ndf) + (size_t)kBW * kRing * 8;
+}
+
+__device__ __forceinline__ unsigned su32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ bool ring_try(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(su32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// waits for the phase of the given parity for at most limit ns
+__device__ __forceinline__ bool ring_wait(uint64_t* bar, unsigned parity,
+                                          unsigned long long limit) {
+  if (ring_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  while (!ring_try(bar, parity))
+    if (gtimer() - t0 > limit) return false;
+  return true;
+}
+__device__ __forceinline__ void ring_issue(void* dst, const void* src, unsigned bytes,
+                                           uint64_t* bar) {
+  // the stage was last read through the generic proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          su32(dst)),
+      "l"(src), "r"(bytes), "r"(su32(bar))
+      : "memory");
+}
+
+// row sums of a cell from its packed triangle, entry by entry with the
+// entry's (row, column) fixed at compile time: entry (a, b), a <= b, adds to
+// row a (times x_b) and, mirrored, to row b
+template <int NDF, int P>
+__device__ __forceinline__ void row_entry(float e, const float (&xv)[NDF], float (&rs)[NDF]) {
+  if constexpr (P < NDF * (NDF + 1) / 2) {
+    constexpr int a = prow<NDF>(P), b = pcol<NDF>(P);
+    rs[a] = fmaf(e, xv[b], rs[a]);
+    if constexpr (a != b) rs[b] = fmaf(e, xv[a], rs[b]);
+  }
+}
+template <int NDF, int PV>
+__device__ __forceinline__ void row_sums(const float4* Ms, bool v, const float (&xv)[NDF],
+                                         float (&rs)[NDF]) {
+  if constexpr (PV < Ring<NDF>::NPV) {
+    const float4 t = v ? Ms[PV] : make_float4(0.f, 0.f, 0.f, 0.f);
+    row_entry<NDF, 4 * PV>(t.x, xv, rs);
+    row_entry<NDF, 4 * PV + 1>(t.y, xv, rs);
+    row_entry<NDF, 4 * PV + 2>(t.z, xv, rs);
+    row_entry<NDF, 4 * PV + 3>(t.w, xv, rs);
+    row_sums<NDF, PV + 1>(Ms, v, xv, rs);
+  }
+}
+
+template <int NDF>
+__device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4* __restrict__ items,
+                                                    int i0, int i1, unsigned char* ring,
+                                                    uint64_t* bars, unsigned seq) {
+  using R = Ring<NDF>;
+  constexpr int NP = R::NP, NPV = R::NPV;
   const int lane = threadIdx.x & 31;
   const int gw = blockIdx.x * kBW + (threadIdx.x >> 5), nw = gridDim.x * kBW;
   for (int u = i0 + gw; u < i1; u += nw) {
@@ -395,82 +510,110 @@ __device__ __noinline__ void apply_phase32_lm(const BParams& P, const int4* __re
     const float* x = D.p;
     float* y = D.z;
     double* part = D.part + 2 * (int64_t)D.nch;
-    const int q0 = it.y, nq = it.z;
+    const int q0 = it.y, nq = it.z, nunit = nq * nseg;
+    // unit j: column j / nseg, segment j % nseg; its levels kf..kl land at
+    // ring slot (level - (sg L - 1)), so lane l finds level sg L + l - 1
+    auto issue = [&](int j) {
+      const int c = j / nseg, sg = j % nseg;
+      const int kf = max(sg * L - 1, 0), kl = min(sg * L + L - 1, nl - 1);
+      const unsigned st = (seq + (unsigned)j) % kRing;
+      ring_issue(ring + st * R::STAGE + (kf - (sg * L - 1)) * R::LEVEL,
+                 M4 + ((size_t)(q0 + c) * nl + kf) * NPV, (unsigned)(kl - kf + 1) * R::LEVEL,
+                 bars + st);
+    };
     if (lane == 0)
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(M4 + (size_t)q0 * nl * NPV),
-                   "r"((unsigned)((size_t)nq * nl * NPV * 16))
-                   : "memory");
-    for (int c = 0; c < nq; ++c) {
-      const int q = q0 + c;
-      const int* dsc = cdesc + (size_t)q * cdints;
-      int mf[NDF];
+      for (int j = 0; j < kRing && j < nunit; ++j) issue(j);
+    int mf[NDF];
+    uint32_t flags = 0, prt = 0;
+    double dot = 0.0;
+    bool ok = true;
+    for (int j = 0; j < nunit; ++j) {
+      const int c = j / nseg, sg = j % nseg;
+      if (sg == 0) {
+        const int* dsc = cdesc + (size_t)(q0 + c) * cdints;
 #pragma unroll
-      for (int j = 0; j < NDF; ++j) mf[j] = __ldg(dsc + j);
-      const uint32_t flags = (uint32_t)__ldg(dsc + NDF), prt = (uint32_t)__ldg(dsc + NDF + 1);
-      double dot = 0.0;
-      for (int sg = 0; sg < nseg; ++sg) {
-        const int k = sg * L + lane - 1;
-        const bool own = lane >= 1 && lane <= L;
-        const bool v = k >= 0 && k < nl && lane <= L;
-        const float4* Mk = M4 + ((size_t)q * nl + (v ? k : 0)) * NPV;
-        float m[NPV * 4], xv[NDF], yo[NDF];
+        for (int jj = 0; jj < NDF; ++jj) mf[jj] = __ldg(dsc + jj);
+        flags = (uint32_t)__ldg(dsc + NDF);
+        prt = (uint32_t)__ldg(dsc + NDF + 1);
+      }
+      const int k = sg * L + lane - 1;
+      const bool own = lane >= 1 && lane <= L;
+      const bool v = k >= 0 && k < nl && lane <= L;
+      float xv[NDF], yo[NDF];
 #pragma unroll
-        for (int pv = 0; pv < NPV; ++pv) {
-          const float4 t = v ? __ldcs(Mk + pv) : make_float4(0.f, 0.f, 0.f, 0.f);
-          m[4 * pv] = t.x; m[4 * pv + 1] = t.y; m[4 * pv + 2] = t.z; m[4 * pv + 3] = t.w;
-        }
+      for (int jj = 0; jj < NDF; ++jj) xv[jj] = v ? __ldcg(x + mf[jj] + k) : 0.f;
 #pragma unroll
-        for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldcg(x + mf[j] + k) : 0.f;
+      for (int df = 0; df < NDF; ++df) {
+        const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+        const bool opens = (flags >> df) & 1u;
+        const bool live = own && (lower ? k <= nl : v);
+        yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + k) : 0.f;
+      }
+      const unsigned g = seq + (unsigned)j, st = g % kRing;
+      if (!ring_wait(bars + st, (g / kRing) & 1u, P.timeout_ns)) {
+        ok = false;
+        break;
+      }
+      // row sums of this lane's cell, four packed entries at a time: entry
+      // (a, b), a <= b, adds to row a (times x_b) and, mirrored, to row b
+      float rs[NDF];
 #pragma unroll
-        for (int df = 0; df < NDF; ++df) {
-          const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
-          const bool opens = (flags >> df) & 1u;
-          const bool live = own && (lower ? k <= nl : v);
-          yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + k) : 0.f;
-        }
-#define MV(i, jx) m[pidx<NDF>(i, jx)]
+      for (int df = 0; df < NDF; ++df) rs[df] = 0.f;
+      row_sums<NDF, 0>(reinterpret_cast<const float4*>(ring + st * R::STAGE) + lane * NPV, v, xv, rs);
+      // every lane has read the stage: it takes unit j + kRing
+      __syncwarp();
+      if (lane == 0 && j + kRing < nunit) issue(j + kRing);
 #pragma unroll
-        for (int df = 0; df < NDF; ++df) {
-          if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
-          const bool last = (flags >> (24 + df)) & 1u;
-          if ((flags >> (8 + df)) & 1u) {
-            const int bsel = (prt >> (4 * df)) & 15u;
+      for (int df = 0; df < NDF; ++df) {
+        if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
+        const bool last = (flags >> (24 + df)) & 1u;
+        if ((flags >> (8 + df)) & 1u) {
+          const int bsel = (prt >> (4 * df)) & 15u;
 #pragma unroll
-            for (int bb = df + 1; bb < NDF; ++bb) {
-              if (bb != bsel) continue;
-              float acc = yo[df];
-#pragma unroll
-              for (int jj = 0; jj < NDF; ++jj) {
-                const float mb = __shfl_up_sync(0xffffffffu, MV(bb, jj), 1);
-                const float xb = __shfl_up_sync(0xffffffffu, xv[jj], 1);
-                if (v) acc = fmaf(MV(df, jj), xv[jj], acc);
-                if (own && k >= 1 && k <= nl) acc = fmaf(mb, xb, acc);
+          for (int bb = df + 1; bb < NDF; ++bb) {
+            if (bb != bsel) continue;
+            const float below = __shfl_up_sync(0xffffffffu, rs[bb], 1);
+            float acc = yo[df] + rs[df];
+            if (own && k >= 1 && k <= nl) acc = acc + below;
+            if (own && k <= nl) {
+              const int row = mf[df] + k;
+              __stcg(y + row, acc);
+              if (last) {
+                const float pr = k < nl ? xv[df] : __ldcg(x + row);
+                dot = fma((double)pr, (double)acc, dot);
               }
-              if (own && k <= nl) {
-                const int row = mf[df] + k;
-                __stcg(y + row, acc);
-                if (last) {
-                  const float pr = k < nl ? xv[df] : __ldcg(x + row);
-                  dot = fma((double)pr, (double)acc, dot);
-                }
-              }
-            }
-          } else {
-            float acc = yo[df];
-#pragma unroll
-            for (int jj = 0; jj < NDF; ++jj) acc = fmaf(MV(df, jj), xv[jj], acc);
-            if (own && v) {
-              __stcg(y + mf[df] + k, acc);
-              if (last) dot = fma((double)xv[df], (double)acc, dot);
             }
           }
+        } else {
+          const float acc = yo[df] + rs[df];
+          if (own && v) {
+            __stcg(y + mf[df] + k, acc);
+            if (last) dot = fma((double)xv[df], (double)acc, dot);
+          }
         }
-#undef MV
       }
-      const double w = warp_butterfly(dot);
-      if (lane == 0) __stcg(part + q, w);
+      if (sg == nseg - 1) {
+        const double w = warp_butterfly(dot);
+        if (lane == 0) __stcg(part + q0 + c, w);
+        dot = 0.0;
+      }
     }
+    if (!ok) {
+      // record the time-out, then wait (bounded) for this warp's copies
+      // still in flight before the kernel leaves
+      if (lane == 0) {
+        atomicExch(P.err, (int)LFX_TIMEOUT);
+        for (int j = 0; j < nunit && j < kRing; ++j) {
+          const unsigned g = seq + (unsigned)j;
+          ring_wait(bars + g % kRing, (g / kRing) & 1u, P.timeout_ns);
+        }
+      }
+      __syncwarp();
+      return seq;
+    }
+    seq += (unsigned)nunit;
   }
+  return seq;
 }
 
 constexpr int kItemCols = 8;  // cell columns per apply item, at most
@@ -774,9 +917,20 @@ template <class T> struct W5 { T a, b, c, d, e; };
 
 // The persistent kernel: `iters` super-iterations of every admitted slot.
 template <int NDF, bool CMA>
-__global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict__ PP) {
-  // the column sweeps of phase C stage their rows here (sweep_bytes())
-  extern __shared__ __align__(16) float sweep_smem[];
+__global__ void __launch_bounds__(kBT, kMaxBps) batch_kernel(const BParams* __restrict__ PP) {
+  // the apply rings, or the column sweeps' staging, then the ring mbarriers
+  // (dyn_bytes(NDF))
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  float* sweep_smem = reinterpret_cast<float*>(dyn_smem);
+  unsigned char* ring = dyn_smem + (size_t)(threadIdx.x >> 5) * Ring<NDF>::WARP;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(dyn_smem + ring_bar_offset(NDF)) +
+                   (threadIdx.x >> 5) * kRing;
+  if ((threadIdx.x & 31) == 0) {
+    for (int i = 0; i < kRing; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(bars + i)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  unsigned seq = 0;  // ring units this warp has issued (and consumed)
   __shared__ BShared sh;
   __shared__ BParams sp;
   __shared__ SweepShared ss;
@@ -805,7 +959,8 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BParams* __restrict
     for (int g = 0; g < P.ngr32; ++g)
       for (int c = 0; c < P.ncolour; ++c) {
         const int o = g * P.ncolour + c;
-        apply_phase32_lm<NDF>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1));
+        seq = apply_phase32_ring<NDF>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1),
+                                      ring, bars, seq);
         if (!grid_sync(P, sh)) return;
       }
     alpha_phase(P, sh);
@@ -1061,7 +1216,6 @@ int upload(lfx_ctx* ctx, T* dst, const std::vector<T>& src) {
   return LFX_OK;
 }
 
-size_t sweep_bytes() { return sizeof(float) * kBRows * (kBCols + 1); }
 
 const void* pick_kernel(int ndf, bool cma) {
   if (ndf == 8) return cma ? kernel_ptr<8, true>() : kernel_ptr<8, false>();
@@ -1188,7 +1342,7 @@ int graph_for(lfx_batch* B, int bps, cudaGraphExec_t* out) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(ctx->num_sms * bps));
   cfg.blockDim = dim3(kBT);
-  cfg.dynamicSmemBytes = sweep_bytes();
+  cfg.dynamicSmemBytes = dyn_bytes(B->ndf);
   cfg.stream = ctx->stream;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeCooperative;
@@ -1328,14 +1482,15 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t reser
       uint64_t thr = UINT64_MAX;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
-    // the kernel holds at most two blocks per SM (launch bounds); fewer if
-    // the device says so
+    // the kernel holds at most kMaxBps blocks per SM (launch bounds); fewer
+    // if the device says so
     int per_sm = 0;
-    cudaFuncSetAttribute(pick_kernel(ndf, ndf == 6), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sweep_bytes());
+    for (int cma = 0; cma < 2; ++cma)
+      cudaFuncSetAttribute(pick_kernel(ndf, cma != 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)dyn_bytes(ndf));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(ndf, ndf == 6), kBT,
-                                                  sweep_bytes());
-    B->max_bps = std::max(1, std::min(per_sm, 2));
+                                                  dyn_bytes(ndf));
+    B->max_bps = std::max(1, std::min(per_sm, kMaxBps));
     B->blocks_per_sm = B->max_bps;
     B->group_bytes = ctx->l2_bytes / 2;
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = LFX_CUDA_ERROR;

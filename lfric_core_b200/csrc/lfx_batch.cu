@@ -71,6 +71,13 @@ constexpr int kMaxSeg = 4;       // warps (segments of <= 31 levels) per cell co
 constexpr int kMaxColours = 8;   // cell colours of a slot, at most
 constexpr int kBCols = 64;       // columns per sweep item
 constexpr int kBRows = 160;      // rows per preconditioner column, at most
+// column sweeps: a sweeping thread's factor ring, kFq chunks of kFr rows of
+// (finv, fa) (the backward sweep reuses it for fc)
+constexpr int kFr = 8, kFq = 4;
+// shared memory of the sweeps: the staged rows, then the sweeping threads'
+// factor rings
+constexpr size_t kSweepRows = sizeof(float) * kBRows * (kBCols + 1);
+constexpr size_t kSweepBytes = kSweepRows + sizeof(float) * kBCols * kFq * kFr * 2;
 
 inline int64_t bchunks(int64_t n) {
   return (n + (int64_t)kBSub * RCHUNK - 1) / ((int64_t)kBSub * RCHUNK);
@@ -344,7 +351,7 @@ __device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const i
 
 // The apply items [i0, i1) of one (group, colour) phase, one warp per item
 // (no block-wide barrier: each warp walks its item's cell columns, and each
-// column's segments, in order). FP32 (the form apply_phase32_lm restates on
+// column's segments, in order). FP32 (the form apply_phase32_ring restates on
 // the level-major copy): z = A32 p for running slots, each column's share of
 // <p, z> (lanes over the column's segments in order, then the lane
 // butterfly) stored at its colour-loop position. FP64 (the form the kernel
@@ -421,10 +428,9 @@ struct Ring {
 // dynamic shared memory: the rings (or the sweeps' staging, which the
 // phases never hold at once), then kRing mbarriers per warp past both
 __host__ __device__ constexpr size_t ring_bar_offset(int ndf) {
-  return ((ndf == 8 ? (size_t)kBW * Ring<8>::WARP : (size_t)kBW * Ring<6>::WARP) >
-                  sizeof(float) * kBRows * (kBCols + 1)
+  return ((ndf == 8 ? (size_t)kBW * Ring<8>::WARP : (size_t)kBW * Ring<6>::WARP) > kSweepBytes
               ? (ndf == 8 ? (size_t)kBW * Ring<8>::WARP : (size_t)kBW * Ring<6>::WARP)
-              : sizeof(float) * kBRows * (kBCols + 1)) +
+              : kSweepBytes) +
          15 & ~(size_t)15;
 }
 __host__ __device__ constexpr size_t dyn_bytes(int ndf) {
@@ -801,6 +807,14 @@ __device__ __noinline__ void vec_phase(const BParams& P, BShared& sh, Pred pred,
   }
 }
 
+// 4-byte asynchronous copy global -> shared (read-only data)
+__device__ __forceinline__ void cp4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+
 // Column sweeps of the line preconditioner for running slots: z = T^{-1} r on
 // the rows of 64 consecutive list items (columns of any slots), staged in
 // shared memory (one warp copies a column's contiguous rows in and out, one
@@ -862,44 +876,68 @@ __device__ __noinline__ void sweep_phase(const BParams& P, float* xs, SweepShare
       const int nrow = ss.nrow[j], nc = D->ncol, c = w.y;
       const float *fa = D->fa, *finv = D->finv, *fc = D->fc;
       float* col = xs + j;
-      double d = 0.0;
-      constexpr int R = 8;
-      for (int i0 = 0; i0 < nrow; i0 += R) {
-        double iv[R], av[R];
+      // this thread's factor ring: kFq chunks of kFr rows, kFq - 1 chunks in
+      // flight while it works on one (one cp.async group per chunk, empty
+      // past the column's end, so the wait counts stay uniform)
+      float* fr = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(xs) + kSweepRows) +
+                  j * (kFq * kFr * 2);
+      const int nchk = (nrow + kFr - 1) / kFr;
+      auto fwd_chunk = [&](int ch) {
+        float* dst = fr + (ch % kFq) * (kFr * 2);
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int i = i0 + q;
-          if (i < nrow) {
-            iv[q] = (double)__ldg(finv + (size_t)i * nc + c);
-            av[q] = (double)__ldg(fa + (size_t)i * nc + c);
+        for (int q = 0; q < kFr; ++q) {
+          const int i = ch * kFr + q;
+          if (ch < nchk && i < nrow) {
+            cp4(dst + 2 * q, finv + (size_t)i * nc + c);
+            cp4(dst + 2 * q + 1, fa + (size_t)i * nc + c);
           }
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      };
+      double d = 0.0;
+      for (int ch = 0; ch < kFq - 1; ++ch) fwd_chunk(ch);
+      for (int ch = 0; ch < nchk; ++ch) {
+        fwd_chunk(ch + kFq - 1);
+        asm volatile("cp.async.wait_group %0;" ::"n"(kFq - 1) : "memory");
+        const float* src = fr + (ch % kFq) * (kFr * 2);
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int i = i0 + q;
+        for (int q = 0; q < kFr; ++q) {
+          const int i = ch * kFr + q;
           if (i < nrow) {
             const double xv = (double)col[i * LD];
-            d = (i == 0) ? iv[q] * xv : iv[q] * fma(-av[q], d, xv);
+            const double iv = (double)src[2 * q], av = (double)src[2 * q + 1];
+            d = (i == 0) ? iv * xv : iv * fma(-av, d, xv);
             col[i * LD] = (float)d;
           }
         }
       }
-      for (int i0 = nrow - 2; i0 >= 0; i0 -= R) {
-        double cv[R];
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      // backward: rows nrow - 2 down to 0 in chunks of kFr (fc only)
+      const int nb = nrow - 1, nbch = (nb + kFr - 1) / kFr;
+      auto bwd_chunk = [&](int ch) {
+        float* dst = fr + (ch % kFq) * (kFr * 2);
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int i = i0 - q;
-          if (i >= 0) cv[q] = (double)__ldg(fc + (size_t)i * nc + c);
+        for (int q = 0; q < kFr; ++q) {
+          const int i = nrow - 2 - (ch * kFr + q);
+          if (ch < nbch && i >= 0) cp4(dst + q, fc + (size_t)i * nc + c);
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      };
+      for (int ch = 0; ch < kFq - 1; ++ch) bwd_chunk(ch);
+      for (int ch = 0; ch < nbch; ++ch) {
+        bwd_chunk(ch + kFq - 1);
+        asm volatile("cp.async.wait_group %0;" ::"n"(kFq - 1) : "memory");
+        const float* src = fr + (ch % kFq) * (kFr * 2);
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int i = i0 - q;
+        for (int q = 0; q < kFr; ++q) {
+          const int i = nrow - 2 - (ch * kFr + q);
           if (i >= 0) {
-            d = fma(-cv[q], d, (double)col[i * LD]);
+            d = fma(-(double)src[q], d, (double)col[i * LD]);
             col[i * LD] = (float)d;
           }
         }
       }
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
     for (int r0 = 0; r0 < maxrow; r0 += 32) {

@@ -583,89 +583,6 @@ struct BcgSmall {
   int rank, done, iters, fail;
 };
 
-// stage rows [row0, row0 + rows) of an n x 64 row-major block into smem,
-// rows scaled by scale[row] when given; rows past n read as zero
-__device__ __forceinline__ void bcg_stage(float (*dst)[kBS], const float* __restrict__ src,
-                                          int64_t row0, int rows, const float* __restrict__ scale) {
-  for (int e = threadIdx.x; e < kBcgRows * (kBS / 4); e += blockDim.x) {
-    const int r = e / (kBS / 4), c4 = e % (kBS / 4);
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (r < rows) {
-      v = ld4(src + (size_t)(row0 + r) * kBS + 4 * c4);
-      if (scale) {
-        const float sc = scale[row0 + r];
-        v.x *= sc; v.y *= sc; v.z *= sc; v.w *= sc;
-      }
-    }
-    *reinterpret_cast<float4*>(&dst[r][4 * c4]) = v;
-  }
-}
-
-// partials[block][v][i][j] = sum over the block's rows of U[row][i] V_v[row][j]
-// (V_v rows scaled by vscale[row] when given); 256 threads, 4 x 4 tiles
-template <int NV>
-__global__ void __launch_bounds__(256) bcg_gram(int64_t n, const float* __restrict__ U,
-                                                const float* __restrict__ V0,
-                                                const float* __restrict__ V1,
-                                                const float* __restrict__ vscale,
-                                                double* __restrict__ partials,
-                                                const BcgSmall* st) {
-  __shared__ __align__(16) float Us[kBcgRows][kBS];
-  __shared__ __align__(16) float Vs[NV][kBcgRows][kBS];
-  if (st->done) return;
-  const int i0 = 4 * (threadIdx.x / 16), j0 = 4 * (threadIdx.x % 16);
-  double acc[NV][4][4];
-#pragma unroll
-  for (int v = 0; v < NV; ++v)
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[v][a][b] = 0.0;
-  for (int64_t c = blockIdx.x; c * kBcgRows < n; c += gridDim.x) {
-    const int64_t row0 = c * kBcgRows;
-    const int rows = (int)(n - row0 < (int64_t)kBcgRows ? n - row0 : (int64_t)kBcgRows);
-    __syncthreads();
-    bcg_stage(Us, U, row0, rows, nullptr);
-    bcg_stage(Vs[0], V0, row0, rows, vscale);
-    if (NV > 1) bcg_stage(Vs[NV - 1], V1, row0, rows, vscale);
-    __syncthreads();
-    float a[NV][4][4];
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-#pragma unroll
-      for (int x = 0; x < 4; ++x)
-#pragma unroll
-        for (int y = 0; y < 4; ++y) a[v][x][y] = 0.f;
-#pragma unroll 4
-    for (int r = 0; r < kBcgRows; ++r) {
-      const float4 u = *reinterpret_cast<const float4*>(&Us[r][i0]);
-      const float uu[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        const float4 w = *reinterpret_cast<const float4*>(&Vs[v][r][j0]);
-        const float ww[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-        for (int x = 0; x < 4; ++x)
-#pragma unroll
-          for (int y = 0; y < 4; ++y) a[v][x][y] = fmaf(uu[x], ww[y], a[v][x][y]);
-      }
-    }
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-#pragma unroll
-      for (int x = 0; x < 4; ++x)
-#pragma unroll
-        for (int y = 0; y < 4; ++y) acc[v][x][y] += (double)a[v][x][y];
-  }
-  double* out = partials + (size_t)blockIdx.x * NV * kBS * kBS;
-#pragma unroll
-  for (int v = 0; v < NV; ++v)
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-      for (int y = 0; y < 4; ++y) out[((size_t)v * kBS + i0 + x) * kBS + j0 + y] = acc[v][x][y];
-}
-
 // ---- The same Gram on the 5th-generation tensor cores (tcgen05).
 // D (64 x 64 NV) = U^T [V_0 .. V_NV-1] accumulates in tensor memory (TMEM,
 // FP32): A = U^T (64 x K) and B = V^T (64 NV x K) are both K-major in shared
@@ -896,31 +813,213 @@ __global__ void bcg_reduce(int nb, int ne, const double* __restrict__ partials,
   out[e] = s;
 }
 
-// Y (+)= B C for one or two row blocks: mode 0: X += P C, R -= Q C and the
-// column sums of R^2 into partials[block][64]; mode 1: W = D^-1 R + P C;
-// mode 2: P = W C. With skip_p the products are left out (taken as zero,
-// whatever the blocks hold): mode 0 then only sums R^2, mode 1 sets
-// W = D^-1 R.
+// ---- The same products with the tall blocks streamed. A block takes the
+// 32-row chunks c = blockIdx.x + i gridDim.x of its operands (each chunk of
+// an n x 64 row-major FP32 block is one contiguous 8 KB run) through a ring
+// of S stages in shared memory: thread 0 moves a chunk's operands with
+// cp.async.bulk copies completing on the stage's mbarrier, S - 1 chunks
+// ahead of the compute, so the bytes in flight cost no registers. Every wait
+// is bounded (kTcWaitNs); the block decides together (__syncthreads_and)
+// and, on a time-out, sets st->fail = 2, waits (bounded) for the copies it
+// issued and stops. Sums: FP32 within a chunk, FP64 across chunks and blocks, in a fixed order.
+constexpr int kChunkBytes = kBcgRows * kBS * 4;  // one operand's chunk
+template <int NA, int S>
+struct ChunkRing {
+  static constexpr int STAGE = NA * kChunkBytes;
+  static constexpr size_t BYTES = (size_t)S * STAGE + (size_t)S * 8;
+};
+__device__ __forceinline__ bool chunk_try(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool chunk_wait(uint64_t* bar, unsigned parity) {
+  if (chunk_try(bar, parity)) return true;
+  const unsigned long long t0 = tc_clock();
+  while (!chunk_try(bar, parity))
+    if (tc_clock() - t0 > kTcWaitNs) return false;
+  return true;
+}
+// thread 0: chunk c of the NA operands into stage buffer dst, on bar
+template <int NA>
+__device__ __forceinline__ void chunk_issue(const float* const (&src)[NA], int64_t c, int64_t n,
+                                            unsigned char* dst, uint64_t* bar) {
+  const int64_t row0 = c * kBcgRows;
+  const int rows = (int)(n - row0 < (int64_t)kBcgRows ? n - row0 : (int64_t)kBcgRows);
+  const unsigned bytes = (unsigned)rows * kBS * 4;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes * NA)
+               : "memory");
+#pragma unroll
+  for (int a = 0; a < NA; ++a)
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst + a * kChunkBytes)),
+        "l"(src[a] + (size_t)row0 * kBS), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// the ring's set-up and its bounded drain after a time-out
+template <int S>
+__device__ __forceinline__ void chunk_ring_init(uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + i)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+template <int S>
+__device__ __forceinline__ void chunk_ring_drain(uint64_t* bar, int from, int to) {
+  if (threadIdx.x == 0)
+    for (int i = from; i < to; ++i) chunk_wait(bar + i % S, (unsigned)((i / S) & 1));
+}
+
+template <int NV>
+__global__ void __launch_bounds__(256) bcg_gram_s(int64_t n, const float* __restrict__ U,
+                                                  const float* __restrict__ V0,
+                                                  const float* __restrict__ V1,
+                                                  const float* __restrict__ vscale,
+                                                  double* __restrict__ partials, BcgSmall* st) {
+  constexpr int NA = 1 + NV, S = 4;
+  using RG = ChunkRing<NA, S>;
+  extern __shared__ __align__(16) unsigned char ring_smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ring_smem + S * RG::STAGE);
+  if (st->done) return;
+  const float* src[NA];
+  src[0] = U;
+  src[1] = V0;
+  if (NV > 1) src[NA - 1] = V1;
+  const int64_t nchunk = (n + kBcgRows - 1) / kBcgRows;
+  const int nmine = blockIdx.x < nchunk ? (int)((nchunk - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  chunk_ring_init<S>(bar);
+  if (threadIdx.x == 0)
+    for (int i = 0; i < S && i < nmine; ++i)
+      chunk_issue<NA>(src, blockIdx.x + (int64_t)i * gridDim.x, n, ring_smem + i * RG::STAGE, bar + i);
+  const int i0 = 4 * (threadIdx.x / 16), j0 = 4 * (threadIdx.x % 16);
+  double acc[NV][4][4];
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[v][a][b] = 0.0;
+  bool failed = false;
+  for (int i = 0; i < nmine; ++i) {
+    const int stg = i % S;
+    const bool ok = chunk_wait(bar + stg, (unsigned)((i / S) & 1));
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) st->fail = 2;
+      chunk_ring_drain<S>(bar, i + 1, nmine < i + S ? nmine : i + S);
+      failed = true;
+      break;
+    }
+    const int64_t c = blockIdx.x + (int64_t)i * gridDim.x, row0 = c * kBcgRows;
+    const int rows = (int)(n - row0 < (int64_t)kBcgRows ? n - row0 : (int64_t)kBcgRows);
+    const float (*Us)[kBS] = reinterpret_cast<const float (*)[kBS]>(ring_smem + stg * RG::STAGE);
+    float a[NV][4][4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) a[v][x][y] = 0.f;
+    for (int r = 0; r < rows; ++r) {
+      const float4 u = *reinterpret_cast<const float4*>(&Us[r][i0]);
+      const float uu[4] = {u.x, u.y, u.z, u.w};
+      const float sc = vscale ? __ldg(vscale + row0 + r) : 1.f;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const float (*Vs)[kBS] =
+            reinterpret_cast<const float (*)[kBS]>(ring_smem + stg * RG::STAGE + (1 + v) * kChunkBytes);
+        float4 w = *reinterpret_cast<const float4*>(&Vs[r][j0]);
+        if (vscale) {
+          w.x *= sc; w.y *= sc; w.z *= sc; w.w *= sc;
+        }
+        const float ww[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) a[v][x][y] = fmaf(uu[x], ww[y], a[v][x][y]);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[v][x][y] += (double)a[v][x][y];
+    __syncthreads();  // the stage is read: it takes chunk i + S
+    if (threadIdx.x == 0 && i + S < nmine)
+      chunk_issue<NA>(src, blockIdx.x + (int64_t)(i + S) * gridDim.x, n, ring_smem + stg * RG::STAGE,
+                      bar + stg);
+  }
+  double* out = partials + (size_t)blockIdx.x * NV * kBS * kBS;
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+        out[((size_t)v * kBS + i0 + x) * kBS + j0 + y] = failed ? 0.0 : acc[v][x][y];
+}
+
+// Y (+)= B C streamed: mode 0 (P, Q, X, R): X += P C, R -= Q C and the column
+// sums of R^2; mode 1 (P, R): W = D^-1 R + P C; mode 2 (W): P = W C
 template <int MODE>
-__global__ void __launch_bounds__(256) bcg_update(int64_t n, const float* __restrict__ A0,
-                                                  const float* __restrict__ A1, float* Y0,
-                                                  float* Y1, const float* __restrict__ dinv,
-                                                  const BcgSmall* st, int skip_p,
-                                                  double* __restrict__ partials) {
+struct UpdOps {
+  static constexpr int NA = MODE == 0 ? 4 : MODE == 1 ? 2 : 1;
+  static constexpr int S = MODE == 0 ? 3 : 4;
+};
+template <int MODE>
+__global__ void __launch_bounds__(256) bcg_update_s(int64_t n, const float* __restrict__ A0,
+                                                    const float* __restrict__ A1, float* Y0,
+                                                    float* Y1, const float* __restrict__ dinv,
+                                                    const BcgSmall* st, int skip_p,
+                                                    double* __restrict__ partials) {
+  constexpr int NA = UpdOps<MODE>::NA, S = UpdOps<MODE>::S;
+  using RG = ChunkRing<NA, S>;
+  extern __shared__ __align__(16) unsigned char ring_smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ring_smem + S * RG::STAGE);
   __shared__ __align__(16) float Cs[kBS][kBS];
-  __shared__ __align__(16) float As[2][kBcgRows][kBS];
-  __shared__ double red[16][kBS];
   if (st->done) return;
   for (int e = threadIdx.x; e < kBS * kBS; e += blockDim.x) Cs[e / kBS][e % kBS] = st->coef[e];
+  // streamed operands: mode 0 P, Q, X, R; mode 1 P, R; mode 2 W
+  const float* src[NA];
+  src[0] = A0;
+  if (MODE == 0) {
+    src[1] = A1;
+    src[2] = Y0;
+    src[3] = Y1;
+  } else if (MODE == 1) {
+    src[1] = A1;
+  }
+  const int64_t nchunk = (n + kBcgRows - 1) / kBcgRows;
+  const int nmine = blockIdx.x < nchunk ? (int)((nchunk - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  chunk_ring_init<S>(bar);
+  if (threadIdx.x == 0)
+    for (int i = 0; i < S && i < nmine; ++i)
+      chunk_issue<NA>(src, blockIdx.x + (int64_t)i * gridDim.x, n, ring_smem + i * RG::STAGE, bar + i);
   const int r0 = 2 * (threadIdx.x / 16), c0 = 4 * (threadIdx.x % 16);
   double nrm[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int64_t c = blockIdx.x; c * kBcgRows < n; c += gridDim.x) {
-    const int64_t row0 = c * kBcgRows;
+  for (int i = 0; i < nmine; ++i) {
+    const int stg = i % S;
+    const bool ok = chunk_wait(bar + stg, (unsigned)((i / S) & 1));
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) const_cast<BcgSmall*>(st)->fail = 2;
+      chunk_ring_drain<S>(bar, i + 1, nmine < i + S ? nmine : i + S);
+      break;
+    }
+    const int64_t c = blockIdx.x + (int64_t)i * gridDim.x, row0 = c * kBcgRows;
     const int rows = (int)(n - row0 < (int64_t)kBcgRows ? n - row0 : (int64_t)kBcgRows);
-    __syncthreads();
-    if (!skip_p) bcg_stage(As[0], A0, row0, rows, nullptr);
-    if (MODE == 0 && !skip_p) bcg_stage(As[1], A1, row0, rows, nullptr);
-    __syncthreads();
+    const unsigned char* stage = ring_smem + stg * RG::STAGE;
+    const float (*As0)[kBS] = reinterpret_cast<const float (*)[kBS]>(stage);
+    const float (*As1)[kBS] = reinterpret_cast<const float (*)[kBS]>(stage + kChunkBytes);
 #pragma unroll
     for (int rr = 0; rr < 2; ++rr) {
       const int r = r0 + rr;
@@ -931,36 +1030,43 @@ __global__ void __launch_bounds__(256) bcg_update(int64_t n, const float* __rest
 #pragma unroll 8
         for (int k = 0; k < kBS; ++k) {
           const float4 cf = *reinterpret_cast<const float4*>(&Cs[k][c0]);
-          const float a0 = As[0][r][k];
+          const float a0 = As0[r][k];
           d0[0] = fmaf(a0, cf.x, d0[0]); d0[1] = fmaf(a0, cf.y, d0[1]);
           d0[2] = fmaf(a0, cf.z, d0[2]); d0[3] = fmaf(a0, cf.w, d0[3]);
           if (MODE == 0) {
-            const float a1 = As[1][r][k];
+            const float a1 = As1[r][k];
             d1[0] = fmaf(a1, cf.x, d1[0]); d1[1] = fmaf(a1, cf.y, d1[1]);
             d1[2] = fmaf(a1, cf.z, d1[2]); d1[3] = fmaf(a1, cf.w, d1[3]);
           }
         }
       }
       if (MODE == 0) {
-        const float4 x = ld4(Y0 + o), rv = ld4(Y1 + o);
+        const float4 x = *reinterpret_cast<const float4*>(stage + 2 * kChunkBytes + (r * kBS + c0) * 4);
+        const float4 rv = *reinterpret_cast<const float4*>(stage + 3 * kChunkBytes + (r * kBS + c0) * 4);
         st4(Y0 + o, make_float4(x.x + d0[0], x.y + d0[1], x.z + d0[2], x.w + d0[3]));
         const float rn[4] = {rv.x - d1[0], rv.y - d1[1], rv.z - d1[2], rv.w - d1[3]};
         st4(Y1 + o, make_float4(rn[0], rn[1], rn[2], rn[3]));
 #pragma unroll
         for (int j = 0; j < 4; ++j) nrm[j] = fma((double)rn[j], (double)rn[j], nrm[j]);
       } else if (MODE == 1) {
-        const float4 rv = ld4(A1 + o);
-        const float dv = dinv[row0 + r];
+        const float4 rv = *reinterpret_cast<const float4*>(&As1[r][c0]);
+        const float dv = __ldg(dinv + row0 + r);
         st4(Y0 + o, make_float4(fmaf(rv.x, dv, d0[0]), fmaf(rv.y, dv, d0[1]),
                                 fmaf(rv.z, dv, d0[2]), fmaf(rv.w, dv, d0[3])));
       } else {
         st4(Y0 + o, make_float4(d0[0], d0[1], d0[2], d0[3]));
       }
     }
+    __syncthreads();  // the stage is read: it takes chunk i + S
+    if (threadIdx.x == 0 && i + S < nmine)
+      chunk_issue<NA>(src, blockIdx.x + (int64_t)(i + S) * gridDim.x, n, ring_smem + stg * RG::STAGE,
+                      bar + stg);
   }
   if (MODE == 0) {
-    // column sums of R^2: threads with the same c0 (16 of them, one per row
-    // pair) in a fixed order
+    // column sums of R^2 in a fixed order, in the ring's memory (every
+    // chunk has been consumed)
+    __syncthreads();
+    double (*red)[kBS] = reinterpret_cast<double (*)[kBS]>(ring_smem);
 #pragma unroll
     for (int j = 0; j < 4; ++j) red[threadIdx.x / 16][c0 + j] = nrm[j];
     __syncthreads();
@@ -1664,7 +1770,14 @@ int gram(lfx_mrhs* m, const float* U, const float* V0, const float* V1, const fl
     bcg_gram_tc<NV><<<m->bgrid, kTcThreads, tc_gram_smem<NV>(), ctx->stream>>>(n, U, V0, V1,
                                                                                vscale, m->bpart, st);
   } else {
-    bcg_gram<NV><<<m->bgrid, 256, 0, ctx->stream>>>(n, U, V0, V1, vscale, m->bpart, st);
+    constexpr size_t smem = ChunkRing<1 + NV, 4>::BYTES;
+    static bool sattr = false;
+    if (!sattr) {
+      LFX_CK(ctx, cudaFuncSetAttribute(bcg_gram_s<NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+      sattr = true;
+    }
+    bcg_gram_s<NV><<<m->bgrid, 256, smem, ctx->stream>>>(n, U, V0, V1, vscale, m->bpart, st);
   }
   const int ne = NV * kBS * kBS;
   bcg_reduce<<<(ne + 255) / 256, 256, 0, ctx->stream>>>(m->bgrid, ne, m->bpart, out, st);
@@ -1687,6 +1800,24 @@ int ensure_bcg(lfx_mrhs* m) {
   return rc;
 }
 
+// the streamed update kernel of a mode with its shared memory set: returns a
+// callable taking the kernel's arguments
+template <int MODE>
+auto upd_launch(lfx_ctx* ctx, int G) {
+  using RG = ChunkRing<UpdOps<MODE>::NA, UpdOps<MODE>::S>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(bcg_update_s<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)RG::BYTES);
+    attr = true;
+  }
+  return [ctx, G](int64_t n, const float* A0, const float* A1, float* Y0, float* Y1,
+                  const float* dinv, const BcgSmall* st, int skip_p, double* partials) {
+    bcg_update_s<MODE><<<G, 256, RG::BYTES, ctx->stream>>>(n, A0, A1, Y0, Y1, dinv, st, skip_p,
+                                                            partials);
+  };
+}
+
 // One inner block-CG solve of A X = R (R from the outer residual, X = 0),
 // each active right-hand side reduced by tol, at most max_inner iterations.
 int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner_its,
@@ -1703,17 +1834,17 @@ int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner
   LFX_CK(ctx, cudaMemsetAsync(m->x32, 0, (size_t)n * kBS * 4, ctx->stream));
   bcg_mask<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(n, m->r32, st->active);
   // r0: column norms of R (the update kernel's norm pass, products left out)
-  bcg_update<0><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 1,
+  upd_launch<0>(ctx, G)(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 1,
                                             m->bpart);
   bcg_reduce<<<1, kBS, 0, ctx->stream>>>(G, kBS, m->bpart, st->rn, st);
   bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(3, st, tol);
   // P = orth(D^-1 R)
-  bcg_update<1><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 1,
+  upd_launch<1>(ctx, G)(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 1,
                                             nullptr);
   int rc = gram<1>(m, m->w32, m->w32, nullptr, nullptr, st, st->G);
   if (rc) return rc;
   bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(2, st, tol);
-  bcg_update<2><<<G, 256, 0, ctx->stream>>>(n, m->w32, nullptr, m->p32, nullptr, nullptr, st, 0,
+  upd_launch<2>(ctx, G)(n, m->w32, nullptr, m->p32, nullptr, nullptr, st, 0,
                                             nullptr);
   ctx->launches += 10;
   LFX_CK(ctx, cudaGetLastError());
@@ -1725,7 +1856,7 @@ int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner
     if (rc) return rc;
     bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(0, st, tol);
     // X += P alpha, R -= Q alpha, ||R_j||
-    bcg_update<0><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 0,
+    upd_launch<0>(ctx, G)(n, m->p32, m->q32, m->x32, m->r32, m->dinv, st, 0,
                                               m->bpart);
     bcg_reduce<<<1, kBS, 0, ctx->stream>>>(G, kBS, m->bpart, st->rn, st);
     // beta (and convergence)
@@ -1733,12 +1864,12 @@ int bcg_inner(lfx_mrhs* m, const int* act, double tol, int max_inner, int* inner
     if (rc) return rc;
     bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(1, st, tol);
     // P = orth(D^-1 R + P beta)
-    bcg_update<1><<<G, 256, 0, ctx->stream>>>(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 0,
+    upd_launch<1>(ctx, G)(n, m->p32, m->r32, m->w32, nullptr, m->dinv, st, 0,
                                               nullptr);
     rc = gram<1>(m, m->w32, m->w32, nullptr, nullptr, st, st->G);
     if (rc) return rc;
     bcg_small<<<1, 256, kBcgSmallSmem, ctx->stream>>>(2, st, tol);
-    bcg_update<2><<<G, 256, 0, ctx->stream>>>(n, m->w32, nullptr, m->p32, nullptr, nullptr, st,
+    upd_launch<2>(ctx, G)(n, m->w32, nullptr, m->p32, nullptr, nullptr, st,
                                               0, nullptr);
     ctx->launches += 13;
     LFX_CK(ctx, cudaGetLastError());

@@ -207,6 +207,28 @@ def _run_mrhs(args):
     print(m.info(), tune, flush=True)
 
 
+def _run_mrhs_solve(args):
+    """One multi-RHS solve of the C48x30 W0 system (64 seeded N(0,1)
+    right-hand sides, 1e-8), per-RHS CG or block CG, after one untimed solve."""
+    import torch
+    ctx = lfx.Context(0)
+    p = mg.w0_problem(args.n, args.nl, seed=1, rhs="normal")
+    s = device_w0(ctx, p)
+    kind = lfx.MRHS_BF16 if args.kind == "bf16" else lfx.MRHS_TF32
+    method = lfx.MRHS_BLOCK_CG if args.method == "block" else lfx.MRHS_PER_RHS_CG
+    m = lfx.MultiRhsOperator(s.op, kind, 64)
+    m.set_gram(args.gram == "tcgen05")
+    m.autotune(reps=1)
+    b = torch.from_numpy(np.stack([mg.normal(1000 + r, p.undf) for r in range(64)])).cuda()
+    x = torch.zeros_like(b)
+    for _ in range(2):
+        x.zero_()
+        torch.cuda.synchronize()
+        info = m.solve(s.op, s.diag, b.data_ptr(), x.data_ptr(), p.undf, r_tol=1e-8, method=method)
+    ctx.synchronize()
+    print("inner iterations", max(i.inner_iterations for i in info), flush=True)
+
+
 def _run_batch_w2(args):
     ctx = lfx.Context(0)
     s = batch_system(ctx, args.n, args.nl, args.seed, mg.W2)
@@ -315,7 +337,7 @@ def _run_solve_w2(args):
 
 def main(argv=None):
     """One named workload, run once, for profilers:
-    ``python -m lfric_core_b200.workloads apply|time-apply|prec|mrhs|batch-w0|batch-w2|solve-w2 [options]``."""
+    ``python -m lfric_core_b200.workloads apply|time-apply|prec|mrhs|mrhs-solve|batch-w0|batch-w2|solve-w2 [options]``."""
     import argparse
     ap = argparse.ArgumentParser(prog="python -m lfric_core_b200.workloads")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -341,6 +363,12 @@ def main(argv=None):
     m.add_argument("--nrhs", type=int, default=64)
     m.add_argument("--autotune-reps", type=int, default=1)
     m.add_argument("--reps", type=int, default=2)
+    ms = sub.add_parser("mrhs-solve", help="one 64-RHS solve of the W0 operator, per-RHS or block CG")
+    ms.add_argument("--n", type=int, default=48)
+    ms.add_argument("--nl", type=int, default=30)
+    ms.add_argument("--kind", choices=["tf32", "bf16"], default="bf16")
+    ms.add_argument("--method", choices=["per-rhs", "block"], default="block")
+    ms.add_argument("--gram", choices=["fp32", "tcgen05"], default="fp32")
     b = sub.add_parser("batch-w2", help="one W2 solve by FP64 CG and by the batch engine")
     b.add_argument("--n", type=int, default=94)
     b.add_argument("--nl", type=int, default=64)
@@ -365,7 +393,7 @@ def main(argv=None):
     w.add_argument("--apply", default="",
                    help="pinned apply kernel:stages for FP32,FP64 (default: autotune)")
     args = ap.parse_args(argv)
-    {"apply": _run_apply, "time-apply": _run_time_apply, "mrhs": _run_mrhs,
+    {"apply": _run_apply, "time-apply": _run_time_apply, "mrhs": _run_mrhs, "mrhs-solve": _run_mrhs_solve,
      "batch-w2": _run_batch_w2, "batch-w0": _run_batch_w0, "solve-w2": _run_solve_w2,
      "prec": _run_prec}[args.cmd](args)
     return 0

@@ -576,7 +576,7 @@ struct BcgSmall {
   double C[2 * kBS * kBS];  // [v][i][j]: v = 0 P^T Q, v = 1 P^T R (gram of P with Q, R)
   double E[kBS * kBS];      // Q^T D^-1 R
   double G[kBS * kBS];      // W^T W
-  double L1[kBS * kBS];     // Cholesky factor of the active block of P^T Q
+  double L1[kBS * kBS];     // inverse of the Cholesky factor of the active block of P^T Q
   double r0[kBS], rn[kBS];
   float coef[kBS * kBS];    // alpha, beta or T [k][j] for the next row update
   int active[kBS];          // right-hand sides the solve works on
@@ -1087,22 +1087,82 @@ __global__ void __launch_bounds__(256) bcg_mask(int64_t n, float* R, const int* 
 }
 
 // The 64 x 64 algebra of one step, in FP64, one block of 256 threads.
-// mode 0 (alpha): L1 = chol(active block of P^T Q); alpha = L1^-T L1^-1 P^T R
+// mode 0 (alpha): L = chol(active r x r block of P^T Q); L1 = L^-1 (kept for
+//   mode 1); alpha = L1^T (L1 P^T R)
 // mode 1 (beta): rn = sqrt(column sums) (convergence: done when every active
-//   right-hand side has rn <= tol r0); beta = -(P^T Q)^-1 Q^T D^-1 R
+//   right-hand side has rn <= tol r0); beta = -L1^T (L1 Q^T D^-1 R)
 // mode 2 (orth): pivoted Cholesky of W^T W -> rank and T (P = W T)
 // mode 3 (norms of the initial residual into r0)
 // The kernel's whole shared state is one dynamic buffer laid out here (no
-// static shared variables beside it): two 64 x 65 FP64 matrices, then the
+// static shared variables beside it): three 64 x 65 FP64 matrices, then the
 // pivot order and two flags.
 constexpr size_t kBcgMatBytes = sizeof(double) * kBS * (kBS + 1);
-constexpr size_t kBcgSmallSmem = 2 * kBcgMatBytes + sizeof(int) * (kBS + 4);
+constexpr size_t kBcgSmallSmem = 3 * kBcgMatBytes + sizeof(int) * (kBS + 4);
+
+// Linv = L^-1 for the r x r lower factor L(i, k): thread j < r forms column
+// j (rows below j by forward substitution, the dot products in four partial
+// sums); rows and columns past r are zero
+template <class Lf>
+__device__ __forceinline__ void lower_inverse(int r, Lf L, double (*Linv)[kBS + 1]) {
+  const int t = threadIdx.x;
+  if (t < kBS) {
+    const int j = t;
+    for (int i = 0; i < kBS; ++i) Linv[i][j] = 0.0;
+    if (j < r) {
+      Linv[j][j] = 1.0 / L(j, j);
+      for (int i = j + 1; i < r; ++i) {
+        double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+        int k = j;
+        for (; k + 3 < i; k += 4) {
+          v0 = fma(L(i, k), Linv[k][j], v0);
+          v1 = fma(L(i, k + 1), Linv[k + 1][j], v1);
+          v2 = fma(L(i, k + 2), Linv[k + 2][j], v2);
+          v3 = fma(L(i, k + 3), Linv[k + 3][j], v3);
+        }
+        for (; k < i; ++k) v0 = fma(L(i, k), Linv[k][j], v0);
+        Linv[i][j] = -((v0 + v1) + (v2 + v3)) / L(i, i);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Out = op(A) B for 64 x 64 operands, op(A) = A or A^T; each thread a 4 x 4
+// tile, k in increasing order
+template <bool TRANS>
+__device__ __forceinline__ void small_mm(const double (*A)[kBS + 1], const double (*B)[kBS + 1],
+                                         double (*Out)[kBS + 1], double scale) {
+  const int i0 = 4 * (threadIdx.x / 16), j0 = 4 * (threadIdx.x % 16);
+  double acc[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+  for (int k = 0; k < kBS; ++k) {
+    double a[4], bv[4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) a[x] = TRANS ? A[k][i0 + x] : A[i0 + x][k];
+#pragma unroll
+    for (int y = 0; y < 4; ++y) bv[y] = B[k][j0 + y];
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], bv[y], acc[x][y]);
+  }
+  __syncthreads();  // Out may alias B
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) Out[i0 + x][j0 + y] = scale * acc[x][y];
+  __syncthreads();
+}
 
 __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double tol) {
   extern __shared__ __align__(16) unsigned char bcg_dyn[];
   double (*M)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn);
   double (*Bm)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn + kBcgMatBytes);
-  int* perm = reinterpret_cast<int*>(bcg_dyn + 2 * kBcgMatBytes);
+  double (*Y)[kBS + 1] = reinterpret_cast<double (*)[kBS + 1]>(bcg_dyn + 2 * kBcgMatBytes);
+  int* perm = reinterpret_cast<int*>(bcg_dyn + 3 * kBcgMatBytes);
   int& s_r = perm[kBS];
   int& s_stop = perm[kBS + 1];
   const int t = threadIdx.x;
@@ -1142,9 +1202,12 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
         if (t == 0) { st->fail = 1; st->done = 1; }
         return;
       }
-      for (int e = t; e < kBS * kBS; e += blockDim.x) st->L1[e] = M[e / kBS][e % kBS];
+      // L1 = L^-1, kept for mode 1
+      lower_inverse(r, [&](int i, int k) { return M[i][k]; }, Bm);
+      for (int e = t; e < kBS * kBS; e += blockDim.x) st->L1[e] = Bm[e / kBS][e % kBS];
       // right-hand sides: P^T R
-      for (int e = t; e < kBS * kBS; e += blockDim.x) Bm[e / kBS][e % kBS] = st->C[kBS * kBS + e];
+      for (int e = t; e < kBS * kBS; e += blockDim.x) M[e / kBS][e % kBS] = st->C[kBS * kBS + e];
+      __syncthreads();
     } else {
       if (t < kBS) st->rn[t] = sqrt(st->rn[t]);
       __syncthreads();
@@ -1161,26 +1224,19 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
         return;
       }
       for (int e = t; e < kBS * kBS; e += blockDim.x) {
-        M[e / kBS][e % kBS] = st->L1[e];
-        Bm[e / kBS][e % kBS] = -st->E[e];
+        Bm[e / kBS][e % kBS] = st->L1[e];
+        M[e / kBS][e % kBS] = st->E[e];
       }
+      __syncthreads();
     }
+    // rows past r of the right-hand sides do not take part
+    for (int e = t; e < kBS * kBS; e += blockDim.x)
+      if (e / kBS >= r) M[e / kBS][e % kBS] = 0.0;
     __syncthreads();
-    // solve L L^T Y = B on the first r rows, column j per thread
-    if (t < kBS) {
-      const int j = t;
-      for (int i = 0; i < r; ++i) {
-        double v = Bm[i][j];
-        for (int k = 0; k < i; ++k) v -= M[i][k] * Bm[k][j];
-        Bm[i][j] = v / M[i][i];
-      }
-      for (int i = r - 1; i >= 0; --i) {
-        double v = Bm[i][j];
-        for (int k = i + 1; k < r; ++k) v -= M[k][i] * Bm[k][j];
-        Bm[i][j] = v / M[i][i];
-      }
-      for (int i = 0; i < kBS; ++i) st->coef[i * kBS + j] = i < r ? (float)Bm[i][j] : 0.f;
-    }
+    // Y = L1 B, then the coefficients L1^T Y (negated for beta)
+    small_mm<false>(Bm, M, Y, 1.0);
+    small_mm<true>(Bm, Y, Y, mode == 0 ? 1.0 : -1.0);
+    for (int e = t; e < kBS * kBS; e += blockDim.x) st->coef[e] = (float)Y[e / kBS][e % kBS];
     return;
   }
   // mode 2: pivoted Cholesky of G = W^T W, stopping at pivots below
@@ -1190,7 +1246,8 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
   // form that swapped rows and columns in place, in one thread inside the
   // loop over steps, lost the pivot's square root on the B200 while the same
   // statements with a constant step index did not; the index form has no
-  // such swaps.)
+  // such swaps.) Warp 0 finds each pivot: the largest remaining diagonal
+  // entry, the first in step order on a tie.
   for (int e = t; e < kBS * kBS; e += blockDim.x) M[e / kBS][e % kBS] = st->G[e];
   if (t < kBS) perm[t] = t;
   if (t == 0) s_r = 0;
@@ -1198,19 +1255,32 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
   double dmax = 0.0;
   for (int i = 0; i < kBS; ++i) dmax = fmax(dmax, M[i][i]);
   for (int k = 0; k < kBS; ++k) {
-    if (t == 0) {
-      int p = k;
-      for (int i = k + 1; i < kBS; ++i)
-        if (M[perm[i]][perm[i]] > M[perm[p]][perm[p]]) p = i;
-      const int pk = perm[p];
-      const int stop = !(M[pk][pk] > kBcgDrop * dmax) || !(dmax > 0.0);
-      if (!stop) {
-        perm[p] = perm[k];
-        perm[k] = pk;
-        M[pk][pk] = sqrt(M[pk][pk]);
-        s_r = k + 1;
+    if (t < 32) {
+      // lane l looks at steps k + l and k + l + 32
+      double bv = -INFINITY;
+      int bi = kBS;  // none (every candidate NaN): the factorisation stops
+      for (int i = k + t; i < kBS; i += 32) {
+        const double dv = M[perm[i]][perm[i]];
+        if (dv > bv) { bv = dv; bi = i; }
       }
-      s_stop = stop;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if (t == 0) {
+        const int p = bi < kBS ? bi : k;
+        const int pk = perm[p];
+        const int stop = bi >= kBS || !(M[pk][pk] > kBcgDrop * dmax) || !(dmax > 0.0);
+        if (!stop) {
+          perm[p] = perm[k];
+          perm[k] = pk;
+          M[pk][pk] = sqrt(M[pk][pk]);
+          s_r = k + 1;
+        }
+        s_stop = stop;
+      }
     }
     __syncthreads();
     if (s_stop) break;
@@ -1225,20 +1295,8 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
     __syncthreads();
   }
   const int r = s_r;
-  // Linv = L^-1 (r x r, lower; L[i][k] = M[perm[i]][perm[k]]): column j per
-  // thread
-  if (t < r) {
-    const int j = t;
-    for (int i = 0; i < r; ++i) Bm[i][j] = 0.0;
-    Bm[j][j] = 1.0 / M[perm[j]][perm[j]];
-    for (int i = j + 1; i < r; ++i) {
-      const int pi = perm[i];
-      double v = 0.0;
-      for (int k = j; k < i; ++k) v -= M[pi][perm[k]] * Bm[k][j];
-      Bm[i][j] = v / M[pi][pi];
-    }
-  }
-  __syncthreads();
+  // Linv = L^-1 (r x r, lower; L[i][k] = M[perm[i]][perm[k]])
+  lower_inverse(r, [&](int i, int k) { return M[perm[i]][perm[k]]; }, Bm);
   // T[perm[i]][j] = Linv[j][i] (i <= j < r), zero elsewhere
   for (int e = t; e < kBS * kBS; e += blockDim.x) st->coef[e] = 0.f;
   __syncthreads();

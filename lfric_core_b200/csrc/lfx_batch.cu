@@ -131,6 +131,7 @@ struct BParams {
   unsigned* tickets;
   int* need;            // [kMaxIters]: a slot takes a true residual in super-iteration it
   unsigned* bar;        // grid barrier {count, generation}
+  unsigned* wq;         // [2] FP32 apply work counters, alternate phases
   int* err;             // LFX_TIMEOUT when a wait ran out
   int ngr32, ngr64, nchunk, ncolitem;
   int iters, max_slots, any_cma, ncolour;
@@ -500,15 +501,25 @@ __device__ __forceinline__ void row_sums(const float4* Ms, bool v, const float (
 template <int NDF>
 __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4* __restrict__ items,
                                                     int i0, int i1, unsigned char* ring,
-                                                    uint64_t* bars, unsigned seq) {
+                                                    uint64_t* bars, unsigned seq, unsigned* ctr) {
   using R = Ring<NDF>;
   constexpr int NP = R::NP, NPV = R::NPV;
   const int lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * kBW + (threadIdx.x >> 5), nw = gridDim.x * kBW;
-  for (int u = i0 + gw; u < i1; u += nw) {
+  // warps take items by the phase's counter (lane 0), the next one asked for
+  // while the current item runs
+  unsigned nxt = 0;
+  if (lane == 0) nxt = atomicAdd(ctr, 1u);
+  nxt = __shfl_sync(0xffffffffu, nxt, 0);
+  for (;;) {
+    const int u = i0 + (int)nxt;
+    if (u >= i1) break;
+    if (lane == 0) nxt = atomicAdd(ctr, 1u);
     const int4 it = __ldg(items + u);
     const int s = it.x;
-    if (!ph_run(__ldcg(&P.st[s].phase))) continue;  // warp-uniform
+    if (!ph_run(__ldcg(&P.st[s].phase))) {  // warp-uniform
+      nxt = __shfl_sync(0xffffffffu, nxt, 0);
+      continue;
+    }
     const BSlot& D = P.slots[s];
     const float4* M4 = D.L32;
     const int* cdesc = D.cdesc;
@@ -618,6 +629,7 @@ __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4
       return seq;
     }
     seq += (unsigned)nunit;
+    nxt = __shfl_sync(0xffffffffu, nxt, 0);
   }
   return seq;
 }
@@ -969,6 +981,7 @@ __global__ void __launch_bounds__(kBT, kMaxBps) batch_kernel(const BParams* __re
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   unsigned seq = 0;  // ring units this warp has issued (and consumed)
+  int aph = 0;       // FP32 apply phases run so far in this launch
   __shared__ BShared sh;
   __shared__ BParams sp;
   __shared__ SweepShared ss;
@@ -997,8 +1010,12 @@ __global__ void __launch_bounds__(kBT, kMaxBps) batch_kernel(const BParams* __re
     for (int g = 0; g < P.ngr32; ++g)
       for (int c = 0; c < P.ncolour; ++c) {
         const int o = g * P.ncolour + c;
+        // this apply phase takes counter aph & 1; the next one's is cleared
+        // now (its last user finished before the last barrier)
+        if (blockIdx.x == 0 && threadIdx.x == 0) P.wq[(aph + 1) & 1] = 0u;
         seq = apply_phase32_ring<NDF>(P, P.items32, __ldg(P.off32 + o), __ldg(P.off32 + o + 1),
-                                      ring, bars, seq);
+                                      ring, bars, seq, P.wq + (aph & 1));
+        ++aph;
         if (!grid_sync(P, sh)) return;
       }
     alpha_phase(P, sh);
@@ -1351,6 +1368,7 @@ int rebuild(lfx_batch* B) {
   P.tickets = B->d_tickets;
   P.need = B->d_need;
   P.bar = B->d_bar;
+  P.wq = B->d_bar + 2;
   P.err = B->d_err;
   P.ngr32 = (int)(off32.size() - 1) / ncolour;
   P.ngr64 = (int)(off64.size() - 1) / ncolour;
@@ -1391,7 +1409,7 @@ int graph_for(lfx_batch* B, int bps, cudaGraphExec_t* out) {
     cfg.numAttrs = B->cooperative ? 1 : 0;
     cudaGraph_t g = nullptr;
     LFX_CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = cudaMemsetAsync(B->d_bar, 0, 2 * sizeof(unsigned), ctx->stream);
+    cudaError_t e1 = cudaMemsetAsync(B->d_bar, 0, 4 * sizeof(unsigned), ctx->stream);
     cudaError_t e2 = cudaLaunchKernelExC(&cfg, k, args);
     cudaError_t e3 = cudaStreamEndCapture(ctx->stream, &g);
     cudaGraphExec_t ex = nullptr;
@@ -1499,7 +1517,7 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t reser
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_state, sizeof(BState) * max_slots);
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_tickets, sizeof(unsigned) * max_slots);
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_need, sizeof(int) * kMaxIters);
-  if (!rc) rc = dmalloc(ctx, (void**)&B->d_bar, sizeof(unsigned) * 2);
+  if (!rc) rc = dmalloc(ctx, (void**)&B->d_bar, sizeof(unsigned) * 4);
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_err, sizeof(int));
   if (!rc) rc = dmalloc(ctx, (void**)&B->d_params, sizeof(BParams));
   if (!rc && cudaMallocHost((void**)&B->h_state, sizeof(BState) * max_slots) != cudaSuccess)
@@ -1512,7 +1530,7 @@ int lfx_batch_create(lfx_ctx* ctx, int32_t ndf, int32_t max_slots, int64_t reser
     cudaMemsetAsync(B->d_state, 0, sizeof(BState) * max_slots, ctx->stream);
     cudaMemsetAsync(B->d_tickets, 0, sizeof(unsigned) * max_slots, ctx->stream);
     cudaMemsetAsync(B->d_need, 0, sizeof(int) * kMaxIters, ctx->stream);
-    cudaMemsetAsync(B->d_bar, 0, sizeof(unsigned) * 2, ctx->stream);
+    cudaMemsetAsync(B->d_bar, 0, sizeof(unsigned) * 4, ctx->stream);
     cudaMemsetAsync(B->d_err, 0, sizeof(int), ctx->stream);
     // memory returned by retired slots stays in the pool for the next ones
     cudaMemPool_t pool;
@@ -1562,7 +1580,7 @@ int lfx_batch_destroy(lfx_batch* B) {
   dfree(ctx, B->d_state, sizeof(BState) * B->max_slots);
   dfree(ctx, B->d_tickets, sizeof(unsigned) * B->max_slots);
   dfree(ctx, B->d_need, sizeof(int) * kMaxIters);
-  dfree(ctx, B->d_bar, sizeof(unsigned) * 2);
+  dfree(ctx, B->d_bar, sizeof(unsigned) * 4);
   dfree(ctx, B->d_err, sizeof(int));
   dfree(ctx, B->d_params, sizeof(BParams));
   if (B->h_state) cudaFreeHost(B->h_state);

@@ -1462,7 +1462,6 @@ int read_back(lfx_batch* B) {
   for (int s = 0; s < B->max_slots; ++s) {
     SlotHost& H = B->slots[s];
     if (!H.used) continue;
-    if (B->h_state[s].phase == PH_DONE && H.last_phase != PH_DONE) B->dirty = true;
     H.last_phase = B->h_state[s].phase;
   }
   return LFX_OK;
@@ -1735,9 +1734,17 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
 int lfx_batch_step(lfx_batch* B, int32_t* ndone) {
   if (!B) return LFX_INVALID_ARGUMENT;
   int rc = LFX_OK;
-  if (B->dirty) rc = rebuild(B);
+  // The work lists are rebuilt when slots were admitted (or the launch shape
+  // changed), and when fewer than two thirds of the slots they cover still
+  // run: every phase skips the items of a slot that is done or retired (its
+  // state on the device says so before its memory is freed), so a slot
+  // that finishes costs no rebuild.
+  int running = 0;
+  for (int s = 0; s < B->max_slots; ++s)
+    if (B->slots[s].used && B->slots[s].last_phase != PH_DONE) ++running;
+  if (B->dirty || 3 * running < 2 * B->nactive) rc = rebuild(B);
   if (rc) return rc;
-  if (B->nactive > 0) {
+  if (running > 0) {
     rc = replay(B);
     if (!rc) rc = read_back(B);
     if (rc) return rc;
@@ -1783,7 +1790,6 @@ int lfx_batch_retire(lfx_batch* B, int32_t slot) {
                               cudaMemcpyHostToDevice, ctx->stream));
   if (H.mem) LFX_CK(ctx, cudaFreeAsync(H.mem, ctx->stream));
   H = SlotHost();
-  B->dirty = true;
   return LFX_OK;
 }
 

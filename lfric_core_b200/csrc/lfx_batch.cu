@@ -544,6 +544,7 @@ __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4
     uint32_t flags = 0, prt = 0;
     double dot = 0.0;
     bool ok = true;
+    int jf = 0;  // the unit whose wait ran out
     for (int j = 0; j < nunit; ++j) {
       const int c = j / nseg, sg = j % nseg;
       if (sg == 0) {
@@ -569,6 +570,7 @@ __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4
       const unsigned g = seq + (unsigned)j, st = g % kRing;
       if (!ring_wait(bars + st, (g / kRing) & 1u, P.timeout_ns)) {
         ok = false;
+        jf = j;
         break;
       }
       // row sums of this lane's cell, four packed entries at a time: entry
@@ -616,13 +618,17 @@ __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4
       }
     }
     if (!ok) {
-      // record the time-out, then wait (bounded) for this warp's copies
-      // still in flight before the kernel leaves
+      // record the time-out, then wait (bounded: the batch's wait limit, at
+      // least 2 s, since a copy in flight lands within microseconds unless
+      // the memory system has stopped) for this warp's copies still in
+      // flight before the kernel leaves
       if (lane == 0) {
         atomicExch(P.err, (int)LFX_TIMEOUT);
-        for (int j = 0; j < nunit && j < kRing; ++j) {
+        const unsigned long long drain = P.timeout_ns > 2000000000ull ? P.timeout_ns : 2000000000ull;
+        // units jf .. jf + kRing - 1 were issued and not consumed
+        for (int j = jf; j < nunit && j < jf + kRing; ++j) {
           const unsigned g = seq + (unsigned)j;
-          ring_wait(bars + g % kRing, (g / kRing) & 1u, P.timeout_ns);
+          ring_wait(bars + g % kRing, (g / kRing) & 1u, drain);
         }
       }
       __syncwarp();
@@ -1218,6 +1224,10 @@ struct lfx_batch {
   lfx_ctx* ctx = nullptr;
   int ndf = 8, max_slots = 0, iters = 8;
   int64_t reserve = 0;
+  // free device memory (plus the pool's unused bytes) as last queried,
+  // less what admissions took since and plus what retirements gave back;
+  // -1: query again (each step starts a new reading)
+  int64_t avail = -1;
   BSlot* d_slots = nullptr;
   std::vector<BSlot> h_slots;
   BState* d_state = nullptr;
@@ -1633,7 +1643,8 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   // work lists, and the batch's reserve must fit
   const int64_t need = slot_bytes(n, nch, L->ncell_2d) + (int64_t)(op32->lmat ? 0 : op_level_major_bytes(op32));
   const int64_t lists = 16 * (2 * ((int64_t)L->ncell_2d / 32 + 8) + nch) + 8 * (cma ? prec32->ncell_2d : 0);
-  if (available_bytes(ctx) - need - 2 * lists < B->reserve)
+  if (B->avail < 0) B->avail = available_bytes(ctx);
+  if (B->avail - need - 2 * lists < B->reserve)
     return fail(ctx, LFX_OUT_OF_MEMORY, "batch: not enough free device memory for the solve");
   {
     const int rcl = op_level_major(op32);
@@ -1724,6 +1735,7 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
     return rc;
   }
   B->dirty = true;
+  B->avail -= need + 2 * lists;
   *slot_out = s;
   return LFX_OK;
 }
@@ -1739,6 +1751,7 @@ int lfx_batch_step(lfx_batch* B, int32_t* ndone) {
   // run: every phase skips the items of a slot that is done or retired (its
   // state on the device says so before its memory is freed), so a slot
   // that finishes costs no rebuild.
+  B->avail = -1;  // admissions after this step read free memory again
   int running = 0;
   for (int s = 0; s < B->max_slots; ++s)
     if (B->slots[s].used && B->slots[s].last_phase != PH_DONE) ++running;
@@ -1789,6 +1802,7 @@ int lfx_batch_retire(lfx_batch* B, int32_t slot) {
   LFX_CK(ctx, cudaMemcpyAsync(B->d_state + slot, &B->h_state[slot], sizeof(BState),
                               cudaMemcpyHostToDevice, ctx->stream));
   if (H.mem) LFX_CK(ctx, cudaFreeAsync(H.mem, ctx->stream));
+  if (B->avail >= 0) B->avail += (int64_t)H.mem_bytes;
   H = SlotHost();
   return LFX_OK;
 }

@@ -864,7 +864,8 @@ __device__ __forceinline__ void chunk_issue(const float* const (&src)[NA], int64
         "l"(src[a] + (size_t)row0 * kBS), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
-// the ring's set-up and its bounded drain after a time-out
+// the ring's set-up and its bounded drain after a time-out (chunks from..to-1:
+// the one whose wait ran out and those issued after it)
 template <int S>
 __device__ __forceinline__ void chunk_ring_init(uint64_t* bar) {
   if (threadIdx.x == 0) {
@@ -915,7 +916,7 @@ __global__ void __launch_bounds__(256) bcg_gram_s(int64_t n, const float* __rest
     const bool ok = chunk_wait(bar + stg, (unsigned)((i / S) & 1));
     if (!__syncthreads_and(ok)) {
       if (threadIdx.x == 0) st->fail = 2;
-      chunk_ring_drain<S>(bar, i + 1, nmine < i + S ? nmine : i + S);
+      chunk_ring_drain<S>(bar, i, nmine < i + S ? nmine : i + S);
       failed = true;
       break;
     }
@@ -1012,7 +1013,7 @@ __global__ void __launch_bounds__(256) bcg_update_s(int64_t n, const float* __re
     const bool ok = chunk_wait(bar + stg, (unsigned)((i / S) & 1));
     if (!__syncthreads_and(ok)) {
       if (threadIdx.x == 0) const_cast<BcgSmall*>(st)->fail = 2;
-      chunk_ring_drain<S>(bar, i + 1, nmine < i + S ? nmine : i + S);
+      chunk_ring_drain<S>(bar, i, nmine < i + S ? nmine : i + S);
       break;
     }
     const int64_t c = blockIdx.x + (int64_t)i * gridDim.x, row0 = c * kBcgRows;

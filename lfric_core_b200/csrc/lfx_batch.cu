@@ -503,7 +503,7 @@ __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4
                                                     int i0, int i1, unsigned char* ring,
                                                     uint64_t* bars, unsigned seq, unsigned* ctr) {
   using R = Ring<NDF>;
-  constexpr int NP = R::NP, NPV = R::NPV;
+  constexpr int NPV = R::NPV;
   const int lane = threadIdx.x & 31;
   // warps take items by the phase's counter (lane 0), the next one asked for
   // while the current item runs
@@ -1220,6 +1220,14 @@ struct SlotHost {
   int last_phase = PH_EMPTY;
 };
 
+// The work lists are expanded on the device from runs the host lays out: a
+// run is one slot's range [a, e) (cell columns of one colour, chunks, or
+// preconditioner columns) and the list index its entries start at, so a
+// rebuild uploads a few hundred runs instead of the lists themselves.
+struct ListRun {
+  int s, a, e, off;
+};
+
 struct lfx_batch {
   lfx_ctx* ctx = nullptr;
   int ndf = 8, max_slots = 0, iters = 8;
@@ -1235,6 +1243,8 @@ struct lfx_batch {
   unsigned* d_tickets = nullptr;
   int* d_need = nullptr;
   unsigned* d_bar = nullptr;
+  ListRun* d_runs = nullptr;
+  size_t cap_runs = 0;
   int* d_err = nullptr;
   int* h_err = nullptr;  // pinned
   BParams* d_params = nullptr;
@@ -1287,12 +1297,33 @@ const void* pick_kernel(int ndf, bool cma) {
   return cma ? kernel_ptr<6, true>() : kernel_ptr<6, false>();
 }
 
-// apply items of one precision: slots greedily grouped so that a group's
+// apply items {slot, first column, columns <= cb, 0} of each run
+__global__ void expand_items(const ListRun* __restrict__ runs, int nrun, int cb,
+                             int4* __restrict__ items) {
+  for (int r = blockIdx.x; r < nrun; r += gridDim.x) {
+    const ListRun R = runs[r];
+    const int n = (R.e - R.a + cb - 1) / cb;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int q = R.a + i * cb;
+      items[R.off + i] = make_int4(R.s, q, min(cb, R.e - q), 0);
+    }
+  }
+}
+// pairs {slot, k} for k in each run's range
+__global__ void expand_pairs(const ListRun* __restrict__ runs, int nrun, int2* __restrict__ out) {
+  for (int r = blockIdx.x; r < nrun; r += gridDim.x) {
+    const ListRun R = runs[r];
+    for (int i = threadIdx.x; i < R.e - R.a; i += blockDim.x) out[R.off + i] = make_int2(R.s, R.a + i);
+  }
+}
+
+// apply item runs of one precision: slots greedily grouped so that a group's
 // vectors (bytes_per_dof per dof) stay within group_bytes; per group and
-// colour the slots' runs of cells_per_item cell columns
-void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int ncolour,
-                       int bytes_per_dof, std::vector<int4>& items, std::vector<int>& off) {
-  items.clear();
+// colour the slots' runs of cells_per_item cell columns. Returns the number
+// of items; off receives each (group, colour)'s first item
+int64_t build_apply_runs(const lfx_batch* B, const std::vector<int>& act, int ncolour,
+                         int bytes_per_dof, std::vector<ListRun>& runs, std::vector<int>& off) {
+  runs.clear();
   off.clear();
   std::vector<std::vector<int>> groups;
   int64_t acc = 0;
@@ -1306,19 +1337,21 @@ void build_apply_items(const lfx_batch* B, const std::vector<int>& act, int ncol
     acc += b;
   }
   const int cb = B->cells_per_item;
+  int64_t n = 0;
   for (auto& g : groups)
     for (int c = 0; c < ncolour; ++c) {
-      off.push_back((int)items.size());
+      off.push_back((int)n);
       for (int s : g) {
         const SlotHost& H = B->slots[s];
         if (c + 1 >= (int)H.cstart.size()) continue;
         const int a = H.cstart[c], e = H.cstart[c + 1];
-        for (int q = a; q < e; q += cb) {
-          items.push_back(make_int4(s, q, std::min(cb, e - q), 0));
-        }
+        if (e <= a) continue;
+        runs.push_back(ListRun{s, a, e, (int)n});
+        n += (e - a + cb - 1) / cb;
       }
     }
-  off.push_back((int)items.size());
+  off.push_back((int)n);
+  return n;
 }
 
 int rebuild(lfx_batch* B) {
@@ -1336,31 +1369,65 @@ int rebuild(lfx_batch* B) {
   // colour phases: as many as the slot with the most colours has
   int ncolour = 1;
   for (int s : act) ncolour = std::max(ncolour, (int)B->slots[s].cstart.size() - 1);
-  std::vector<int4> it32, it64;
+  std::vector<ListRun> r32, r64, rch, rcol;
   std::vector<int> off32, off64;
-  build_apply_items(B, act, ncolour, 8, it32, off32);
-  build_apply_items(B, act, ncolour, 16, it64, off64);
-  std::vector<int2> ch, col;
+  const int64_t n32 = build_apply_runs(B, act, ncolour, 8, r32, off32);
+  const int64_t n64 = build_apply_runs(B, act, ncolour, 16, r64, off64);
+  int64_t nch = 0, ncol = 0;
   for (int s : act) {
     const SlotHost& H = B->slots[s];
-    for (int c = 0; c < H.nch; ++c) ch.push_back(make_int2(s, c));
-    if (H.cma)
-      for (int c = 0; c < H.ncol; ++c) col.push_back(make_int2(s, c));
+    rch.push_back(ListRun{s, 0, H.nch, (int)nch});
+    nch += H.nch;
+    if (H.cma && H.ncol > 0) {
+      rcol.push_back(ListRun{s, 0, H.ncol, (int)ncol});
+      ncol += H.ncol;
+    }
   }
-  int rc = grow(ctx, &B->d_items32, &B->cap_items32, it32.size());
-  if (!rc) rc = grow(ctx, &B->d_items64, &B->cap_items64, it64.size());
+  // one upload of all runs: apply32, apply64, chunks, columns
+  std::vector<ListRun> runs;
+  runs.reserve(r32.size() + r64.size() + rch.size() + rcol.size());
+  runs.insert(runs.end(), r32.begin(), r32.end());
+  runs.insert(runs.end(), r64.begin(), r64.end());
+  runs.insert(runs.end(), rch.begin(), rch.end());
+  runs.insert(runs.end(), rcol.begin(), rcol.end());
+  int rc = grow(ctx, &B->d_items32, &B->cap_items32, (size_t)n32);
+  if (!rc) rc = grow(ctx, &B->d_items64, &B->cap_items64, (size_t)n64);
   if (!rc) rc = grow(ctx, &B->d_off32, &B->cap_off32, off32.size());
   if (!rc) rc = grow(ctx, &B->d_off64, &B->cap_off64, off64.size());
-  if (!rc) rc = grow(ctx, &B->d_chunks, &B->cap_chunks, ch.size());
-  if (!rc) rc = grow(ctx, &B->d_cols, &B->cap_cols, col.size());
+  if (!rc) rc = grow(ctx, &B->d_chunks, &B->cap_chunks, (size_t)nch);
+  if (!rc) rc = grow(ctx, &B->d_cols, &B->cap_cols, (size_t)ncol);
+  if (!rc) rc = grow(ctx, &B->d_runs, &B->cap_runs, runs.size());
   if (rc) return rc;
-  rc = upload(ctx, B->d_items32, it32);
-  if (!rc) rc = upload(ctx, B->d_items64, it64);
-  if (!rc) rc = upload(ctx, B->d_off32, off32);
+  rc = upload(ctx, B->d_off32, off32);
   if (!rc) rc = upload(ctx, B->d_off64, off64);
-  if (!rc) rc = upload(ctx, B->d_chunks, ch);
-  if (!rc) rc = upload(ctx, B->d_cols, col);
+  if (!rc) rc = upload(ctx, B->d_runs, runs);
   if (rc) return rc;
+  {
+    const ListRun* d = B->d_runs;
+    const int g = ctx->num_sms * 4;
+    int nl = 0;
+    if (!r32.empty()) {
+      expand_items<<<g, 256, 0, ctx->stream>>>(d, (int)r32.size(), B->cells_per_item, B->d_items32);
+      ++nl;
+    }
+    d += r32.size();
+    if (!r64.empty()) {
+      expand_items<<<g, 256, 0, ctx->stream>>>(d, (int)r64.size(), B->cells_per_item, B->d_items64);
+      ++nl;
+    }
+    d += r64.size();
+    if (!rch.empty()) {
+      expand_pairs<<<g, 256, 0, ctx->stream>>>(d, (int)rch.size(), B->d_chunks);
+      ++nl;
+    }
+    d += rch.size();
+    if (!rcol.empty()) {
+      expand_pairs<<<g, 256, 0, ctx->stream>>>(d, (int)rcol.size(), B->d_cols);
+      ++nl;
+    }
+    ctx->launches += nl;
+    LFX_CK(ctx, cudaGetLastError());
+  }
   rc = grow(ctx, &B->d_slotlist, &B->cap_slotlist, act.size());
   if (!rc) rc = upload(ctx, B->d_slotlist, act);
   if (rc) return rc;
@@ -1383,8 +1450,8 @@ int rebuild(lfx_batch* B) {
   P.ngr32 = (int)(off32.size() - 1) / ncolour;
   P.ngr64 = (int)(off64.size() - 1) / ncolour;
   P.ncolour = ncolour;
-  P.nchunk = (int)ch.size();
-  P.ncolitem = (int)col.size();
+  P.nchunk = (int)nch;
+  P.ncolitem = (int)ncol;
   P.iters = B->iters;
   P.max_slots = B->max_slots;
   P.any_cma = any_cma ? 1 : 0;
@@ -1582,7 +1649,7 @@ int lfx_batch_destroy(lfx_batch* B) {
   for (auto& H : B->slots)
     if (H.mem) cudaFreeAsync(H.mem, ctx->stream);
   for (void* p : {(void*)B->d_items32, (void*)B->d_items64, (void*)B->d_off32, (void*)B->d_off64,
-                  (void*)B->d_chunks, (void*)B->d_cols, (void*)B->d_slotlist})
+                  (void*)B->d_chunks, (void*)B->d_cols, (void*)B->d_slotlist, (void*)B->d_runs})
     if (p) cudaFreeAsync(p, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   dfree(ctx, B->d_slots, sizeof(BSlot) * B->max_slots);

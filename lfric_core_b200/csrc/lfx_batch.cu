@@ -69,15 +69,19 @@ constexpr int kBSub = 8;         // a chunk item: kBSub chunks of RCHUNK values 
 constexpr int kMaxIters = 64;    // super-iterations per launch, at most
 constexpr int kMaxSeg = 4;       // warps (segments of <= 31 levels) per cell column, at most
 constexpr int kMaxColours = 8;   // cell colours of a slot, at most
-constexpr int kBCols = 64;       // columns per sweep item
 constexpr int kBRows = 160;      // rows per preconditioner column, at most
-// column sweeps: a sweeping thread's factor ring, kFq chunks of kFr rows of
-// (finv, fa) (the backward sweep reuses it for fc)
-constexpr int kFr = 8, kFq = 4;
-// shared memory of the sweeps: the staged rows, then the sweeping threads'
-// factor rings
-constexpr size_t kSweepRows = sizeof(float) * kBRows * (kBCols + 1);
-constexpr size_t kSweepBytes = kSweepRows + sizeof(float) * kBCols * kFq * kFr * 2;
+// column sweeps: a warp's 32 columns move in chunks of kSwCh rows through a
+// tile of kSwLd-float rows, beside the warp's table of its columns
+constexpr int kSwCh = 8;                      // rows per chunk
+constexpr int kSwLd = 33;                     // tile row stride (floats)
+struct SweepCol {                             // a warp's columns, per lane
+  const int* ind[32];
+  const float* r[32];
+  float* z[32];
+  int f[32], nrow[32];
+};
+constexpr size_t kSweepWarpBytes = sizeof(float) * kSwCh * kSwLd + sizeof(SweepCol);
+constexpr size_t kSweepBytes = kBW * kSweepWarpBytes;
 
 inline int64_t bchunks(int64_t n) {
   return (n + (int64_t)kBSub * RCHUNK - 1) / ((int64_t)kBSub * RCHUNK);
@@ -825,146 +829,105 @@ __device__ __noinline__ void vec_phase(const BParams& P, BShared& sh, Pred pred,
   }
 }
 
-// 4-byte asynchronous copy global -> shared (read-only data)
-__device__ __forceinline__ void cp4(float* dst, const float* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
-                   (unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
-
-// Column sweeps of the line preconditioner for running slots: z = T^{-1} r on
-// the rows of 64 consecutive list items (columns of any slots), staged in
-// shared memory (one warp copies a column's contiguous rows in and out, one
-// thread sweeps a column with the factors read coalesced from [row][column]);
-// the arithmetic of thomas_sweep.
-struct SweepShared {
-  int nrow[kBCols], f[kBCols], maxrow;
-  const int* ind[kBCols];
-  const float* r[kBCols];
-  float* z[kBCols];
-};
-
-__device__ __noinline__ void sweep_phase(const BParams& P, float* xs, SweepShared& ss) {
-  constexpr int LD = kBCols + 1, CPW = kBCols / kBW;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int u0 = blockIdx.x * kBCols; u0 < P.ncolitem; u0 += gridDim.x * kBCols) {
-    __syncthreads();
-    if (threadIdx.x == 0) ss.maxrow = 0;
-    __syncthreads();
-    if (threadIdx.x < kBCols) {
-      const int t = threadIdx.x, u = u0 + t;
-      int nrow = 0;
-      if (u < P.ncolitem) {
-        const int2 w = __ldg(P.cols + u);
-        if (ph_run(__ldcg(&P.st[w.x].phase))) {
-          // slot records are read-only during a launch
-          const BSlot* D = P.slots + w.x;
-          nrow = D->nrow;
-          ss.f[t] = __ldg(D->first + w.y);
-          ss.ind[t] = D->ind;
-          ss.r[t] = D->r;
-          ss.z[t] = D->z;
-        }
-      }
-      ss.nrow[t] = nrow;
-      atomicMax(&ss.maxrow, nrow);
-    }
-    __syncthreads();
-    const int maxrow = ss.maxrow;
-    for (int r0 = 0; r0 < maxrow; r0 += 32) {
-      const int i = r0 + lane;
-      float v[CPW];
-#pragma unroll
-      for (int k = 0; k < CPW; ++k) {
-        const int j = warp + kBW * k;
-        v[k] = i < ss.nrow[j] ? __ldcg(ss.r[j] + ss.f[j] + __ldg(ss.ind[j] + i)) : 0.0f;
-      }
-#pragma unroll
-      for (int k = 0; k < CPW; ++k) {
-        const int j = warp + kBW * k;
-        if (i < ss.nrow[j]) xs[i * LD + j] = v[k];
+// Column sweeps, one warp per 32 consecutive list columns (one column a
+// lane, any slots), no block barrier: rows move in chunks of kSwCh through a
+// per-warp tile in shared memory (a column's rows are read and written as
+// one coalesced run, kSwCh lanes a column), the factors come straight from
+// [row][column] (coalesced across the lanes of one slot). The forward sweep
+// leaves its values in z (FP32), the backward sweep reads them back; the
+// arithmetic of thomas_sweep (FP64 carries, FP32 rows between the sweeps).
+__device__ __noinline__ void sweep_phase_w(const BParams& P, unsigned char* wsm) {
+  float (*tile)[kSwLd] = reinterpret_cast<float (*)[kSwLd]>(wsm);
+  SweepCol& sc = *reinterpret_cast<SweepCol*>(wsm + sizeof(float) * kSwCh * kSwLd);
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kBW + (threadIdx.x >> 5), nw = gridDim.x * kBW;
+  for (int u0 = gw * 32; u0 < P.ncolitem; u0 += nw * 32) {
+    // this lane's column
+    const int u = u0 + lane;
+    int nrow = 0, nc = 1, c = 0;
+    const float *fa = nullptr, *finv = nullptr, *fc = nullptr;
+    __syncwarp();
+    sc.nrow[lane] = 0;
+    if (u < P.ncolitem) {
+      const int2 w = __ldg(P.cols + u);
+      if (ph_run(__ldcg(&P.st[w.x].phase))) {
+        const BSlot& D = P.slots[w.x];
+        nrow = D.nrow;
+        nc = D.ncol;
+        c = w.y;
+        fa = D.fa;
+        finv = D.finv;
+        fc = D.fc;
+        sc.ind[lane] = D.ind;
+        sc.r[lane] = D.r;
+        sc.z[lane] = D.z;
+        sc.f[lane] = __ldg(D.first + w.y);
+        sc.nrow[lane] = nrow;
       }
     }
-    __syncthreads();
-    const int j = threadIdx.x;
-    if (j < kBCols && ss.nrow[j] > 0) {
-      const int2 w = __ldg(P.cols + u0 + j);
-      const BSlot* D = P.slots + w.x;
-      const int nrow = ss.nrow[j], nc = D->ncol, c = w.y;
-      const float *fa = D->fa, *finv = D->finv, *fc = D->fc;
-      float* col = xs + j;
-      // this thread's factor ring: kFq chunks of kFr rows, kFq - 1 chunks in
-      // flight while it works on one (one cp.async group per chunk, empty
-      // past the column's end, so the wait counts stay uniform)
-      float* fr = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(xs) + kSweepRows) +
-                  j * (kFq * kFr * 2);
-      const int nchk = (nrow + kFr - 1) / kFr;
-      auto fwd_chunk = [&](int ch) {
-        float* dst = fr + (ch % kFq) * (kFr * 2);
+    int maxrow = nrow;
 #pragma unroll
-        for (int q = 0; q < kFr; ++q) {
-          const int i = ch * kFr + q;
-          if (ch < nchk && i < nrow) {
-            cp4(dst + 2 * q, finv + (size_t)i * nc + c);
-            cp4(dst + 2 * q + 1, fa + (size_t)i * nc + c);
-          }
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-      };
-      double d = 0.0;
-      for (int ch = 0; ch < kFq - 1; ++ch) fwd_chunk(ch);
-      for (int ch = 0; ch < nchk; ++ch) {
-        fwd_chunk(ch + kFq - 1);
-        asm volatile("cp.async.wait_group %0;" ::"n"(kFq - 1) : "memory");
-        const float* src = fr + (ch % kFq) * (kFr * 2);
+    for (int o = 16; o > 0; o >>= 1) maxrow = max(maxrow, __shfl_xor_sync(0xffffffffu, maxrow, o));
+    __syncwarp();
+    if (maxrow == 0) continue;
+    // staging: lane = (column offset, row in the chunk); 32 / kSwCh columns
+    // an instruction
+    constexpr int CPI = 32 / kSwCh;
+    const int hr = lane % kSwCh, hc = lane / kSwCh;
+    // forward: d_i = finv_i (r_i - fa_i d_{i-1}), left in z
+    double d = 0.0;
+    for (int i0 = 0; i0 < maxrow; i0 += kSwCh) {
+      const int i = i0 + hr;
+      for (int j = hc; j < 32; j += CPI)
+        if (i < sc.nrow[j]) tile[hr][j] = __ldcg(sc.r[j] + sc.f[j] + __ldg(sc.ind[j] + i));
+      float iv[kSwCh], av[kSwCh];
 #pragma unroll
-        for (int q = 0; q < kFr; ++q) {
-          const int i = ch * kFr + q;
-          if (i < nrow) {
-            const double xv = (double)col[i * LD];
-            const double iv = (double)src[2 * q], av = (double)src[2 * q + 1];
-            d = (i == 0) ? iv * xv : iv * fma(-av, d, xv);
-            col[i * LD] = (float)d;
-          }
+      for (int q = 0; q < kSwCh; ++q) {
+        const int ii = i0 + q;
+        iv[q] = ii < nrow ? __ldg(finv + (size_t)ii * nc + c) : 0.f;
+        av[q] = ii < nrow ? __ldg(fa + (size_t)ii * nc + c) : 0.f;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < kSwCh; ++q) {
+        const int ii = i0 + q;
+        if (ii < nrow) {
+          const double xv = (double)tile[q][lane];
+          d = (ii == 0) ? (double)iv[q] * xv : (double)iv[q] * fma(-(double)av[q], d, xv);
+          tile[q][lane] = (float)d;
         }
       }
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
-      // backward: rows nrow - 2 down to 0 in chunks of kFr (fc only)
-      const int nb = nrow - 1, nbch = (nb + kFr - 1) / kFr;
-      auto bwd_chunk = [&](int ch) {
-        float* dst = fr + (ch % kFq) * (kFr * 2);
-#pragma unroll
-        for (int q = 0; q < kFr; ++q) {
-          const int i = nrow - 2 - (ch * kFr + q);
-          if (ch < nbch && i >= 0) cp4(dst + q, fc + (size_t)i * nc + c);
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-      };
-      for (int ch = 0; ch < kFq - 1; ++ch) bwd_chunk(ch);
-      for (int ch = 0; ch < nbch; ++ch) {
-        bwd_chunk(ch + kFq - 1);
-        asm volatile("cp.async.wait_group %0;" ::"n"(kFq - 1) : "memory");
-        const float* src = fr + (ch % kFq) * (kFr * 2);
-#pragma unroll
-        for (int q = 0; q < kFr; ++q) {
-          const int i = nrow - 2 - (ch * kFr + q);
-          if (i >= 0) {
-            d = fma(-(double)src[q], d, (double)col[i * LD]);
-            col[i * LD] = (float)d;
-          }
-        }
-      }
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      __syncwarp();
+      for (int j = hc; j < 32; j += CPI)
+        if (i < sc.nrow[j]) __stcg(sc.z[j] + sc.f[j] + __ldg(sc.ind[j] + i), tile[hr][j]);
+      __syncwarp();
     }
-    __syncthreads();
-    for (int r0 = 0; r0 < maxrow; r0 += 32) {
-      const int i = r0 + lane;
+    // backward: z_i = d_i - fc_i z_{i+1}, rows nrow - 2 .. 0, chunks from the top
+    for (int i0 = ((maxrow - 1) / kSwCh) * kSwCh; i0 >= 0; i0 -= kSwCh) {
+      const int i = i0 + hr;
+      for (int j = hc; j < 32; j += CPI)
+        if (i < sc.nrow[j]) tile[hr][j] = __ldcg(sc.z[j] + sc.f[j] + __ldg(sc.ind[j] + i));
+      float cv[kSwCh];
 #pragma unroll
-      for (int k = 0; k < CPW; ++k) {
-        const int jj = warp + kBW * k;
-        if (i < ss.nrow[jj]) __stcg(ss.z[jj] + ss.f[jj] + __ldg(ss.ind[jj] + i), xs[i * LD + jj]);
+      for (int q = 0; q < kSwCh; ++q) {
+        const int ii = i0 + q;
+        cv[q] = ii < nrow - 1 ? __ldg(fc + (size_t)ii * nc + c) : 0.f;
       }
+      __syncwarp();
+#pragma unroll
+      for (int q = kSwCh - 1; q >= 0; --q) {
+        const int ii = i0 + q;
+        if (ii == nrow - 1) {
+          d = (double)tile[q][lane];
+        } else if (ii < nrow - 1) {
+          d = fma(-(double)cv[q], d, (double)tile[q][lane]);
+          tile[q][lane] = (float)d;
+        }
+      }
+      __syncwarp();
+      for (int j = hc; j < 32; j += CPI)
+        if (i < sc.nrow[j]) __stcg(sc.z[j] + sc.f[j] + __ldg(sc.ind[j] + i), tile[hr][j]);
+      __syncwarp();
     }
   }
 }
@@ -974,10 +937,9 @@ template <class T> struct W5 { T a, b, c, d, e; };
 // The persistent kernel: `iters` super-iterations of every admitted slot.
 template <int NDF, bool CMA>
 __global__ void __launch_bounds__(kBT, kMaxBps) batch_kernel(const BParams* __restrict__ PP) {
-  // the apply rings, or the column sweeps' staging, then the ring mbarriers
+  // the apply rings, or the column sweeps' tiles, then the ring mbarriers
   // (dyn_bytes(NDF))
   extern __shared__ __align__(16) unsigned char dyn_smem[];
-  float* sweep_smem = reinterpret_cast<float*>(dyn_smem);
   unsigned char* ring = dyn_smem + (size_t)(threadIdx.x >> 5) * Ring<NDF>::WARP;
   uint64_t* bars = reinterpret_cast<uint64_t*>(dyn_smem + ring_bar_offset(NDF)) +
                    (threadIdx.x >> 5) * kRing;
@@ -990,7 +952,6 @@ __global__ void __launch_bounds__(kBT, kMaxBps) batch_kernel(const BParams* __re
   int aph = 0;       // FP32 apply phases run so far in this launch
   __shared__ BShared sh;
   __shared__ BParams sp;
-  __shared__ SweepShared ss;
   {
     const int* src = reinterpret_cast<const int*>(PP);
     int* dst = reinterpret_cast<int*>(&sp);
@@ -1145,7 +1106,7 @@ __global__ void __launch_bounds__(kBT, kMaxBps) batch_kernel(const BParams* __re
     }
     // ---- C: column sweeps, then the Jacobi rows with <r, z> and beta
     if (CMA && P.any_cma) {
-      sweep_phase(P, sweep_smem, ss);
+      sweep_phase_w(P, dyn_smem + (size_t)(threadIdx.x >> 5) * kSweepWarpBytes);
       if (!grid_sync(P, sh)) return;
       vec_phase<1>(
           P, sh, [](int ph, int) { return ph_run(ph); },

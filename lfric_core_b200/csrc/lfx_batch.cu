@@ -99,6 +99,7 @@ struct BSlot {
   int32_t sblk32, sblk64, cdints, nl;
   int32_t nseg, segL, nch, ncell;
   int32_t npv, cma, ncol, nrow;
+  int32_t canon, pad1;  // canon: every cell has the space's reference pair structure
   int64_t n;
   double* part;  // [0, 2 nch): chunk sums; [2 nch, 2 nch + ncell): <p, z> per cell column
   // preconditioner: FP32 Jacobi diagonal (zero on the column rows of a
@@ -422,6 +423,29 @@ __device__ __noinline__ void apply_phase(const BParams& P, const int4* __restric
 // and returns; the kernel leaves at its next grid barrier.
 constexpr int kRing = 2;  // ring stages per warp
 
+// The vertical-pair structure of the reference elements (dof bit masks of
+// the lower and upper records of each pair, and each lower dof's partner in
+// its nibble): W0, bottom vertices 0-3 below top vertices 4-7; W2, the bottom
+// face 4 below the top face 5
+template <int NDF>
+struct Canon;
+template <>
+struct Canon<8> {
+  static constexpr uint32_t lower = 0x0Fu, upper = 0xF0u, part = 0x7654u;
+};
+template <>
+struct Canon<6> {
+  static constexpr uint32_t lower = 0x10u, upper = 0x20u, part = 0x50000u;
+};
+// the same in the descriptors' flag layout (bits 8-15 lower, 16-23 upper)
+__host__ __device__ constexpr uint32_t canon_flags(int ndf) {
+  return ndf == 8 ? ((Canon<8>::lower << 8) | (Canon<8>::upper << 16))
+                  : ((Canon<6>::lower << 8) | (Canon<6>::upper << 16));
+}
+__host__ __device__ constexpr uint32_t canon_part(int ndf) {
+  return ndf == 8 ? Canon<8>::part : Canon<6>::part;
+}
+
 template <int NDF>
 struct Ring {
   static constexpr int NP = NDF * (NDF + 1) / 2, NPV = (NP + 3) / 4;
@@ -502,12 +526,150 @@ __device__ __forceinline__ void row_sums(const float4* Ms, bool v, const float (
   }
 }
 
+// the vertical-pair tests of a descriptor, as compile-time constants for a
+// slot with its space's reference structure (CANON)
+template <int NDF, bool CANON>
+__device__ __forceinline__ bool is_lower(uint32_t flags, int df) {
+  return CANON ? ((Canon<NDF>::lower >> df) & 1u) : ((flags >> (8 + df)) & 1u);
+}
+template <int NDF, bool CANON>
+__device__ __forceinline__ bool is_upper(uint32_t flags, int df) {
+  return CANON ? ((Canon<NDF>::upper >> df) & 1u) : ((flags >> (16 + df)) & 1u);
+}
+template <int NDF, bool CANON>
+__device__ __forceinline__ int partner(uint32_t prt, int df) {
+  return CANON ? (int)((Canon<NDF>::part >> (4 * df)) & 15u) : (int)((prt >> (4 * df)) & 15u);
+}
+
+// one apply item (nq cell columns from q0 of slot record D) through the
+// warp's ring; false when a ring wait ran out (recorded and drained)
+template <int NDF, bool CANON>
+__device__ __forceinline__ bool ring_item(const BParams& P, const BSlot& D, int q0, int nq,
+                                          unsigned char* ring, uint64_t* bars, unsigned& seq,
+                                          int lane) {
+  using R = Ring<NDF>;
+  constexpr int NPV = R::NPV;
+  const float4* M4 = D.L32;
+  const int* cdesc = D.cdesc;
+  const int cdints = D.cdints, nl = D.nl, nseg = D.nseg, L = D.segL;
+  const float* x = D.p;
+  float* y = D.z;
+  double* part = D.part + 2 * (int64_t)D.nch;
+  const int nunit = nq * nseg;
+  // unit j: column j / nseg, segment j % nseg; its levels kf..kl land at
+  // ring slot (level - (sg L - 1)), so lane l finds level sg L + l - 1
+  auto issue = [&](int j) {
+    const int c = j / nseg, sg = j % nseg;
+    const int kf = max(sg * L - 1, 0), kl = min(sg * L + L - 1, nl - 1);
+    const unsigned st = (seq + (unsigned)j) % kRing;
+    ring_issue(ring + st * R::STAGE + (kf - (sg * L - 1)) * R::LEVEL,
+               M4 + ((size_t)(q0 + c) * nl + kf) * NPV, (unsigned)(kl - kf + 1) * R::LEVEL,
+               bars + st);
+  };
+  if (lane == 0)
+    for (int j = 0; j < kRing && j < nunit; ++j) issue(j);
+  int mf[NDF];
+  uint32_t flags = 0, prt = 0;
+  double dot = 0.0;
+  bool ok = true;
+  int jf = 0;  // the unit whose wait ran out
+  for (int j = 0; j < nunit; ++j) {
+    const int c = j / nseg, sg = j % nseg;
+    if (sg == 0) {
+      const int* dsc = cdesc + (size_t)(q0 + c) * cdints;
+#pragma unroll
+      for (int jj = 0; jj < NDF; ++jj) mf[jj] = __ldg(dsc + jj);
+      flags = (uint32_t)__ldg(dsc + NDF);
+      prt = (uint32_t)__ldg(dsc + NDF + 1);
+    }
+    const int k = sg * L + lane - 1;
+    const bool own = lane >= 1 && lane <= L;
+    const bool v = k >= 0 && k < nl && lane <= L;
+    float xv[NDF], yo[NDF];
+#pragma unroll
+    for (int jj = 0; jj < NDF; ++jj) xv[jj] = v ? __ldcg(x + mf[jj] + k) : 0.f;
+#pragma unroll
+    for (int df = 0; df < NDF; ++df) {
+      const bool lower = is_lower<NDF, CANON>(flags, df), upper = is_upper<NDF, CANON>(flags, df);
+      const bool opens = (flags >> df) & 1u;
+      const bool live = own && (lower ? k <= nl : v);
+      yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + k) : 0.f;
+    }
+    const unsigned g = seq + (unsigned)j, st = g % kRing;
+    if (!ring_wait(bars + st, (g / kRing) & 1u, P.timeout_ns)) {
+      ok = false;
+      jf = j;
+      break;
+    }
+    // row sums of this lane's cell, four packed entries at a time: entry
+    // (a, b), a <= b, adds to row a (times x_b) and, mirrored, to row b
+    float rs[NDF];
+#pragma unroll
+    for (int df = 0; df < NDF; ++df) rs[df] = 0.f;
+    row_sums<NDF, 0>(reinterpret_cast<const float4*>(ring + st * R::STAGE) + lane * NPV, v, xv, rs);
+    // every lane has read the stage: it takes unit j + kRing
+    __syncwarp();
+    if (lane == 0 && j + kRing < nunit) issue(j + kRing);
+#pragma unroll
+    for (int df = 0; df < NDF; ++df) {
+      if (is_upper<NDF, CANON>(flags, df)) continue;  // upper record: summed with its lower one
+      const bool last = (flags >> (24 + df)) & 1u;
+      if (is_lower<NDF, CANON>(flags, df)) {
+        const int bsel = partner<NDF, CANON>(prt, df);
+#pragma unroll
+        for (int bb = df + 1; bb < NDF; ++bb) {
+          if (bb != bsel) continue;
+          const float below = __shfl_up_sync(0xffffffffu, rs[bb], 1);
+          float acc = yo[df] + rs[df];
+          if (own && k >= 1 && k <= nl) acc = acc + below;
+          if (own && k <= nl) {
+            const int row = mf[df] + k;
+            __stcg(y + row, acc);
+            if (last) {
+              const float pr = k < nl ? xv[df] : __ldcg(x + row);
+              dot = fma((double)pr, (double)acc, dot);
+            }
+          }
+        }
+      } else {
+        const float acc = yo[df] + rs[df];
+        if (own && v) {
+          __stcg(y + mf[df] + k, acc);
+          if (last) dot = fma((double)xv[df], (double)acc, dot);
+        }
+      }
+    }
+    if (sg == nseg - 1) {
+      const double w = warp_butterfly(dot);
+      if (lane == 0) __stcg(part + q0 + c, w);
+      dot = 0.0;
+    }
+  }
+  if (!ok) {
+    // record the time-out, then wait (bounded: the batch's wait limit, at
+    // least 2 s, since a copy in flight lands within microseconds unless
+    // the memory system has stopped) for this warp's copies still in
+    // flight before the kernel leaves
+    if (lane == 0) {
+      atomicExch(P.err, (int)LFX_TIMEOUT);
+      const unsigned long long drain = P.timeout_ns > 2000000000ull ? P.timeout_ns : 2000000000ull;
+      // units jf .. jf + kRing - 1 were issued and not consumed
+      for (int j = jf; j < nunit && j < jf + kRing; ++j) {
+        const unsigned g = seq + (unsigned)j;
+        ring_wait(bars + g % kRing, (g / kRing) & 1u, drain);
+      }
+    }
+    __syncwarp();
+    return false;
+  }
+  seq += (unsigned)nunit;
+  return true;
+}
+
 template <int NDF>
 __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4* __restrict__ items,
                                                     int i0, int i1, unsigned char* ring,
                                                     uint64_t* bars, unsigned seq, unsigned* ctr) {
-  using R = Ring<NDF>;
-  constexpr int NPV = R::NPV;
   const int lane = threadIdx.x & 31;
   // warps take items by the phase's counter (lane 0), the next one asked for
   // while the current item runs
@@ -525,120 +687,9 @@ __device__ __noinline__ unsigned apply_phase32_ring(const BParams& P, const int4
       continue;
     }
     const BSlot& D = P.slots[s];
-    const float4* M4 = D.L32;
-    const int* cdesc = D.cdesc;
-    const int cdints = D.cdints, nl = D.nl, nseg = D.nseg, L = D.segL;
-    const float* x = D.p;
-    float* y = D.z;
-    double* part = D.part + 2 * (int64_t)D.nch;
-    const int q0 = it.y, nq = it.z, nunit = nq * nseg;
-    // unit j: column j / nseg, segment j % nseg; its levels kf..kl land at
-    // ring slot (level - (sg L - 1)), so lane l finds level sg L + l - 1
-    auto issue = [&](int j) {
-      const int c = j / nseg, sg = j % nseg;
-      const int kf = max(sg * L - 1, 0), kl = min(sg * L + L - 1, nl - 1);
-      const unsigned st = (seq + (unsigned)j) % kRing;
-      ring_issue(ring + st * R::STAGE + (kf - (sg * L - 1)) * R::LEVEL,
-                 M4 + ((size_t)(q0 + c) * nl + kf) * NPV, (unsigned)(kl - kf + 1) * R::LEVEL,
-                 bars + st);
-    };
-    if (lane == 0)
-      for (int j = 0; j < kRing && j < nunit; ++j) issue(j);
-    int mf[NDF];
-    uint32_t flags = 0, prt = 0;
-    double dot = 0.0;
-    bool ok = true;
-    int jf = 0;  // the unit whose wait ran out
-    for (int j = 0; j < nunit; ++j) {
-      const int c = j / nseg, sg = j % nseg;
-      if (sg == 0) {
-        const int* dsc = cdesc + (size_t)(q0 + c) * cdints;
-#pragma unroll
-        for (int jj = 0; jj < NDF; ++jj) mf[jj] = __ldg(dsc + jj);
-        flags = (uint32_t)__ldg(dsc + NDF);
-        prt = (uint32_t)__ldg(dsc + NDF + 1);
-      }
-      const int k = sg * L + lane - 1;
-      const bool own = lane >= 1 && lane <= L;
-      const bool v = k >= 0 && k < nl && lane <= L;
-      float xv[NDF], yo[NDF];
-#pragma unroll
-      for (int jj = 0; jj < NDF; ++jj) xv[jj] = v ? __ldcg(x + mf[jj] + k) : 0.f;
-#pragma unroll
-      for (int df = 0; df < NDF; ++df) {
-        const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
-        const bool opens = (flags >> df) & 1u;
-        const bool live = own && (lower ? k <= nl : v);
-        yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + k) : 0.f;
-      }
-      const unsigned g = seq + (unsigned)j, st = g % kRing;
-      if (!ring_wait(bars + st, (g / kRing) & 1u, P.timeout_ns)) {
-        ok = false;
-        jf = j;
-        break;
-      }
-      // row sums of this lane's cell, four packed entries at a time: entry
-      // (a, b), a <= b, adds to row a (times x_b) and, mirrored, to row b
-      float rs[NDF];
-#pragma unroll
-      for (int df = 0; df < NDF; ++df) rs[df] = 0.f;
-      row_sums<NDF, 0>(reinterpret_cast<const float4*>(ring + st * R::STAGE) + lane * NPV, v, xv, rs);
-      // every lane has read the stage: it takes unit j + kRing
-      __syncwarp();
-      if (lane == 0 && j + kRing < nunit) issue(j + kRing);
-#pragma unroll
-      for (int df = 0; df < NDF; ++df) {
-        if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
-        const bool last = (flags >> (24 + df)) & 1u;
-        if ((flags >> (8 + df)) & 1u) {
-          const int bsel = (prt >> (4 * df)) & 15u;
-#pragma unroll
-          for (int bb = df + 1; bb < NDF; ++bb) {
-            if (bb != bsel) continue;
-            const float below = __shfl_up_sync(0xffffffffu, rs[bb], 1);
-            float acc = yo[df] + rs[df];
-            if (own && k >= 1 && k <= nl) acc = acc + below;
-            if (own && k <= nl) {
-              const int row = mf[df] + k;
-              __stcg(y + row, acc);
-              if (last) {
-                const float pr = k < nl ? xv[df] : __ldcg(x + row);
-                dot = fma((double)pr, (double)acc, dot);
-              }
-            }
-          }
-        } else {
-          const float acc = yo[df] + rs[df];
-          if (own && v) {
-            __stcg(y + mf[df] + k, acc);
-            if (last) dot = fma((double)xv[df], (double)acc, dot);
-          }
-        }
-      }
-      if (sg == nseg - 1) {
-        const double w = warp_butterfly(dot);
-        if (lane == 0) __stcg(part + q0 + c, w);
-        dot = 0.0;
-      }
-    }
-    if (!ok) {
-      // record the time-out, then wait (bounded: the batch's wait limit, at
-      // least 2 s, since a copy in flight lands within microseconds unless
-      // the memory system has stopped) for this warp's copies still in
-      // flight before the kernel leaves
-      if (lane == 0) {
-        atomicExch(P.err, (int)LFX_TIMEOUT);
-        const unsigned long long drain = P.timeout_ns > 2000000000ull ? P.timeout_ns : 2000000000ull;
-        // units jf .. jf + kRing - 1 were issued and not consumed
-        for (int j = jf; j < nunit && j < jf + kRing; ++j) {
-          const unsigned g = seq + (unsigned)j;
-          ring_wait(bars + g % kRing, (g / kRing) & 1u, drain);
-        }
-      }
-      __syncwarp();
-      return seq;
-    }
-    seq += (unsigned)nunit;
+    const bool ok = D.canon ? ring_item<NDF, true>(P, D, it.y, it.z, ring, bars, seq, lane)
+                            : ring_item<NDF, false>(P, D, it.y, it.z, ring, bars, seq, lane);
+    if (!ok) return seq;
     nxt = __shfl_sync(0xffffffffu, nxt, 0);
   }
   return seq;
@@ -1703,6 +1754,10 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   D.S64 = (const double*)op64->smat;
   D.L32 = (const float4*)op32->lmat;
   D.npv = op32->lnpv;
+  D.canon = (L->cs_uniform && L->cs_struct_flags == canon_flags(B->ndf) &&
+             L->cs_struct_part == canon_part(B->ndf))
+                ? 1
+                : 0;
   D.cdesc = L->cs_desc;
   D.sblk32 = op32->sblk;
   D.sblk64 = op64->sblk;

@@ -319,6 +319,10 @@ struct lfx_lma_layout {
   // partners: 4 bits per df, the upper record of df's pair.
   bool cs_ok = false;
   int32_t cs_ints = 0;
+  // the cells' vertical-pair structure (descriptor flag bits 8-23: lower and
+  // upper records; partners) when every cell has the same one
+  bool cs_uniform = false;
+  uint32_t cs_struct_flags = 0, cs_struct_part = 0;
   std::vector<int32_t> colour_start;
   int32_t* cs_cells = nullptr;
   int32_t* cs_desc = nullptr;

@@ -1277,6 +1277,16 @@ int build_layout(lfx_ctx* ctx, lfx_lma_layout* L, int32_t ncell, int32_t nl, int
     up((void**)&L->cs_cells, order.data(), order.size() * 4);
     up((void**)&L->cs_desc, d.data(), d.size() * 4);
     L->cs_ok = rc == 0;
+    // one vertical-pair structure for every cell (the reference element's)?
+    constexpr uint32_t kStructBits = 0x00FFFF00u;
+    L->cs_uniform = ncell > 0;
+    for (int32_t c = 1; c < ncell && L->cs_uniform; ++c)
+      L->cs_uniform = (cs_flags[c] & kStructBits) == (cs_flags[0] & kStructBits) &&
+                      cs_part[c] == cs_part[0];
+    if (L->cs_uniform) {
+      L->cs_struct_flags = cs_flags[0] & kStructBits;
+      L->cs_struct_part = cs_part[0];
+    }
   }
   if (mf0) {
     std::vector<int4> ep(L->nent);

@@ -240,3 +240,51 @@ def test_batch_barrier_wait_limit_runs_out_and_context_survives(ctx):
     assert e.value.status == 6  # LFX_TIMEOUT
     B.close()
     assert same(run_batch(ctx, [s], [1e-8])[0][0], ref)
+
+
+def test_batch_general_pair_structure_matches_oracle(ctx):
+    """The batch apply specialises the vertical-pair structure of the
+    reference elements (W0: bottom vertices 0-3 under top vertices 4-7); an
+    operator with another uniform structure takes the general path. The W0
+    operator with its local dofs interleaved (bottom, top, bottom, top, ...,
+    pairs (0, 1), (2, 3), ...) is the same global operator: the batch solve
+    reaches its tolerance on the oracle's FP64 residual and agrees with the
+    oracle's CG solution, and its bits differ from the reference-numbered
+    solve's (the per-cell sums run in another order), so the other path ran."""
+    p = mg.w0_problem(12, 31, seed=5)
+    perm = [0, 4, 1, 5, 2, 6, 3, 7]
+    full = p.lma.reshape(p.ndf, p.ndf, -1)
+    lma_p = np.ascontiguousarray(full[np.ix_(perm, perm)]).reshape(-1)
+    map_p = np.ascontiguousarray(p.map[:, perm])
+    npc, cic = p.mesh.colour_lookup()
+    b = lfx.FieldVector.from_array(ctx, mg.uniform(11, p.undf))
+    tol = 1e-9
+    xs = []
+    for m, lma in ((map_p, lma_p), (p.map, p.lma)):
+        op64 = lfx.LmaOperator(ctx, p.ncell_2d, p.nlayers, p.ndf, p.ndf, m, m, p.undf, p.undf,
+                               lma, npc, cic, precision=lfx.R64)
+        ops = {lfx.R64: op64, lfx.R32: op64.like(lma, lfx.R32)}
+        d32 = lfx.FieldVector(ctx, [p.undf], lfx.R32)
+        ops[lfx.R32].diagonal(d32)
+        prec = lfx.DiagonalPreconditioner(ctx, d32)
+        B = lfx.Batch(ctx, 8, 1, reserve_bytes=1 << 30, iters=8)
+        x = lfx.FieldVector(ctx, [p.undf])
+        x.set_scalar(0.0)
+        slot = B.admit(ops[lfx.R64], ops[lfx.R32], prec, b, x, tol, 20000)
+        for _ in range(2000):
+            if B.step() == 1:
+                break
+        ph, _, info = B.slot(slot)
+        assert ph == 3 and info.status == 0, info.as_dict()
+        xs.append(x.export_field())
+    o = orc.LmaOperator(p.ncell_2d, p.nlayers, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf, p.lma,
+                        npc, cic)
+    bh = b.export_field()
+    xo, oi = orc.solve("cg", o, orc.Preconditioner.diagonal(o.diagonal()), bh, r_tol=tol,
+                       a_tol=0.0, max_iter=20000)
+    assert oi.converged
+    for xv in xs:
+        rel = np.linalg.norm(bh - o.apply(xv)) / np.linalg.norm(bh)
+        assert rel <= tol * 1.0001, rel
+        assert np.linalg.norm(xv - xo) <= 1e4 * tol * np.linalg.norm(xo)
+    assert not same(xs[0], xs[1])

@@ -423,29 +423,6 @@ __device__ __noinline__ void apply_phase(const BParams& P, const int4* __restric
 // and returns; the kernel leaves at its next grid barrier.
 constexpr int kRing = 2;  // ring stages per warp
 
-// The vertical-pair structure of the reference elements (dof bit masks of
-// the lower and upper records of each pair, and each lower dof's partner in
-// its nibble): W0, bottom vertices 0-3 below top vertices 4-7; W2, the bottom
-// face 4 below the top face 5
-template <int NDF>
-struct Canon;
-template <>
-struct Canon<8> {
-  static constexpr uint32_t lower = 0x0Fu, upper = 0xF0u, part = 0x7654u;
-};
-template <>
-struct Canon<6> {
-  static constexpr uint32_t lower = 0x10u, upper = 0x20u, part = 0x50000u;
-};
-// the same in the descriptors' flag layout (bits 8-15 lower, 16-23 upper)
-__host__ __device__ constexpr uint32_t canon_flags(int ndf) {
-  return ndf == 8 ? ((Canon<8>::lower << 8) | (Canon<8>::upper << 16))
-                  : ((Canon<6>::lower << 8) | (Canon<6>::upper << 16));
-}
-__host__ __device__ constexpr uint32_t canon_part(int ndf) {
-  return ndf == 8 ? Canon<8>::part : Canon<6>::part;
-}
-
 template <int NDF>
 struct Ring {
   static constexpr int NP = NDF * (NDF + 1) / 2, NPV = (NP + 3) / 4;
@@ -524,21 +501,6 @@ __device__ __forceinline__ void row_sums(const float4* Ms, bool v, const float (
     row_entry<NDF, 4 * PV + 3>(t.w, xv, rs);
     row_sums<NDF, PV + 1>(Ms, v, xv, rs);
   }
-}
-
-// the vertical-pair tests of a descriptor, as compile-time constants for a
-// slot with its space's reference structure (CANON)
-template <int NDF, bool CANON>
-__device__ __forceinline__ bool is_lower(uint32_t flags, int df) {
-  return CANON ? ((Canon<NDF>::lower >> df) & 1u) : ((flags >> (8 + df)) & 1u);
-}
-template <int NDF, bool CANON>
-__device__ __forceinline__ bool is_upper(uint32_t flags, int df) {
-  return CANON ? ((Canon<NDF>::upper >> df) & 1u) : ((flags >> (16 + df)) & 1u);
-}
-template <int NDF, bool CANON>
-__device__ __forceinline__ int partner(uint32_t prt, int df) {
-  return CANON ? (int)((Canon<NDF>::part >> (4 * df)) & 15u) : (int)((prt >> (4 * df)) & 15u);
 }
 
 // one apply item (nq cell columns from q0 of slot record D) through the
@@ -1754,10 +1716,7 @@ int lfx_batch_admit(lfx_batch* B, lfx_op* op64, lfx_op* op32, lfx_prec* prec32, 
   D.S64 = (const double*)op64->smat;
   D.L32 = (const float4*)op32->lmat;
   D.npv = op32->lnpv;
-  D.canon = (L->cs_uniform && L->cs_struct_flags == canon_flags(B->ndf) &&
-             L->cs_struct_part == canon_part(B->ndf))
-                ? 1
-                : 0;
+  D.canon = layout_canon(L, B->ndf) ? 1 : 0;
   D.cdesc = L->cs_desc;
   D.sblk32 = op32->sblk;
   D.sblk64 = op64->sblk;

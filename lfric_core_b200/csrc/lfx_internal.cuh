@@ -396,6 +396,46 @@ struct lfx_prec {
 };
 
 namespace lfx {
+// The vertical-pair structure of the reference elements, as cell
+// descriptors encode it (flag bits 8-15: lower records, 16-23: upper
+// records; each lower dof's partner in its nibble): W0 (8 dofs), bottom
+// vertices 0-3 under top vertices 4-7; W2 (6 dofs), the bottom face 4 under
+// the top face 5. Other dof counts have none (never used with CANON).
+template <int NDF>
+struct Canon {
+  static constexpr uint32_t lower = 0u, upper = 0u, part = 0u;
+};
+template <>
+struct Canon<8> {
+  static constexpr uint32_t lower = 0x0Fu, upper = 0xF0u, part = 0x7654u;
+};
+template <>
+struct Canon<6> {
+  static constexpr uint32_t lower = 0x10u, upper = 0x20u, part = 0x50000u;
+};
+inline bool layout_canon(const lfx_lma_layout* L, int ndf) {
+  if (!L->cs_uniform || (ndf != 6 && ndf != 8)) return false;
+  const uint32_t fl = ndf == 8 ? ((Canon<8>::lower << 8) | (Canon<8>::upper << 16))
+                               : ((Canon<6>::lower << 8) | (Canon<6>::upper << 16));
+  const uint32_t pt = ndf == 8 ? Canon<8>::part : Canon<6>::part;
+  return L->cs_struct_flags == fl && L->cs_struct_part == pt;
+}
+// a descriptor's pair tests, compile-time constants with CANON
+template <int NDF, bool CANON>
+__device__ __forceinline__ bool is_lower(uint32_t flags, int df) {
+  return CANON ? ((Canon<NDF>::lower >> df) & 1u) : ((flags >> (8 + df)) & 1u);
+}
+template <int NDF, bool CANON>
+__device__ __forceinline__ bool is_upper(uint32_t flags, int df) {
+  return CANON ? ((Canon<NDF>::upper >> df) & 1u) : ((flags >> (16 + df)) & 1u);
+}
+template <int NDF, bool CANON>
+__device__ __forceinline__ int partner(uint32_t prt, int df) {
+  return CANON ? (int)((Canon<NDF>::part >> (4 * df)) & 15u) : (int)((prt >> (4 * df)) & 15u);
+}
+}  // namespace lfx
+
+namespace lfx {
 int op_apply_impl(lfx_op* op, const void* x, void* y, const void* b, const int* skip);
 // bytes of the level-major copy an FP32 operator with a packed copy would
 // take, and its creation (a no-op when it exists); both LFX_NOT_SUPPORTED

@@ -813,7 +813,7 @@ struct CellArgs {
   int q0;
 };
 
-template <class T, int NDF, bool SYM, bool RESID>
+template <class T, int NDF, bool SYM, bool RESID, bool CANON>
 __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict__ M,
                                                  const T* __restrict__ x, T* __restrict__ y,
                                                  const T* __restrict__ b, const int* skip) {
@@ -847,7 +847,7 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
   asm volatile("griddepcontrol.wait;" ::: "memory");
 #pragma unroll
   for (int df = 0; df < NDF; ++df) {
-    const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+    const bool lower = is_lower<NDF, CANON>(flags, df), upper = is_upper<NDF, CANON>(flags, df);
     const bool opens = (flags >> df) & 1u;
     const bool live = lower ? lane <= nl : v;
     yo[df] = (!upper && !opens && live) ? y[mf[df] + lane] : T(0);
@@ -855,9 +855,9 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
 #define MV(i, j) m[SYM ? pidx<NDF>(i, j) : (i) * NDF + (j)]
 #pragma unroll
   for (int df = 0; df < NDF; ++df) {
-    if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
-    if ((flags >> (8 + df)) & 1u) {
-      const int bsel = (part >> (4 * df)) & 15u;
+    if (is_upper<NDF, CANON>(flags, df)) continue;  // upper record: summed with its lower one
+    if (is_lower<NDF, CANON>(flags, df)) {
+      const int bsel = partner<NDF, CANON>(part, df);
 #pragma unroll
       for (int bb = df + 1; bb < NDF; ++bb) {
         if (bb != bsel) continue;
@@ -896,7 +896,7 @@ __global__ void __launch_bounds__(256) lma_cells(CellArgs C, const T* __restrict
 // the lane below); lane 0 holds the level just below the segment only to
 // supply those terms to lane 1 and writes nothing. Every dof therefore gets
 // the terms of lma_cells in the same order (the same bits).
-template <class T, int NDF, bool SYM, bool RESID>
+template <class T, int NDF, bool SYM, bool RESID, bool CANON>
 __global__ void __launch_bounds__(256) lma_cells_seg(CellArgs C, int nseg, int L,
                                                      const T* __restrict__ M,
                                                      const T* __restrict__ x, T* __restrict__ y,
@@ -928,7 +928,7 @@ __global__ void __launch_bounds__(256) lma_cells_seg(CellArgs C, int nseg, int L
   asm volatile("griddepcontrol.wait;" ::: "memory");
 #pragma unroll
   for (int df = 0; df < NDF; ++df) {
-    const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+    const bool lower = is_lower<NDF, CANON>(flags, df), upper = is_upper<NDF, CANON>(flags, df);
     const bool opens = (flags >> df) & 1u;
     const bool live = own && (lower ? k <= nl : v);
     yo[df] = (!upper && !opens && live) ? y[mf[df] + k] : T(0);
@@ -936,9 +936,9 @@ __global__ void __launch_bounds__(256) lma_cells_seg(CellArgs C, int nseg, int L
 #define MV(i, j) m[SYM ? pidx<NDF>(i, j) : (i) * NDF + (j)]
 #pragma unroll
   for (int df = 0; df < NDF; ++df) {
-    if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
-    if ((flags >> (8 + df)) & 1u) {
-      const int bsel = (part >> (4 * df)) & 15u;
+    if (is_upper<NDF, CANON>(flags, df)) continue;  // upper record: summed with its lower one
+    if (is_lower<NDF, CANON>(flags, df)) {
+      const int bsel = partner<NDF, CANON>(part, df);
 #pragma unroll
       for (int bb = df + 1; bb < NDF; ++bb) {
         if (bb != bsel) continue;
@@ -976,7 +976,7 @@ __global__ void __launch_bounds__(256) lma_cells_seg(CellArgs C, int nseg, int L
 // memory. Same arithmetic as lma_cells.
 constexpr int kCellWarps = 4;
 
-template <class T, int NDF, bool SYM, int S, bool RESID>
+template <class T, int NDF, bool SYM, int S, bool RESID, bool CANON>
 __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, const T* __restrict__ M,
                                                                  const T* __restrict__ x,
                                                                  T* __restrict__ y,
@@ -1024,7 +1024,7 @@ __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, co
     for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldg(x + mf[j] + lane) : T(0);
 #pragma unroll
     for (int df = 0; df < NDF; ++df) {
-      const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+      const bool lower = is_lower<NDF, CANON>(flags, df), upper = is_upper<NDF, CANON>(flags, df);
       const bool opens = (flags >> df) & 1u;
       const bool live = lower ? lane <= nl : v;
       yo[df] = (!upper && !opens && live) ? y[mf[df] + lane] : T(0);
@@ -1039,9 +1039,9 @@ __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, co
 #define MV(i, j) m[SYM ? pidx<NDF>(i, j) : (i) * NDF + (j)]
 #pragma unroll
     for (int df = 0; df < NDF; ++df) {
-      if ((flags >> (16 + df)) & 1u) continue;
-      if ((flags >> (8 + df)) & 1u) {
-        const int bsel = (part >> (4 * df)) & 15u;
+      if (is_upper<NDF, CANON>(flags, df)) continue;
+      if (is_lower<NDF, CANON>(flags, df)) {
+        const int bsel = partner<NDF, CANON>(part, df);
 #pragma unroll
         for (int bb = df + 1; bb < NDF; ++bb) {
           if (bb != bsel) continue;
@@ -1628,7 +1628,7 @@ size_t cells_stage_bytes(const lfx_op* op) {
 constexpr size_t kCellSmemMax = 200 * 1024;
 
 // stages: 0 one cell per warp (lma_cells), 2 or 3 the staged pipeline
-template <class T, int N, bool SYM, int S, bool RESID>
+template <class T, int N, bool SYM, int S, bool RESID, bool CANON>
 void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const void* b,
                     const int* skip) {
   const lfx_lma_layout* L = op->lay;
@@ -1640,11 +1640,11 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
   if constexpr (S > 0) {
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(lma_cells_pipe<T, N, SYM, S, RESID>,
+      cudaFuncSetAttribute(lma_cells_pipe<T, N, SYM, S, RESID, CANON>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellSmemMax);
       attr = true;
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_cells_pipe<T, N, SYM, S, RESID>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lma_cells_pipe<T, N, SYM, S, RESID, CANON>,
                                                   32 * kCellWarps, smem);
     if (per_sm < 1) per_sm = 1;
   }
@@ -1657,7 +1657,7 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
     if constexpr (S > 0) {
       const int grid = (int)std::min<int64_t>(((int64_t)C.ncells + kCellWarps - 1) / kCellWarps,
                                               (int64_t)ctx->num_sms * per_sm);
-      lma_cells_pipe<T, N, SYM, S, RESID><<<grid, 32 * kCellWarps, smem, ctx->stream>>>(
+      lma_cells_pipe<T, N, SYM, S, RESID, CANON><<<grid, 32 * kCellWarps, smem, ctx->stream>>>(
           C, M, (const T*)x, (T*)y, (const T*)b, sb, skip);
     } else {
       // colours after the first launch as programmatic dependents of the
@@ -1677,10 +1677,10 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
       cfg.attrs = at;
       cfg.numAttrs = k > 0 ? 1 : 0;
       if (nseg == 1)
-        cudaLaunchKernelEx(&cfg, lma_cells<T, N, SYM, RESID>, C, M, (const T*)x, (T*)y,
+        cudaLaunchKernelEx(&cfg, lma_cells<T, N, SYM, RESID, CANON>, C, M, (const T*)x, (T*)y,
                            (const T*)b, skip);
       else
-        cudaLaunchKernelEx(&cfg, lma_cells_seg<T, N, SYM, RESID>, C, nseg, seg_l, M,
+        cudaLaunchKernelEx(&cfg, lma_cells_seg<T, N, SYM, RESID, CANON>, C, nseg, seg_l, M,
                            (const T*)x, (T*)y, (const T*)b, skip);
     }
     ctx->launches++;
@@ -1688,22 +1688,37 @@ void launch_cells_t(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, cons
   ctx->launches--;  // counted once by the caller
 }
 
-template <class T, int N, int S>
-void launch_cells_s(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const void* b,
+template <class T, int N, int S, bool CANON>
+void launch_cells_c(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const void* b,
                     const int* skip) {
   // the residual form is its own instantiation: the plain apply keeps its
   // register count (and occupancy)
   if (op->smat) {
     if (b)
-      launch_cells_t<T, N, true, S, true>(ctx, op, x, y, b, skip);
+      launch_cells_t<T, N, true, S, true, CANON>(ctx, op, x, y, b, skip);
     else
-      launch_cells_t<T, N, true, S, false>(ctx, op, x, y, b, skip);
+      launch_cells_t<T, N, true, S, false, CANON>(ctx, op, x, y, b, skip);
   } else {
     if (b)
-      launch_cells_t<T, N, false, S, true>(ctx, op, x, y, b, skip);
+      launch_cells_t<T, N, false, S, true, CANON>(ctx, op, x, y, b, skip);
     else
-      launch_cells_t<T, N, false, S, false>(ctx, op, x, y, b, skip);
+      launch_cells_t<T, N, false, S, false, CANON>(ctx, op, x, y, b, skip);
   }
+}
+
+// operators whose cells carry their space's reference pair structure take
+// the instantiation with the pair tests at compile time (same arithmetic,
+// same bits)
+template <class T, int N, int S>
+void launch_cells_s(lfx_ctx* ctx, const lfx_op* op, const void* x, void* y, const void* b,
+                    const int* skip) {
+  if constexpr (N == 6 || N == 8) {
+    if (layout_canon(op->lay, N)) {
+      launch_cells_c<T, N, S, true>(ctx, op, x, y, b, skip);
+      return;
+    }
+  }
+  launch_cells_c<T, N, S, false>(ctx, op, x, y, b, skip);
 }
 
 template <class T, int N>

@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the batched and serving legs")
     ap.add_argument("--apply", default="",
-                    help="pin the LMA apply configuration kernel:stages for FP32,FP64, e.g. 5:0,5:0 "
+                    help="pin the LMA apply configuration kernel:stages[:warps] for FP32,FP64, e.g. 5:0,5:0 "
                          "(default: the autotuner's choice; a profiler's replays can move that "
                          "choice, so profiled runs pin the one an unprofiled run tunes to)")
     return ap.parse_args()
@@ -668,10 +668,10 @@ def main():
     if args.apply:
         tuning = {}
         for name, sys_, spec in zip(("fp32", "fp64"), (s32, s64), args.apply.split(",")):
-            k, st = (int(v) for v in spec.split(":"))
-            sys_.op.set_apply(k, st)
-            tuning[name] = {"kernel": lfx.APPLY_KERNEL_NAMES[k], "stages": st, "warps": 0,
-                            "us": round(sys_.op.time_apply(k, st, 0, 10), 2), "pinned": True}
+            k, st, w = ([int(v) for v in spec.split(":")] + [0])[:3]
+            sys_.op.set_apply(k, st, w)
+            tuning[name] = {"kernel": lfx.APPLY_KERNEL_NAMES[k], "stages": st, "warps": w,
+                            "us": round(sys_.op.time_apply(k, st, w, 10), 2), "pinned": True}
     else:
         tuning = {"fp32": s32.op.autotune(reps=10), "fp64": s64.op.autotune(reps=10)}
     fp64 = lfx.GMRES(s64.op, s64.prec, GCRK, RTOL, 1e-16, 200)
@@ -824,7 +824,8 @@ def main():
 
     def apply_bytes(op, esz, kernel):
         st = op.storage()
-        mat = st["packed_bytes"] if kernel == "cell-scatter" and st["packed_bytes"] else st["full_bytes"]
+        mat = (st["packed_bytes"] if kernel.startswith("cell-scatter") and st["packed_bytes"]
+               else st["full_bytes"])
         return mat + 2 * p.undf * esz + p.ncell_2d * 6 * 4
     bytes32 = apply_bytes(s32.op, 4, tuning["fp32"]["kernel"])
     # FP32 applies that did work: the refined solve counts its initial
@@ -846,8 +847,10 @@ def main():
                                "the committed capture profiles/lma_apply_fp32_c96x30.json (not "
                                "measured in this run)") if traffic else None,
             "algorithmic_bytes_per_launch": bytes32,
-            "launch": ("one apply (the cell scatter: one kernel per colour)"
-                       if tuning["fp32"]["kernel"] == "cell-scatter" else "one apply (one launch)"),
+            "launch": {"cell-scatter": "one apply (the cell scatter: one kernel per colour)",
+                       "cell-scatter-persistent": "one apply (the cell scatter: one persistent "
+                                                  "launch over the colours)"}.get(
+                           tuning["fp32"]["kernel"], "one apply (one launch)"),
             "launches_timed": n32, "applies_executed": K * exec32,
             "avg_launch_us": round(1e3 * avg32, 2),
             "timed_pass": "a second pass of the same solves with events around each apply "

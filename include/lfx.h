@@ -137,13 +137,14 @@ int lfx_lma_sum(const lfx_op* x, double a, const lfx_op* y, lfx_op** out);
  * pipeline with 2..8 stages and 1..8 warps per block, and the copy-staged
  * pipeline with 2..6 stages and 2..8 warps, those that fit the shared memory,
  * and the cell scatter (square operators on one dofmap; one launch per
- * colour, reading a symmetric operator's packed upper triangle) -- over
+ * colour, reading a symmetric operator's packed upper triangle; or, ndf 6
+ * or 8 with at most 31 levels, one persistent launch whose colours meet at
+ * bounded grid barriers, 4 or 6 ring stages of 4 or 8 warps) -- over
  * `reps` launches and keeps the fastest for later applies. Outputs
  * (nullable) name the choice: kernel 0 pipeline / 1 register gather / 2
  * generic / 3 register gather with prefetched descriptors / 4 copy-staged
  * pipeline (matrix blocks and x values both staged in shared memory) / 5 cell
- * scatter, and its time per
- * apply. */
+ * scatter / 6 persistent cell scatter, and its time per apply. */
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
                     float* us);
 /* time one configuration (as above) without keeping it. Both time on
@@ -154,7 +155,8 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
                       float* us);
 /* keep one configuration (as above) for later applies, as the autotuner
  * would; LFX_NOT_SUPPORTED if it does not fit the operator. Kernel 5 takes
- * stages 0 (one cell per warp) or 2, 3 (cells staged ahead in shared memory). */
+ * stages 0 (one cell per warp) or 2, 3 (cells staged ahead in shared memory);
+ * kernel 6 stages 4 or 6 (ring stages per warp) and warps 4 or 8 per block. */
 int lfx_op_set_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps);
 /* bytes of the stored local matrices: the full copy every kernel can read
  * and the packed upper triangle of a bitwise symmetric operator on one
@@ -380,7 +382,10 @@ int64_t lfx_ctx_launch_count(const lfx_ctx* ctx);
  * bulk-copy pipeline; 1 = force the register gather; 3 = force the register
  * gather with prefetched descriptors (the register gather where the operator
  * does not fit it); 4 = force the copy-staged pipeline; 5 = force the cell
- * scatter where the operator fits it. All give bit-identical results. */
+ * scatter where the operator fits it; 6 = force the cell scatter as one
+ * persistent (cooperative) launch over the colours where the operator fits
+ * it (ndf 6 or 8, at most 31 levels and 16 colours). All give bit-identical
+ * results. */
 int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which);
 /* LFX_TIMEOUT if a kernel's bounded device-side wait ran out since the last
  * check (the kernel then skipped its work); synchronises the stream */

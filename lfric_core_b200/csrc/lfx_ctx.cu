@@ -232,7 +232,7 @@ int lfx_ctx_apply_timing(lfx_ctx* ctx, int32_t precision, int64_t* launches, dou
 int64_t lfx_ctx_launch_count(const lfx_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int lfx_ctx_set_apply_kernel(lfx_ctx* ctx, int32_t which) {
-  if (!ctx || which < -1 || which > 5 || which == 2) return LFX_INVALID_ARGUMENT;
+  if (!ctx || which < -1 || which > 6 || which == 2) return LFX_INVALID_ARGUMENT;
   ctx->lma_kernel = which;
   return LFX_OK;
 }
@@ -243,7 +243,8 @@ int lfx_ctx_check_device_error(lfx_ctx* ctx) {
   LFX_CK(ctx, cudaStreamSynchronize(ctx->stream));
   LFX_CK(ctx, cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h) {
-    LFX_CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int)));
+    // the flag, and the grid barrier words of a persistent apply that left early
+    LFX_CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int) * 4));
     return fail(ctx, LFX_TIMEOUT, "a device-side bounded wait ran out (pipeline stage never filled)");
   }
   return LFX_OK;

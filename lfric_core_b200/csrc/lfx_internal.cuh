@@ -49,7 +49,7 @@ struct lfx_ctx {
   double timed_ms[2] = {0.0, 0.0};
   int64_t launches = 0;  // kernels launched on this context
   int lma_kernel = -1;   // -1: per-operator choice, 0: force pipeline, 1: force gather
-  int* d_err = nullptr;  // set by a kernel whose bounded wait ran out
+  int* d_err = nullptr;  // [0] set by a kernel whose bounded wait ran out; [2..3] grid barrier words
   // while a solver captures a CUDA graph, timed applies record into fresh
   // event pairs owned by that graph
   std::vector<TimedPair>* capture_ev = nullptr;

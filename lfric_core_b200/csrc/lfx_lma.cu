@@ -1075,6 +1075,290 @@ __global__ void __launch_bounds__(32 * kCellWarps) lma_cells_pipe(CellArgs C, co
   cp_async_wait<0>();
 }
 
+// The cell scatter as ONE persistent launch over all colours (kernel 6).
+// Every warp of the grid walks its cells (stride: warps in the grid) colour
+// after colour, through a ring of S stages in shared memory:
+//   - S cells ahead, lane 0 moves the cell's matrix block and descriptor
+//     with two cp.async.bulk copies completing on the stage's mbarrier;
+//   - D cells ahead (D < S, so the descriptor has landed), every lane copies
+//     its level's x values and partial sums of y for that cell with 4/8-byte
+//     cp.async (zero-filled where the reference adds nothing), one commit
+//     group per cell;
+//   - the cell itself is summed from shared memory with the arithmetic of
+//     lma_cells (the same bits).
+// Colours are separated by a grid-wide barrier (the launch is cooperative:
+// all blocks are resident). The matrix stream and the x copies run on across
+// the barrier; the partial sums of y of a cell of the next colour are read
+// only after it (a cell whose y would have been copied before the barrier is
+// marked and reads y from L2 when its turn comes). Every wait is bounded by
+// limit_ns; a time-out writes LFX_TIMEOUT to err, the grid leaves at the next
+// barrier, and each warp first waits (bounded) for the copies it issued.
+constexpr int kRingMaxCol = 16;  // colours of one ring launch, at most
+
+struct CellRingArgs {
+  int nl, blk, cstride, dints;
+  const int* cells;  // colour-loop order -> cell (the full-storage matrix)
+  const int* desc;
+  int ncol, stages;
+  unsigned* bar;  // [0] arrivals, [1] generation
+  int* err;
+  unsigned long long limit_ns;
+  int cs[kRingMaxCol + 1];  // first position of each colour in the colour-loop order
+};
+
+__device__ __forceinline__ unsigned long long ring_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool ring_wait_ns(uint64_t* bar, unsigned parity,
+                                             unsigned long long limit) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = ring_clock();
+  while (!mbar_try_wait(bar, parity))
+    if (ring_clock() - t0 > limit) return false;
+  return true;
+}
+// BYTES-byte asynchronous copy that writes zeros instead when !on
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zf(void* dst, const void* src, bool on) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src),
+               "n"(BYTES), "r"(on ? BYTES : 0)
+               : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// grid-wide barrier; false when a block reported an error or the wait ran out
+__device__ bool ring_grid_sync(const CellRingArgs& R, int* bad) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = *(volatile int*)R.err == 0;
+    if (ok) {
+      const unsigned gen = ld_acquire_u32(R.bar + 1);
+      __threadfence();
+      const unsigned arrived = atomicAdd(R.bar, 1u);
+      if (arrived == gridDim.x - 1) {
+        R.bar[0] = 0u;
+        __threadfence();
+        atomicExch(R.bar + 1, gen + 1u);
+      } else {
+        const unsigned long long t0 = ring_clock();
+        while (ld_acquire_u32(R.bar + 1) == gen) {
+          if (*(volatile int*)R.err) {
+            ok = 0;
+            break;
+          }
+          if (ring_clock() - t0 > R.limit_ns) {
+            atomicExch(R.err, (int)LFX_TIMEOUT);
+            ok = 0;
+            break;
+          }
+        }
+      }
+      __threadfence();
+    }
+    *bad = !ok;
+  }
+  __syncthreads();
+  return !*(volatile int*)bad;
+}
+
+template <class T, int NDF, bool SYM, int D, bool RESID, bool CANON>
+__global__ void __launch_bounds__(256) lma_cells_ring(CellRingArgs R, const T* __restrict__ M,
+                                                      const T* __restrict__ x, T* __restrict__ y,
+                                                      const T* __restrict__ b, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  extern __shared__ __align__(128) unsigned char ring_smem[];
+  __shared__ int bad;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nwb = blockDim.x >> 5;
+  const int S = R.stages, nl = R.nl;
+  const int gw = blockIdx.x * nwb + wib, nw = gridDim.x * nwb;
+  const unsigned mat_bytes = (unsigned)R.cstride * sizeof(T), dsc_bytes = (unsigned)R.dints * 4;
+  // stage: matrix block, descriptor, x[NDF][32], y[NDF][32]
+  const unsigned stage_bytes = mat_bytes + dsc_bytes + 2u * NDF * 32u * sizeof(T);
+  unsigned char* ring = ring_smem + (size_t)wib * S * stage_bytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring_smem + (size_t)nwb * S * stage_bytes) + wib * S;
+  if (lane == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+
+  // a cursor over this warp's cells: colour k, position q in the colour loop
+  auto advance = [&](int& k, int& q) {
+    q += nw;
+    while (k < R.ncol && q >= R.cs[k + 1]) {
+      ++k;
+      if (k < R.ncol) q = R.cs[k] + gw;
+    }
+  };
+  auto first = [&](int& k, int& q) {
+    k = 0;
+    q = R.cs[0] + gw;
+    while (k < R.ncol && q >= R.cs[k + 1]) {
+      ++k;
+      if (k < R.ncol) q = R.cs[k] + gw;
+    }
+  };
+  // far copy (lane 0): matrix block and descriptor of the cell at (fk, fq)
+  int fk, fq;
+  unsigned nfar = 0;  // cells far-issued (lane 0's count)
+  auto far_issue = [&]() {
+    const unsigned s = nfar % (unsigned)S;
+    unsigned char* st = ring + (size_t)s * stage_bytes;
+    const int c = SYM ? fq : __ldg(R.cells + fq);
+    fence_proxy_async();
+    mbar_expect_tx(&bars[s], mat_bytes + dsc_bytes);
+    bulk_load(st, M + (size_t)c * R.cstride, mat_bytes, &bars[s]);
+    bulk_load(st + mat_bytes, R.desc + (size_t)fq * R.dints, dsc_bytes, &bars[s]);
+    ++nfar;
+    advance(fk, fq);
+  };
+  first(fk, fq);
+  if (lane == 0)
+    for (int i = 0; i < S && fk < R.ncol; ++i) far_issue();
+  // near copy (all lanes): x and y of the cell at (nk, nq), after its
+  // descriptor has landed; y only while the consumer is in the same colour
+  int nk, nq;
+  first(nk, nq);
+  unsigned nnear = 0;    // cells near-issued (their descriptors waited for)
+  unsigned ydefer = 0u;  // per stage: y of this cell not copied (read from L2 later)
+  bool ok = true;
+  const bool v = lane < nl;
+  auto near_issue = [&](int kc) {
+    if (nk < R.ncol) {
+      const unsigned s = nnear % (unsigned)S;
+      unsigned char* st = ring + (size_t)s * stage_bytes;
+      if (!ring_wait_ns(&bars[s], (nnear / (unsigned)S) & 1u, R.limit_ns)) {
+        ok = false;
+        cp_async_commit();
+        return;
+      }
+      const int* dsc = reinterpret_cast<const int*>(st + mat_bytes);
+      const uint32_t flags = (uint32_t)dsc[NDF];
+      T* xs = reinterpret_cast<T*>(st + mat_bytes + dsc_bytes);
+      T* ys = xs + NDF * 32;
+#pragma unroll
+      for (int j = 0; j < NDF; ++j) {
+        const int mf = dsc[j];
+        cp_async_zf<sizeof(T)>(xs + j * 32 + lane, x + mf + (v ? lane : 0), v);
+      }
+      if (nk == kc) {
+#pragma unroll
+        for (int df = 0; df < NDF; ++df) {
+          const bool lower = is_lower<NDF, CANON>(flags, df), upper = is_upper<NDF, CANON>(flags, df);
+          const bool opens = (flags >> df) & 1u;
+          const bool live = lower ? lane <= nl : v;
+          const bool on = !upper && !opens && live;
+          cp_async_zf<sizeof(T)>(ys + df * 32 + lane, y + dsc[df] + (on ? lane : 0), on);
+        }
+        ydefer &= ~(1u << s);
+      } else {
+        ydefer |= 1u << s;
+      }
+      ++nnear;
+      advance(nk, nq);
+    }
+    cp_async_commit();
+  };
+  for (int i = 0; i < D; ++i) near_issue(0);
+
+  unsigned ncons = 0;
+  for (int kc = 0; kc < R.ncol; ++kc) {
+    if (kc > 0) {
+      if (!ok) atomicExch(R.err, (int)LFX_TIMEOUT);
+      if (!ring_grid_sync(R, &bad)) break;
+    }
+    for (int q = R.cs[kc] + gw; q < R.cs[kc + 1] && ok; q += nw) {
+      near_issue(kc);
+      if (!ok) break;
+      cp_async_wait<D>();
+      __syncwarp();
+      const unsigned s = ncons % (unsigned)S;
+      const unsigned char* st = ring + (size_t)s * stage_bytes;
+      const T* sm = reinterpret_cast<const T*>(st) + (v ? lane : 0);
+      const int* dsc = reinterpret_cast<const int*>(st + mat_bytes);
+      const T* xs = reinterpret_cast<const T*>(st + mat_bytes + dsc_bytes);
+      const T* ys = xs + NDF * 32;
+      int mf[NDF];
+#pragma unroll
+      for (int j = 0; j < NDF; ++j) mf[j] = dsc[j];
+      const uint32_t flags = (uint32_t)dsc[NDF], part = (uint32_t)dsc[NDF + 1];
+      constexpr int NP = SYM ? NDF * (NDF + 1) / 2 : NDF * NDF;
+      T m[NP], xv[NDF], yo[NDF];
+#pragma unroll
+      for (int j = 0; j < NDF; ++j) xv[j] = xs[j * 32 + lane];
+      if ((ydefer >> s) & 1u) {
+#pragma unroll
+        for (int df = 0; df < NDF; ++df) {
+          const bool lower = is_lower<NDF, CANON>(flags, df), upper = is_upper<NDF, CANON>(flags, df);
+          const bool opens = (flags >> df) & 1u;
+          const bool live = lower ? lane <= nl : v;
+          yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + lane) : T(0);
+        }
+      } else {
+#pragma unroll
+        for (int df = 0; df < NDF; ++df) yo[df] = ys[df * 32 + lane];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        m[p] = v ? sm[SYM ? p * nl : (p / NDF) * R.blk + (p % NDF) * nl] : T(0);
+      __syncwarp();
+      // every lane has read the stage: lane 0 refills it S cells ahead
+      if (lane == 0 && fk < R.ncol) far_issue();
+      ++ncons;
+#define MV(i, j) m[SYM ? pidx<NDF>(i, j) : (i) * NDF + (j)]
+#pragma unroll
+      for (int df = 0; df < NDF; ++df) {
+        if (is_upper<NDF, CANON>(flags, df)) continue;
+        if (is_lower<NDF, CANON>(flags, df)) {
+          const int bsel = partner<NDF, CANON>(part, df);
+#pragma unroll
+          for (int bb = df + 1; bb < NDF; ++bb) {
+            if (bb != bsel) continue;
+            T acc = yo[df];
+#pragma unroll
+            for (int j = 0; j < NDF; ++j) {
+              const T mb = __shfl_up_sync(0xffffffffu, MV(bb, j), 1);
+              const T xb = __shfl_up_sync(0xffffffffu, xv[j], 1);
+              if (v) acc = fmaT(MV(df, j), xv[j], acc);
+              if (lane >= 1 && lane <= nl) acc = fmaT(mb, xb, acc);
+            }
+            if (lane <= nl) {
+              const int row = mf[df] + lane;
+              __stcg(y + row, (RESID && ((flags >> (24 + df)) & 1u)) ? __ldg(b + row) - acc : acc);
+            }
+          }
+        } else {
+          T acc = yo[df];
+#pragma unroll
+          for (int j = 0; j < NDF; ++j) acc = fmaT(MV(df, j), xv[j], acc);
+          if (v) {
+            const int row = mf[df] + lane;
+            __stcg(y + row, (RESID && ((flags >> (24 + df)) & 1u)) ? __ldg(b + row) - acc : acc);
+          }
+        }
+      }
+#undef MV
+    }
+  }
+  if (!ok) atomicExch(R.err, (int)LFX_TIMEOUT);
+  // leave with nothing in flight: this warp's per-lane copies, then (lane 0,
+  // bounded, at least 2 s) the bulk copies it issued and nobody waited for
+  cp_async_wait<0>();
+  if (lane == 0) {
+    const unsigned long long drain = R.limit_ns > 2000000000ull ? R.limit_ns : 2000000000ull;
+    for (unsigned i = nnear; i < nfar; ++i)
+      ring_wait_ns(&bars[i % (unsigned)S], (i / (unsigned)S) & 1u, drain);
+  }
+  __syncwarp();
+}
+
 // level-major copy of the FP32 packed triangles: dst[(q nl + k) 4 npv + p]
 // = src[q sblk + p nl + k], zero in the padding p >= np
 __global__ void relayout_level_major(const float* __restrict__ src, float* __restrict__ dst,
@@ -1739,14 +2023,124 @@ bool cells_stages_ok(const lfx_op* op, int stages) {
   return (size_t)kCellWarps * stages * cells_stage_bytes(op) <= kCellSmemMax;
 }
 
+// ---- the persistent ring cell scatter (kernel 6): `stages` ring stages per
+// warp (4 or 6; x and y copied stages / 2 cells ahead), `warps` per block
+// (4 or 8)
+constexpr size_t kRingSmemMax = 220 * 1024;
+
+size_t ring_stage_bytes(const lfx_op* op) {
+  const size_t esz = op->precision == LFX_R64 ? 8 : 4;
+  const lfx_lma_layout* L = op->lay;
+  const size_t m = op->smat ? (size_t)op->sblk * esz : (size_t)L->ndf_to * op->blk * esz;
+  return m + (size_t)L->cs_ints * 4 + 2 * (size_t)L->ndf_to * 32 * esz;
+}
+size_t ring_smem_bytes(const lfx_op* op, int stages, int warps) {
+  return (size_t)warps * stages * (ring_stage_bytes(op) + 8);
+}
+bool ring_ok(const lfx_op* op, int stages, int warps) {
+  const lfx_lma_layout* L = op->lay;
+  if (!cells_ok(op) || (L->ndf_to != 6 && L->ndf_to != 8)) return false;
+  if (L->nlayers + 1 > 32) return false;  // one warp per cell column
+  if (L->colour_start.size() < 2 || L->colour_start.size() > (size_t)kRingMaxCol + 1) return false;
+  if (stages != 4 && stages != 6) return false;
+  if (warps != 4 && warps != 8) return false;
+  return ring_smem_bytes(op, stages, warps) <= kRingSmemMax;
+}
+
+template <class T, int N, bool SYM, int D, bool RESID, bool CANON>
+void launch_ring_t(lfx_ctx* ctx, const lfx_op* op, int stages, int warps, const void* x, void* y,
+                   const void* b, const int* skip) {
+  const lfx_lma_layout* L = op->lay;
+  CellRingArgs R{};
+  R.nl = L->nlayers;
+  R.blk = op->blk;
+  R.cstride = SYM ? op->sblk : N * op->blk;
+  R.dints = L->cs_ints;
+  R.cells = L->cs_cells;
+  R.desc = L->cs_desc;
+  R.ncol = (int)L->colour_start.size() - 1;
+  R.stages = stages;
+  R.bar = reinterpret_cast<unsigned*>(ctx->d_err + 2);
+  R.err = ctx->d_err;
+  R.limit_ns = 2000000000ull;
+  for (int k = 0; k <= R.ncol; ++k) R.cs[k] = L->colour_start[k];
+  const size_t smem = ring_smem_bytes(op, stages, warps);
+  auto kern = lma_cells_ring<T, N, SYM, D, RESID, CANON>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRingSmemMax);
+    attr = true;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, smem);
+  if (per_sm < 1) per_sm = 1;
+  // every block resident (cooperative launch): the colours meet at grid barriers
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ctx->num_sms * per_sm));
+  cfg.blockDim = dim3((unsigned)(32 * warps));
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, R, (const T*)(SYM ? op->smat : op->mat), (const T*)x, (T*)y,
+                     (const T*)b, skip);
+}
+
+template <class T, int N, bool SYM, int D>
+void launch_ring_d(lfx_ctx* ctx, const lfx_op* op, int stages, int warps, const void* x, void* y,
+                   const void* b, const int* skip) {
+  const bool canon = layout_canon(op->lay, N);
+  if (b) {
+    if (canon) launch_ring_t<T, N, SYM, D, true, true>(ctx, op, stages, warps, x, y, b, skip);
+    else launch_ring_t<T, N, SYM, D, true, false>(ctx, op, stages, warps, x, y, b, skip);
+  } else {
+    if (canon) launch_ring_t<T, N, SYM, D, false, true>(ctx, op, stages, warps, x, y, b, skip);
+    else launch_ring_t<T, N, SYM, D, false, false>(ctx, op, stages, warps, x, y, b, skip);
+  }
+}
+
+template <class T, int N>
+void launch_ring(lfx_ctx* ctx, const lfx_op* op, int stages, int warps, const void* x, void* y,
+                 const void* b, const int* skip) {
+  if (op->smat) {
+    if (stages == 6) launch_ring_d<T, N, true, 3>(ctx, op, stages, warps, x, y, b, skip);
+    else launch_ring_d<T, N, true, 2>(ctx, op, stages, warps, x, y, b, skip);
+  } else {
+    if (stages == 6) launch_ring_d<T, N, false, 3>(ctx, op, stages, warps, x, y, b, skip);
+    else launch_ring_d<T, N, false, 2>(ctx, op, stages, warps, x, y, b, skip);
+  }
+}
+
+// the first ring shape that fits: 6 stages of 8 warps, else fewer
+TmaShape ring_default(const lfx_op* op) {
+  TmaShape ts;
+  for (int w : {8, 4})
+    for (int st : {6, 4})
+      if (!ts.warps && ring_ok(op, st, w)) {
+        ts.warps = w;
+        ts.stages = st;
+      }
+  return ts;
+}
+
 // kernel: 0 bulk-copy pipelined (shape ts), 1 register gather, 2 generic,
 // 3 register gather with prefetched descriptors, 4 copy-staged pipeline (shape ts),
-// 5 cell scatter
+// 5 cell scatter, 6 the cell scatter as one persistent launch (shape ts)
 template <class T>
 void launch_apply_t(lfx_ctx* ctx, const lfx_op* op, int kernel, const TmaShape& ts,
                     const void* x, void* y, const void* b, const int* skip) {
   const lfx_lma_layout* L = op->lay;
   const LayoutArgs A = args_of(L, op->blk);
+  if (kernel == 6) {
+    if (L->ndf_to == 6)
+      launch_ring<T, 6>(ctx, op, ts.stages, ts.warps, x, y, b, skip);
+    else
+      launch_ring<T, 8>(ctx, op, ts.stages, ts.warps, x, y, b, skip);
+    return;
+  }
   if (kernel == 5) {
     switch (L->ndf_to) {
       case 1: launch_cells<T, 1>(ctx, op, ts.stages, x, y, b, skip); return;
@@ -1814,6 +2208,13 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     *kernel = 5;
     return;
   }
+  if (ctx->lma_kernel == 6) {
+    *ts = ring_default(op);
+    if (ts->warps) {
+      *kernel = 6;
+      return;
+    }
+  }
   if ((ctx->lma_kernel == 1 || ctx->lma_kernel == 3) && gather2_ok(op)) {
     *kernel = 1;
     return;
@@ -1828,6 +2229,10 @@ void pick_apply(const lfx_ctx* ctx, const lfx_op* op, int* kernel, TmaShape* ts)
     if (*kernel == 0) *ts = tma_shape(op, op->tune_stages, op->tune_warps);
     if (*kernel == 4) *ts = pipe_shape(op, op->tune_stages, op->tune_warps);
     if (*kernel == 3 || *kernel == 5) ts->stages = op->tune_stages;
+    if (*kernel == 6) {
+      ts->stages = op->tune_stages;
+      ts->warps = op->tune_warps;
+    }
     if ((*kernel != 0 && *kernel != 4) || ts->warps) return;
   }
   // untuned: the prefetching gather where it fits (fastest measured on W2
@@ -2073,7 +2478,7 @@ int lfx_op_apply(lfx_op* op, const lfx_vec* x, lfx_vec* y) {
 // Times `reps` applies of one launch configuration on scratch vectors.
 int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps, int32_t reps,
                       float* us) {
-  if (!op || !us || reps < 1 || kernel < 0 || kernel > 5) return LFX_INVALID_ARGUMENT;
+  if (!op || !us || reps < 1 || kernel < 0 || kernel > 6) return LFX_INVALID_ARGUMENT;
   lfx_ctx* ctx = op->ctx;
   const lfx_lma_layout* L = op->lay;
   TmaShape ts;
@@ -2092,6 +2497,12 @@ int lfx_op_time_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps,
     if (!cells_ok(op) || !cells_stages_ok(op, stages))
       return fail(ctx, LFX_NOT_SUPPORTED, "cell scatter does not fit this operator");
     ts.stages = stages;
+  }
+  if (kernel == 6) {
+    if (!ring_ok(op, stages, warps))
+      return fail(ctx, LFX_NOT_SUPPORTED, "persistent cell scatter does not fit this operator");
+    ts.stages = stages;
+    ts.warps = warps;
   }
   const size_t esz = op->precision == LFX_R64 ? 8 : 4;
   // consecutive applies take different x and y (enough pairs to hold twice
@@ -2156,6 +2567,7 @@ int lfx_op_set_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps) 
     case 3: ok = fetch_ok(op) && (stages == 0 || stages == 1); break;
     case 4: ok = pipe_shape(op, stages, warps).warps > 0; break;
     case 5: ok = cells_ok(op) && cells_stages_ok(op, stages); break;
+    case 6: ok = ring_ok(op, stages, warps); break;
     default: return fail(ctx, LFX_INVALID_ARGUMENT, "no such apply kernel");
   }
   if (!ok) return fail(ctx, LFX_NOT_SUPPORTED, "configuration does not fit this operator");
@@ -2167,7 +2579,7 @@ int lfx_op_set_apply(lfx_op* op, int32_t kernel, int32_t stages, int32_t warps) 
 
 // Picks the fastest apply configuration for this operator by timing the
 // candidates (register gather, the prefetching gather at two register caps, the
-// cell scatter, bulk-copy
+// cell scatter per colour and as one persistent launch, bulk-copy
 // pipeline with 2..8 stages and 1..8 warps per block that fit the shared
 // memory) and keeps it for later applies.
 int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, int32_t* warps,
@@ -2195,6 +2607,9 @@ int lfx_op_autotune(lfx_op* op, int32_t reps, int32_t* kernel, int32_t* stages, 
     if (!rc && fetch_ok(op)) rc = consider(3, 1, 0);
     for (int st : {0, 2, 3})
       if (!rc && cells_ok(op) && cells_stages_ok(op, st)) rc = consider(5, st, 0);
+    for (int st : {4, 6})
+      for (int w : {4, 8})
+        if (!rc && ring_ok(op, st, w)) rc = consider(6, st, w);
   } else {
     rc = consider(2, 0, 0);
   }

@@ -808,8 +808,17 @@ __global__ void bcg_reduce(int nb, int ne, const double* __restrict__ partials,
   if (st->done) return;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= ne) return;
+  // block order, as before; eight loads in flight ahead of the additions
   double s = 0.0;
-  for (int b = 0; b < nb; ++b) s = s + partials[(size_t)b * ne + e];
+  int b = 0;
+  for (; b + 8 <= nb; b += 8) {
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = __ldg(partials + (size_t)(b + q) * ne + e);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s = s + v[q];
+  }
+  for (; b < nb; ++b) s = s + __ldg(partials + (size_t)b * ne + e);
   out[e] = s;
 }
 

@@ -397,7 +397,8 @@ class FieldVector(_Handle):
 
 # LMA apply kernels by number (lfx_op_autotune / lfx_op_set_apply)
 APPLY_KERNEL_NAMES = {0: "pipeline", 1: "register-gather", 2: "generic",
-                      3: "register-gather-prefetch", 4: "staged-pipeline", 5: "cell-scatter"}
+                      3: "register-gather-prefetch", 4: "staged-pipeline", 5: "cell-scatter",
+                      6: "cell-scatter-persistent"}
 
 
 class LmaOperator(_Handle):

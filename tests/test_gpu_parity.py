@@ -153,7 +153,7 @@ def test_lma_apply_w2_bitwise(ctx, n, nl):
     assert same(sysd.diag.export_field(), op.diagonal())
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 3, 4, 5])
+@pytest.mark.parametrize("kernel", [0, 1, 3, 4, 5, 6])
 @pytest.mark.parametrize("space,n,nl,prec", [("w0", 6, 5, 64), ("w2", 8, 7, 64), ("w2", 8, 7, 32),
                                              ("w2", 12, 30, 64), ("w0", 5, 21, 32),
                                              ("w2", 6, 40, 64), ("w2", 7, 33, 32)])
@@ -204,12 +204,12 @@ def test_cell_scatter_nonsymmetric(ctx, prec, space):
     X = lfx.FieldVector.from_array(ctx, x, prec)
     Y = lfx.FieldVector(ctx, [p.undf], prec)
     got = {}
-    for k, st in ((5, 0), (5, 2), (5, 3), (1, 0)):
-        op.set_apply(k, st)
+    for k, st, w in ((5, 0, 0), (5, 2, 0), (5, 3, 0), (1, 0, 0), (6, 4, 4)):
+        op.set_apply(k, st, w)
         op.apply(X, Y)
         got[(k, st)] = Y.export_field()
-    for st in (0, 2, 3):
-        assert same(got[(5, st)], got[(1, 0)])
+    for k, st in ((5, 0), (5, 2), (5, 3), (6, 4)):
+        assert same(got[(k, st)], got[(1, 0)])
     if prec == 64:
         oop = orc.LmaOperator(p.ncell_2d, 9, p.ndf, p.ndf, p.map, p.map, p.undf, p.undf, lma,
                               npc, cic)
@@ -237,6 +237,18 @@ def test_cell_scatter_stages_symmetric(ctx, space, n, nl, prec):
         Y.set_scalar(7.0)
         op.apply(X, Y)
         assert same(Y.export_field(), ref)
+    # the persistent form in every ring shape that fits (at least one does)
+    ran = 0
+    for st, w in ((4, 4), (4, 8), (6, 4), (6, 8)):
+        if op.time_apply(6, st, w, reps=1) is None:
+            continue
+        op.set_apply(6, st, w)
+        Y.set_scalar(7.0)
+        op.apply(X, Y)
+        ctx.check_device_error()
+        assert same(Y.export_field(), ref), (st, w)
+        ran += 1
+    assert ran >= 1
 
 
 @pytest.mark.parametrize("space,n,nl", [("w2", 5, 32), ("w2", 4, 40), ("w0", 4, 63),
@@ -288,18 +300,23 @@ def test_cell_scatter_long_columns_in_gmres(ctx):
     assert same(X.export_field(), x_o)
 
 
-def test_cell_scatter_in_gmres(ctx):
+@pytest.mark.parametrize("kernel", [5, 6])
+def test_cell_scatter_in_gmres(ctx, kernel):
+    """A W2 GMRES solve with every apply (plain and residual form) through the
+    cell scatter, per colour or as one persistent launch, equals the oracle's
+    solve bit for bit."""
     p = mg.w2_problem(16, 12, seed=2)
     sysd = wl.device_w2(ctx, p)
     op = o_lma(p)
     oprec, _ = o_w2_prec(p, op)
     x_o, info_o = orc.solve("gmres", op, oprec, p.rhs, r_tol=1e-8, a_tol=1e-16, max_iter=200,
                             gcrk=10)
-    ctx.set_apply_kernel(5)
+    ctx.set_apply_kernel(kernel)
     try:
         g = lfx.GMRES(sysd.op, sysd.prec, 10, 1e-8, 1e-16, 200)
         X, B = sysd.vector(), sysd.vector(p.rhs)
         info = g.apply(X, B)
+        ctx.check_device_error()
     finally:
         ctx.set_apply_kernel(-1)
     assert info.converged and info.iterations == info_o.iterations
@@ -332,7 +349,8 @@ def test_autotune_keeps_results(ctx):
     choice = op.autotune(reps=3)
     assert choice["us"] > 0 and choice["kernel"] in ("pipeline", "register-gather",
                                                      "register-gather-prefetch",
-                                                     "staged-pipeline")
+                                                     "staged-pipeline", "cell-scatter",
+                                                     "cell-scatter-persistent")
     op.apply(X, Y)
     assert same(Y.export_field(), o_lma(p).apply(x))
 

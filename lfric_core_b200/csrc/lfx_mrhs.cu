@@ -1015,7 +1015,18 @@ __global__ void __launch_bounds__(256) bcg_update_s(int64_t n, const float* __re
   if (threadIdx.x == 0)
     for (int i = 0; i < S && i < nmine; ++i)
       chunk_issue<NA>(src, blockIdx.x + (int64_t)i * gridDim.x, n, ring_smem + i * RG::STAGE, bar + i);
-  const int r0 = 2 * (threadIdx.x / 16), c0 = 4 * (threadIdx.x % 16);
+  // thread: column c of the output for the 8 rows 8 rg .. 8 rg + 7 of each
+  // chunk, with column c of the coefficients in registers; the operand rows
+  // are read four values at a time, every lane of a warp at the same address
+  // (one shared-memory wavefront). Each output is one fmaf chain over
+  // k = 0..63, as before the tiling changed.
+  const int c = 32 * ((threadIdx.x >> 5) & 1) + (threadIdx.x & 31), rg = threadIdx.x >> 6;
+  float cr[kBS];
+  __syncthreads();  // Cs is written
+#pragma unroll
+  for (int k = 0; k < kBS; ++k) cr[k] = Cs[k][c];
+  // the squared-residual sums of row pairs 4 rg + i, in the order of the
+  // earlier two-rows-a-thread form (row 2q, then 2q + 1, chunk by chunk)
   double nrm[4] = {0.0, 0.0, 0.0, 0.0};
   for (int i = 0; i < nmine; ++i) {
     const int stg = i % S;
@@ -1025,46 +1036,53 @@ __global__ void __launch_bounds__(256) bcg_update_s(int64_t n, const float* __re
       chunk_ring_drain<S>(bar, i, nmine < i + S ? nmine : i + S);
       break;
     }
-    const int64_t c = blockIdx.x + (int64_t)i * gridDim.x, row0 = c * kBcgRows;
+    const int64_t ch = blockIdx.x + (int64_t)i * gridDim.x, row0 = ch * kBcgRows;
     const int rows = (int)(n - row0 < (int64_t)kBcgRows ? n - row0 : (int64_t)kBcgRows);
     const unsigned char* stage = ring_smem + stg * RG::STAGE;
     const float (*As0)[kBS] = reinterpret_cast<const float (*)[kBS]>(stage);
     const float (*As1)[kBS] = reinterpret_cast<const float (*)[kBS]>(stage + kChunkBytes);
-#pragma unroll
-    for (int rr = 0; rr < 2; ++rr) {
-      const int r = r0 + rr;
-      if (r >= rows) continue;
-      const size_t o = (size_t)(row0 + r) * kBS + c0;
-      float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int i8 = 0; i8 < 8; ++i8) {
+      const int r = 8 * rg + i8;
+      if (r >= rows) break;
+      const size_t o = (size_t)(row0 + r) * kBS + c;
+      float d0 = 0.f, d1 = 0.f;
       if (!skip_p) {
-#pragma unroll 8
-        for (int k = 0; k < kBS; ++k) {
-          const float4 cf = *reinterpret_cast<const float4*>(&Cs[k][c0]);
-          const float a0 = As0[r][k];
-          d0[0] = fmaf(a0, cf.x, d0[0]); d0[1] = fmaf(a0, cf.y, d0[1]);
-          d0[2] = fmaf(a0, cf.z, d0[2]); d0[3] = fmaf(a0, cf.w, d0[3]);
+#pragma unroll
+        for (int k = 0; k < kBS; k += 4) {
+          const float4 a0 = *reinterpret_cast<const float4*>(&As0[r][k]);
+          d0 = fmaf(a0.x, cr[k], d0);
+          d0 = fmaf(a0.y, cr[k + 1], d0);
+          d0 = fmaf(a0.z, cr[k + 2], d0);
+          d0 = fmaf(a0.w, cr[k + 3], d0);
           if (MODE == 0) {
-            const float a1 = As1[r][k];
-            d1[0] = fmaf(a1, cf.x, d1[0]); d1[1] = fmaf(a1, cf.y, d1[1]);
-            d1[2] = fmaf(a1, cf.z, d1[2]); d1[3] = fmaf(a1, cf.w, d1[3]);
+            const float4 a1 = *reinterpret_cast<const float4*>(&As1[r][k]);
+            d1 = fmaf(a1.x, cr[k], d1);
+            d1 = fmaf(a1.y, cr[k + 1], d1);
+            d1 = fmaf(a1.z, cr[k + 2], d1);
+            d1 = fmaf(a1.w, cr[k + 3], d1);
           }
         }
       }
       if (MODE == 0) {
-        const float4 x = *reinterpret_cast<const float4*>(stage + 2 * kChunkBytes + (r * kBS + c0) * 4);
-        const float4 rv = *reinterpret_cast<const float4*>(stage + 3 * kChunkBytes + (r * kBS + c0) * 4);
-        st4(Y0 + o, make_float4(x.x + d0[0], x.y + d0[1], x.z + d0[2], x.w + d0[3]));
-        const float rn[4] = {rv.x - d1[0], rv.y - d1[1], rv.z - d1[2], rv.w - d1[3]};
-        st4(Y1 + o, make_float4(rn[0], rn[1], rn[2], rn[3]));
-#pragma unroll
-        for (int j = 0; j < 4; ++j) nrm[j] = fma((double)rn[j], (double)rn[j], nrm[j]);
+        const float x = reinterpret_cast<const float*>(stage + 2 * kChunkBytes)[r * kBS + c];
+        const float rv = reinterpret_cast<const float*>(stage + 3 * kChunkBytes)[r * kBS + c];
+        Y0[o] = x + d0;
+        const float rn = rv - d1;
+        Y1[o] = rn;
+        const double rd = (double)rn;
+        switch (i8 >> 1) {
+          case 0: nrm[0] = fma(rd, rd, nrm[0]); break;
+          case 1: nrm[1] = fma(rd, rd, nrm[1]); break;
+          case 2: nrm[2] = fma(rd, rd, nrm[2]); break;
+          default: nrm[3] = fma(rd, rd, nrm[3]); break;
+        }
       } else if (MODE == 1) {
-        const float4 rv = *reinterpret_cast<const float4*>(&As1[r][c0]);
+        const float rv = As1[r][c];
         const float dv = __ldg(dinv + row0 + r);
-        st4(Y0 + o, make_float4(fmaf(rv.x, dv, d0[0]), fmaf(rv.y, dv, d0[1]),
-                                fmaf(rv.z, dv, d0[2]), fmaf(rv.w, dv, d0[3])));
+        Y0[o] = fmaf(rv, dv, d0);
       } else {
-        st4(Y0 + o, make_float4(d0[0], d0[1], d0[2], d0[3]));
+        Y0[o] = d0;
       }
     }
     __syncthreads();  // the stage is read: it takes chunk i + S
@@ -1078,7 +1096,7 @@ __global__ void __launch_bounds__(256) bcg_update_s(int64_t n, const float* __re
     __syncthreads();
     double (*red)[kBS] = reinterpret_cast<double (*)[kBS]>(ring_smem);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) red[threadIdx.x / 16][c0 + j] = nrm[j];
+    for (int j = 0; j < 4; ++j) red[4 * rg + j][c] = nrm[j];
     __syncthreads();
     if (threadIdx.x < kBS) {
       double s = 0.0;

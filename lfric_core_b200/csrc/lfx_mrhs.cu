@@ -891,7 +891,7 @@ __device__ __forceinline__ void chunk_ring_drain(uint64_t* bar, int from, int to
 }
 
 template <int NV>
-__global__ void __launch_bounds__(256) bcg_gram_s(int64_t n, const float* __restrict__ U,
+__global__ void __launch_bounds__(256, 2) bcg_gram_s(int64_t n, const float* __restrict__ U,
                                                   const float* __restrict__ V0,
                                                   const float* __restrict__ V1,
                                                   const float* __restrict__ vscale,
@@ -939,10 +939,17 @@ __global__ void __launch_bounds__(256) bcg_gram_s(int64_t n, const float* __rest
       for (int x = 0; x < 4; ++x)
 #pragma unroll
         for (int y = 0; y < 4; ++y) a[v][x][y] = 0.f;
+    // the row scales of this chunk: one load a lane, then shuffles (the
+    // two-operand form measured faster this way; the one-operand form keeps
+    // a load per row)
+    const int lane = threadIdx.x & 31;
+    const float sc_lane = (NV == 2 && vscale && lane < rows) ? __ldg(vscale + row0 + lane) : 1.f;
     for (int r = 0; r < rows; ++r) {
       const float4 u = *reinterpret_cast<const float4*>(&Us[r][i0]);
       const float uu[4] = {u.x, u.y, u.z, u.w};
-      const float sc = vscale ? __ldg(vscale + row0 + r) : 1.f;
+      const float sc = !vscale ? 1.f
+                       : NV == 2 ? __shfl_sync(0xffffffffu, sc_lane, r)
+                                 : __ldg(vscale + row0 + r);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         const float (*Vs)[kBS] =
@@ -1041,6 +1048,35 @@ __global__ void __launch_bounds__(256) bcg_update_s(int64_t n, const float* __re
     const unsigned char* stage = ring_smem + stg * RG::STAGE;
     const float (*As0)[kBS] = reinterpret_cast<const float (*)[kBS]>(stage);
     const float (*As1)[kBS] = reinterpret_cast<const float (*)[kBS]>(stage + kChunkBytes);
+    if (MODE == 1 && rows == kBcgRows) {
+      // a full chunk: the thread's 8 rows with their fmaf chains
+      // interleaved (independent chains, each still over k = 0..63 in
+      // order; measured faster for this mode only)
+      const int rb = 8 * rg;
+      float d[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) d[q] = 0.f;
+      if (!skip_p) {
+#pragma unroll
+        for (int k = 0; k < kBS; k += 4) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const float4 a0 = *reinterpret_cast<const float4*>(&As0[rb + q][k]);
+            d[q] = fmaf(a0.x, cr[k], d[q]);
+            d[q] = fmaf(a0.y, cr[k + 1], d[q]);
+            d[q] = fmaf(a0.z, cr[k + 2], d[q]);
+            d[q] = fmaf(a0.w, cr[k + 3], d[q]);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int r = rb + q;
+        const float rv = As1[r][c];
+        const float dv = __ldg(dinv + row0 + r);
+        Y0[(size_t)(row0 + r) * kBS + c] = fmaf(rv, dv, d[q]);
+      }
+    } else
 #pragma unroll 1
     for (int i8 = 0; i8 < 8; ++i8) {
       const int r = 8 * rg + i8;

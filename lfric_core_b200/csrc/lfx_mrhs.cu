@@ -1244,25 +1244,30 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
     if (mode == 0) {
       // Cholesky of the r x r active block of P^T Q (column by column)
       for (int e = t; e < kBS * kBS; e += blockDim.x) M[e / kBS][e % kBS] = st->C[e];
-      if (t == 0) s_stop = 0;
       __syncthreads();
+      // two barriers a step: every thread takes the pivot's root from the
+      // diagonal itself (written back only in the update phase, which does
+      // not read it), the column is divided, then the trailing triangle is
+      // updated by a 16 x 16 thread grid (no index division)
+      const int ti = t >> 4, tj = t & 15;
+      bool stop = false;
       for (int k = 0; k < r; ++k) {
-        if (t == 0) {
-          const double d = M[k][k];
-          if (!(d > 0.0)) s_stop = 1;
-          M[k][k] = d > 0.0 ? sqrt(d) : 1.0;
+        const double d = M[k][k];
+        if (!(d > 0.0)) {
+          stop = true;  // every thread reads the same d
+          break;
         }
+        const double sk = sqrt(d);
+        for (int i = k + 1 + t; i < r; i += blockDim.x) M[i][k] /= sk;
         __syncthreads();
-        if (s_stop) break;
-        for (int i = k + 1 + t; i < r; i += blockDim.x) M[i][k] /= M[k][k];
-        __syncthreads();
-        for (int e = t; e < (r - k - 1) * (r - k - 1); e += blockDim.x) {
-          const int i = k + 1 + e / (r - k - 1), j = k + 1 + e % (r - k - 1);
-          if (j <= i) M[i][j] -= M[i][k] * M[j][k];
+        if (t == 0) M[k][k] = sk;
+        for (int i = k + 1 + ti; i < r; i += 16) {
+          const double lik = M[i][k];
+          for (int j = k + 1 + tj; j <= i; j += 16) M[i][j] -= lik * M[j][k];
         }
         __syncthreads();
       }
-      if (s_stop) {
+      if (stop) {
         if (t == 0) { st->fail = 1; st->done = 1; }
         return;
       }
@@ -1318,6 +1323,7 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
   __syncthreads();
   double dmax = 0.0;
   for (int i = 0; i < kBS; ++i) dmax = fmax(dmax, M[i][i]);
+  const int ti = t >> 4, tj = t & 15;
   for (int k = 0; k < kBS; ++k) {
     if (t < 32) {
       // lane l looks at steps k + l and k + l + 32
@@ -1351,10 +1357,15 @@ __global__ void __launch_bounds__(256) bcg_small(int mode, BcgSmall* st, double 
     const int pk = perm[k];
     for (int i = k + 1 + t; i < kBS; i += blockDim.x) M[perm[i]][pk] /= M[pk][pk];
     __syncthreads();
+    // the trailing square by a 16 x 16 thread grid (no index division)
     const int m = kBS - k - 1;
-    for (int e = t; e < m * m; e += blockDim.x) {
-      const int pi = perm[k + 1 + e / m], pj = perm[k + 1 + e % m];
-      M[pi][pj] -= M[pi][pk] * M[pj][pk];
+    for (int a = ti; a < m; a += 16) {
+      const int pi = perm[k + 1 + a];
+      const double lik = M[pi][pk];
+      for (int b = tj; b < m; b += 16) {
+        const int pj = perm[k + 1 + b];
+        M[pi][pj] -= lik * M[pj][pk];
+      }
     }
     __syncthreads();
   }

@@ -80,7 +80,11 @@ struct SweepCol {                             // a warp's columns, per lane
   float* z[32];
   int f[32], nrow[32];
 };
-constexpr size_t kSweepWarpBytes = sizeof(float) * kSwCh * kSwLd + sizeof(SweepCol);
+// per warp: the tile, the column table, then two buffers of the factors of a
+// chunk (two arrays of kSwCh x 32 each)
+constexpr size_t kSweepTileBytes = sizeof(float) * kSwCh * kSwLd;
+constexpr size_t kSweepFacBytes = sizeof(float) * 2 * 2 * kSwCh * 32;
+constexpr size_t kSweepWarpBytes = kSweepTileBytes + sizeof(SweepCol) + kSweepFacBytes;
 constexpr size_t kSweepBytes = kBW * kSweepWarpBytes;
 
 inline int64_t bchunks(int64_t n) {
@@ -849,16 +853,26 @@ __device__ __noinline__ void vec_phase(const BParams& P, BShared& sh, Pred pred,
 // [row][column] (coalesced across the lanes of one slot). The forward sweep
 // leaves its values in z (FP32), the backward sweep reads them back; the
 // arithmetic of thomas_sweep (FP64 carries, FP32 rows between the sweeps).
+// 4-byte asynchronous copy of a read-only factor (zeros when !on)
+__device__ __forceinline__ void sweep_fac_copy(float* dst, const float* src, bool on) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(su32(dst)), "l"(src),
+               "r"(on ? 4 : 0)
+               : "memory");
+}
+
 __device__ __noinline__ void sweep_phase_w(const BParams& P, unsigned char* wsm) {
   float (*tile)[kSwLd] = reinterpret_cast<float (*)[kSwLd]>(wsm);
-  SweepCol& sc = *reinterpret_cast<SweepCol*>(wsm + sizeof(float) * kSwCh * kSwLd);
+  SweepCol& sc = *reinterpret_cast<SweepCol*>(wsm + kSweepTileBytes);
+  float* facb = reinterpret_cast<float*>(wsm + kSweepTileBytes + sizeof(SweepCol));
   const int lane = threadIdx.x & 31;
   const int gw = blockIdx.x * kBW + (threadIdx.x >> 5), nw = gridDim.x * kBW;
+  // a valid address for the copies that read nothing
+  const float* dummy = reinterpret_cast<const float*>(P.cols);
   for (int u0 = gw * 32; u0 < P.ncolitem; u0 += nw * 32) {
     // this lane's column
     const int u = u0 + lane;
     int nrow = 0, nc = 1, c = 0;
-    const float *fa = nullptr, *finv = nullptr, *fc = nullptr;
+    const float *fa = dummy, *finv = dummy, *fc = dummy;
     __syncwarp();
     sc.nrow[lane] = 0;
     if (u < P.ncolitem) {
@@ -884,48 +898,97 @@ __device__ __noinline__ void sweep_phase_w(const BParams& P, unsigned char* wsm)
     __syncwarp();
     if (maxrow == 0) continue;
     // staging: lane = (column offset, row in the chunk); 32 / kSwCh columns
-    // an instruction
-    constexpr int CPI = 32 / kSwCh;
+    // an instruction. The next chunk's rows (into registers, through L2:
+    // other phases write r) and factors (into the other factor buffer, by
+    // 4-byte cp.async: read-only) are in flight while a chunk is swept.
+    constexpr int CPI = 32 / kSwCh, NG = 32 / CPI;
     const int hr = lane % kSwCh, hc = lane / kSwCh;
-    // forward: d_i = finv_i (r_i - fa_i d_{i-1}), left in z
-    double d = 0.0;
-    for (int i0 = 0; i0 < maxrow; i0 += kSwCh) {
+    auto fac = [&](int buf, int kind, int q) -> float* {
+      return facb + ((buf * 2 + kind) * kSwCh + q) * 32 + lane;
+    };
+    auto gather = [&](const float* const* base, int i0, float (&v)[NG]) {
+      const int i = i0 + hr;
+#pragma unroll
+      for (int m = 0; m < NG; ++m) {
+        const int j = hc + CPI * m;
+        v[m] = i < sc.nrow[j] ? __ldcg(base[j] + sc.f[j] + __ldg(sc.ind[j] + i)) : 0.f;
+      }
+    };
+    auto stage = [&](int i0, const float (&v)[NG]) {
+      const int i = i0 + hr;
+#pragma unroll
+      for (int m = 0; m < NG; ++m) {
+        const int j = hc + CPI * m;
+        if (i < sc.nrow[j]) tile[hr][j] = v[m];
+      }
+    };
+    auto store = [&](int i0) {
       const int i = i0 + hr;
       for (int j = hc; j < 32; j += CPI)
-        if (i < sc.nrow[j]) tile[hr][j] = __ldcg(sc.r[j] + sc.f[j] + __ldg(sc.ind[j] + i));
-      float iv[kSwCh], av[kSwCh];
+        if (i < sc.nrow[j]) __stcg(sc.z[j] + sc.f[j] + __ldg(sc.ind[j] + i), tile[hr][j]);
+    };
+    float pv[NG];
+    // forward: d_i = finv_i (r_i - fa_i d_{i-1}), left in z
+    auto fwd_fac = [&](int i0, int buf) {
 #pragma unroll
       for (int q = 0; q < kSwCh; ++q) {
         const int ii = i0 + q;
-        iv[q] = ii < nrow ? __ldg(finv + (size_t)ii * nc + c) : 0.f;
-        av[q] = ii < nrow ? __ldg(fa + (size_t)ii * nc + c) : 0.f;
+        const bool on = ii < nrow;
+        sweep_fac_copy(fac(buf, 0, q), on ? finv + (size_t)ii * nc + c : dummy, on);
+        sweep_fac_copy(fac(buf, 1, q), on ? fa + (size_t)ii * nc + c : dummy, on);
       }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    double d = 0.0;
+    gather(sc.r, 0, pv);
+    fwd_fac(0, 0);
+    int buf = 0;
+    for (int i0 = 0; i0 < maxrow; i0 += kSwCh, buf ^= 1) {
+      stage(i0, pv);
+      if (i0 + kSwCh < maxrow) {
+        gather(sc.r, i0 + kSwCh, pv);
+        fwd_fac(i0 + kSwCh, buf ^ 1);
+      } else {
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      }
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < kSwCh; ++q) {
         const int ii = i0 + q;
         if (ii < nrow) {
+          const double iv = (double)*fac(buf, 0, q), av = (double)*fac(buf, 1, q);
           const double xv = (double)tile[q][lane];
-          d = (ii == 0) ? (double)iv[q] * xv : (double)iv[q] * fma(-(double)av[q], d, xv);
+          d = (ii == 0) ? iv * xv : iv * fma(-av, d, xv);
           tile[q][lane] = (float)d;
         }
       }
       __syncwarp();
-      for (int j = hc; j < 32; j += CPI)
-        if (i < sc.nrow[j]) __stcg(sc.z[j] + sc.f[j] + __ldg(sc.ind[j] + i), tile[hr][j]);
+      store(i0);
       __syncwarp();
     }
     // backward: z_i = d_i - fc_i z_{i+1}, rows nrow - 2 .. 0, chunks from the top
-    for (int i0 = ((maxrow - 1) / kSwCh) * kSwCh; i0 >= 0; i0 -= kSwCh) {
-      const int i = i0 + hr;
-      for (int j = hc; j < 32; j += CPI)
-        if (i < sc.nrow[j]) tile[hr][j] = __ldcg(sc.z[j] + sc.f[j] + __ldg(sc.ind[j] + i));
-      float cv[kSwCh];
+    auto bwd_fac = [&](int i0, int b2) {
 #pragma unroll
       for (int q = 0; q < kSwCh; ++q) {
         const int ii = i0 + q;
-        cv[q] = ii < nrow - 1 ? __ldg(fc + (size_t)ii * nc + c) : 0.f;
+        const bool on = ii < nrow - 1;
+        sweep_fac_copy(fac(b2, 0, q), on ? fc + (size_t)ii * nc + c : dummy, on);
       }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int top = ((maxrow - 1) / kSwCh) * kSwCh;
+    gather(sc.z, top, pv);
+    bwd_fac(top, buf);
+    for (int i0 = top; i0 >= 0; i0 -= kSwCh, buf ^= 1) {
+      stage(i0, pv);
+      if (i0 - kSwCh >= 0) {
+        gather(sc.z, i0 - kSwCh, pv);
+        bwd_fac(i0 - kSwCh, buf ^ 1);
+      } else {
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      }
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
       __syncwarp();
 #pragma unroll
       for (int q = kSwCh - 1; q >= 0; --q) {
@@ -933,15 +996,16 @@ __device__ __noinline__ void sweep_phase_w(const BParams& P, unsigned char* wsm)
         if (ii == nrow - 1) {
           d = (double)tile[q][lane];
         } else if (ii < nrow - 1) {
-          d = fma(-(double)cv[q], d, (double)tile[q][lane]);
+          d = fma(-(double)*fac(buf, 0, q), d, (double)tile[q][lane]);
           tile[q][lane] = (float)d;
         }
       }
       __syncwarp();
-      for (int j = hc; j < 32; j += CPI)
-        if (i < sc.nrow[j]) __stcg(sc.z[j] + sc.f[j] + __ldg(sc.ind[j] + i), tile[hr][j]);
+      store(i0);
       __syncwarp();
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
   }
 }
 

@@ -283,7 +283,7 @@ __host__ __device__ constexpr int pcol(int p) {
 // starts from zero, later ones from the stored sum, and in the residual form
 // the last writes b - sum. With DOT the lane returns the sum of p_i y_i over
 // the dofs it finished (the last writer of each dof).
-template <class T, int NDF, bool RESID, bool DOT>
+template <class T, int NDF, bool RESID, bool DOT, bool CANON>
 __device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const int* __restrict__ dsc,
                                                int nl, int L, int sg, int lane,
                                                const T* x, T* y, const double* __restrict__ b) {
@@ -305,7 +305,7 @@ __device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const i
   for (int j = 0; j < NDF; ++j) xv[j] = v ? __ldcg(x + mf[j] + k) : T(0);
 #pragma unroll
   for (int df = 0; df < NDF; ++df) {
-    const bool lower = (flags >> (8 + df)) & 1u, upper = (flags >> (16 + df)) & 1u;
+    const bool lower = is_lower<NDF, CANON>(flags, df), upper = is_upper<NDF, CANON>(flags, df);
     const bool opens = (flags >> df) & 1u;
     const bool live = own && (lower ? k <= nl : v);
     yo[df] = (!upper && !opens && live) ? __ldcg(y + mf[df] + k) : T(0);
@@ -314,10 +314,10 @@ __device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const i
 #define MV(i, j) m[pidx<NDF>(i, j)]
 #pragma unroll
   for (int df = 0; df < NDF; ++df) {
-    if ((flags >> (16 + df)) & 1u) continue;  // upper record: summed with its lower one
+    if (is_upper<NDF, CANON>(flags, df)) continue;  // upper record: summed with its lower one
     const bool last = (flags >> (24 + df)) & 1u;
-    if ((flags >> (8 + df)) & 1u) {
-      const int bsel = (part >> (4 * df)) & 15u;
+    if (is_lower<NDF, CANON>(flags, df)) {
+      const int bsel = partner<NDF, CANON>(part, df);
 #pragma unroll
       for (int bb = df + 1; bb < NDF; ++bb) {
         if (bb != bsel) continue;
@@ -357,6 +357,14 @@ __device__ __forceinline__ double scatter_unit(const T* __restrict__ Mq, const i
   }
 #undef MV
   return dot;
+}
+// one form per pair structure, each its own function (the apply phase keeps
+// one register allocation for both)
+template <class T, int NDF, bool FP64, bool CANON>
+__device__ __noinline__ double scatter_unit_c(const T* __restrict__ Mq, const int* __restrict__ dsc,
+                                              int nl, int L, int sg, int lane, const T* x, T* y,
+                                              const double* __restrict__ b) {
+  return scatter_unit<T, NDF, FP64, !FP64, CANON>(Mq, dsc, nl, L, sg, lane, x, y, b);
 }
 
 // The apply items [i0, i1) of one (group, colour) phase, one warp per item
@@ -400,8 +408,12 @@ __device__ __noinline__ void apply_phase(const BParams& P, const int4* __restric
       const int q = q0 + c;
       double dot = 0.0;
       for (int sg = 0; sg < nseg; ++sg)
-        dot += scatter_unit<T, NDF, FP64, !FP64>(M + (size_t)q * sblk, cdesc + (size_t)q * cdints,
-                                                 nl, L, sg, lane, x, y, bb);
+        dot += D->canon ? scatter_unit_c<T, NDF, FP64, true>(M + (size_t)q * sblk,
+                                                             cdesc + (size_t)q * cdints, nl, L, sg,
+                                                             lane, x, y, bb)
+                        : scatter_unit_c<T, NDF, FP64, false>(M + (size_t)q * sblk,
+                                                              cdesc + (size_t)q * cdints, nl, L,
+                                                              sg, lane, x, y, bb);
       if (!FP64) {
         const double w = warp_butterfly(dot);
         if (lane == 0) __stcg(part + q, w);

@@ -446,7 +446,8 @@ typedef struct {
  * shape on the admitted slots (these replays advance the solves, which do not
  * depend on the shape) -- blocks per SM, then 1/2/4/8 columns per item,
  * then L2 groups of a quarter, half, all of L2 or one group -- and keeps the
- * fastest. */
+ * fastest. A trial with no running slot measures nothing and is not chosen
+ * (step the batch once after admitting, so the slots are running). */
 int lfx_batch_autotune(lfx_batch* b, int32_t iters, lfx_batch_tuning* out);
 int lfx_batch_get_tuning(const lfx_batch* b, lfx_batch_tuning* out);
 /* pin a launch shape (cells_per_item 1 to 8) */

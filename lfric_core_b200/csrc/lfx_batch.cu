@@ -2004,7 +2004,8 @@ int lfx_batch_autotune(lfx_batch* B, int32_t iters, lfx_batch_tuning* out) {
       B->dirty = true;
       rc = trial(&t);
       if (rc) break;
-      if (best == 0.f || t < best) {
+      // a trial with no running slot measured nothing: it cannot win
+      if (t > 0.f && (best == 0.f || t < best)) {
         best = t;
         if (stage == 0) bb = (int)c;
         if (stage == 1) bc = (int)c;
